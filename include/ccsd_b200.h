@@ -1,0 +1,203 @@
+/*
+ * ccsd_b200.h -- C ABI of the B200 engine for the CCSD amplitude iteration.
+ *
+ * The engine replaces, for one GPU, the tensor leaf and the irrep-block loop
+ * under the reference's indexed-tensor interface
+ *   (src/tensor/indexable_tensor.hpp:133-155: mult/sum/scale/dot;
+ *    src/tensor/spinorbital_tensor.cxx:455-1109: spin-orbital semantics;
+ *    src/tensor/symblocked_tensor.cxx:863-1395: irrep-block loop;
+ *    src/tensor/ctf_tensor.cxx:402-514: leaf norm/mult/sum/scale/dot/weight)
+ * plus the CCSD iteration driver around it
+ *   (src/cc/ccsd.cxx:29-193, src/util/iterative.hpp:126-188,
+ *    src/convergence/diis.hpp:70-227, src/operator/denominator.hpp:14-95).
+ *
+ * Conventions
+ *  - Every entry point returns an int status (CCSD_OK = 0); no exception ever
+ *    crosses the ABI.  ccsd_last_error() gives a message for the last failure
+ *    on a context.
+ *  - Spin-orbital tensors follow the reference's SpinorbitalTensor layout:
+ *    index positions are ordered [upper vrt, upper occ, lower vrt, lower occ]
+ *    (spaces {vrt, occ}, src/operator/2eoperator.cxx:13-21); a spin case is
+ *    the number of alpha indices in each of those four groups, alpha indices
+ *    first inside a group (src/tensor/spinorbital_tensor.cxx:387-432).
+ *  - Within a spin case, blocks are irrep tuples whose XOR is 0 (Abelian
+ *    groups C1, C2, C2v/D2 type, D2h: 1, 2, 4 or 8 irreps).
+ *  - Dense block storage puts the FIRST index fastest, as the reference's key
+ *    convention does (src/tensor/ctf_tensor.hpp:221-226), so a key is the
+ *    linear offset inside its block.  Antisymmetric same-spin pairs are stored
+ *    unpacked (both orders), except in tensors created CCSD_TENSOR_PACKED,
+ *    which store each same-spin pair of a group once (first index < second).
+ *  - All calls on a context are ordered on its CUDA stream.  A context is not
+ *    thread-safe; several contexts may share a device.
+ */
+#ifndef CCSD_B200_H
+#define CCSD_B200_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+    CCSD_OK              = 0,
+    CCSD_ERR_ARG         = 1,   /* bad argument / unknown handle / bad index string */
+    CCSD_ERR_CUDA        = 2,   /* a CUDA runtime call failed */
+    CCSD_ERR_OOM         = 3,   /* device allocation failed or admission refused */
+    CCSD_ERR_PLAN        = 4,   /* contraction pattern not supported by the planner */
+    CCSD_DIVERGED        = 5,   /* NaN/Inf or runaway residual detected */
+    CCSD_NOT_CONVERGED   = 6,   /* max_iter reached without conv < conv_tol */
+    CCSD_ERR_SINGULAR    = 7,   /* DIIS system singular after the eps retry (diis.hpp:187) */
+    CCSD_ERR_TIMEOUT     = 8,   /* a bounded device wait gave up */
+    CCSD_ERR_UNSUPPORTED = 9
+};
+
+typedef struct ccsd_ctx_s* ccsd_ctx;
+typedef int32_t ccsd_tensor;          /* tensor handle, > 0 */
+typedef struct ccsd_solver_s* ccsd_solver;
+
+/* precision of the contraction layer */
+enum {
+    CCSD_PREC_FP64  = 0,   /* native FP64 GEMMs (plain path) */
+    CCSD_PREC_SPLIT = 1    /* split BF16 slices on tcgen05, FP32 accumulate, summed in FP64 */
+};
+
+/* tensor creation flags */
+enum {
+    CCSD_TENSOR_PACKED = 1   /* store same-spin antisymmetric pairs once (i<j) */
+};
+
+/* ---- context ------------------------------------------------------------ */
+/* stream: a cudaStream_t, or NULL to let the context create its own */
+int ccsd_ctx_create(int device, void* stream, ccsd_ctx* out);
+int ccsd_ctx_destroy(ccsd_ctx ctx);
+const char* ccsd_last_error(ccsd_ctx ctx);
+int ccsd_ctx_synchronize(ccsd_ctx ctx);
+/* bytes currently held on the device by this context */
+int ccsd_ctx_device_bytes(ccsd_ctx ctx, int64_t* bytes);
+/* number of engine kernels launched on this context since creation */
+int ccsd_ctx_launch_count(ccsd_ctx ctx, int64_t* count);
+/* precision used by subsequent ccsd_contract calls (CCSD_PREC_*); slices=0: default */
+int ccsd_ctx_set_precision(ccsd_ctx ctx, int precision, int slices);
+
+/* Orbital spaces (Space of src/operator/space.hpp): per-irrep counts of
+ * alpha/beta virtual and occupied orbitals.  nirrep in {1,2,4,8}. */
+int ccsd_ctx_set_spaces(ccsd_ctx ctx, int nirrep,
+                        const int* vrt_alpha, const int* vrt_beta,
+                        const int* occ_alpha, const int* occ_beta);
+
+/* ---- tensors ------------------------------------------------------------ */
+/* nout[2], nin[2]: number of upper / lower indices in {vrt, occ}
+ * (SpinorbitalTensor ctor, src/tensor/spinorbital_tensor.cxx:166-272) */
+int ccsd_tensor_create(ccsd_ctx ctx, const char* name, const int nout[2], const int nin[2],
+                       int flags, ccsd_tensor* out);
+int ccsd_tensor_destroy(ccsd_ctx ctx, ccsd_tensor t);
+int ccsd_tensor_ndim(ccsd_ctx ctx, ccsd_tensor t, int* ndim);
+/* number of spin cases; case k has alpha counts alpha[4*k .. 4*k+3] */
+int ccsd_tensor_spin_cases(ccsd_ctx ctx, ccsd_tensor t, int* ncases, int* alpha /* 4*ncases or NULL */);
+/* element count of one block (spin case + irreps[ndim]) -- 0 if the block is not stored */
+int ccsd_tensor_block_size(ccsd_ctx ctx, ccsd_tensor t, const int alpha[4], const int* irreps, int64_t* n);
+/* whole-block dense host<->device copies (first index fastest) */
+int ccsd_tensor_write_block(ccsd_ctx ctx, ccsd_tensor t, const int alpha[4], const int* irreps,
+                            const double* host);
+int ccsd_tensor_read_block(ccsd_ctx ctx, ccsd_tensor t, const int alpha[4], const int* irreps,
+                           double* host);
+/* key/value access inside one block (tCTF_Tensor::write/read, ctf_tensor.hpp:139-247):
+ * value <- beta*value + alpha*vals[k] */
+int ccsd_tensor_write(ccsd_ctx ctx, ccsd_tensor t, const int alpha_spin[4], const int* irreps,
+                      int64_t n, const int64_t* keys, const double* vals, double alpha, double beta);
+int ccsd_tensor_read(ccsd_ctx ctx, ccsd_tensor t, const int alpha_spin[4], const int* irreps,
+                     int64_t n, const int64_t* keys, double* vals);
+/* set every stored element to val */
+int ccsd_tensor_fill(ccsd_ctx ctx, ccsd_tensor t, double val);
+
+/* ---- indexed-tensor operations (IndexableTensorBase, indexable_tensor.hpp:133-155) ---- */
+/* C[idxC] = beta*C[idxC] + alpha * A[idxA] * B[idxB], with the reference's implicit
+ * antisymmetrisation of external lines split between A and B
+ * (SpinorbitalTensor::mult, spinorbital_tensor.cxx:455-790).  beta is applied
+ * once to every block of C that receives a contribution. */
+int ccsd_contract(ccsd_ctx ctx, double alpha, ccsd_tensor A, const char* idxA,
+                  ccsd_tensor B, const char* idxB, double beta, ccsd_tensor C, const char* idxC);
+/* B[idxB] = beta*B[idxB] + alpha*A[idxA]  (SpinorbitalTensor::sum, spinorbital_tensor.cxx:793-1018) */
+int ccsd_sum(ccsd_ctx ctx, double alpha, ccsd_tensor A, const char* idxA,
+             double beta, ccsd_tensor B, const char* idxB);
+/* A *= alpha  (SpinorbitalTensor::scale) */
+int ccsd_scale(ccsd_ctx ctx, ccsd_tensor A, double alpha);
+/* full spin-orbital contraction to a scalar (SpinorbitalTensor::dot, :1063-1074) */
+int ccsd_dot(ccsd_ctx ctx, ccsd_tensor A, const char* idxA, ccsd_tensor B, const char* idxB, double* out);
+/* p = 0 (max-abs), 1 or 2 (SpinorbitalTensor::norm, :1077-1109) */
+int ccsd_norm(ccsd_ctx ctx, ccsd_tensor A, int p, double* out);
+/* Jacobi weight x /= (sum of index denominators + shift), 0 if |den+shift| < 1e-4
+ * (CTFTensor::weight, ctf_tensor.cxx:480-514).  Denominators per spin and irrep,
+ * concatenated over irreps: dvrt_a/dvrt_b = -f_aa, docc_a/docc_b = +f_ii
+ * (Denominator, denominator.hpp:50-73). */
+int ccsd_weight(ccsd_ctx ctx, ccsd_tensor A, const double* dvrt_a, const double* dvrt_b,
+                const double* docc_a, const double* docc_b, double shift);
+
+/* ---- CCSD solver (CCSD<U>::run / iterate, Iterative<U>::run, DIIS) -------- */
+typedef struct {
+    double conv_tol;      /* default 1e-9  (ccsd.cxx:269-270) */
+    int    max_iter;      /* default 50    (ccsd.cxx:271-272) */
+    int    diis_order;    /* default 5     (ccsd.cxx:281-282) */
+    int    diis_start;    /* default 1     (ccsd.cxx:279-280) */
+    double diis_damping;  /* default 0.0   (ccsd.cxx:277-278) */
+    int    precision;     /* CCSD_PREC_FP64 or CCSD_PREC_SPLIT */
+    int    slices;        /* split-BF16 slice count; 0 = autotuned */
+    int    use_graph;     /* capture one iteration as a CUDA graph and replay it */
+} ccsd_options;
+
+void ccsd_options_default(ccsd_options* opts);
+
+/* The 13 blocks of H in the order of TwoElectronOperator
+ * (2eoperator.cxx:13-21, 1eoperator.hpp:39-44):
+ *   fAI "ai", fME "ia", fAE "ab", fMI "ij",
+ *   VMNIJ "ijkl", VAMIJ "aijk", VMNEJ "ijak", VABIJ "abij", VMNEF "ijab",
+ *   VAMEI "aibj", VAMEF "aibc", VABEJ "abci", VABEF "abcd". */
+typedef struct {
+    ccsd_tensor fAI, fME, fAE, fMI;
+    ccsd_tensor VMNIJ, VAMIJ, VMNEJ, VABIJ, VMNEF, VAMEI, VAMEF, VABEJ, VABEF;
+} ccsd_hamiltonian;
+
+/* Build the 13 H blocks on the device from a three-index factor
+ * (pq|rs) = sum_P B[P,p,q] B[P,r,s] (closed shell, spatial orbitals shared by
+ * both spins) and a diagonal Fock matrix eps[n].  Orbitals are ordered occupied
+ * first, irrep-major inside occ and vrt, matching ccsd_ctx_set_spaces.
+ * B is a host array [naux][n][n]. */
+int ccsd_hamiltonian_from_factor(ccsd_ctx ctx, int naux, const double* B, const double* eps,
+                                 ccsd_hamiltonian* H);
+int ccsd_hamiltonian_destroy(ccsd_ctx ctx, ccsd_hamiltonian* H);
+
+/* Solver: allocates T, Z, Tau, the 7 intermediates and the DIIS ring, forms the
+ * MP1 guess and the MP2 energy (ccsd.cxx:37-62), and plans one iteration. */
+int ccsd_solver_create(ccsd_ctx ctx, const ccsd_hamiltonian* H, const ccsd_options* opts,
+                       ccsd_solver* out);
+int ccsd_solver_destroy(ccsd_solver s);
+int ccsd_solver_mp2(ccsd_solver s, double* mp2);
+/* one CCSD::iterate; energy and conv (max-abs of the weighted update) come back to the host */
+int ccsd_solver_iterate(ccsd_solver s, double* energy, double* conv);
+/* one iteration without reading energy/conv back (stream-ordered, no host sync) */
+int ccsd_solver_iterate_async(ccsd_solver s);
+/* read the energy / convergence of the last iteration (synchronises the stream) */
+int ccsd_solver_status(ccsd_solver s, double* energy, double* conv, int* iterations);
+/* Iterative::run: iterate until conv < conv_tol or max_iter */
+int ccsd_solver_run(ccsd_solver s, double* energy, double* conv, int* iterations);
+/* amplitudes T1 / T2 as tensors of the solver (for reading) */
+int ccsd_solver_amplitudes(ccsd_solver s, ccsd_tensor* T1, ccsd_tensor* T2);
+/* algorithmic FP64 flops of one iteration as planned (packed-pair counts) */
+int ccsd_solver_flops(ccsd_solver s, double* flops);
+
+/* ---- synthetic inputs (seeded; identical on every host) -------------------- */
+/* irrep sizes: Dirichlet(1.5) split of o, v and naux = 3(o+v) (aux may be NULL) */
+int ccsd_synth_irreps(uint64_t seed, int nirrep, int o, int v,
+                      int* occ_per_irrep, int* vrt_per_irrep, int* aux_per_irrep);
+/* eps[n] (n = o+v) and B[naux][n][n] (either may be NULL) */
+int ccsd_synth_problem(uint64_t seed, int nirrep,
+                       const int* occ_per_irrep, const int* vrt_per_irrep, const int* aux_per_irrep,
+                       double* eps, double* B);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
