@@ -1,0 +1,514 @@
+"""Python binding of the B200 CCSD engine (ctypes over libccsd_b200.so).
+
+The C ABI (include/ccsd_b200.h) is the product boundary; this module mirrors it for
+tests, benchmarks and Python callers:
+
+    ctx = Context(device=0)
+    ctx.set_spaces(nirrep=1, vrt=[v], occ=[o])
+    H = ctx.hamiltonian_from_factor(B, eps)
+    s = ctx.solver(H, conv_tol=1e-9, diis_order=8, precision="fp64")
+    energy, conv, iters = s.run()
+
+Every failing call raises CcsdError with the engine's message.  There is no
+fallback: if the shared library or a CUDA device is missing, calls fail loudly.
+"""
+from __future__ import annotations
+
+import ctypes
+import itertools
+import os
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libccsd_b200.so"
+
+CCSD_OK = 0
+STATUS = {
+    0: "CCSD_OK", 1: "CCSD_ERR_ARG", 2: "CCSD_ERR_CUDA", 3: "CCSD_ERR_OOM", 4: "CCSD_ERR_PLAN",
+    5: "CCSD_DIVERGED", 6: "CCSD_NOT_CONVERGED", 7: "CCSD_ERR_SINGULAR", 8: "CCSD_ERR_TIMEOUT",
+    9: "CCSD_ERR_UNSUPPORTED",
+}
+PREC = {"fp64": 0, "split": 1}
+TENSOR_PACKED = 1
+
+# symbols declared in include/ccsd_b200.h
+EXPORTS = [
+    "ccsd_ctx_create", "ccsd_ctx_destroy", "ccsd_last_error", "ccsd_ctx_synchronize", "ccsd_ctx_device_bytes",
+    "ccsd_ctx_launch_count", "ccsd_ctx_set_precision", "ccsd_ctx_set_spaces", "ccsd_tensor_create",
+    "ccsd_tensor_destroy", "ccsd_tensor_ndim", "ccsd_tensor_spin_cases", "ccsd_tensor_block_size",
+    "ccsd_tensor_write_block", "ccsd_tensor_read_block", "ccsd_tensor_write", "ccsd_tensor_read", "ccsd_tensor_fill",
+    "ccsd_contract", "ccsd_sum", "ccsd_scale", "ccsd_dot", "ccsd_norm", "ccsd_weight", "ccsd_options_default",
+    "ccsd_hamiltonian_from_factor", "ccsd_hamiltonian_destroy", "ccsd_solver_create", "ccsd_solver_destroy",
+    "ccsd_solver_mp2", "ccsd_solver_iterate", "ccsd_solver_iterate_async", "ccsd_solver_status", "ccsd_solver_run",
+    "ccsd_solver_amplitudes", "ccsd_solver_flops", "ccsd_synth_irreps", "ccsd_synth_problem",
+]
+
+
+class CcsdError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{STATUS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Options(ctypes.Structure):
+    _fields_ = [
+        ("conv_tol", ctypes.c_double), ("max_iter", ctypes.c_int), ("diis_order", ctypes.c_int),
+        ("diis_start", ctypes.c_int), ("diis_damping", ctypes.c_double), ("precision", ctypes.c_int),
+        ("slices", ctypes.c_int), ("use_graph", ctypes.c_int),
+    ]
+
+
+H_FIELDS = ["fAI", "fME", "fAE", "fMI", "VMNIJ", "VAMIJ", "VMNEJ", "VABIJ", "VMNEF", "VAMEI", "VAMEF", "VABEJ",
+            "VABEF"]
+# (nout, nin) per H block, {vrt, occ} order (src/operator/2eoperator.cxx:13-21)
+H_SHAPES = {
+    "fAI": ((1, 0), (0, 1)), "fME": ((0, 1), (1, 0)), "fAE": ((1, 0), (1, 0)), "fMI": ((0, 1), (0, 1)),
+    "VMNIJ": ((0, 2), (0, 2)), "VAMIJ": ((1, 1), (0, 2)), "VMNEJ": ((0, 2), (1, 1)), "VABIJ": ((2, 0), (0, 2)),
+    "VMNEF": ((0, 2), (2, 0)), "VAMEI": ((1, 1), (1, 1)), "VAMEF": ((1, 1), (2, 0)), "VABEJ": ((2, 0), (1, 1)),
+    "VABEF": ((2, 0), (2, 0)),
+}
+
+
+class Hamiltonian(ctypes.Structure):
+    _fields_ = [(f, ctypes.c_int32) for f in H_FIELDS]
+
+
+_lib = None
+
+
+def lib():
+    """Load the shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise CcsdError(-1, f"{LIB_PATH} is missing: run aquarius_b200.build.build()")
+        L = ctypes.CDLL(str(LIB_PATH))
+        vp, i32, i64, dbl = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_double
+        P = ctypes.POINTER
+        sig = {
+            "ccsd_ctx_create": [ctypes.c_int, vp, P(vp)],
+            "ccsd_ctx_destroy": [vp],
+            "ccsd_ctx_synchronize": [vp],
+            "ccsd_ctx_device_bytes": [vp, P(i64)],
+            "ccsd_ctx_launch_count": [vp, P(i64)],
+            "ccsd_ctx_set_precision": [vp, ctypes.c_int, ctypes.c_int],
+            "ccsd_ctx_set_spaces": [vp, ctypes.c_int, vp, vp, vp, vp],
+            "ccsd_tensor_create": [vp, ctypes.c_char_p, vp, vp, ctypes.c_int, P(i32)],
+            "ccsd_tensor_destroy": [vp, i32],
+            "ccsd_tensor_ndim": [vp, i32, P(ctypes.c_int)],
+            "ccsd_tensor_spin_cases": [vp, i32, P(ctypes.c_int), vp],
+            "ccsd_tensor_block_size": [vp, i32, vp, vp, P(i64)],
+            "ccsd_tensor_write_block": [vp, i32, vp, vp, vp],
+            "ccsd_tensor_read_block": [vp, i32, vp, vp, vp],
+            "ccsd_tensor_write": [vp, i32, vp, vp, i64, vp, vp, dbl, dbl],
+            "ccsd_tensor_read": [vp, i32, vp, vp, i64, vp, vp],
+            "ccsd_tensor_fill": [vp, i32, dbl],
+            "ccsd_contract": [vp, dbl, i32, ctypes.c_char_p, i32, ctypes.c_char_p, dbl, i32, ctypes.c_char_p],
+            "ccsd_sum": [vp, dbl, i32, ctypes.c_char_p, dbl, i32, ctypes.c_char_p],
+            "ccsd_scale": [vp, i32, dbl],
+            "ccsd_dot": [vp, i32, ctypes.c_char_p, i32, ctypes.c_char_p, P(dbl)],
+            "ccsd_norm": [vp, i32, ctypes.c_int, P(dbl)],
+            "ccsd_weight": [vp, i32, vp, vp, vp, vp, dbl],
+            "ccsd_options_default": [P(Options)],
+            "ccsd_hamiltonian_from_factor": [vp, ctypes.c_int, vp, vp, vp, ctypes.c_int, P(Hamiltonian)],
+            "ccsd_hamiltonian_destroy": [vp, P(Hamiltonian)],
+            "ccsd_solver_create": [vp, P(Hamiltonian), P(Options), P(vp)],
+            "ccsd_solver_destroy": [vp],
+            "ccsd_solver_mp2": [vp, P(dbl)],
+            "ccsd_solver_iterate": [vp, P(dbl), P(dbl)],
+            "ccsd_solver_iterate_async": [vp],
+            "ccsd_solver_status": [vp, P(dbl), P(dbl), P(ctypes.c_int)],
+            "ccsd_solver_run": [vp, P(dbl), P(dbl), P(ctypes.c_int)],
+            "ccsd_solver_amplitudes": [vp, P(i32), P(i32)],
+            "ccsd_solver_flops": [vp, P(dbl)],
+            "ccsd_synth_irreps": [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp],
+            "ccsd_synth_problem": [ctypes.c_uint64, ctypes.c_int, vp, vp, vp, vp, vp],
+        }
+        for name, args in sig.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = None if name == "ccsd_options_default" else ctypes.c_int
+        L.ccsd_last_error.argtypes = [vp]
+        L.ccsd_last_error.restype = ctypes.c_char_p
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def _ints(xs):
+    return np.ascontiguousarray(np.asarray(xs, dtype=np.int32))
+
+
+def _check(code, ctx=None):
+    if code != CCSD_OK:
+        msg = lib().ccsd_last_error(ctx)
+        raise CcsdError(code, (msg or b"").decode())
+
+
+# ---------------------------------------------------------------------------
+# synthetic inputs
+# ---------------------------------------------------------------------------
+
+def synth_irreps(seed: int, nirrep: int, o: int, v: int):
+    occ = np.zeros(nirrep, np.int32)
+    vrt = np.zeros(nirrep, np.int32)
+    aux = np.zeros(nirrep, np.int32)
+    _check(lib().ccsd_synth_irreps(seed, nirrep, o, v, _ptr(occ), _ptr(vrt), _ptr(aux)))
+    return occ, vrt, aux
+
+
+def synth_problem(seed: int, o: int, v: int, nirrep: int = 1, with_B: bool = True):
+    """Seeded synthetic closed-shell problem: (eps[n], B[naux,n,n] or None, occ, vrt, aux irrep counts)."""
+    if nirrep == 1:
+        occ, vrt = np.array([o], np.int32), np.array([v], np.int32)
+        aux = np.array([3 * (o + v)], np.int32)
+    else:
+        occ, vrt, aux = synth_irreps(seed, nirrep, o, v)
+    n = o + v
+    naux = int(aux.sum())
+    eps = np.zeros(n)
+    B = np.zeros((naux, n, n)) if with_B else None
+    _check(lib().ccsd_synth_problem(seed, nirrep, _ptr(occ), _ptr(vrt), _ptr(aux), _ptr(eps), _ptr(B)))
+    return eps, B, occ, vrt, aux
+
+
+# ---------------------------------------------------------------------------
+# context / tensors
+# ---------------------------------------------------------------------------
+
+class Tensor:
+    def __init__(self, ctx: "Context", handle: int, name: str, nout, nin, packed=False):
+        self.ctx, self.h, self.name, self.packed = ctx, handle, name, packed
+        self.nout, self.nin = tuple(nout), tuple(nin)
+        self.group = [0] * nout[0] + [1] * nout[1] + [2] * nin[0] + [3] * nin[1]
+        self.ndim = len(self.group)
+
+    def spin_cases(self):
+        n = ctypes.c_int()
+        _check(lib().ccsd_tensor_spin_cases(self.ctx.c, self.h, ctypes.byref(n), None), self.ctx.c)
+        a = np.zeros(4 * n.value, np.int32)
+        _check(lib().ccsd_tensor_spin_cases(self.ctx.c, self.h, ctypes.byref(n), _ptr(a)), self.ctx.c)
+        return [tuple(a[4 * i:4 * i + 4]) for i in range(n.value)]
+
+    def case_spins(self, alpha):
+        """spin (0 alpha, 1 beta) of every position for a spin case."""
+        gs = [self.nout[0], self.nout[1], self.nin[0], self.nin[1]]
+        out = []
+        for g in range(4):
+            out += [0] * alpha[g] + [1] * (gs[g] - alpha[g])
+        return out
+
+    def block_size(self, alpha, irreps=None):
+        n = ctypes.c_int64()
+        irr = _ints(irreps if irreps is not None else [0] * self.ndim)
+        _check(lib().ccsd_tensor_block_size(self.ctx.c, self.h, _ptr(_ints(alpha)), _ptr(irr), ctypes.byref(n)),
+               self.ctx.c)
+        return n.value
+
+    def block_shape(self, alpha, irreps=None):
+        irreps = irreps if irreps is not None else [0] * self.ndim
+        sp = self.case_spins(alpha)
+        return tuple(self.ctx.count(self.group[p] % 2, sp[p], irreps[p]) for p in range(self.ndim))
+
+    def read_block(self, alpha, irreps=None):
+        n = self.block_size(alpha, irreps)
+        out = np.zeros(max(n, 1))
+        irr = _ints(irreps if irreps is not None else [0] * self.ndim)
+        _check(lib().ccsd_tensor_read_block(self.ctx.c, self.h, _ptr(_ints(alpha)), _ptr(irr), _ptr(out)), self.ctx.c)
+        return out[:n]
+
+    def write_block(self, alpha, data, irreps=None):
+        data = np.ascontiguousarray(np.asarray(data, dtype=np.float64).reshape(-1, order="F"))
+        irr = _ints(irreps if irreps is not None else [0] * self.ndim)
+        _check(lib().ccsd_tensor_write_block(self.ctx.c, self.h, _ptr(_ints(alpha)), _ptr(irr), _ptr(data)),
+               self.ctx.c)
+
+    def write(self, alpha, keys, vals, a=1.0, b=0.0, irreps=None):
+        keys = np.ascontiguousarray(np.asarray(keys, dtype=np.int64))
+        vals = np.ascontiguousarray(np.asarray(vals, dtype=np.float64))
+        irr = _ints(irreps if irreps is not None else [0] * self.ndim)
+        _check(lib().ccsd_tensor_write(self.ctx.c, self.h, _ptr(_ints(alpha)), _ptr(irr), len(keys), _ptr(keys),
+                                       _ptr(vals), a, b), self.ctx.c)
+
+    def read(self, alpha, keys, irreps=None):
+        keys = np.ascontiguousarray(np.asarray(keys, dtype=np.int64))
+        vals = np.zeros(len(keys))
+        irr = _ints(irreps if irreps is not None else [0] * self.ndim)
+        _check(lib().ccsd_tensor_read(self.ctx.c, self.h, _ptr(_ints(alpha)), _ptr(irr), len(keys), _ptr(keys),
+                                      _ptr(vals)), self.ctx.c)
+        return vals
+
+    def fill(self, val):
+        _check(lib().ccsd_tensor_fill(self.ctx.c, self.h, float(val)), self.ctx.c)
+
+    def norm(self, p=0):
+        out = ctypes.c_double()
+        _check(lib().ccsd_norm(self.ctx.c, self.h, p, ctypes.byref(out)), self.ctx.c)
+        return out.value
+
+    def __getitem__(self, idx):
+        return _Indexed(self, idx, 1.0)
+
+    def __setitem__(self, idx, expr):
+        if isinstance(expr, _Assign):      # produced by += / -= on an _Indexed
+            return
+        _assign(self, idx, expr, beta=0.0)
+
+    # -- full spin-orbital array (tests) -------------------------------------------------
+    def to_full(self):
+        """Dense full spin-orbital array: every index runs over [alpha | beta] of its space,
+        irrep-major inside a spin; antisymmetric images inside groups are filled in."""
+        ctx = self.ctx
+        dims = []
+        for p in range(self.ndim):
+            sp = self.group[p] % 2
+            dims.append(2 * ctx.total(sp))
+        full = np.zeros(dims)
+        groups = [[p for p in range(self.ndim) if self.group[p] == g] for g in range(4)]
+        for alpha in self.spin_cases():
+            spins = self.case_spins(alpha)
+            for irr in itertools.product(range(ctx.nirrep), repeat=self.ndim):
+                x = 0
+                for h in irr:
+                    x ^= h
+                if x:
+                    continue
+                if self.block_size(alpha, irr) == 0:
+                    continue
+                shape = self.block_shape(alpha, irr)
+                blk = self.read_block(alpha, irr).reshape(shape, order="F")
+                perms = [list(itertools.permutations(gp)) for gp in groups]
+                for combo in itertools.product(*perms):
+                    perm = list(range(self.ndim))
+                    for gp, pg in zip(groups, combo):
+                        for a_, b_ in zip(gp, pg):
+                            perm[a_] = b_
+                    sign = 1
+                    pp = list(perm)
+                    for i in range(len(pp)):
+                        while pp[i] != i:
+                            j = pp[i]
+                            pp[i], pp[j] = pp[j], pp[i]
+                            sign = -sign
+                    # position q of the image takes original position perm[q]
+                    sl = []
+                    for q in range(self.ndim):
+                        p0 = perm[q]
+                        sp = self.group[p0] % 2
+                        lo = spins[p0] * ctx.total(sp) + ctx.offset(sp, irr[p0])
+                        sl.append(slice(lo, lo + shape[p0]))
+                    full[tuple(sl)] = sign * np.transpose(blk, perm)
+        return full
+
+
+class _Indexed:
+    def __init__(self, t, idx, f):
+        self.t, self.idx, self.f = t, idx, f
+
+    def __mul__(self, other):
+        if isinstance(other, _Indexed):
+            return _Mult(self, other, self.f * other.f)
+        return _Indexed(self.t, self.idx, self.f * other)
+
+    def __rmul__(self, f):
+        return _Indexed(self.t, self.idx, self.f * f)
+
+    def __iadd__(self, expr):
+        _assign(self.t, self.idx, expr, beta=1.0)
+        return _Assign()
+
+    def __isub__(self, expr):
+        _assign(self.t, self.idx, -1.0 * expr, beta=1.0)
+        return _Assign()
+
+
+class _Mult:
+    def __init__(self, a, b, f):
+        self.a, self.b, self.f = a, b, f
+
+    def __rmul__(self, f):
+        return _Mult(self.a, self.b, self.f * f)
+
+
+class _Assign:
+    pass
+
+
+def _assign(t, idx, expr, beta):
+    ctx = t.ctx
+    if isinstance(expr, _Mult):
+        ctx.contract(expr.f, expr.a.t, expr.a.idx, expr.b.t, expr.b.idx, beta, t, idx)
+    elif isinstance(expr, _Indexed):
+        ctx.sum(expr.f, expr.t, expr.idx, beta, t, idx)
+    else:
+        raise TypeError("unsupported expression")
+
+
+class Context:
+    def __init__(self, device: int = 0, stream: int | None = None):
+        c = ctypes.c_void_p()
+        _check(lib().ccsd_ctx_create(device, stream, ctypes.byref(c)))
+        self.c = c
+        self.nirrep = 1
+        self._counts = None
+
+    def close(self):
+        if self.c:
+            _check(lib().ccsd_ctx_destroy(self.c))
+            self.c = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_spaces(self, vrt, occ, vrt_beta=None, occ_beta=None):
+        vrt, occ = _ints(vrt), _ints(occ)
+        vb = _ints(vrt_beta if vrt_beta is not None else vrt)
+        ob = _ints(occ_beta if occ_beta is not None else occ)
+        self.nirrep = len(vrt)
+        _check(lib().ccsd_ctx_set_spaces(self.c, self.nirrep, _ptr(vrt), _ptr(vb), _ptr(occ), _ptr(ob)), self.c)
+        self._counts = {(0, 0): vrt, (0, 1): vb, (1, 0): occ, (1, 1): ob}
+
+    def count(self, space, spin, irrep):
+        return int(self._counts[(space, spin)][irrep])
+
+    def total(self, space, spin=0):
+        return int(self._counts[(space, spin)].sum())
+
+    def offset(self, space, irrep, spin=0):
+        return int(self._counts[(space, spin)][:irrep].sum())
+
+    def set_precision(self, precision="fp64", slices=0):
+        _check(lib().ccsd_ctx_set_precision(self.c, PREC[precision], slices), self.c)
+
+    def tensor(self, name, nout, nin, packed=False):
+        h = ctypes.c_int32()
+        _check(lib().ccsd_tensor_create(self.c, name.encode(), _ptr(_ints(nout)), _ptr(_ints(nin)),
+                                        TENSOR_PACKED if packed else 0, ctypes.byref(h)), self.c)
+        return Tensor(self, h.value, name, nout, nin, packed)
+
+    def contract(self, alpha, A, ia, B, ib, beta, C, ic):
+        _check(lib().ccsd_contract(self.c, alpha, A.h, ia.encode(), B.h, ib.encode(), beta, C.h, ic.encode()), self.c)
+
+    def sum(self, alpha, A, ia, beta, B, ib):
+        _check(lib().ccsd_sum(self.c, alpha, A.h, ia.encode(), beta, B.h, ib.encode()), self.c)
+
+    def dot(self, A, ia, B, ib):
+        out = ctypes.c_double()
+        _check(lib().ccsd_dot(self.c, A.h, ia.encode(), B.h, ib.encode(), ctypes.byref(out)), self.c)
+        return out.value
+
+    def scale(self, A, alpha):
+        _check(lib().ccsd_scale(self.c, A.h, alpha), self.c)
+
+    def weight(self, A, dvrt, docc, dvrt_b=None, docc_b=None, shift=0.0):
+        dv = np.ascontiguousarray(dvrt, dtype=np.float64)
+        do = np.ascontiguousarray(docc, dtype=np.float64)
+        dvb = np.ascontiguousarray(dvrt_b if dvrt_b is not None else dv, dtype=np.float64)
+        dob = np.ascontiguousarray(docc_b if docc_b is not None else do, dtype=np.float64)
+        _check(lib().ccsd_weight(self.c, A.h, _ptr(dv), _ptr(dvb), _ptr(do), _ptr(dob), shift), self.c)
+
+    def synchronize(self):
+        _check(lib().ccsd_ctx_synchronize(self.c), self.c)
+
+    def device_bytes(self):
+        n = ctypes.c_int64()
+        _check(lib().ccsd_ctx_device_bytes(self.c, ctypes.byref(n)), self.c)
+        return n.value
+
+    def launch_count(self):
+        n = ctypes.c_int64()
+        _check(lib().ccsd_ctx_launch_count(self.c, ctypes.byref(n)), self.c)
+        return n.value
+
+    def hamiltonian_from_factor(self, B, eps, aux_per_irrep=None, pack_vvvv=True):
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        eps = np.ascontiguousarray(eps, dtype=np.float64)
+        H = Hamiltonian()
+        aux = _ints(aux_per_irrep) if aux_per_irrep is not None else None
+        _check(lib().ccsd_hamiltonian_from_factor(self.c, B.shape[0], _ptr(B), _ptr(eps), _ptr(aux),
+                                                  1 if pack_vvvv else 0, ctypes.byref(H)), self.c)
+        return HamiltonianHandle(self, H, pack_vvvv)
+
+    def solver(self, H, **kw):
+        return Solver(self, H, **kw)
+
+
+class HamiltonianHandle:
+    def __init__(self, ctx, H, packed):
+        self.ctx, self.H = ctx, H
+        self.tensors = {f: Tensor(ctx, getattr(H, f), f, *H_SHAPES[f], packed=(packed and f == "VABEF"))
+                        for f in H_FIELDS}
+
+    def __getitem__(self, name):
+        return self.tensors[name]
+
+    def destroy(self):
+        if self.ctx.c:
+            _check(lib().ccsd_hamiltonian_destroy(self.ctx.c, ctypes.byref(self.H)), self.ctx.c)
+
+
+class Solver:
+    def __init__(self, ctx, H: HamiltonianHandle, conv_tol=1e-9, max_iter=50, diis_order=5, diis_start=1,
+                 precision="fp64", slices=0, use_graph=False):
+        self.ctx = ctx
+        o = Options()
+        lib().ccsd_options_default(ctypes.byref(o))
+        o.conv_tol, o.max_iter, o.diis_order, o.diis_start = conv_tol, max_iter, diis_order, diis_start
+        o.precision, o.slices, o.use_graph = PREC[precision], slices, 1 if use_graph else 0
+        s = ctypes.c_void_p()
+        _check(lib().ccsd_solver_create(ctx.c, ctypes.byref(H.H), ctypes.byref(o), ctypes.byref(s)), ctx.c)
+        self.s = s
+        t1, t2 = ctypes.c_int32(), ctypes.c_int32()
+        _check(lib().ccsd_solver_amplitudes(s, ctypes.byref(t1), ctypes.byref(t2)), ctx.c)
+        self.T1 = Tensor(ctx, t1.value, "T1", (1, 0), (0, 1))
+        self.T2 = Tensor(ctx, t2.value, "T2", (2, 0), (0, 2))
+
+    def close(self):
+        if self.s:
+            _check(lib().ccsd_solver_destroy(self.s), self.ctx.c)
+            self.s = None
+
+    @property
+    def mp2(self):
+        x = ctypes.c_double()
+        _check(lib().ccsd_solver_mp2(self.s, ctypes.byref(x)), self.ctx.c)
+        return x.value
+
+    def iterate(self):
+        e, c = ctypes.c_double(), ctypes.c_double()
+        _check(lib().ccsd_solver_iterate(self.s, ctypes.byref(e), ctypes.byref(c)), self.ctx.c)
+        return e.value, c.value
+
+    def iterate_async(self):
+        _check(lib().ccsd_solver_iterate_async(self.s), self.ctx.c)
+
+    def status(self):
+        e, c, i = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        _check(lib().ccsd_solver_status(self.s, ctypes.byref(e), ctypes.byref(c), ctypes.byref(i)), self.ctx.c)
+        return e.value, c.value, i.value
+
+    def run(self):
+        e, c, i = ctypes.c_double(), ctypes.c_double(), ctypes.c_int()
+        code = lib().ccsd_solver_run(self.s, ctypes.byref(e), ctypes.byref(c), ctypes.byref(i))
+        if code not in (CCSD_OK, 6):
+            _check(code, self.ctx.c)
+        return e.value, c.value, i.value
+
+    def flops(self):
+        x = ctypes.c_double()
+        _check(lib().ccsd_solver_flops(self.s, ctypes.byref(x)), self.ctx.c)
+        return x.value

@@ -1,0 +1,562 @@
+// extern "C" entry points (declared in include/ccsd_b200.h).  Every call converts
+// engine exceptions into status codes; nothing throws across the ABI.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <sstream>
+
+#include "engine.hpp"
+#include "hbuild.hpp"
+#include "solver.hpp"
+
+struct ccsd_ctx_s {
+    ccsd::Context* c = nullptr;
+};
+
+struct ccsd_solver_s {
+    ccsd_ctx_s* ctx = nullptr;
+    ccsd::Solver* s = nullptr;
+};
+
+namespace ccsd {
+Context* from_handle(ccsd_ctx c) {
+    if (!c || !c->c) throw Error(CCSD_ERR_ARG, "null context");
+    return c->c;
+}
+}  // namespace ccsd
+
+using namespace ccsd;
+
+namespace {
+
+thread_local std::string g_global_error;
+
+template <class F>
+int guarded(ccsd_ctx ctx, F f) {
+    try {
+        if (ctx && ctx->c) CCSD_CUDA(cudaSetDevice(ctx->c->device));
+        f();
+        return CCSD_OK;
+    } catch (const Error& e) {
+        if (ctx && ctx->c) ctx->c->last_error = e.what();
+        else g_global_error = e.what();
+        return e.code;
+    } catch (const std::exception& e) {
+        if (ctx && ctx->c) ctx->c->last_error = e.what();
+        else g_global_error = e.what();
+        return CCSD_ERR_ARG;
+    }
+}
+
+const Block& block_at(Tensor& T, const int alpha[4], const int* irreps, int& cs) {
+    cs = T.find_case(alpha);
+    if (cs < 0) throw Error(CCSD_ERR_ARG, "no such spin case in " + T.name);
+    std::vector<int> irr(T.ndim, 0);
+    if (irreps)
+        for (int p = 0; p < T.ndim; p++) irr[p] = irreps[p];
+    auto it = T.cases[cs].block_of.find(irr);
+    if (it == T.cases[cs].block_of.end()) throw Error(CCSD_ERR_ARG, "block not stored in " + T.name);
+    return T.cases[cs].blocks[it->second];
+}
+
+// Expand a key (first index fastest, full block index) into the storage offsets of all
+// its images under permutations inside same-spin groups, with signs; for packed pairs
+// only the canonical image is stored.
+void key_images(const Tensor& T, int cs, const Block& b, int64_t key, std::vector<std::pair<int64_t, double>>& out) {
+    out.clear();
+    const int nd = T.ndim;
+    std::vector<int64_t> x(nd);
+    int64_t r = key;
+    for (int p = 0; p < nd; p++) {
+        if (b.len[p] == 0) return;
+        x[p] = r % b.len[p];
+        r /= b.len[p];
+    }
+    if (r != 0) throw Error(CCSD_ERR_ARG, "key out of range");
+    const SpinCase& sc = T.cases[cs];
+    // same-spin pairs inside a group with equal irreps can be swapped (AS symmetry)
+    std::vector<std::pair<int, int>> swaps;
+    for (int p = 0; p + 1 < nd; p++)
+        if (T.group[p] == T.group[p + 1] && sc.spin[p] == sc.spin[p + 1] && b.irrep[p] == b.irrep[p + 1])
+            swaps.push_back({p, p + 1});
+    const int ns = (int)swaps.size();
+    for (int mask = 0; mask < (1 << ns); mask++) {
+        std::vector<int64_t> y = x;
+        double sign = 1;
+        for (int i = 0; i < ns; i++)
+            if (mask & (1 << i)) {
+                std::swap(y[swaps[i].first], y[swaps[i].second]);
+                sign = -sign;
+            }
+        bool skip = false;
+        int64_t off = b.offset;
+        for (int p = 0; p < nd; p++) {
+            int pi = b.pair_of(p);
+            if (pi >= 0) {
+                const auto& pr = b.pairs[pi];
+                if (pr.p != p) continue;
+                int64_t u = y[pr.p], v = y[pr.q];
+                if (pr.kind == 1) {
+                    if (u >= v) {
+                        skip = true;
+                        break;
+                    }
+                    off += pr.stride * (v * (v - 1) / 2 + u);
+                } else {
+                    off += pr.stride * (u + (int64_t)b.len[pr.p] * v);
+                }
+            } else {
+                off += b.stride[p] * y[p];
+            }
+        }
+        bool diag = false;
+        for (auto& s : swaps) diag |= x[s.first] == x[s.second];
+        if (diag) {
+            // antisymmetric diagonal elements are zero: store nothing but a zero
+            if (mask == 0 && !skip) out.push_back({off, 0.0});
+            continue;
+        }
+        if (!skip) out.push_back({off, sign});
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int ccsd_ctx_create(int device, void* stream, ccsd_ctx* out) {
+    if (!out) return CCSD_ERR_ARG;
+    *out = nullptr;
+    return guarded(nullptr, [&] {
+        CCSD_CUDA(cudaSetDevice(device));
+        auto* h = new ccsd_ctx_s;
+        try {
+            h->c = new Context(device, (cudaStream_t)stream);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int ccsd_ctx_destroy(ccsd_ctx ctx) {
+    if (!ctx) return CCSD_ERR_ARG;
+    int st = guarded(ctx, [&] { delete ctx->c; });
+    ctx->c = nullptr;
+    delete ctx;
+    return st;
+}
+
+const char* ccsd_last_error(ccsd_ctx ctx) {
+    if (ctx && ctx->c) return ctx->c->last_error.c_str();
+    return g_global_error.c_str();
+}
+
+int ccsd_ctx_synchronize(ccsd_ctx ctx) {
+    return guarded(ctx, [&] { CCSD_CUDA(cudaStreamSynchronize(from_handle(ctx)->stream)); });
+}
+
+int ccsd_ctx_device_bytes(ccsd_ctx ctx, int64_t* bytes) {
+    return guarded(ctx, [&] { *bytes = from_handle(ctx)->device_bytes; });
+}
+
+int ccsd_ctx_launch_count(ccsd_ctx ctx, int64_t* count) {
+    return guarded(ctx, [&] {
+        from_handle(ctx);
+        *count = kern::launch_count();
+    });
+}
+
+int ccsd_ctx_set_precision(ccsd_ctx ctx, int precision, int slices) {
+    return guarded(ctx, [&] {
+        Context* c = from_handle(ctx);
+        if (precision != CCSD_PREC_FP64 && precision != CCSD_PREC_SPLIT) throw Error(CCSD_ERR_ARG, "bad precision");
+        if (precision == CCSD_PREC_SPLIT && !kern::split_supported())
+            throw Error(CCSD_ERR_UNSUPPORTED, "split-BF16 GEMMs need an sm_100 device");
+        if (slices < 0 || slices > 4) throw Error(CCSD_ERR_ARG, "slices must be in 0..4");
+        c->precision = precision;
+        c->slices = slices;
+    });
+}
+
+int ccsd_ctx_set_spaces(ccsd_ctx ctx, int nirrep, const int* vrt_alpha, const int* vrt_beta, const int* occ_alpha,
+                        const int* occ_beta) {
+    return guarded(ctx, [&] {
+        Context* c = from_handle(ctx);
+        if (nirrep != 1 && nirrep != 2 && nirrep != 4 && nirrep != 8) throw Error(CCSD_ERR_ARG, "nirrep must be 1,2,4,8");
+        if (!c->tensors.empty()) throw Error(CCSD_ERR_ARG, "spaces cannot change while tensors exist");
+        Spaces S;
+        S.nirrep = nirrep;
+        const int* src[2][2] = {{vrt_alpha, vrt_beta}, {occ_alpha, occ_beta}};
+        for (int sp = 0; sp < 2; sp++)
+            for (int s = 0; s < 2; s++) {
+                int off = 0;
+                for (int h = 0; h < nirrep; h++) {
+                    int v = src[sp][s][h];
+                    if (v < 0) throw Error(CCSD_ERR_ARG, "negative orbital count");
+                    S.n[sp][s][h] = v;
+                    S.off[sp][s][h] = off;
+                    off += v;
+                }
+            }
+        c->spaces = S;
+        c->spaces_set = true;
+    });
+}
+
+int ccsd_tensor_create(ccsd_ctx ctx, const char* name, const int nout[2], const int nin[2], int flags,
+                       ccsd_tensor* out) {
+    return guarded(ctx, [&] { *out = from_handle(ctx)->create_tensor(name ? name : "", nout, nin, flags); });
+}
+
+int ccsd_tensor_destroy(ccsd_ctx ctx, ccsd_tensor t) {
+    return guarded(ctx, [&] { from_handle(ctx)->destroy_tensor(t); });
+}
+
+int ccsd_tensor_ndim(ccsd_ctx ctx, ccsd_tensor t, int* ndim) {
+    return guarded(ctx, [&] { *ndim = from_handle(ctx)->tensor(t).ndim; });
+}
+
+int ccsd_tensor_spin_cases(ccsd_ctx ctx, ccsd_tensor t, int* ncases, int* alpha) {
+    return guarded(ctx, [&] {
+        Tensor& T = from_handle(ctx)->tensor(t);
+        *ncases = (int)T.cases.size();
+        if (alpha)
+            for (size_t c = 0; c < T.cases.size(); c++)
+                for (int g = 0; g < 4; g++) alpha[4 * c + g] = T.cases[c].alpha[g];
+    });
+}
+
+int ccsd_tensor_block_size(ccsd_ctx ctx, ccsd_tensor t, const int alpha[4], const int* irreps, int64_t* n) {
+    return guarded(ctx, [&] {
+        Tensor& T = from_handle(ctx)->tensor(t);
+        int cs = T.find_case(alpha);
+        *n = 0;
+        if (cs < 0) return;
+        std::vector<int> irr(T.ndim, 0);
+        if (irreps)
+            for (int p = 0; p < T.ndim; p++) irr[p] = irreps[p];
+        auto it = T.cases[cs].block_of.find(irr);
+        if (it != T.cases[cs].block_of.end()) *n = T.cases[cs].blocks[it->second].size;
+    });
+}
+
+int ccsd_tensor_write_block(ccsd_ctx ctx, ccsd_tensor t, const int alpha[4], const int* irreps, const double* host) {
+    return guarded(ctx, [&] {
+        Context* c = from_handle(ctx);
+        Tensor& T = c->tensor(t);
+        int cs;
+        const Block& b = block_at(T, alpha, irreps, cs);
+        CCSD_CUDA(cudaMemcpyAsync(T.data + b.offset, host, b.size * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CCSD_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int ccsd_tensor_read_block(ccsd_ctx ctx, ccsd_tensor t, const int alpha[4], const int* irreps, double* host) {
+    return guarded(ctx, [&] {
+        Context* c = from_handle(ctx);
+        Tensor& T = c->tensor(t);
+        int cs;
+        const Block& b = block_at(T, alpha, irreps, cs);
+        CCSD_CUDA(cudaMemcpyAsync(host, T.data + b.offset, b.size * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CCSD_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int ccsd_tensor_write(ccsd_ctx ctx, ccsd_tensor t, const int alpha_spin[4], const int* irreps, int64_t n,
+                      const int64_t* keys, const double* vals, double alpha, double beta) {
+    return guarded(ctx, [&] {
+        Context* c = from_handle(ctx);
+        Tensor& T = c->tensor(t);
+        int cs;
+        const Block& b = block_at(T, alpha_spin, irreps, cs);
+        std::vector<int64_t> offs;
+        std::vector<double> v;
+        std::vector<std::pair<int64_t, double>> img;
+        for (int64_t i = 0; i < n; i++) {
+            key_images(T, cs, b, keys[i], img);
+            for (auto& im : img) {
+                offs.push_back(im.first);
+                v.push_back(im.second * vals[i]);
+            }
+        }
+        if (offs.empty()) return;
+        int64_t* dk = (int64_t*)c->dmalloc(offs.size() * sizeof(int64_t));
+        double* dv = (double*)c->dmalloc(v.size() * sizeof(double));
+        CCSD_CUDA(cudaMemcpyAsync(dk, offs.data(), offs.size() * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+        CCSD_CUDA(cudaMemcpyAsync(dv, v.data(), v.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        kern::kv_write(T.data, dk, dv, (int64_t)offs.size(), alpha, beta, c->stream);
+        CCSD_CUDA(cudaStreamSynchronize(c->stream));
+        c->dfree(dk, offs.size() * sizeof(int64_t));
+        c->dfree(dv, v.size() * sizeof(double));
+    });
+}
+
+int ccsd_tensor_read(ccsd_ctx ctx, ccsd_tensor t, const int alpha_spin[4], const int* irreps, int64_t n,
+                     const int64_t* keys, double* vals) {
+    return guarded(ctx, [&] {
+        Context* c = from_handle(ctx);
+        Tensor& T = c->tensor(t);
+        int cs;
+        const Block& b = block_at(T, alpha_spin, irreps, cs);
+        std::vector<int64_t> offs(n);
+        std::vector<double> sign(n, 1.0);
+        std::vector<std::pair<int64_t, double>> img;
+        for (int64_t i = 0; i < n; i++) {
+            key_images(T, cs, b, keys[i], img);
+            if (img.empty()) throw Error(CCSD_ERR_ARG, "key maps to no stored element");
+            offs[i] = img[0].first;
+            sign[i] = img[0].second;
+        }
+        if (n == 0) return;
+        int64_t* dk = (int64_t*)c->dmalloc(n * sizeof(int64_t));
+        double* dv = (double*)c->dmalloc(n * sizeof(double));
+        CCSD_CUDA(cudaMemcpyAsync(dk, offs.data(), n * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream));
+        kern::kv_read(T.data, dk, dv, n, c->stream);
+        CCSD_CUDA(cudaMemcpyAsync(vals, dv, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CCSD_CUDA(cudaStreamSynchronize(c->stream));
+        for (int64_t i = 0; i < n; i++) vals[i] *= sign[i] == 0.0 ? 0.0 : sign[i];
+        c->dfree(dk, n * sizeof(int64_t));
+        c->dfree(dv, n * sizeof(double));
+    });
+}
+
+int ccsd_tensor_fill(ccsd_ctx ctx, ccsd_tensor t, double val) {
+    return guarded(ctx, [&] {
+        Context* c = from_handle(ctx);
+        Tensor& T = c->tensor(t);
+        kern::fill(T.data, T.total, val, c->stream);
+    });
+}
+
+static std::string plan_key(const char* kind, double alpha, int A, const char* iA, int B, const char* iB, double beta,
+                            int C, const char* iC, int prec) {
+    std::ostringstream o;
+    o.precision(17);
+    o << kind << '|' << alpha << '|' << A << ':' << iA << '|' << B << ':' << (iB ? iB : "") << '|' << beta << '|' << C
+      << ':' << (iC ? iC : "") << '|' << prec;
+    return o.str();
+}
+
+int ccsd_contract(ccsd_ctx ctx, double alpha, ccsd_tensor A, const char* idxA, ccsd_tensor B, const char* idxB,
+                  double beta, ccsd_tensor C, const char* idxC) {
+    return guarded(ctx, [&] {
+        Context* c = from_handle(ctx);
+        if (!idxA || !idxB || !idxC) throw Error(CCSD_ERR_ARG, "null index string");
+        std::string key = plan_key("mult", alpha, A, idxA, B, idxB, beta, C, idxC, 0);
+        auto it = c->plan_cache.find(key);
+        if (it == c->plan_cache.end()) {
+            auto p = std::make_unique<Plan>(plan_contract(*c, alpha, A, idxA, B, idxB, beta, C, idxC));
+            it = c->plan_cache.emplace(key, std::move(p)).first;
+        }
+        c->run(*it->second);
+    });
+}
+
+int ccsd_sum(ccsd_ctx ctx, double alpha, ccsd_tensor A, const char* idxA, double beta, ccsd_tensor B,
+             const char* idxB) {
+    return guarded(ctx, [&] {
+        Context* c = from_handle(ctx);
+        if (!idxA || !idxB) throw Error(CCSD_ERR_ARG, "null index string");
+        std::string key = plan_key("sum", alpha, A, idxA, 0, nullptr, beta, B, idxB, 0);
+        auto it = c->plan_cache.find(key);
+        if (it == c->plan_cache.end()) {
+            auto p = std::make_unique<Plan>(plan_sum(*c, alpha, A, idxA, beta, B, idxB));
+            it = c->plan_cache.emplace(key, std::move(p)).first;
+        }
+        c->run(*it->second);
+    });
+}
+
+int ccsd_scale(ccsd_ctx ctx, ccsd_tensor A, double alpha) {
+    return guarded(ctx, [&] {
+        Context* c = from_handle(ctx);
+        Tensor& T = c->tensor(A);
+        kern::scale(T.data, T.total, alpha, c->stream);
+    });
+}
+
+int ccsd_dot(ccsd_ctx ctx, ccsd_tensor A, const char* idxA, ccsd_tensor B, const char* idxB, double* out) {
+    return guarded(ctx, [&] {
+        Context* c = from_handle(ctx);
+        if (!idxA || !idxB || !out) throw Error(CCSD_ERR_ARG, "null argument");
+        std::string key = plan_key("dot", 1.0, A, idxA, B, idxB, 0.0, 0, nullptr, 0);
+        auto it = c->plan_cache.find(key);
+        if (it == c->plan_cache.end()) {
+            auto p = std::make_unique<Plan>(plan_dot(*c, A, idxA, B, idxB));
+            it = c->plan_cache.emplace(key, std::move(p)).first;
+        }
+        c->run(*it->second, out);
+    });
+}
+
+// SpinorbitalTensor::norm (spinorbital_tensor.cxx:1077-1109): p=0 max over spin cases;
+// p=1,2 weight each case by the number of spin-orbital arrangements it stands for.
+// Inside a case each antisymmetric same-spin element counts once (packed semantics).
+int ccsd_norm(ccsd_ctx ctx, ccsd_tensor A, int p, double* out) {
+    return guarded(ctx, [&] {
+        Context* c = from_handle(ctx);
+        if (p != 0 && p != 1 && p != 2) throw Error(CCSD_ERR_ARG, "p must be 0, 1 or 2");
+        Tensor& T = c->tensor(A);
+        CCSD_CUDA(cudaMemsetAsync(c->d_scalar, 0, sizeof(double), c->stream));
+        const int gs[4] = {T.nout[0], T.nout[1], T.nin[0], T.nin[1]};
+        for (auto& sc : T.cases) {
+            double factor = 1, perms = 1;
+            for (int g = 0; g < 4; g++) {
+                double b = 1;
+                for (int k = 0; k < sc.alpha[g]; k++) b = b * (gs[g] - k) / (k + 1);
+                factor *= b;
+                // unpacked storage holds every order of a same-spin run: a! * (n-a)!
+                int na = sc.alpha[g], nb = gs[g] - sc.alpha[g];
+                double f = 1;
+                for (int k = 2; k <= na; k++) f *= k;
+                for (int k = 2; k <= nb; k++) f *= k;
+                if (!T.packed()) perms *= f;
+            }
+            for (auto& b : sc.blocks) {
+                if (b.size == 0) continue;
+                kern::norm_accum(T.data + b.offset, b.size, p, factor / perms, c->d_scalar, c->stream);
+            }
+        }
+        double h = 0;
+        CCSD_CUDA(cudaMemcpyAsync(&h, c->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CCSD_CUDA(cudaStreamSynchronize(c->stream));
+        *out = p == 2 ? std::sqrt(h) : h;
+    });
+}
+
+int ccsd_weight(ccsd_ctx ctx, ccsd_tensor A, const double* dvrt_a, const double* dvrt_b, const double* docc_a,
+                const double* docc_b, double shift) {
+    return guarded(ctx, [&] {
+        Context* c = from_handle(ctx);
+        Tensor& T = c->tensor(A);
+        const Spaces& S = c->spaces;
+        const double* src[2][2] = {{dvrt_a, dvrt_b}, {docc_a, docc_b}};
+        double* dev[2][2];
+        for (int sp = 0; sp < 2; sp++)
+            for (int s = 0; s < 2; s++) {
+                int n = std::max(1, S.total(sp, s));
+                dev[sp][s] = (double*)c->dmalloc(n * sizeof(double));
+                if (S.total(sp, s) > 0)
+                    CCSD_CUDA(cudaMemcpyAsync(dev[sp][s], src[sp][s], S.total(sp, s) * sizeof(double),
+                                              cudaMemcpyHostToDevice, c->stream));
+            }
+        for (auto& sc : T.cases)
+            for (auto& b : sc.blocks) {
+                if (b.size == 0) continue;
+                if (!b.pairs.empty()) throw Error(CCSD_ERR_UNSUPPORTED, "weight of a packed tensor");
+                kern::WeightArgs w;
+                w.ndim = T.ndim;
+                w.total = b.size;
+                for (int p = 0; p < T.ndim; p++) {
+                    int sp = group_space(T.group[p]);
+                    w.len[p] = b.len[p];
+                    w.d[p] = dev[sp][sc.spin[p]] + S.off[sp][sc.spin[p]][b.irrep[p]];
+                }
+                kern::weight_block(T.data + b.offset, w, shift, c->stream);
+            }
+        CCSD_CUDA(cudaStreamSynchronize(c->stream));
+        for (int sp = 0; sp < 2; sp++)
+            for (int s = 0; s < 2; s++) c->dfree(dev[sp][s], std::max(1, S.total(sp, s)) * sizeof(double));
+    });
+}
+
+void ccsd_options_default(ccsd_options* opts) {
+    if (opts) options_default(opts);
+}
+
+int ccsd_hamiltonian_from_factor(ccsd_ctx ctx, int naux, const double* B, const double* eps,
+                                 const int* aux_per_irrep, int pack_vvvv, ccsd_hamiltonian* H) {
+    return guarded(ctx, [&] {
+        if (!B || !eps || !H || naux <= 0) throw Error(CCSD_ERR_ARG, "bad factor arguments");
+        build_hamiltonian(*from_handle(ctx), naux, B, eps, aux_per_irrep, pack_vvvv != 0, H);
+    });
+}
+
+int ccsd_hamiltonian_destroy(ccsd_ctx ctx, ccsd_hamiltonian* H) {
+    return guarded(ctx, [&] {
+        Context* c = from_handle(ctx);
+        for (ccsd_tensor* t : {&H->fAI, &H->fME, &H->fAE, &H->fMI, &H->VMNIJ, &H->VAMIJ, &H->VMNEJ, &H->VABIJ,
+                               &H->VMNEF, &H->VAMEI, &H->VAMEF, &H->VABEJ, &H->VABEF}) {
+            if (*t && c->tensors.count(*t)) c->destroy_tensor(*t);
+            *t = 0;
+        }
+    });
+}
+
+int ccsd_solver_create(ccsd_ctx ctx, const ccsd_hamiltonian* H, const ccsd_options* opts, ccsd_solver* out) {
+    if (!out) return CCSD_ERR_ARG;
+    *out = nullptr;
+    return guarded(ctx, [&] {
+        Context* c = from_handle(ctx);
+        ccsd_options o;
+        options_default(&o);
+        if (opts) o = *opts;
+        if (o.precision == CCSD_PREC_SPLIT && !kern::split_supported())
+            throw Error(CCSD_ERR_UNSUPPORTED, "split-BF16 GEMMs need an sm_100 device");
+        auto* h = new ccsd_solver_s;
+        h->ctx = ctx;
+        try {
+            h->s = new Solver(*c, *H, o);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int ccsd_solver_destroy(ccsd_solver s) {
+    if (!s) return CCSD_ERR_ARG;
+    int st = guarded(s->ctx, [&] { delete s->s; });
+    delete s;
+    return st;
+}
+
+int ccsd_solver_mp2(ccsd_solver s, double* mp2) {
+    if (!s) return CCSD_ERR_ARG;
+    return guarded(s->ctx, [&] { *mp2 = s->s->mp2; });
+}
+
+int ccsd_solver_iterate(ccsd_solver s, double* energy, double* conv) {
+    if (!s) return CCSD_ERR_ARG;
+    return guarded(s->ctx, [&] { s->s->iterate(energy, conv); });
+}
+
+int ccsd_solver_iterate_async(ccsd_solver s) {
+    if (!s) return CCSD_ERR_ARG;
+    return guarded(s->ctx, [&] { s->s->iterate_async(); });
+}
+
+int ccsd_solver_status(ccsd_solver s, double* energy, double* conv, int* iterations) {
+    if (!s) return CCSD_ERR_ARG;
+    return guarded(s->ctx, [&] {
+        s->s->read_status();
+        if (energy) *energy = s->s->energy;
+        if (conv) *conv = s->s->conv;
+        if (iterations) *iterations = s->s->iterations;
+    });
+}
+
+int ccsd_solver_run(ccsd_solver s, double* energy, double* conv, int* iterations) {
+    if (!s) return CCSD_ERR_ARG;
+    int status = CCSD_OK;
+    int g = guarded(s->ctx, [&] { status = s->s->run(energy, conv, iterations); });
+    return g != CCSD_OK ? g : status;
+}
+
+int ccsd_solver_amplitudes(ccsd_solver s, ccsd_tensor* T1, ccsd_tensor* T2) {
+    if (!s) return CCSD_ERR_ARG;
+    return guarded(s->ctx, [&] {
+        if (T1) *T1 = s->s->T1;
+        if (T2) *T2 = s->s->T2;
+    });
+}
+
+int ccsd_solver_flops(ccsd_solver s, double* flops) {
+    if (!s) return CCSD_ERR_ARG;
+    return guarded(s->ctx, [&] { *flops = s->s->flops_per_iter; });
+}
+
+}  // extern "C"

@@ -1,0 +1,331 @@
+// Context, device tensors and the step executor.
+//
+// Tensor layout follows the reference's SpinorbitalTensor / SymmetryBlockedTensor:
+// spin cases are the alpha counts of the four index groups with alpha indices first
+// (src/tensor/spinorbital_tensor.cxx:166-272, 387-432); inside a case, blocks are the
+// totally symmetric irrep tuples (src/tensor/symblocked_tensor.cxx:551-690), each a
+// dense array with the first index fastest (src/tensor/ctf_tensor.hpp:221-226).
+#include <algorithm>
+#include <cstring>
+#include <numeric>
+
+#include "engine.hpp"
+
+namespace ccsd {
+
+Context::Context(int dev, cudaStream_t s) : device(dev), stream(s) {
+    CCSD_CUDA(cudaSetDevice(device));
+    if (!stream) {
+        CCSD_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        own_stream = true;
+    }
+    d_scalar = (double*)dmalloc(64 * sizeof(double));
+}
+
+Context::~Context() {
+    cudaSetDevice(device);
+    cudaStreamSynchronize(stream);
+    for (auto& kv : plan_cache) release(*kv.second);
+    plan_cache.clear();
+    for (auto& kv : split_cache) {
+        cudaFree(kv.second.data);
+        cudaFree(kv.second.scale);
+    }
+    cudaFree(split_ws.a.data);
+    cudaFree(split_ws.a.scale);
+    cudaFree(split_ws.b.data);
+    cudaFree(split_ws.b.scale);
+    cudaFree(split_ws.rowmax);
+    for (auto& kv : tensors) cudaFree(kv.second->data);
+    cudaFree(d_scalar);
+    if (own_stream) cudaStreamDestroy(stream);
+}
+
+void* Context::dmalloc(size_t bytes) {
+    void* p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMallocAsync(&p, bytes, stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        throw Error(CCSD_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes failed");
+    }
+    device_bytes += bytes;
+    return p;
+}
+
+void Context::dfree(void* p, size_t bytes) {
+    if (!p) return;
+    cudaFreeAsync(p, stream);
+    device_bytes -= bytes;
+}
+
+Tensor& Context::tensor(int h) {
+    auto it = tensors.find(h);
+    if (it == tensors.end()) throw Error(CCSD_ERR_ARG, "unknown tensor handle " + std::to_string(h));
+    return *it->second;
+}
+
+bool Context::is_constant(int h) const {
+    return std::find(constant_tensors.begin(), constant_tensors.end(), h) != constant_tensors.end();
+}
+
+int Context::create_tensor(const std::string& name, const int nout[2], const int nin[2], int flags) {
+    if (!spaces_set) throw Error(CCSD_ERR_ARG, "spaces not set on this context");
+    auto T = std::make_unique<Tensor>();
+    T->name = name;
+    T->flags = flags;
+    for (int s = 0; s < 2; s++) {
+        if (nout[s] < 0 || nin[s] < 0 || nout[s] > 4 || nin[s] > 4) throw Error(CCSD_ERR_ARG, "bad tensor shape");
+        T->nout[s] = nout[s];
+        T->nin[s] = nin[s];
+    }
+    const int gsize[4] = {nout[0], nout[1], nin[0], nin[1]};
+    for (int g = 0; g < 4; g++)
+        for (int k = 0; k < gsize[g]; k++) T->group.push_back(g);
+    T->ndim = (int)T->group.size();
+    if (T->ndim > 8) throw Error(CCSD_ERR_ARG, "tensor rank above 8");
+    const int nouttot = nout[0] + nout[1], nintot = nin[0] + nin[1];
+    if ((nintot - nouttot) % 2) throw Error(CCSD_ERR_ARG, "odd spin imbalance");
+    const int nirr = spaces.nirrep;
+    int64_t offset = 0;
+    // spin cases: #alpha(lower) = #alpha(upper) + (nin - nout)/2  (spinorbital_tensor.cxx:183)
+    for (int a0 = 0; a0 <= gsize[0]; a0++)
+        for (int a1 = 0; a1 <= gsize[1]; a1++)
+            for (int a2 = 0; a2 <= gsize[2]; a2++)
+                for (int a3 = 0; a3 <= gsize[3]; a3++) {
+                    if (a2 + a3 != a0 + a1 + (nintot - nouttot) / 2) continue;
+                    SpinCase sc;
+                    sc.alpha[0] = a0;
+                    sc.alpha[1] = a1;
+                    sc.alpha[2] = a2;
+                    sc.alpha[3] = a3;
+                    for (int g = 0; g < 4; g++)
+                        for (int k = 0; k < gsize[g]; k++) sc.spin.push_back(k < sc.alpha[g] ? ALPHA : BETA);
+                    // irrep tuples with XOR 0
+                    std::vector<int> irr(T->ndim, 0);
+                    while (true) {
+                        int x = 0;
+                        for (int h : irr) x ^= h;
+                        if (x == 0) {
+                            Block b;
+                            b.irrep = irr;
+                            b.len.resize(T->ndim);
+                            b.stride.assign(T->ndim, 0);
+                            bool stored = true;
+                            for (int p = 0; p < T->ndim; p++)
+                                b.len[p] = spaces.n[group_space(T->group[p])][sc.spin[p]][irr[p]];
+                            // packed same-spin pairs
+                            if (T->packed()) {
+                                for (int g = 0; g < 4; g++) {
+                                    if (gsize[g] != 2) continue;
+                                    int p = 0;
+                                    while (T->group[p] != g) p++;
+                                    if (sc.spin[p] != sc.spin[p + 1]) continue;
+                                    Block::Pair pr;
+                                    pr.p = p;
+                                    pr.q = p + 1;
+                                    if (irr[p] == irr[p + 1]) pr.kind = 1;
+                                    else if (irr[p] < irr[p + 1]) pr.kind = 2;
+                                    else stored = false;
+                                    b.pairs.push_back(pr);
+                                }
+                            }
+                            if (stored) {
+                                int64_t st = 1;
+                                for (int p = 0; p < T->ndim; p++) {
+                                    int pi = b.pair_of(p);
+                                    if (pi >= 0) {
+                                        auto& pr = b.pairs[pi];
+                                        if (pr.p != p) continue;
+                                        pr.stride = st;
+                                        int64_t n0 = b.len[pr.p], n1 = b.len[pr.q];
+                                        st *= pr.kind == 1 ? n0 * (n0 - 1) / 2 : n0 * n1;
+                                    } else {
+                                        b.stride[p] = st;
+                                        st *= b.len[p];
+                                    }
+                                }
+                                b.size = st;
+                                b.offset = offset;
+                                offset += st;
+                                sc.block_of[irr] = (int)sc.blocks.size();
+                                sc.blocks.push_back(b);
+                            }
+                        }
+                        int i = 0;
+                        for (; i < T->ndim; i++) {
+                            if (++irr[i] < nirr) break;
+                            irr[i] = 0;
+                        }
+                        if (i == T->ndim) break;
+                    }
+                    T->cases.push_back(sc);
+                }
+    T->total = offset;
+    T->data = (double*)dmalloc(std::max<int64_t>(offset, 1) * sizeof(double));
+    CCSD_CUDA(cudaMemsetAsync(T->data, 0, std::max<int64_t>(offset, 1) * sizeof(double), stream));
+    int h = next_handle++;
+    tensors[h] = std::move(T);
+    return h;
+}
+
+void Context::destroy_tensor(int h) {
+    Tensor& T = tensor(h);
+    // drop cached plans that mention this tensor
+    for (auto it = plan_cache.begin(); it != plan_cache.end();) {
+        bool uses = false;
+        for (auto& g : it->second->gemms) uses |= g.tA == h || g.tB == h || g.tC == h;
+        for (auto& g : it->second->sums) uses |= g.tA == h || g.tC == h;
+        for (auto& g : it->second->scales) uses |= g.tC == h;
+        for (auto& g : it->second->dots) uses |= g.tA == h || g.tB == h;
+        if (uses) {
+            release(*it->second);
+            it = plan_cache.erase(it);
+        } else {
+            ++it;
+        }
+    }
+    for (auto it = split_cache.begin(); it != split_cache.end();) {
+        // cache keys are opaque; drop everything conservatively
+        dfree(it->second.data, 0);
+        dfree(it->second.scale, 0);
+        device_bytes -= it->second.bytes;
+        it = split_cache.erase(it);
+    }
+    constant_tensors.erase(std::remove(constant_tensors.begin(), constant_tensors.end(), h), constant_tensors.end());
+    dfree(T.data, std::max<int64_t>(T.total, 1) * sizeof(double));
+    tensors.erase(h);
+}
+
+// ---------------------------------------------------------------------------
+// executor
+// ---------------------------------------------------------------------------
+
+static int64_t* upload_table(Context& ctx, const std::vector<int64_t>& h) {
+    if (h.empty()) return nullptr;
+    int64_t* d = (int64_t*)ctx.dmalloc(h.size() * sizeof(int64_t));
+    CCSD_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(int64_t), cudaMemcpyHostToDevice, ctx.stream));
+    return d;
+}
+
+void Context::upload(Plan& p) {
+    bool any = false;
+    for (auto& g : p.gemms) {
+        if (g.dAm) continue;
+        any = true;
+        g.dAm = upload_table(*this, g.hAm);
+        g.dAk = upload_table(*this, g.hAk);
+        g.dBk = upload_table(*this, g.hBk);
+        g.dBn = upload_table(*this, g.hBn);
+        for (int v = 0; v < g.nvm; v++) g.dCm[v] = upload_table(*this, g.hCm[v]);
+        for (int v = 0; v < g.nvn; v++) g.dCn[v] = upload_table(*this, g.hCn[v]);
+    }
+    // tables are uploaded from pageable host memory; make sure the copies have been
+    // staged before the host vectors could change
+    if (any) CCSD_CUDA(cudaStreamSynchronize(stream));
+}
+
+void Context::release(Plan& p) {
+    for (auto& g : p.gemms) {
+        auto fr = [&](int64_t*& d, size_t n) {
+            if (d) dfree(d, n * sizeof(int64_t));
+            d = nullptr;
+        };
+        fr(g.dAm, g.hAm.size());
+        fr(g.dAk, g.hAk.size());
+        fr(g.dBk, g.hBk.size());
+        fr(g.dBn, g.hBn.size());
+        for (int v = 0; v < 2; v++) {
+            fr(g.dCm[v], g.hCm[v].size());
+            fr(g.dCn[v], g.hCn[v].size());
+        }
+    }
+}
+
+void Context::run_gemm(GemmStep& g) {
+    Tensor& A = tensor(g.tA);
+    Tensor& B = tensor(g.tB);
+    Tensor& C = tensor(g.tC);
+    kern::GemmArgs a;
+    a.A = A.data;
+    a.B = B.data;
+    a.C = C.data;
+    a.M = g.M;
+    a.N = g.N;
+    a.K = g.K;
+    a.alpha = g.alpha;
+    a.Am = g.dAm;
+    a.Ak = g.dAk;
+    a.Bk = g.dBk;
+    a.Bn = g.dBn;
+    a.Cm[0] = g.dCm[0];
+    a.Cm[1] = g.dCm[1];
+    a.Cn[0] = g.dCn[0];
+    a.Cn[1] = g.dCn[1];
+    a.nvm = g.nvm;
+    a.nvn = g.nvn;
+    for (int i = 0; i < 4; i++) a.vsign[i] = g.vsign[i];
+    a.a_kcontig = g.a_kcontig;
+    a.b_kcontig = g.b_kcontig;
+    if (precision == CCSD_PREC_SPLIT && kern::split_supported()) {
+        run_split_gemm(g, a);
+    } else {
+        kern::gemm_fp64(a, stream);
+    }
+}
+
+void Context::run(Plan& p, double* scalar_out, double* dot_target) {
+    upload(p);
+    bool zeroed = dot_target != nullptr;
+    double* acc = dot_target ? dot_target : d_scalar;
+    for (auto& st : p.steps) {
+        switch (st.kind) {
+            case Step::GEMM: run_gemm(p.gemms[st.idx]); break;
+            case Step::SUM: {
+                auto& s = p.sums[st.idx];
+                kern::StridedArgs a;
+                a.ndim = s.ndim;
+                a.total = 1;
+                for (int d = 0; d < s.ndim; d++) {
+                    a.len[d] = s.len[d];
+                    a.sA[d] = s.sA[d];
+                    a.sB[d] = s.sC[d];
+                    a.total *= s.len[d];
+                }
+                kern::sum_strided(tensor(s.tA).data + s.offA, tensor(s.tC).data + s.offC, a, s.alpha, stream);
+                break;
+            }
+            case Step::SCALE: {
+                auto& s = p.scales[st.idx];
+                kern::scale(tensor(s.tC).data + s.off, s.n, s.beta, stream);
+                break;
+            }
+            case Step::DOT: {
+                auto& d = p.dots[st.idx];
+                if (!zeroed) {
+                    CCSD_CUDA(cudaMemsetAsync(d_scalar, 0, sizeof(double), stream));
+                    zeroed = true;
+                }
+                kern::StridedArgs a;
+                a.ndim = d.ndim;
+                a.total = 1;
+                for (int k = 0; k < d.ndim; k++) {
+                    a.len[k] = d.len[k];
+                    a.sA[k] = d.sA[k];
+                    a.sB[k] = d.sB[k];
+                    a.total *= d.len[k];
+                }
+                kern::dot_strided(tensor(d.tA).data + d.offA, tensor(d.tB).data + d.offB, a, d.alpha, acc, stream);
+                break;
+            }
+        }
+    }
+    if (scalar_out) {
+        if (!zeroed) CCSD_CUDA(cudaMemsetAsync(d_scalar, 0, sizeof(double), stream));
+        CCSD_CUDA(cudaMemcpyAsync(scalar_out, d_scalar, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CCSD_CUDA(cudaStreamSynchronize(stream));
+    }
+    CCSD_CUDA(cudaGetLastError());
+}
+
+}  // namespace ccsd

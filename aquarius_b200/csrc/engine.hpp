@@ -1,0 +1,227 @@
+// Host-side engine: device tensors, the statement planner and the step executor.
+//
+// The planner reproduces, once per statement, what the reference recomputes on
+// every call: the spin-case expansion of SpinorbitalTensor::mult/sum
+// (src/tensor/spinorbital_tensor.cxx:455-1018) and the irrep-block walk of
+// SymmetryBlockedTensor::mult/sum (src/tensor/symblocked_tensor.cxx:863-1223).
+// Its output is a list of steps (block GEMMs with gather/scatter tables,
+// strided block sums, scalings) that the executor replays on a CUDA stream.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+#include <map>
+#include <memory>
+#include <stdexcept>
+
+#include <cuda_runtime.h>
+
+#include "ccsd_b200.h"
+#include "kernels.hpp"
+
+namespace ccsd {
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define CCSD_CUDA(call)                                                                  \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            throw ::ccsd::Error(CCSD_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+enum { VRT = 0, OCC = 1 };
+enum { ALPHA = 0, BETA = 1 };
+
+// group g of a spin-orbital tensor: 0 upper vrt, 1 upper occ, 2 lower vrt, 3 lower occ
+inline int group_space(int g) { return g % 2 == 0 ? VRT : OCC; }
+
+struct Spaces {
+    int nirrep = 1;
+    int n[2][2][8] = {};          // [space][spin][irrep]
+    int off[2][2][8] = {};        // offset of irrep inside the spin-space range
+    int total(int space, int spin) const {
+        int s = 0;
+        for (int h = 0; h < nirrep; h++) s += n[space][spin][h];
+        return s;
+    }
+};
+
+struct Block {
+    std::vector<int> irrep;       // per position
+    std::vector<int> len;         // per position
+    std::vector<int64_t> stride;  // per position (unpacked dims); packed pairs handled via pair_* fields
+    int64_t offset = 0;           // element offset in the tensor storage
+    int64_t size = 0;
+    // packed pairs (adjacent positions p, p+1 of one group, same spin) stored once in
+    // canonical order: kind 1 = triangle x<y (equal irreps), kind 2 = rectangle (irrep p < irrep q)
+    struct Pair {
+        int p = -1, q = -1;
+        int kind = 0;
+        int64_t stride = 0;
+    };
+    std::vector<Pair> pairs;
+    int pair_of(int pos) const {
+        for (size_t i = 0; i < pairs.size(); i++)
+            if (pairs[i].p == pos || pairs[i].q == pos) return (int)i;
+        return -1;
+    }
+};
+
+struct SpinCase {
+    int alpha[4] = {0, 0, 0, 0};  // alpha count per group
+    std::vector<int> spin;        // per position
+    std::vector<Block> blocks;
+    std::map<std::vector<int>, int> block_of;   // irreps -> block index (only stored blocks)
+};
+
+struct Tensor {
+    std::string name;
+    int nout[2] = {0, 0}, nin[2] = {0, 0};
+    int ndim = 0;
+    int flags = 0;
+    std::vector<int> group;       // per position
+    std::vector<SpinCase> cases;
+    double* data = nullptr;       // device
+    int64_t total = 0;
+
+    int find_case(const int alpha[4]) const {
+        for (size_t c = 0; c < cases.size(); c++) {
+            bool ok = true;
+            for (int g = 0; g < 4; g++) ok &= cases[c].alpha[g] == alpha[g];
+            if (ok) return (int)c;
+        }
+        return -1;
+    }
+    bool packed() const { return flags & CCSD_TENSOR_PACKED; }
+};
+
+// ---------------------------------------------------------------------------
+// planned steps
+// ---------------------------------------------------------------------------
+
+// One block contraction lowered to GEMM form:
+//   for every destination variant v (sign s_v):
+//     C[offCm_v[m] + offCn_v[n]] += s_v * alpha * sum_k A[offAm[m]+offAk[k]] * B[offBk[k]+offBn[n]]
+struct GemmStep {
+    int tA = 0, tB = 0, tC = 0;        // tensor handles (for slicing caches / constness)
+    int M = 0, N = 0, K = 0;
+    double alpha = 0;
+    int nvm = 1, nvn = 1;              // destination variants along m and n
+    double vsign[4] = {1, 1, 1, 1};    // sign of variant (im * nvn + in)
+    // host copies (for planning / flop counts) and device tables
+    std::vector<int64_t> hAm, hAk, hBk, hBn, hCm[2], hCn[2];
+    int64_t *dAm = nullptr, *dAk = nullptr, *dBk = nullptr, *dBn = nullptr;
+    int64_t *dCm[2] = {nullptr, nullptr}, *dCn[2] = {nullptr, nullptr};
+    bool a_mcontig = false, a_kcontig = false, b_kcontig = false, b_ncontig = false;
+    double flops() const { return 2.0 * M * N * (double)K; }
+    int64_t split_cache = -1;          // key of cached A slices (constant operand)
+};
+
+// C[perm] += alpha * A  over one block (strided, up to 8 dims)
+struct SumStep {
+    int tA = 0, tC = 0;
+    int ndim = 0;
+    int64_t len[8];
+    int64_t sA[8], sC[8];
+    int64_t offA = 0, offC = 0;
+    double alpha = 0;
+};
+
+// C_block *= beta (beta == 0: zero-fill)
+struct ScaleStep {
+    int tC = 0;
+    int64_t off = 0, n = 0;
+    double beta = 1;
+};
+
+// scalar += alpha * sum A_blk[x] * B_blk[perm x]  (strided)
+struct DotStep {
+    int tA = 0, tB = 0;
+    int ndim = 0;
+    int64_t len[8];
+    int64_t sA[8], sB[8];
+    int64_t offA = 0, offB = 0;
+    double alpha = 0;
+};
+
+struct Step {
+    enum Kind { GEMM, SUM, SCALE, DOT } kind;
+    int idx;                           // index into the typed vector of the plan
+};
+
+struct Plan {
+    std::vector<Step> steps;
+    std::vector<GemmStep> gemms;
+    std::vector<SumStep> sums;
+    std::vector<ScaleStep> scales;
+    std::vector<DotStep> dots;
+    double flops() const {
+        double f = 0;
+        for (auto& g : gemms) f += g.flops();
+        return f;
+    }
+    void append(Plan&& other);
+};
+
+class Context;
+
+// Plans C[idxC] = beta C + alpha A[idxA] B[idxB]  (B may be 0 for a sum)
+Plan plan_contract(Context& ctx, double alpha, int A, const std::string& idxA, int B, const std::string& idxB,
+                   double beta, int C, const std::string& idxC);
+Plan plan_sum(Context& ctx, double alpha, int A, const std::string& idxA, double beta, int C,
+              const std::string& idxC);
+Plan plan_dot(Context& ctx, int A, const std::string& idxA, int B, const std::string& idxB);
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+
+class Context {
+public:
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    Spaces spaces;
+    bool spaces_set = false;
+    std::map<int, std::unique_ptr<Tensor>> tensors;
+    int next_handle = 1;
+    std::string last_error;
+    int64_t device_bytes = 0;
+    int64_t launches = 0;
+    int precision = CCSD_PREC_FP64;
+    int slices = 0;
+    double* d_scalar = nullptr;        // device accumulator for dots
+    kern::SplitWorkspace split_ws;     // scratch for split-BF16 GEMMs
+    std::map<int64_t, kern::SlicedOperand> split_cache;   // sliced constant operands
+    int64_t split_cache_next = 1;
+    std::map<std::string, std::unique_ptr<Plan>> plan_cache;
+
+    Context(int device, cudaStream_t s);
+    ~Context();
+
+    Tensor& tensor(int h);
+    int create_tensor(const std::string& name, const int nout[2], const int nin[2], int flags);
+    void destroy_tensor(int h);
+    void* dmalloc(size_t bytes);
+    void dfree(void* p, size_t bytes);
+
+    // execute a plan on the stream (device tables uploaded lazily)
+    void upload(Plan& p);
+    void release(Plan& p);
+    // scalar_out: host destination of the dot result (synchronises); dot_target: device
+    // accumulator the dots add into instead of the context scalar (not zeroed here)
+    void run(Plan& p, double* scalar_out = nullptr, double* dot_target = nullptr);
+    void run_gemm(GemmStep& g);
+    void run_split_gemm(GemmStep& g, kern::GemmArgs& a);
+    std::vector<int> constant_tensors;  // handles whose contents never change (sliced once)
+    bool is_constant(int h) const;
+};
+
+Context* from_handle(ccsd_ctx c);
+
+}  // namespace ccsd

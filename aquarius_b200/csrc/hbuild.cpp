@@ -1,0 +1,260 @@
+// Device-side assembly of the 13 spin-orbital blocks of H from a three-index factor.
+//
+// Role of the reference's H producers (src/operator/aomoints.cxx:1357-1387 assembly,
+// src/operator/fakemoints.cxx:15-52 for synthetic sizes): every two-electron block is
+// the antisymmetrised physicist-notation integral
+//     <pq||rs> = (pr|qs) d(sp,sr) d(sq,ss) - (ps|qr) d(sp,ss) d(sq,sr),
+// with the index order [upper..., lower...] of TwoElectronOperator
+// (src/operator/2eoperator.cxx:13-21), and (pq|rs) = sum_P B[P,p,q] B[P,r,s].
+// Each Coulomb / exchange piece of a block is one FP64 gather-GEMM over P whose
+// epilogue scatters straight into the block; blocks stored with packed pairs (V_abcd)
+// go through a chunked temporary and a pack kernel.
+#include <algorithm>
+#include <cstring>
+
+#include "engine.hpp"
+#include "hbuild.hpp"
+
+namespace ccsd {
+
+namespace {
+
+// device copies of host index tables, freed together
+struct Tables {
+    Context& ctx;
+    std::vector<std::pair<int64_t*, size_t>> held;
+    int64_t* up(const std::vector<int64_t>& h) {
+        int64_t* d = (int64_t*)ctx.dmalloc(h.size() * sizeof(int64_t));
+        CCSD_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(int64_t), cudaMemcpyHostToDevice, ctx.stream));
+        held.push_back({d, h.size() * sizeof(int64_t)});
+        return d;
+    }
+    ~Tables() {
+        cudaStreamSynchronize(ctx.stream);
+        for (auto& p : held) ctx.dfree(p.first, p.second);
+    }
+};
+
+struct Builder {
+    Context& ctx;
+    int n, naux, o;
+    double* dB = nullptr;
+    std::vector<int> aux_irrep;   // per P
+    bool aux_known = false;
+
+    // global spatial index of (space, irrep, x)
+    int gidx(int space, int irrep, int x) const {
+        const Spaces& S = ctx.spaces;
+        int base = space == OCC ? 0 : o;
+        return base + S.off[space][ALPHA][irrep] + x;
+    }
+
+    std::vector<int64_t> aux_list(int irrep) const {
+        std::vector<int64_t> k;
+        for (int P = 0; P < naux; P++)
+            if (!aux_known || aux_irrep[P] == irrep) k.push_back((int64_t)P * n * n);
+        return k;
+    }
+
+    // (x0 x1 | x2 x3) pieces over positions (pa, pb | pc, pd) of a block, scattered into
+    // C with sign: C[off + sum stride*x] += sign * sum_P B[P,a,b] B[P,c,d]
+    void coulomb(double* C, int64_t off, const int* space, const int* irrep, const int* len,
+                 const int64_t* stride, int pa, int pb, int pc, int pd, double sign) {
+        int64_t M = (int64_t)len[pa] * len[pb], N = (int64_t)len[pc] * len[pd];
+        if (M == 0 || N == 0) return;
+        std::vector<int64_t> k = aux_list(irrep[pa] ^ irrep[pb]);
+        if (k.empty()) return;
+        kern::GemmArgs a;
+        std::vector<int64_t> Am(M), Bn(N), Cm(M), Cn(N);
+        for (int y = 0; y < len[pb]; y++)
+            for (int x = 0; x < len[pa]; x++) {
+                int64_t m = x + (int64_t)len[pa] * y;
+                Am[m] = (int64_t)gidx(space[pa], irrep[pa], x) * n + gidx(space[pb], irrep[pb], y);
+                Cm[m] = off + stride[pa] * x + stride[pb] * y;
+            }
+        for (int y = 0; y < len[pd]; y++)
+            for (int x = 0; x < len[pc]; x++) {
+                int64_t m = x + (int64_t)len[pc] * y;
+                Bn[m] = (int64_t)gidx(space[pc], irrep[pc], x) * n + gidx(space[pd], irrep[pd], y);
+                Cn[m] = stride[pc] * x + stride[pd] * y;
+            }
+        Tables tb{ctx, {}};
+        int64_t *dAm = tb.up(Am), *dK = tb.up(k), *dBn = tb.up(Bn), *dCm = tb.up(Cm), *dCn = tb.up(Cn);
+        a.A = dB;
+        a.B = dB;
+        a.C = C;
+        a.M = (int)M;
+        a.N = (int)N;
+        a.K = (int)k.size();
+        a.alpha = sign;
+        a.Am = dAm;
+        a.Ak = dK;
+        a.Bk = dK;
+        a.Bn = dBn;
+        a.Cm[0] = dCm;
+        a.Cn[0] = dCn;
+        a.a_kcontig = false;
+        a.b_kcontig = false;
+        kern::gemm_fp64(a, ctx.stream);
+    }
+
+    void one_electron(int h, const double* eps) {
+        Tensor& T = ctx.tensor(h);
+        for (auto& sc : T.cases)
+            for (auto& b : sc.blocks) {
+                if (b.size == 0) continue;
+                int sp0 = group_space(T.group[0]), sp1 = group_space(T.group[1]);
+                if (sp0 != sp1 || b.irrep[0] != b.irrep[1] || sc.spin[0] != sc.spin[1]) continue;
+                std::vector<double> host(b.size, 0.0);
+                for (int x = 0; x < b.len[0]; x++) host[x + (int64_t)x * b.len[0]] = eps[gidx(sp0, b.irrep[0], x)];
+                CCSD_CUDA(cudaMemcpy(T.data + b.offset, host.data(), b.size * sizeof(double), cudaMemcpyHostToDevice));
+            }
+    }
+
+    void two_electron(int h) {
+        Tensor& T = ctx.tensor(h);
+        for (auto& sc : T.cases)
+            for (auto& b : sc.blocks) {
+                if (b.size == 0) continue;
+                int space[4], irr[4], len[4];
+                for (int p = 0; p < 4; p++) {
+                    space[p] = group_space(T.group[p]);
+                    irr[p] = b.irrep[p];
+                    len[p] = b.len[p];
+                }
+                const std::vector<int>& s = sc.spin;
+                bool J = s[0] == s[2] && s[1] == s[3];
+                bool K = s[0] == s[3] && s[1] == s[2];
+                if (b.pairs.empty()) {
+                    if (J) coulomb(T.data, b.offset, space, irr, len, b.stride.data(), 0, 2, 1, 3, 1.0);
+                    if (K) coulomb(T.data, b.offset, space, irr, len, b.stride.data(), 0, 3, 1, 2, -1.0);
+                } else {
+                    packed_block(T, sc, b, space, irr, len, J, K);
+                }
+            }
+    }
+
+    // packed V_abcd-type block: chunk over the first index, build (ac|bd) and (ad|bc)
+    // unpacked for the chunk, then pack <ab||cd> for canonical pairs
+    void packed_block(Tensor& T, const SpinCase& sc, const Block& b, const int* space, const int* irr,
+                      const int* len, bool J, bool K) {
+        (void)sc;
+        if (b.pairs.size() != 2 || b.pairs[0].p != 0 || b.pairs[1].p != 2)
+            throw Error(CCSD_ERR_UNSUPPORTED, "packed build supports <ab||cd> pair layouts only");
+        const int64_t per_a = (int64_t)len[1] * len[2] * len[3];
+        int64_t chunk = std::max<int64_t>(1, (int64_t)(256ll << 20) / std::max<int64_t>(per_a, 1));
+        chunk = std::min<int64_t>(chunk, len[0]);
+        double* tJ = (double*)ctx.dmalloc(std::max<int64_t>(chunk * per_a, 1) * sizeof(double));
+        double* tK = (double*)ctx.dmalloc(std::max<int64_t>(chunk * per_a, 1) * sizeof(double));
+        for (int a0 = 0; a0 < len[0]; a0 += (int)chunk) {
+            int a1 = std::min<int>(len[0], a0 + (int)chunk);
+            int ca = a1 - a0;
+            CCSD_CUDA(cudaMemsetAsync(tJ, 0, (size_t)ca * per_a * sizeof(double), ctx.stream));
+            CCSD_CUDA(cudaMemsetAsync(tK, 0, (size_t)ca * per_a * sizeof(double), ctx.stream));
+            // tJ[a', c, b, d] = (a c | b d) ; tK[a', d, b, c] = (a d | b c)   (a' = a - a0)
+            int lenc[4] = {ca, len[2], len[1], len[3]};
+            int spc[4] = {space[0], space[2], space[1], space[3]};
+            int irc[4] = {irr[0], irr[2], irr[1], irr[3]};
+            int64_t st[4] = {1, ca, (int64_t)ca * len[2], (int64_t)ca * len[2] * len[1]};
+            if (J) coulomb_shift(tJ, spc, irc, lenc, st, a0, 1.0);
+            int lenk[4] = {ca, len[3], len[1], len[2]};
+            int spk[4] = {space[0], space[3], space[1], space[2]};
+            int irk[4] = {irr[0], irr[3], irr[1], irr[2]};
+            int64_t sk[4] = {1, ca, (int64_t)ca * len[3], (int64_t)ca * len[3] * len[1]};
+            if (K) coulomb_shift(tK, spk, irk, lenk, sk, a0, 1.0);
+            kern::pack_vvvv(T.data + b.offset, b.pairs[0].kind, b.pairs[1].kind, len[0], len[1], len[2], len[3],
+                            b.pairs[1].stride, tJ, tK, a0, a1, J, K, ctx.stream);
+        }
+        CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
+        ctx.dfree(tJ, chunk * per_a * sizeof(double));
+        ctx.dfree(tK, chunk * per_a * sizeof(double));
+    }
+
+    // like coulomb() over positions (0,1 | 2,3) of a temporary whose position 0 starts at a0
+    void coulomb_shift(double* C, const int* space, const int* irrep, const int* len, const int64_t* stride, int a0,
+                       double sign) {
+        int64_t M = (int64_t)len[0] * len[1], N = (int64_t)len[2] * len[3];
+        if (M == 0 || N == 0) return;
+        std::vector<int64_t> k = aux_list(irrep[0] ^ irrep[1]);
+        if (k.empty()) return;
+        std::vector<int64_t> Am(M), Bn(N), Cm(M), Cn(N);
+        for (int y = 0; y < len[1]; y++)
+            for (int x = 0; x < len[0]; x++) {
+                int64_t m = x + (int64_t)len[0] * y;
+                Am[m] = (int64_t)gidx(space[0], irrep[0], a0 + x) * n + gidx(space[1], irrep[1], y);
+                Cm[m] = stride[0] * x + stride[1] * y;
+            }
+        for (int y = 0; y < len[3]; y++)
+            for (int x = 0; x < len[2]; x++) {
+                int64_t m = x + (int64_t)len[2] * y;
+                Bn[m] = (int64_t)gidx(space[2], irrep[2], x) * n + gidx(space[3], irrep[3], y);
+                Cn[m] = stride[2] * x + stride[3] * y;
+            }
+        Tables tb{ctx, {}};
+        int64_t *dAm = tb.up(Am), *dK = tb.up(k), *dBn = tb.up(Bn), *dCm = tb.up(Cm), *dCn = tb.up(Cn);
+        kern::GemmArgs a;
+        a.A = dB;
+        a.B = dB;
+        a.C = C;
+        a.M = (int)M;
+        a.N = (int)N;
+        a.K = (int)k.size();
+        a.alpha = sign;
+        a.Am = dAm;
+        a.Ak = dK;
+        a.Bk = dK;
+        a.Bn = dBn;
+        a.Cm[0] = dCm;
+        a.Cn[0] = dCn;
+        kern::gemm_fp64(a, ctx.stream);
+    }
+};
+
+int mk(Context& c, const char* name, int o0, int o1, int i0, int i1, int flags = 0) {
+    int nout[2] = {o0, o1}, nin[2] = {i0, i1};
+    return c.create_tensor(name, nout, nin, flags);
+}
+
+}  // namespace
+
+void build_hamiltonian(Context& ctx, int naux, const double* B, const double* eps, const int* aux_per_irrep,
+                       bool pack_vvvv, ccsd_hamiltonian* H) {
+    const Spaces& S = ctx.spaces;
+    for (int h = 0; h < S.nirrep; h++)
+        for (int sp = 0; sp < 2; sp++)
+            if (S.n[sp][ALPHA][h] != S.n[sp][BETA][h])
+                throw Error(CCSD_ERR_ARG, "the factor builder needs a closed-shell (alpha = beta) space");
+    Builder bld{ctx, S.total(VRT, ALPHA) + S.total(OCC, ALPHA), naux, S.total(OCC, ALPHA)};
+    if (aux_per_irrep) {
+        bld.aux_known = true;
+        for (int h = 0; h < S.nirrep; h++)
+            for (int k = 0; k < aux_per_irrep[h]; k++) bld.aux_irrep.push_back(h);
+        if ((int)bld.aux_irrep.size() != naux) throw Error(CCSD_ERR_ARG, "aux_per_irrep does not sum to naux");
+    }
+    const int64_t nB = (int64_t)naux * bld.n * bld.n;
+    bld.dB = (double*)ctx.dmalloc(nB * sizeof(double));
+    CCSD_CUDA(cudaMemcpyAsync(bld.dB, B, nB * sizeof(double), cudaMemcpyHostToDevice, ctx.stream));
+
+    H->fAI = mk(ctx, "f(ai)", 1, 0, 0, 1);
+    H->fME = mk(ctx, "f(ia)", 0, 1, 1, 0);
+    H->fAE = mk(ctx, "f(ab)", 1, 0, 1, 0);
+    H->fMI = mk(ctx, "f(ij)", 0, 1, 0, 1);
+    H->VMNIJ = mk(ctx, "<ij||kl>", 0, 2, 0, 2);
+    H->VAMIJ = mk(ctx, "<ai||jk>", 1, 1, 0, 2);
+    H->VMNEJ = mk(ctx, "<ij||ak>", 0, 2, 1, 1);
+    H->VABIJ = mk(ctx, "<ab||ij>", 2, 0, 0, 2);
+    H->VMNEF = mk(ctx, "<ij||ab>", 0, 2, 2, 0);
+    H->VAMEI = mk(ctx, "<ai||bj>", 1, 1, 1, 1);
+    H->VAMEF = mk(ctx, "<ai||bc>", 1, 1, 2, 0);
+    H->VABEJ = mk(ctx, "<ab||ci>", 2, 0, 1, 1);
+    H->VABEF = mk(ctx, "<ab||cd>", 2, 0, 2, 0, pack_vvvv ? CCSD_TENSOR_PACKED : 0);
+
+    bld.one_electron(H->fAE, eps);
+    bld.one_electron(H->fMI, eps);
+    for (int h : {H->VMNIJ, H->VAMIJ, H->VMNEJ, H->VABIJ, H->VMNEF, H->VAMEI, H->VAMEF, H->VABEJ, H->VABEF})
+        bld.two_electron(h);
+    CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
+    ctx.dfree(bld.dB, nB * sizeof(double));
+}
+
+}  // namespace ccsd

@@ -1,0 +1,127 @@
+// Launch wrappers for the engine's CUDA kernels (implemented in *.cu).
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ccsd {
+namespace kern {
+
+// C[Cm_v[m] + Cn_w[n]] += sign_vw * alpha * sum_k A[Am[m]+Ak[k]] * B[Bk[k]+Bn[n]]
+struct GemmArgs {
+    const double* A = nullptr;
+    const double* B = nullptr;
+    double* C = nullptr;
+    int M = 0, N = 0, K = 0;
+    double alpha = 0;
+    const int64_t *Am = nullptr, *Ak = nullptr, *Bk = nullptr, *Bn = nullptr;
+    const int64_t* Cm[2] = {nullptr, nullptr};
+    const int64_t* Cn[2] = {nullptr, nullptr};
+    int nvm = 1, nvn = 1;
+    double vsign[4] = {1, 1, 1, 1};
+    bool a_kcontig = false;   // consecutive k -> consecutive A addresses
+    bool b_kcontig = false;   // consecutive k -> consecutive B addresses
+};
+
+// native FP64 tensor-core (DMMA) GETT kernel
+void gemm_fp64(const GemmArgs& g, cudaStream_t s);
+
+// ---- split-BF16 (Ozaki-style) path ------------------------------------------------
+// An operand sliced for the tcgen05 GEMM: rows x kpad bf16 values per slice, K-major,
+// row scale 2^e per row.  rows is padded to a multiple of 128, kpad to a multiple of 64.
+struct SlicedOperand {
+    uint16_t* data = nullptr;   // [nslices][rows][kpad]
+    double* scale = nullptr;    // [rows]  value = scale * (s0 + s1 + s2 ...)
+    int rows = 0, kpad = 0, nslices = 0;
+    int64_t bytes = 0;
+};
+
+struct SplitWorkspace {
+    SlicedOperand a, b;          // per-call slices of non-constant operands
+    double* rowmax = nullptr;
+    int64_t rowmax_n = 0;
+};
+
+// number of bf16 slices used when the caller does not say otherwise
+constexpr int kDefaultSlices = 3;
+
+// slice rows of X(r,k) = X[R[r] + Kt[k]] (r < nrows, k < K) into `out` (allocated by caller)
+void slice_rows(const double* X, const int64_t* R, const int64_t* Kt, int nrows, int K, bool kcontig,
+                int nslices, SlicedOperand& out, cudaStream_t s);
+// tcgen05 GEMM over slices; epilogue scatters into C like gemm_fp64
+void gemm_split(const SlicedOperand& a, const SlicedOperand& b, int M, int N, int K,
+                const GemmArgs& g, cudaStream_t s);
+bool split_supported();
+
+// ---- elementwise / reductions ----------------------------------------------------
+struct StridedArgs {
+    int ndim = 0;
+    int64_t len[8];
+    int64_t sA[8], sB[8];
+    int64_t total = 1;
+};
+// C[offC + sum idx*sB] += alpha * A[offA + sum idx*sA]
+void sum_strided(const double* A, double* C, const StridedArgs& a, double alpha, cudaStream_t s);
+// out[0] += alpha * sum A[..]*B[..]
+void dot_strided(const double* A, const double* B, const StridedArgs& a, double alpha, double* out,
+                 cudaStream_t s);
+void scale(double* X, int64_t n, double beta, cudaStream_t s);
+void fill(double* X, int64_t n, double val, cudaStream_t s);
+// max |x| (p=0), sum |x| (p=1) or sum x^2 (p=2) of n elements, accumulated into out[0]
+// with weight w (p=1,2) or max (p=0)
+void norm_accum(const double* X, int64_t n, int p, double w, double* out, cudaStream_t s);
+// out = alpha*x + beta*out
+void axpby(const double* x, double* out, int64_t n, double alpha, double beta, cudaStream_t s);
+
+// Jacobi weight of one block: x /= (sum_p d_p[idx_p] + shift), 0 if |.| < 1e-4
+struct WeightArgs {
+    int ndim = 0;
+    int64_t len[8];
+    const double* d[8];
+    int64_t total = 1;
+};
+void weight_block(double* X, const WeightArgs& w, double shift, cudaStream_t s);
+
+// key/value scatter: X[keys[i]] = beta*X[keys[i]] + alpha*vals[i]
+void kv_write(double* X, const int64_t* keys, const double* vals, int64_t n, double alpha, double beta,
+              cudaStream_t s);
+void kv_read(const double* X, const int64_t* keys, double* vals, int64_t n, cudaStream_t s);
+
+// ---- fused CCSD update / DIIS -------------------------------------------------------
+// z = w * z_raw / den (den from per-position denominators), t += z, track max|z|;
+// blocks described by WeightArgs; results accumulated into red[0] (max)
+void update_block(double* Z, double* T, const WeightArgs& w, double* red_max, cudaStream_t s);
+
+// batched dot: out[j] += w * sum x[i]*ys[j][i], j < ny  (ys: device array of pointers)
+void dot_batch(const double* x, const double* const* ys, int ny, int64_t n, double w, double* out,
+               cudaStream_t s);
+// out[i] = sum_j c[j] * xs[j][i]  (c on device); i < n1 goes to out1, the rest to out2
+void lincomb(double* out1, int64_t n1, double* out2, int64_t n2, const double* const* xs, const double* c, int nx,
+             cudaStream_t s);
+
+// ---- device-resident DIIS (src/convergence/diis.hpp:70-227) -----------------------------
+// state[0] = slot of the newest vector, state[1] = stored vectors, state[2] = start counter,
+// state[3] = singular flag.  The ring keeps `order` vectors; slot (head - k) mod order holds
+// the vector of k iterations ago.
+void diis_advance(int* state, int order, cudaStream_t s);
+// xs[head] = [t1 | t2], dxs[head] = [z1 | z2]
+void diis_store(const int* state, const double* const* xs, const double* const* dxs, const double* t1, int64_t n1,
+                const double* t2, int64_t n2, const double* z1, const double* z2, cudaStream_t s);
+// dots[j] += w * <dxs[head][off:off+len], dxs[j][off:off+len]>,  j < order
+void diis_dots(const int* state, const double* const* dxs, int order, int64_t off, int64_t len, double w,
+               double* dots, cudaStream_t s);
+// update the error matrix with the new row, solve the bordered system and write the
+// coefficients by slot into c (unit vector at head when no extrapolation happens)
+void diis_solve(int* state, double* e, double* c, const double* dots, int order, cudaStream_t s);
+
+// Pack <ab||cd> = J - K for canonical pairs of a packed block, a in [a0,a1):
+//   J = tJ[a-a0, c, b, d] = (ac|bd),  K = tK[a-a0, d, b, c] = (ad|bc)
+// kind 1: triangle (x<y, equal irreps), kind 2: full rectangle.  The (a,b) pair has
+// stride 1, the (c,d) pair stride `scd`.
+void pack_vvvv(double* V, int kind_ab, int kind_cd, int n0, int n1, int n2, int n3, int64_t scd, const double* tJ,
+               const double* tK, int a0, int a1, bool J, bool K, cudaStream_t s);
+
+int64_t launch_count();
+void reset_launch_count();
+
+}  // namespace kern
+}  // namespace ccsd

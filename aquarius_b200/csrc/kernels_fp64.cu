@@ -1,0 +1,721 @@
+// Native-FP64 kernels: the DMMA gather-GEMM ("plain path" contraction layer) and the
+// HBM-bound elementwise / reduction kernels of the iteration.
+//
+// The GEMM computes, for one planned block contraction,
+//   C[Cm_v[m] + Cn_w[n]] += s_vw * alpha * sum_k A[Am[m]+Ak[k]] * B[Bk[k]+Bn[n]]
+// i.e. a GEMM whose operands are gathered straight from the stored tensor blocks
+// through per-dimension offset tables (no separate transpose pass), and whose
+// epilogue scatters into the output block, once per antisymmetric image.
+#include <cstdint>
+#include <map>
+#include <mutex>
+#include <utility>
+#include <cuda_runtime.h>
+
+#include "kernels.hpp"
+
+namespace ccsd {
+namespace kern {
+
+int64_t g_launches = 0;
+int64_t launch_count() { return g_launches; }
+void reset_launch_count() { g_launches = 0; }
+#define COUNT_LAUNCH() (g_launches++)
+
+// ---------------------------------------------------------------------------
+// FP64 DMMA gather-GEMM
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int BM = 128, BN = 64, BK = 16, STAGES = 3, THREADS = 256;
+constexpr int LDMK = BM + 8;   // A stored [k][m]
+constexpr int LDNK = BN + 8;   // B stored [k][n]
+constexpr int LDK = BK + 4;    // operands stored [m][k] / [n][k]
+
+template <bool AK, bool BK_>
+struct Smem {
+    static constexpr int a_elems = AK ? BM * LDK : BK * LDMK;
+    static constexpr int b_elems = BK_ ? BN * LDK : BK * LDNK;
+    static constexpr size_t bytes = (size_t)STAGES * (a_elems + b_elems) * sizeof(double) + (BM + BN) * sizeof(int64_t);
+};
+
+__device__ __forceinline__ void cp_async8(void* smem, const void* gmem, bool valid) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    int sz = valid ? 8 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(s), "l"(gmem), "r"(sz));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+template <bool AK, bool BKc>
+__global__ void __launch_bounds__(THREADS, 1) gemm_fp64_kernel(GemmArgs g) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    using S = Smem<AK, BKc>;
+    double* As = reinterpret_cast<double*>(smem_raw);
+    double* Bs = As + STAGES * S::a_elems;
+    int64_t* sAm = reinterpret_cast<int64_t*>(Bs + STAGES * S::b_elems);
+    int64_t* sBn = sAm + BM;
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
+
+    for (int i = tid; i < BM; i += THREADS) sAm[i] = (m0 + i < g.M) ? g.Am[m0 + i] : 0;
+    for (int i = tid; i < BN; i += THREADS) sBn[i] = (n0 + i < g.N) ? g.Bn[n0 + i] : 0;
+    __syncthreads();
+
+    const int ktiles = (g.K + BK - 1) / BK;
+
+    auto load_stage = [&](int stage, int kt) {
+        const int k0 = kt * BK;
+        double* as = As + stage * S::a_elems;
+        double* bs = Bs + stage * S::b_elems;
+        // A tile: BM x BK
+#pragma unroll
+        for (int i = 0; i < (BM * BK) / THREADS; i++) {
+            int e = tid + i * THREADS;
+            int m, k;
+            if (AK) { k = e % BK; m = e / BK; }
+            else    { m = e % BM; k = e / BM; }
+            bool ok = (m0 + m < g.M) && (k0 + k < g.K);
+            const double* src = ok ? g.A + sAm[m] + __ldg(g.Ak + k0 + k) : g.A;
+            double* dst = AK ? as + m * LDK + k : as + k * LDMK + m;
+            cp_async8(dst, src, ok);
+        }
+        // B tile: BK x BN
+#pragma unroll
+        for (int i = 0; i < (BN * BK) / THREADS; i++) {
+            int e = tid + i * THREADS;
+            int n, k;
+            if (BKc) { k = e % BK; n = e / BK; }
+            else     { n = e % BN; k = e / BN; }
+            bool ok = (n0 + n < g.N) && (k0 + k < g.K);
+            const double* src = ok ? g.B + sBn[n] + __ldg(g.Bk + k0 + k) : g.B;
+            double* dst = BKc ? bs + n * LDK + k : bs + k * LDNK + n;
+            cp_async8(dst, src, ok);
+        }
+    };
+
+    double acc[4][4][2];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; s++) {
+        if (s < ktiles) load_stage(s, s);
+        cp_commit();
+    }
+
+    for (int kt = 0; kt < ktiles; kt++) {
+        cp_wait<STAGES - 2>();
+        __syncthreads();
+        {
+            int nk = kt + STAGES - 1;
+            if (nk < ktiles) load_stage(nk % STAGES, nk);
+            cp_commit();
+        }
+        const double* as = As + (kt % STAGES) * S::a_elems;
+        const double* bs = Bs + (kt % STAGES) * S::b_elems;
+#pragma unroll
+        for (int kk = 0; kk < BK; kk += 4) {
+            double af[4], bf[4];
+            const int kr = kk + (lane & 3);
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                int m = wm + i * 8 + (lane >> 2);
+                af[i] = AK ? as[m * LDK + kr] : as[kr * LDMK + m];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; j++) {
+                int n = wn + j * 8 + (lane >> 2);
+                bf[j] = BKc ? bs[n * LDK + kr] : bs[kr * LDNK + n];
+            }
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) dmma(acc[i][j][0], acc[i][j][1], af[i], bf[j]);
+        }
+    }
+    cp_wait<0>();
+
+    // epilogue: scatter to every destination variant
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        int m = m0 + wm + i * 8 + (lane >> 2);
+        if (m >= g.M) continue;
+        int64_t cm[2];
+        cm[0] = g.Cm[0][m];
+        cm[1] = g.nvm > 1 ? g.Cm[1][m] : 0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) {
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                int n = n0 + wn + j * 8 + 2 * (lane & 3) + h;
+                if (n >= g.N) continue;
+                double v = g.alpha * acc[i][j][h];
+                for (int a = 0; a < g.nvm; a++)
+                    for (int b = 0; b < g.nvn; b++) {
+                        double* dst = g.C + cm[a] + g.Cn[b][n];
+                        *dst += g.vsign[a * g.nvn + b] * v;
+                    }
+            }
+        }
+    }
+}
+
+template <bool AK, bool BKc>
+void launch_fp64(const GemmArgs& g, cudaStream_t s) {
+    using S = Smem<AK, BKc>;
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(gemm_fp64_kernel<AK, BKc>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
+        configured = true;
+    }
+    dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM);
+    gemm_fp64_kernel<AK, BKc><<<grid, THREADS, S::bytes, s>>>(g);
+    COUNT_LAUNCH();
+}
+
+}  // namespace
+
+void gemm_fp64(const GemmArgs& g, cudaStream_t s) {
+    if (g.M <= 0 || g.N <= 0 || g.K <= 0) return;
+    if (g.a_kcontig) {
+        if (g.b_kcontig) launch_fp64<true, true>(g, s);
+        else launch_fp64<true, false>(g, s);
+    } else {
+        if (g.b_kcontig) launch_fp64<false, true>(g, s);
+        else launch_fp64<false, false>(g, s);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// elementwise and reductions
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr int EW_THREADS = 256;
+
+inline int ew_blocks(int64_t n) {
+    int64_t b = (n + EW_THREADS - 1) / EW_THREADS;
+    if (b > 148 * 16) b = 148 * 16;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+__global__ void sum_strided_kernel(const double* __restrict__ A, double* __restrict__ C, StridedArgs a,
+                                   double alpha) {
+    for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < a.total;
+         l += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = l, oa = 0, oc = 0;
+        for (int d = 0; d < a.ndim; d++) {
+            int64_t x = r % a.len[d];
+            r /= a.len[d];
+            oa += x * a.sA[d];
+            oc += x * a.sB[d];
+        }
+        C[oc] += alpha * A[oa];
+    }
+}
+
+__device__ __forceinline__ double block_sum(double v) {
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    v = 0;
+    if (threadIdx.x < (blockDim.x >> 5)) v = red[threadIdx.x];
+    if (w == 0)
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double block_max(double v) {
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) red[w] = v;
+    __syncthreads();
+    v = 0;
+    if (threadIdx.x < (blockDim.x >> 5)) v = red[threadIdx.x];
+    if (w == 0)
+        for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// deterministic two-pass reductions: blocks write partials, one block folds them
+__global__ void dot_strided_kernel(const double* __restrict__ A, const double* __restrict__ B, StridedArgs a,
+                                   double* partial) {
+    double s = 0;
+    for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < a.total;
+         l += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = l, oa = 0, ob = 0;
+        for (int d = 0; d < a.ndim; d++) {
+            int64_t x = r % a.len[d];
+            r /= a.len[d];
+            oa += x * a.sA[d];
+            ob += x * a.sB[d];
+        }
+        s += A[oa] * B[ob];
+    }
+    s = block_sum(s);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+__global__ void fold_sum_kernel(const double* partial, int n, double alpha, double* out) {
+    double s = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s += partial[i];
+    s = block_sum(s);
+    if (threadIdx.x == 0) out[0] += alpha * s;
+}
+
+__global__ void norm_kernel(const double* __restrict__ X, int64_t n, int p, double* partial) {
+    double s = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double x = X[i];
+        if (p == 0) s = fmax(s, fabs(x));
+        else if (p == 1) s += fabs(x);
+        else s += x * x;
+    }
+    s = p == 0 ? block_max(s) : block_sum(s);
+    if (threadIdx.x == 0) partial[blockIdx.x] = s;
+}
+
+__global__ void fold_norm_kernel(const double* partial, int n, int p, double w, double* out) {
+    double s = 0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) s = p == 0 ? fmax(s, partial[i]) : s + partial[i];
+    s = p == 0 ? block_max(s) : block_sum(s);
+    if (threadIdx.x == 0) out[0] = p == 0 ? fmax(out[0], s) : out[0] + w * s;
+}
+
+__global__ void scale_kernel(double* X, int64_t n, double beta) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        X[i] = beta == 0.0 ? 0.0 : beta * X[i];
+}
+
+__global__ void fill_kernel(double* X, int64_t n, double v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        X[i] = v;
+}
+
+__global__ void axpby_kernel(const double* __restrict__ x, double* __restrict__ y, int64_t n, double a, double b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        y[i] = a * x[i] + (b == 0.0 ? 0.0 : b * y[i]);
+}
+
+__device__ __forceinline__ double den_of(const WeightArgs& w, int64_t l) {
+    double den = 0;
+    int64_t r = l;
+    for (int d = 0; d < w.ndim; d++) {
+        int64_t x = r % w.len[d];
+        r /= w.len[d];
+        den += w.d[d][x];
+    }
+    return den;
+}
+
+__global__ void weight_kernel(double* X, WeightArgs w, double shift) {
+    for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < w.total;
+         l += (int64_t)gridDim.x * blockDim.x) {
+        double den = den_of(w, l) + shift;
+        X[l] = fabs(den) < 1e-4 ? 0.0 : X[l] / den;
+    }
+}
+
+// z = z/den (0 if |den| < 1e-4), t += z, block max |z|
+__global__ void update_kernel(double* __restrict__ Z, double* __restrict__ T, WeightArgs w, double* partial) {
+    double mx = 0;
+    for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < w.total;
+         l += (int64_t)gridDim.x * blockDim.x) {
+        double den = den_of(w, l);
+        double z = fabs(den) < 1e-4 ? 0.0 : Z[l] / den;
+        Z[l] = z;
+        T[l] += z;
+        mx = fmax(mx, fabs(z));
+    }
+    mx = block_max(mx);
+    if (threadIdx.x == 0) partial[blockIdx.x] = mx;
+}
+
+__global__ void kv_write_kernel(double* X, const int64_t* keys, const double* vals, int64_t n, double a, double b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double* p = X + keys[i];
+        *p = (b == 0.0 ? 0.0 : b * *p) + a * vals[i];
+    }
+}
+
+__global__ void kv_read_kernel(const double* X, const int64_t* keys, double* vals, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        vals[i] = X[keys[i]];
+}
+
+// batched dot: partial[b * ny + j] = sum over the block's range of x * ys[j]
+__global__ void dot_batch_kernel(const double* __restrict__ x, const double* const* ys, int ny, int64_t n,
+                                 double* partial) {
+    double s[16];
+    for (int j = 0; j < 16; j++) s[j] = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double xv = x[i];
+        for (int j = 0; j < ny; j++) s[j] += xv * ys[j][i];
+    }
+    for (int j = 0; j < ny; j++) {
+        double t = block_sum(s[j]);
+        if (threadIdx.x == 0) partial[blockIdx.x * ny + j] = t;
+    }
+}
+
+__global__ void fold_batch_kernel(const double* partial, int nb, int ny, double w, double* out) {
+    for (int j = 0; j < ny; j++) {
+        double s = 0;
+        for (int b = threadIdx.x; b < nb; b += blockDim.x) s += partial[b * ny + j];
+        s = block_sum(s);
+        if (threadIdx.x == 0) out[j] += w * s;
+    }
+}
+
+__global__ void lincomb_kernel(double* __restrict__ out1, int64_t n1, double* __restrict__ out2, int64_t n2,
+                               const double* const* xs, const double* c, int nx) {
+    const int64_t n = n1 + n2;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int j = 0; j < nx; j++) {
+            double cj = c[j];
+            if (cj != 0.0) s += cj * xs[j][i];
+        }
+        if (i < n1) out1[i] = s;
+        else out2[i - n1] = s;
+    }
+}
+
+// Scratch for the two-pass reductions, one buffer per stream: work on one stream is
+// ordered, and each fold consumes its partials before the next reduction on that
+// stream overwrites them.  Buffers live until process exit.
+}  // namespace
+
+double* partial_buffer(cudaStream_t s) {
+    static std::mutex mu;
+    static std::map<std::pair<int, cudaStream_t>, double*> bufs;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_pair(dev, s);
+    auto it = bufs.find(key);
+    if (it != bufs.end()) return it->second;
+    double* p = nullptr;
+    cudaMalloc(&p, sizeof(double) * 148 * 16 * 16);
+    bufs[key] = p;
+    return p;
+}
+
+void sum_strided(const double* A, double* C, const StridedArgs& a, double alpha, cudaStream_t s) {
+    if (a.total <= 0) return;
+    sum_strided_kernel<<<ew_blocks(a.total), EW_THREADS, 0, s>>>(A, C, a, alpha);
+    COUNT_LAUNCH();
+}
+
+void dot_strided(const double* A, const double* B, const StridedArgs& a, double alpha, double* out,
+                 cudaStream_t s) {
+    if (a.total <= 0) return;
+    int nb = ew_blocks(a.total);
+    double* part = partial_buffer(s);
+    dot_strided_kernel<<<nb, EW_THREADS, 0, s>>>(A, B, a, part);
+    fold_sum_kernel<<<1, 1024, 0, s>>>(part, nb, alpha, out);
+    COUNT_LAUNCH();
+    COUNT_LAUNCH();
+}
+
+void scale(double* X, int64_t n, double beta, cudaStream_t s) {
+    if (n <= 0 || beta == 1.0) return;
+    scale_kernel<<<ew_blocks(n), EW_THREADS, 0, s>>>(X, n, beta);
+    COUNT_LAUNCH();
+}
+
+void fill(double* X, int64_t n, double val, cudaStream_t s) {
+    if (n <= 0) return;
+    fill_kernel<<<ew_blocks(n), EW_THREADS, 0, s>>>(X, n, val);
+    COUNT_LAUNCH();
+}
+
+void norm_accum(const double* X, int64_t n, int p, double w, double* out, cudaStream_t s) {
+    if (n <= 0) return;
+    int nb = ew_blocks(n);
+    double* part = partial_buffer(s);
+    norm_kernel<<<nb, EW_THREADS, 0, s>>>(X, n, p, part);
+    fold_norm_kernel<<<1, 1024, 0, s>>>(part, nb, p, w, out);
+    COUNT_LAUNCH();
+    COUNT_LAUNCH();
+}
+
+void axpby(const double* x, double* out, int64_t n, double alpha, double beta, cudaStream_t s) {
+    if (n <= 0) return;
+    axpby_kernel<<<ew_blocks(n), EW_THREADS, 0, s>>>(x, out, n, alpha, beta);
+    COUNT_LAUNCH();
+}
+
+void weight_block(double* X, const WeightArgs& w, double shift, cudaStream_t s) {
+    if (w.total <= 0) return;
+    weight_kernel<<<ew_blocks(w.total), EW_THREADS, 0, s>>>(X, w, shift);
+    COUNT_LAUNCH();
+}
+
+void update_block(double* Z, double* T, const WeightArgs& w, double* red_max, cudaStream_t s) {
+    if (w.total <= 0) return;
+    int nb = ew_blocks(w.total);
+    double* part = partial_buffer(s);
+    update_kernel<<<nb, EW_THREADS, 0, s>>>(Z, T, w, part);
+    fold_norm_kernel<<<1, 1024, 0, s>>>(part, nb, 0, 1.0, red_max);
+    COUNT_LAUNCH();
+    COUNT_LAUNCH();
+}
+
+void kv_write(double* X, const int64_t* keys, const double* vals, int64_t n, double alpha, double beta,
+              cudaStream_t s) {
+    if (n <= 0) return;
+    kv_write_kernel<<<ew_blocks(n), EW_THREADS, 0, s>>>(X, keys, vals, n, alpha, beta);
+    COUNT_LAUNCH();
+}
+
+void kv_read(const double* X, const int64_t* keys, double* vals, int64_t n, cudaStream_t s) {
+    if (n <= 0) return;
+    kv_read_kernel<<<ew_blocks(n), EW_THREADS, 0, s>>>(X, keys, vals, n);
+    COUNT_LAUNCH();
+}
+
+void dot_batch(const double* x, const double* const* ys, int ny, int64_t n, double w, double* out,
+               cudaStream_t s) {
+    if (n <= 0 || ny <= 0) return;
+    int nb = ew_blocks(n);
+    double* part = partial_buffer(s);
+    dot_batch_kernel<<<nb, EW_THREADS, 0, s>>>(x, ys, ny, n, part);
+    fold_batch_kernel<<<1, 1024, 0, s>>>(part, nb, ny, w, out);
+    COUNT_LAUNCH();
+    COUNT_LAUNCH();
+}
+
+void lincomb(double* out1, int64_t n1, double* out2, int64_t n2, const double* const* xs, const double* c, int nx,
+             cudaStream_t s) {
+    if (n1 + n2 <= 0) return;
+    lincomb_kernel<<<ew_blocks(n1 + n2), EW_THREADS, 0, s>>>(out1, n1, out2, n2, xs, c, nx);
+    COUNT_LAUNCH();
+}
+
+
+// ---------------------------------------------------------------------------
+// device-resident DIIS
+// ---------------------------------------------------------------------------
+namespace {
+
+__global__ void diis_advance_kernel(int* st, int order) {
+    st[0] = (st[0] + 1) % order;
+    st[1] = min(st[1] + 1, order);
+}
+
+__global__ void diis_store_kernel(const int* st, const double* const* xs, const double* const* dxs,
+                                  const double* __restrict__ t1, int64_t n1, const double* __restrict__ t2, int64_t n2,
+                                  const double* __restrict__ z1, const double* __restrict__ z2) {
+    const int h = st[0];
+    double* x = const_cast<double*>(xs[h]);
+    double* dx = const_cast<double*>(dxs[h]);
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n1 + n2; i += (int64_t)gridDim.x * blockDim.x) {
+        if (i < n1) {
+            x[i] = t1[i];
+            dx[i] = z1[i];
+        } else {
+            x[i] = t2[i - n1];
+            dx[i] = z2[i - n1];
+        }
+    }
+}
+
+__global__ void diis_dots_kernel(const int* st, const double* const* dxs, int order, int64_t off, int64_t len,
+                                 double* partial) {
+    const double* x = dxs[st[0]] + off;
+    double s[16];
+    for (int j = 0; j < 16; j++) s[j] = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x) {
+        double xv = x[i];
+#pragma unroll
+        for (int j = 0; j < 16; j++)
+            if (j < order) s[j] += xv * dxs[j][off + i];
+    }
+    for (int j = 0; j < order; j++) {
+        double t = block_sum(s[j]);
+        if (threadIdx.x == 0) partial[blockIdx.x * order + j] = t;
+    }
+}
+
+// Gaussian elimination with partial pivoting on an m x m system (m <= 17); false if a
+// pivot is exactly zero
+__device__ bool small_solve(double (*A)[17], double* b, int m) {
+    for (int k = 0; k < m; k++) {
+        int p = k;
+        for (int i = k + 1; i < m; i++)
+            if (fabs(A[i][k]) > fabs(A[p][k])) p = i;
+        if (A[p][k] == 0.0) return false;
+        if (p != k) {
+            for (int j = 0; j < m; j++) {
+                double t = A[k][j];
+                A[k][j] = A[p][j];
+                A[p][j] = t;
+            }
+            double t = b[k];
+            b[k] = b[p];
+            b[p] = t;
+        }
+        for (int i = k + 1; i < m; i++) {
+            double f = A[i][k] / A[k][k];
+            for (int j = k; j < m; j++) A[i][j] -= f * A[k][j];
+            b[i] -= f * b[k];
+        }
+    }
+    for (int k = m - 1; k >= 0; k--) {
+        double t = b[k];
+        for (int j = k + 1; j < m; j++) t -= A[k][j] * b[j];
+        b[k] = t / A[k][k];
+    }
+    return true;
+}
+
+__global__ void diis_solve_kernel(int* st, double* e, double* c, const double* dots, int order) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int ld = order + 1;
+    const int head = st[0], cnt = st[1];
+    for (int j = 0; j < order; j++) {
+        e[head * ld + j] = dots[j];
+        e[j * ld + head] = dots[j];
+    }
+    for (int j = 0; j <= order; j++) c[j] = 0.0;
+    // diis.hpp:151: a single vector gives no extrapolation
+    if (cnt == 1) {
+        c[head] = 1.0;
+        return;
+    }
+    // diis.hpp:153: --start > 1 delays the extrapolation
+    int start = --st[2];
+    if (start > 1) {
+        c[head] = 1.0;
+        return;
+    }
+    double A[17][17], b[17];
+    auto slot = [&](int age) { return ((head - age) % order + order) % order; };
+    auto fill = [&](double shift) {
+        for (int i = 0; i < cnt; i++) {
+            for (int j = 0; j < cnt; j++) A[i][j] = e[slot(i) * ld + slot(j)];
+            A[i][i] += shift;
+            A[i][cnt] = -1.0;
+            A[cnt][i] = -1.0;
+            b[i] = 0.0;
+        }
+        A[cnt][cnt] = 0.0;
+        b[cnt] = -1.0;
+    };
+    fill(0.0);
+    bool ok = small_solve(A, b, cnt + 1);
+    if (!ok) {
+        // diis.hpp:177-185: shift the diagonal by eps * e[n-1][n-1] and retry
+        double eps = e[slot(cnt - 1) * ld + slot(cnt - 1)] * 2.220446049250313e-16;
+        fill(eps);
+        ok = small_solve(A, b, cnt + 1);
+    }
+    if (!ok) {
+        st[3] = 1;
+        c[head] = 1.0;
+        return;
+    }
+    for (int i = 0; i < cnt; i++) c[slot(i)] = b[i];
+}
+
+}  // namespace
+
+namespace {
+
+__device__ __forceinline__ void tri_decode(int64_t p, int64_t& x, int64_t& y) {
+    // p = y(y-1)/2 + x with 0 <= x < y
+    int64_t yy = (int64_t)((1.0 + sqrt(1.0 + 8.0 * (double)p)) * 0.5);
+    while (yy * (yy - 1) / 2 > p) yy--;
+    while ((yy + 1) * yy / 2 <= p) yy++;
+    y = yy;
+    x = p - yy * (yy - 1) / 2;
+}
+
+__global__ void pack_vvvv_kernel(double* V, int kab, int kcd, int n0, int n1, int n2, int n3, int64_t scd,
+                                 const double* __restrict__ tJ, const double* __restrict__ tK, int a0, int a1,
+                                 bool J, bool K) {
+    const int ca = a1 - a0;
+    const int64_t ncd = kcd == 1 ? (int64_t)n2 * (n2 - 1) / 2 : (int64_t)n2 * n3;
+    const int64_t total = (int64_t)ca * n1 * ncd;
+    for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < total; l += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = l;
+        int a = (int)(r % ca) + a0;
+        r /= ca;
+        int b = (int)(r % n1);
+        int64_t pcd = r / n1;
+        if (kab == 1 && b <= a) continue;
+        int64_t c, d;
+        if (kcd == 1) tri_decode(pcd, c, d);
+        else {
+            c = pcd % n2;
+            d = pcd / n2;
+        }
+        int64_t pab = kab == 1 ? (int64_t)b * (b - 1) / 2 + a : (int64_t)a + (int64_t)n0 * b;
+        const int64_t ap = a - a0;
+        double v = 0;
+        if (J) v += tJ[ap + ca * (c + (int64_t)n2 * (b + (int64_t)n1 * d))];
+        if (K) v -= tK[ap + ca * (d + (int64_t)n3 * (b + (int64_t)n1 * c))];
+        V[pab + scd * pcd] = v;
+    }
+}
+
+}  // namespace
+
+void pack_vvvv(double* V, int kind_ab, int kind_cd, int n0, int n1, int n2, int n3, int64_t scd, const double* tJ,
+               const double* tK, int a0, int a1, bool J, bool K, cudaStream_t s) {
+    int64_t ncd = kind_cd == 1 ? (int64_t)n2 * (n2 - 1) / 2 : (int64_t)n2 * n3;
+    int64_t total = (int64_t)(a1 - a0) * n1 * ncd;
+    if (total <= 0) return;
+    pack_vvvv_kernel<<<ew_blocks(total), EW_THREADS, 0, s>>>(V, kind_ab, kind_cd, n0, n1, n2, n3, scd, tJ, tK, a0,
+                                                              a1, J, K);
+    COUNT_LAUNCH();
+}
+
+void diis_advance(int* state, int order, cudaStream_t s) {
+    diis_advance_kernel<<<1, 1, 0, s>>>(state, order);
+    COUNT_LAUNCH();
+}
+
+void diis_store(const int* state, const double* const* xs, const double* const* dxs, const double* t1, int64_t n1,
+                const double* t2, int64_t n2, const double* z1, const double* z2, cudaStream_t s) {
+    diis_store_kernel<<<ew_blocks(n1 + n2), EW_THREADS, 0, s>>>(state, xs, dxs, t1, n1, t2, n2, z1, z2);
+    COUNT_LAUNCH();
+}
+
+void diis_dots(const int* state, const double* const* dxs, int order, int64_t off, int64_t len, double w,
+               double* dots, cudaStream_t s) {
+    if (len <= 0) return;
+    int nb = ew_blocks(len);
+    double* part = partial_buffer(s);
+    diis_dots_kernel<<<nb, EW_THREADS, 0, s>>>(state, dxs, order, off, len, part);
+    fold_batch_kernel<<<1, 1024, 0, s>>>(part, nb, order, w, dots);
+    COUNT_LAUNCH();
+    COUNT_LAUNCH();
+}
+
+void diis_solve(int* state, double* e, double* c, const double* dots, int order, cudaStream_t s) {
+    diis_solve_kernel<<<1, 32, 0, s>>>(state, e, c, dots, order);
+    COUNT_LAUNCH();
+}
+
+}  // namespace kern
+}  // namespace ccsd

@@ -1,0 +1,414 @@
+// CCSD solver: CCSD<U>::run / iterate (src/cc/ccsd.cxx:29-193), the iterative driver
+// (src/util/iterative.hpp:126-188) and DIIS (src/convergence/diis.hpp:70-227), kept on
+// the device so that one iteration is a fixed sequence of kernel launches (and can be
+// captured as a CUDA graph).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+#include "expr.hpp"
+#include "solver.hpp"
+
+namespace ccsd {
+
+namespace {
+
+int mk(Context& c, const char* name, int o0, int o1, int i0, int i1, int flags = 0) {
+    int nout[2] = {o0, o1}, nin[2] = {i0, i1};
+    return c.create_tensor(name, nout, nin, flags);
+}
+
+}  // namespace
+
+void options_default(ccsd_options* o) {
+    o->conv_tol = 1e-9;
+    o->max_iter = 50;
+    o->diis_order = 5;
+    o->diis_start = 1;
+    o->diis_damping = 0.0;
+    o->precision = CCSD_PREC_FP64;
+    o->slices = 0;
+    o->use_graph = 0;
+}
+
+Solver::Solver(Context& c, const ccsd_hamiltonian& h, const ccsd_options& o) : ctx(c), H(h), opts(o) {
+    if (opts.diis_damping != 0.0) throw Error(CCSD_ERR_UNSUPPORTED, "DIIS damping is not supported");
+    if (opts.diis_order < 1 || opts.diis_order > 16) throw Error(CCSD_ERR_ARG, "diis_order must be in 1..16");
+    ctx.precision = opts.precision;
+    ctx.slices = opts.slices;
+    // constants: the H blocks never change, so their split slices can be cached
+    for (int t : {H.fAI, H.fME, H.fAE, H.fMI, H.VMNIJ, H.VAMIJ, H.VMNEJ, H.VABIJ, H.VMNEF, H.VAMEI, H.VAMEF,
+                  H.VABEJ, H.VABEF})
+        ctx.constant_tensors.push_back(t);
+
+    // ccsd.cxx:37-48
+    T1 = mk(ctx, "T(1)", 1, 0, 0, 1);
+    T2 = mk(ctx, "T(2)", 2, 0, 0, 2);
+    Z1 = mk(ctx, "Z(1)", 1, 0, 0, 1);
+    Z2 = mk(ctx, "Z(2)", 2, 0, 0, 2);
+    Tau = mk(ctx, "Tau", 2, 0, 0, 2);
+    FME = mk(ctx, "F(me)", 0, 1, 1, 0);
+    FMI = mk(ctx, "F(mi)", 0, 1, 0, 1);
+    FAE = mk(ctx, "F(ae)", 1, 0, 1, 0);
+    WMNIJ = mk(ctx, "W(mn,ij)", 0, 2, 0, 2);
+    WMNEJ = mk(ctx, "W(mn,ej)", 0, 2, 1, 1);
+    WAMIJ = mk(ctx, "W~(am,ij)", 1, 1, 0, 2);
+    WAMEI = mk(ctx, "W~(am,ei)", 1, 1, 1, 1);
+
+    build_denominators();
+    build_diis();
+    d_red = (double*)ctx.dmalloc(8 * sizeof(double));
+    CCSD_CUDA(cudaMemsetAsync(d_red, 0, 8 * sizeof(double), ctx.stream));
+    h_red = nullptr;
+    CCSD_CUDA(cudaMallocHost(&h_red, 8 * sizeof(double)));
+    CCSD_CUDA(cudaMallocHost(&h_state, 8 * sizeof(int)));
+
+    // ---- initial guess and MP2 (ccsd.cxx:50-62) -------------------------------
+    {
+        Plan init;
+        Recorder r{&ctx, &init};
+        TensorRef t1{&r, T1}, t2{&r, T2}, fai{&r, H.fAI}, vabij{&r, H.VABIJ};
+        t1["ai"] = fai["ai"];
+        t2["abij"] = vabij["abij"];
+        ctx.run(init);
+        weight_tensor(T1);
+        weight_tensor(T2);
+    }
+    record_tau(tau_plan);
+    record_energy(energy_plan);
+    ctx.run(tau_plan);
+    CCSD_CUDA(cudaMemsetAsync(d_red, 0, sizeof(double), ctx.stream));
+    ctx.run(energy_plan, nullptr, d_red + 0);
+    CCSD_CUDA(cudaMemcpyAsync(h_red, d_red, sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+    CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
+    mp2 = h_red[0];
+    energy = mp2;
+    conv = std::numeric_limits<double>::max();
+
+    record_iteration();
+    ctx.upload(iter_plan);
+    ctx.upload(tau_plan);
+    ctx.upload(energy_plan);
+    flops_per_iter = iter_plan.flops() + tau_plan.flops();
+}
+
+Solver::~Solver() {
+    if (graph_exec) cudaGraphExecDestroy(graph_exec);
+    if (graph) cudaGraphDestroy(graph);
+    ctx.release(iter_plan);
+    ctx.release(tau_plan);
+    ctx.release(energy_plan);
+    for (int t : {T1, T2, Z1, Z2, Tau, FME, FMI, FAE, WMNIJ, WMNEJ, WAMIJ, WAMEI})
+        if (ctx.tensors.count(t)) ctx.destroy_tensor(t);
+    for (auto p : owned) ctx.dfree(p.first, p.second);
+    if (h_red) cudaFreeHost(h_red);
+    if (h_state) cudaFreeHost(h_state);
+    for (int t : {H.fAI, H.fME, H.fAE, H.fMI, H.VMNIJ, H.VAMIJ, H.VMNEJ, H.VABIJ, H.VMNEF, H.VAMEI, H.VAMEF,
+                  H.VABEJ, H.VABEF})
+        ctx.constant_tensors.erase(std::remove(ctx.constant_tensors.begin(), ctx.constant_tensors.end(), t),
+                                   ctx.constant_tensors.end());
+}
+
+void* Solver::alloc(size_t bytes) {
+    void* p = ctx.dmalloc(bytes);
+    owned.push_back({p, bytes});
+    return p;
+}
+
+// Denominator (denominator.hpp:50-73): d_a = -f_aa for virtuals, d_i = +f_ii for occupied,
+// per spin, concatenated over irreps.  Read from the diagonal of the fAE / fMI blocks.
+void Solver::build_denominators() {
+    const Spaces& S = ctx.spaces;
+    for (int sp = 0; sp < 2; sp++)
+        for (int s = 0; s < 2; s++) {
+            int n = S.total(sp, s);
+            den[sp][s] = (double*)alloc(std::max(n, 1) * sizeof(double));
+            std::vector<double> host(std::max(n, 1), 0.0);
+            int tf = sp == VRT ? H.fAE : H.fMI;
+            Tensor& F = ctx.tensor(tf);
+            int alpha[4] = {0, 0, 0, 0};
+            if (s == ALPHA) {
+                if (sp == VRT) alpha[0] = alpha[2] = 1;
+                else alpha[1] = alpha[3] = 1;
+            }
+            int cs = F.find_case(alpha);
+            int off = 0;
+            for (int h = 0; h < S.nirrep; h++) {
+                int nh = S.n[sp][s][h];
+                auto it = F.cases[cs].block_of.find(std::vector<int>{h, h});
+                if (nh > 0 && it != F.cases[cs].block_of.end()) {
+                    const Block& b = F.cases[cs].blocks[it->second];
+                    std::vector<double> blk(b.size);
+                    CCSD_CUDA(cudaMemcpy(blk.data(), F.data + b.offset, b.size * sizeof(double), cudaMemcpyDeviceToHost));
+                    for (int x = 0; x < nh; x++) host[off + x] = (sp == VRT ? -1.0 : 1.0) * blk[x + (int64_t)x * nh];
+                }
+                off += nh;
+            }
+            CCSD_CUDA(cudaMemcpy(den[sp][s], host.data(), std::max(n, 1) * sizeof(double), cudaMemcpyHostToDevice));
+        }
+}
+
+kern::WeightArgs Solver::weight_args(const Tensor& T, int cs, const Block& b) const {
+    kern::WeightArgs w;
+    w.ndim = T.ndim;
+    w.total = b.size;
+    for (int p = 0; p < T.ndim; p++) {
+        int sp = group_space(T.group[p]);
+        int s = T.cases[cs].spin[p];
+        w.len[p] = b.len[p];
+        w.d[p] = den[sp][s] + ctx.spaces.off[sp][s][b.irrep[p]];
+    }
+    return w;
+}
+
+void Solver::weight_tensor(int h) {
+    Tensor& T = ctx.tensor(h);
+    for (size_t c = 0; c < T.cases.size(); c++)
+        for (auto& b : T.cases[c].blocks) {
+            if (b.size == 0) continue;
+            kern::weight_block(T.data + b.offset, weight_args(T, (int)c, b), 0.0, ctx.stream);
+        }
+}
+
+// ---- recorded statements ---------------------------------------------------------
+
+void Solver::record_tau(Plan& p) {
+    Recorder r{&ctx, &p};
+    TensorRef tau{&r, Tau}, t1{&r, T1}, t2{&r, T2};
+    // ccsd.cxx:123-124
+    tau["abij"] = t2["abij"];
+    tau["abij"] += 0.5 * t1["ai"] * t1["bj"];
+}
+
+void Solver::record_energy(Plan& p) {
+    // energy = <fAI|T1> + 1/4 <VABIJ|Tau> over full spin-orbital ranges (ccsd.cxx:189)
+    Plan a = plan_dot(ctx, H.fAI, "ai", T1, "ai");
+    Plan b = plan_dot(ctx, H.VABIJ, "abij", Tau, "abij");
+    for (auto& d : b.dots) d.alpha *= 0.25;
+    p.append(std::move(a));
+    p.append(std::move(b));
+}
+
+void Solver::record_iteration() {
+    Plan& p = iter_plan;
+    Recorder r{&ctx, &p};
+    TensorRef fAI{&r, H.fAI}, fME{&r, H.fME}, fAE{&r, H.fAE}, fMI{&r, H.fMI};
+    TensorRef VABIJ{&r, H.VABIJ}, VMNEF{&r, H.VMNEF}, VAMEF{&r, H.VAMEF}, VABEJ{&r, H.VABEJ}, VABEF{&r, H.VABEF};
+    TensorRef VMNIJ{&r, H.VMNIJ}, VMNEJ{&r, H.VMNEJ}, VAMIJ{&r, H.VAMIJ}, VAMEI{&r, H.VAMEI};
+    TensorRef T1r{&r, T1}, T2r{&r, T2}, Z1r{&r, Z1}, Z2r{&r, Z2}, Taur{&r, Tau};
+    TensorRef FMEr{&r, FME}, FAEr{&r, FAE}, FMIr{&r, FMI};
+    TensorRef WMNIJr{&r, WMNIJ}, WMNEJr{&r, WMNEJ}, WAMIJr{&r, WAMIJ}, WAMEIr{&r, WAMEI};
+
+    // ccsd.cxx:123-124
+    Taur["abij"] = T2r["abij"];
+    Taur["abij"] += 0.5 * T1r["ai"] * T1r["bj"];
+
+    // intermediates, ccsd.cxx:130-157
+    FMEr["me"] = fME["me"];
+    FMEr["me"] += VMNEF["mnef"] * T1r["fn"];
+
+    FMIr["mi"] = fMI["mi"];
+    FMIr["mi"] += 0.5 * VMNEF["mnef"] * T2r["efin"];
+    FMIr["mi"] += FMEr["me"] * T1r["ei"];
+    FMIr["mi"] += VMNEJ["nmfi"] * T1r["fn"];
+
+    FAEr["ae"] = fAE["ae"];
+    FAEr["ae"] -= 0.5 * VMNEF["mnef"] * T2r["afmn"];
+    FAEr["ae"] -= FMEr["me"] * T1r["am"];
+    FAEr["ae"] += VAMEF["amef"] * T1r["fm"];
+
+    WMNIJr["mnij"] = VMNIJ["mnij"];
+    WMNIJr["mnij"] += 0.5 * VMNEF["mnef"] * Taur["efij"];
+    WMNIJr["mnij"] += VMNEJ["mnej"] * T1r["ei"];
+
+    WMNEJr["mnej"] = VMNEJ["mnej"];
+    WMNEJr["mnej"] += VMNEF["mnef"] * T1r["fj"];
+
+    WAMIJr["amij"] = VAMIJ["amij"];
+    WAMIJr["amij"] += 0.5 * VAMEF["amef"] * Taur["efij"];
+    WAMIJr["amij"] += VAMEI["amej"] * T1r["ei"];
+
+    WAMEIr["amei"] = VAMEI["amei"];
+    WAMEIr["amei"] += 0.5 * VMNEF["mnef"] * T2r["afni"];
+    WAMEIr["amei"] += VAMEF["amef"] * T1r["fi"];
+    WAMEIr["amei"] -= WMNEJr["nmei"] * T1r["an"];
+
+    // residual, ccsd.cxx:165-180
+    Z1r["ai"] = fAI["ai"];
+    Z1r["ai"] += fAE["ae"] * T1r["ei"];
+    Z1r["ai"] -= FMIr["mi"] * T1r["am"];
+    Z1r["ai"] -= VAMEI["amei"] * T1r["em"];
+    Z1r["ai"] += FMEr["me"] * T2r["aeim"];
+    Z1r["ai"] += 0.5 * VAMEF["amef"] * Taur["efim"];
+    Z1r["ai"] -= 0.5 * WMNEJr["mnei"] * T2r["eamn"];
+
+    Z2r["abij"] = VABIJ["abij"];
+    Z2r["abij"] += VABEJ["abej"] * T1r["ei"];
+    Z2r["abij"] -= WAMIJr["amij"] * T1r["bm"];
+    Z2r["abij"] += FAEr["ae"] * T2r["ebij"];
+    Z2r["abij"] -= FMIr["mi"] * T2r["abmj"];
+    Z2r["abij"] += 0.5 * VABEF["abef"] * Taur["efij"];
+    Z2r["abij"] += 0.5 * WMNIJr["mnij"] * Taur["abmn"];
+    Z2r["abij"] += WAMEIr["amei"] * T2r["ebjm"];
+}
+
+// ---- DIIS state ----------------------------------------------------------------------
+
+void Solver::build_diis() {
+    const int n = opts.diis_order;
+    Tensor& t1 = ctx.tensor(T1);
+    Tensor& t2 = ctx.tensor(T2);
+    vec_len = t1.total + t2.total;
+    // segments with the ExcitationOperator::dot weights (1 for T1, 1/4 for T2) times the
+    // number of spin-orbital arrangements a stored spin case stands for
+    // (binomial factors, spinorbital_tensor.cxx:1084-1088)
+    auto add_segments = [&](Tensor& T, int64_t base, double w) {
+        for (auto& sc : T.cases) {
+            if (sc.blocks.empty()) continue;
+            int64_t lo = sc.blocks.front().offset, hi = sc.blocks.back().offset + sc.blocks.back().size;
+            double mult = 1;
+            const int gs[4] = {T.nout[0], T.nout[1], T.nin[0], T.nin[1]};
+            for (int g = 0; g < 4; g++) {
+                double b = 1;
+                for (int k = 0; k < sc.alpha[g]; k++) b = b * (gs[g] - k) / (k + 1);
+                mult *= b;
+            }
+            segs.push_back({base + lo, hi - lo, w * mult});
+        }
+    };
+    add_segments(t1, 0, 1.0);
+    add_segments(t2, t1.total, 0.25);
+    if (n <= 1) return;
+    xs.resize(n);
+    dxs.resize(n);
+    for (int i = 0; i < n; i++) {
+        xs[i] = (double*)alloc(vec_len * sizeof(double));
+        dxs[i] = (double*)alloc(vec_len * sizeof(double));
+        CCSD_CUDA(cudaMemsetAsync(xs[i], 0, vec_len * sizeof(double), ctx.stream));
+        CCSD_CUDA(cudaMemsetAsync(dxs[i], 0, vec_len * sizeof(double), ctx.stream));
+    }
+    d_xs = (const double**)alloc(n * sizeof(double*));
+    d_dxs = (const double**)alloc(n * sizeof(double*));
+    CCSD_CUDA(cudaMemcpy(d_xs, xs.data(), n * sizeof(double*), cudaMemcpyHostToDevice));
+    CCSD_CUDA(cudaMemcpy(d_dxs, dxs.data(), n * sizeof(double*), cudaMemcpyHostToDevice));
+    d_e = (double*)alloc((n + 1) * (n + 1) * sizeof(double));
+    d_c = (double*)alloc((n + 1) * sizeof(double));
+    d_dots = (double*)alloc(n * sizeof(double));
+    d_state = (int*)alloc(8 * sizeof(int));
+    CCSD_CUDA(cudaMemsetAsync(d_e, 0, (n + 1) * (n + 1) * sizeof(double), ctx.stream));
+    CCSD_CUDA(cudaMemsetAsync(d_c, 0, (n + 1) * sizeof(double), ctx.stream));
+    int st[8] = {0, 0, opts.diis_start, 0, 0, 0, 0, 0};   // head, count, start, status
+    CCSD_CUDA(cudaMemcpy(d_state, st, sizeof(st), cudaMemcpyHostToDevice));
+}
+
+// ---- one iteration ---------------------------------------------------------------------
+
+void Solver::launch_iteration() {
+    cudaStream_t s = ctx.stream;
+    // contractions (ccsd.cxx:123-180)
+    ctx.run(iter_plan);
+    // Z.weight(D); T += Z; conv = Z.norm(00)  (ccsd.cxx:184-185,190), fused
+    CCSD_CUDA(cudaMemsetAsync(d_red, 0, 2 * sizeof(double), s));
+    for (int pair = 0; pair < 2; pair++) {
+        Tensor& Z = ctx.tensor(pair == 0 ? Z1 : Z2);
+        Tensor& T = ctx.tensor(pair == 0 ? T1 : T2);
+        for (size_t c = 0; c < Z.cases.size(); c++)
+            for (auto& b : Z.cases[c].blocks) {
+                if (b.size == 0) continue;
+                kern::update_block(Z.data + b.offset, T.data + b.offset, weight_args(Z, (int)c, b), d_red + 1, s);
+            }
+    }
+    // Tau from the updated T, energy (ccsd.cxx:187-189)
+    ctx.run(tau_plan);
+    ctx.run(energy_plan, nullptr, d_red + 0);
+    // DIIS (diis.hpp:70-227)
+    if (opts.diis_order > 1) diis_step();
+}
+
+void Solver::diis_step() {
+    cudaStream_t s = ctx.stream;
+    const int n = opts.diis_order;
+    Tensor& t1 = ctx.tensor(T1);
+    Tensor& t2 = ctx.tensor(T2);
+    Tensor& z1 = ctx.tensor(Z1);
+    Tensor& z2 = ctx.tensor(Z2);
+    // advance the ring: slot of the newest vector
+    kern::diis_advance(d_state, n, s);
+    // copy x, dx into the head slot (device-side slot index)
+    kern::diis_store(d_state, d_xs, d_dxs, t1.data, t1.total, t2.data, t2.total, z1.data, z2.data, s);
+    // new error-matrix row: <dx_head, dx_j> for all slots (absent slots are zero vectors)
+    CCSD_CUDA(cudaMemsetAsync(d_dots, 0, n * sizeof(double), s));
+    for (auto& sg : segs) kern::diis_dots(d_state, d_dxs, n, sg.off, sg.len, sg.w, d_dots, s);
+    // bordered system, solve, coefficients by slot
+    kern::diis_solve(d_state, d_e, d_c, d_dots, n, s);
+    // x = sum c_j x_j, dx = sum c_j dx_j  (diis.hpp:205-226)
+    kern::lincomb(t1.data, t1.total, t2.data, t2.total, d_xs, d_c, n, s);
+    kern::lincomb(z1.data, z1.total, z2.data, z2.total, d_dxs, d_c, n, s);
+}
+
+void Solver::iterate_async() {
+    if (opts.use_graph) {
+        if (!graph_exec) {
+            // the first iteration runs eagerly (it also warms every kernel), the graph is
+            // captured from the second one on
+            if (captured_once) {
+                CCSD_CUDA(cudaStreamBeginCapture(ctx.stream, cudaStreamCaptureModeThreadLocal));
+                try {
+                    launch_iteration();
+                } catch (...) {
+                    cudaGraph_t g;
+                    cudaStreamEndCapture(ctx.stream, &g);
+                    if (g) cudaGraphDestroy(g);
+                    throw;
+                }
+                CCSD_CUDA(cudaStreamEndCapture(ctx.stream, &graph));
+                CCSD_CUDA(cudaGraphInstantiate(&graph_exec, graph, 0));
+            } else {
+                launch_iteration();
+                captured_once = true;
+                iterations++;
+                return;
+            }
+        }
+        CCSD_CUDA(cudaGraphLaunch(graph_exec, ctx.stream));
+    } else {
+        launch_iteration();
+    }
+    iterations++;
+}
+
+void Solver::read_status() {
+    CCSD_CUDA(cudaMemcpyAsync(h_red, d_red, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
+    if (opts.diis_order > 1) {
+        CCSD_CUDA(cudaMemcpyAsync(h_state, d_state, 8 * sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
+    }
+    CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
+    energy = h_red[0];
+    conv = h_red[1];
+    if (opts.diis_order > 1 && h_state[3] != 0)
+        throw Error(CCSD_ERR_SINGULAR, "DIIS: singular error matrix after the eps retry");
+    if (!std::isfinite(energy) || !std::isfinite(conv)) throw Error(CCSD_DIVERGED, "NaN/Inf in energy or residual");
+}
+
+void Solver::iterate(double* e, double* c) {
+    iterate_async();
+    read_status();
+    if (e) *e = energy;
+    if (c) *c = conv;
+}
+
+int Solver::run(double* e, double* c, int* it) {
+    // Iterative::run: for (iter = 1; iter <= maxiter && !converged; iter++)
+    int status = CCSD_OK;
+    while (iterations < opts.max_iter && !(conv < opts.conv_tol)) {
+        iterate(nullptr, nullptr);
+    }
+    if (!(conv < opts.conv_tol)) status = CCSD_NOT_CONVERGED;
+    if (e) *e = energy;
+    if (c) *c = conv;
+    if (it) *it = iterations;
+    return status;
+}
+
+}  // namespace ccsd

@@ -1,0 +1,67 @@
+// CCSD solver state (see solver.cpp).
+#pragma once
+#include <vector>
+#include <utility>
+
+#include "engine.hpp"
+
+namespace ccsd {
+
+void options_default(ccsd_options* o);
+
+struct DiisSegment {
+    int64_t off, len;
+    double w;
+};
+
+class Solver {
+public:
+    Context& ctx;
+    ccsd_hamiltonian H;
+    ccsd_options opts;
+    int T1 = 0, T2 = 0, Z1 = 0, Z2 = 0, Tau = 0;
+    int FME = 0, FMI = 0, FAE = 0, WMNIJ = 0, WMNEJ = 0, WAMIJ = 0, WAMEI = 0;
+    double* den[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [space][spin]
+    Plan iter_plan, tau_plan, energy_plan;
+    double* d_red = nullptr;    // [0] energy, [1] conv
+    double* h_red = nullptr;
+    int* h_state = nullptr;
+    // DIIS
+    std::vector<double*> xs, dxs;
+    const double** d_xs = nullptr;
+    const double** d_dxs = nullptr;
+    double *d_e = nullptr, *d_c = nullptr, *d_dots = nullptr;
+    int* d_state = nullptr;
+    int64_t vec_len = 0;
+    std::vector<DiisSegment> segs;
+    // graph
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    bool captured_once = false;
+
+    int iterations = 0;
+    double energy = 0, conv = 0, mp2 = 0;
+    double flops_per_iter = 0;
+    std::vector<std::pair<void*, size_t>> owned;
+
+    Solver(Context& c, const ccsd_hamiltonian& h, const ccsd_options& o);
+    ~Solver();
+    void iterate(double* e, double* c);
+    void iterate_async();
+    void read_status();
+    int run(double* e, double* c, int* it);
+
+private:
+    void* alloc(size_t bytes);
+    void build_denominators();
+    void build_diis();
+    kern::WeightArgs weight_args(const Tensor& T, int cs, const Block& b) const;
+    void weight_tensor(int h);
+    void record_tau(Plan& p);
+    void record_energy(Plan& p);
+    void record_iteration();
+    void launch_iteration();
+    void diis_step();
+};
+
+}  // namespace ccsd

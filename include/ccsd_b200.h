@@ -164,9 +164,11 @@ typedef struct {
  * (pq|rs) = sum_P B[P,p,q] B[P,r,s] (closed shell, spatial orbitals shared by
  * both spins) and a diagonal Fock matrix eps[n].  Orbitals are ordered occupied
  * first, irrep-major inside occ and vrt, matching ccsd_ctx_set_spaces.
- * B is a host array [naux][n][n]. */
+ * B is a host array [naux][n][n]; aux_per_irrep (may be NULL) gives the irrep
+ * split of P so that each block only sums over the P of matching irrep.
+ * pack_vvvv != 0 stores VABEF with packed same-spin pairs (halves its memory). */
 int ccsd_hamiltonian_from_factor(ccsd_ctx ctx, int naux, const double* B, const double* eps,
-                                 ccsd_hamiltonian* H);
+                                 const int* aux_per_irrep, int pack_vvvv, ccsd_hamiltonian* H);
 int ccsd_hamiltonian_destroy(ccsd_ctx ctx, ccsd_hamiltonian* H);
 
 /* Solver: allocates T, Z, Tau, the 7 intermediates and the DIIS ring, forms the

@@ -1,0 +1,36 @@
+"""Seeded synthetic inputs (host code in the product library; no device needed)."""
+import numpy as np
+
+import aquarius_b200 as A
+
+
+def test_factor_is_symmetric_and_deterministic(built_lib):
+    e1, B1, *_ = A.synth_problem(7, 3, 9)
+    e2, B2, *_ = A.synth_problem(7, 3, 9)
+    assert np.array_equal(B1, B2) and np.array_equal(e1, e2)
+    assert np.array_equal(B1, B1.transpose(0, 2, 1))
+    assert B1.shape == (3 * 12, 12, 12)
+
+
+def test_orbital_energy_ranges(built_lib):
+    eps, _, occ, vrt, _ = A.synth_problem(3, 5, 20, with_B=False)
+    assert np.all((eps[:5] >= -1.2) & (eps[:5] <= -0.4))
+    assert np.all((eps[5:] >= 0.3) & (eps[5:] <= 4.0))
+    assert np.all(np.diff(eps[:5]) >= 0) and np.all(np.diff(eps[5:]) >= 0)
+
+
+def test_d2h_split_and_zero_pattern(built_lib):
+    eps, B, occ, vrt, aux = A.synth_problem(11, 12, 40, nirrep=8)
+    assert occ.sum() == 12 and vrt.sum() == 40 and aux.sum() == 3 * 52
+    assert (occ >= 1).all() and (vrt >= 1).all() and (aux >= 1).all()
+    irr = np.concatenate([np.repeat(np.arange(8), occ), np.repeat(np.arange(8), vrt)])
+    airr = np.repeat(np.arange(8), aux)
+    allowed = (irr[None, :, None] ^ irr[None, None, :]) == airr[:, None, None]
+    assert np.all(B[~allowed] == 0)
+    assert np.count_nonzero(B[allowed]) > 0.99 * allowed.sum()
+
+
+def test_different_seeds_differ(built_lib):
+    _, B1, *_ = A.synth_problem(1, 3, 6)
+    _, B2, *_ = A.synth_problem(2, 3, 6)
+    assert not np.allclose(B1, B2)
