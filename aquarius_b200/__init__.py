@@ -36,13 +36,14 @@ TENSOR_PACKED = 1
 # symbols declared in include/ccsd_b200.h
 EXPORTS = [
     "ccsd_ctx_create", "ccsd_ctx_destroy", "ccsd_last_error", "ccsd_ctx_synchronize", "ccsd_ctx_device_bytes",
-    "ccsd_ctx_launch_count", "ccsd_ctx_set_precision", "ccsd_ctx_set_spaces", "ccsd_tensor_create",
+    "ccsd_ctx_launch_count", "ccsd_ctx_set_precision", "ccsd_ctx_set_profiling", "ccsd_ctx_profile_report",
+    "ccsd_ctx_set_spaces", "ccsd_tensor_create",
     "ccsd_tensor_destroy", "ccsd_tensor_ndim", "ccsd_tensor_spin_cases", "ccsd_tensor_block_size",
     "ccsd_tensor_write_block", "ccsd_tensor_read_block", "ccsd_tensor_write", "ccsd_tensor_read", "ccsd_tensor_fill",
     "ccsd_contract", "ccsd_sum", "ccsd_scale", "ccsd_dot", "ccsd_norm", "ccsd_weight", "ccsd_options_default",
     "ccsd_hamiltonian_from_factor", "ccsd_hamiltonian_destroy", "ccsd_solver_create", "ccsd_solver_destroy",
     "ccsd_solver_mp2", "ccsd_solver_iterate", "ccsd_solver_iterate_async", "ccsd_solver_status", "ccsd_solver_run",
-    "ccsd_solver_amplitudes", "ccsd_solver_flops", "ccsd_synth_irreps", "ccsd_synth_problem",
+    "ccsd_solver_amplitudes", "ccsd_solver_flops", "ccsd_plan_query", "ccsd_synth_irreps", "ccsd_synth_problem",
 ]
 
 
@@ -94,6 +95,8 @@ def lib():
             "ccsd_ctx_device_bytes": [vp, P(i64)],
             "ccsd_ctx_launch_count": [vp, P(i64)],
             "ccsd_ctx_set_precision": [vp, ctypes.c_int, ctypes.c_int],
+            "ccsd_ctx_set_profiling": [vp, ctypes.c_int],
+            "ccsd_ctx_profile_report": [vp, ctypes.c_char_p, i64, P(i64)],
             "ccsd_ctx_set_spaces": [vp, ctypes.c_int, vp, vp, vp, vp],
             "ccsd_tensor_create": [vp, ctypes.c_char_p, vp, vp, ctypes.c_int, P(i32)],
             "ccsd_tensor_destroy": [vp, i32],
@@ -123,6 +126,7 @@ def lib():
             "ccsd_solver_run": [vp, P(dbl), P(dbl), P(ctypes.c_int)],
             "ccsd_solver_amplitudes": [vp, P(i32), P(i32)],
             "ccsd_solver_flops": [vp, P(dbl)],
+            "ccsd_plan_query": [ctypes.c_int, vp, vp, P(Options), ctypes.c_int, P(dbl), P(i64)],
             "ccsd_synth_irreps": [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp],
             "ccsd_synth_problem": [ctypes.c_uint64, ctypes.c_int, vp, vp, vp, vp, vp],
         }
@@ -175,6 +179,19 @@ def synth_problem(seed: int, o: int, v: int, nirrep: int = 1, with_B: bool = Tru
     B = np.zeros((naux, n, n)) if with_B else None
     _check(lib().ccsd_synth_problem(seed, nirrep, _ptr(occ), _ptr(vrt), _ptr(aux), _ptr(eps), _ptr(B)))
     return eps, B, occ, vrt, aux
+
+
+def plan_query(vrt, occ, diis_order=8, pack_vvvv=True, precision="fp64"):
+    """Host-only planning: (algorithmic FP64 flops per iteration, device bytes of a solve)."""
+    vrt, occ = _ints(vrt), _ints(occ)
+    o = Options()
+    lib().ccsd_options_default(ctypes.byref(o))
+    o.diis_order = diis_order
+    o.precision = PREC[precision]
+    fl, by = ctypes.c_double(), ctypes.c_int64()
+    _check(lib().ccsd_plan_query(len(vrt), _ptr(vrt), _ptr(occ), ctypes.byref(o), 1 if pack_vvvv else 0,
+                                 ctypes.byref(fl), ctypes.byref(by)))
+    return fl.value, by.value
 
 
 # ---------------------------------------------------------------------------
@@ -428,6 +445,19 @@ class Context:
         n = ctypes.c_int64()
         _check(lib().ccsd_ctx_device_bytes(self.c, ctypes.byref(n)), self.c)
         return n.value
+
+    def set_profiling(self, on=True):
+        _check(lib().ccsd_ctx_set_profiling(self.c, 1 if on else 0), self.c)
+
+    def profile_report(self):
+        """{statement: {"launches", "ms", "flops"}} for the contraction kernels timed since
+        profiling was enabled (clears the totals)."""
+        import json
+        need = ctypes.c_int64()
+        _check(lib().ccsd_ctx_profile_report(self.c, None, 0, ctypes.byref(need)), self.c)
+        buf = ctypes.create_string_buffer(int(need.value) + 16)
+        _check(lib().ccsd_ctx_profile_report(self.c, buf, len(buf), ctypes.byref(need)), self.c)
+        return json.loads(buf.value.decode())
 
     def launch_count(self):
         n = ctypes.c_int64()

@@ -180,6 +180,45 @@ int ccsd_ctx_set_precision(ccsd_ctx ctx, int precision, int slices) {
     });
 }
 
+int ccsd_ctx_set_profiling(ccsd_ctx ctx, int on) {
+    return guarded(ctx, [&] {
+        Context* c = from_handle(ctx);
+        c->collect_profile();
+        c->profiling = on != 0;
+    });
+}
+
+int ccsd_ctx_profile_report(ccsd_ctx ctx, char* buf, int64_t buflen, int64_t* needed) {
+    return guarded(ctx, [&] {
+        Context* c = from_handle(ctx);
+        c->collect_profile();
+        std::ostringstream o;
+        o.precision(10);
+        o << "{";
+        bool first = true;
+        for (auto& kv : c->profile) {
+            if (!first) o << ",";
+            first = false;
+            o << "\"";
+            for (char ch : kv.first) {
+                if (ch == '"' || ch == '\\') o << '\\';
+                o << ch;
+            }
+            o << "\":{\"launches\":" << kv.second.launches << ",\"ms\":" << kv.second.ms
+              << ",\"flops\":" << kv.second.flops << "}";
+        }
+        o << "}";
+        std::string s = o.str();
+        if (needed) *needed = (int64_t)s.size() + 1;
+        if (buf && buflen > (int64_t)s.size()) {
+            std::memcpy(buf, s.c_str(), s.size() + 1);
+            c->profile.clear();
+        } else if (buf) {
+            throw Error(CCSD_ERR_ARG, "profile buffer too small");
+        }
+    });
+}
+
 int ccsd_ctx_set_spaces(ccsd_ctx ctx, int nirrep, const int* vrt_alpha, const int* vrt_beta, const int* occ_alpha,
                         const int* occ_beta) {
     return guarded(ctx, [&] {
@@ -482,6 +521,42 @@ int ccsd_hamiltonian_destroy(ccsd_ctx ctx, ccsd_hamiltonian* H) {
             if (*t && c->tensors.count(*t)) c->destroy_tensor(*t);
             *t = 0;
         }
+    });
+}
+
+int ccsd_plan_query(int nirrep, const int* vrt, const int* occ, const ccsd_options* opts, int pack_vvvv,
+                    double* flops_per_iter, int64_t* device_bytes) {
+    return guarded(nullptr, [&] {
+        if (nirrep != 1 && nirrep != 2 && nirrep != 4 && nirrep != 8) throw Error(CCSD_ERR_ARG, "nirrep must be 1,2,4,8");
+        Context host(-1, nullptr);
+        Spaces S;
+        S.nirrep = nirrep;
+        int n = 0;
+        for (int s = 0; s < 2; s++) {
+            int ov = 0, oo = 0;
+            for (int h = 0; h < nirrep; h++) {
+                S.n[VRT][s][h] = vrt[h];
+                S.n[OCC][s][h] = occ[h];
+                S.off[VRT][s][h] = ov;
+                S.off[OCC][s][h] = oo;
+                ov += vrt[h];
+                oo += occ[h];
+            }
+            n = ov + oo;
+        }
+        host.spaces = S;
+        host.spaces_set = true;
+        ccsd_hamiltonian H;
+        create_hamiltonian_tensors(host, pack_vvvv != 0, &H);
+        const int64_t h_bytes = host.device_bytes;
+        // factor build: B (3n x n x n) plus two 256 MiB chunk buffers for packed blocks
+        const int64_t build_peak = h_bytes + (int64_t)3 * n * n * n * 8 + (int64_t)2 * (256ll << 20) * 8 / 8;
+        ccsd_options o;
+        options_default(&o);
+        if (opts) o = *opts;
+        Solver s(host, H, o);
+        if (flops_per_iter) *flops_per_iter = s.flops_per_iter;
+        if (device_bytes) *device_bytes = std::max(host.peak_bytes, build_peak);
     });
 }
 

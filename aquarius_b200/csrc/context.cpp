@@ -14,15 +14,19 @@
 namespace ccsd {
 
 Context::Context(int dev, cudaStream_t s) : device(dev), stream(s) {
-    CCSD_CUDA(cudaSetDevice(device));
-    if (!stream) {
-        CCSD_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-        own_stream = true;
+    host_only = device < 0;
+    if (!host_only) {
+        CCSD_CUDA(cudaSetDevice(device));
+        if (!stream) {
+            CCSD_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+            own_stream = true;
+        }
     }
     d_scalar = (double*)dmalloc(64 * sizeof(double));
 }
 
 Context::~Context() {
+    if (host_only) return;
     cudaSetDevice(device);
     cudaStreamSynchronize(stream);
     for (auto& kv : plan_cache) release(*kv.second);
@@ -38,24 +42,38 @@ Context::~Context() {
     cudaFree(split_ws.rowmax);
     for (auto& kv : tensors) cudaFree(kv.second->data);
     cudaFree(d_scalar);
+    for (auto& p : pending) {
+        cudaEventDestroy(p.second.first);
+        cudaEventDestroy(p.second.second);
+    }
+    for (auto e : event_pool) cudaEventDestroy(e);
     if (own_stream) cudaStreamDestroy(stream);
 }
 
 void* Context::dmalloc(size_t bytes) {
     void* p = nullptr;
     if (bytes == 0) bytes = 16;
+    if (host_only) {
+        // planning only: account the bytes, hand out a distinct never-dereferenced address
+        static uintptr_t next = 0x1000;
+        next += (bytes + 255) & ~(size_t)255;
+        device_bytes += bytes;
+        peak_bytes = std::max(peak_bytes, device_bytes);
+        return reinterpret_cast<void*>(next);
+    }
     cudaError_t e = cudaMallocAsync(&p, bytes, stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         throw Error(CCSD_ERR_OOM, "device allocation of " + std::to_string(bytes) + " bytes failed");
     }
     device_bytes += bytes;
+    peak_bytes = std::max(peak_bytes, device_bytes);
     return p;
 }
 
 void Context::dfree(void* p, size_t bytes) {
     if (!p) return;
-    cudaFreeAsync(p, stream);
+    if (!host_only) cudaFreeAsync(p, stream);
     device_bytes -= bytes;
 }
 
@@ -163,7 +181,7 @@ int Context::create_tensor(const std::string& name, const int nout[2], const int
                 }
     T->total = offset;
     T->data = (double*)dmalloc(std::max<int64_t>(offset, 1) * sizeof(double));
-    CCSD_CUDA(cudaMemsetAsync(T->data, 0, std::max<int64_t>(offset, 1) * sizeof(double), stream));
+    if (!host_only) CCSD_CUDA(cudaMemsetAsync(T->data, 0, std::max<int64_t>(offset, 1) * sizeof(double), stream));
     int h = next_handle++;
     tensors[h] = std::move(T);
     return h;
@@ -204,8 +222,26 @@ void Context::destroy_tensor(int h) {
 static int64_t* upload_table(Context& ctx, const std::vector<int64_t>& h) {
     if (h.empty()) return nullptr;
     int64_t* d = (int64_t*)ctx.dmalloc(h.size() * sizeof(int64_t));
+    if (ctx.host_only) return d;
     CCSD_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(int64_t), cudaMemcpyHostToDevice, ctx.stream));
     return d;
+}
+
+// fold recorded event pairs into per-statement totals (synchronises the stream)
+void Context::collect_profile() {
+    CCSD_CUDA(cudaStreamSynchronize(stream));
+    for (size_t i = 0; i < pending.size(); i++) {
+        float ms = 0;
+        CCSD_CUDA(cudaEventElapsedTime(&ms, pending[i].second.first, pending[i].second.second));
+        auto& e = profile[pending[i].first];
+        e.launches++;
+        e.ms += ms;
+        e.flops += pending_flops[i];
+        event_pool.push_back(pending[i].second.first);
+        event_pool.push_back(pending[i].second.second);
+    }
+    pending.clear();
+    pending_flops.clear();
 }
 
 void Context::upload(Plan& p) {
@@ -222,7 +258,7 @@ void Context::upload(Plan& p) {
     }
     // tables are uploaded from pageable host memory; make sure the copies have been
     // staged before the host vectors could change
-    if (any) CCSD_CUDA(cudaStreamSynchronize(stream));
+    if (any && !host_only) CCSD_CUDA(cudaStreamSynchronize(stream));
 }
 
 void Context::release(Plan& p) {
@@ -280,7 +316,29 @@ void Context::run(Plan& p, double* scalar_out, double* dot_target) {
     double* acc = dot_target ? dot_target : d_scalar;
     for (auto& st : p.steps) {
         switch (st.kind) {
-            case Step::GEMM: run_gemm(p.gemms[st.idx]); break;
+            case Step::GEMM: {
+                GemmStep& g = p.gemms[st.idx];
+                if (profiling) {
+                    cudaEvent_t e0, e1;
+                    if (event_pool.size() >= 2) {
+                        e0 = event_pool.back();
+                        event_pool.pop_back();
+                        e1 = event_pool.back();
+                        event_pool.pop_back();
+                    } else {
+                        CCSD_CUDA(cudaEventCreate(&e0));
+                        CCSD_CUDA(cudaEventCreate(&e1));
+                    }
+                    CCSD_CUDA(cudaEventRecord(e0, stream));
+                    run_gemm(g);
+                    CCSD_CUDA(cudaEventRecord(e1, stream));
+                    pending.push_back({g.label.empty() ? std::string("gemm") : g.label, {e0, e1}});
+                    pending_flops.push_back(g.flops());
+                } else {
+                    run_gemm(g);
+                }
+                break;
+            }
             case Step::SUM: {
                 auto& s = p.sums[st.idx];
                 kern::StridedArgs a;

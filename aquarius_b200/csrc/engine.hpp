@@ -119,6 +119,7 @@ struct GemmStep {
     int64_t *dCm[2] = {nullptr, nullptr}, *dCn[2] = {nullptr, nullptr};
     bool a_mcontig = false, a_kcontig = false, b_kcontig = false, b_ncontig = false;
     double flops() const { return 2.0 * M * N * (double)K; }
+    std::string label;                 // statement this block contraction came from
     int64_t split_cache = -1;          // key of cached A slices (constant operand)
 };
 
@@ -192,6 +193,8 @@ public:
     int next_handle = 1;
     std::string last_error;
     int64_t device_bytes = 0;
+    int64_t peak_bytes = 0;
+    bool host_only = false;            // device < 0: plan and account memory, launch nothing
     int64_t launches = 0;
     int precision = CCSD_PREC_FP64;
     int slices = 0;
@@ -200,6 +203,18 @@ public:
     std::map<int64_t, kern::SlicedOperand> split_cache;   // sliced constant operands
     int64_t split_cache_next = 1;
     std::map<std::string, std::unique_ptr<Plan>> plan_cache;
+
+    // optional per-statement timing of GEMM steps with CUDA events on the stream
+    bool profiling = false;
+    struct ProfEntry {
+        int64_t launches = 0;
+        double flops = 0, ms = 0;
+    };
+    std::map<std::string, ProfEntry> profile;
+    std::vector<std::pair<std::string, std::pair<cudaEvent_t, cudaEvent_t>>> pending;
+    std::vector<double> pending_flops;
+    std::vector<cudaEvent_t> event_pool;
+    void collect_profile();
 
     Context(int device, cudaStream_t s);
     ~Context();

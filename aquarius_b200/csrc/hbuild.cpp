@@ -217,6 +217,22 @@ int mk(Context& c, const char* name, int o0, int o1, int i0, int i1, int flags =
 
 }  // namespace
 
+void create_hamiltonian_tensors(Context& ctx, bool pack_vvvv, ccsd_hamiltonian* H) {
+    H->fAI = mk(ctx, "f(ai)", 1, 0, 0, 1);
+    H->fME = mk(ctx, "f(ia)", 0, 1, 1, 0);
+    H->fAE = mk(ctx, "f(ab)", 1, 0, 1, 0);
+    H->fMI = mk(ctx, "f(ij)", 0, 1, 0, 1);
+    H->VMNIJ = mk(ctx, "<ij||kl>", 0, 2, 0, 2);
+    H->VAMIJ = mk(ctx, "<ai||jk>", 1, 1, 0, 2);
+    H->VMNEJ = mk(ctx, "<ij||ak>", 0, 2, 1, 1);
+    H->VABIJ = mk(ctx, "<ab||ij>", 2, 0, 0, 2);
+    H->VMNEF = mk(ctx, "<ij||ab>", 0, 2, 2, 0);
+    H->VAMEI = mk(ctx, "<ai||bj>", 1, 1, 1, 1);
+    H->VAMEF = mk(ctx, "<ai||bc>", 1, 1, 2, 0);
+    H->VABEJ = mk(ctx, "<ab||ci>", 2, 0, 1, 1);
+    H->VABEF = mk(ctx, "<ab||cd>", 2, 0, 2, 0, pack_vvvv ? CCSD_TENSOR_PACKED : 0);
+}
+
 void build_hamiltonian(Context& ctx, int naux, const double* B, const double* eps, const int* aux_per_irrep,
                        bool pack_vvvv, ccsd_hamiltonian* H) {
     const Spaces& S = ctx.spaces;
@@ -235,19 +251,7 @@ void build_hamiltonian(Context& ctx, int naux, const double* B, const double* ep
     bld.dB = (double*)ctx.dmalloc(nB * sizeof(double));
     CCSD_CUDA(cudaMemcpyAsync(bld.dB, B, nB * sizeof(double), cudaMemcpyHostToDevice, ctx.stream));
 
-    H->fAI = mk(ctx, "f(ai)", 1, 0, 0, 1);
-    H->fME = mk(ctx, "f(ia)", 0, 1, 1, 0);
-    H->fAE = mk(ctx, "f(ab)", 1, 0, 1, 0);
-    H->fMI = mk(ctx, "f(ij)", 0, 1, 0, 1);
-    H->VMNIJ = mk(ctx, "<ij||kl>", 0, 2, 0, 2);
-    H->VAMIJ = mk(ctx, "<ai||jk>", 1, 1, 0, 2);
-    H->VMNEJ = mk(ctx, "<ij||ak>", 0, 2, 1, 1);
-    H->VABIJ = mk(ctx, "<ab||ij>", 2, 0, 0, 2);
-    H->VMNEF = mk(ctx, "<ij||ab>", 0, 2, 2, 0);
-    H->VAMEI = mk(ctx, "<ai||bj>", 1, 1, 1, 1);
-    H->VAMEF = mk(ctx, "<ai||bc>", 1, 1, 2, 0);
-    H->VABEJ = mk(ctx, "<ab||ci>", 2, 0, 1, 1);
-    H->VABEF = mk(ctx, "<ab||cd>", 2, 0, 2, 0, pack_vvvv ? CCSD_TENSOR_PACKED : 0);
+    create_hamiltonian_tensors(ctx, pack_vvvv, H);
 
     bld.one_electron(H->fAE, eps);
     bld.one_electron(H->fMI, eps);

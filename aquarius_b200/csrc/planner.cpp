@@ -617,6 +617,15 @@ Plan plan_contract(Context& ctx, double alpha, int hA, const std::string& idxA, 
                         // the other half is reached through the pair restriction
                         t.A.blk = find_block(A, csA, irrA);
                         t.B.blk = find_block(B, csB, irrB);
+                        // beta applies to every C block for which both factor blocks exist
+                        // (totally symmetric irrep tuples), even when they are empty
+                        // (symblocked_tensor.cxx:1033-1062).  Packed factors store only the
+                        // irrep-ordered half of their pair blocks; the other half is reached
+                        // through the pair restriction, so existence is decided by symmetry.
+                        int xa = 0, xb = 0;
+                        for (int h : irrA) xa ^= h;
+                        for (int h : irrB) xb ^= h;
+                        if (xa == 0 && xb == 0) touched.insert({(int)cc, (int)bi});
                         if (!t.A.blk || !t.B.blk) return;
                         if (t.A.blk->size == 0 || t.B.blk->size == 0) return;
                         t.bC = &bC;

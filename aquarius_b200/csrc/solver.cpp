@@ -56,6 +56,21 @@ Solver::Solver(Context& c, const ccsd_hamiltonian& h, const ccsd_options& o) : c
     WAMIJ = mk(ctx, "W~(am,ij)", 1, 1, 0, 2);
     WAMEI = mk(ctx, "W~(am,ei)", 1, 1, 1, 1);
 
+    if (ctx.host_only) {
+        // planning query: account every allocation and plan one iteration, launch nothing
+        for (int sp = 0; sp < 2; sp++)
+            for (int s = 0; s < 2; s++) den[sp][s] = (double*)alloc(std::max(ctx.spaces.total(sp, s), 1) * sizeof(double));
+        build_diis();
+        d_red = (double*)alloc(8 * sizeof(double));
+        record_tau(tau_plan);
+        record_energy(energy_plan);
+        record_iteration();
+        ctx.upload(iter_plan);
+        ctx.upload(tau_plan);
+        ctx.upload(energy_plan);
+        flops_per_iter = iter_plan.flops() + tau_plan.flops();
+        return;
+    }
     build_denominators();
     build_diis();
     d_red = (double*)ctx.dmalloc(8 * sizeof(double));
@@ -285,17 +300,20 @@ void Solver::build_diis() {
     for (int i = 0; i < n; i++) {
         xs[i] = (double*)alloc(vec_len * sizeof(double));
         dxs[i] = (double*)alloc(vec_len * sizeof(double));
-        CCSD_CUDA(cudaMemsetAsync(xs[i], 0, vec_len * sizeof(double), ctx.stream));
-        CCSD_CUDA(cudaMemsetAsync(dxs[i], 0, vec_len * sizeof(double), ctx.stream));
     }
     d_xs = (const double**)alloc(n * sizeof(double*));
     d_dxs = (const double**)alloc(n * sizeof(double*));
-    CCSD_CUDA(cudaMemcpy(d_xs, xs.data(), n * sizeof(double*), cudaMemcpyHostToDevice));
-    CCSD_CUDA(cudaMemcpy(d_dxs, dxs.data(), n * sizeof(double*), cudaMemcpyHostToDevice));
     d_e = (double*)alloc((n + 1) * (n + 1) * sizeof(double));
     d_c = (double*)alloc((n + 1) * sizeof(double));
     d_dots = (double*)alloc(n * sizeof(double));
     d_state = (int*)alloc(8 * sizeof(int));
+    if (ctx.host_only) return;
+    for (int i = 0; i < n; i++) {
+        CCSD_CUDA(cudaMemsetAsync(xs[i], 0, vec_len * sizeof(double), ctx.stream));
+        CCSD_CUDA(cudaMemsetAsync(dxs[i], 0, vec_len * sizeof(double), ctx.stream));
+    }
+    CCSD_CUDA(cudaMemcpy(d_xs, xs.data(), n * sizeof(double*), cudaMemcpyHostToDevice));
+    CCSD_CUDA(cudaMemcpy(d_dxs, dxs.data(), n * sizeof(double*), cudaMemcpyHostToDevice));
     CCSD_CUDA(cudaMemsetAsync(d_e, 0, (n + 1) * (n + 1) * sizeof(double), ctx.stream));
     CCSD_CUDA(cudaMemsetAsync(d_c, 0, (n + 1) * sizeof(double), ctx.stream));
     int st[8] = {0, 0, opts.diis_start, 0, 0, 0, 0, 0};   // head, count, start, status

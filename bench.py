@@ -1,0 +1,345 @@
+#!/usr/bin/env python
+"""CCSD amplitude-iteration benchmark: iterations/s and TFLOP/s on synthetic integrals.
+
+Default workload: closed-shell spin-orbital CCSD, C1, o=32, v=256 (the split-precision
+configuration of the benchmark spec), seeded synthetic integrals.  One "step" is one
+CCSD iteration (residual contractions, Jacobi update, energy, DIIS) with every input
+resident in HBM.  Inputs are far larger than L2 (V_abcd alone is ~51 GB), so no L2
+flush is needed between steps.
+
+  python bench.py [--steps K] [--warmup W] [--gpus N] [--workload cfg3|cfg2|...]
+                  [--precision split|fp64] [--impl engine|reference]
+
+For N>1 (torchrun, one rank per GPU) every rank runs an independent replica of the
+workload (the north star fixes one GPU per solve: "replicas only"); the value is the
+sum over ranks, timed as the max over ranks.
+
+--impl reference times the reference algorithm's CPU restatement (the oracle, numpy
++ OpenBLAS on all host cores) on a bounded sample of the same workload, scaled to the
+workload by the planner's algorithmic flop count.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "cfg2": dict(o=16, v=128, nirrep=1, seed=2, desc="synthetic closed-shell spin-orbital CCSD, C1, o=16 v=128"),
+    "cfg3": dict(o=32, v=256, nirrep=1, seed=3, desc="synthetic closed-shell spin-orbital CCSD, C1, o=32 v=256"),
+    "cfg4": dict(o=48, v=336, nirrep=8, seed=4, desc="synthetic closed-shell spin-orbital CCSD, D2h, o=48 v=336"),
+    "small": dict(o=8, v=48, nirrep=1, seed=5, desc="synthetic closed-shell spin-orbital CCSD, C1, o=8 v=48"),
+}
+# bounded CPU sample: same occupied count, fewer virtuals
+CPU_SAMPLE = {"cfg2": (16, 64), "cfg3": (32, 80), "cfg4": (24, 80), "small": (8, 48)}
+LADDER = "Z(2)[abij] += <ab||cd>[abef]*Tau[efij]"
+DIIS_ORDER = 8
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, device):
+        self.device = device
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def fp64_gemm_peak(torch, device):
+    """Measured cuBLAS DGEMM TFLOP/s (the FP64 roofline denominator; not in MEASURED_PEAKS)."""
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    best = 0.0
+    for _ in range(4):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    torch.cuda.empty_cache()
+    return best
+
+
+def cpu_sample(workload, steps=1):
+    """Time the oracle (numpy/OpenBLAS, all host threads) on a bounded sample: full
+    iterations at (o_s, v_s), scaled to the workload by the algorithmic flop ratio."""
+    import aquarius_b200 as A
+    from oracle import ccsd_oracle as O
+    w = WORKLOADS[workload]
+    o_s, v_s = CPU_SAMPLE[workload]
+    eps, B, *_ = A.synth_problem(w["seed"], o_s, v_s)
+    ref = O.CCSD(O.hamiltonian_from_factor(B, eps, o_s), diis_order=DIIS_ORDER)
+    f_sample, _ = A.plan_query([v_s], [o_s], diis_order=DIIS_ORDER)
+    if w["nirrep"] == 1:
+        f_full, _ = A.plan_query([w["v"]], [w["o"]], diis_order=DIIS_ORDER)
+    else:
+        occ, vrt, _ = A.synth_irreps(w["seed"], w["nirrep"], w["o"], w["v"])
+        f_full, _ = A.plan_query(vrt, occ, diis_order=DIIS_ORDER)
+    times = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        ref.iterate()
+        times.append(time.perf_counter() - t0)
+    return dict(times=times, f_sample=f_sample, f_full=f_full, o=o_s, v=v_s, cores=os.cpu_count())
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    w = WORKLOADS[args.workload]
+    res = cpu_sample(args.workload, steps=args.warmup + args.steps)
+    t = res["times"][args.warmup:]
+    per_iter_full = np.mean(t) * res["f_full"] / res["f_sample"]
+    value = 1.0 / per_iter_full
+    sample = (f"oracle CCSD iterations at o={res['o']} v={res['v']} (same generator), "
+              f"{len(t)} timed after {args.warmup} warm-up, scaled by algorithmic flops "
+              f"{res['f_sample']:.3e} -> {res['f_full']:.3e} per iteration")
+    line = {
+        "impl": "reference", "metric": "CCSD iterations/s", "value": value, "unit": "iter/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_iter_full * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w["desc"], "o": w["o"], "v": w["v"], "nirrep": w["nirrep"]},
+        "tflops": res["f_full"] * value / 1e12,
+        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": res["cores"], "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def timed_iterations(torch, ctx, s, stream, steps, warmup, profile):
+    for _ in range(warmup):
+        s.iterate()
+    ctx.synchronize()
+    if profile:
+        ctx.set_profiling(True)
+    ctx.profile_report() if profile else None
+    n0 = ctx.launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(steps):
+        s.iterate_async()
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = ctx.launch_count() - n0
+    prof = ctx.profile_report() if profile else {}
+    if profile:
+        ctx.set_profiling(False)
+    e, c, it = s.status()
+    return ms, launches, prof, e, c
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--workload", default="cfg3", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="auto", choices=["auto", "split", "fp64"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64-ref", action="store_true", help="skip the native-FP64 comparison run")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import aquarius_b200 as A
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    w = WORKLOADS[args.workload]
+    split_ok = A.lib() is not None and _split_available(A)
+    prec = args.precision if args.precision != "auto" else ("split" if split_ok else "fp64")
+
+    stream = torch.cuda.Stream(device=local)
+    ctx = A.Context(local, stream.cuda_stream)
+    eps, B, occ, vrt, aux = A.synth_problem(w["seed"] + rank, w["o"], w["v"], nirrep=w["nirrep"])
+    ctx.set_spaces(vrt=vrt, occ=occ)
+    t0 = time.perf_counter()
+    H = ctx.hamiltonian_from_factor(B, eps, aux_per_irrep=aux if w["nirrep"] > 1 else None)
+    ctx.synchronize()
+    log(f"[bench] H built in {time.perf_counter() - t0:.1f}s, device bytes {ctx.device_bytes() / 1e9:.1f} GB")
+
+    peaks, peak_kind = measured_peaks()
+    results = {}
+    order = ["fp64", prec] if (prec == "split" and not args.no_fp64_ref) else [prec]
+    for p in order:
+        s = ctx.solver(H, diis_order=DIIS_ORDER, precision=p, conv_tol=1e-9, max_iter=1000)
+        flops = s.flops()
+        with Clocks(local) as clk:
+            if dist:
+                dist.barrier()
+            torch.cuda.synchronize()
+            ms, launches, prof, e, c = timed_iterations(torch, ctx, s, stream, args.steps, args.warmup, True)
+            torch.cuda.synchronize()
+        if dist:
+            t = torch.tensor([ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        results[p] = dict(ms=ms, launches=launches, prof=prof, energy=e, conv=c, flops=flops,
+                          clocks=clk.summary(), energies=None)
+        log(f"[bench] {p}: {ms / args.steps:.1f} ms/iter, E={e:.12f}, conv={c:.3e}, launches={launches}")
+        s.close()
+    head = results[prec]
+    ms_step = head["ms"] / args.steps
+    value = world * args.steps / (head["ms"] * 1e-3)
+
+    # roofline of the dominant kernel (the particle-ladder contraction)
+    lad = head["prof"].get(LADDER, {"ms": 0, "flops": 0, "launches": 0})
+    fp64_peak = fp64_gemm_peak(torch, local) if True else None
+    if prec == "fp64":
+        peak, unit_kind = fp64_peak, "measured cuBLAS DGEMM (this run)"
+    else:
+        peak, unit_kind = peaks["bf16_tflops"], f"{peak_kind} bf16 (MEASURED_PEAKS.json)"
+    achieved = lad["flops"] / (lad["ms"] * 1e-3) / 1e12 if lad["ms"] else 0.0
+    roofline = {"bound": "tensor", "kernel": LADDER, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": achieved / peak if peak else None, "traffic": None, "peak_kind": unit_kind,
+                "launches_per_step": lad["launches"] / args.steps,
+                "share_of_step": lad["ms"] / head["ms"] if head["ms"] else None}
+
+    # end to end through the public API: host factor -> H on device -> solve -> energy
+    e2e = None
+    if not args.no_e2e:
+        H.destroy()
+        Bp = torch.empty(B.shape, dtype=torch.float64, pin_memory=True).numpy()
+        Bp[...] = B
+        epsp = torch.empty(eps.shape, dtype=torch.float64, pin_memory=True).numpy()
+        epsp[...] = eps
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        H2 = ctx.hamiltonian_from_factor(Bp, epsp, aux_per_irrep=aux if w["nirrep"] > 1 else None)
+        s = ctx.solver(H2, diis_order=DIIS_ORDER, precision=prec, conv_tol=1e-9, max_iter=60)
+        e_fin, c_fin, iters = s.run()
+        t_tot = time.perf_counter() - t0
+        s.close()
+        H2.destroy()
+        e2e = {"value": iters / t_tot, "unit": "iter/s", "h2d_bytes_per_step": int(Bp.nbytes + epsp.nbytes),
+               "d2h_bytes_per_step": int(16 * iters + 8), "time_to_converged_s": t_tot, "iterations": iters,
+               "energy": e_fin, "conv": c_fin, "step": "one full solve from host factor to converged energy"}
+        log(f"[bench] e2e: {iters} iterations in {t_tot:.1f}s, E={e_fin:.12f}")
+    ctx.close()
+
+    cpu = None
+    if not args.no_cpu and rank == 0:
+        res = cpu_sample(args.workload, steps=1)
+        per_iter_full = res["times"][0] * res["f_full"] / res["f_sample"]
+        cpu = {"value": 1.0 / per_iter_full, "unit": "iter/s", "cores": res["cores"], "kind": "port",
+               "sample": f"1 oracle iteration at o={res['o']} v={res['v']} ({res['times'][0]:.1f}s), scaled by "
+                         f"algorithmic flops {res['f_sample']:.3e} -> {res['f_full']:.3e}"}
+
+    if rank == 0:
+        line = {
+            "metric": "CCSD iterations/s", "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "bf16x3-split->f64",
+            "data": "synthetic (seeded generator, B[P,p,q] factor, eps occ U[-1.2,-0.4] vrt U[0.3,4.0])",
+            "config": {"workload": w["desc"], "o": w["o"], "v": w["v"], "nirrep": w["nirrep"], "precision": prec,
+                       "diis_order": DIIS_ORDER, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (V_abcd ~51 GB at o=32 v=256); no flush"},
+            "tflops": head["flops"] * value / world / 1e12 * world,
+            "flops_per_iter": head["flops"],
+            "energy": head["energy"], "conv": head["conv"],
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": head["clocks"],
+            "gpu_launches": head["launches"],
+        }
+        if "fp64" in results and prec != "fp64":
+            f = results["fp64"]
+            line["fp64_plain"] = {"iters_per_s": world * args.steps / (f["ms"] * 1e-3),
+                                  "ms_per_step": f["ms"] / args.steps, "energy": f["energy"],
+                                  "abs_dE_vs_split": abs(f["energy"] - head["energy"])}
+            line["speedup_vs_fp64_plain"] = f["ms"] / head["ms"]
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def _split_available(A):
+    try:
+        ctx = A.Context(int(os.environ.get("LOCAL_RANK", "0")))
+        ctx.set_spaces(vrt=[2], occ=[1])
+        ctx.set_precision("split")
+        ctx.close()
+        return True
+    except A.CcsdError:
+        return False
+
+
+if __name__ == "__main__":
+    sys.exit(main())

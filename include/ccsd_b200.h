@@ -81,6 +81,12 @@ int ccsd_ctx_device_bytes(ccsd_ctx ctx, int64_t* bytes);
 int ccsd_ctx_launch_count(ccsd_ctx ctx, int64_t* count);
 /* precision used by subsequent ccsd_contract calls (CCSD_PREC_*); slices=0: default */
 int ccsd_ctx_set_precision(ccsd_ctx ctx, int precision, int slices);
+/* Per-statement timing of contraction kernels with CUDA events on the context stream
+ * (the role of the reference's named timers, src/time/time.hpp:103-147).  The report is
+ * a JSON object {statement: {"launches": n, "ms": t, "flops": f}}; it synchronises the
+ * stream and clears the totals.  *needed receives the buffer size required. */
+int ccsd_ctx_set_profiling(ccsd_ctx ctx, int on);
+int ccsd_ctx_profile_report(ccsd_ctx ctx, char* buf, int64_t buflen, int64_t* needed);
 
 /* Orbital spaces (Space of src/operator/space.hpp): per-irrep counts of
  * alpha/beta virtual and occupied orbitals.  nirrep in {1,2,4,8}. */
@@ -189,6 +195,14 @@ int ccsd_solver_run(ccsd_solver s, double* energy, double* conv, int* iterations
 int ccsd_solver_amplitudes(ccsd_solver s, ccsd_tensor* T1, ccsd_tensor* T2);
 /* algorithmic FP64 flops of one iteration as planned (packed-pair counts) */
 int ccsd_solver_flops(ccsd_solver s, double* flops);
+
+/* Planning query, host only (no device is touched): algorithmic FP64 flops of one
+ * iteration (reference flop convention: packed same-spin pairs count once) and the
+ * device bytes a solve of these spaces needs (H + amplitudes + intermediates + DIIS
+ * ring + plan tables; the peak of the factor build included).  Serves admission by
+ * HBM footprint.  Closed-shell spaces: alpha = beta counts. */
+int ccsd_plan_query(int nirrep, const int* vrt_per_irrep, const int* occ_per_irrep, const ccsd_options* opts,
+                    int pack_vvvv, double* flops_per_iter, int64_t* device_bytes);
 
 /* ---- synthetic inputs (seeded; identical on every host) -------------------- */
 /* irrep sizes: Dirichlet(1.5) split of o, v and naux = 3(o+v) (aux may be NULL) */

@@ -143,3 +143,95 @@ def reference_contract(alpha, A, ia, B, ib, beta, C, ic, groupC):
             axes[m[p]] = p
         acc += sign * np.transpose(X, axes)
     return beta * C + alpha * acc
+
+
+def _spin_cases(nout, nin):
+    gs = [nout[0], nout[1], nin[0], nin[1]]
+    out = []
+    for a in itertools.product(*[range(g + 1) for g in gs]):
+        if a[2] + a[3] == a[0] + a[1] + (sum(nin) - sum(nout)) // 2:
+            out.append(a)
+    return out
+
+
+def _case_exists(nout, nin, spins):
+    """spins per position -> does the spin case exist (spin conservation)"""
+    group = [0] * nout[0] + [1] * nout[1] + [2] * nin[0] + [3] * nin[1]
+    a = [0, 0, 0, 0]
+    for p, s in enumerate(spins):
+        if s == 0:
+            a[group[p]] += 1
+    return a[2] + a[3] == a[0] + a[1] + (sum(nin) - sum(nout)) // 2
+
+
+def beta_mask(ctx, shapes, ia, ib, ic):
+    """Full-array mask of C elements whose block receives beta: blocks (spin case, irrep
+    tuple) of C for which some antisymmetriser term, internal spin and internal irrep
+    assignment has symmetry-allowed A and B blocks (symblocked_tensor.cxx:1033-1062)."""
+    (anout, anin), (bnout, bnin), (cnout, cnin) = shapes
+    cgroup = [0] * cnout[0] + [1] * cnout[1] + [2] * cnin[0] + [3] * cnin[1]
+    cspace = [g % 2 for g in cgroup]
+    internal = sorted(set(ia) & set(ib))
+    groups = []
+    for g in range(4):
+        pos = [p for p in range(len(ic)) if cgroup[p] == g]
+        if pos:
+            groups.append((pos, [0 if ic[p] in ia else (1 if ic[p] in ib else 2) for p in pos]))
+    terms = shuffles(groups)
+    dims = [2 * ctx.total(s) for s in cspace]
+    mask = np.zeros(dims, dtype=bool)
+    nirr = ctx.nirrep
+    for case in _spin_cases((cnout[0], cnout[1]), (cnin[0], cnin[1])):
+        cspins = []
+        for g, gs in enumerate([cnout[0], cnout[1], cnin[0], cnin[1]]):
+            cspins += [0] * case[g] + [1] * (gs - case[g])
+        for cirr in itertools.product(range(nirr), repeat=len(ic)):
+            x = 0
+            for h in cirr:
+                x ^= h
+            if x:
+                continue
+            hit = False
+            for m, _sign in terms:
+                for ispin in itertools.product((0, 1), repeat=len(internal)):
+                    for iirr in itertools.product(range(nirr), repeat=len(internal)):
+                        sp, hh = {}, {}
+                        for p in range(len(ic)):
+                            sp[ic[p]] = cspins[m[p]]
+                            hh[ic[p]] = cirr[m[p]]
+                        for k, l in enumerate(internal):
+                            sp[l] = ispin[k]
+                            hh[l] = iirr[k]
+                        xa = 0
+                        for l in ia:
+                            xa ^= hh[l]
+                        xb = 0
+                        for l in ib:
+                            xb ^= hh[l]
+                        if xa or xb:
+                            continue
+                        if not _case_exists(anout, anin, [sp[l] for l in ia]):
+                            continue
+                        if not _case_exists(bnout, bnin, [sp[l] for l in ib]):
+                            continue
+                        hit = True
+                        break
+                    if hit:
+                        break
+                if hit:
+                    break
+            if not hit:
+                continue
+            sl = []
+            for p in range(len(ic)):
+                lo = cspins[p] * ctx.total(cspace[p]) + ctx.offset(cspace[p], cirr[p])
+                sl.append(slice(lo, lo + ctx.count(cspace[p], cspins[p], cirr[p])))
+            # every arrangement of the block inside its groups shares the block's beta
+            gpos = [[p for p in range(len(ic)) if cgroup[p] == g] for g in range(4)]
+            for combo in itertools.product(*[list(itertools.permutations(gp)) for gp in gpos]):
+                perm = list(range(len(ic)))
+                for gp, pg in zip(gpos, combo):
+                    for a_, b_ in zip(gp, pg):
+                        perm[a_] = b_
+                mask[tuple(sl[perm[q]] for q in range(len(ic)))] = True
+    return mask

@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 import aquarius_b200 as A
-from tests.helpers import random_so, reference_contract, write_full
+from tests.helpers import beta_mask, random_so, reference_contract, write_full
 
 pytestmark = pytest.mark.gpu
 
@@ -53,7 +53,8 @@ def _ctx(nirrep):
     if nirrep == 1:
         ctx.set_spaces(vrt=[5], occ=[3])
     else:
-        ctx.set_spaces(vrt=[2, 1, 2, 1][:nirrep] if nirrep == 4 else [3, 2], occ=[1, 1, 1, 0][:nirrep] if nirrep == 4 else [2, 1])
+        # irrep 3 has no occupied orbital: blocks exist but are empty
+        ctx.set_spaces(vrt=[2, 1, 2, 1] if nirrep == 4 else [3, 2], occ=[1, 1, 1, 0] if nirrep == 4 else [2, 1])
     return ctx
 
 
@@ -76,7 +77,10 @@ def test_statement_matches_reference(nirrep, stmt):
         alpha, beta = 0.75, -1.25
         ctx.contract(alpha, tA, ia, tB, ib, beta, tC, ic)
         got = tC.to_full()
-        ref = reference_contract(alpha, fa, ia, fb, ib, beta, fc, ic, tC.group)
+        ref = reference_contract(alpha, fa, ia, fb, ib, 1.0, fc, ic, tC.group)
+        # beta reaches only the C blocks that receive a contribution (lazy beta)
+        bm = beta_mask(ctx, (SHAPES[as_], SHAPES[bs], SHAPES[cs]), ia, ib, ic)
+        ref = ref + np.where(bm, (beta - 1.0) * fc, 0.0)
         assert np.abs(got - ref).max() < 1e-12 * max(1.0, np.abs(ref).max())
     finally:
         ctx.close()
