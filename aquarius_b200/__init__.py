@@ -44,6 +44,7 @@ EXPORTS = [
     "ccsd_hamiltonian_from_factor", "ccsd_hamiltonian_destroy", "ccsd_solver_create", "ccsd_solver_destroy",
     "ccsd_solver_mp2", "ccsd_solver_iterate", "ccsd_solver_iterate_async", "ccsd_solver_status", "ccsd_solver_run",
     "ccsd_solver_amplitudes", "ccsd_solver_flops", "ccsd_plan_query", "ccsd_synth_irreps", "ccsd_synth_problem",
+    "ccsd_dot_batch_noalloc",
 ]
 
 
@@ -127,6 +128,7 @@ def lib():
             "ccsd_solver_amplitudes": [vp, P(i32), P(i32)],
             "ccsd_solver_flops": [vp, P(dbl)],
             "ccsd_plan_query": [ctypes.c_int, vp, vp, P(Options), ctypes.c_int, P(dbl), P(i64)],
+            "ccsd_dot_batch_noalloc": [vp, vp, vp, ctypes.c_int, i64, vp],
             "ccsd_synth_irreps": [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp],
             "ccsd_synth_problem": [ctypes.c_uint64, ctypes.c_int, vp, vp, vp, vp, vp],
         }
@@ -179,6 +181,14 @@ def synth_problem(seed: int, o: int, v: int, nirrep: int = 1, with_B: bool = Tru
     B = np.zeros((naux, n, n)) if with_B else None
     _check(lib().ccsd_synth_problem(seed, nirrep, _ptr(occ), _ptr(vrt), _ptr(aux), _ptr(eps), _ptr(B)))
     return eps, B, occ, vrt, aux
+
+
+def dot_batch_noalloc(stream: int, x_ptr: int, y_ptrs, n: int, out_ptr: int):
+    """out[j] = <x, y_j> on caller-owned device buffers; the library allocates nothing
+    (see ccsd_dot_batch_noalloc in include/ccsd_b200.h).  Stream-ordered, no sync."""
+    ys = (ctypes.c_void_p * max(len(y_ptrs), 1))(*[ctypes.c_void_p(p) for p in y_ptrs])
+    _check(lib().ccsd_dot_batch_noalloc(ctypes.c_void_p(stream), ctypes.c_void_p(x_ptr), ys, len(y_ptrs), n,
+                                        ctypes.c_void_p(out_ptr)))
 
 
 def plan_query(vrt, occ, diis_order=8, pack_vvvv=True, precision="fp64"):

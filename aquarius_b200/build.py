@@ -15,7 +15,7 @@ CSRC = HERE / "csrc"
 OUT = HERE / "libccsd_b200.so"
 BUILD = HERE / "_build"
 
-CU = ["kernels_fp64.cu", "kernels_split.cu"]
+CU = ["kernels_fp64.cu", "kernels_split.cu", "noalloc.cu"]
 CPP = ["context.cpp", "planner.cpp", "solver.cpp", "hbuild.cpp", "capi.cpp", "synth.cpp", "split_exec.cpp"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

@@ -18,18 +18,22 @@ struct ccsd_solver_s {
     ccsd::Solver* s = nullptr;
 };
 
+namespace {
+thread_local std::string g_global_error;
+}
+
 namespace ccsd {
 Context* from_handle(ccsd_ctx c) {
     if (!c || !c->c) throw Error(CCSD_ERR_ARG, "null context");
     return c->c;
 }
+// message for entry points that have no context (ccsd_last_error(NULL))
+void set_global_error(const std::string& msg) { g_global_error = msg; }
 }  // namespace ccsd
 
 using namespace ccsd;
 
 namespace {
-
-thread_local std::string g_global_error;
 
 template <class F>
 int guarded(ccsd_ctx ctx, F f) {

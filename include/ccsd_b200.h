@@ -204,6 +204,21 @@ int ccsd_solver_flops(ccsd_solver s, double* flops);
 int ccsd_plan_query(int nirrep, const int* vrt_per_irrep, const int* occ_per_irrep, const ccsd_options* opts,
                     int pack_vvvv, double* flops_per_iter, int64_t* device_bytes);
 
+/* ---- allocation-free variant -------------------------------------------------
+ * No counterpart in the reference.  out[j] = <x, ys[j]> for j < ny, the batched dot of
+ * the DIIS error-matrix row, for callers that must not have the library allocate device
+ * memory (an application owning all device memory through its own arena, or a call
+ * issued while a stream is being captured).  x, every ys[j] (n doubles each) and out
+ * (ny doubles) are caller-owned device buffers on the current device; ys itself is a
+ * HOST array of ny device pointers; work is ordered on `stream` (a cudaStream_t, NULL
+ * for the default stream) and the call does not synchronise.  The partial sums live in
+ * a fixed 32 KiB device array inside the library: ny is limited to 1..16 (else
+ * CCSD_ERR_ARG, message in ccsd_last_error(NULL)); calls whose kernels overlap on the
+ * GPU share that array and race, so serialise them; the first call on a device looks
+ * the array up with cudaGetSymbolAddress and should precede any stream capture. */
+int ccsd_dot_batch_noalloc(void* stream, const double* x, const double* const* ys, int ny, int64_t n,
+                           double* out);
+
 /* ---- synthetic inputs (seeded; identical on every host) -------------------- */
 /* irrep sizes: Dirichlet(1.5) split of o, v and naux = 3(o+v) (aux may be NULL) */
 int ccsd_synth_irreps(uint64_t seed, int nirrep, int o, int v,
