@@ -246,6 +246,7 @@ void Context::collect_profile() {
 
 void Context::upload(Plan& p) {
     bool any = false;
+    if (p.scratch_elems > 0 && !p.scratch) p.scratch = (double*)dmalloc(p.scratch_elems * sizeof(double));
     for (auto& g : p.gemms) {
         if (g.dAm) continue;
         any = true;
@@ -262,6 +263,8 @@ void Context::upload(Plan& p) {
 }
 
 void Context::release(Plan& p) {
+    if (p.scratch) dfree(p.scratch, p.scratch_elems * sizeof(double));
+    p.scratch = nullptr;
     for (auto& g : p.gemms) {
         auto fr = [&](int64_t*& d, size_t n) {
             if (d) dfree(d, n * sizeof(int64_t));
@@ -278,14 +281,19 @@ void Context::release(Plan& p) {
     }
 }
 
-void Context::run_gemm(GemmStep& g) {
-    Tensor& A = tensor(g.tA);
-    Tensor& B = tensor(g.tB);
-    Tensor& C = tensor(g.tC);
+double* Context::data_of(Plan& p, int h) {
+    if (h == kScratch) {
+        if (!p.scratch) throw Error(CCSD_ERR_PLAN, "plan scratch not allocated");
+        return p.scratch;
+    }
+    return tensor(h).data;
+}
+
+void Context::run_gemm(Plan& p, GemmStep& g) {
     kern::GemmArgs a;
-    a.A = A.data;
-    a.B = B.data;
-    a.C = C.data;
+    a.A = data_of(p, g.tA);
+    a.B = data_of(p, g.tB);
+    a.C = data_of(p, g.tC);
     a.M = g.M;
     a.N = g.N;
     a.K = g.K;
@@ -330,12 +338,12 @@ void Context::run(Plan& p, double* scalar_out, double* dot_target) {
                         CCSD_CUDA(cudaEventCreate(&e1));
                     }
                     CCSD_CUDA(cudaEventRecord(e0, stream));
-                    run_gemm(g);
+                    run_gemm(p, g);
                     CCSD_CUDA(cudaEventRecord(e1, stream));
                     pending.push_back({g.label.empty() ? std::string("gemm") : g.label, {e0, e1}});
                     pending_flops.push_back(g.flops());
                 } else {
-                    run_gemm(g);
+                    run_gemm(p, g);
                 }
                 break;
             }
@@ -350,12 +358,12 @@ void Context::run(Plan& p, double* scalar_out, double* dot_target) {
                     a.sB[d] = s.sC[d];
                     a.total *= s.len[d];
                 }
-                kern::sum_strided(tensor(s.tA).data + s.offA, tensor(s.tC).data + s.offC, a, s.alpha, stream);
+                kern::sum_strided(data_of(p, s.tA) + s.offA, data_of(p, s.tC) + s.offC, a, s.alpha, stream);
                 break;
             }
             case Step::SCALE: {
                 auto& s = p.scales[st.idx];
-                kern::scale(tensor(s.tC).data + s.off, s.n, s.beta, stream);
+                kern::scale(data_of(p, s.tC) + s.off, s.n, s.beta, stream);
                 break;
             }
             case Step::DOT: {

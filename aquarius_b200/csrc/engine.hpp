@@ -155,7 +155,12 @@ struct Step {
     int idx;                           // index into the typed vector of the plan
 };
 
+// tensor handle standing for the plan's scratch product buffer
+constexpr int kScratch = -1;
+
 struct Plan {
+    int64_t scratch_elems = 0;         // doubles of scratch the steps need (products X)
+    double* scratch = nullptr;         // allocated at upload
     std::vector<Step> steps;
     std::vector<GemmStep> gemms;
     std::vector<SumStep> sums;
@@ -231,7 +236,8 @@ public:
     // scalar_out: host destination of the dot result (synchronises); dot_target: device
     // accumulator the dots add into instead of the context scalar (not zeroed here)
     void run(Plan& p, double* scalar_out = nullptr, double* dot_target = nullptr);
-    void run_gemm(GemmStep& g);
+    void run_gemm(Plan& p, GemmStep& g);
+    double* data_of(Plan& p, int h);
     void run_split_gemm(GemmStep& g, kern::GemmArgs& a);
     std::vector<int> constant_tensors;  // handles whose contents never change (sliced once)
     bool is_constant(int h) const;

@@ -48,6 +48,7 @@ void Plan::append(Plan&& o) {
     for (auto& g : o.sums) sums.push_back(g);
     for (auto& g : o.scales) scales.push_back(g);
     for (auto& g : o.dots) dots.push_back(g);
+    scratch_elems = std::max(scratch_elems, o.scratch_elems);
 }
 
 namespace {
@@ -341,8 +342,16 @@ bool unit_ok(const std::vector<Unit>& units, const std::vector<Var>& vars) {
     return true;
 }
 
+// Destination of a lowered block contraction: a block of C (external pair restrictions
+// allowed), or the plan's scratch product X with the given strides per C position.
+struct Dest {
+    int handle = 0;
+    bool scratch = false;
+    std::vector<int64_t> stride;   // per C position (scratch only)
+};
+
 void lower_gemm(Context& ctx, Term& t, int hA, int hB, int hC, int cc, std::set<std::pair<int, int>>& touched,
-                Plan& plan) {
+                Plan& plan, const Dest* dest_x = nullptr) {
     const auto& vars = t.vars;
     // pair restrictions
     std::vector<std::pair<int, int>> kpairs, mpairs, npairs;
@@ -378,8 +387,10 @@ void lower_gemm(Context& ctx, Term& t, int hA, int hB, int hC, int cc, std::set<
             }
     };
     find_pairs(t.kvars, t.A, &t.B, kpairs, false);
-    find_pairs(t.mvars, t.A, nullptr, mpairs, true);
-    find_pairs(t.nvars, t.B, nullptr, npairs, true);
+    if (!dest_x) {
+        find_pairs(t.mvars, t.A, nullptr, mpairs, true);
+        find_pairs(t.nvars, t.B, nullptr, npairs, true);
+    }
     for (size_t i = 0; i < kpairs.size(); i++) factor *= 2.0;
 
     // packed operands must be read through restricted pairs only
@@ -403,7 +414,7 @@ void lower_gemm(Context& ctx, Term& t, int hA, int hB, int hC, int cc, std::set<
     GemmStep g;
     g.tA = hA;
     g.tB = hB;
-    g.tC = hC;
+    g.tC = dest_x ? kScratch : hC;
     int64_t M = 1, N = 1, K = 1;
     for (auto& u : mu) M *= u.size;
     for (auto& u : nu) N *= u.size;
@@ -432,53 +443,75 @@ void lower_gemm(Context& ctx, Term& t, int hA, int hB, int hC, int cc, std::set<
     enumerate_dim(nu, vars, [&](int64_t k, const std::vector<int64_t>& val) {
         g.hBn[k] = bB.offset + operand_offset(t.B, val, all_n);
     });
-    // C destinations (C unpacked): variants swap the values (and irreps) of restricted pairs;
-    // a swapped pair with unequal irreps lands in the C block with those irreps exchanged.
-    const Tensor& Ct = *ctx.tensors[hC];
-    g.nvm = mpairs.empty() ? 1 : 2;
-    g.nvn = npairs.empty() ? 1 : 2;
-    if (mpairs.size() > 1 || npairs.size() > 1) fail(CCSD_ERR_PLAN, "more than one restricted output pair per factor");
-    const Block* dest[2][2];
-    for (int a = 0; a < g.nvm; a++)
-        for (int b = 0; b < g.nvn; b++) {
-            std::vector<int> irr = bC.irrep;
-            if (a) std::swap(irr[mpairs[0].first], irr[mpairs[0].second]);
-            if (b) std::swap(irr[npairs[0].first], irr[npairs[0].second]);
-            dest[a][b] = find_block(Ct, cc, irr);
-            if (!dest[a][b]) fail(CCSD_ERR_PLAN, "missing destination block for a restricted pair");
-            touched.insert({cc, (int)Ct.cases[cc].block_of.at(irr)});
-        }
-    if (g.nvm == 2 && g.nvn == 2 && dest[1][1]->offset - dest[1][0]->offset != dest[0][1]->offset - dest[0][0]->offset)
-        fail(CCSD_ERR_PLAN, "restricted pairs in both dimensions across irrep blocks");
-    auto c_off = [&](const std::vector<int64_t>& val, const std::vector<int>& vl, int swapmask,
-                     const std::vector<std::pair<int, int>>& prs, const Block& blk) {
-        std::vector<int64_t> v2 = val;
-        if (swapmask)
-            for (auto& pr : prs) std::swap(v2[pr.first], v2[pr.second]);
-        int64_t off = 0;
-        std::vector<char> use(vars.size(), 0);
-        for (int v : vl) use[v] = 1;
-        for (size_t p = 0; p < t.cvar.size(); p++)
-            if (use[t.cvar[p]]) off += blk.stride[p] * v2[t.cvar[p]];
-        return off;
-    };
-    for (int v = 0; v < g.nvm; v++) {
-        g.hCm[v].resize(M);
-        const Block& blk = *dest[v][0];
+    if (dest_x) {
+        // plain column-major scratch product: no variants
+        g.nvm = g.nvn = 1;
+        std::vector<char> um(vars.size(), 0), un(vars.size(), 0);
+        for (int v : all_m) um[v] = 1;
+        for (int v : all_n) un[v] = 1;
+        g.hCm[0].resize(M);
+        g.hCn[0].resize(N);
         enumerate_dim(mu, vars, [&](int64_t k, const std::vector<int64_t>& val) {
-            g.hCm[v][k] = blk.offset + c_off(val, all_m, v, mpairs, blk);
+            int64_t off = 0;
+            for (size_t p = 0; p < t.cvar.size(); p++)
+                if (um[t.cvar[p]]) off += dest_x->stride[p] * val[t.cvar[p]];
+            g.hCm[0][k] = off;
         });
-    }
-    for (int v = 0; v < g.nvn; v++) {
-        g.hCn[v].resize(N);
-        const Block& blk = *dest[0][v];
-        const int64_t shift = dest[0][v]->offset - dest[0][0]->offset;
         enumerate_dim(nu, vars, [&](int64_t k, const std::vector<int64_t>& val) {
-            g.hCn[v][k] = shift + c_off(val, all_n, v, npairs, blk);
+            int64_t off = 0;
+            for (size_t p = 0; p < t.cvar.size(); p++)
+                if (un[t.cvar[p]]) off += dest_x->stride[p] * val[t.cvar[p]];
+            g.hCn[0][k] = off;
         });
+    } else {
+        // C destinations (C unpacked): variants swap the values (and irreps) of restricted pairs;
+        // a swapped pair with unequal irreps lands in the C block with those irreps exchanged.
+        const Tensor& Ct = *ctx.tensors[hC];
+        g.nvm = mpairs.empty() ? 1 : 2;
+        g.nvn = npairs.empty() ? 1 : 2;
+        if (mpairs.size() > 1 || npairs.size() > 1) fail(CCSD_ERR_PLAN, "more than one restricted output pair per factor");
+        const Block* dest[2][2];
+        for (int a = 0; a < g.nvm; a++)
+            for (int b = 0; b < g.nvn; b++) {
+                std::vector<int> irr = bC.irrep;
+                if (a) std::swap(irr[mpairs[0].first], irr[mpairs[0].second]);
+                if (b) std::swap(irr[npairs[0].first], irr[npairs[0].second]);
+                dest[a][b] = find_block(Ct, cc, irr);
+                if (!dest[a][b]) fail(CCSD_ERR_PLAN, "missing destination block for a restricted pair");
+                touched.insert({cc, (int)Ct.cases[cc].block_of.at(irr)});
+            }
+        if (g.nvm == 2 && g.nvn == 2 && dest[1][1]->offset - dest[1][0]->offset != dest[0][1]->offset - dest[0][0]->offset)
+            fail(CCSD_ERR_PLAN, "restricted pairs in both dimensions across irrep blocks");
+        auto c_off = [&](const std::vector<int64_t>& val, const std::vector<int>& vl, int swapmask,
+                         const std::vector<std::pair<int, int>>& prs, const Block& blk) {
+            std::vector<int64_t> v2 = val;
+            if (swapmask)
+                for (auto& pr : prs) std::swap(v2[pr.first], v2[pr.second]);
+            int64_t off = 0;
+            std::vector<char> use(vars.size(), 0);
+            for (int v : vl) use[v] = 1;
+            for (size_t p = 0; p < t.cvar.size(); p++)
+                if (use[t.cvar[p]]) off += blk.stride[p] * v2[t.cvar[p]];
+            return off;
+        };
+        for (int v = 0; v < g.nvm; v++) {
+            g.hCm[v].resize(M);
+            const Block& blk = *dest[v][0];
+            enumerate_dim(mu, vars, [&](int64_t k, const std::vector<int64_t>& val) {
+                g.hCm[v][k] = blk.offset + c_off(val, all_m, v, mpairs, blk);
+            });
+        }
+        for (int v = 0; v < g.nvn; v++) {
+            g.hCn[v].resize(N);
+            const Block& blk = *dest[0][v];
+            const int64_t shift = dest[0][v]->offset - dest[0][0]->offset;
+            enumerate_dim(nu, vars, [&](int64_t k, const std::vector<int64_t>& val) {
+                g.hCn[v][k] = shift + c_off(val, all_n, v, npairs, blk);
+            });
+        }
+        for (int a = 0; a < g.nvm; a++)
+            for (int b = 0; b < g.nvn; b++) g.vsign[a * g.nvn + b] = ((a + b) % 2) ? -1.0 : 1.0;
     }
-    for (int a = 0; a < g.nvm; a++)
-        for (int b = 0; b < g.nvn; b++) g.vsign[a * g.nvn + b] = ((a + b) % 2) ? -1.0 : 1.0;
     // contiguity hints
     auto contig = [](const std::vector<int64_t>& t) {
         if (t.size() < 2) return true;
@@ -558,13 +591,66 @@ Plan plan_contract(Context& ctx, double alpha, int hA, const std::string& idxA, 
     std::set<std::pair<int, int>> touched;   // (case, block) of C that received a term
     std::vector<Plan> parts;
 
+    // Internal pairs antisymmetric in both factors (same group of A and same group of B,
+    // nothing else internal in those groups): the spin assignments (a,b) and (b,a) give
+    // equal contributions, so only alpha-before-beta is kept, with weight 2 -- the merge
+    // of equal terms done by the reference's spin integration (spinorbital_tensor.cxx:676-694).
+    std::vector<std::pair<int, int>> sym_int;
+    {
+        auto group_internal_count = [&](const Tensor& T, const std::map<char, int>& pos, int g) {
+            int n = 0;
+            for (char c : internal)
+                if (T.group[pos.at(c)] == g) n++;
+            return n;
+        };
+        for (int i = 0; i < nint; i++)
+            for (int j = i + 1; j < nint; j++) {
+                int gA = A.group[L.inA[internal[i]]], gB = B.group[L.inB[internal[i]]];
+                if (A.group[L.inA[internal[j]]] != gA || B.group[L.inB[internal[j]]] != gB) continue;
+                if (group_internal_count(A, L.inA, gA) != 2 || group_internal_count(B, L.inB, gB) != 2) continue;
+                sym_int.push_back({i, j});
+            }
+    }
+
+    // external letters in C order
+    std::vector<char> ext(idxC.begin(), idxC.end());
+
     for (size_t cc = 0; cc < C.cases.size(); cc++) {
         const SpinCase& scC = C.cases[cc];
         for (size_t bi = 0; bi < scC.blocks.size(); bi++) {
             const Block& bC = scC.blocks[bi];
             if (bC.size == 0) continue;
-            for (auto& sh : shuffles) {
+            // Antisymmetriser terms that only exchange C positions of equal spin and irrep
+            // compute the same product; group them by the (spin, irrep) each external letter
+            // receives, compute the product once and write it to every image.
+            struct Group {
+                std::vector<std::pair<size_t, int>> images;   // (shuffle index, sign)
+                std::vector<Term> terms;                      // built with the first shuffle
+            };
+            std::map<std::vector<int>, Group> groups;
+            std::vector<std::vector<int>> group_order;
+            for (size_t si = 0; si < shuffles.size(); si++) {
+                auto& sh = shuffles[si];
+                std::vector<int> key;
+                for (char c : ext) {
+                    int p = sh.first.count(c) ? sh.first.at(c) : L.inC[c];
+                    key.push_back(scC.spin[p]);
+                    key.push_back(bC.irrep[p]);
+                }
+                auto it = groups.find(key);
+                if (it != groups.end()) {
+                    it->second.images.push_back({si, sh.second});
+                    continue;
+                }
+                Group& G = groups[key];
+                group_order.push_back(key);
+                G.images.push_back({si, sh.second});
                 for_each_assignment(nint, 2, [&](const std::vector<int>& ispin) {
+                    double wspin = 1.0;
+                    for (auto& pr : sym_int) {
+                        if (ispin[pr.first] > ispin[pr.second]) return;
+                        if (ispin[pr.first] < ispin[pr.second]) wspin *= 2.0;
+                    }
                     // variables: 0..C.ndim-1 = C positions, then internal letters
                     std::vector<Var> vars(C.ndim + nint);
                     std::map<char, int> var_of;
@@ -613,8 +699,6 @@ Plan plan_contract(Context& ctx, double alpha, int hA, const std::string& idxA, 
                             t.B.var[q] = var_of[idxB[ordB[q]]];
                             irrB[q] = vv[t.B.var[q]].irrep;
                         }
-                        // a packed factor stores only the irrep-ordered half of its pair blocks;
-                        // the other half is reached through the pair restriction
                         t.A.blk = find_block(A, csA, irrA);
                         t.B.blk = find_block(B, csB, irrB);
                         // beta applies to every C block for which both factor blocks exist
@@ -629,22 +713,78 @@ Plan plan_contract(Context& ctx, double alpha, int hA, const std::string& idxA, 
                         if (!t.A.blk || !t.B.blk) return;
                         if (t.A.blk->size == 0 || t.B.blk->size == 0) return;
                         t.bC = &bC;
-                        t.coef = alpha * sh.second * sgA * sgB;
-                        for (int p = 0; p < C.ndim; p++) {
-                            char c = idxC[p];
-                            (void)c;
-                        }
+                        t.coef = alpha * wspin * sgA * sgB;   // shuffle sign applied per image
                         // m: C positions whose variable appears in A; n: in B
                         for (int q = 0; q < A.ndim; q++)
                             if (t.A.var[q] < C.ndim) t.mvars.push_back(t.A.var[q]);
                         for (int q = 0; q < B.ndim; q++)
                             if (t.B.var[q] < C.ndim) t.nvars.push_back(t.B.var[q]);
                         for (int i = 0; i < nint; i++) t.kvars.push_back(C.ndim + i);
+                        G.terms.push_back(std::move(t));
+                    });
+                });
+            }
+            for (auto& key : group_order) {
+                Group& G = groups[key];
+                if (G.terms.empty()) continue;
+                if (G.images.size() == 1) {
+                    // a single image: contract straight into C
+                    for (auto& t : G.terms) {
+                        t.coef *= G.images[0].second;
                         Plan part;
                         lower_gemm(ctx, t, hA, hB, hC, (int)cc, touched, part);
                         if (!part.gemms.empty()) parts.push_back(std::move(part));
-                    });
-                });
+                    }
+                    continue;
+                }
+                // several images: X[letters] = product (first shuffle), then C += sign * X per image
+                const auto& sh0 = shuffles[G.images[0].first].first;
+                const int ne = (int)ext.size();
+                std::vector<int64_t> lenX(ne), strideX(ne);
+                int64_t nX = 1;
+                for (int k = 0; k < ne; k++) {
+                    lenX[k] = ctx.spaces.n[group_space(C.group[L.inC[ext[k]]])][key[2 * k]][key[2 * k + 1]];
+                    strideX[k] = nX;
+                    nX *= lenX[k];
+                }
+                Dest dx;
+                dx.scratch = true;
+                dx.stride.assign(C.ndim, 0);
+                for (int k = 0; k < ne; k++) {
+                    int p0 = sh0.count(ext[k]) ? sh0.at(ext[k]) : L.inC[ext[k]];
+                    dx.stride[p0] = strideX[k];
+                }
+                Plan part;
+                part.scratch_elems = nX;
+                {
+                    ScaleStep z;
+                    z.tC = kScratch;
+                    z.off = 0;
+                    z.n = nX;
+                    z.beta = 0.0;
+                    part.steps.push_back({Step::SCALE, (int)part.scales.size()});
+                    part.scales.push_back(z);
+                }
+                for (auto& t : G.terms) lower_gemm(ctx, t, hA, hB, hC, (int)cc, touched, part, &dx);
+                for (auto& im : G.images) {
+                    const auto& shm = shuffles[im.first].first;
+                    SumStep s;
+                    s.tA = kScratch;
+                    s.tC = hC;
+                    s.ndim = ne;
+                    s.offA = 0;
+                    s.offC = bC.offset;
+                    s.alpha = im.second;
+                    for (int k = 0; k < ne; k++) {
+                        int p = shm.count(ext[k]) ? shm.at(ext[k]) : L.inC[ext[k]];
+                        s.len[k] = lenX[k];
+                        s.sA[k] = strideX[k];
+                        s.sC[k] = bC.stride[p];
+                    }
+                    part.steps.push_back({Step::SUM, (int)part.sums.size()});
+                    part.sums.push_back(s);
+                }
+                parts.push_back(std::move(part));
             }
         }
     }

@@ -4,6 +4,8 @@
 // captured as a CUDA graph).
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 
@@ -69,6 +71,12 @@ Solver::Solver(Context& c, const ccsd_hamiltonian& h, const ccsd_options& o) : c
         ctx.upload(tau_plan);
         ctx.upload(energy_plan);
         flops_per_iter = iter_plan.flops() + tau_plan.flops();
+        if (std::getenv("CCSD_PLAN_DUMP")) {
+            for (auto& g : iter_plan.gemms)
+                std::fprintf(stderr, "%-48s M=%-8d N=%-8d K=%-8d %.3e flop a_k=%d a_m=%d b_k=%d b_n=%d var=%dx%d\n",
+                             g.label.c_str(), g.M, g.N, g.K, g.flops(), g.a_kcontig, g.a_mcontig, g.b_kcontig,
+                             g.b_ncontig, g.nvm, g.nvn);
+        }
         return;
     }
     build_denominators();

@@ -38,6 +38,7 @@ WORKLOADS = {
     "cfg3": dict(o=32, v=256, nirrep=1, seed=3, desc="synthetic closed-shell spin-orbital CCSD, C1, o=32 v=256"),
     "cfg4": dict(o=48, v=336, nirrep=8, seed=4, desc="synthetic closed-shell spin-orbital CCSD, D2h, o=48 v=336"),
     "small": dict(o=8, v=48, nirrep=1, seed=5, desc="synthetic closed-shell spin-orbital CCSD, C1, o=8 v=48"),
+    "mid": dict(o=16, v=96, nirrep=1, seed=6, desc="synthetic closed-shell spin-orbital CCSD, C1, o=16 v=96"),
 }
 # bounded CPU sample: same occupied count, fewer virtuals
 CPU_SAMPLE = {"cfg2": (16, 64), "cfg3": (32, 80), "cfg4": (24, 80), "small": (8, 48)}
@@ -193,8 +194,49 @@ def timed_iterations(torch, ctx, s, stream, steps, warmup, profile):
     return ms, launches, prof, e, c
 
 
+def run_kernel(args):
+    """Micro-benchmark of one contraction kernel: the particle ladder
+    Z2["abij"] += 1/2 VABEF["abef"] * Tau["efij"] on filled tensors (no H build), so
+    that the first contraction launches of the process are the ladder's block GEMMs."""
+    import torch
+    import aquarius_b200 as A
+    w = WORKLOADS[args.workload]
+    stream = torch.cuda.Stream()
+    ctx = A.Context(0, stream.cuda_stream)
+    ctx.set_spaces(vrt=[w["v"]], occ=[w["o"]])
+    if args.precision == "split":
+        ctx.set_precision("split")
+    V = ctx.tensor("<ab||cd>", (2, 0), (2, 0), packed=True)
+    T = ctx.tensor("Tau", (2, 0), (0, 2))
+    Z = ctx.tensor("Z(2)", (2, 0), (0, 2))
+    V.fill(0.01)
+    T.fill(0.001)
+    ctx.set_profiling(True)
+    for _ in range(args.warmup):
+        ctx.contract(0.5, V, "abef", T, "efij", 1.0, Z, "abij")
+    ctx.synchronize()
+    ctx.profile_report()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        ctx.contract(0.5, V, "abef", T, "efij", 1.0, Z, "abij")
+    ev1.record(stream)
+    ev1.synchronize()
+    prof = ctx.profile_report()
+    ent = next(iter(prof.values()))
+    tfl = ent["flops"] / (ent["ms"] * 1e-3) / 1e12
+    print(json.dumps({"kernel": "ladder", "workload": w["desc"], "precision": args.precision,
+                      "ms_per_contraction": ev0.elapsed_time(ev1) / args.steps,
+                      "gemm_ms": ent["ms"] / args.steps, "launches_per_contraction": ent["launches"] / args.steps,
+                      "tflops": tfl, "flops_per_contraction": ent["flops"] / args.steps}), flush=True)
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--kernel", default=None, choices=[None, "ladder"],
+                    help="micro-benchmark one contraction kernel instead of the iteration")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -208,6 +250,10 @@ def main():
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.kernel:
+        if args.precision == "auto":
+            args.precision = "fp64"
+        return run_kernel(args)
 
     import torch
     import aquarius_b200 as A
