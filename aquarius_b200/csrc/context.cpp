@@ -34,12 +34,13 @@ Context::~Context() {
     for (auto& kv : split_cache) {
         cudaFree(kv.second.data);
         cudaFree(kv.second.scale);
+        cudaFree(kv.second.rowmax);
     }
-    cudaFree(split_ws.a.data);
-    cudaFree(split_ws.a.scale);
-    cudaFree(split_ws.b.data);
-    cudaFree(split_ws.b.scale);
-    cudaFree(split_ws.rowmax);
+    for (auto* w : {&split_ws.a, &split_ws.b}) {
+        cudaFree(w->data);
+        cudaFree(w->scale);
+        cudaFree(w->rowmax);
+    }
     for (auto& kv : tensors) cudaFree(kv.second->data);
     cudaFree(d_scalar);
     for (auto& p : pending) {
@@ -203,12 +204,15 @@ void Context::destroy_tensor(int h) {
             ++it;
         }
     }
+    // drop cached slices of this tensor
     for (auto it = split_cache.begin(); it != split_cache.end();) {
-        // cache keys are opaque; drop everything conservatively
-        dfree(it->second.data, 0);
-        dfree(it->second.scale, 0);
-        device_bytes -= it->second.bytes;
-        it = split_cache.erase(it);
+        if (split_owner[it->first] == h) {
+            free_sliced(it->second);
+            split_owner.erase(it->first);
+            it = split_cache.erase(it);
+        } else {
+            ++it;
+        }
     }
     constant_tensors.erase(std::remove(constant_tensors.begin(), constant_tensors.end(), h), constant_tensors.end());
     dfree(T.data, std::max<int64_t>(T.total, 1) * sizeof(double));
@@ -259,6 +263,10 @@ void Context::upload(Plan& p) {
     }
     // tables are uploaded from pageable host memory; make sure the copies have been
     // staged before the host vectors could change
+    if (precision == CCSD_PREC_SPLIT && !p.split_reserved && (host_only || kern::split_supported())) {
+        reserve_split(p);
+        p.split_reserved = true;
+    }
     if (any && !host_only) CCSD_CUDA(cudaStreamSynchronize(stream));
 }
 

@@ -120,7 +120,8 @@ struct GemmStep {
     bool a_mcontig = false, a_kcontig = false, b_kcontig = false, b_ncontig = false;
     double flops() const { return 2.0 * M * N * (double)K; }
     std::string label;                 // statement this block contraction came from
-    int64_t split_cache = -1;          // key of cached A slices (constant operand)
+    int64_t split_cache_a = -1;        // keys of cached slices of constant operands
+    int64_t split_cache_b = -1;
 };
 
 // C[perm] += alpha * A  over one block (strided, up to 8 dims)
@@ -161,6 +162,7 @@ constexpr int kScratch = -1;
 struct Plan {
     int64_t scratch_elems = 0;         // doubles of scratch the steps need (products X)
     double* scratch = nullptr;         // allocated at upload
+    bool split_reserved = false;       // split-path workspace sized for this plan
     std::vector<Step> steps;
     std::vector<GemmStep> gemms;
     std::vector<SumStep> sums;
@@ -206,7 +208,13 @@ public:
     double* d_scalar = nullptr;        // device accumulator for dots
     kern::SplitWorkspace split_ws;     // scratch for split-BF16 GEMMs
     std::map<int64_t, kern::SlicedOperand> split_cache;   // sliced constant operands
+    std::map<int64_t, int> split_owner;                    // cache key -> tensor handle
     int64_t split_cache_next = 1;
+    kern::SlicedOperand ws_view[2];                        // workspace views of the current call
+    kern::SlicedOperand alloc_sliced(int rows, int K);
+    void free_sliced(kern::SlicedOperand& s);
+    void ensure_ws(kern::SlicedOperand& w, int rows, int K);
+    void reserve_split(const Plan& p);
     std::map<std::string, std::unique_ptr<Plan>> plan_cache;
 
     // optional per-statement timing of GEMM steps with CUDA events on the stream

@@ -30,27 +30,31 @@ void gemm_fp64(const GemmArgs& g, cudaStream_t s);
 // row scale 2^e per row.  rows is padded to a multiple of 128, kpad to a multiple of 64.
 struct SlicedOperand {
     uint16_t* data = nullptr;   // [nslices][rows][kpad]
-    double* scale = nullptr;    // [rows]  value = scale * (s0 + s1 + s2 ...)
+    double* scale = nullptr;    // [rows]  value = scale * (s1 + s2 + s3)
+    double* rowmax = nullptr;   // [rows]  scratch of the slicing pass
     int rows = 0, kpad = 0, nslices = 0;
     int64_t bytes = 0;
 };
 
 struct SplitWorkspace {
     SlicedOperand a, b;          // per-call slices of non-constant operands
-    double* rowmax = nullptr;
-    int64_t rowmax_n = 0;
 };
 
-// number of bf16 slices used when the caller does not say otherwise
+// number of bf16 slices of the split path
 constexpr int kDefaultSlices = 3;
+int split_rows_pad(int rows);
+int split_k_pad(int k);
 
-// slice rows of X(r,k) = X[R[r] + Kt[k]] (r < nrows, k < K) into `out` (allocated by caller)
+// slice rows of X(r,k) = X[R[r] + Kt[k]] (r < nrows, k < K) into `out` (allocated by caller
+// with out.rows >= nrows padded, out.kpad >= K padded)
 void slice_rows(const double* X, const int64_t* R, const int64_t* Kt, int nrows, int K, bool kcontig,
                 int nslices, SlicedOperand& out, cudaStream_t s);
 // tcgen05 GEMM over slices; epilogue scatters into C like gemm_fp64
 void gemm_split(const SlicedOperand& a, const SlicedOperand& b, int M, int N, int K,
                 const GemmArgs& g, cudaStream_t s);
 bool split_supported();
+// nonzero if a split-GEMM wait expired (1..4 = which wait); reset clears it
+int split_error(bool reset);
 
 // ---- elementwise / reductions ----------------------------------------------------
 struct StridedArgs {

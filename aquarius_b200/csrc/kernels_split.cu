@@ -1,18 +1,548 @@
-// Split-BF16 (Ozaki-style) contraction path on tcgen05 tensor cores.
+// Split-BF16 (Ozaki-style) contraction path on the sm_100a tensor cores.
+//
+// Each FP64 operand row x (a row of A(m,:) or a column of B(:,n), gathered through
+// the planner's offset tables) is written as
+//     x = 2^(e-6) * (s1 + s2 + s3),   2^e <= max|x| < 2^(e+1),
+// with s1 an integer in [-128,128], s2 = integer/2^8, s3 = integer/2^16, all exact in
+// BF16 (round-to-nearest at each step, so the truncation error is unbiased and below
+// 2^-23 of the row maximum).  The tcgen05 GEMM keeps two FP32 accumulators in TMEM:
+//     L2  = sum_k s1a*s1b                          (products <= 2^14: a chunk of 1024 k
+//                                                     sums exactly in FP32)
+//     L34 = sum_k (s1a*s2b + s2a*s1b + s1a*s3b + s2a*s2b + s3a*s1b)   (2^-8 smaller)
+// and every 1024-k chunk is drained into FP64 registers, so the leading term is exact
+// and the FP32 rounding of the rest sits ~2^-32 below the result.  The dropped
+// products (s2*s3, s3*s2, s3*s3) are below 2^-23 of the row maxima.
+//
+// Kernel structure (one 128x128 output tile per CTA, 320 threads):
+//   warp 0      TMA producer: 3 A-slice + 3 B-slice tiles of 128x64 BF16 per stage
+//               (128-byte swizzle), 2 stages of 96 KiB, mbarrier full/empty ring;
+//   warp 1      TMEM allocation (512 columns) and the single-thread MMA issuer:
+//               tcgen05.mma kind::f16 M128 N128 K16, 6 MMAs per k-step, commit to
+//               release smem stages and to publish a finished chunk;
+//   warps 2..9  epilogue: TMEM accumulator sets are double-buffered across chunks;
+//               each warp drains its 32 lanes x 64 columns into FP64 registers and
+//               scatters the scaled result into the destination through the planner's
+//               offset tables at the end.
+// Every mbarrier wait is bounded (about 2 s); on expiry the kernel records an error
+// code, stops issuing work and returns after releasing its TMEM.
+#include <cstdint>
+#include <cstdio>
+#include <map>
+#include <mutex>
 #include <stdexcept>
+#include <string>
+
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
 #include "kernels.hpp"
 
 namespace ccsd {
 namespace kern {
 
-bool split_supported() { return false; }
+extern int64_t g_launches;
+double* partial_buffer(cudaStream_t s);
 
-void slice_rows(const double*, const int64_t*, const int64_t*, int, int, bool, int, SlicedOperand&, cudaStream_t) {
-    throw std::runtime_error("split path not built");
+namespace split {
+
+constexpr int BM = 128, BN = 128, BK = 64;
+constexpr int NSLICE = 3;
+constexpr int STAGES = 2;
+constexpr int CHUNK_KB = 16;                       // 16 x 64 = 1024 k per exact FP32 chunk
+constexpr int EPI_WARPS = 8;
+constexpr int THREADS = 32 * (2 + EPI_WARPS);
+constexpr int TILE_A_BYTES = BM * BK * 2;           // 16 KiB
+constexpr int TILE_B_BYTES = BN * BK * 2;           // 16 KiB
+constexpr int STAGE_BYTES = NSLICE * (TILE_A_BYTES + TILE_B_BYTES);   // 96 KiB
+constexpr int TMEM_COLS = 512;                      // 2 x (L2: 128 + L34: 128)
+constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES + 256;
+constexpr long long WAIT_CYCLES = 4000000000ll;     // ~2 s at 1.9 GHz
+
+// instruction descriptor: D=F32, A=B=BF16, K-major both, N=128, M=128
+constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(BM >> 4) << 24);
+
+struct Params {
+    int M, N, K;
+    int Mp, Np, Kp;
+    int tiles_n;
+    double alpha;
+    const double* scaleA;
+    const double* scaleB;
+    double* C;
+    const int64_t* Cm0;
+    const int64_t* Cm1;
+    const int64_t* Cn0;
+    const int64_t* Cn1;
+    int nvm, nvn;
+    double vsign[4];
+    int* err;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
 }
 
-void gemm_split(const SlicedOperand&, const SlicedOperand&, int, int, int, const GemmArgs&, cudaStream_t) {
-    throw std::runtime_error("split path not built");
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// bounded wait; false on expiry (the error code is recorded and the abort flag set)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort_flag, int* err,
+                                          int code) {
+    if (mbar_try(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (true) {
+        if (mbar_try(bar, parity)) return true;
+        if (*abort_flag) return false;
+        if (clock64() - t0 > WAIT_CYCLES) {
+            *abort_flag = 1;
+            atomicCAS(err, 0, code);
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_u32(dst)),
+        "l"(map), "r"(x), "r"(y), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// K-major, 128-byte swizzled tile descriptor (rows of 128 B, 8-row groups 1024 B apart)
+__device__ __forceinline__ uint64_t sdesc(const void* p) {
+    uint64_t d = 0;
+    d |= (uint64_t)((smem_u32(p) >> 4) & 0x3FFF);
+    d |= (uint64_t)1 << 16;                 // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)(1024 >> 4) << 32;       // stride byte offset
+    d |= (uint64_t)1 << 46;                 // descriptor version (sm_100)
+    d |= (uint64_t)2 << 61;                 // SWIZZLE_128B
+    return d;
+}
+
+__device__ __forceinline__ void umma(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(dtmem),
+        "l"(a), "l"(b), "r"(IDESC), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__global__ void __launch_bounds__(THREADS, 1)
+    split_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params p) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+    uint8_t* stages = smem;
+    uint64_t* bars = (uint64_t*)(smem + (size_t)STAGES * STAGE_BYTES);
+    uint64_t* full = bars;          // [STAGES]
+    uint64_t* empty = bars + 2;     // [STAGES]
+    uint64_t* tfull = bars + 4;     // [2]
+    uint64_t* tempty = bars + 6;    // [2]
+    uint32_t* tmem_slot = (uint32_t*)(bars + 8);
+    volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int tile = blockIdx.x;
+    const int tm = tile / p.tiles_n, tn = tile % p.tiles_n;
+    const int m0 = tm * BM, n0 = tn * BN;
+    const int nkb = p.Kp / BK;
+    const int nchunks = (nkb + CHUNK_KB - 1) / CHUNK_KB;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; s++) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], 1);
+        }
+        for (int b = 0; b < 2; b++) {
+            mbar_init(&tfull[b], 1);
+            mbar_init(&tempty[b], EPI_WARPS);
+        }
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // ---------------- TMA producer ----------------
+            for (int kb = 0; kb < nkb && !*abort_flag; kb++) {
+                const int s = kb % STAGES;
+                if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1, abort_flag, p.err, 1)) break;
+                mbar_expect_tx(&full[s], STAGE_BYTES);
+                uint8_t* base = stages + (size_t)s * STAGE_BYTES;
+                for (int i = 0; i < NSLICE; i++)
+                    tma_load_2d(base + i * TILE_A_BYTES, &tmA, kb * BK, i * p.Mp + m0, &full[s]);
+                for (int i = 0; i < NSLICE; i++)
+                    tma_load_2d(base + NSLICE * TILE_A_BYTES + i * TILE_B_BYTES, &tmB, kb * BK, i * p.Np + n0,
+                                &full[s]);
+            }
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // ---------------- MMA issuer ----------------
+            int kb = 0;
+            for (int c = 0; c < nchunks && !*abort_flag; c++) {
+                const int b = c & 1;
+                if (c >= 2 && !mbar_wait(&tempty[b], ((c >> 1) - 1) & 1, abort_flag, p.err, 2)) break;
+                tc_fence_after();
+                const uint32_t dL2 = tmem + b * 256, dL34 = tmem + b * 256 + 128;
+                const int kb_end = min(nkb, (c + 1) * CHUNK_KB);
+                bool first = true;
+                bool ok = true;
+                for (; kb < kb_end; kb++) {
+                    const int s = kb % STAGES;
+                    if (!mbar_wait(&full[s], (kb / STAGES) & 1, abort_flag, p.err, 3)) {
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint8_t* base = stages + (size_t)s * STAGE_BYTES;
+                    const uint64_t a0 = sdesc(base), a1 = sdesc(base + TILE_A_BYTES),
+                                   a2 = sdesc(base + 2 * TILE_A_BYTES);
+                    const uint8_t* bb = base + NSLICE * TILE_A_BYTES;
+                    const uint64_t b0 = sdesc(bb), b1 = sdesc(bb + TILE_B_BYTES), b2 = sdesc(bb + 2 * TILE_B_BYTES);
+#pragma unroll
+                    for (int kk = 0; kk < BK / 16; kk++) {
+                        const uint64_t o = (uint64_t)(kk * 32) >> 4;   // 16 bf16 = 32 bytes along K
+                        const uint32_t acc = first ? 0u : 1u;
+                        umma(dL2, a0 + o, b0 + o, acc);
+                        umma(dL34, a0 + o, b1 + o, acc);
+                        umma(dL34, a1 + o, b0 + o, 1u);
+                        umma(dL34, a0 + o, b2 + o, 1u);
+                        umma(dL34, a1 + o, b1 + o, 1u);
+                        umma(dL34, a2 + o, b0 + o, 1u);
+                        first = false;
+                    }
+                    umma_commit(&empty[s]);
+                }
+                if (!ok) break;
+                umma_commit(&tfull[b]);
+            }
+        }
+    } else {
+        // ---------------- epilogue ----------------
+        const int ew = warp - 2;
+        const int q = warp & 3;          // TMEM lane quadrant this warp may access
+        const int h = ew >> 2;           // column half
+        double acc[64];
+#pragma unroll
+        for (int j = 0; j < 64; j++) acc[j] = 0.0;
+        bool ok = true;
+        for (int c = 0; c < nchunks; c++) {
+            const int b = c & 1;
+            if (!mbar_wait(&tfull[b], (c >> 1) & 1, abort_flag, p.err, 4)) {
+                ok = false;
+                break;
+            }
+            tc_fence_after();
+            const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + b * 256 + h * 64;
+#pragma unroll
+            for (int j4 = 0; j4 < 4; j4++) {
+                uint32_t r2[16], r34[16];
+                tmem_ld16(base + j4 * 16, r2);
+                tmem_ld16(base + 128 + j4 * 16, r34);
+                tmem_wait_ld();
+#pragma unroll
+                for (int t = 0; t < 16; t++)
+                    acc[j4 * 16 + t] += (double)__uint_as_float(r2[t]) + (double)__uint_as_float(r34[t]);
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&tempty[b]);
+        }
+        if (ok) {
+            const int m = m0 + q * 32 + lane;
+            if (m < p.M) {
+                const double sa = p.alpha * p.scaleA[m];
+                const int64_t cm0 = p.Cm0[m];
+                const int64_t cm1 = p.nvm > 1 ? p.Cm1[m] : 0;
+#pragma unroll
+                for (int j = 0; j < 64; j++) {
+                    const int n = n0 + h * 64 + j;
+                    if (n < p.N) {
+                        const double v = sa * p.scaleB[n] * acc[j];
+                        const int64_t cn0 = p.Cn0[n];
+                        p.C[cm0 + cn0] += p.vsign[0] * v;
+                        if (p.nvn > 1) p.C[cm0 + p.Cn1[n]] += p.vsign[1] * v;
+                        if (p.nvm > 1) {
+                            p.C[cm1 + cn0] += p.vsign[p.nvn] * v;
+                            if (p.nvn > 1) p.C[cm1 + p.Cn1[n]] += p.vsign[3] * v;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 1) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// slicing: two passes over 32-row x 64-k tiles of the gathered operand
+// ---------------------------------------------------------------------------
+constexpr int SR = 32, SK = 64, STHREADS = 256;
+
+template <bool KC>
+__device__ __forceinline__ void load_tile(const double* __restrict__ X, const int64_t* __restrict__ R,
+                                          const int64_t* __restrict__ Kt, int nrows, int K, int r0, int k0,
+                                          double (*tile)[SK + 1], int64_t* sR, int64_t* sK) {
+    for (int i = threadIdx.x; i < SR; i += STHREADS) sR[i] = (r0 + i < nrows) ? R[r0 + i] : -1;
+    for (int i = threadIdx.x; i < SK; i += STHREADS) sK[i] = (k0 + i < K) ? Kt[k0 + i] : -1;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < (SR * SK) / STHREADS; i++) {
+        const int e = threadIdx.x + i * STHREADS;
+        int r, k;
+        if (KC) {
+            k = e % SK;
+            r = e / SK;
+        } else {
+            r = e % SR;
+            k = e / SR;
+        }
+        double v = 0.0;
+        if (sR[r] >= 0 && sK[k] >= 0) v = X[sR[r] + sK[k]];
+        tile[r][k] = v;
+    }
+    __syncthreads();
+}
+
+template <bool KC>
+__global__ void __launch_bounds__(STHREADS) rowmax_kernel(const double* __restrict__ X, const int64_t* __restrict__ R,
+                                                          const int64_t* __restrict__ Kt, int nrows, int K,
+                                                          unsigned long long* rowmax) {
+    __shared__ double tile[SR][SK + 1];
+    __shared__ int64_t sR[SR], sK[SK];
+    const int r0 = blockIdx.y * SR, k0 = blockIdx.x * SK;
+    load_tile<KC>(X, R, Kt, nrows, K, r0, k0, tile, sR, sK);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int r = warp; r < SR; r += STHREADS / 32) {
+        double m = fmax(fabs(tile[r][lane]), fabs(tile[r][lane + 32]));
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        if (lane == 0 && r0 + r < nrows && m > 0.0) atomicMax(&rowmax[r0 + r], (unsigned long long)__double_as_longlong(m));
+    }
+}
+
+__device__ __forceinline__ unsigned short bf16_bits(double v) {
+    __nv_bfloat16 b = __float2bfloat16_rn((float)v);
+    return *reinterpret_cast<unsigned short*>(&b);
+}
+
+template <bool KC>
+__global__ void __launch_bounds__(STHREADS)
+    slice_kernel(const double* __restrict__ X, const int64_t* __restrict__ R, const int64_t* __restrict__ Kt, int nrows,
+                 int K, const unsigned long long* __restrict__ rowmax, int rows_p, int kpad,
+                 unsigned short* __restrict__ out, double* __restrict__ scale) {
+    __shared__ double tile[SR][SK + 1];
+    __shared__ int64_t sR[SR], sK[SK];
+    const int r0 = blockIdx.y * SR, k0 = blockIdx.x * SK;
+    load_tile<KC>(X, R, Kt, nrows, K, r0, k0, tile, sR, sK);
+    const size_t plane = (size_t)rows_p * kpad;
+#pragma unroll
+    for (int i = 0; i < (SR * SK) / STHREADS; i++) {
+        const int e = threadIdx.x + i * STHREADS;
+        const int k = e % SK, r = e / SK;
+        const int row = r0 + r;
+        double mx = row < nrows ? __longlong_as_double((long long)rowmax[row]) : 0.0;
+        unsigned short b1 = 0, b2 = 0, b3 = 0;
+        if (mx > 0.0) {
+            const int ex = ilogb(mx);                // mx in [2^ex, 2^(ex+1))
+            const double y = ldexp(tile[r][k], 6 - ex);   // |y| < 128
+            const double s1 = rint(y);
+            const double y2 = (y - s1) * 256.0;
+            const double s2 = rint(y2);
+            const double y3 = (y2 - s2) * 256.0;
+            const double s3 = rint(y3);
+            b1 = bf16_bits(s1);
+            b2 = bf16_bits(s2 * 0.00390625);
+            b3 = bf16_bits(s3 * 1.52587890625e-05);
+        }
+        const size_t o = (size_t)row * kpad + (k0 + k);
+        out[o] = b1;
+        out[plane + o] = b2;
+        out[2 * plane + o] = b3;
+        if (blockIdx.x == 0 && k == 0) scale[row] = mx > 0.0 ? ldexp(1.0, ilogb(mx) - 6) : 0.0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)f;
+    });
+    return fn;
+}
+
+void make_map(CUtensorMap* map, const uint16_t* base, int rows_total, int kpad) {
+    EncodeTiledFn enc = encode_fn();
+    if (!enc) throw std::runtime_error("cuTensorMapEncodeTiled is not available");
+    cuuint64_t dims[2] = {(cuuint64_t)kpad, (cuuint64_t)rows_total};
+    cuuint64_t strides[1] = {(cuuint64_t)kpad * 2};
+    cuuint32_t box[2] = {BK, 128};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)base, dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+}
+
+int* error_flag() {
+    static std::mutex mu;
+    static std::map<int, int*> flags;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = flags.find(dev);
+    if (it != flags.end()) return it->second;
+    int* f = nullptr;
+    cudaMalloc(&f, sizeof(int));
+    cudaMemset(f, 0, sizeof(int));
+    flags[dev] = f;
+    return f;
+}
+
+}  // namespace split
+
+bool split_supported() {
+    static int cached = -1;
+    if (cached < 0) {
+        int dev = 0;
+        cudaDeviceProp prop;
+        cached = (cudaGetDevice(&dev) == cudaSuccess && cudaGetDeviceProperties(&prop, dev) == cudaSuccess &&
+                  prop.major == 10 && split::encode_fn() != nullptr)
+                     ? 1
+                     : 0;
+    }
+    return cached == 1;
+}
+
+int split_rows_pad(int rows) { return (rows + split::BM - 1) / split::BM * split::BM; }
+int split_k_pad(int k) { return (k + split::BK - 1) / split::BK * split::BK; }
+
+void slice_rows(const double* X, const int64_t* R, const int64_t* Kt, int nrows, int K, bool kcontig, int nslices,
+                SlicedOperand& out, cudaStream_t s) {
+    using namespace split;
+    if (nslices != NSLICE) throw std::runtime_error("only 3 slices are built");
+    unsigned long long* rowmax = reinterpret_cast<unsigned long long*>(out.rowmax);
+    cudaMemsetAsync(rowmax, 0, sizeof(double) * out.rows, s);
+    dim3 grid(out.kpad / SK, out.rows / SR);
+    if (kcontig) rowmax_kernel<true><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax);
+    else rowmax_kernel<false><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax);
+    if (kcontig)
+        slice_kernel<true><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax, out.rows, out.kpad, out.data, out.scale);
+    else
+        slice_kernel<false><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax, out.rows, out.kpad, out.data, out.scale);
+    g_launches += 2;
+}
+
+void gemm_split(const SlicedOperand& a, const SlicedOperand& b, int M, int N, int K, const GemmArgs& g,
+                cudaStream_t s) {
+    using namespace split;
+    (void)K;
+    static bool configured[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (!configured[dev]) {
+        cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
+        configured[dev] = true;
+    }
+    CUtensorMap ma, mb;
+    make_map(&ma, a.data, NSLICE * a.rows, a.kpad);
+    make_map(&mb, b.data, NSLICE * b.rows, b.kpad);
+    Params p;
+    p.M = M;
+    p.N = N;
+    p.K = K;
+    p.Mp = a.rows;
+    p.Np = b.rows;
+    p.Kp = a.kpad;
+    p.tiles_n = b.rows / BN;
+    p.alpha = g.alpha;
+    p.scaleA = a.scale;
+    p.scaleB = b.scale;
+    p.C = g.C;
+    p.Cm0 = g.Cm[0];
+    p.Cm1 = g.Cm[1];
+    p.Cn0 = g.Cn[0];
+    p.Cn1 = g.Cn[1];
+    p.nvm = g.nvm;
+    p.nvn = g.nvn;
+    for (int i = 0; i < 4; i++) p.vsign[i] = g.vsign[i];
+    p.err = error_flag();
+    const int tiles = (a.rows / BM) * p.tiles_n;
+    split_gemm_kernel<<<tiles, THREADS, SMEM_BYTES, s>>>(ma, mb, p);
+    g_launches++;
+}
+
+int split_error(bool reset) {
+    int* f = split::error_flag();
+    int h = 0;
+    cudaMemcpy(&h, f, sizeof(int), cudaMemcpyDeviceToHost);
+    if (reset && h) cudaMemset(f, 0, sizeof(int));
+    return h;
 }
 
 }  // namespace kern

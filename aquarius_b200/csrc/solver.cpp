@@ -412,6 +412,10 @@ void Solver::read_status() {
     CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
     energy = h_red[0];
     conv = h_red[1];
+    if (opts.precision == CCSD_PREC_SPLIT) {
+        int e = kern::split_error(true);
+        if (e) throw Error(CCSD_ERR_TIMEOUT, "split GEMM wait " + std::to_string(e) + " expired");
+    }
     if (opts.diis_order > 1 && h_state[3] != 0)
         throw Error(CCSD_ERR_SINGULAR, "DIIS: singular error matrix after the eps retry");
     if (!std::isfinite(energy) || !std::isfinite(conv)) throw Error(CCSD_DIVERGED, "NaN/Inf in energy or residual");

@@ -1,12 +1,119 @@
-// Host side of the split-BF16 contraction path: slicing of operands (cached for the
-// constant H blocks) and the tcgen05 GEMM launch.
+// Host side of the split-BF16 contraction path: which block contractions use it, slicing
+// of their operands (cached for the constant H blocks, per call for the amplitudes and
+// intermediates), and the tcgen05 GEMM launch.
+#include <algorithm>
+#include <cstdlib>
+
 #include "engine.hpp"
 
 namespace ccsd {
 
+namespace {
+
+// Small contractions stay on the FP64 tensor-core kernel: a 128x128 tile would be mostly
+// padding and the slicing passes would cost more than the product.
+// CCSD_SPLIT_ALL=1 routes every contraction through the split kernel (coverage tests).
+bool use_split(const GemmStep& g) {
+    static const bool all = [] {
+        const char* e = std::getenv("CCSD_SPLIT_ALL");
+        return e && e[0] == '1';
+    }();
+    if (all) return g.M > 0 && g.N > 0 && g.K > 0;
+    return g.M >= 64 && g.N >= 64 && g.K >= 256 && g.flops() >= 5e8;
+}
+
+}  // namespace
+
+kern::SlicedOperand Context::alloc_sliced(int rows, int K) {
+    kern::SlicedOperand s;
+    s.rows = kern::split_rows_pad(rows);
+    s.kpad = kern::split_k_pad(K);
+    s.nslices = kern::kDefaultSlices;
+    const int64_t nd = (int64_t)s.nslices * s.rows * s.kpad;
+    s.data = (uint16_t*)dmalloc(nd * sizeof(uint16_t));
+    s.scale = (double*)dmalloc(s.rows * sizeof(double));
+    s.rowmax = (double*)dmalloc(s.rows * sizeof(double));
+    s.bytes = nd * (int64_t)sizeof(uint16_t) + 2 * (int64_t)s.rows * (int64_t)sizeof(double);
+    return s;
+}
+
+void Context::free_sliced(kern::SlicedOperand& s) {
+    const int64_t nd = (int64_t)s.nslices * s.rows * s.kpad;
+    dfree(s.data, nd * sizeof(uint16_t));
+    dfree(s.scale, s.rows * sizeof(double));
+    dfree(s.rowmax, s.rows * sizeof(double));
+    s = kern::SlicedOperand();
+}
+
+// make the per-call workspace hold a rows x K operand (never shrinks)
+void Context::ensure_ws(kern::SlicedOperand& w, int rows, int K) {
+    const int rp = kern::split_rows_pad(rows), kp = kern::split_k_pad(K);
+    if (w.data && (int64_t)w.rows * w.kpad >= (int64_t)rp * kp && w.rows >= rp) {
+        return;
+    }
+    int keep_rows = std::max(rp, w.rows);
+    int64_t keep_elems = std::max<int64_t>((int64_t)rp * kp, (int64_t)w.rows * w.kpad);
+    if (w.data) free_sliced(w);
+    // capacity is tracked in elements; rows/kpad are set per call
+    w = alloc_sliced(keep_rows, (int)std::min<int64_t>((keep_elems + keep_rows - 1) / keep_rows, INT32_MAX));
+}
+
+// reserve workspace for every split contraction of a plan (called before any capture)
+void Context::reserve_split(const Plan& p) {
+    if (host_only) {
+        int64_t need_a = 0, need_b = 0, rows_a = 0, rows_b = 0;
+        for (auto& g : p.gemms) {
+            if (!use_split(g)) continue;
+            int64_t ea = (int64_t)kern::split_rows_pad(g.M) * kern::split_k_pad(g.K);
+            int64_t eb = (int64_t)kern::split_rows_pad(g.N) * kern::split_k_pad(g.K);
+            if (!is_constant(g.tA)) need_a = std::max(need_a, ea), rows_a = std::max<int64_t>(rows_a, g.M);
+            else dmalloc(3 * ea * 2);
+            if (!is_constant(g.tB)) need_b = std::max(need_b, eb), rows_b = std::max<int64_t>(rows_b, g.N);
+            else dmalloc(3 * eb * 2);
+        }
+        dmalloc(3 * need_a * 2 + 16 * rows_a + 3 * need_b * 2 + 16 * rows_b + 1);
+        return;
+    }
+    for (auto& g : p.gemms) {
+        if (!use_split(g)) continue;
+        if (!is_constant(g.tA)) ensure_ws(split_ws.a, g.M, g.K);
+        if (!is_constant(g.tB)) ensure_ws(split_ws.b, g.N, g.K);
+    }
+}
+
 void Context::run_split_gemm(GemmStep& g, kern::GemmArgs& a) {
-    (void)g;
-    kern::gemm_fp64(a, stream);
+    if (!use_split(g)) {
+        kern::gemm_fp64(a, stream);
+        return;
+    }
+    const int ns = kern::kDefaultSlices;
+    auto prepare = [&](bool is_a, int64_t& key, kern::SlicedOperand& ws) -> kern::SlicedOperand* {
+        const int h = is_a ? g.tA : g.tB;
+        const int rows = is_a ? g.M : g.N;
+        const double* X = is_a ? a.A : a.B;
+        const int64_t* R = is_a ? a.Am : a.Bn;
+        const int64_t* Kt = is_a ? a.Ak : a.Bk;
+        const bool kc = is_a ? a.a_kcontig : a.b_kcontig;
+        if (h != kScratch && is_constant(h)) {
+            if (key < 0) {
+                key = split_cache_next++;
+                split_cache[key] = alloc_sliced(rows, g.K);
+                split_owner[key] = h;
+                kern::slice_rows(X, R, Kt, rows, g.K, kc, ns, split_cache[key], stream);
+            }
+            return &split_cache[key];
+        }
+        ensure_ws(ws, rows, g.K);
+        kern::SlicedOperand view = ws;
+        view.rows = kern::split_rows_pad(rows);
+        view.kpad = kern::split_k_pad(g.K);
+        ws_view[is_a ? 0 : 1] = view;
+        kern::slice_rows(X, R, Kt, rows, g.K, kc, ns, ws_view[is_a ? 0 : 1], stream);
+        return &ws_view[is_a ? 0 : 1];
+    };
+    kern::SlicedOperand* sa = prepare(true, g.split_cache_a, split_ws.a);
+    kern::SlicedOperand* sb = prepare(false, g.split_cache_b, split_ws.b);
+    kern::gemm_split(*sa, *sb, g.M, g.N, g.K, a, stream);
 }
 
 }  // namespace ccsd
