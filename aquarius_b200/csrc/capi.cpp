@@ -285,12 +285,36 @@ int ccsd_tensor_block_size(ccsd_ctx ctx, ccsd_tensor t, const int alpha[4], cons
     });
 }
 
+// storage offset (relative to the block) of every element of a block in first-index-fastest
+// order; the identity for ordinary blocks, a permutation for views
+static std::vector<int64_t> block_order(const Block& b) {
+    std::vector<int64_t> off(b.size);
+    const int nd = (int)b.len.size();
+    for (int64_t l = 0; l < b.size; l++) {
+        int64_t r = l, o = 0;
+        for (int p = 0; p < nd; p++) {
+            int64_t x = r % b.len[p];
+            r /= b.len[p];
+            o += x * b.stride[p];
+        }
+        off[l] = o;
+    }
+    return off;
+}
+
 int ccsd_tensor_write_block(ccsd_ctx ctx, ccsd_tensor t, const int alpha[4], const int* irreps, const double* host) {
     return guarded(ctx, [&] {
         Context* c = from_handle(ctx);
         Tensor& T = c->tensor(t);
         int cs;
         const Block& b = block_at(T, alpha, irreps, cs);
+        if (T.view_of) {
+            std::vector<int64_t> ord = block_order(b);
+            std::vector<double> buf(b.size);
+            for (int64_t l = 0; l < b.size; l++) buf[ord[l]] = host[l];
+            CCSD_CUDA(cudaMemcpy(T.data + b.offset, buf.data(), b.size * sizeof(double), cudaMemcpyHostToDevice));
+            return;
+        }
         CCSD_CUDA(cudaMemcpyAsync(T.data + b.offset, host, b.size * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         CCSD_CUDA(cudaStreamSynchronize(c->stream));
     });
@@ -302,6 +326,14 @@ int ccsd_tensor_read_block(ccsd_ctx ctx, ccsd_tensor t, const int alpha[4], cons
         Tensor& T = c->tensor(t);
         int cs;
         const Block& b = block_at(T, alpha, irreps, cs);
+        CCSD_CUDA(cudaStreamSynchronize(c->stream));
+        if (T.view_of) {
+            std::vector<int64_t> ord = block_order(b);
+            std::vector<double> buf(b.size);
+            CCSD_CUDA(cudaMemcpy(buf.data(), T.data + b.offset, b.size * sizeof(double), cudaMemcpyDeviceToHost));
+            for (int64_t l = 0; l < b.size; l++) host[l] = buf[ord[l]];
+            return;
+        }
         CCSD_CUDA(cudaMemcpyAsync(host, T.data + b.offset, b.size * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         CCSD_CUDA(cudaStreamSynchronize(c->stream));
     });
@@ -489,6 +521,7 @@ int ccsd_weight(ccsd_ctx ctx, ccsd_tensor A, const double* dvrt_a, const double*
             for (auto& b : sc.blocks) {
                 if (b.size == 0) continue;
                 if (!b.pairs.empty()) throw Error(CCSD_ERR_UNSUPPORTED, "weight of a packed tensor");
+                if (T.view_of) throw Error(CCSD_ERR_UNSUPPORTED, "weight of a view tensor");
                 kern::WeightArgs w;
                 w.ndim = T.ndim;
                 w.total = b.size;
@@ -520,8 +553,9 @@ int ccsd_hamiltonian_from_factor(ccsd_ctx ctx, int naux, const double* B, const 
 int ccsd_hamiltonian_destroy(ccsd_ctx ctx, ccsd_hamiltonian* H) {
     return guarded(ctx, [&] {
         Context* c = from_handle(ctx);
-        for (ccsd_tensor* t : {&H->fAI, &H->fME, &H->fAE, &H->fMI, &H->VMNIJ, &H->VAMIJ, &H->VMNEJ, &H->VABIJ,
-                               &H->VMNEF, &H->VAMEI, &H->VAMEF, &H->VABEJ, &H->VABEF}) {
+        // views first, then the tensors they alias
+        for (ccsd_tensor* t : {&H->VMNEJ, &H->VABIJ, &H->VABEJ, &H->fAI, &H->fME, &H->fAE, &H->fMI, &H->VMNIJ,
+                               &H->VAMIJ, &H->VMNEF, &H->VAMEI, &H->VAMEF, &H->VABEF}) {
             if (*t && c->tensors.count(*t)) c->destroy_tensor(*t);
             *t = 0;
         }

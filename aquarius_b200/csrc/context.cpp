@@ -215,8 +215,66 @@ void Context::destroy_tensor(int h) {
         }
     }
     constant_tensors.erase(std::remove(constant_tensors.begin(), constant_tensors.end(), h), constant_tensors.end());
-    dfree(T.data, std::max<int64_t>(T.total, 1) * sizeof(double));
+    for (auto& kv : tensors)
+        if (kv.second->view_of == h && kv.first != h)
+            throw Error(CCSD_ERR_ARG, "tensor " + T.name + " still has views (" + kv.second->name + ")");
+    if (!T.view_of) dfree(T.data, std::max<int64_t>(T.total, 1) * sizeof(double));
     tensors.erase(h);
+}
+
+int Context::create_view(const std::string& name, int hb, const int nout[2], const int nin[2], const int* perm) {
+    Tensor& Bt = tensor(hb);
+    if (Bt.view_of) throw Error(CCSD_ERR_ARG, "a view of a view is not supported");
+    if (Bt.packed()) throw Error(CCSD_ERR_ARG, "views of packed tensors are not supported");
+    auto T = std::make_unique<Tensor>();
+    T->name = name;
+    const int gsize[4] = {nout[0], nout[1], nin[0], nin[1]};
+    for (int g = 0; g < 4; g++)
+        for (int k = 0; k < gsize[g]; k++) T->group.push_back(g);
+    T->ndim = (int)T->group.size();
+    if (T->ndim != Bt.ndim) throw Error(CCSD_ERR_ARG, "view rank differs from its base");
+    for (int s = 0; s < 2; s++) {
+        T->nout[s] = nout[s];
+        T->nin[s] = nin[s];
+    }
+    for (int p = 0; p < T->ndim; p++)
+        if (group_space(T->group[p]) != group_space(Bt.group[perm[p]]))
+            throw Error(CCSD_ERR_ARG, "view permutation mixes occupied and virtual positions");
+    // every view group must map, in order, onto one base group (alpha-first order is kept)
+    for (int p = 0; p + 1 < T->ndim; p++)
+        if (T->group[p] == T->group[p + 1] &&
+            (Bt.group[perm[p]] != Bt.group[perm[p + 1]] || perm[p + 1] != perm[p] + 1))
+            throw Error(CCSD_ERR_ARG, "view permutation splits an antisymmetric group");
+    for (auto& bc : Bt.cases) {
+        SpinCase sc;
+        sc.spin.resize(T->ndim);
+        for (int p = 0; p < T->ndim; p++) {
+            sc.spin[p] = bc.spin[perm[p]];
+            if (sc.spin[p] == ALPHA) sc.alpha[T->group[p]]++;
+        }
+        for (auto& bb : bc.blocks) {
+            Block b;
+            b.irrep.resize(T->ndim);
+            b.len.resize(T->ndim);
+            b.stride.resize(T->ndim);
+            for (int p = 0; p < T->ndim; p++) {
+                b.irrep[p] = bb.irrep[perm[p]];
+                b.len[p] = bb.len[perm[p]];
+                b.stride[p] = bb.stride[perm[p]];
+            }
+            b.offset = bb.offset;
+            b.size = bb.size;
+            sc.block_of[b.irrep] = (int)sc.blocks.size();
+            sc.blocks.push_back(b);
+        }
+        T->cases.push_back(sc);
+    }
+    T->data = Bt.data;
+    T->total = Bt.total;
+    T->view_of = hb;
+    int h = next_handle++;
+    tensors[h] = std::move(T);
+    return h;
 }
 
 // ---------------------------------------------------------------------------

@@ -88,6 +88,7 @@ struct Tensor {
     std::vector<SpinCase> cases;
     double* data = nullptr;       // device
     int64_t total = 0;
+    int view_of = 0;              // > 0: blocks alias the storage of that tensor (no own data)
 
     int find_case(const int alpha[4]) const {
         for (size_t c = 0; c < cases.size(); c++) {
@@ -234,6 +235,9 @@ public:
 
     Tensor& tensor(int h);
     int create_tensor(const std::string& name, const int nout[2], const int nin[2], int flags);
+    // A tensor whose element (x_0..x_{n-1}) is the base tensor's element with x_p at base
+    // position perm[p] (e.g. <ab||ci> = <ci||ab>); its blocks alias the base's storage.
+    int create_view(const std::string& name, int base, const int nout[2], const int nin[2], const int* perm);
     void destroy_tensor(int h);
     void* dmalloc(size_t bytes);
     void dfree(void* p, size_t bytes);

@@ -224,13 +224,25 @@ void create_hamiltonian_tensors(Context& ctx, bool pack_vvvv, ccsd_hamiltonian* 
     H->fMI = mk(ctx, "f(ij)", 0, 1, 0, 1);
     H->VMNIJ = mk(ctx, "<ij||kl>", 0, 2, 0, 2);
     H->VAMIJ = mk(ctx, "<ai||jk>", 1, 1, 0, 2);
-    H->VMNEJ = mk(ctx, "<ij||ak>", 0, 2, 1, 1);
-    H->VABIJ = mk(ctx, "<ab||ij>", 2, 0, 0, 2);
     H->VMNEF = mk(ctx, "<ij||ab>", 0, 2, 2, 0);
     H->VAMEI = mk(ctx, "<ai||bj>", 1, 1, 1, 1);
     H->VAMEF = mk(ctx, "<ai||bc>", 1, 1, 2, 0);
-    H->VABEJ = mk(ctx, "<ab||ci>", 2, 0, 1, 1);
     H->VABEF = mk(ctx, "<ab||cd>", 2, 0, 2, 0, pack_vvvv ? CCSD_TENSOR_PACKED : 0);
+    // blocks equal by Hermiticity (aomoints.cxx:1375-1387) are views with permuted
+    // strides instead of copies: <ij||ak> = <ak||ij>, <ab||ij> = <ij||ab>, <ab||ci> = <ci||ab>
+    const int perm[4] = {2, 3, 0, 1};
+    {
+        int no[2] = {0, 2}, ni[2] = {1, 1};
+        H->VMNEJ = ctx.create_view("<ij||ak>", H->VAMIJ, no, ni, perm);
+    }
+    {
+        int no[2] = {2, 0}, ni[2] = {0, 2};
+        H->VABIJ = ctx.create_view("<ab||ij>", H->VMNEF, no, ni, perm);
+    }
+    {
+        int no[2] = {2, 0}, ni[2] = {1, 1};
+        H->VABEJ = ctx.create_view("<ab||ci>", H->VAMEF, no, ni, perm);
+    }
 }
 
 void build_hamiltonian(Context& ctx, int naux, const double* B, const double* eps, const int* aux_per_irrep,
@@ -255,8 +267,7 @@ void build_hamiltonian(Context& ctx, int naux, const double* B, const double* ep
 
     bld.one_electron(H->fAE, eps);
     bld.one_electron(H->fMI, eps);
-    for (int h : {H->VMNIJ, H->VAMIJ, H->VMNEJ, H->VABIJ, H->VMNEF, H->VAMEI, H->VAMEF, H->VABEJ, H->VABEF})
-        bld.two_electron(h);
+    for (int h : {H->VMNIJ, H->VAMIJ, H->VMNEF, H->VAMEI, H->VAMEF, H->VABEF}) bld.two_electron(h);
     CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
     ctx.dfree(bld.dB, nB * sizeof(double));
 }
