@@ -41,7 +41,8 @@ Context::~Context() {
         cudaFree(w->scale);
         cudaFree(w->rowmax);
     }
-    for (auto& kv : tensors) cudaFree(kv.second->data);
+    for (auto& kv : tensors)
+        if (!kv.second->view_of) cudaFree(kv.second->data);   // views alias their base
     cudaFree(d_scalar);
     for (auto& p : pending) {
         cudaEventDestroy(p.second.first);
@@ -289,6 +290,27 @@ static int64_t* upload_table(Context& ctx, const std::vector<int64_t>& h) {
     return d;
 }
 
+std::pair<cudaEvent_t, cudaEvent_t> Context::prof_begin() {
+    cudaEvent_t e0, e1;
+    if (event_pool.size() >= 2) {
+        e0 = event_pool.back();
+        event_pool.pop_back();
+        e1 = event_pool.back();
+        event_pool.pop_back();
+    } else {
+        CCSD_CUDA(cudaEventCreate(&e0));
+        CCSD_CUDA(cudaEventCreate(&e1));
+    }
+    CCSD_CUDA(cudaEventRecord(e0, stream));
+    return {e0, e1};
+}
+
+void Context::prof_end(std::pair<cudaEvent_t, cudaEvent_t> ev, const std::string& label, double flops) {
+    CCSD_CUDA(cudaEventRecord(ev.second, stream));
+    pending.push_back({label, ev});
+    pending_flops.push_back(flops);
+}
+
 // fold recorded event pairs into per-statement totals (synchronises the stream)
 void Context::collect_profile() {
     CCSD_CUDA(cudaStreamSynchronize(stream));
@@ -393,21 +415,9 @@ void Context::run(Plan& p, double* scalar_out, double* dot_target) {
             case Step::GEMM: {
                 GemmStep& g = p.gemms[st.idx];
                 if (profiling) {
-                    cudaEvent_t e0, e1;
-                    if (event_pool.size() >= 2) {
-                        e0 = event_pool.back();
-                        event_pool.pop_back();
-                        e1 = event_pool.back();
-                        event_pool.pop_back();
-                    } else {
-                        CCSD_CUDA(cudaEventCreate(&e0));
-                        CCSD_CUDA(cudaEventCreate(&e1));
-                    }
-                    CCSD_CUDA(cudaEventRecord(e0, stream));
+                    auto ev = prof_begin();
                     run_gemm(p, g);
-                    CCSD_CUDA(cudaEventRecord(e1, stream));
-                    pending.push_back({g.label.empty() ? std::string("gemm") : g.label, {e0, e1}});
-                    pending_flops.push_back(g.flops());
+                    prof_end(ev, g.label.empty() ? std::string("gemm") : g.label, g.flops());
                 } else {
                     run_gemm(p, g);
                 }
@@ -424,12 +434,16 @@ void Context::run(Plan& p, double* scalar_out, double* dot_target) {
                     a.sB[d] = s.sC[d];
                     a.total *= s.len[d];
                 }
+                auto ev = profiling ? prof_begin() : std::make_pair((cudaEvent_t) nullptr, (cudaEvent_t) nullptr);
                 kern::sum_strided(data_of(p, s.tA) + s.offA, data_of(p, s.tC) + s.offC, a, s.alpha, stream);
+                if (profiling) prof_end(ev, s.label.empty() ? std::string("sum") : s.label, 0.0);
                 break;
             }
             case Step::SCALE: {
                 auto& s = p.scales[st.idx];
+                auto ev = profiling ? prof_begin() : std::make_pair((cudaEvent_t) nullptr, (cudaEvent_t) nullptr);
                 kern::scale(data_of(p, s.tC) + s.off, s.n, s.beta, stream);
+                if (profiling) prof_end(ev, s.label.empty() ? std::string("scale") : s.label, 0.0);
                 break;
             }
             case Step::DOT: {

@@ -127,6 +127,7 @@ struct GemmStep {
 
 // C[perm] += alpha * A  over one block (strided, up to 8 dims)
 struct SumStep {
+    std::string label;
     int tA = 0, tC = 0;
     int ndim = 0;
     int64_t len[8];
@@ -137,6 +138,7 @@ struct SumStep {
 
 // C_block *= beta (beta == 0: zero-fill)
 struct ScaleStep {
+    std::string label;
     int tC = 0;
     int64_t off = 0, n = 0;
     double beta = 1;
@@ -229,6 +231,8 @@ public:
     std::vector<double> pending_flops;
     std::vector<cudaEvent_t> event_pool;
     void collect_profile();
+    std::pair<cudaEvent_t, cudaEvent_t> prof_begin();
+    void prof_end(std::pair<cudaEvent_t, cudaEvent_t> ev, const std::string& label, double flops);
 
     Context(int device, cudaStream_t s);
     ~Context();

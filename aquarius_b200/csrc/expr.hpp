@@ -44,13 +44,19 @@ struct Lhs {
     int h;
     std::string idx;
     void sum(double alpha, const Indexed& x, double beta) {
-        r->plan->append(plan_sum(*r->ctx, alpha, x.h, x.idx, beta, h, idx));
+        Plan p = plan_sum(*r->ctx, alpha, x.h, x.idx, beta, h, idx);
+        std::string label = r->ctx->tensor(h).name + "[" + idx + "] += " + r->ctx->tensor(x.h).name + "[" + x.idx + "]";
+        for (auto& g : p.sums) g.label = label;
+        for (auto& g : p.scales) g.label = label + " (scale)";
+        r->plan->append(std::move(p));
     }
     void mult(double alpha, const IndexedMult& m, double beta) {
         Plan p = plan_contract(*r->ctx, alpha, m.a.h, m.a.idx, m.b.h, m.b.idx, beta, h, idx);
         std::string label = r->ctx->tensor(h).name + "[" + idx + "] += " + r->ctx->tensor(m.a.h).name + "[" + m.a.idx +
                             "]*" + r->ctx->tensor(m.b.h).name + "[" + m.b.idx + "]";
         for (auto& g : p.gemms) g.label = label;
+        for (auto& g : p.sums) g.label = label + " (images)";
+        for (auto& g : p.scales) g.label = label + " (scale)";
         r->plan->append(std::move(p));
     }
     void operator=(const Indexed& x) { sum(x.f, x, 0.0); }

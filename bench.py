@@ -300,6 +300,10 @@ def main():
         results[p] = dict(ms=ms, launches=launches, prof=prof, energy=e, conv=c, flops=flops,
                           clocks=clk.summary(), energies=None)
         log(f"[bench] {p}: {ms / args.steps:.1f} ms/iter, E={e:.12f}, conv={c:.3e}, launches={launches}")
+        for k, ent in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])[:14]:
+            tf = ent["flops"] / (ent["ms"] * 1e-3) / 1e12 if ent["ms"] and ent["flops"] else 0.0
+            log(f"[bench]   {ent['ms'] / args.steps:9.2f} ms/iter {ent['launches'] // args.steps:4d} launches "
+                f"{tf:7.1f} TF/s  {k}")
         s.close()
     head = results[prec]
     ms_step = head["ms"] / args.steps
