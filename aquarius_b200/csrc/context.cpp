@@ -44,6 +44,7 @@ Context::~Context() {
     for (auto& kv : tensors)
         if (!kv.second->view_of) cudaFree(kv.second->data);   // views alias their base
     cudaFree(d_scalar);
+    cudaFree(splitk_ws);
     for (auto& p : pending) {
         cudaEventDestroy(p.second.first);
         cudaEventDestroy(p.second.second);
@@ -331,6 +332,17 @@ void Context::collect_profile() {
 void Context::upload(Plan& p) {
     bool any = false;
     if (p.scratch_elems > 0 && !p.scratch) p.scratch = (double*)dmalloc(p.scratch_elems * sizeof(double));
+    // split-K workspace of the FP64 GEMM, grown before any capture
+    int64_t need = 0;
+    for (auto& g : p.gemms) {
+        int ks = kern::fp64_ksplit(g.M, g.N, g.K);
+        if (ks > 1) need = std::max<int64_t>(need, (int64_t)ks * g.M * g.N);
+    }
+    if (need > splitk_elems) {
+        if (splitk_ws) dfree(splitk_ws, splitk_elems * sizeof(double));
+        splitk_ws = (double*)dmalloc(need * sizeof(double));
+        splitk_elems = need;
+    }
     for (auto& g : p.gemms) {
         if (g.dAm) continue;
         any = true;
@@ -399,6 +411,8 @@ void Context::run_gemm(Plan& p, GemmStep& g) {
     for (int i = 0; i < 4; i++) a.vsign[i] = g.vsign[i];
     a.a_kcontig = g.a_kcontig;
     a.b_kcontig = g.b_kcontig;
+    a.ws = splitk_ws;
+    a.ws_elems = splitk_elems;
     if (precision == CCSD_PREC_SPLIT && kern::split_supported()) {
         run_split_gemm(g, a);
     } else {

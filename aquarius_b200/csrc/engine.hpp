@@ -214,6 +214,8 @@ public:
     std::map<int64_t, int> split_owner;                    // cache key -> tensor handle
     int64_t split_cache_next = 1;
     kern::SlicedOperand ws_view[2];                        // workspace views of the current call
+    double* splitk_ws = nullptr;                           // FP64 split-K partials
+    int64_t splitk_elems = 0;
     kern::SlicedOperand alloc_sliced(int rows, int K);
     void free_sliced(kern::SlicedOperand& s);
     void ensure_ws(kern::SlicedOperand& w, int rows, int K);

@@ -20,7 +20,14 @@ struct GemmArgs {
     double vsign[4] = {1, 1, 1, 1};
     bool a_kcontig = false;   // consecutive k -> consecutive A addresses
     bool b_kcontig = false;   // consecutive k -> consecutive B addresses
+    // split-K: partial products of ksplit K-ranges go to ws[z][m][n] (M*N*ksplit doubles)
+    // and are folded in a fixed order before the scatter into C
+    double* ws = nullptr;
+    int64_t ws_elems = 0;
 };
+
+// K-ranges the FP64 GEMM splits a contraction into (1 = none); ws needs ksplit*M*N doubles
+int fp64_ksplit(int M, int N, int K);
 
 // native FP64 tensor-core (DMMA) GETT kernel
 void gemm_fp64(const GemmArgs& g, cudaStream_t s);

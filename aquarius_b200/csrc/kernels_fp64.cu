@@ -10,6 +10,7 @@
 #include <map>
 #include <mutex>
 #include <utility>
+#include <algorithm>
 #include <cuda_runtime.h>
 
 #include "kernels.hpp"
@@ -71,7 +72,11 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_fp64_kernel(GemmArgs g) {
     for (int i = tid; i < BN; i += THREADS) sBn[i] = (n0 + i < g.N) ? g.Bn[n0 + i] : 0;
     __syncthreads();
 
-    const int ktiles = (g.K + BK - 1) / BK;
+    // this CTA's K-range (split-K along gridDim.z)
+    const int ktiles_all = (g.K + BK - 1) / BK;
+    const int per_split = (ktiles_all + gridDim.z - 1) / gridDim.z;
+    const int kt0 = blockIdx.z * per_split;
+    const int ktiles = max(0, min(ktiles_all, kt0 + per_split) - kt0);
 
     auto load_stage = [&](int stage, int kt) {
         const int k0 = kt * BK;
@@ -111,7 +116,7 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_fp64_kernel(GemmArgs g) {
 
 #pragma unroll
     for (int s = 0; s < STAGES - 1; s++) {
-        if (s < ktiles) load_stage(s, s);
+        if (s < ktiles) load_stage(s, kt0 + s);
         cp_commit();
     }
 
@@ -120,7 +125,7 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_fp64_kernel(GemmArgs g) {
         __syncthreads();
         {
             int nk = kt + STAGES - 1;
-            if (nk < ktiles) load_stage(nk % STAGES, nk);
+            if (nk < ktiles) load_stage(nk % STAGES, kt0 + nk);
             cp_commit();
         }
         const double* as = As + (kt % STAGES) * S::a_elems;
@@ -147,6 +152,24 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_fp64_kernel(GemmArgs g) {
     }
     cp_wait<0>();
 
+    if (gridDim.z > 1) {
+        // split-K: raw partial sums, folded by splitk_fold_kernel
+        double* wz = g.ws + (int64_t)blockIdx.z * g.M * g.N;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            int m = m0 + wm + i * 8 + (lane >> 2);
+            if (m >= g.M) continue;
+#pragma unroll
+            for (int j = 0; j < 4; j++)
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    int n = n0 + wn + j * 8 + 2 * (lane & 3) + h;
+                    if (n < g.N) wz[(int64_t)m * g.N + n] = acc[i][j][h];
+                }
+        }
+        return;
+    }
+
     // epilogue: scatter to every destination variant
 #pragma unroll
     for (int i = 0; i < 4; i++) {
@@ -172,6 +195,19 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_fp64_kernel(GemmArgs g) {
     }
 }
 
+// fold split-K partials in a fixed order and scatter alpha * sum into every variant
+__global__ void splitk_fold_kernel(GemmArgs g, int ks) {
+    const int64_t mn = (int64_t)g.M * g.N;
+    for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < mn; l += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        for (int z = 0; z < ks; z++) s += g.ws[z * mn + l];
+        const int m = (int)(l / g.N), n = (int)(l % g.N);
+        const double v = g.alpha * s;
+        for (int a = 0; a < g.nvm; a++)
+            for (int b = 0; b < g.nvn; b++) g.C[g.Cm[a][m] + g.Cn[b][n]] += g.vsign[a * g.nvn + b] * v;
+    }
+}
+
 template <bool AK, bool BKc>
 void launch_fp64(const GemmArgs& g, cudaStream_t s) {
     using S = Smem<AK, BKc>;
@@ -180,12 +216,32 @@ void launch_fp64(const GemmArgs& g, cudaStream_t s) {
         cudaFuncSetAttribute(gemm_fp64_kernel<AK, BKc>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
         configured = true;
     }
-    dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM);
+    int ks = fp64_ksplit(g.M, g.N, g.K);
+    if (!g.ws || (int64_t)ks * g.M * g.N > g.ws_elems) ks = 1;
+    dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, ks);
     gemm_fp64_kernel<AK, BKc><<<grid, THREADS, S::bytes, s>>>(g);
     COUNT_LAUNCH();
+    if (ks > 1) {
+        const int64_t mn = (int64_t)g.M * g.N;
+        int nb = (int)std::min<int64_t>((mn + 255) / 256, 148 * 16);
+        splitk_fold_kernel<<<nb, 256, 0, s>>>(g, ks);
+        COUNT_LAUNCH();
+    }
 }
 
 }  // namespace
+
+// Few output tiles and a long K: split K so that about two waves of CTAs stream the
+// operands; every split keeps at least 512 k.
+int fp64_ksplit(int M, int N, int K) {
+    const int64_t tiles = (int64_t)((M + BM - 1) / BM) * ((N + BN - 1) / BN);
+    const int ktiles = (K + BK - 1) / BK;
+    if (tiles >= 148) return 1;
+    int64_t ks = (2 * 148 + tiles - 1) / tiles;
+    ks = std::min<int64_t>(ks, ktiles / 32);
+    ks = std::min<int64_t>(ks, 256);
+    return (int)std::max<int64_t>(ks, 1);
+}
 
 void gemm_fp64(const GemmArgs& g, cudaStream_t s) {
     if (g.M <= 0 || g.N <= 0 || g.K <= 0) return;
