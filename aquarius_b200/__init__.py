@@ -58,7 +58,7 @@ class Options(ctypes.Structure):
     _fields_ = [
         ("conv_tol", ctypes.c_double), ("max_iter", ctypes.c_int), ("diis_order", ctypes.c_int),
         ("diis_start", ctypes.c_int), ("diis_damping", ctypes.c_double), ("precision", ctypes.c_int),
-        ("slices", ctypes.c_int), ("use_graph", ctypes.c_int),
+        ("slices", ctypes.c_int), ("use_graph", ctypes.c_int), ("refine_tol", ctypes.c_double),
     ]
 
 
@@ -503,12 +503,13 @@ class HamiltonianHandle:
 
 class Solver:
     def __init__(self, ctx, H: HamiltonianHandle, conv_tol=1e-9, max_iter=50, diis_order=5, diis_start=1,
-                 precision="fp64", slices=0, use_graph=False):
+                 precision="fp64", slices=0, use_graph=False, refine_tol=0.0):
         self.ctx = ctx
         o = Options()
         lib().ccsd_options_default(ctypes.byref(o))
         o.conv_tol, o.max_iter, o.diis_order, o.diis_start = conv_tol, max_iter, diis_order, diis_start
         o.precision, o.slices, o.use_graph = PREC[precision], slices, 1 if use_graph else 0
+        o.refine_tol = refine_tol
         s = ctypes.c_void_p()
         _check(lib().ccsd_solver_create(ctx.c, ctypes.byref(H.H), ctypes.byref(o), ctypes.byref(s)), ctx.c)
         self.s = s

@@ -123,6 +123,7 @@ struct GemmStep {
     std::string label;                 // statement this block contraction came from
     int64_t split_cache_a = -1;        // keys of cached slices of constant operands
     int64_t split_cache_b = -1;
+    bool cache_a = false, cache_b = false;   // operand slices kept across calls (set at reserve)
 };
 
 // C[perm] += alpha * A  over one block (strided, up to 8 dims)
@@ -219,7 +220,7 @@ public:
     kern::SlicedOperand alloc_sliced(int rows, int K);
     void free_sliced(kern::SlicedOperand& s);
     void ensure_ws(kern::SlicedOperand& w, int rows, int K);
-    void reserve_split(const Plan& p);
+    void reserve_split(Plan& p);
     std::map<std::string, std::unique_ptr<Plan>> plan_cache;
 
     // optional per-statement timing of GEMM steps with CUDA events on the stream

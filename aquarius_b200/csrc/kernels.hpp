@@ -131,6 +131,17 @@ void diis_solve(int* state, double* e, double* c, const double* dots, int order,
 void pack_vvvv(double* V, int kind_ab, int kind_cd, int n0, int n1, int n2, int n3, int64_t scd, const double* tJ,
                const double* tK, int a0, int a1, bool J, bool K, cudaStream_t s);
 
+// One block of Tau: tau[a,b,i,j] = t2[a,b,i,j] + t1ai[a,i] t1bj[b,j] - t1aj[a,j] t1bi[b,i]
+// (blocks first index fastest; a T1 block [x,y] has leading dimension len of x; a null
+// pair drops its term)
+struct TauArgs {
+    double* tau = nullptr;
+    const double* t2 = nullptr;
+    const double *t1ai = nullptr, *t1bj = nullptr, *t1aj = nullptr, *t1bi = nullptr;
+    int64_t len[4] = {0, 0, 0, 0};
+};
+void tau_block(const TauArgs& a, cudaStream_t s);
+
 int64_t launch_count();
 void reset_launch_count();
 

@@ -736,6 +736,33 @@ __global__ void pack_vvvv_kernel(double* V, int kab, int kcd, int n0, int n1, in
 
 }  // namespace
 
+namespace {
+__global__ void tau_kernel(TauArgs a) {
+    const int64_t la = a.len[0], lb = a.len[1], li = a.len[2], lj = a.len[3];
+    const int64_t n = la * lb * li * lj;
+    for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < n; l += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = l;
+        const int64_t x = r % la;
+        r /= la;
+        const int64_t y = r % lb;
+        r /= lb;
+        const int64_t i = r % li;
+        const int64_t j = r / li;
+        double v = a.t2[l];
+        if (a.t1ai) v += a.t1ai[x + la * i] * a.t1bj[y + lb * j];
+        if (a.t1aj) v -= a.t1aj[x + la * j] * a.t1bi[y + lb * i];
+        a.tau[l] = v;
+    }
+}
+}  // namespace
+
+void tau_block(const TauArgs& a, cudaStream_t s) {
+    const int64_t n = a.len[0] * a.len[1] * a.len[2] * a.len[3];
+    if (n <= 0) return;
+    tau_kernel<<<ew_blocks(n), EW_THREADS, 0, s>>>(a);
+    COUNT_LAUNCH();
+}
+
 void pack_vvvv(double* V, int kind_ab, int kind_cd, int n0, int n1, int n2, int n3, int64_t scd, const double* tJ,
                const double* tK, int a0, int a1, bool J, bool K, cudaStream_t s) {
     int64_t ncd = kind_cd == 1 ? (int64_t)n2 * (n2 - 1) / 2 : (int64_t)n2 * n3;

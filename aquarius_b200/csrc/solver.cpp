@@ -32,6 +32,7 @@ void options_default(ccsd_options* o) {
     o->precision = CCSD_PREC_FP64;
     o->slices = 0;
     o->use_graph = 0;
+    o->refine_tol = 0.0;
 }
 
 Solver::Solver(Context& c, const ccsd_hamiltonian& h, const ccsd_options& o) : ctx(c), H(h), opts(o) {
@@ -100,7 +101,8 @@ Solver::Solver(Context& c, const ccsd_hamiltonian& h, const ccsd_options& o) : c
     }
     record_tau(tau_plan);
     record_energy(energy_plan);
-    ctx.run(tau_plan);
+    build_tau_blocks();
+    launch_tau();
     CCSD_CUDA(cudaMemsetAsync(d_red, 0, sizeof(double), ctx.stream));
     ctx.run(energy_plan, nullptr, d_red + 0);
     CCSD_CUDA(cudaMemcpyAsync(h_red, d_red, sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
@@ -196,6 +198,57 @@ void Solver::weight_tensor(int h) {
 
 // ---- recorded statements ---------------------------------------------------------
 
+// Fused Tau (ccsd.cxx:123-124): tau_abij = t_abij + t_ai t_bj - t_aj t_bi, one pass per
+// block of Tau with the T1 blocks each product term needs (spin and irrep of a match i, ...)
+void Solver::build_tau_blocks() {
+    Tensor& tau = ctx.tensor(Tau);
+    Tensor& t2 = ctx.tensor(T2);
+    Tensor& t1 = ctx.tensor(T1);
+    auto t1_block = [&](int spin, int h) -> const Block* {
+        int alpha[4] = {spin == ALPHA ? 1 : 0, 0, 0, spin == ALPHA ? 1 : 0};
+        int cs = t1.find_case(alpha);
+        if (cs < 0) return nullptr;
+        auto it = t1.cases[cs].block_of.find(std::vector<int>{h, h});
+        return it == t1.cases[cs].block_of.end() ? nullptr : &t1.cases[cs].blocks[it->second];
+    };
+    tau_blocks.clear();
+    for (size_t c = 0; c < tau.cases.size(); c++) {
+        const SpinCase& sc = tau.cases[c];
+        for (size_t bi = 0; bi < sc.blocks.size(); bi++) {
+            const Block& b = sc.blocks[bi];
+            if (b.size == 0) continue;
+            const Block& b2 = t2.cases[c].blocks[bi];
+            kern::TauArgs a;
+            a.tau = tau.data + b.offset;
+            a.t2 = t2.data + b2.offset;
+            for (int p = 0; p < 4; p++) a.len[p] = b.len[p];
+            const int sa = sc.spin[0], sb = sc.spin[1], si = sc.spin[2], sj = sc.spin[3];
+            const int ha = b.irrep[0], hb = b.irrep[1], hi = b.irrep[2], hj = b.irrep[3];
+            if (sa == si && sb == sj && ha == hi && hb == hj) {
+                const Block* x = t1_block(sa, ha);
+                const Block* y = t1_block(sb, hb);
+                if (x && y && x->size && y->size) {
+                    a.t1ai = t1.data + x->offset;
+                    a.t1bj = t1.data + y->offset;
+                }
+            }
+            if (sa == sj && sb == si && ha == hj && hb == hi) {
+                const Block* x = t1_block(sa, ha);
+                const Block* y = t1_block(sb, hb);
+                if (x && y && x->size && y->size) {
+                    a.t1aj = t1.data + x->offset;
+                    a.t1bi = t1.data + y->offset;
+                }
+            }
+            tau_blocks.push_back(a);
+        }
+    }
+}
+
+void Solver::launch_tau() {
+    for (auto& a : tau_blocks) kern::tau_block(a, ctx.stream);
+}
+
 void Solver::record_tau(Plan& p) {
     Recorder r{&ctx, &p};
     TensorRef tau{&r, Tau}, t1{&r, T1}, t2{&r, T2};
@@ -223,9 +276,8 @@ void Solver::record_iteration() {
     TensorRef FMEr{&r, FME}, FAEr{&r, FAE}, FMIr{&r, FMI};
     TensorRef WMNIJr{&r, WMNIJ}, WMNEJr{&r, WMNEJ}, WAMIJr{&r, WAMIJ}, WAMEIr{&r, WAMEI};
 
-    // ccsd.cxx:123-124
-    Taur["abij"] = T2r["abij"];
-    Taur["abij"] += 0.5 * T1r["ai"] * T1r["bj"];
+    // ccsd.cxx:123-124 (Tau = T2 + 1/2 P(ab)P(ij) t_ai t_bj) is formed by the fused Tau
+    // kernel before this plan runs (launch_tau); tau_plan keeps the statement's flop count
 
     // intermediates, ccsd.cxx:130-157
     FMEr["me"] = fME["me"];
@@ -333,6 +385,7 @@ void Solver::build_diis() {
 void Solver::launch_iteration() {
     cudaStream_t s = ctx.stream;
     // contractions (ccsd.cxx:123-180)
+    launch_tau();
     ctx.run(iter_plan);
     // Z.weight(D); T += Z; conv = Z.norm(00)  (ccsd.cxx:184-185,190), fused
     CCSD_CUDA(cudaMemsetAsync(d_red, 0, 2 * sizeof(double), s));
@@ -346,7 +399,7 @@ void Solver::launch_iteration() {
             }
     }
     // Tau from the updated T, energy (ccsd.cxx:187-189)
-    ctx.run(tau_plan);
+    launch_tau();
     ctx.run(energy_plan, nullptr, d_red + 0);
     // DIIS (diis.hpp:70-227)
     if (opts.diis_order > 1) diis_step();
@@ -374,6 +427,18 @@ void Solver::diis_step() {
 }
 
 void Solver::iterate_async() {
+    // split-precision residuals bottom out near 1e-9; past refine_tol the contractions
+    // switch to native FP64 for the rest of the solve (graphs are recaptured)
+    if (opts.precision == CCSD_PREC_SPLIT && opts.refine_tol > 0 && conv < opts.refine_tol &&
+        ctx.precision != CCSD_PREC_FP64) {
+        ctx.precision = CCSD_PREC_FP64;
+        refined = true;
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        if (graph) cudaGraphDestroy(graph);
+        graph_exec = nullptr;
+        graph = nullptr;
+        captured_once = false;
+    }
     if (opts.use_graph) {
         if (!graph_exec) {
             // the first iteration runs eagerly (it also warms every kernel), the graph is

@@ -38,6 +38,8 @@ public:
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     bool captured_once = false;
+    bool refined = false;           // switched to FP64 contractions (refine_tol reached)
+    std::vector<kern::TauArgs> tau_blocks;
 
     int iterations = 0;
     double energy = 0, conv = 0, mp2 = 0;
@@ -58,6 +60,8 @@ private:
     kern::WeightArgs weight_args(const Tensor& T, int cs, const Block& b) const;
     void weight_tensor(int h);
     void record_tau(Plan& p);
+    void build_tau_blocks();
+    void launch_tau();
     void record_energy(Plan& p);
     void record_iteration();
     void launch_iteration();

@@ -19,7 +19,22 @@ bool use_split(const GemmStep& g) {
         return e && e[0] == '1';
     }();
     if (all) return g.M > 0 && g.N > 0 && g.K > 0;
-    return g.M >= 64 && g.N >= 64 && g.K >= 256 && g.flops() >= 5e8;
+    // skinny contractions (N of a few tens, K of a few hundred) are HBM-bound; the tensor
+    // path reads 6 bytes per operand element instead of 8 and is not DMMA-issue bound
+    return g.M >= 128 && g.N >= 16 && g.K >= 64 && g.flops() >= 1e8;
+}
+
+// bytes of the three BF16 slices of a rows x K operand
+int64_t slice_bytes(int rows, int K) {
+    return (int64_t)kern::kDefaultSlices * kern::split_rows_pad(rows) * kern::split_k_pad(K) * 2 +
+           2 * (int64_t)kern::split_rows_pad(rows) * 8;
+}
+
+// device bytes the sliced constant operands may occupy (CCSD_SPLIT_CACHE_GB, default 56)
+int64_t cache_budget() {
+    const char* e = std::getenv("CCSD_SPLIT_CACHE_GB");
+    double gb = e ? std::atof(e) : 50.0;
+    return (int64_t)(gb * 1e9);
 }
 
 }  // namespace
@@ -58,26 +73,51 @@ void Context::ensure_ws(kern::SlicedOperand& w, int rows, int K) {
     w = alloc_sliced(keep_rows, (int)std::min<int64_t>((keep_elems + keep_rows - 1) / keep_rows, INT32_MAX));
 }
 
-// reserve workspace for every split contraction of a plan (called before any capture)
-void Context::reserve_split(const Plan& p) {
-    if (host_only) {
-        int64_t need_a = 0, need_b = 0, rows_a = 0, rows_b = 0;
-        for (auto& g : p.gemms) {
-            if (!use_split(g)) continue;
-            int64_t ea = (int64_t)kern::split_rows_pad(g.M) * kern::split_k_pad(g.K);
-            int64_t eb = (int64_t)kern::split_rows_pad(g.N) * kern::split_k_pad(g.K);
-            if (!is_constant(g.tA)) need_a = std::max(need_a, ea), rows_a = std::max<int64_t>(rows_a, g.M);
-            else dmalloc(3 * ea * 2);
-            if (!is_constant(g.tB)) need_b = std::max(need_b, eb), rows_b = std::max<int64_t>(rows_b, g.N);
-            else dmalloc(3 * eb * 2);
+// Decide, for every split contraction of a plan, which constant operands keep cached
+// slices (largest contractions first, within the byte budget), and size the per-call
+// workspace for the rest (called before any capture).
+void Context::reserve_split(Plan& p) {
+    std::vector<GemmStep*> order;
+    for (auto& g : p.gemms)
+        if (use_split(g)) order.push_back(&g);
+    std::stable_sort(order.begin(), order.end(), [](GemmStep* a, GemmStep* b) { return a->flops() > b->flops(); });
+    int64_t used = 0;
+    for (auto& kv : split_cache) used += kv.second.bytes;
+    const int64_t budget = cache_budget();
+    for (GemmStep* g : order) {
+        for (int side = 0; side < 2; side++) {
+            const int h = side == 0 ? g->tA : g->tB;
+            const int rows = side == 0 ? g->M : g->N;
+            bool& cache = side == 0 ? g->cache_a : g->cache_b;
+            cache = false;
+            if (h == kScratch || !is_constant(h)) continue;
+            const int64_t b = slice_bytes(rows, g->K);
+            if (used + b <= budget) {
+                cache = true;
+                used += b;
+            }
         }
-        dmalloc(3 * need_a * 2 + 16 * rows_a + 3 * need_b * 2 + 16 * rows_b + 1);
+    }
+    int64_t need_a = 0, need_b = 0, rows_a = 0, rows_b = 0;
+    for (GemmStep* g : order) {
+        if (!g->cache_a) {
+            need_a = std::max<int64_t>(need_a, (int64_t)kern::split_rows_pad(g->M) * kern::split_k_pad(g->K));
+            rows_a = std::max<int64_t>(rows_a, kern::split_rows_pad(g->M));
+        }
+        if (!g->cache_b) {
+            need_b = std::max<int64_t>(need_b, (int64_t)kern::split_rows_pad(g->N) * kern::split_k_pad(g->K));
+            rows_b = std::max<int64_t>(rows_b, kern::split_rows_pad(g->N));
+        }
+    }
+    if (host_only) {
+        // account the cached slices and the workspace as if they were allocated
+        dmalloc(used + 1);
+        dmalloc(6 * (need_a + need_b) + 16 * (rows_a + rows_b) + 1);
         return;
     }
-    for (auto& g : p.gemms) {
-        if (!use_split(g)) continue;
-        if (!is_constant(g.tA)) ensure_ws(split_ws.a, g.M, g.K);
-        if (!is_constant(g.tB)) ensure_ws(split_ws.b, g.N, g.K);
+    for (GemmStep* g : order) {
+        if (!g->cache_a) ensure_ws(split_ws.a, g->M, g->K);
+        if (!g->cache_b) ensure_ws(split_ws.b, g->N, g->K);
     }
 }
 
@@ -88,13 +128,13 @@ void Context::run_split_gemm(GemmStep& g, kern::GemmArgs& a) {
     }
     const int ns = kern::kDefaultSlices;
     auto prepare = [&](bool is_a, int64_t& key, kern::SlicedOperand& ws) -> kern::SlicedOperand* {
-        const int h = is_a ? g.tA : g.tB;
         const int rows = is_a ? g.M : g.N;
         const double* X = is_a ? a.A : a.B;
         const int64_t* R = is_a ? a.Am : a.Bn;
         const int64_t* Kt = is_a ? a.Ak : a.Bk;
         const bool kc = is_a ? a.a_kcontig : a.b_kcontig;
-        if (h != kScratch && is_constant(h)) {
+        const int h = is_a ? g.tA : g.tB;
+        if (is_a ? g.cache_a : g.cache_b) {
             if (key < 0) {
                 key = split_cache_next++;
                 split_cache[key] = alloc_sliced(rows, g.K);

@@ -152,6 +152,8 @@ typedef struct {
     int    precision;     /* CCSD_PREC_FP64 or CCSD_PREC_SPLIT */
     int    slices;        /* split-BF16 slice count; 0 = autotuned */
     int    use_graph;     /* capture one iteration as a CUDA graph and replay it */
+    double refine_tol;    /* split precision only: once conv < refine_tol, the remaining
+                             iterations use native-FP64 contractions (0 = never) */
 } ccsd_options;
 
 void ccsd_options_default(ccsd_options* opts);
