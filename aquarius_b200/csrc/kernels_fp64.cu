@@ -11,6 +11,7 @@
 #include <mutex>
 #include <utility>
 #include <algorithm>
+#include <stdexcept>
 #include <cuda_runtime.h>
 
 #include "kernels.hpp"
@@ -218,6 +219,7 @@ void launch_fp64(const GemmArgs& g, cudaStream_t s) {
     }
     int ks = fp64_ksplit(g.M, g.N, g.K);
     if (!g.ws || (int64_t)ks * g.M * g.N > g.ws_elems) ks = 1;
+    if ((g.M + BM - 1) / BM > 65535) throw std::runtime_error("FP64 GEMM: M too large for the grid");
     dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, ks);
     gemm_fp64_kernel<AK, BKc><<<grid, THREADS, S::bytes, s>>>(g);
     COUNT_LAUNCH();

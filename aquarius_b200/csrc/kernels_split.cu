@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(STHREADS) rowmax_kernel(const double* __restri
                                                           unsigned long long* rowmax) {
     __shared__ double tile[SR][SK + 1];
     __shared__ int64_t sR[SR], sK[SK];
-    const int r0 = blockIdx.y * SR, k0 = blockIdx.x * SK;
+    const int r0 = blockIdx.x * SR, k0 = blockIdx.y * SK;   // rows on x: up to 2^31 tiles
     load_tile<KC>(X, R, Kt, nrows, K, r0, k0, tile, sR, sK);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int r = warp; r < SR; r += STHREADS / 32) {
@@ -386,7 +386,7 @@ __global__ void __launch_bounds__(STHREADS)
                  unsigned short* __restrict__ out, double* __restrict__ scale) {
     __shared__ double tile[SR][SK + 1];
     __shared__ int64_t sR[SR], sK[SK];
-    const int r0 = blockIdx.y * SR, k0 = blockIdx.x * SK;
+    const int r0 = blockIdx.x * SR, k0 = blockIdx.y * SK;   // rows on x: up to 2^31 tiles
     load_tile<KC>(X, R, Kt, nrows, K, r0, k0, tile, sR, sK);
     const size_t plane = (size_t)rows_p * kpad;
 #pragma unroll
@@ -412,7 +412,7 @@ __global__ void __launch_bounds__(STHREADS)
         out[o] = b1;
         out[plane + o] = b2;
         out[2 * plane + o] = b3;
-        if (blockIdx.x == 0 && k == 0) scale[row] = mx > 0.0 ? ldexp(1.0, ilogb(mx) - 6) : 0.0;
+        if (blockIdx.y == 0 && k == 0) scale[row] = mx > 0.0 ? ldexp(1.0, ilogb(mx) - 6) : 0.0;
     }
 }
 
@@ -488,7 +488,8 @@ void slice_rows(const double* X, const int64_t* R, const int64_t* Kt, int nrows,
     if (nslices != NSLICE) throw std::runtime_error("only 3 slices are built");
     unsigned long long* rowmax = reinterpret_cast<unsigned long long*>(out.rowmax);
     cudaMemsetAsync(rowmax, 0, sizeof(double) * out.rows, s);
-    dim3 grid(out.kpad / SK, out.rows / SR);
+    if (out.kpad / SK > 65535) throw std::runtime_error("split operand K too long for the slicing grid");
+    dim3 grid(out.rows / SR, out.kpad / SK);
     if (kcontig) rowmax_kernel<true><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax);
     else rowmax_kernel<false><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax);
     if (kcontig)
