@@ -19,9 +19,11 @@ bool use_split(const GemmStep& g) {
         return e && e[0] == '1';
     }();
     if (all) return g.M > 0 && g.N > 0 && g.K > 0;
-    // skinny contractions (N of a few tens, K of a few hundred) are HBM-bound; the tensor
-    // path reads 6 bytes per operand element instead of 8 and is not DMMA-issue bound
-    return g.M >= 128 && g.N >= 16 && g.K >= 64 && g.flops() >= 1e8;
+    // Skinny (N of a few tens) or few-tile contractions stay on the FP64 kernel: the
+    // tensor kernel has no split-K, and re-slicing a large operand on every call costs
+    // more than the FP64 product when its slices cannot stay cached.
+    const int64_t tiles = (int64_t)((g.M + 127) / 128) * ((g.N + 127) / 128);
+    return g.M >= 128 && g.N >= 64 && g.K >= 256 && tiles >= 148 && g.flops() >= 5e8;
 }
 
 // bytes of the three BF16 slices of a rows x K operand
