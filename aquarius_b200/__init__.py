@@ -294,7 +294,7 @@ class Tensor:
         dims = []
         for p in range(self.ndim):
             sp = self.group[p] % 2
-            dims.append(2 * ctx.total(sp))
+            dims.append(ctx.total(sp, 0) + ctx.total(sp, 1))
         full = np.zeros(dims)
         groups = [[p for p in range(self.ndim) if self.group[p] == g] for g in range(4)]
         for alpha in self.spin_cases():
@@ -327,7 +327,7 @@ class Tensor:
                     for q in range(self.ndim):
                         p0 = perm[q]
                         sp = self.group[p0] % 2
-                        lo = spins[p0] * ctx.total(sp) + ctx.offset(sp, irr[p0])
+                        lo = ctx.spin_start(sp, spins[p0]) + ctx.offset(sp, irr[p0], spins[p0])
                         sl.append(slice(lo, lo + shape[p0]))
                     full[tuple(sl)] = sign * np.transpose(blk, perm)
         return full
@@ -417,6 +417,10 @@ class Context:
 
     def offset(self, space, irrep, spin=0):
         return int(self._counts[(space, spin)][:irrep].sum())
+
+    def spin_start(self, space, spin):
+        """first full spin-orbital index of a spin inside a space ([alpha | beta])"""
+        return 0 if spin == 0 else self.total(space, 0)
 
     def set_precision(self, precision="fp64", slices=0):
         _check(lib().ccsd_ctx_set_precision(self.c, PREC[precision], slices), self.c)

@@ -236,7 +236,7 @@ class DIIS:
 class CCSD:
     def __init__(self, H: Hamiltonian, diis_order=5, diis_start=1, diis_damping=0.0):
         self.H = H
-        o2, v2 = 2 * H.o, 2 * H.v
+        v2, o2 = H.fAI.shape
         self.D1 = H.dv[:, None] + H.do[None, :]
         self.D2 = (H.dv[:, None, None, None] + H.dv[None, :, None, None]
                    + H.do[None, None, :, None] + H.do[None, None, None, :])
@@ -258,9 +258,9 @@ class CCSD:
 
     def ladder(self, Tau):
         H = self.H
-        v, o2 = H.v, 2 * H.o
         if H.VABEF is not None:
             return 0.5 * es('abef,efij->abij', H.VABEF, Tau)
+        v, o2 = H.v, 2 * H.o
         tr = Tau.reshape(2, v, 2, v, o2, o2)
         out = np.zeros((2, v, 2, v, o2, o2))
         for sa in (0, 1):

@@ -88,7 +88,7 @@ def write_full(T, full):
             sl = []
             for p in range(T.ndim):
                 sp = T.group[p] % 2
-                lo = spins[p] * ctx.total(sp) + ctx.offset(sp, irr[p])
+                lo = ctx.spin_start(sp, spins[p]) + ctx.offset(sp, irr[p], spins[p])
                 sl.append(slice(lo, lo + shape[p]))
             blk = full[tuple(sl)]
             if getattr(T, "packed", False):
