@@ -44,7 +44,8 @@ EXPORTS = [
     "ccsd_hamiltonian_from_factor", "ccsd_hamiltonian_destroy", "ccsd_solver_create", "ccsd_solver_destroy",
     "ccsd_solver_mp2", "ccsd_solver_iterate", "ccsd_solver_iterate_async", "ccsd_solver_status", "ccsd_solver_run",
     "ccsd_solver_amplitudes", "ccsd_solver_flops", "ccsd_plan_query", "ccsd_synth_irreps", "ccsd_synth_problem",
-    "ccsd_dot_batch_noalloc",
+    "ccsd_dot_batch_noalloc", "ccsd_hamiltonian_create", "ccsd_hamiltonian_from_integrals", "ccsd_fcidump_read",
+    "ccsd_hamiltonian_from_fcidump", "ccsd_ctx_set_split_routing", "ccsd_ctx_split_launches",
 ]
 
 
@@ -97,6 +98,8 @@ def lib():
             "ccsd_ctx_launch_count": [vp, P(i64)],
             "ccsd_ctx_set_precision": [vp, ctypes.c_int, ctypes.c_int],
             "ccsd_ctx_set_profiling": [vp, ctypes.c_int],
+            "ccsd_ctx_set_split_routing": [vp, ctypes.c_int],
+            "ccsd_ctx_split_launches": [vp, P(i64)],
             "ccsd_ctx_profile_report": [vp, ctypes.c_char_p, i64, P(i64)],
             "ccsd_ctx_set_spaces": [vp, ctypes.c_int, vp, vp, vp, vp],
             "ccsd_tensor_create": [vp, ctypes.c_char_p, vp, vp, ctypes.c_int, P(i32)],
@@ -118,6 +121,11 @@ def lib():
             "ccsd_options_default": [P(Options)],
             "ccsd_hamiltonian_from_factor": [vp, ctypes.c_int, vp, vp, vp, ctypes.c_int, P(Hamiltonian)],
             "ccsd_hamiltonian_destroy": [vp, P(Hamiltonian)],
+            "ccsd_hamiltonian_create": [vp, ctypes.c_int, P(Hamiltonian)],
+            "ccsd_hamiltonian_from_integrals": [vp, ctypes.c_int, vp, vp, ctypes.c_int, P(Hamiltonian)],
+            "ccsd_fcidump_read": [ctypes.c_char_p, ctypes.c_int, P(ctypes.c_int), P(ctypes.c_int), P(dbl), vp, vp],
+            "ccsd_hamiltonian_from_fcidump": [vp, ctypes.c_char_p, ctypes.c_int, ctypes.c_int, P(Hamiltonian),
+                                              P(dbl)],
             "ccsd_solver_create": [vp, P(Hamiltonian), P(Options), P(vp)],
             "ccsd_solver_destroy": [vp],
             "ccsd_solver_mp2": [vp, P(dbl)],
@@ -202,6 +210,26 @@ def plan_query(vrt, occ, diis_order=8, pack_vvvv=True, precision="fp64"):
     _check(lib().ccsd_plan_query(len(vrt), _ptr(vrt), _ptr(occ), ctypes.byref(o), 1 if pack_vvvv else 0,
                                  ctypes.byref(fl), ctypes.byref(by)))
     return fl.value, by.value
+
+
+FCIDUMP_FULL_FOCK = 1
+FCIDUMP_SEMICANONICAL = 2
+
+
+def fcidump_read(path, full_fock=False):
+    """Parse an FCIDUMP on the host (ccsd_fcidump_read): dict with norb, nelec, ecore,
+    h (n x n) and eri (n^4, (pq|rs) with all eight images)."""
+    flags = FCIDUMP_FULL_FOCK if full_fock else 0
+    norb, nelec, ecore = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+    p = os.fsencode(path)
+    _check(lib().ccsd_fcidump_read(p, flags, ctypes.byref(norb), ctypes.byref(nelec), ctypes.byref(ecore), None,
+                                   None))
+    n = norb.value
+    h = np.zeros((n, n))
+    eri = np.zeros((n, n, n, n))
+    _check(lib().ccsd_fcidump_read(p, flags, ctypes.byref(norb), ctypes.byref(nelec), ctypes.byref(ecore), _ptr(h),
+                                   _ptr(eri)))
+    return {"norb": n, "nelec": nelec.value, "ecore": ecore.value, "h": h, "eri": eri}
 
 
 # ---------------------------------------------------------------------------
@@ -425,6 +453,15 @@ class Context:
     def set_precision(self, precision="fp64", slices=0):
         _check(lib().ccsd_ctx_set_precision(self.c, PREC[precision], slices), self.c)
 
+    def set_split_routing(self, mode="auto"):
+        """"auto": size thresholds keep small products on FP64; "all": every product split."""
+        _check(lib().ccsd_ctx_set_split_routing(self.c, {"auto": 0, "all": 1}[mode]), self.c)
+
+    def split_launches(self):
+        n = ctypes.c_int64()
+        _check(lib().ccsd_ctx_split_launches(self.c, ctypes.byref(n)), self.c)
+        return n.value
+
     def tensor(self, name, nout, nin, packed=False):
         h = ctypes.c_int32()
         _check(lib().ccsd_tensor_create(self.c, name.encode(), _ptr(_ints(nout)), _ptr(_ints(nin)),
@@ -477,6 +514,41 @@ class Context:
         n = ctypes.c_int64()
         _check(lib().ccsd_ctx_launch_count(self.c, ctypes.byref(n)), self.c)
         return n.value
+
+    def hamiltonian(self, pack_vvvv=False):
+        """The 13 H blocks, zero-filled, for the caller to write (ccsd_hamiltonian_create)."""
+        H = Hamiltonian()
+        _check(lib().ccsd_hamiltonian_create(self.c, 1 if pack_vvvv else 0, ctypes.byref(H)), self.c)
+        return HamiltonianHandle(self, H, pack_vvvv)
+
+    def hamiltonian_from_integrals(self, fock, eri, pack_vvvv=True):
+        """Closed-shell H from a spatial Fock matrix and dense (pq|rs) (occupied first)."""
+        fock = np.ascontiguousarray(fock, dtype=np.float64)
+        eri = np.ascontiguousarray(eri, dtype=np.float64)
+        n = fock.shape[0]
+        if fock.shape != (n, n) or eri.shape != (n, n, n, n):
+            raise ValueError("fock must be (n, n) and eri (n, n, n, n)")
+        H = Hamiltonian()
+        _check(lib().ccsd_hamiltonian_from_integrals(self.c, n, _ptr(fock), _ptr(eri), 1 if pack_vvvv else 0,
+                                                     ctypes.byref(H)), self.c)
+        return HamiltonianHandle(self, H, pack_vvvv)
+
+    def hamiltonian_from_fcidump(self, path, semicanonical=False, full_fock=False, pack_vvvv=True):
+        """Read an FCIDUMP, set C1 closed-shell spaces and build H: (handle, E(SCF))."""
+        flags = (FCIDUMP_SEMICANONICAL if semicanonical else 0) | (FCIDUMP_FULL_FOCK if full_fock else 0)
+        H = Hamiltonian()
+        escf = ctypes.c_double()
+        _check(lib().ccsd_hamiltonian_from_fcidump(self.c, os.fsencode(path), flags, 1 if pack_vvvv else 0,
+                                                   ctypes.byref(H), ctypes.byref(escf)), self.c)
+        norb = ctypes.c_int()
+        nelec = ctypes.c_int()
+        _check(lib().ccsd_fcidump_read(os.fsencode(path), flags, ctypes.byref(norb), ctypes.byref(nelec), None, None,
+                                       None))
+        no = nelec.value // 2
+        self.nirrep = 1
+        self._counts = {(0, 0): _ints([norb.value - no]), (0, 1): _ints([norb.value - no]), (1, 0): _ints([no]),
+                        (1, 1): _ints([no])}
+        return HamiltonianHandle(self, H, pack_vvvv), escf.value
 
     def hamiltonian_from_factor(self, B, eps, aux_per_irrep=None, pack_vvvv=True):
         B = np.ascontiguousarray(B, dtype=np.float64)

@@ -184,6 +184,20 @@ int ccsd_ctx_set_precision(ccsd_ctx ctx, int precision, int slices) {
     });
 }
 
+int ccsd_ctx_set_split_routing(ccsd_ctx ctx, int mode) {
+    return guarded(ctx, [&] {
+        if (mode != CCSD_SPLIT_ROUTE_AUTO && mode != CCSD_SPLIT_ROUTE_ALL) throw Error(CCSD_ERR_ARG, "bad routing mode");
+        from_handle(ctx)->split_routing = mode;
+    });
+}
+
+int ccsd_ctx_split_launches(ccsd_ctx ctx, int64_t* launches) {
+    return guarded(ctx, [&] {
+        if (!launches) throw Error(CCSD_ERR_ARG, "null output");
+        *launches = from_handle(ctx)->split_launches;
+    });
+}
+
 int ccsd_ctx_set_profiling(ccsd_ctx ctx, int on) {
     return guarded(ctx, [&] {
         Context* c = from_handle(ctx);
@@ -547,6 +561,62 @@ int ccsd_hamiltonian_from_factor(ccsd_ctx ctx, int naux, const double* B, const 
     return guarded(ctx, [&] {
         if (!B || !eps || !H || naux <= 0) throw Error(CCSD_ERR_ARG, "bad factor arguments");
         build_hamiltonian(*from_handle(ctx), naux, B, eps, aux_per_irrep, pack_vvvv != 0, H);
+    });
+}
+
+int ccsd_hamiltonian_create(ccsd_ctx ctx, int pack_vvvv, ccsd_hamiltonian* H) {
+    return guarded(ctx, [&] {
+        if (!H) throw Error(CCSD_ERR_ARG, "null hamiltonian");
+        Context* c = from_handle(ctx);
+        if (!c->spaces_set) throw Error(CCSD_ERR_ARG, "set the orbital spaces first");
+        create_hamiltonian_tensors(*c, pack_vvvv != 0, H);
+    });
+}
+
+int ccsd_hamiltonian_from_integrals(ccsd_ctx ctx, int n, const double* fock, const double* eri, int pack_vvvv,
+                                    ccsd_hamiltonian* H) {
+    return guarded(ctx, [&] {
+        if (!fock || !eri || !H || n <= 0) throw Error(CCSD_ERR_ARG, "bad integral arguments");
+        Context* c = from_handle(ctx);
+        if (!c->spaces_set) throw Error(CCSD_ERR_ARG, "set the orbital spaces first");
+        build_hamiltonian_dense(*c, n, fock, eri, pack_vvvv != 0, H);
+    });
+}
+
+int ccsd_fcidump_read(const char* path, int flags, int* norb, int* nelec, double* ecore, double* h, double* eri) {
+    return guarded(nullptr, [&] {
+        if (!path) throw Error(CCSD_ERR_ARG, "null path");
+        Fcidump d = read_fcidump(path, (flags & CCSD_FCIDUMP_FULL_FOCK) != 0, !h && !eri);
+        if (norb) *norb = d.norb;
+        if (nelec) *nelec = d.nelec;
+        if (ecore) *ecore = d.ecore;
+        if (h && !d.h.empty()) std::memcpy(h, d.h.data(), d.h.size() * sizeof(double));
+        if (eri && !d.eri.empty()) std::memcpy(eri, d.eri.data(), d.eri.size() * sizeof(double));
+    });
+}
+
+int ccsd_hamiltonian_from_fcidump(ccsd_ctx ctx, const char* path, int flags, int pack_vvvv, ccsd_hamiltonian* H,
+                                  double* escf) {
+    return guarded(ctx, [&] {
+        if (!path || !H) throw Error(CCSD_ERR_ARG, "bad FCIDUMP arguments");
+        Context* c = from_handle(ctx);
+        Fcidump d = read_fcidump(path, (flags & CCSD_FCIDUMP_FULL_FOCK) != 0, false);
+        const int n = d.norb, no = d.nelec / 2, nv = n - no;
+        if (!c->tensors.empty()) {
+            const Spaces& S = c->spaces;
+            bool same = c->spaces_set && S.nirrep == 1;
+            for (int s = 0; s < 2 && same; s++) same = S.n[VRT][s][0] == nv && S.n[OCC][s][0] == no;
+            if (!same) throw Error(CCSD_ERR_ARG, "context has tensors over other spaces than the FCIDUMP's");
+        } else {
+            int v[1] = {nv}, o[1] = {no};
+            const int st = ccsd_ctx_set_spaces(ctx, 1, v, v, o, o);
+            if (st != CCSD_OK) throw Error(st, "setting the FCIDUMP spaces failed");
+        }
+        std::vector<double> f((size_t)n * n);
+        const double e = closed_shell_fock(n, no, d.h.data(), d.eri.data(), f.data());
+        if (flags & CCSD_FCIDUMP_SEMICANONICAL) semicanonicalize(n, no, f.data(), d.eri.data());
+        build_hamiltonian_dense(*c, n, f.data(), d.eri.data(), pack_vvvv != 0, H);
+        if (escf) *escf = d.ecore + e;
     });
 }
 

@@ -6,6 +6,7 @@
 // totally symmetric irrep tuples (src/tensor/symblocked_tensor.cxx:551-690), each a
 // dense array with the first index fastest (src/tensor/ctf_tensor.hpp:221-226).
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 
@@ -15,6 +16,7 @@ namespace ccsd {
 
 Context::Context(int dev, cudaStream_t s) : device(dev), stream(s) {
     host_only = device < 0;
+    if (const char* e = std::getenv("CCSD_SPLIT_ALL")) split_routing = e[0] == '1' ? CCSD_SPLIT_ROUTE_ALL : split_routing;
     if (!host_only) {
         CCSD_CUDA(cudaSetDevice(device));
         if (!stream) {

@@ -209,6 +209,8 @@ public:
     int64_t launches = 0;
     int precision = CCSD_PREC_FP64;
     int slices = 0;
+    int split_routing = CCSD_SPLIT_ROUTE_AUTO;  // which contractions take the split kernel
+    int64_t split_launches = 0;        // split-BF16 GEMMs issued (host count)
     double* d_scalar = nullptr;        // device accumulator for dots
     kern::SplitWorkspace split_ws;     // scratch for split-BF16 GEMMs
     std::map<int64_t, kern::SlicedOperand> split_cache;   // sliced constant operands

@@ -5,10 +5,12 @@
 // the antisymmetrised physicist-notation integral
 //     <pq||rs> = (pr|qs) d(sp,sr) d(sq,ss) - (ps|qr) d(sp,ss) d(sq,sr),
 // with the index order [upper..., lower...] of TwoElectronOperator
-// (src/operator/2eoperator.cxx:13-21), and (pq|rs) = sum_P B[P,p,q] B[P,r,s].
-// Each Coulomb / exchange piece of a block is one FP64 gather-GEMM over P whose
-// epilogue scatters straight into the block; blocks stored with packed pairs (V_abcd)
-// go through a chunked temporary and a pack kernel.
+// (src/operator/2eoperator.cxx:13-21), and either (pq|rs) = sum_P B[P,p,q] B[P,r,s]
+// or a dense (pq|rs) array (integrals read from an FCIDUMP, src/operator/fcidump.cxx).
+// With the factor, each Coulomb / exchange piece of a block is one FP64 gather-GEMM
+// over P whose epilogue scatters straight into the block; with the dense array it is
+// one gather launch.  Blocks stored with packed pairs (V_abcd) go through a chunked
+// temporary and a pack kernel.
 #include <algorithm>
 #include <cstring>
 
@@ -22,11 +24,12 @@ namespace {
 // device copies of host index tables, freed together
 struct Tables {
     Context& ctx;
-    std::vector<std::pair<int64_t*, size_t>> held;
-    int64_t* up(const std::vector<int64_t>& h) {
-        int64_t* d = (int64_t*)ctx.dmalloc(h.size() * sizeof(int64_t));
-        CCSD_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(int64_t), cudaMemcpyHostToDevice, ctx.stream));
-        held.push_back({d, h.size() * sizeof(int64_t)});
+    std::vector<std::pair<void*, size_t>> held;
+    template <class T>
+    T* up(const std::vector<T>& h) {
+        T* d = (T*)ctx.dmalloc(std::max<size_t>(h.size(), 1) * sizeof(T));
+        CCSD_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, ctx.stream));
+        held.push_back({d, std::max<size_t>(h.size(), 1) * sizeof(T)});
         return d;
     }
     ~Tables() {
@@ -41,6 +44,7 @@ struct Builder {
     double* dB = nullptr;
     std::vector<int> aux_irrep;   // per P
     bool aux_known = false;
+    const double* dEri = nullptr;  // dense (pq|rs) on the device instead of the factor
 
     // global spatial index of (space, irrep, x)
     int gidx(int space, int irrep, int x) const {
@@ -56,10 +60,40 @@ struct Builder {
         return k;
     }
 
+    // dense path: C[off + sum stride*x] += sign * (g_pa g_pb | g_pc g_pd), position 0
+    // shifted by a0 (one gather launch; no arithmetic beyond the sign)
+    void gather(double* C, int64_t off, const int* space, const int* irrep, const int* len, const int64_t* stride,
+                int pa, int pb, int pc, int pd, double sign, int a0 = 0) {
+        for (int p = 0; p < 4; p++)
+            if (len[p] == 0) return;
+        kern::EriGatherArgs g;
+        Tables tb{ctx, {}};
+        for (int p = 0; p < 4; p++) {
+            std::vector<int> idx(len[p]);
+            for (int x = 0; x < len[p]; x++) idx[x] = gidx(space[p], irrep[p], (p == 0 ? a0 : 0) + x);
+            g.g[p] = tb.up(idx);
+            g.len[p] = len[p];
+            g.st[p] = stride[p];
+        }
+        g.C = C;
+        g.off = off;
+        g.pos[0] = pa;
+        g.pos[1] = pb;
+        g.pos[2] = pc;
+        g.pos[3] = pd;
+        g.n = n;
+        g.sign = sign;
+        kern::eri_gather(g, dEri, ctx.stream);
+    }
+
     // (x0 x1 | x2 x3) pieces over positions (pa, pb | pc, pd) of a block, scattered into
     // C with sign: C[off + sum stride*x] += sign * sum_P B[P,a,b] B[P,c,d]
     void coulomb(double* C, int64_t off, const int* space, const int* irrep, const int* len,
                  const int64_t* stride, int pa, int pb, int pc, int pd, double sign) {
+        if (dEri) {
+            gather(C, off, space, irrep, len, stride, pa, pb, pc, pd, sign);
+            return;
+        }
         int64_t M = (int64_t)len[pa] * len[pb], N = (int64_t)len[pc] * len[pd];
         if (M == 0 || N == 0) return;
         std::vector<int64_t> k = aux_list(irrep[pa] ^ irrep[pb]);
@@ -107,6 +141,24 @@ struct Builder {
                 if (sp0 != sp1 || b.irrep[0] != b.irrep[1] || sc.spin[0] != sc.spin[1]) continue;
                 std::vector<double> host(b.size, 0.0);
                 for (int x = 0; x < b.len[0]; x++) host[x + (int64_t)x * b.len[0]] = eps[gidx(sp0, b.irrep[0], x)];
+                CCSD_CUDA(cudaMemcpy(T.data + b.offset, host.data(), b.size * sizeof(double), cudaMemcpyHostToDevice));
+            }
+    }
+
+    // every same-spin block of a one-electron operator from a full spatial matrix
+    // f[p*n + q] (row = upper index); alpha and beta share it
+    void one_electron_full(int h, const double* f) {
+        Tensor& T = ctx.tensor(h);
+        for (auto& sc : T.cases)
+            for (auto& b : sc.blocks) {
+                if (b.size == 0) continue;
+                if (sc.spin[0] != sc.spin[1] || b.irrep[0] != b.irrep[1]) continue;
+                const int sp0 = group_space(T.group[0]), sp1 = group_space(T.group[1]);
+                std::vector<double> host(b.size, 0.0);
+                for (int y = 0; y < b.len[1]; y++)
+                    for (int x = 0; x < b.len[0]; x++)
+                        host[b.stride[0] * x + b.stride[1] * y] =
+                            f[(int64_t)gidx(sp0, b.irrep[0], x) * n + gidx(sp1, b.irrep[1], y)];
                 CCSD_CUDA(cudaMemcpy(T.data + b.offset, host.data(), b.size * sizeof(double), cudaMemcpyHostToDevice));
             }
     }
@@ -173,6 +225,10 @@ struct Builder {
     // like coulomb() over positions (0,1 | 2,3) of a temporary whose position 0 starts at a0
     void coulomb_shift(double* C, const int* space, const int* irrep, const int* len, const int64_t* stride, int a0,
                        double sign) {
+        if (dEri) {
+            gather(C, 0, space, irrep, len, stride, 0, 1, 2, 3, sign, a0);
+            return;
+        }
         int64_t M = (int64_t)len[0] * len[1], N = (int64_t)len[2] * len[3];
         if (M == 0 || N == 0) return;
         std::vector<int64_t> k = aux_list(irrep[0] ^ irrep[1]);
@@ -270,6 +326,35 @@ void build_hamiltonian(Context& ctx, int naux, const double* B, const double* ep
     for (int h : {H->VMNIJ, H->VAMIJ, H->VMNEF, H->VAMEI, H->VAMEF, H->VABEF}) bld.two_electron(h);
     CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
     ctx.dfree(bld.dB, nB * sizeof(double));
+}
+
+void build_hamiltonian_dense(Context& ctx, int n, const double* fock, const double* eri, bool pack_vvvv,
+                             ccsd_hamiltonian* H) {
+    const Spaces& S = ctx.spaces;
+    for (int h = 0; h < S.nirrep; h++)
+        for (int sp = 0; sp < 2; sp++)
+            if (S.n[sp][ALPHA][h] != S.n[sp][BETA][h])
+                throw Error(CCSD_ERR_ARG, "the dense-integral builder needs a closed-shell (alpha = beta) space");
+    if (n != S.total(VRT, ALPHA) + S.total(OCC, ALPHA))
+        throw Error(CCSD_ERR_ARG, "orbital count differs from the context's spaces");
+    const int64_t ne = (int64_t)n * n * n * n;
+    Builder bld{ctx, n, 0, S.total(OCC, ALPHA)};
+    double* d = (double*)ctx.dmalloc(ne * sizeof(double));
+    struct Free {
+        Context& c;
+        double* p;
+        int64_t b;
+        ~Free() {
+            cudaStreamSynchronize(c.stream);
+            c.dfree(p, b);
+        }
+    } guard{ctx, d, ne * (int64_t)sizeof(double)};
+    CCSD_CUDA(cudaMemcpyAsync(d, eri, ne * sizeof(double), cudaMemcpyHostToDevice, ctx.stream));
+    bld.dEri = d;
+    create_hamiltonian_tensors(ctx, pack_vvvv, H);
+    for (int h : {H->fAI, H->fME, H->fAE, H->fMI}) bld.one_electron_full(h, fock);
+    for (int h : {H->VMNIJ, H->VAMIJ, H->VMNEF, H->VAMEI, H->VAMEF, H->VABEF}) bld.two_electron(h);
+    CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
 }
 
 }  // namespace ccsd

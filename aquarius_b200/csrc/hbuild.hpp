@@ -1,4 +1,5 @@
-// Device-side assembly of H from a three-index factor (see hbuild.cpp).
+// Device-side assembly of H from a three-index factor or dense integrals (hbuild.cpp),
+// and the FCIDUMP reader (fcidump.cpp).
 #pragma once
 #include "engine.hpp"
 
@@ -7,4 +8,22 @@ namespace ccsd {
 void create_hamiltonian_tensors(Context& ctx, bool pack_vvvv, ccsd_hamiltonian* H);
 void build_hamiltonian(Context& ctx, int naux, const double* B, const double* eps, const int* aux_per_irrep,
                        bool pack_vvvv, ccsd_hamiltonian* H);
+// closed shell: fock[n*n] (row = upper index) and dense eri[n^4] = (pq|rs), last index
+// fastest, orbitals ordered occupied first, irrep-major inside occ and vrt
+void build_hamiltonian_dense(Context& ctx, int n, const double* fock, const double* eri, bool pack_vvvv,
+                             ccsd_hamiltonian* H);
+
+// FCIDUMP contents: h[n*n], eri[n^4] dense, core energy
+struct Fcidump {
+    int norb = 0, nelec = 0;
+    double ecore = 0.0;
+    std::vector<double> h, eri;
+};
+Fcidump read_fcidump(const char* path, bool full_fock, bool header_only);
+// closed-shell Fock f = h + sum_i 2(pq|ii) - (pi|iq) over the first nocc orbitals;
+// returns the electronic SCF energy sum_i (h_ii + f_ii)
+double closed_shell_fock(int n, int nocc, const double* h, const double* eri, double* fock);
+// rotate the occupied and the virtual orbitals separately to diagonalise the Fock
+// blocks (fock and eri rewritten in place)
+void semicanonicalize(int n, int nocc, double* fock, double* eri);
 }

@@ -142,6 +142,23 @@ struct TauArgs {
 };
 void tau_block(const TauArgs& a, cudaStream_t s);
 
+// Gather of a dense spatial (pq|rs) array (n^4, last index fastest) into a block:
+//   C[off + sum_p st[p] x_p] += sign * eri[((g0 n + g1) n + g2) n + g3],
+//   g_k = g[pos[k]][x_pos[k]]
+// with g[p] the orbital index of every x on position p (device tables).  Distinct x
+// must map to distinct elements of C.
+struct EriGatherArgs {
+    double* C = nullptr;
+    int64_t off = 0;
+    int len[4] = {1, 1, 1, 1};
+    int64_t st[4] = {0, 0, 0, 0};
+    const int* g[4] = {nullptr, nullptr, nullptr, nullptr};
+    int pos[4] = {0, 1, 2, 3};
+    int64_t n = 0;
+    double sign = 1.0;
+};
+void eri_gather(const EriGatherArgs& a, const double* eri, cudaStream_t s);
+
 int64_t launch_count();
 void reset_launch_count();
 

@@ -756,7 +756,31 @@ __global__ void tau_kernel(TauArgs a) {
         a.tau[l] = v;
     }
 }
+__global__ void eri_gather_kernel(EriGatherArgs a, const double* __restrict__ eri) {
+    const int64_t total = (int64_t)a.len[0] * a.len[1] * a.len[2] * a.len[3];
+    for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < total; l += (int64_t)gridDim.x * blockDim.x) {
+        int64_t r = l, dst = a.off;
+        int64_t g[4];
+#pragma unroll
+        for (int p = 0; p < 4; p++) {
+            const int x = (int)(r % a.len[p]);
+            r /= a.len[p];
+            dst += a.st[p] * x;
+            g[p] = a.g[p][x];
+        }
+        const int64_t src = ((g[a.pos[0]] * a.n + g[a.pos[1]]) * a.n + g[a.pos[2]]) * a.n + g[a.pos[3]];
+        a.C[dst] += a.sign * eri[src];
+    }
+}
+
 }  // namespace
+
+void eri_gather(const EriGatherArgs& a, const double* eri, cudaStream_t s) {
+    const int64_t n = (int64_t)a.len[0] * a.len[1] * a.len[2] * a.len[3];
+    if (n <= 0) return;
+    eri_gather_kernel<<<ew_blocks(n), EW_THREADS, 0, s>>>(a, eri);
+    COUNT_LAUNCH();
+}
 
 void tau_block(const TauArgs& a, cudaStream_t s) {
     const int64_t n = a.len[0] * a.len[1] * a.len[2] * a.len[3];

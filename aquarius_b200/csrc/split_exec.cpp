@@ -12,13 +12,9 @@ namespace {
 
 // Small contractions stay on the FP64 tensor-core kernel: a 128x128 tile would be mostly
 // padding and the slicing passes would cost more than the product.
-// CCSD_SPLIT_ALL=1 routes every contraction through the split kernel (coverage tests).
-bool use_split(const GemmStep& g) {
-    static const bool all = [] {
-        const char* e = std::getenv("CCSD_SPLIT_ALL");
-        return e && e[0] == '1';
-    }();
-    if (all) return g.M > 0 && g.N > 0 && g.K > 0;
+// CCSD_SPLIT_ROUTE_ALL sends every contraction through the split kernel (coverage tests).
+bool use_split(const GemmStep& g, int routing) {
+    if (routing == CCSD_SPLIT_ROUTE_ALL) return g.M > 0 && g.N > 0 && g.K > 0;
     // Skinny (N of a few tens) or few-tile contractions stay on the FP64 kernel: the
     // tensor kernel has no split-K, and re-slicing a large operand on every call costs
     // more than the FP64 product when its slices cannot stay cached.
@@ -81,7 +77,7 @@ void Context::ensure_ws(kern::SlicedOperand& w, int rows, int K) {
 void Context::reserve_split(Plan& p) {
     std::vector<GemmStep*> order;
     for (auto& g : p.gemms)
-        if (use_split(g)) order.push_back(&g);
+        if (use_split(g, split_routing)) order.push_back(&g);
     std::stable_sort(order.begin(), order.end(), [](GemmStep* a, GemmStep* b) { return a->flops() > b->flops(); });
     int64_t used = 0;
     for (auto& kv : split_cache) used += kv.second.bytes;
@@ -124,10 +120,11 @@ void Context::reserve_split(Plan& p) {
 }
 
 void Context::run_split_gemm(GemmStep& g, kern::GemmArgs& a) {
-    if (!use_split(g)) {
+    if (!use_split(g, split_routing)) {
         kern::gemm_fp64(a, stream);
         return;
     }
+    split_launches++;
     const int ns = kern::kDefaultSlices;
     auto prepare = [&](bool is_a, int64_t& key, kern::SlicedOperand& ws) -> kern::SlicedOperand* {
         const int rows = is_a ? g.M : g.N;

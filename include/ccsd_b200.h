@@ -81,6 +81,14 @@ int ccsd_ctx_device_bytes(ccsd_ctx ctx, int64_t* bytes);
 int ccsd_ctx_launch_count(ccsd_ctx ctx, int64_t* count);
 /* precision used by subsequent ccsd_contract calls (CCSD_PREC_*); slices=0: default */
 int ccsd_ctx_set_precision(ccsd_ctx ctx, int precision, int slices);
+/* Which contractions the split precision sends to the tensor-core kernel: AUTO keeps
+ * small, skinny or few-tile products on the FP64 kernel; ALL routes every product
+ * (coverage of small cases).  The environment variable CCSD_SPLIT_ALL=1 sets ALL at
+ * context creation.  ccsd_ctx_split_launches gives the split GEMMs issued so far.
+ * No counterpart in the reference (its contractions have one precision). */
+enum { CCSD_SPLIT_ROUTE_AUTO = 0, CCSD_SPLIT_ROUTE_ALL = 1 };
+int ccsd_ctx_set_split_routing(ccsd_ctx ctx, int mode);
+int ccsd_ctx_split_launches(ccsd_ctx ctx, int64_t* launches);
 /* Per-statement timing of contraction kernels with CUDA events on the context stream
  * (the role of the reference's named timers, src/time/time.hpp:103-147).  The report is
  * a JSON object {statement: {"launches": n, "ms": t, "flops": f}}; it synchronises the
@@ -178,6 +186,34 @@ typedef struct {
 int ccsd_hamiltonian_from_factor(ccsd_ctx ctx, int naux, const double* B, const double* eps,
                                  const int* aux_per_irrep, int pack_vvvv, ccsd_hamiltonian* H);
 int ccsd_hamiltonian_destroy(ccsd_ctx ctx, ccsd_hamiltonian* H);
+
+/* The 13 H blocks, zero-filled, for the caller to write (ccsd_tensor_write_block /
+ * ccsd_tensor_write): the TwoElectronOperator constructor (src/operator/2eoperator.cxx:10-21)
+ * that an integral transformation (src/operator/aomoints.cxx) then fills.  Any spaces,
+ * open shell included.  <ij||ak>, <ab||ij> and <ab||ci> are views of <ai||jk>, <ij||ab>
+ * and <ai||bc> (Hermiticity): write those three and the views follow. */
+int ccsd_hamiltonian_create(ccsd_ctx ctx, int pack_vvvv, ccsd_hamiltonian* H);
+
+/* Closed-shell H from dense spatial integrals (the assembly of src/operator/fcidump.cxx:472-514):
+ * fock[n*n] (row = upper index), eri[n^4] = (pq|rs) in chemists' notation, last index
+ * fastest; orbitals occupied first, irrep-major inside occ and vrt as in
+ * ccsd_ctx_set_spaces (alpha = beta, n = occ + vrt). */
+int ccsd_hamiltonian_from_integrals(ccsd_ctx ctx, int n, const double* fock, const double* eri, int pack_vvvv,
+                                    ccsd_hamiltonian* H);
+
+/* FCIDUMP input (src/operator/fcidump.cxx:35-516, task "fcidump"; options
+ * "1eints full" and "semicanonical"). */
+enum {
+    CCSD_FCIDUMP_FULL_FOCK = 1,      /* one-electron records are the full matrix (no mirroring) */
+    CCSD_FCIDUMP_SEMICANONICAL = 2   /* diagonalise the occupied and virtual Fock blocks */
+};
+/* Parse a file on the host.  h (n*n) and eri (n^4, dense, all eight images filled) may
+ * be NULL: then only NORB / NELEC are read.  No device needed. */
+int ccsd_fcidump_read(const char* path, int flags, int* norb, int* nelec, double* ecore, double* h, double* eri);
+/* Read a file, set the context's spaces (C1, NELEC/2 occupied, closed shell), build the
+ * Fock matrix and H on the device; escf (may be NULL) receives E_core + sum_i (h_ii + f_ii). */
+int ccsd_hamiltonian_from_fcidump(ccsd_ctx ctx, const char* path, int flags, int pack_vvvv, ccsd_hamiltonian* H,
+                                  double* escf);
 
 /* Solver: allocates T, Z, Tau, the 7 intermediates and the DIIS ring, forms the
  * MP1 guess and the MP2 energy (ccsd.cxx:37-62), and plans one iteration. */

@@ -322,3 +322,16 @@ def solve_scf(fixture: dict, name: str):
     mol, basis = from_fixture(fixture, name)
     S, H, eri = ao_integrals(mol, basis)
     return scf(mol, S, H, eri), H, eri
+
+
+def mo_integrals(res: SCFResult, H, eri):
+    """Spatial MO integrals of a closed-shell result: (h, (pq|rs)) over the alpha
+    orbitals, with the 8-fold symmetry made exact."""
+    C = res.Ca
+    h = C.T @ H @ C
+    h = 0.5 * (h + h.T)
+    mo = np.einsum("pqrs,pa,qb,rc,sd->abcd", eri, C, C, C, C, optimize=True)
+    mo = 0.5 * (mo + mo.transpose(1, 0, 2, 3))
+    mo = 0.5 * (mo + mo.transpose(0, 1, 3, 2))
+    mo = 0.5 * (mo + mo.transpose(2, 3, 0, 1))
+    return h, mo

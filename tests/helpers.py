@@ -235,3 +235,28 @@ def beta_mask(ctx, shapes, ia, ib, ic):
                         perm[a_] = b_
                 mask[tuple(sl[perm[q]] for q in range(len(ic)))] = True
     return mask
+
+
+def write_fcidump(path, h, eri, nelec, ecore, all_images=False, full_fock=False, ms2=0):
+    """Write spatial integrals as an FCIDUMP (1-based indices, canonical records
+    p>=q, r>=s, pq>=rs unless all_images; h lower triangle unless full_fock)."""
+    n = h.shape[0]
+    lines = [f"&FCI NORB={n},NELEC={nelec},MS2={ms2},", "ORBSYM=" + "1," * n, "ISYM=1,", "&END"]
+    for p in range(n):
+        for q in range(n):
+            for r in range(n):
+                for s in range(n):
+                    v = eri[p, q, r, s]
+                    if v == 0.0:
+                        continue
+                    if not all_images and not (p >= q and r >= s and (p > r or (p == r and q >= s))):
+                        continue
+                    lines.append(f"{float(v)!r} {p + 1} {q + 1} {r + 1} {s + 1}")
+    for p in range(n):
+        for q in range(n):
+            if full_fock or p >= q:
+                if h[p, q] != 0.0:
+                    lines.append(f"{float(h[p, q])!r} {p + 1} {q + 1} 0 0")
+    lines.append(f"{float(ecore)!r} 0 0 0 0")
+    with open(path, "w") as f:
+        f.write("\n".join(lines) + "\n")

@@ -24,12 +24,17 @@ def _contract(precision, o, v, ia, sa, ib, sb, ic, sc, seed, packed_a=False):
         ctx.set_spaces(vrt=[v], occ=[o])
         if precision == "split":
             ctx.set_precision("split")
+            ctx.set_split_routing("all")   # these sizes would stay on FP64 otherwise
         tA = ctx.tensor("A", *SHAPES[sa], packed=packed_a)
         tB = ctx.tensor("B", *SHAPES[sb])
         tC = ctx.tensor("C", *SHAPES[sc])
         write_full(tA, random_so(ctx, *SHAPES[sa], rng, scale=0.05))
         write_full(tB, random_so(ctx, *SHAPES[sb], rng, scale=0.01))
         ctx.contract(0.5, tA, ia, tB, ib, 0.0, tC, ic)
+        if precision == "split":
+            assert ctx.split_launches() > 0
+        else:
+            assert ctx.split_launches() == 0
         return tC.to_full()
     finally:
         ctx.close()
@@ -57,12 +62,14 @@ def test_split_solve_matches_oracle_every_iteration(o, v, seed):
     ctx = A.Context(0)
     try:
         ctx.set_spaces(vrt=[v], occ=[o])
+        ctx.set_split_routing("all")
         H = ctx.hamiltonian_from_factor(B, eps)
         s = ctx.solver(H, diis_order=8, precision="split")
         for it in range(10):
             e_ref, _ = ref.iterate()
             e, _ = s.iterate()
             assert abs(e - e_ref) <= 1e-8, (it, e, e_ref)
+        assert ctx.split_launches() > 0
         assert np.abs(s.T2.to_full() - ref.T.T2).max() <= 1e-7
         assert np.abs(s.T1.to_full() - ref.T.T1).max() <= 1e-7
         s.close()

@@ -54,6 +54,34 @@ def test_spin_orbital_hamiltonian_symmetries(system):
     assert np.abs(Hso.fAE[:va, va:]).max() == 0.0
 
 
+def h2o_equilibrium():
+    """H2O with O-H 0.9572 A and H-O-H 104.52 deg, O at the origin (C1), in bohr."""
+    r = 0.9572 / 0.529177210903
+    half = np.deg2rad(104.52) / 2
+    return scf.Molecule(["O", "H", "H"], [[0, 0, 0], [r * np.sin(half), 0, r * np.cos(half)],
+                                          [-r * np.sin(half), 0, r * np.cos(half)]])
+
+
+def test_h2o_equilibrium_two_oracles_agree():
+    """The CPU-runnable workload (H2O/cc-pVDZ at its equilibrium geometry, all electrons,
+    residual 1e-10, DIIS 8): no reference energy exists for it, so the spin-orbital
+    oracle is checked against the independent spin-adapted one."""
+    from oracle import rhf_ccsd as R
+    basis = {el: [(l, np.array(e), np.array(c)) for l, e, c in sh] for el, sh in FIXTURE["basis"]["cc-pVDZ"].items()}
+    mol = h2o_equilibrium()
+    S, H, eri = scf.ao_integrals(mol, basis)
+    res = scf.scf(mol, S, H, eri)
+    assert -76.1 < res.energy < -75.9
+    h, mo = scf.mo_integrals(res, H, eri)
+    fock = h + 2 * np.einsum("pqii->pq", mo[:, :, :5, :5]) - np.einsum("piiq->pq", mo[:, :5, :5, :])
+    so = O.CCSD(O.Hamiltonian(fock, mo, 5), diis_order=8)
+    e_so = so.run(conv_tol=1e-10, max_iter=100)
+    rhf = R.RHFCCSD(fock, mo, 5, diis_order=8)
+    e_rhf = rhf.run(1e-10, 100)
+    assert abs(so.mp2 - rhf.mp2) < 1e-12
+    assert abs(e_so - e_rhf) < 1e-9
+
+
 def test_integrals_overlap_normalised():
     mol, basis = scf.from_fixture(FIXTURE, "h2o-pvdz")
     S, H, eri = scf.ao_integrals(mol, basis)
