@@ -322,6 +322,9 @@ def main():
                 "frac": achieved / peak if peak else None, "traffic": None, "peak_kind": unit_kind,
                 "launches_per_step": lad["launches"] / args.steps,
                 "share_of_step": lad["ms"] / head["ms"] if head["ms"] else None}
+    if prec == "split" and peak:
+        # three BF16 slices per operand: six tcgen05 products per FP64-equivalent product
+        roofline["tensor_pipe_frac"] = 6 * achieved / peak
 
     # end to end through the public API: host factor -> H on device -> solve -> energy
     e2e = None
