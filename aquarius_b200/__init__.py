@@ -46,6 +46,8 @@ EXPORTS = [
     "ccsd_solver_amplitudes", "ccsd_solver_flops", "ccsd_plan_query", "ccsd_synth_irreps", "ccsd_synth_problem",
     "ccsd_dot_batch_noalloc", "ccsd_hamiltonian_create", "ccsd_hamiltonian_from_integrals", "ccsd_fcidump_read",
     "ccsd_hamiltonian_from_fcidump", "ccsd_ctx_set_split_routing", "ccsd_ctx_split_launches",
+    "ccsd_server_options_default", "ccsd_server_create", "ccsd_server_submit_synthetic", "ccsd_server_submit_factor",
+    "ccsd_server_poll", "ccsd_server_wait", "ccsd_server_stats", "ccsd_server_destroy",
 ]
 
 
@@ -78,6 +80,18 @@ class Hamiltonian(ctypes.Structure):
     _fields_ = [(f, ctypes.c_int32) for f in H_FIELDS]
 
 
+class ServerOptions(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int), ("memory_budget", ctypes.c_int64), ("max_active", ctypes.c_int),
+                ("pack_vvvv", ctypes.c_int), ("solve", Options)]
+
+
+class ServerResult(ctypes.Structure):
+    _fields_ = [("id", ctypes.c_int64), ("status", ctypes.c_int), ("iterations", ctypes.c_int),
+                ("energy", ctypes.c_double), ("mp2", ctypes.c_double), ("conv", ctypes.c_double),
+                ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double),
+                ("device_bytes", ctypes.c_int64), ("flops_per_iter", ctypes.c_double)]
+
+
 _lib = None
 
 
@@ -100,6 +114,14 @@ def lib():
             "ccsd_ctx_set_profiling": [vp, ctypes.c_int],
             "ccsd_ctx_set_split_routing": [vp, ctypes.c_int],
             "ccsd_ctx_split_launches": [vp, P(i64)],
+            "ccsd_server_options_default": [P(ServerOptions)],
+            "ccsd_server_create": [P(ServerOptions), P(vp)],
+            "ccsd_server_submit_synthetic": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_uint64, P(i64)],
+            "ccsd_server_submit_factor": [vp, ctypes.c_int, vp, vp, ctypes.c_int, vp, vp, vp, P(i64)],
+            "ccsd_server_poll": [vp, ctypes.c_int, P(ServerResult), P(ctypes.c_int)],
+            "ccsd_server_wait": [vp, dbl],
+            "ccsd_server_stats": [vp, P(ctypes.c_int), P(ctypes.c_int), P(i64), P(ctypes.c_int)],
+            "ccsd_server_destroy": [vp],
             "ccsd_ctx_profile_report": [vp, ctypes.c_char_p, i64, P(i64)],
             "ccsd_ctx_set_spaces": [vp, ctypes.c_int, vp, vp, vp, vp],
             "ccsd_tensor_create": [vp, ctypes.c_char_p, vp, vp, ctypes.c_int, P(i32)],
@@ -143,7 +165,7 @@ def lib():
         for name, args in sig.items():
             f = getattr(L, name)
             f.argtypes = args
-            f.restype = None if name == "ccsd_options_default" else ctypes.c_int
+            f.restype = None if name in ("ccsd_options_default", "ccsd_server_options_default") else ctypes.c_int
         L.ccsd_last_error.argtypes = [vp]
         L.ccsd_last_error.restype = ctypes.c_char_p
         _lib = L
@@ -300,6 +322,18 @@ class Tensor:
 
     def fill(self, val):
         _check(lib().ccsd_tensor_fill(self.ctx.c, self.h, float(val)), self.ctx.c)
+
+    def elements(self):
+        """stored elements over every spin case and irrep block"""
+        n = 0
+        for alpha in self.spin_cases():
+            for irr in itertools.product(range(self.ctx.nirrep), repeat=self.ndim):
+                x = 0
+                for h in irr:
+                    x ^= h
+                if not x:
+                    n += self.block_size(alpha, irr)
+        return n
 
     def norm(self, p=0):
         out = ctypes.c_double()
@@ -629,3 +663,67 @@ class Solver:
         x = ctypes.c_double()
         _check(lib().ccsd_solver_flops(self.s, ctypes.byref(x)), self.ctx.c)
         return x.value
+
+
+class Server:
+    """Continuous batching of solves on one device (ccsd_server_*): submit requests as
+    they arrive, poll finished results; admission by planned device bytes."""
+
+    def __init__(self, device=0, memory_budget=0, max_active=16, pack_vvvv=True, precision="fp64", conv_tol=1e-9,
+                 max_iter=100, diis_order=8, diis_start=1, refine_tol=0.0, use_graph=False):
+        o = ServerOptions()
+        lib().ccsd_server_options_default(ctypes.byref(o))
+        o.device, o.memory_budget, o.max_active, o.pack_vvvv = device, int(memory_budget), max_active, int(pack_vvvv)
+        o.solve.precision, o.solve.conv_tol, o.solve.max_iter = PREC[precision], conv_tol, max_iter
+        o.solve.diis_order, o.solve.diis_start, o.solve.refine_tol = diis_order, diis_start, refine_tol
+        o.solve.use_graph = 1 if use_graph else 0
+        s = ctypes.c_void_p()
+        _check(lib().ccsd_server_create(ctypes.byref(o), ctypes.byref(s)))
+        self.s = s
+
+    def submit_synthetic(self, o, v, nirrep=1, seed=0):
+        i = ctypes.c_int64()
+        _check(lib().ccsd_server_submit_synthetic(self.s, nirrep, o, v, seed, ctypes.byref(i)))
+        return i.value
+
+    def submit_factor(self, B, eps, vrt, occ, aux_per_irrep=None):
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        eps = np.ascontiguousarray(eps, dtype=np.float64)
+        vrt, occ = _ints(vrt), _ints(occ)
+        aux = _ints(aux_per_irrep) if aux_per_irrep is not None else None
+        i = ctypes.c_int64()
+        _check(lib().ccsd_server_submit_factor(self.s, len(vrt), _ptr(vrt), _ptr(occ), B.shape[0], _ptr(B), _ptr(eps),
+                                               _ptr(aux), ctypes.byref(i)))
+        return i.value
+
+    def poll(self, max_results=256):
+        buf = (ServerResult * max_results)()
+        n = ctypes.c_int()
+        _check(lib().ccsd_server_poll(self.s, max_results, buf, ctypes.byref(n)))
+        return [{f: getattr(buf[k], f) for f, _ in ServerResult._fields_} for k in range(n.value)]
+
+    def wait(self, timeout=3600.0):
+        _check(lib().ccsd_server_wait(self.s, timeout))
+
+    def stats(self):
+        q, a, pa = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        pb = ctypes.c_int64()
+        _check(lib().ccsd_server_stats(self.s, ctypes.byref(q), ctypes.byref(a), ctypes.byref(pb), ctypes.byref(pa)))
+        return {"queued": q.value, "active": a.value, "peak_bytes": pb.value, "peak_active": pa.value}
+
+    def close(self):
+        if self.s:
+            _check(lib().ccsd_server_destroy(self.s))
+            self.s = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -16,7 +16,8 @@ OUT = HERE / "libccsd_b200.so"
 BUILD = HERE / "_build"
 
 CU = ["kernels_fp64.cu", "kernels_split.cu", "noalloc.cu"]
-CPP = ["context.cpp", "planner.cpp", "solver.cpp", "hbuild.cpp", "fcidump.cpp", "capi.cpp", "synth.cpp", "split_exec.cpp"]
+CPP = ["context.cpp", "planner.cpp", "solver.cpp", "hbuild.cpp", "fcidump.cpp", "capi.cpp", "synth.cpp", "split_exec.cpp",
+       "server.cpp"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -17,6 +17,8 @@ namespace ccsd {
 Context::Context(int dev, cudaStream_t s) : device(dev), stream(s) {
     host_only = device < 0;
     if (const char* e = std::getenv("CCSD_SPLIT_ALL")) split_routing = e[0] == '1' ? CCSD_SPLIT_ROUTE_ALL : split_routing;
+    // CCSD_FP64_TILED=1: every FP64 product on the tiled DMMA kernel (coverage tests)
+    if (const char* e = std::getenv("CCSD_FP64_TILED")) fp64_tiled_only = e[0] == '1';
     if (!host_only) {
         CCSD_CUDA(cudaSetDevice(device));
         if (!stream) {
@@ -52,6 +54,7 @@ Context::~Context() {
         cudaEventDestroy(p.second.second);
     }
     for (auto e : event_pool) cudaEventDestroy(e);
+    kern::release_stream_buffers(stream);
     if (own_stream) cudaStreamDestroy(stream);
 }
 
@@ -337,7 +340,7 @@ void Context::upload(Plan& p) {
     // split-K workspace of the FP64 GEMM, grown before any capture
     int64_t need = 0;
     for (auto& g : p.gemms) {
-        int ks = kern::fp64_ksplit(g.M, g.N, g.K);
+        int ks = kern::fp64_ksplit(g.M, g.N, g.K, !fp64_tiled_only);
         if (ks > 1) need = std::max<int64_t>(need, (int64_t)ks * g.M * g.N);
     }
     if (need > splitk_elems) {
@@ -415,6 +418,7 @@ void Context::run_gemm(Plan& p, GemmStep& g) {
     a.b_kcontig = g.b_kcontig;
     a.ws = splitk_ws;
     a.ws_elems = splitk_elems;
+    a.skinny_ok = !fp64_tiled_only;
     if (precision == CCSD_PREC_SPLIT && kern::split_supported()) {
         run_split_gemm(g, a);
     } else {

@@ -210,6 +210,7 @@ public:
     int precision = CCSD_PREC_FP64;
     int slices = 0;
     int split_routing = CCSD_SPLIT_ROUTE_AUTO;  // which contractions take the split kernel
+    bool fp64_tiled_only = false;      // keep skinny FP64 products on the tiled kernel
     int64_t split_launches = 0;        // split-BF16 GEMMs issued (host count)
     double* d_scalar = nullptr;        // device accumulator for dots
     kern::SplitWorkspace split_ws;     // scratch for split-BF16 GEMMs

@@ -24,10 +24,12 @@ struct GemmArgs {
     // and are folded in a fixed order before the scatter into C
     double* ws = nullptr;
     int64_t ws_elems = 0;
+    // products with an extent <= 32 may take the skinny kernel (false: the tiled kernel only)
+    bool skinny_ok = true;
 };
 
 // K-ranges the FP64 GEMM splits a contraction into (1 = none); ws needs ksplit*M*N doubles
-int fp64_ksplit(int M, int N, int K);
+int fp64_ksplit(int M, int N, int K, bool skinny_ok = true);
 
 // native FP64 tensor-core (DMMA) GETT kernel
 void gemm_fp64(const GemmArgs& g, cudaStream_t s);
@@ -161,6 +163,8 @@ void eri_gather(const EriGatherArgs& a, const double* eri, cudaStream_t s);
 
 int64_t launch_count();
 void reset_launch_count();
+// free the reduction scratch kept for a stream (before the stream is destroyed)
+void release_stream_buffers(cudaStream_t s);
 
 }  // namespace kern
 }  // namespace ccsd

@@ -6,9 +6,11 @@
 // i.e. a GEMM whose operands are gathered straight from the stored tensor blocks
 // through per-dimension offset tables (no separate transpose pass), and whose
 // epilogue scatters into the output block, once per antisymmetric image.
+#include <atomic>
 #include <cstdint>
 #include <map>
 #include <mutex>
+#include <set>
 #include <utility>
 #include <algorithm>
 #include <stdexcept>
@@ -19,10 +21,21 @@
 namespace ccsd {
 namespace kern {
 
-int64_t g_launches = 0;
-int64_t launch_count() { return g_launches; }
+std::atomic<int64_t> g_launches{0};
+int64_t launch_count() { return g_launches.load(); }
 void reset_launch_count() { g_launches = 0; }
 #define COUNT_LAUNCH() (g_launches++)
+
+// dynamic shared memory above 48 KiB must be opted into once per kernel and device;
+// contexts on several host threads may launch the same kernel first
+void set_smem_once(const void* kernel, int bytes) {
+    static std::mutex mu;
+    static std::set<std::pair<const void*, int>> done;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(mu);
+    if (done.insert({kernel, dev}).second) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
 
 // ---------------------------------------------------------------------------
 // FP64 DMMA gather-GEMM
@@ -209,15 +222,241 @@ __global__ void splitk_fold_kernel(GemmArgs g, int ks) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Skinny FP64 product: one small extent (<= 32) against a long operand.
+//   C[Cr_v[r] + Cs_w[s]] += sign_vw * alpha * sum_k L[Lr[r] + Lk[k]] * S[Sk[k] + Sn[s]]
+// The long operand L streams through shared memory in TM x KC tiles (cp.async, three
+// stages, coalesced along whichever of r / k is contiguous); the small operand's KC x 8*NT
+// tile is read by every thread as a broadcast.  Each thread keeps 4 rows x 8 columns in
+// registers (CUDA-core FP64 FMA: on this part the FP64 tensor rate is no higher, and a
+// 128x64 tensor tile would be mostly padding).  A short long-extent splits K over
+// gridDim.z into ws[z][r][s], folded in a fixed order.
+// ---------------------------------------------------------------------------
+struct SkinnyArgs {
+    const double* L = nullptr;
+    const double* S = nullptr;
+    double* C = nullptr;
+    const int64_t *Lr = nullptr, *Lk = nullptr, *Sk = nullptr, *Sn = nullptr;
+    const int64_t* Cr[2] = {nullptr, nullptr};
+    const int64_t* Cs[2] = {nullptr, nullptr};
+    int R = 0, NS = 0, K = 0, nvr = 1, nvs = 1;
+    double vsign[4] = {1, 1, 1, 1};   // [vr * nvs + vs]
+    double alpha = 0;
+    double* ws = nullptr;
+};
+
+constexpr int SK_THREADS = 256, SK_STAGES = 3, SK_RPT = 4, SK_TILE = 4096;   // TM * KC doubles per stage
+
+template <int NT>
+struct SkinnyShape {
+    static constexpr int TX = SK_THREADS / NT;     // threads along r
+    static constexpr int TM = SK_RPT * TX;         // rows per CTA
+    static constexpr int KC = SK_TILE / TM;        // k per stage
+    static constexpr int LDA = TM + 1;             // As[k][r], odd pitch
+    static constexpr int LDB = 8 * NT;             // Bs[k][s]
+    static constexpr size_t bytes = (size_t)SK_STAGES * (KC * LDA + KC * LDB) * sizeof(double) + TM * sizeof(int64_t);
+};
+
+template <int NT, bool LK>
+__global__ void __launch_bounds__(SK_THREADS, 1) skinny_kernel(SkinnyArgs g) {
+    using Sh = SkinnyShape<NT>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* As = reinterpret_cast<double*>(smem_raw);
+    double* Bs = As + SK_STAGES * Sh::KC * Sh::LDA;
+    int64_t* sLr = reinterpret_cast<int64_t*>(Bs + SK_STAGES * Sh::KC * Sh::LDB);
+
+    const int tid = threadIdx.x;
+    const int tx = tid % Sh::TX, ty = tid / Sh::TX;
+    const int r0 = blockIdx.x * Sh::TM;
+    for (int i = tid; i < Sh::TM; i += SK_THREADS) sLr[i] = (r0 + i < g.R) ? g.Lr[r0 + i] : 0;
+    __syncthreads();
+
+    const int kchunks_all = (g.K + Sh::KC - 1) / Sh::KC;
+    const int per_split = (kchunks_all + gridDim.z - 1) / gridDim.z;
+    const int kc0 = blockIdx.z * per_split;
+    const int kchunks = max(0, min(kchunks_all, kc0 + per_split) - kc0);
+
+    auto load_stage = [&](int stage, int kc) {
+        const int k0 = kc * Sh::KC;
+        double* as = As + stage * Sh::KC * Sh::LDA;
+        double* bs = Bs + stage * Sh::KC * Sh::LDB;
+#pragma unroll
+        for (int i = 0; i < SK_TILE / SK_THREADS; i++) {
+            const int e = tid + i * SK_THREADS;
+            int r, k;
+            if (LK) { k = e % Sh::KC; r = e / Sh::KC; }
+            else    { r = e % Sh::TM; k = e / Sh::TM; }
+            const bool ok = (r0 + r < g.R) && (k0 + k < g.K);
+            const double* src = ok ? g.L + sLr[r] + __ldg(g.Lk + k0 + k) : g.L;
+            cp_async8(as + k * Sh::LDA + r, src, ok);
+        }
+        for (int e = tid; e < Sh::KC * Sh::LDB; e += SK_THREADS) {
+            const int s = e % Sh::LDB, k = e / Sh::LDB;
+            const bool ok = (s < g.NS) && (k0 + k < g.K);
+            const double* src = ok ? g.S + __ldg(g.Sn + s) + __ldg(g.Sk + k0 + k) : g.S;
+            cp_async8(bs + k * Sh::LDB + s, src, ok);
+        }
+    };
+
+    double acc[SK_RPT][8];
+#pragma unroll
+    for (int i = 0; i < SK_RPT; i++)
+#pragma unroll
+        for (int j = 0; j < 8; j++) acc[i][j] = 0.0;
+
+#pragma unroll
+    for (int st = 0; st < SK_STAGES - 1; st++) {
+        if (st < kchunks) load_stage(st, kc0 + st);
+        cp_commit();
+    }
+    for (int c = 0; c < kchunks; c++) {
+        cp_wait<SK_STAGES - 2>();
+        __syncthreads();
+        {
+            const int nc = c + SK_STAGES - 1;
+            if (nc < kchunks) load_stage(nc % SK_STAGES, kc0 + nc);
+            cp_commit();
+        }
+        const double* as = As + (c % SK_STAGES) * Sh::KC * Sh::LDA;
+        const double* bs = Bs + (c % SK_STAGES) * Sh::KC * Sh::LDB + ty * 8;
+#pragma unroll 4
+        for (int k = 0; k < Sh::KC; k++) {
+            double a[SK_RPT], b[8];
+#pragma unroll
+            for (int i = 0; i < SK_RPT; i++) a[i] = as[k * Sh::LDA + tx + i * Sh::TX];
+#pragma unroll
+            for (int j = 0; j < 8; j += 2) {
+                const double2 v = *reinterpret_cast<const double2*>(bs + k * Sh::LDB + j);
+                b[j] = v.x;
+                b[j + 1] = v.y;
+            }
+#pragma unroll
+            for (int i = 0; i < SK_RPT; i++)
+#pragma unroll
+                for (int j = 0; j < 8; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+    }
+    cp_wait<0>();
+
+    if (gridDim.z > 1) {
+        double* wz = g.ws + (int64_t)blockIdx.z * g.R * g.NS;
+#pragma unroll
+        for (int i = 0; i < SK_RPT; i++) {
+            const int r = r0 + tx + i * Sh::TX;
+            if (r >= g.R) continue;
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int s = ty * 8 + j;
+                if (s < g.NS) wz[(int64_t)r * g.NS + s] = acc[i][j];
+            }
+        }
+        return;
+    }
+#pragma unroll
+    for (int i = 0; i < SK_RPT; i++) {
+        const int r = r0 + tx + i * Sh::TX;
+        if (r >= g.R) continue;
+        int64_t cr[2];
+        cr[0] = g.Cr[0][r];
+        cr[1] = g.nvr > 1 ? g.Cr[1][r] : 0;
+#pragma unroll
+        for (int j = 0; j < 8; j++) {
+            const int s = ty * 8 + j;
+            if (s >= g.NS) continue;
+            const double v = g.alpha * acc[i][j];
+            for (int a = 0; a < g.nvr; a++)
+                for (int b = 0; b < g.nvs; b++) g.C[cr[a] + g.Cs[b][s]] += g.vsign[a * g.nvs + b] * v;
+        }
+    }
+}
+
+__global__ void skinny_fold_kernel(SkinnyArgs g, int ks) {
+    const int64_t rs = (int64_t)g.R * g.NS;
+    for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < rs; l += (int64_t)gridDim.x * blockDim.x) {
+        double sum = 0.0;
+        for (int z = 0; z < ks; z++) sum += g.ws[z * rs + l];
+        const int r = (int)(l / g.NS), s = (int)(l % g.NS);
+        const double v = g.alpha * sum;
+        for (int a = 0; a < g.nvr; a++)
+            for (int b = 0; b < g.nvs; b++) g.C[g.Cr[a][r] + g.Cs[b][s]] += g.vsign[a * g.nvs + b] * v;
+    }
+}
+
+// n-groups of 8 for a small extent (0: not a skinny product)
+int skinny_groups(int M, int N) {
+    const int small = std::min(M, N);
+    if (small > 32) return 0;
+    return small <= 8 ? 1 : (small <= 16 ? 2 : 4);
+}
+
+int skinny_tm(int nt) { return SK_RPT * (SK_THREADS / nt); }
+
+// K-ranges for the skinny kernel: about two waves of CTAs, at least 16 k-chunks each
+int skinny_ksplit(int R, int K, int nt) {
+    const int tm = skinny_tm(nt), kc = SK_TILE / tm;
+    const int64_t tiles = (R + tm - 1) / tm;
+    if (tiles >= 2 * 148) return 1;
+    const int64_t kchunks = (K + kc - 1) / kc;
+    int64_t ks = (2 * 148 + tiles - 1) / tiles;
+    ks = std::min<int64_t>(ks, kchunks / 16);
+    ks = std::min<int64_t>(ks, 1024);
+    return (int)std::max<int64_t>(ks, 1);
+}
+
+template <int NT, bool LK>
+void launch_skinny_t(const SkinnyArgs& a, int ks, cudaStream_t s) {
+    using Sh = SkinnyShape<NT>;
+    set_smem_once((const void*)skinny_kernel<NT, LK>, (int)Sh::bytes);
+    dim3 grid((a.R + Sh::TM - 1) / Sh::TM, 1, ks);
+    skinny_kernel<NT, LK><<<grid, SK_THREADS, Sh::bytes, s>>>(a);
+}
+
+void launch_skinny(const GemmArgs& g, int nt, cudaStream_t s) {
+    SkinnyArgs a;
+    const bool long_a = g.M >= g.N;
+    bool lk;
+    a.C = g.C;
+    a.alpha = g.alpha;
+    a.K = g.K;
+    if (long_a) {
+        a.L = g.A; a.Lr = g.Am; a.Lk = g.Ak; a.S = g.B; a.Sk = g.Bk; a.Sn = g.Bn;
+        a.R = g.M; a.NS = g.N; a.nvr = g.nvm; a.nvs = g.nvn;
+        for (int v = 0; v < 2; v++) { a.Cr[v] = g.Cm[v]; a.Cs[v] = g.Cn[v]; }
+        for (int i = 0; i < 4; i++) a.vsign[i] = g.vsign[i];
+        lk = g.a_kcontig;
+    } else {
+        a.L = g.B; a.Lr = g.Bn; a.Lk = g.Bk; a.S = g.A; a.Sk = g.Ak; a.Sn = g.Am;
+        a.R = g.N; a.NS = g.M; a.nvr = g.nvn; a.nvs = g.nvm;
+        for (int v = 0; v < 2; v++) { a.Cr[v] = g.Cn[v]; a.Cs[v] = g.Cm[v]; }
+        for (int r = 0; r < g.nvn; r++)
+            for (int c = 0; c < g.nvm; c++) a.vsign[r * g.nvm + c] = g.vsign[c * g.nvn + r];
+        lk = g.b_kcontig;
+    }
+    int ks = skinny_ksplit(a.R, a.K, nt);
+    if (!g.ws || (int64_t)ks * a.R * a.NS > g.ws_elems) ks = 1;
+    a.ws = g.ws;
+    switch (nt * 2 + (lk ? 1 : 0)) {
+        case 2: launch_skinny_t<1, false>(a, ks, s); break;
+        case 3: launch_skinny_t<1, true>(a, ks, s); break;
+        case 4: launch_skinny_t<2, false>(a, ks, s); break;
+        case 5: launch_skinny_t<2, true>(a, ks, s); break;
+        case 8: launch_skinny_t<4, false>(a, ks, s); break;
+        default: launch_skinny_t<4, true>(a, ks, s); break;
+    }
+    COUNT_LAUNCH();
+    if (ks > 1) {
+        const int64_t rs = (int64_t)a.R * a.NS;
+        const int nb = (int)std::min<int64_t>((rs + 255) / 256, 148 * 16);
+        skinny_fold_kernel<<<nb, 256, 0, s>>>(a, ks);
+        COUNT_LAUNCH();
+    }
+}
+
 template <bool AK, bool BKc>
 void launch_fp64(const GemmArgs& g, cudaStream_t s) {
     using S = Smem<AK, BKc>;
-    static bool configured = false;
-    if (!configured) {
-        cudaFuncSetAttribute(gemm_fp64_kernel<AK, BKc>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::bytes);
-        configured = true;
-    }
-    int ks = fp64_ksplit(g.M, g.N, g.K);
+    set_smem_once((const void*)gemm_fp64_kernel<AK, BKc>, (int)S::bytes);
+    int ks = fp64_ksplit(g.M, g.N, g.K, false);
     if (!g.ws || (int64_t)ks * g.M * g.N > g.ws_elems) ks = 1;
     if ((g.M + BM - 1) / BM > 65535) throw std::runtime_error("FP64 GEMM: M too large for the grid");
     dim3 grid((g.N + BN - 1) / BN, (g.M + BM - 1) / BM, ks);
@@ -235,7 +474,8 @@ void launch_fp64(const GemmArgs& g, cudaStream_t s) {
 
 // Few output tiles and a long K: split K so that about two waves of CTAs stream the
 // operands; every split keeps at least 512 k.
-int fp64_ksplit(int M, int N, int K) {
+int fp64_ksplit(int M, int N, int K, bool skinny_ok) {
+    if (const int nt = skinny_ok ? skinny_groups(M, N) : 0) return skinny_ksplit(std::max(M, N), K, nt);
     const int64_t tiles = (int64_t)((M + BM - 1) / BM) * ((N + BN - 1) / BN);
     const int ktiles = (K + BK - 1) / BK;
     if (tiles >= 148) return 1;
@@ -247,6 +487,10 @@ int fp64_ksplit(int M, int N, int K) {
 
 void gemm_fp64(const GemmArgs& g, cudaStream_t s) {
     if (g.M <= 0 || g.N <= 0 || g.K <= 0) return;
+    if (const int nt = g.skinny_ok ? skinny_groups(g.M, g.N) : 0) {
+        launch_skinny(g, nt, s);
+        return;
+    }
     if (g.a_kcontig) {
         if (g.b_kcontig) launch_fp64<true, true>(g, s);
         else launch_fp64<true, false>(g, s);
@@ -462,19 +706,33 @@ __global__ void lincomb_kernel(double* __restrict__ out1, int64_t n1, double* __
 // stream overwrites them.  Buffers live until process exit.
 }  // namespace
 
+namespace {
+std::mutex g_partial_mu;
+std::map<std::pair<int, cudaStream_t>, double*> g_partial;
+}  // namespace
+
 double* partial_buffer(cudaStream_t s) {
-    static std::mutex mu;
-    static std::map<std::pair<int, cudaStream_t>, double*> bufs;
     int dev = 0;
     cudaGetDevice(&dev);
-    std::lock_guard<std::mutex> lock(mu);
+    std::lock_guard<std::mutex> lock(g_partial_mu);
     auto key = std::make_pair(dev, s);
-    auto it = bufs.find(key);
-    if (it != bufs.end()) return it->second;
+    auto it = g_partial.find(key);
+    if (it != g_partial.end()) return it->second;
     double* p = nullptr;
     cudaMalloc(&p, sizeof(double) * 148 * 16 * 16);
-    bufs[key] = p;
+    g_partial[key] = p;
     return p;
+}
+
+void release_stream_buffers(cudaStream_t s) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::lock_guard<std::mutex> lock(g_partial_mu);
+    auto it = g_partial.find(std::make_pair(dev, s));
+    if (it == g_partial.end()) return;
+    cudaStreamSynchronize(s);
+    cudaFree(it->second);
+    g_partial.erase(it);
 }
 
 void sum_strided(const double* A, double* C, const StridedArgs& a, double alpha, cudaStream_t s) {

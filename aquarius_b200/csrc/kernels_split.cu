@@ -25,6 +25,7 @@
 //               offset tables at the end.
 // Every mbarrier wait is bounded (about 2 s); on expiry the kernel records an error
 // code, stops issuing work and returns after releasing its TMEM.
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <map>
@@ -41,8 +42,9 @@
 namespace ccsd {
 namespace kern {
 
-extern int64_t g_launches;
+extern std::atomic<int64_t> g_launches;
 double* partial_buffer(cudaStream_t s);
+void set_smem_once(const void* kernel, int bytes);
 
 namespace split {
 
@@ -467,16 +469,13 @@ int* error_flag() {
 }  // namespace split
 
 bool split_supported() {
-    static int cached = -1;
-    if (cached < 0) {
+    static const bool ok = [] {
         int dev = 0;
         cudaDeviceProp prop;
-        cached = (cudaGetDevice(&dev) == cudaSuccess && cudaGetDeviceProperties(&prop, dev) == cudaSuccess &&
-                  prop.major == 10 && split::encode_fn() != nullptr)
-                     ? 1
-                     : 0;
-    }
-    return cached == 1;
+        return cudaGetDevice(&dev) == cudaSuccess && cudaGetDeviceProperties(&prop, dev) == cudaSuccess &&
+               prop.major == 10 && split::encode_fn() != nullptr;
+    }();
+    return ok;
 }
 
 int split_rows_pad(int rows) { return (rows + split::BM - 1) / split::BM * split::BM; }
@@ -503,13 +502,7 @@ void gemm_split(const SlicedOperand& a, const SlicedOperand& b, int M, int N, in
                 cudaStream_t s) {
     using namespace split;
     (void)K;
-    static bool configured[64] = {false};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (!configured[dev]) {
-        cudaFuncSetAttribute(split_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES);
-        configured[dev] = true;
-    }
+    set_smem_once((const void*)split_gemm_kernel, (int)SMEM_BYTES);
     CUtensorMap ma, mb;
     make_map(&ma, a.data, NSLICE * a.rows, a.kpad);
     make_map(&mb, b.data, NSLICE * b.rows, b.kpad);

@@ -470,11 +470,19 @@ void Solver::iterate_async() {
 }
 
 void Solver::read_status() {
+    post_status();
+    CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
+    check_status();
+}
+
+void Solver::post_status() {
     CCSD_CUDA(cudaMemcpyAsync(h_red, d_red, 2 * sizeof(double), cudaMemcpyDeviceToHost, ctx.stream));
     if (opts.diis_order > 1) {
         CCSD_CUDA(cudaMemcpyAsync(h_state, d_state, 8 * sizeof(int), cudaMemcpyDeviceToHost, ctx.stream));
     }
-    CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+void Solver::check_status() {
     energy = h_red[0];
     conv = h_red[1];
     if (opts.precision == CCSD_PREC_SPLIT) {

@@ -51,6 +51,10 @@ public:
     void iterate(double* e, double* c);
     void iterate_async();
     void read_status();
+    // read_status in two halves: queue the copies of energy / residual / DIIS state to
+    // the host on the context stream, and, once the stream has passed them, check them
+    void post_status();
+    void check_status();
     int run(double* e, double* c, int* it);
 
 private:

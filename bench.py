@@ -171,6 +171,70 @@ def run_reference(args):
     return 0
 
 
+def serve_requests(n, seed):
+    """The serving workload's request mix: o ~ U{6..32}, v = round(o * U[6, 9]), C1 or
+    D2h with p = 0.5 (D2h needs one occupied orbital per irrep: o < 8 stays C1), own seed."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        o = int(rng.integers(6, 33))
+        v = int(round(o * rng.uniform(6.0, 9.0)))
+        h = 8 if (rng.random() < 0.5 and o >= 8) else 1
+        out.append((o, v, h, 1000 + k))
+    return out
+
+
+def serve(A, n_req, rate, seed, precision, log_each=False):
+    """Poisson arrivals at `rate` req/s into the serving loop; time-to-converged per request."""
+    reqs = serve_requests(n_req, seed)
+    gaps = np.random.default_rng(seed + 1).exponential(1.0 / rate, size=n_req)
+    srv = A.Server(0, max_active=16, precision=precision, conv_tol=1e-9, max_iter=100, diis_order=DIIS_ORDER,
+                   refine_tol=1e-7 if precision == "split" else 0.0)
+    t0 = time.perf_counter()
+    t = 0.0
+    ids = {}
+    for (o, v, h, s), g in zip(reqs, gaps):
+        t += g
+        dt = t0 + t - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        ids[srv.submit_synthetic(o, v, nirrep=h, seed=s)] = (o, v, h, s)
+    srv.wait(3600)
+    makespan = time.perf_counter() - t0
+    res = srv.poll(n_req)
+    st = srv.stats()
+    srv.close()
+    ttc = np.array([r["t_done"] - r["t_submit"] for r in res])
+    iters = sum(r["iterations"] for r in res)
+    flops = sum(r["iterations"] * r["flops_per_iter"] for r in res)
+    bad = [r for r in res if r["status"] != 0]
+    if log_each:
+        for r in sorted(res, key=lambda r: r["id"]):
+            o, v, h, s = ids[r["id"]]
+            log(f"[serve] id={r['id']:3d} o={o:2d} v={v:3d} nirrep={h} status={r['status']} it={r['iterations']:3d} "
+                f"wait={r['t_admit'] - r['t_submit']:6.2f}s ttc={r['t_done'] - r['t_submit']:6.2f}s "
+                f"bytes={r['device_bytes'] / 1e9:6.1f}GB")
+    return {"requests": n_req, "rate_req_s": rate, "precision": precision,
+            "p50_s": float(np.percentile(ttc, 50)), "p99_s": float(np.percentile(ttc, 99)),
+            "mean_s": float(ttc.mean()), "makespan_s": makespan, "iterations": iters,
+            "aggregate_iters_per_s": iters / makespan, "aggregate_tflops": flops / makespan / 1e12,
+            "peak_active": st["peak_active"], "peak_bytes_gb": st["peak_bytes"] / 1e9, "failed": len(bad),
+            "mix": "o~U{6..32}, v=round(o*U[6,9]), C1/D2h p=0.5 (o<8 stays C1), per-request seed"}
+
+
+def run_serve(args):
+    import aquarius_b200 as A
+    prec = args.precision if args.precision != "auto" else "split"
+    lines = []
+    for rate in args.rates:
+        r = serve(A, args.requests, rate, args.serve_seed, prec, log_each=True)
+        line = {"metric": "CCSD serving time-to-converged", "value": r["p50_s"], "unit": "s",
+                "higher_is_better": False, "n_gpus": 1, "data": "synthetic", **r}
+        print(json.dumps(line), flush=True)
+        lines.append(line)
+    return 0
+
+
 def timed_iterations(torch, ctx, s, stream, steps, warmup, profile):
     for _ in range(warmup):
         s.iterate()
@@ -194,48 +258,60 @@ def timed_iterations(torch, ctx, s, stream, steps, warmup, profile):
     return ms, launches, prof, e, c
 
 
+# single-statement micro-benchmarks: (A shape, packed, idx, B shape, idx, C shape, idx)
+KERNELS = {
+    # particle ladder  Z2["abij"] += 1/2 VABEF["abef"] * Tau["efij"]
+    "ladder": (((2, 0), (2, 0)), True, "abef", ((2, 0), (0, 2)), "efij", ((2, 0), (0, 2)), "abij"),
+    # skinny ring piece  W(am,ei) += 1/2 VAMEF["amef"] * T1["fi"]  (N = o)
+    "skinny": (((1, 1), (2, 0)), False, "amef", ((1, 0), (0, 1)), "fi", ((1, 1), (1, 1)), "amei"),
+}
+
+
 def run_kernel(args):
-    """Micro-benchmark of one contraction kernel: the particle ladder
-    Z2["abij"] += 1/2 VABEF["abef"] * Tau["efij"] on filled tensors (no H build), so
-    that the first contraction launches of the process are the ladder's block GEMMs."""
+    """Micro-benchmark of one contraction statement on filled tensors (no H build), so
+    that the first contraction launches of the process are the statement's block GEMMs."""
     import torch
     import aquarius_b200 as A
     w = WORKLOADS[args.workload]
+    sa, packed, ia, sb, ib, sc, ic = KERNELS[args.kernel]
     stream = torch.cuda.Stream()
     ctx = A.Context(0, stream.cuda_stream)
     ctx.set_spaces(vrt=[w["v"]], occ=[w["o"]])
     if args.precision == "split":
         ctx.set_precision("split")
-    V = ctx.tensor("<ab||cd>", (2, 0), (2, 0), packed=True)
-    T = ctx.tensor("Tau", (2, 0), (0, 2))
-    Z = ctx.tensor("Z(2)", (2, 0), (0, 2))
+    V = ctx.tensor("A", *sa, packed=packed)
+    T = ctx.tensor("B", *sb)
+    Z = ctx.tensor("C", *sc)
     V.fill(0.01)
     T.fill(0.001)
     ctx.set_profiling(True)
     for _ in range(args.warmup):
-        ctx.contract(0.5, V, "abef", T, "efij", 1.0, Z, "abij")
+        ctx.contract(0.5, V, ia, T, ib, 1.0, Z, ic)
     ctx.synchronize()
     ctx.profile_report()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(args.steps):
-        ctx.contract(0.5, V, "abef", T, "efij", 1.0, Z, "abij")
+        ctx.contract(0.5, V, ia, T, ib, 1.0, Z, ic)
     ev1.record(stream)
     ev1.synchronize()
     prof = ctx.profile_report()
     ent = next(iter(prof.values()))
     tfl = ent["flops"] / (ent["ms"] * 1e-3) / 1e12
-    print(json.dumps({"kernel": "ladder", "workload": w["desc"], "precision": args.precision,
+    # operand + read-modify-write output bytes of the whole statement (FP64)
+    nbytes = 8 * (V.elements() + T.elements() + 2 * Z.elements())
+    print(json.dumps({"kernel": args.kernel, "workload": w["desc"], "precision": args.precision,
                       "ms_per_contraction": ev0.elapsed_time(ev1) / args.steps,
                       "gemm_ms": ent["ms"] / args.steps, "launches_per_contraction": ent["launches"] / args.steps,
-                      "tflops": tfl, "flops_per_contraction": ent["flops"] / args.steps}), flush=True)
+                      "tflops": tfl, "flops_per_contraction": ent["flops"] / args.steps,
+                      "gbs_algorithmic": nbytes / (ent["ms"] / args.steps * 1e-3) / 1e9}), flush=True)
     ctx.close()
     return 0
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel", default=None, choices=[None, "ladder"],
+    ap.add_argument("--kernel", default=None, choices=[None, "ladder", "skinny"],
                     help="micro-benchmark one contraction kernel instead of the iteration")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -246,10 +322,18 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64-ref", action="store_true", help="skip the native-FP64 comparison run")
+    ap.add_argument("--serve", action="store_true", help="serving sweep instead of the iteration benchmark")
+    ap.add_argument("--requests", type=int, default=256)
+    ap.add_argument("--rates", type=float, nargs="+", default=[0.5, 1, 2, 5, 10, 20])
+    ap.add_argument("--serve-seed", type=int, default=5)
+    ap.add_argument("--serve-sample", type=int, default=24,
+                    help="requests of the bounded serving run inside the default benchmark (0: none)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         return run_reference(args)
+    if args.serve:
+        return run_serve(args)
     if args.kernel:
         if args.precision == "auto":
             args.precision = "fp64"
@@ -350,6 +434,13 @@ def main():
         log(f"[bench] e2e: {iters} iterations in {t_tot:.1f}s, E={e_fin:.12f}")
     ctx.close()
 
+    # bounded serving run (the full sweep is `--serve`): Poisson arrivals at 2 req/s
+    serving = None
+    if args.serve_sample > 0 and rank == 0:
+        serving = serve(A, args.serve_sample, 2.0, args.serve_seed, prec, log_each=True)
+        log(f"[bench] serving: p50 {serving['p50_s']:.2f}s p99 {serving['p99_s']:.2f}s, "
+            f"{serving['aggregate_iters_per_s']:.1f} iter/s aggregate, peak {serving['peak_active']} active")
+
     cpu = None
     if not args.no_cpu and rank == 0:
         res = cpu_sample(args.workload, steps=1)
@@ -371,7 +462,7 @@ def main():
             "flops_per_iter": head["flops"],
             "energy": head["energy"], "conv": head["conv"],
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": head["clocks"],
-            "gpu_launches": head["launches"],
+            "gpu_launches": head["launches"], "serving": serving,
         }
         if "fp64" in results and prec != "fp64":
             f = results["fp64"]

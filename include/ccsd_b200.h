@@ -257,6 +257,48 @@ int ccsd_plan_query(int nirrep, const int* vrt_per_irrep, const int* occ_per_irr
 int ccsd_dot_batch_noalloc(void* stream, const double* x, const double* const* ys, int ny, int64_t n,
                            double* out);
 
+/* ---- serving: continuous batching of solves on one device ------------------
+ * No counterpart in the reference (it runs one solve per job).  Requests of any size
+ * are queued on submission; an admission thread takes them in arrival order as soon as
+ * their planned device bytes (ccsd_plan_query) fit in the memory budget next to the
+ * active solves and a slot is free, builds H on a context and stream of their own, and
+ * hands them to the iteration thread.  That thread keeps one iteration of every active
+ * solve in flight (stream-ordered, no host synchronisation), polls their completion
+ * events, and retires a solve when its residual is below conv_tol or max_iter is
+ * reached, freeing its memory for the next admission.  Every solve's kernels and
+ * reductions are those of a lone solve, so its result does not depend on the mix. */
+typedef struct ccsd_server_s* ccsd_server;
+typedef struct {
+    int device;
+    int64_t memory_budget;   /* bytes the active solves may hold; 0: 90% of the free memory */
+    int max_active;          /* concurrent solves; 0: 16 */
+    int pack_vvvv;
+    ccsd_options solve;      /* per-solve options (precision, conv_tol, max_iter, DIIS, ...) */
+} ccsd_server_options;
+typedef struct {
+    int64_t id;
+    int status;              /* CCSD_OK, CCSD_NOT_CONVERGED or the error of the solve */
+    int iterations;
+    double energy, mp2, conv;
+    double t_submit, t_admit, t_done;   /* seconds since the server started */
+    int64_t device_bytes;    /* planned bytes the solve was admitted with */
+    double flops_per_iter;
+} ccsd_server_result;
+void ccsd_server_options_default(ccsd_server_options* o);
+int ccsd_server_create(const ccsd_server_options* o, ccsd_server* out);
+/* a synthetic request (the seeded generator below, o and v split over nirrep irreps) */
+int ccsd_server_submit_synthetic(ccsd_server s, int nirrep, int o, int v, uint64_t seed, int64_t* id);
+/* a request from a three-index factor (copied; arguments as ccsd_hamiltonian_from_factor) */
+int ccsd_server_submit_factor(ccsd_server s, int nirrep, const int* vrt, const int* occ, int naux, const double* B,
+                              const double* eps, const int* aux_per_irrep, int64_t* id);
+/* move up to max finished results into out (non-blocking); *n receives their count */
+int ccsd_server_poll(ccsd_server s, int max, ccsd_server_result* out, int* n);
+/* block until every submitted request has finished or timeout_s passed (CCSD_ERR_TIMEOUT) */
+int ccsd_server_wait(ccsd_server s, double timeout_s);
+/* requests queued, solves active, peak bytes admitted at once, peak solves active at once */
+int ccsd_server_stats(ccsd_server s, int* queued, int* active, int64_t* peak_bytes, int* peak_active);
+int ccsd_server_destroy(ccsd_server s);
+
 /* ---- synthetic inputs (seeded; identical on every host) -------------------- */
 /* irrep sizes: Dirichlet(1.5) split of o, v and naux = 3(o+v) (aux may be NULL) */
 int ccsd_synth_irreps(uint64_t seed, int nirrep, int o, int v,

@@ -58,9 +58,13 @@ def _ctx(nirrep):
     return ctx
 
 
+@pytest.mark.parametrize("path", ["auto", "tiled"])
 @pytest.mark.parametrize("nirrep", [1, 2, 4])
 @pytest.mark.parametrize("stmt", STATEMENTS, ids=[f"{s[1]}+={s[3]}*{s[5]}" for s in STATEMENTS])
-def test_statement_matches_reference(nirrep, stmt):
+def test_statement_matches_reference(nirrep, stmt, path, monkeypatch):
+    """At these sizes every product has an extent <= 32, so "auto" runs the skinny FP64
+    kernel and "tiled" (CCSD_FP64_TILED=1) the 128x64 DMMA kernel."""
+    monkeypatch.setenv("CCSD_FP64_TILED", "1" if path == "tiled" else "0")
     cs, ic, as_, ia, bs, ib = stmt
     rng = np.random.default_rng(abs(hash((nirrep,) + stmt)) % 2**32)
     ctx = _ctx(nirrep)
