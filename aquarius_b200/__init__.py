@@ -47,7 +47,7 @@ EXPORTS = [
     "ccsd_dot_batch_noalloc", "ccsd_hamiltonian_create", "ccsd_hamiltonian_from_integrals", "ccsd_fcidump_read",
     "ccsd_hamiltonian_from_fcidump", "ccsd_ctx_set_split_routing", "ccsd_ctx_split_launches",
     "ccsd_server_options_default", "ccsd_server_create", "ccsd_server_submit_synthetic", "ccsd_server_submit_factor",
-    "ccsd_server_poll", "ccsd_server_wait", "ccsd_server_stats", "ccsd_server_destroy",
+    "ccsd_server_poll", "ccsd_server_wait", "ccsd_server_stats", "ccsd_server_destroy", "ccsd_solver_mode",
 ]
 
 
@@ -157,6 +157,7 @@ def lib():
             "ccsd_solver_run": [vp, P(dbl), P(dbl), P(ctypes.c_int)],
             "ccsd_solver_amplitudes": [vp, P(i32), P(i32)],
             "ccsd_solver_flops": [vp, P(dbl)],
+            "ccsd_solver_mode": [vp, P(ctypes.c_int), P(ctypes.c_int)],
             "ccsd_plan_query": [ctypes.c_int, vp, vp, P(Options), ctypes.c_int, P(dbl), P(i64)],
             "ccsd_dot_batch_noalloc": [vp, vp, vp, ctypes.c_int, i64, vp],
             "ccsd_synth_irreps": [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp],
@@ -658,6 +659,12 @@ class Solver:
         if code not in (CCSD_OK, 6):
             _check(code, self.ctx.c)
         return e.value, c.value, i.value
+
+    def mode(self):
+        """contraction mode of the next iteration: "fp64", "split3" or "split4\""""
+        p, n = ctypes.c_int(), ctypes.c_int()
+        _check(lib().ccsd_solver_mode(self.s, ctypes.byref(p), ctypes.byref(n)), self.ctx.c)
+        return "fp64" if p.value == 0 else f"split{n.value}"
 
     def flops(self):
         x = ctypes.c_double()

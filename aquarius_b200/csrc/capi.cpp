@@ -178,7 +178,7 @@ int ccsd_ctx_set_precision(ccsd_ctx ctx, int precision, int slices) {
         if (precision != CCSD_PREC_FP64 && precision != CCSD_PREC_SPLIT) throw Error(CCSD_ERR_ARG, "bad precision");
         if (precision == CCSD_PREC_SPLIT && !kern::split_supported())
             throw Error(CCSD_ERR_UNSUPPORTED, "split-BF16 GEMMs need an sm_100 device");
-        if (slices < 0 || slices > 4) throw Error(CCSD_ERR_ARG, "slices must be in 0..4");
+        if (slices != 0 && slices != 3 && slices != 4) throw Error(CCSD_ERR_ARG, "slices must be 0 (default), 3 or 4");
         c->precision = precision;
         c->slices = slices;
     });
@@ -740,6 +740,14 @@ int ccsd_solver_amplitudes(ccsd_solver s, ccsd_tensor* T1, ccsd_tensor* T2) {
 int ccsd_solver_flops(ccsd_solver s, double* flops) {
     if (!s) return CCSD_ERR_ARG;
     return guarded(s->ctx, [&] { *flops = s->s->flops_per_iter; });
+}
+
+int ccsd_solver_mode(ccsd_solver s, int* precision, int* slices) {
+    if (!s) return CCSD_ERR_ARG;
+    return guarded(s->ctx, [&] {
+        if (precision) *precision = s->s->ctx.precision;
+        if (slices) *slices = s->s->ctx.split_slices();
+    });
 }
 
 }  // extern "C"

@@ -19,6 +19,8 @@ Context::Context(int dev, cudaStream_t s) : device(dev), stream(s) {
     if (const char* e = std::getenv("CCSD_SPLIT_ALL")) split_routing = e[0] == '1' ? CCSD_SPLIT_ROUTE_ALL : split_routing;
     // CCSD_FP64_TILED=1: every FP64 product on the tiled DMMA kernel (coverage tests)
     if (const char* e = std::getenv("CCSD_FP64_TILED")) fp64_tiled_only = e[0] == '1';
+    // CCSD_GROUP_GEMMS=0: every block contraction in a launch of its own (coverage tests)
+    if (const char* e = std::getenv("CCSD_GROUP_GEMMS")) group_gemms = e[0] != '0';
     if (!host_only) {
         CCSD_CUDA(cudaSetDevice(device));
         if (!stream) {
@@ -342,6 +344,10 @@ void Context::upload(Plan& p) {
     for (auto& g : p.gemms) {
         int ks = kern::fp64_ksplit(g.M, g.N, g.K, !fp64_tiled_only);
         if (ks > 1) need = std::max<int64_t>(need, (int64_t)ks * g.M * g.N);
+        for (int ns : {3, 4}) {   // split-precision GEMMs share the space
+            const int kss = kern::split_ksplit(g.M, g.N, g.K, ns);
+            if (kss > 1) need = std::max<int64_t>(need, (int64_t)kss * g.M * g.N);
+        }
     }
     if (need > splitk_elems) {
         if (splitk_ws) dfree(splitk_ws, splitk_elems * sizeof(double));
@@ -357,6 +363,17 @@ void Context::upload(Plan& p) {
         g.dBn = upload_table(*this, g.hBn);
         for (int v = 0; v < g.nvm; v++) g.dCm[v] = upload_table(*this, g.hCm[v]);
         for (int v = 0; v < g.nvn; v++) g.dCn[v] = upload_table(*this, g.hCn[v]);
+        // k tables that are arithmetic progressions let the kernels compute the offsets
+        auto affine = [](const std::vector<int64_t>& t, int64_t& b0, int64_t& st) {
+            if (t.empty()) return false;
+            b0 = t[0];
+            st = t.size() > 1 ? t[1] - t[0] : 0;
+            for (size_t k = 2; k < t.size(); k++)
+                if (t[k] - t[k - 1] != st) return false;
+            return true;
+        };
+        g.ak_affine = affine(g.hAk, g.ak0, g.ak_step);
+        g.bk_affine = affine(g.hBk, g.bk0, g.bk_step);
     }
     // tables are uploaded from pageable host memory; make sure the copies have been
     // staged before the host vectors could change
@@ -384,6 +401,15 @@ void Context::release(Plan& p) {
             fr(g.dCn[v], g.hCn[v].size());
         }
     }
+    for (auto& kv : p.schedules)
+        for (auto& r : kv.second.runs)
+            for (auto& l : r.launches) {
+                if (l.d_probs) dfree(l.d_probs, l.nprob * sizeof(kern::GemmArgs));
+                if (l.d_tile_start) dfree(l.d_tile_start, l.nprob * sizeof(int));
+                if (l.d_desc) dfree(l.d_desc, l.desc_bytes);
+                if (l.d_chunks) dfree(l.d_chunks, l.nprob * sizeof(int64_t));
+            }
+    p.schedules.clear();
 }
 
 double* Context::data_of(Plan& p, int h) {
@@ -395,6 +421,15 @@ double* Context::data_of(Plan& p, int h) {
 }
 
 void Context::run_gemm(Plan& p, GemmStep& g) {
+    kern::GemmArgs a = gemm_args(p, g);
+    if (precision == CCSD_PREC_SPLIT && kern::split_supported()) {
+        run_split_gemm(g, a);
+    } else {
+        kern::gemm_fp64(a, stream);
+    }
+}
+
+kern::GemmArgs Context::gemm_args(Plan& p, const GemmStep& g) {
     kern::GemmArgs a;
     a.A = data_of(p, g.tA);
     a.B = data_of(p, g.tB);
@@ -419,18 +454,312 @@ void Context::run_gemm(Plan& p, GemmStep& g) {
     a.ws = splitk_ws;
     a.ws_elems = splitk_elems;
     a.skinny_ok = !fp64_tiled_only;
-    if (precision == CCSD_PREC_SPLIT && kern::split_supported()) {
-        run_split_gemm(g, a);
-    } else {
-        kern::gemm_fp64(a, stream);
+    a.ak_affine = g.ak_affine;
+    a.bk_affine = g.bk_affine;
+    a.ak0 = g.ak0;
+    a.ak_step = g.ak_step;
+    a.bk0 = g.bk0;
+    a.bk_step = g.bk_step;
+    return a;
+}
+
+// Grouped schedule of a plan under the current routing.  A run is a maximal sequence of
+// GEMM steps of one statement: they read only the statement's operands and write its
+// output (or the plan scratch), so the only hazard among them is two writes to one
+// output block.  Each step gets a level one above the last level that wrote any of its
+// output blocks; within a level the small FP64 products (fewer than a wave of tiles, no
+// split-K) become one grouped launch per operand contiguity, the rest launch alone.
+// Every output block thus receives its contributions in plan order.  Runs of permuted
+// sums (antisymmetriser images, copies) and of block scalings of one statement are
+// batched the same way, one launch per level.
+RunSchedule& Context::schedule(Plan& p) {
+    const int key = (precision == CCSD_PREC_SPLIT ? 1 : 0) | (split_routing << 1) | (fp64_tiled_only ? 4 : 0) |
+                    (group_gemms ? 8 : 0);
+    auto it = p.schedules.find(key);
+    if (it != p.schedules.end()) return it->second;
+    RunSchedule& rs = p.schedules[key];
+    rs.run_at.assign(p.steps.size(), -1);
+    if (!group_gemms || host_only) return rs;
+    auto label_of = [&](const Step& st) -> const std::string& {
+        switch (st.kind) {
+            case Step::GEMM: return p.gemms[st.idx].label;
+            case Step::SUM: return p.sums[st.idx].label;
+            case Step::SCALE: return p.scales[st.idx].label;
+            default: {
+                static const std::string none;
+                return none;
+            }
+        }
+    };
+    size_t s = 0;
+    while (s < p.steps.size()) {
+        const Step::Kind kind = p.steps[s].kind;
+        if (kind == Step::DOT) {
+            s++;
+            continue;
+        }
+        const std::string& lab = label_of(p.steps[s]);
+        size_t e = s;
+        while (e < p.steps.size() && p.steps[e].kind == kind && label_of(p.steps[e]) == lab) e++;
+        if (e - s >= 2) {
+            if (kind == Step::GEMM) build_run(p, rs, (int)s, (int)e);
+            else build_elementwise_run(p, rs, (int)s, (int)e);
+        }
+        s = e;
     }
+    return rs;
+}
+
+void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
+    // output block of an element offset: (buffer, start of the block containing it)
+    std::map<int, std::vector<int64_t>> starts;
+    auto block_of = [&](int h, int64_t off) -> std::pair<int, int64_t> {
+        if (h == kScratch) return {h, off};   // a product region starts at its lowest offset
+        auto& v = starts[h];
+        if (v.empty()) {
+            for (auto& sc : tensor(h).cases)
+                for (auto& b : sc.blocks) v.push_back(b.offset);
+            std::sort(v.begin(), v.end());
+        }
+        auto ub = std::upper_bound(v.begin(), v.end(), off);
+        return {h, ub == v.begin() ? 0 : *(ub - 1)};
+    };
+    // small products (less than a wave of tiles; either little work or no split-K on
+    // their own) gain from sharing a launch; larger ones keep their own kernel choice
+    auto groupable = [&](const GemmStep& g) {
+        if (routes_split(g) || g.M <= 0 || g.N <= 0 || g.K <= 0) return false;
+        if (kern::fp64_tiles(g.M, g.N) >= 148) return false;
+        // a grouped tile walks the whole K range: long-K products keep their split-K launch
+        if (g.flops() < 4e8 && g.K <= 4096) return true;
+        return kern::fp64_ksplit(g.M, g.N, g.K, !fp64_tiled_only) == 1 && kern::fp64_ksplit(g.M, g.N, g.K, false) == 1;
+    };
+    std::map<std::pair<int, int64_t>, int> last;
+    std::vector<int> level(end - first, 0);
+    int maxlvl = 0;
+    int ngroupable = 0;
+    for (int i = first; i < end; i++) {
+        const GemmStep& g = p.gemms[p.steps[i].idx];
+        std::vector<std::pair<int, int64_t>> keys;
+        for (int v = 0; v < g.nvm; v++)
+            for (int w = 0; w < g.nvn; w++) {
+                if (g.hCm[v].empty() || g.hCn[w].empty()) continue;
+                const int64_t lo = *std::min_element(g.hCm[v].begin(), g.hCm[v].end()) +
+                                   *std::min_element(g.hCn[w].begin(), g.hCn[w].end());
+                keys.push_back(block_of(g.tC, lo));
+            }
+        int lvl = 0;
+        for (auto& k : keys) {
+            auto f = last.find(k);
+            if (f != last.end()) lvl = std::max(lvl, f->second + 1);
+        }
+        for (auto& k : keys) last[k] = lvl;
+        level[i - first] = lvl;
+        maxlvl = std::max(maxlvl, lvl);
+        if (groupable(g)) ngroupable++;
+    }
+    if (ngroupable < 2) return;
+    GemmRun run;
+    run.first = first;
+    run.end = end;
+    bool any_group = false;
+    for (int L = 0; L <= maxlvl; L++) {
+        std::vector<int> grp[4];
+        for (int i = first; i < end; i++) {
+            if (level[i - first] != L) continue;
+            const int gi = p.steps[i].idx;
+            const GemmStep& g = p.gemms[gi];
+            if (groupable(g)) {
+                grp[(g.a_kcontig ? 2 : 0) + (g.b_kcontig ? 1 : 0)].push_back(gi);
+            } else {
+                GemmLaunch l;
+                l.gemm = gi;
+                l.flops = g.flops();
+                run.launches.push_back(l);
+            }
+        }
+        for (int c = 0; c < 4; c++) {
+            if (grp[c].empty()) continue;
+            if (grp[c].size() == 1) {
+                GemmLaunch l;
+                l.gemm = grp[c][0];
+                l.flops = p.gemms[grp[c][0]].flops();
+                run.launches.push_back(l);
+                continue;
+            }
+            GemmLaunch l;
+            l.kind = GemmLaunch::GEMM_GROUPED;
+            l.ak = (c & 2) != 0;
+            l.bk = (c & 1) != 0;
+            std::vector<kern::GemmArgs> probs;
+            std::vector<int> tstart;
+            int tiles = 0;
+            for (int gi : grp[c]) {
+                const GemmStep& g = p.gemms[gi];
+                kern::GemmArgs a = gemm_args(p, g);
+                a.ws = nullptr;
+                a.ws_elems = 0;
+                probs.push_back(a);
+                tstart.push_back(tiles);
+                tiles += kern::fp64_tiles(g.M, g.N);
+                l.flops += g.flops();
+            }
+            l.nprob = (int)probs.size();
+            l.tiles = tiles;
+            l.d_probs = (kern::GemmArgs*)dmalloc(probs.size() * sizeof(kern::GemmArgs));
+            l.d_tile_start = (int*)dmalloc(tstart.size() * sizeof(int));
+            CCSD_CUDA(cudaMemcpyAsync(l.d_probs, probs.data(), probs.size() * sizeof(kern::GemmArgs),
+                                      cudaMemcpyHostToDevice, stream));
+            CCSD_CUDA(cudaMemcpyAsync(l.d_tile_start, tstart.data(), tstart.size() * sizeof(int),
+                                      cudaMemcpyHostToDevice, stream));
+            CCSD_CUDA(cudaStreamSynchronize(stream));   // the host vectors go out of scope
+            run.launches.push_back(l);
+            any_group = true;
+        }
+    }
+    if (!any_group) return;
+    rs.run_at[first] = (int)rs.runs.size();
+    rs.runs.push_back(std::move(run));
+}
+
+// A run of permuted sums or of scalings of one statement.  Sums read their A blocks (an
+// operand or a product region, never written in the run) and write C blocks: each gets a
+// level above the last sum into the same C block, and every level is one batched launch.
+// Scalings touch distinct blocks: one launch.
+void Context::build_elementwise_run(Plan& p, RunSchedule& rs, int first, int end) {
+    const bool is_sum = p.steps[first].kind == Step::SUM;
+    std::map<int, std::vector<int64_t>> starts;
+    auto block_of = [&](int h, int64_t off) -> std::pair<int, int64_t> {
+        if (h == kScratch) return {h, off};
+        auto& v = starts[h];
+        if (v.empty()) {
+            for (auto& sc : tensor(h).cases)
+                for (auto& b : sc.blocks) v.push_back(b.offset);
+            std::sort(v.begin(), v.end());
+        }
+        auto ub = std::upper_bound(v.begin(), v.end(), off);
+        return {h, ub == v.begin() ? 0 : *(ub - 1)};
+    };
+    std::vector<int> level(end - first, 0);
+    int maxlvl = 0;
+    if (is_sum) {
+        std::map<std::pair<int, int64_t>, int> last;
+        for (int i = first; i < end; i++) {
+            const SumStep& s = p.sums[p.steps[i].idx];
+            auto k = block_of(s.tC, s.offC);
+            auto f = last.find(k);
+            const int lvl = f == last.end() ? 0 : f->second + 1;
+            last[k] = lvl;
+            level[i - first] = lvl;
+            maxlvl = std::max(maxlvl, lvl);
+        }
+    }
+    GemmRun run;
+    run.first = first;
+    run.end = end;
+    for (int L = 0; L <= maxlvl; L++) {
+        std::vector<int> idx;
+        for (int i = first; i < end; i++)
+            if (level[i - first] == L) idx.push_back(p.steps[i].idx);
+        if (idx.empty()) continue;
+        GemmLaunch l;
+        std::vector<int64_t> cs;
+        int64_t chunks = 0;
+        auto nchunks = [](int64_t n) { return (n + kern::kBatchChunk - 1) / kern::kBatchChunk; };
+        if (is_sum) {
+            l.kind = GemmLaunch::SUM_BATCHED;
+            std::vector<kern::SumDesc> d;
+            for (int k : idx) {
+                const SumStep& s = p.sums[k];
+                kern::SumDesc x;
+                x.A = data_of(p, s.tA) + s.offA;
+                x.C = data_of(p, s.tC) + s.offC;
+                x.alpha = s.alpha;
+                x.ndim = s.ndim;
+                x.total = 1;
+                for (int q = 0; q < s.ndim; q++) {
+                    x.len[q] = s.len[q];
+                    x.sA[q] = s.sA[q];
+                    x.sC[q] = s.sC[q];
+                    x.total *= s.len[q];
+                }
+                if (x.total <= 0) continue;
+                d.push_back(x);
+                cs.push_back(chunks);
+                chunks += nchunks(x.total);
+            }
+            if (d.empty()) continue;
+            l.desc_bytes = d.size() * sizeof(kern::SumDesc);
+            l.d_desc = dmalloc(l.desc_bytes);
+            CCSD_CUDA(cudaMemcpyAsync(l.d_desc, d.data(), l.desc_bytes, cudaMemcpyHostToDevice, stream));
+            l.nprob = (int)d.size();
+        } else {
+            l.kind = GemmLaunch::SCALE_BATCHED;
+            std::vector<kern::ScaleDesc> d;
+            for (int k : idx) {
+                const ScaleStep& s = p.scales[k];
+                if (s.n <= 0) continue;
+                kern::ScaleDesc x;
+                x.X = data_of(p, s.tC) + s.off;
+                x.n = s.n;
+                x.beta = s.beta;
+                d.push_back(x);
+                cs.push_back(chunks);
+                chunks += nchunks(x.n);
+            }
+            if (d.empty()) continue;
+            l.desc_bytes = d.size() * sizeof(kern::ScaleDesc);
+            l.d_desc = dmalloc(l.desc_bytes);
+            CCSD_CUDA(cudaMemcpyAsync(l.d_desc, d.data(), l.desc_bytes, cudaMemcpyHostToDevice, stream));
+            l.nprob = (int)d.size();
+        }
+        if (chunks > INT32_MAX) throw Error(CCSD_ERR_PLAN, "batched launch too large");
+        l.chunks = chunks;
+        l.d_chunks = (int64_t*)dmalloc(cs.size() * sizeof(int64_t));
+        CCSD_CUDA(cudaMemcpyAsync(l.d_chunks, cs.data(), cs.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream));
+        CCSD_CUDA(cudaStreamSynchronize(stream));   // the host vectors go out of scope
+        run.launches.push_back(l);
+    }
+    rs.run_at[first] = (int)rs.runs.size();
+    rs.runs.push_back(std::move(run));
+}
+
+void Context::launch(Plan& p, const GemmLaunch& l, const std::string& label) {
+    auto ev = profiling ? prof_begin() : std::make_pair((cudaEvent_t) nullptr, (cudaEvent_t) nullptr);
+    switch (l.kind) {
+        case GemmLaunch::GEMM: run_gemm(p, p.gemms[l.gemm]); break;
+        case GemmLaunch::GEMM_GROUPED:
+            kern::gemm_fp64_grouped(l.d_probs, l.d_tile_start, l.nprob, l.tiles, l.ak, l.bk, stream);
+            break;
+        case GemmLaunch::SUM_BATCHED:
+            kern::sum_batched((const kern::SumDesc*)l.d_desc, l.d_chunks, l.nprob, l.chunks, stream);
+            break;
+        case GemmLaunch::SCALE_BATCHED:
+            kern::scale_batched((const kern::ScaleDesc*)l.d_desc, l.d_chunks, l.nprob, l.chunks, stream);
+            break;
+        default: throw Error(CCSD_ERR_PLAN, "bad launch record");
+    }
+    if (profiling) prof_end(ev, label, l.flops);
 }
 
 void Context::run(Plan& p, double* scalar_out, double* dot_target) {
     upload(p);
     bool zeroed = dot_target != nullptr;
     double* acc = dot_target ? dot_target : d_scalar;
-    for (auto& st : p.steps) {
+    RunSchedule* rs = host_only ? nullptr : &schedule(p);
+    for (size_t si = 0; si < p.steps.size(); si++) {
+        const Step& st = p.steps[si];
+        if (rs && rs->run_at[si] >= 0) {
+            GemmRun& r = rs->runs[rs->run_at[si]];
+            std::string lab;
+            switch (st.kind) {
+                case Step::GEMM: lab = p.gemms[st.idx].label.empty() ? "gemm" : p.gemms[st.idx].label; break;
+                case Step::SUM: lab = p.sums[st.idx].label.empty() ? "sum" : p.sums[st.idx].label; break;
+                default: lab = p.scales[st.idx].label.empty() ? "scale" : p.scales[st.idx].label; break;
+            }
+            for (auto& l : r.launches) launch(p, l, lab);
+            si = r.end - 1;
+            continue;
+        }
         switch (st.kind) {
             case Step::GEMM: {
                 GemmStep& g = p.gemms[st.idx];

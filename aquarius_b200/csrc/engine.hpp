@@ -119,6 +119,9 @@ struct GemmStep {
     int64_t *dAm = nullptr, *dAk = nullptr, *dBk = nullptr, *dBn = nullptr;
     int64_t *dCm[2] = {nullptr, nullptr}, *dCn[2] = {nullptr, nullptr};
     bool a_mcontig = false, a_kcontig = false, b_kcontig = false, b_ncontig = false;
+    // k tables found to be arithmetic progressions at upload (Ak[k] = ak0 + k * ak_step)
+    bool ak_affine = false, bk_affine = false;
+    int64_t ak0 = 0, ak_step = 0, bk0 = 0, bk_step = 0;
     double flops() const { return 2.0 * M * N * (double)K; }
     std::string label;                 // statement this block contraction came from
     int64_t split_cache_a = -1;        // keys of cached slices of constant operands
@@ -163,6 +166,34 @@ struct Step {
 // tensor handle standing for the plan's scratch product buffer
 constexpr int kScratch = -1;
 
+// One launch inside a run of consecutive steps of one kind and one statement: a single
+// step, or one batched launch over several steps whose outputs are disjoint (GEMMs on the
+// grouped tiled-FP64 kernel, permuted sums, block scalings).
+struct GemmLaunch {
+    enum Kind { GEMM, GEMM_GROUPED, SUM, SUM_BATCHED, SCALE, SCALE_BATCHED };
+    Kind kind = GEMM;
+    int gemm = -1;                     // single GEMM: index into Plan::gemms
+    int step = -1;                     // single SUM / SCALE: index into Plan::sums / scales
+    bool ak = false, bk = false;       // grouped GEMM: operand contiguity
+    int nprob = 0, tiles = 0;
+    kern::GemmArgs* d_probs = nullptr;
+    int* d_tile_start = nullptr;
+    void* d_desc = nullptr;            // batched sums / scalings: descriptors
+    int64_t* d_chunks = nullptr;       // ... and their first chunks
+    size_t desc_bytes = 0;
+    int64_t chunks = 0;
+    double flops = 0;
+};
+struct GemmRun {
+    int first = 0, end = 0;            // steps [first, end)
+    std::vector<GemmLaunch> launches;
+};
+// the grouped schedule of a plan under one routing (precision, split routing, kernels)
+struct RunSchedule {
+    std::vector<GemmRun> runs;
+    std::vector<int> run_at;           // per step: index of the run starting there, or -1
+};
+
 struct Plan {
     int64_t scratch_elems = 0;         // doubles of scratch the steps need (products X)
     double* scratch = nullptr;         // allocated at upload
@@ -172,6 +203,7 @@ struct Plan {
     std::vector<SumStep> sums;
     std::vector<ScaleStep> scales;
     std::vector<DotStep> dots;
+    std::map<int, RunSchedule> schedules;   // grouped launches per routing key (built on first run)
     double flops() const {
         double f = 0;
         for (auto& g : gemms) f += g.flops();
@@ -211,6 +243,7 @@ public:
     int slices = 0;
     int split_routing = CCSD_SPLIT_ROUTE_AUTO;  // which contractions take the split kernel
     bool fp64_tiled_only = false;      // keep skinny FP64 products on the tiled kernel
+    bool group_gemms = true;           // batch small block contractions of a statement into grouped launches
     int64_t split_launches = 0;        // split-BF16 GEMMs issued (host count)
     double* d_scalar = nullptr;        // device accumulator for dots
     kern::SplitWorkspace split_ws;     // scratch for split-BF16 GEMMs
@@ -220,7 +253,8 @@ public:
     kern::SlicedOperand ws_view[2];                        // workspace views of the current call
     double* splitk_ws = nullptr;                           // FP64 split-K partials
     int64_t splitk_elems = 0;
-    kern::SlicedOperand alloc_sliced(int rows, int K);
+    kern::SlicedOperand alloc_sliced(int rows, int K, int nslices);
+    int split_slices() const { return slices == 4 ? 4 : 3; }   // BF16 slices per operand
     void free_sliced(kern::SlicedOperand& s);
     void ensure_ws(kern::SlicedOperand& w, int rows, int K);
     void reserve_split(Plan& p);
@@ -261,6 +295,12 @@ public:
     void run_gemm(Plan& p, GemmStep& g);
     double* data_of(Plan& p, int h);
     void run_split_gemm(GemmStep& g, kern::GemmArgs& a);
+    bool routes_split(const GemmStep& g) const;   // would run_gemm send g to the split kernel
+    kern::GemmArgs gemm_args(Plan& p, const GemmStep& g);
+    RunSchedule& schedule(Plan& p);
+    void build_run(Plan& p, RunSchedule& rs, int first, int end);
+    void build_elementwise_run(Plan& p, RunSchedule& rs, int first, int end);
+    void launch(Plan& p, const GemmLaunch& l, const std::string& label);
     std::vector<int> constant_tensors;  // handles whose contents never change (sliced once)
     bool is_constant(int h) const;
 };

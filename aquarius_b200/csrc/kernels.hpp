@@ -26,6 +26,10 @@ struct GemmArgs {
     int64_t ws_elems = 0;
     // products with an extent <= 32 may take the skinny kernel (false: the tiled kernel only)
     bool skinny_ok = true;
+    // Ak / Bk as arithmetic progressions (offset0 + k * step): no table loads on the
+    // kernels' address path (the tables stay valid for the other users)
+    bool ak_affine = false, bk_affine = false;
+    int64_t ak0 = 0, ak_step = 0, bk0 = 0, bk_step = 0;
 };
 
 // K-ranges the FP64 GEMM splits a contraction into (1 = none); ws needs ksplit*M*N doubles
@@ -33,6 +37,13 @@ int fp64_ksplit(int M, int N, int K, bool skinny_ok = true);
 
 // native FP64 tensor-core (DMMA) GETT kernel
 void gemm_fp64(const GemmArgs& g, cudaStream_t s);
+// output tiles of the tiled FP64 kernel for an M x N product
+int fp64_tiles(int M, int N);
+// One launch of the tiled FP64 kernel over nprob problems (device array of GemmArgs, all
+// with the given operand contiguity, no split-K, pairwise disjoint outputs); tile_start
+// (device, nprob entries) holds each problem's first tile.
+void gemm_fp64_grouped(const GemmArgs* probs, const int* tile_start, int nprob, int total_tiles, bool a_kcontig,
+                       bool b_kcontig, cudaStream_t s);
 
 // ---- split-BF16 (Ozaki-style) path ------------------------------------------------
 // An operand sliced for the tcgen05 GEMM: rows x kpad bf16 values per slice, K-major,
@@ -58,9 +69,15 @@ int split_k_pad(int k);
 // with out.rows >= nrows padded, out.kpad >= K padded)
 void slice_rows(const double* X, const int64_t* R, const int64_t* Kt, int nrows, int K, bool kcontig,
                 int nslices, SlicedOperand& out, cudaStream_t s);
-// tcgen05 GEMM over slices; epilogue scatters into C like gemm_fp64
+// tcgen05 GEMM over slices; epilogue scatters into C like gemm_fp64.  ks > 1 splits K
+// into ks ranges whose partials go to g.ws (ks * M * N doubles) and are folded into C.
 void gemm_split(const SlicedOperand& a, const SlicedOperand& b, int M, int N, int K,
-                const GemmArgs& g, cudaStream_t s);
+                const GemmArgs& g, cudaStream_t s, int ks = 1);
+// K-ranges for a split GEMM: enough CTAs for about two waves when the output has few
+// tiles, each range at least one exact 1024-k chunk (1 = none)
+int split_ksplit(int M, int N, int K, int nslices = 3);
+// alpha * sum_z ws[z][m][n] scattered into every destination variant of g (fixed order)
+void splitk_fold(const GemmArgs& g, int ks, cudaStream_t s);
 bool split_supported();
 // nonzero if a split-GEMM wait expired (1..4 = which wait); reset clears it
 int split_error(bool reset);
@@ -165,6 +182,26 @@ int64_t launch_count();
 void reset_launch_count();
 // free the reduction scratch kept for a stream (before the stream is destroyed)
 void release_stream_buffers(cudaStream_t s);
+
+// Batched permuted sums C[perm] += alpha * A and block scalings, one launch each: the
+// problems (device arrays) must write pairwise disjoint elements; chunk_start[p] is the
+// first 2048-element chunk of problem p.
+constexpr int kBatchChunk = 2048;
+struct SumDesc {
+    const double* A = nullptr;
+    double* C = nullptr;
+    double alpha = 0;
+    int ndim = 0;
+    int64_t len[8], sA[8], sC[8];
+    int64_t total = 0;
+};
+struct ScaleDesc {
+    double* X = nullptr;
+    int64_t n = 0;
+    double beta = 1;   // 0: zero-fill
+};
+void sum_batched(const SumDesc* d, const int64_t* chunk_start, int n, int64_t chunks, cudaStream_t s);
+void scale_batched(const ScaleDesc* d, const int64_t* chunk_start, int n, int64_t chunks, cudaStream_t s);
 
 }  // namespace kern
 }  // namespace ccsd

@@ -69,9 +69,11 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
                  : "d"(a), "d"(b));
 }
 
+// One BM x BN output tile of one problem, K-range kz of nz (split-K writes raw partials
+// to g.ws[kz]).  smem_raw: the dynamic shared memory of Smem<AK, BKc>.
 template <bool AK, bool BKc>
-__global__ void __launch_bounds__(THREADS, 1) gemm_fp64_kernel(GemmArgs g) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+__device__ __forceinline__ void fp64_tile(const GemmArgs& g, const int m0, const int n0, const int kz, const int nz,
+                                          unsigned char* smem_raw) {
     using S = Smem<AK, BKc>;
     double* As = reinterpret_cast<double*>(smem_raw);
     double* Bs = As + STAGES * S::a_elems;
@@ -79,17 +81,16 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_fp64_kernel(GemmArgs g) {
     int64_t* sBn = sAm + BM;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
     const int wm = (warp & 3) * 32, wn = (warp >> 2) * 32;
 
     for (int i = tid; i < BM; i += THREADS) sAm[i] = (m0 + i < g.M) ? g.Am[m0 + i] : 0;
     for (int i = tid; i < BN; i += THREADS) sBn[i] = (n0 + i < g.N) ? g.Bn[n0 + i] : 0;
     __syncthreads();
 
-    // this CTA's K-range (split-K along gridDim.z)
+    // this CTA's K-range (split-K: range kz of nz)
     const int ktiles_all = (g.K + BK - 1) / BK;
-    const int per_split = (ktiles_all + gridDim.z - 1) / gridDim.z;
-    const int kt0 = blockIdx.z * per_split;
+    const int per_split = (ktiles_all + nz - 1) / nz;
+    const int kt0 = kz * per_split;
     const int ktiles = max(0, min(ktiles_all, kt0 + per_split) - kt0);
 
     auto load_stage = [&](int stage, int kt) {
@@ -104,7 +105,8 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_fp64_kernel(GemmArgs g) {
             if (AK) { k = e % BK; m = e / BK; }
             else    { m = e % BM; k = e / BM; }
             bool ok = (m0 + m < g.M) && (k0 + k < g.K);
-            const double* src = ok ? g.A + sAm[m] + __ldg(g.Ak + k0 + k) : g.A;
+            const double* src =
+                ok ? g.A + sAm[m] + (g.ak_affine ? g.ak0 + g.ak_step * (k0 + k) : __ldg(g.Ak + k0 + k)) : g.A;
             double* dst = AK ? as + m * LDK + k : as + k * LDMK + m;
             cp_async8(dst, src, ok);
         }
@@ -116,7 +118,8 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_fp64_kernel(GemmArgs g) {
             if (BKc) { k = e % BK; n = e / BK; }
             else     { n = e % BN; k = e / BN; }
             bool ok = (n0 + n < g.N) && (k0 + k < g.K);
-            const double* src = ok ? g.B + sBn[n] + __ldg(g.Bk + k0 + k) : g.B;
+            const double* src =
+                ok ? g.B + sBn[n] + (g.bk_affine ? g.bk0 + g.bk_step * (k0 + k) : __ldg(g.Bk + k0 + k)) : g.B;
             double* dst = BKc ? bs + n * LDK + k : bs + k * LDNK + n;
             cp_async8(dst, src, ok);
         }
@@ -166,9 +169,9 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_fp64_kernel(GemmArgs g) {
     }
     cp_wait<0>();
 
-    if (gridDim.z > 1) {
+    if (nz > 1) {
         // split-K: raw partial sums, folded by splitk_fold_kernel
-        double* wz = g.ws + (int64_t)blockIdx.z * g.M * g.N;
+        double* wz = g.ws + (int64_t)kz * g.M * g.N;
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             int m = m0 + wm + i * 8 + (lane >> 2);
@@ -209,6 +212,37 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_fp64_kernel(GemmArgs g) {
     }
 }
 
+template <bool AK, bool BKc>
+__global__ void __launch_bounds__(THREADS, 1) gemm_fp64_kernel(GemmArgs g) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    fp64_tile<AK, BKc>(g, blockIdx.y * BM, blockIdx.x * BN, blockIdx.z, gridDim.z, smem_raw);
+}
+
+// Grouped launch: one CTA per output tile of any of nprob problems whose outputs are
+// pairwise disjoint; tile_start[p] is the first tile of problem p.
+template <bool AK, bool BKc>
+__global__ void __launch_bounds__(THREADS, 1)
+    gemm_fp64_grouped_kernel(const GemmArgs* __restrict__ probs, const int* __restrict__ tile_start, int nprob) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ GemmArgs sg;
+    __shared__ int sp;
+    const int t = blockIdx.x;
+    if (threadIdx.x == 0) {
+        int lo = 0, hi = nprob - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (tile_start[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        sp = lo;
+        sg = probs[lo];
+    }
+    __syncthreads();
+    const int local = t - tile_start[sp];
+    const int tn = (sg.N + BN - 1) / BN;
+    fp64_tile<AK, BKc>(sg, (local / tn) * BM, (local % tn) * BN, 0, 1, smem_raw);
+}
+
 // fold split-K partials in a fixed order and scatter alpha * sum into every variant
 __global__ void splitk_fold_kernel(GemmArgs g, int ks) {
     const int64_t mn = (int64_t)g.M * g.N;
@@ -237,6 +271,8 @@ struct SkinnyArgs {
     const double* S = nullptr;
     double* C = nullptr;
     const int64_t *Lr = nullptr, *Lk = nullptr, *Sk = nullptr, *Sn = nullptr;
+    bool lk_affine = false, sk_affine = false;     // Lk / Sk as offset0 + k * step
+    int64_t lk0 = 0, lk_step = 0, sk0 = 0, sk_step = 0;
     const int64_t* Cr[2] = {nullptr, nullptr};
     const int64_t* Cs[2] = {nullptr, nullptr};
     int R = 0, NS = 0, K = 0, nvr = 1, nvs = 1;
@@ -254,7 +290,8 @@ struct SkinnyShape {
     static constexpr int KC = SK_TILE / TM;        // k per stage
     static constexpr int LDA = TM + 1;             // As[k][r], odd pitch
     static constexpr int LDB = 8 * NT;             // Bs[k][s]
-    static constexpr size_t bytes = (size_t)SK_STAGES * (KC * LDA + KC * LDB) * sizeof(double) + TM * sizeof(int64_t);
+    static constexpr size_t bytes =
+        (size_t)SK_STAGES * (KC * LDA + KC * LDB) * sizeof(double) + (TM + LDB) * sizeof(int64_t);
 };
 
 template <int NT, bool LK>
@@ -264,11 +301,13 @@ __global__ void __launch_bounds__(SK_THREADS, 1) skinny_kernel(SkinnyArgs g) {
     double* As = reinterpret_cast<double*>(smem_raw);
     double* Bs = As + SK_STAGES * Sh::KC * Sh::LDA;
     int64_t* sLr = reinterpret_cast<int64_t*>(Bs + SK_STAGES * Sh::KC * Sh::LDB);
+    int64_t* sSn = sLr + Sh::TM;
 
     const int tid = threadIdx.x;
     const int tx = tid % Sh::TX, ty = tid / Sh::TX;
     const int r0 = blockIdx.x * Sh::TM;
     for (int i = tid; i < Sh::TM; i += SK_THREADS) sLr[i] = (r0 + i < g.R) ? g.Lr[r0 + i] : 0;
+    for (int i = tid; i < Sh::LDB; i += SK_THREADS) sSn[i] = (i < g.NS) ? g.Sn[i] : 0;
     __syncthreads();
 
     const int kchunks_all = (g.K + Sh::KC - 1) / Sh::KC;
@@ -287,13 +326,15 @@ __global__ void __launch_bounds__(SK_THREADS, 1) skinny_kernel(SkinnyArgs g) {
             if (LK) { k = e % Sh::KC; r = e / Sh::KC; }
             else    { r = e % Sh::TM; k = e / Sh::TM; }
             const bool ok = (r0 + r < g.R) && (k0 + k < g.K);
-            const double* src = ok ? g.L + sLr[r] + __ldg(g.Lk + k0 + k) : g.L;
+            const double* src =
+                ok ? g.L + sLr[r] + (g.lk_affine ? g.lk0 + g.lk_step * (k0 + k) : __ldg(g.Lk + k0 + k)) : g.L;
             cp_async8(as + k * Sh::LDA + r, src, ok);
         }
         for (int e = tid; e < Sh::KC * Sh::LDB; e += SK_THREADS) {
             const int s = e % Sh::LDB, k = e / Sh::LDB;
             const bool ok = (s < g.NS) && (k0 + k < g.K);
-            const double* src = ok ? g.S + __ldg(g.Sn + s) + __ldg(g.Sk + k0 + k) : g.S;
+            const double* src =
+                ok ? g.S + sSn[s] + (g.sk_affine ? g.sk0 + g.sk_step * (k0 + k) : __ldg(g.Sk + k0 + k)) : g.S;
             cp_async8(bs + k * Sh::LDB + s, src, ok);
         }
     };
@@ -424,6 +465,8 @@ void launch_skinny(const GemmArgs& g, int nt, cudaStream_t s) {
         for (int v = 0; v < 2; v++) { a.Cr[v] = g.Cm[v]; a.Cs[v] = g.Cn[v]; }
         for (int i = 0; i < 4; i++) a.vsign[i] = g.vsign[i];
         lk = g.a_kcontig;
+        a.lk_affine = g.ak_affine; a.lk0 = g.ak0; a.lk_step = g.ak_step;
+        a.sk_affine = g.bk_affine; a.sk0 = g.bk0; a.sk_step = g.bk_step;
     } else {
         a.L = g.B; a.Lr = g.Bn; a.Lk = g.Bk; a.S = g.A; a.Sk = g.Ak; a.Sn = g.Am;
         a.R = g.N; a.NS = g.M; a.nvr = g.nvn; a.nvs = g.nvm;
@@ -431,6 +474,8 @@ void launch_skinny(const GemmArgs& g, int nt, cudaStream_t s) {
         for (int r = 0; r < g.nvn; r++)
             for (int c = 0; c < g.nvm; c++) a.vsign[r * g.nvm + c] = g.vsign[c * g.nvn + r];
         lk = g.b_kcontig;
+        a.lk_affine = g.bk_affine; a.lk0 = g.bk0; a.lk_step = g.bk_step;
+        a.sk_affine = g.ak_affine; a.sk0 = g.ak0; a.sk_step = g.ak_step;
     }
     int ks = skinny_ksplit(a.R, a.K, nt);
     if (!g.ws || (int64_t)ks * a.R * a.NS > g.ws_elems) ks = 1;
@@ -498,6 +543,38 @@ void gemm_fp64(const GemmArgs& g, cudaStream_t s) {
         if (g.b_kcontig) launch_fp64<false, true>(g, s);
         else launch_fp64<false, false>(g, s);
     }
+}
+
+int fp64_tiles(int M, int N) { return ((M + BM - 1) / BM) * ((N + BN - 1) / BN); }
+
+void splitk_fold(const GemmArgs& g, int ks, cudaStream_t s) {
+    const int64_t mn = (int64_t)g.M * g.N;
+    if (mn <= 0 || ks <= 1) return;
+    const int nb = (int)std::min<int64_t>((mn + 255) / 256, 148 * 16);
+    splitk_fold_kernel<<<nb, 256, 0, s>>>(g, ks);
+    COUNT_LAUNCH();
+}
+
+namespace {
+template <bool AK, bool BKc>
+void launch_grouped_t(const GemmArgs* probs, const int* tile_start, int nprob, int total_tiles, cudaStream_t s) {
+    using S = Smem<AK, BKc>;
+    set_smem_once((const void*)gemm_fp64_grouped_kernel<AK, BKc>, (int)S::bytes);
+    gemm_fp64_grouped_kernel<AK, BKc><<<total_tiles, THREADS, S::bytes, s>>>(probs, tile_start, nprob);
+}
+}  // namespace
+
+void gemm_fp64_grouped(const GemmArgs* probs, const int* tile_start, int nprob, int total_tiles, bool a_kcontig,
+                       bool b_kcontig, cudaStream_t s) {
+    if (nprob <= 0 || total_tiles <= 0) return;
+    if (a_kcontig) {
+        if (b_kcontig) launch_grouped_t<true, true>(probs, tile_start, nprob, total_tiles, s);
+        else launch_grouped_t<true, false>(probs, tile_start, nprob, total_tiles, s);
+    } else {
+        if (b_kcontig) launch_grouped_t<false, true>(probs, tile_start, nprob, total_tiles, s);
+        else launch_grouped_t<false, false>(probs, tile_start, nprob, total_tiles, s);
+    }
+    COUNT_LAUNCH();
 }
 
 // ---------------------------------------------------------------------------
@@ -722,6 +799,69 @@ double* partial_buffer(cudaStream_t s) {
     cudaMalloc(&p, sizeof(double) * 148 * 16 * 16);
     g_partial[key] = p;
     return p;
+}
+
+namespace {
+
+__device__ __forceinline__ int find_problem(const int64_t* __restrict__ cs, int n, int64_t c) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (cs[mid] <= c) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+__global__ void __launch_bounds__(256) sum_batched_kernel(const SumDesc* __restrict__ d, const int64_t* __restrict__ cs,
+                                                          int n) {
+    __shared__ int sp;
+    const int64_t c = blockIdx.x;
+    if (threadIdx.x == 0) sp = find_problem(cs, n, c);
+    __syncthreads();
+    const SumDesc& D = d[sp];
+    const int64_t base = (c - cs[sp]) * kBatchChunk;
+    for (int i = threadIdx.x; i < kBatchChunk; i += blockDim.x) {
+        const int64_t l = base + i;
+        if (l >= D.total) break;
+        int64_t r = l, oa = 0, oc = 0;
+        for (int k = 0; k < D.ndim; k++) {
+            const int64_t x = r % D.len[k];
+            r /= D.len[k];
+            oa += x * D.sA[k];
+            oc += x * D.sC[k];
+        }
+        D.C[oc] += D.alpha * D.A[oa];
+    }
+}
+
+__global__ void __launch_bounds__(256) scale_batched_kernel(const ScaleDesc* __restrict__ d,
+                                                            const int64_t* __restrict__ cs, int n) {
+    __shared__ int sp;
+    const int64_t c = blockIdx.x;
+    if (threadIdx.x == 0) sp = find_problem(cs, n, c);
+    __syncthreads();
+    const ScaleDesc& D = d[sp];
+    const int64_t base = (c - cs[sp]) * kBatchChunk;
+    for (int i = threadIdx.x; i < kBatchChunk; i += blockDim.x) {
+        const int64_t l = base + i;
+        if (l >= D.n) break;
+        D.X[l] = D.beta == 0.0 ? 0.0 : D.beta * D.X[l];
+    }
+}
+
+}  // namespace
+
+void sum_batched(const SumDesc* d, const int64_t* chunk_start, int n, int64_t chunks, cudaStream_t s) {
+    if (n <= 0 || chunks <= 0) return;
+    sum_batched_kernel<<<(unsigned)chunks, 256, 0, s>>>(d, chunk_start, n);
+    COUNT_LAUNCH();
+}
+
+void scale_batched(const ScaleDesc* d, const int64_t* chunk_start, int n, int64_t chunks, cudaStream_t s) {
+    if (n <= 0 || chunks <= 0) return;
+    scale_batched_kernel<<<(unsigned)chunks, 256, 0, s>>>(d, chunk_start, n);
+    COUNT_LAUNCH();
 }
 
 void release_stream_buffers(cudaStream_t s) {

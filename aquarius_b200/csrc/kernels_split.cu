@@ -48,22 +48,34 @@ void set_smem_once(const void* kernel, int bytes);
 
 namespace split {
 
-constexpr int BM = 128, BN = 128, BK = 64;
-constexpr int NSLICE = 3;
+constexpr int BM = 128, BN = 128, BK = 64;           // BN: tile width of the 3-slice kernel
 constexpr int STAGES = 2;
-constexpr int CHUNK_KB = 16;                       // 16 x 64 = 1024 k per exact FP32 chunk
+constexpr int CHUNK_KB = 16;                       // 16 x 64 = 1024 k: the 3-slice exact FP32 chunk
 constexpr int EPI_WARPS = 8;
 constexpr int THREADS = 32 * (2 + EPI_WARPS);
 constexpr int TILE_A_BYTES = BM * BK * 2;           // 16 KiB
-constexpr int TILE_B_BYTES = BN * BK * 2;           // 16 KiB
-constexpr int STAGE_BYTES = NSLICE * (TILE_A_BYTES + TILE_B_BYTES);   // 96 KiB
-constexpr int TMEM_COLS = 512;                      // 2 x (L2: 128 + L34: 128)
-constexpr size_t SMEM_BYTES = 1024 + (size_t)STAGES * STAGE_BYTES + 256;
 constexpr long long WAIT_CYCLES = 4000000000ll;     // ~2 s at 1.9 GHz
 
-// instruction descriptor: D=F32, A=B=BF16, K-major both, N=128, M=128
-constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
-                           ((uint32_t)(BM >> 4) << 24);
+// Kernel shape per slice count: 3 slices on 128x128 tiles, 4 slices on 128x64 tiles, so
+// that a stage (NS A tiles + NS B tiles) is 96 KiB either way.
+template <int NS>
+struct Shape {
+    static constexpr int TBN = NS == 3 ? 128 : 64;
+    static constexpr int TILE_B = TBN * BK * 2;
+    static constexpr int STAGE = NS * (TILE_A_BYTES + TILE_B);
+    // TMEM accumulators per buffer: 3 slices keep s1*s1 (exact over 1024 k) and the rest;
+    // 4 slices also keep s1*s2 + s2*s1 apart (exact over 512 k), so that the FP32 rounding
+    // of the remaining terms sits below the 4-slice truncation
+    static constexpr int NACC = NS == 4 ? 3 : 2;
+    static constexpr int CHUNK = NS == 4 ? 8 : CHUNK_KB;   // K blocks per drained chunk
+    static constexpr int BUF = NACC * TBN;                 // TMEM columns per buffer
+    static constexpr int TMEM_COLS = 2 * BUF <= 256 ? 256 : 512;
+    static constexpr int COLS = TBN / 2;             // columns per epilogue warp
+    static constexpr size_t SMEM = 1024 + (size_t)STAGES * STAGE + 256;
+    // instruction descriptor: D=F32, A=B=BF16, K-major both, N=TBN, M=128
+    static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TBN >> 3) << 17) |
+                                      ((uint32_t)(BM >> 4) << 24);
+};
 
 struct Params {
     int M, N, K;
@@ -80,6 +92,11 @@ struct Params {
     int nvm, nvn;
     double vsign[4];
     int* err;
+    // split-K over gridDim.y: K-block range blockIdx.y of ks, partials (scales applied,
+    // alpha not) to ws[z][m][n], folded into C by the FP64 fold kernel
+    int ks;
+    int kb_per;                    // K blocks per range (a multiple of the exact chunk)
+    double* ws;
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -144,12 +161,12 @@ __device__ __forceinline__ uint64_t sdesc(const void* p) {
     return d;
 }
 
-__device__ __forceinline__ void umma(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t acc) {
+__device__ __forceinline__ void umma(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(dtmem),
-        "l"(a), "l"(b), "r"(IDESC), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+        "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
 }
 
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
@@ -169,12 +186,15 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
+template <int NS>
 __global__ void __launch_bounds__(THREADS, 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params p) {
+    using Sh = Shape<NS>;
+    constexpr int TBN = Sh::TBN, COLS = Sh::COLS;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint8_t* stages = smem;
-    uint64_t* bars = (uint64_t*)(smem + (size_t)STAGES * STAGE_BYTES);
+    uint64_t* bars = (uint64_t*)(smem + (size_t)STAGES * Sh::STAGE);
     uint64_t* full = bars;          // [STAGES]
     uint64_t* empty = bars + 2;     // [STAGES]
     uint64_t* tfull = bars + 4;     // [2]
@@ -185,9 +205,11 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int tile = blockIdx.x;
     const int tm = tile / p.tiles_n, tn = tile % p.tiles_n;
-    const int m0 = tm * BM, n0 = tn * BN;
-    const int nkb = p.Kp / BK;
-    const int nchunks = (nkb + CHUNK_KB - 1) / CHUNK_KB;
+    const int m0 = tm * BM, n0 = tn * TBN;
+    // this CTA's K blocks [kb0, kb0 + nkb)
+    const int kb0 = blockIdx.y * p.kb_per;
+    const int nkb = max(0, min(p.Kp / BK, kb0 + p.kb_per) - kb0);
+    const int nchunks = (nkb + Sh::CHUNK - 1) / Sh::CHUNK;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; s++) {
@@ -203,7 +225,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(TMEM_COLS));
+                     "r"(Sh::TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     tc_fence_before();
@@ -217,12 +239,12 @@ __global__ void __launch_bounds__(THREADS, 1)
             for (int kb = 0; kb < nkb && !*abort_flag; kb++) {
                 const int s = kb % STAGES;
                 if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1, abort_flag, p.err, 1)) break;
-                mbar_expect_tx(&full[s], STAGE_BYTES);
-                uint8_t* base = stages + (size_t)s * STAGE_BYTES;
-                for (int i = 0; i < NSLICE; i++)
-                    tma_load_2d(base + i * TILE_A_BYTES, &tmA, kb * BK, i * p.Mp + m0, &full[s]);
-                for (int i = 0; i < NSLICE; i++)
-                    tma_load_2d(base + NSLICE * TILE_A_BYTES + i * TILE_B_BYTES, &tmB, kb * BK, i * p.Np + n0,
+                mbar_expect_tx(&full[s], Sh::STAGE);
+                uint8_t* base = stages + (size_t)s * Sh::STAGE;
+                for (int i = 0; i < NS; i++)
+                    tma_load_2d(base + i * TILE_A_BYTES, &tmA, (kb0 + kb) * BK, i * p.Mp + m0, &full[s]);
+                for (int i = 0; i < NS; i++)
+                    tma_load_2d(base + NS * TILE_A_BYTES + i * Sh::TILE_B, &tmB, (kb0 + kb) * BK, i * p.Np + n0,
                                 &full[s]);
             }
         }
@@ -234,8 +256,8 @@ __global__ void __launch_bounds__(THREADS, 1)
                 const int b = c & 1;
                 if (c >= 2 && !mbar_wait(&tempty[b], ((c >> 1) - 1) & 1, abort_flag, p.err, 2)) break;
                 tc_fence_after();
-                const uint32_t dL2 = tmem + b * 256, dL34 = tmem + b * 256 + 128;
-                const int kb_end = min(nkb, (c + 1) * CHUNK_KB);
+                const uint32_t dbase = tmem + b * Sh::BUF;
+                const int kb_end = min(nkb, (c + 1) * Sh::CHUNK);
                 bool first = true;
                 bool ok = true;
                 for (; kb < kb_end; kb++) {
@@ -245,21 +267,29 @@ __global__ void __launch_bounds__(THREADS, 1)
                         break;
                     }
                     tc_fence_after();
-                    const uint8_t* base = stages + (size_t)s * STAGE_BYTES;
-                    const uint64_t a0 = sdesc(base), a1 = sdesc(base + TILE_A_BYTES),
-                                   a2 = sdesc(base + 2 * TILE_A_BYTES);
-                    const uint8_t* bb = base + NSLICE * TILE_A_BYTES;
-                    const uint64_t b0 = sdesc(bb), b1 = sdesc(bb + TILE_B_BYTES), b2 = sdesc(bb + 2 * TILE_B_BYTES);
+                    const uint8_t* base = stages + (size_t)s * Sh::STAGE;
+                    uint64_t ad[NS], bd[NS];
+#pragma unroll
+                    for (int i = 0; i < NS; i++) {
+                        ad[i] = sdesc(base + i * TILE_A_BYTES);
+                        bd[i] = sdesc(base + NS * TILE_A_BYTES + i * Sh::TILE_B);
+                    }
 #pragma unroll
                     for (int kk = 0; kk < BK / 16; kk++) {
                         const uint64_t o = (uint64_t)(kk * 32) >> 4;   // 16 bf16 = 32 bytes along K
-                        const uint32_t acc = first ? 0u : 1u;
-                        umma(dL2, a0 + o, b0 + o, acc);
-                        umma(dL34, a0 + o, b1 + o, acc);
-                        umma(dL34, a1 + o, b0 + o, 1u);
-                        umma(dL34, a0 + o, b2 + o, 1u);
-                        umma(dL34, a1 + o, b1 + o, 1u);
-                        umma(dL34, a2 + o, b0 + o, 1u);
+                        // slice products (i, t - i) with t < NS: t = 0 into accumulator 0,
+                        // the rest into accumulator min(t, NACC - 1)
+                        bool fresh[Sh::NACC];
+#pragma unroll
+                        for (int j = 0; j < Sh::NACC; j++) fresh[j] = first;
+#pragma unroll
+                        for (int t = 0; t < NS; t++)
+#pragma unroll
+                            for (int i = 0; i <= t; i++) {
+                                const int j = t < Sh::NACC - 1 ? t : Sh::NACC - 1;
+                                umma(dbase + j * TBN, ad[i] + o, bd[t - i] + o, Sh::IDESC, fresh[j] ? 0u : 1u);
+                                fresh[j] = false;
+                            }
                         first = false;
                     }
                     umma_commit(&empty[s]);
@@ -273,9 +303,9 @@ __global__ void __launch_bounds__(THREADS, 1)
         const int ew = warp - 2;
         const int q = warp & 3;          // TMEM lane quadrant this warp may access
         const int h = ew >> 2;           // column half
-        double acc[64];
+        double acc[COLS];
 #pragma unroll
-        for (int j = 0; j < 64; j++) acc[j] = 0.0;
+        for (int j = 0; j < COLS; j++) acc[j] = 0.0;
         bool ok = true;
         for (int c = 0; c < nchunks; c++) {
             const int b = c & 1;
@@ -284,30 +314,45 @@ __global__ void __launch_bounds__(THREADS, 1)
                 break;
             }
             tc_fence_after();
-            const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + b * 256 + h * 64;
+            const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + b * Sh::BUF + h * COLS;
 #pragma unroll
-            for (int j4 = 0; j4 < 4; j4++) {
-                uint32_t r2[16], r34[16];
-                tmem_ld16(base + j4 * 16, r2);
-                tmem_ld16(base + 128 + j4 * 16, r34);
+            for (int j4 = 0; j4 < COLS / 16; j4++) {
+                uint32_t r[Sh::NACC][16];
+#pragma unroll
+                for (int j = 0; j < Sh::NACC; j++) tmem_ld16(base + j * TBN + j4 * 16, r[j]);
                 tmem_wait_ld();
 #pragma unroll
-                for (int t = 0; t < 16; t++)
-                    acc[j4 * 16 + t] += (double)__uint_as_float(r2[t]) + (double)__uint_as_float(r34[t]);
+                for (int t = 0; t < 16; t++) {
+                    double v = 0.0;
+#pragma unroll
+                    for (int j = 0; j < Sh::NACC; j++) v += (double)__uint_as_float(r[j][t]);
+                    acc[j4 * 16 + t] += v;
+                }
             }
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[b]);
         }
-        if (ok) {
+        if (ok && p.ks > 1) {
+            const int m = m0 + q * 32 + lane;
+            if (m < p.M) {
+                const double sa = p.scaleA[m];
+                double* wz = p.ws + ((int64_t)blockIdx.y * p.M + m) * p.N;
+#pragma unroll
+                for (int j = 0; j < COLS; j++) {
+                    const int n = n0 + h * COLS + j;
+                    if (n < p.N) wz[n] = sa * p.scaleB[n] * acc[j];
+                }
+            }
+        } else if (ok) {
             const int m = m0 + q * 32 + lane;
             if (m < p.M) {
                 const double sa = p.alpha * p.scaleA[m];
                 const int64_t cm0 = p.Cm0[m];
                 const int64_t cm1 = p.nvm > 1 ? p.Cm1[m] : 0;
 #pragma unroll
-                for (int j = 0; j < 64; j++) {
-                    const int n = n0 + h * 64 + j;
+                for (int j = 0; j < COLS; j++) {
+                    const int n = n0 + h * COLS + j;
                     if (n < p.N) {
                         const double v = sa * p.scaleB[n] * acc[j];
                         const int64_t cn0 = p.Cn0[n];
@@ -326,7 +371,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     __syncthreads();
     if (warp == 1) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(Sh::TMEM_COLS));
     }
 }
 
@@ -381,7 +426,7 @@ __device__ __forceinline__ unsigned short bf16_bits(double v) {
     return *reinterpret_cast<unsigned short*>(&b);
 }
 
-template <bool KC>
+template <bool KC, int NS>
 __global__ void __launch_bounds__(STHREADS)
     slice_kernel(const double* __restrict__ X, const int64_t* __restrict__ R, const int64_t* __restrict__ Kt, int nrows,
                  int K, const unsigned long long* __restrict__ rowmax, int rows_p, int kpad,
@@ -397,23 +442,24 @@ __global__ void __launch_bounds__(STHREADS)
         const int k = e % SK, r = e / SK;
         const int row = r0 + r;
         double mx = row < nrows ? __longlong_as_double((long long)rowmax[row]) : 0.0;
-        unsigned short b1 = 0, b2 = 0, b3 = 0;
+        unsigned short bits[NS];
+#pragma unroll
+        for (int t = 0; t < NS; t++) bits[t] = 0;
         if (mx > 0.0) {
             const int ex = ilogb(mx);                // mx in [2^ex, 2^(ex+1))
-            const double y = ldexp(tile[r][k], 6 - ex);   // |y| < 128
-            const double s1 = rint(y);
-            const double y2 = (y - s1) * 256.0;
-            const double s2 = rint(y2);
-            const double y3 = (y2 - s2) * 256.0;
-            const double s3 = rint(y3);
-            b1 = bf16_bits(s1);
-            b2 = bf16_bits(s2 * 0.00390625);
-            b3 = bf16_bits(s3 * 1.52587890625e-05);
+            double y = ldexp(tile[r][k], 6 - ex);    // |y| < 128
+            double w = 1.0;                          // weight of slice t: 2^(-8t)
+#pragma unroll
+            for (int t = 0; t < NS; t++) {
+                const double st = rint(y);           // an integer of at most 8 significant bits
+                bits[t] = bf16_bits(st * w);
+                y = (y - st) * 256.0;
+                w *= 0.00390625;
+            }
         }
         const size_t o = (size_t)row * kpad + (k0 + k);
-        out[o] = b1;
-        out[plane + o] = b2;
-        out[2 * plane + o] = b3;
+#pragma unroll
+        for (int t = 0; t < NS; t++) out[t * plane + o] = bits[t];
         if (blockIdx.y == 0 && k == 0) scale[row] = mx > 0.0 ? ldexp(1.0, ilogb(mx) - 6) : 0.0;
     }
 }
@@ -438,12 +484,12 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 
-void make_map(CUtensorMap* map, const uint16_t* base, int rows_total, int kpad) {
+void make_map(CUtensorMap* map, const uint16_t* base, int rows_total, int kpad, int box_rows) {
     EncodeTiledFn enc = encode_fn();
     if (!enc) throw std::runtime_error("cuTensorMapEncodeTiled is not available");
     cuuint64_t dims[2] = {(cuuint64_t)kpad, (cuuint64_t)rows_total};
     cuuint64_t strides[1] = {(cuuint64_t)kpad * 2};
-    cuuint32_t box[2] = {BK, 128};
+    cuuint32_t box[2] = {BK, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)base, dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -484,28 +530,51 @@ int split_k_pad(int k) { return (k + split::BK - 1) / split::BK * split::BK; }
 void slice_rows(const double* X, const int64_t* R, const int64_t* Kt, int nrows, int K, bool kcontig, int nslices,
                 SlicedOperand& out, cudaStream_t s) {
     using namespace split;
-    if (nslices != NSLICE) throw std::runtime_error("only 3 slices are built");
+    if (nslices != 3 && nslices != 4) throw std::runtime_error("3 or 4 slices are built");
+    if (out.nslices != nslices) throw std::runtime_error("sliced operand allocated for another slice count");
     unsigned long long* rowmax = reinterpret_cast<unsigned long long*>(out.rowmax);
     cudaMemsetAsync(rowmax, 0, sizeof(double) * out.rows, s);
     if (out.kpad / SK > 65535) throw std::runtime_error("split operand K too long for the slicing grid");
     dim3 grid(out.rows / SR, out.kpad / SK);
     if (kcontig) rowmax_kernel<true><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax);
     else rowmax_kernel<false><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax);
-    if (kcontig)
-        slice_kernel<true><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax, out.rows, out.kpad, out.data, out.scale);
-    else
-        slice_kernel<false><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax, out.rows, out.kpad, out.data, out.scale);
+    auto* d = out.data;
+    if (nslices == 3) {
+        if (kcontig) slice_kernel<true, 3><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax, out.rows, out.kpad, d, out.scale);
+        else slice_kernel<false, 3><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax, out.rows, out.kpad, d, out.scale);
+    } else {
+        if (kcontig) slice_kernel<true, 4><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax, out.rows, out.kpad, d, out.scale);
+        else slice_kernel<false, 4><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax, out.rows, out.kpad, d, out.scale);
+    }
     g_launches += 2;
 }
 
+int split_ksplit(int M, int N, int K, int nslices) {
+    using namespace split;
+    const int tbn = nslices == 4 ? Shape<4>::TBN : Shape<3>::TBN;
+    const int64_t tiles = (int64_t)((M + BM - 1) / BM) * ((N + tbn - 1) / tbn);
+    if (tiles >= 148) return 1;
+    const int chunk = nslices == 4 ? Shape<4>::CHUNK : Shape<3>::CHUNK;
+    const int64_t chunks = (split_k_pad(K) / BK + chunk - 1) / chunk;
+    int64_t ks = (2 * 148 + tiles - 1) / tiles;
+    ks = std::min<int64_t>(ks, chunks);
+    ks = std::min<int64_t>(ks, 256);
+    return (int)std::max<int64_t>(ks, 1);
+}
+
 void gemm_split(const SlicedOperand& a, const SlicedOperand& b, int M, int N, int K, const GemmArgs& g,
-                cudaStream_t s) {
+                cudaStream_t s, int ks) {
     using namespace split;
     (void)K;
-    set_smem_once((const void*)split_gemm_kernel, (int)SMEM_BYTES);
+    const int ns = a.nslices;
+    if ((ns != 3 && ns != 4) || b.nslices != ns) throw std::runtime_error("split GEMM operands with different slice counts");
+    const int tbn = ns == 4 ? Shape<4>::TBN : Shape<3>::TBN;
+    const size_t smem = ns == 4 ? Shape<4>::SMEM : Shape<3>::SMEM;
+    const void* kfn = ns == 4 ? (const void*)split_gemm_kernel<4> : (const void*)split_gemm_kernel<3>;
+    set_smem_once(kfn, (int)smem);
     CUtensorMap ma, mb;
-    make_map(&ma, a.data, NSLICE * a.rows, a.kpad);
-    make_map(&mb, b.data, NSLICE * b.rows, b.kpad);
+    make_map(&ma, a.data, ns * a.rows, a.kpad, BM);
+    make_map(&mb, b.data, ns * b.rows, b.kpad, tbn);
     Params p;
     p.M = M;
     p.N = N;
@@ -513,7 +582,7 @@ void gemm_split(const SlicedOperand& a, const SlicedOperand& b, int M, int N, in
     p.Mp = a.rows;
     p.Np = b.rows;
     p.Kp = a.kpad;
-    p.tiles_n = b.rows / BN;
+    p.tiles_n = b.rows / tbn;
     p.alpha = g.alpha;
     p.scaleA = a.scale;
     p.scaleB = b.scale;
@@ -526,9 +595,20 @@ void gemm_split(const SlicedOperand& a, const SlicedOperand& b, int M, int N, in
     p.nvn = g.nvn;
     for (int i = 0; i < 4; i++) p.vsign[i] = g.vsign[i];
     p.err = error_flag();
+    const int nkb = a.kpad / BK;
+    if (ks > 1 && (!g.ws || (int64_t)ks * M * N > g.ws_elems)) ks = 1;
+    if (ks > 65535) ks = 65535;
+    // K blocks per range: whole exact chunks
+    const int chunk = ns == 4 ? Shape<4>::CHUNK : Shape<3>::CHUNK;
+    const int per_chunks = ((nkb + chunk - 1) / chunk + ks - 1) / ks;
+    p.ks = ks;
+    p.kb_per = ks > 1 ? per_chunks * chunk : nkb;
+    p.ws = g.ws;
     const int tiles = (a.rows / BM) * p.tiles_n;
-    split_gemm_kernel<<<tiles, THREADS, SMEM_BYTES, s>>>(ma, mb, p);
+    if (ns == 4) split_gemm_kernel<4><<<dim3(tiles, ks), THREADS, smem, s>>>(ma, mb, p);
+    else split_gemm_kernel<3><<<dim3(tiles, ks), THREADS, smem, s>>>(ma, mb, p);
     g_launches++;
+    if (ks > 1) splitk_fold(g, ks, s);
 }
 
 int split_error(bool reset) {

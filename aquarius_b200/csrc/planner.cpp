@@ -590,6 +590,18 @@ Plan plan_contract(Context& ctx, double alpha, int hA, const std::string& idxA, 
     Plan plan;
     std::set<std::pair<int, int>> touched;   // (case, block) of C that received a term
     std::vector<Plan> parts;
+    // products X of the multi-image groups; those that fit in kBatchX together get disjoint
+    // regions of the plan scratch, so that all products of the statement can run before
+    // all image sums (and be grouped into few launches)
+    struct XGroup {
+        Plan part;          // [zero X] [GEMMs into X] [sums X -> C], X at offset 0
+        int64_t nX = 0;
+        bool batched = false;
+        size_t slot = 0;    // position among the statement's parts
+    };
+    std::vector<XGroup> xgroups;
+    constexpr int64_t kBatchX = 64ll << 20;   // doubles
+    int64_t batched_total = 0;
 
     // Internal pairs antisymmetric in both factors (same group of A and same group of B,
     // nothing else internal in those groups): the spin assignments (a,b) and (b,a) give
@@ -784,7 +796,15 @@ Plan plan_contract(Context& ctx, double alpha, int hA, const std::string& idxA, 
                     part.steps.push_back({Step::SUM, (int)part.sums.size()});
                     part.sums.push_back(s);
                 }
-                parts.push_back(std::move(part));
+                XGroup xg;
+                xg.nX = nX;
+                xg.batched = batched_total + nX <= kBatchX;
+                if (xg.batched) batched_total += nX;
+                xg.part = std::move(part);
+                // the group's products keep their place among the direct products
+                xg.slot = parts.size();
+                parts.push_back(Plan());
+                xgroups.push_back(std::move(xg));
             }
         }
     }
@@ -801,7 +821,49 @@ Plan plan_contract(Context& ctx, double alpha, int hA, const std::string& idxA, 
             plan.scales.push_back(s);
         }
     }
+    // Batched groups: one zero-fill of their regions, their products in group order among
+    // the direct products, then all their image sums; the other groups (X too large to
+    // keep apart) follow one by one, each reusing the start of the scratch.
+    Plan sums;
+    int64_t off = 0, classic_max = 0;
+    std::vector<Plan> classic;
+    if (batched_total > 0) {
+        ScaleStep z;
+        z.tC = kScratch;
+        z.off = 0;
+        z.n = batched_total;
+        z.beta = 0.0;
+        plan.steps.push_back({Step::SCALE, (int)plan.scales.size()});
+        plan.scales.push_back(z);
+    }
+    for (auto& xg : xgroups) {
+        const size_t slot = xg.slot;
+        if (!xg.batched) {
+            classic_max = std::max(classic_max, xg.nX);
+            classic.push_back(std::move(xg.part));
+            continue;
+        }
+        Plan g;
+        for (auto& st : xg.part.steps) {
+            if (st.kind == Step::GEMM) {
+                GemmStep gs = std::move(xg.part.gemms[st.idx]);
+                for (auto& v : gs.hCm[0]) v += off;
+                g.steps.push_back({Step::GEMM, (int)g.gemms.size()});
+                g.gemms.push_back(std::move(gs));
+            } else if (st.kind == Step::SUM) {
+                SumStep s = xg.part.sums[st.idx];
+                s.offA += off;
+                sums.steps.push_back({Step::SUM, (int)sums.sums.size()});
+                sums.sums.push_back(s);
+            }
+        }
+        parts[slot] = std::move(g);
+        off += xg.nX;
+    }
     for (auto& p : parts) plan.append(std::move(p));
+    plan.append(std::move(sums));
+    for (auto& p : classic) plan.append(std::move(p));
+    plan.scratch_elems = std::max(plan.scratch_elems, std::max(batched_total, classic_max));
     return plan;
 }
 

@@ -1,16 +1,20 @@
 // Serving loop: continuous batching of CCSD solves on one device.
 //
-// Two host threads share a request queue:
-// * admission: takes requests in arrival order once their planned device bytes
-//   (ccsd_plan_query) fit in the budget beside the active solves and a slot is free;
-//   builds each one's H and solver on a context with its own stream;
-// * iteration: keeps exactly one iteration of every active solve queued on its stream,
-//   polls completion events (no host synchronisation), decides convergence from the
-//   energy / residual copied back with the iteration, and retires finished solves,
-//   which frees their budget for the next admission.
+// * Admission (one host thread): takes requests in arrival order once their planned
+//   device bytes (ccsd_plan_query) fit in the budget beside the active solves and a slot
+//   is free, reserves the bytes and the slot, and starts a worker for the request.
+// * Workers (one host thread per active solve): build the request's H and solver on a
+//   context with its own stream, then run its iterations back to back: each iteration is
+//   queued on the stream with the copy of its energy / residual to the host, the worker
+//   sleeps on the iteration's completion event (blocking sync, no spinning), checks
+//   convergence, and queues the next one.  The GPU interleaves the iterations of all
+//   active solves through their streams; the host work of planning and launching runs on
+//   as many threads as there are active solves.  A finished solve frees its context,
+//   which returns its bytes for the next admission.
 // Solves share nothing on the device but the memory pool; each one runs the same kernels
 // and reductions it would run alone, so its result does not depend on the mix.
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
@@ -42,15 +46,6 @@ struct Request {
     double flops = 0;
 };
 
-struct Active {
-    std::shared_ptr<Request> req;
-    std::unique_ptr<Context> ctx;
-    std::unique_ptr<Solver> solver;
-    cudaEvent_t ev = nullptr;
-    bool in_flight = false;
-    double t_admit = 0;
-};
-
 }  // namespace
 
 class Server {
@@ -64,7 +59,6 @@ public:
             opts.memory_budget = (int64_t)(0.9 * (double)fr);
         }
         admit_thread = std::thread([this] { admit_loop(); });
-        iter_thread = std::thread([this] { iter_loop(); });
     }
 
     ~Server() {
@@ -73,9 +67,10 @@ public:
             stop = true;
         }
         cv_admit.notify_all();
-        cv_iter.notify_all();
         if (admit_thread.joinable()) admit_thread.join();
-        if (iter_thread.joinable()) iter_thread.join();
+        // workers leave after their current iteration
+        for (auto& w : workers)
+            if (w.t.joinable()) w.t.join();
     }
 
     double now() const {
@@ -119,15 +114,24 @@ private:
     ccsd_server_options opts;
     std::chrono::steady_clock::time_point t0;
     std::mutex mu;
-    std::condition_variable cv_admit, cv_iter, cv_done;
+    std::condition_variable cv_admit, cv_done;
     std::deque<std::shared_ptr<Request>> queue;
-    std::vector<std::unique_ptr<Active>> admitted;   // handed from admission to iteration
     std::deque<ccsd_server_result> results;
     int64_t next_id = 1, submitted = 0, finished = 0;
     int64_t used_bytes = 0, peak_bytes = 0;
     int n_active = 0, peak_active = 0;
     bool stop = false;
-    std::thread admit_thread, iter_thread;
+    std::thread admit_thread;
+    struct Worker {
+        std::thread t;
+        std::shared_ptr<std::atomic<bool>> done;
+    };
+    std::vector<Worker> workers;   // touched by the admission thread and the destructor only
+
+    bool stopping() {
+        std::lock_guard<std::mutex> lk(mu);
+        return stop;
+    }
 
     void plan(Request& r) {
         ccsd_options o = opts.solve;
@@ -198,23 +202,18 @@ private:
                 peak_bytes = std::max(peak_bytes, used_bytes);
                 peak_active = std::max(peak_active, n_active);
             }
-            auto a = std::make_unique<Active>();
-            a->req = r;
-            a->t_admit = now();
-            try {
-                build(*a);
-            } catch (const Error& e) {
-                fail(std::move(a), e.code);
-                continue;
-            } catch (const std::exception& e) {
-                fail(std::move(a), CCSD_ERR_ARG);
-                continue;
-            }
-            {
-                std::lock_guard<std::mutex> lk(mu);
-                admitted.push_back(std::move(a));
-            }
-            cv_iter.notify_all();
+            const double t_admit = now();
+            // join the workers that have finished, then start this request's
+            for (auto& w : workers)
+                if (w.done->load() && w.t.joinable()) w.t.join();
+            workers.erase(std::remove_if(workers.begin(), workers.end(), [](Worker& w) { return !w.t.joinable(); }),
+                          workers.end());
+            auto done = std::make_shared<std::atomic<bool>>(false);
+            workers.push_back({std::thread([this, r, t_admit, done] {
+                                   run_solve(r, t_admit);
+                                   done->store(true);
+                               }),
+                               done});
         }
     }
 
@@ -226,9 +225,8 @@ private:
         finish(r, status, 0, 0, 0, 0, now());
     }
 
-    void build(Active& a) {
-        Request& r = *a.req;
-        a.ctx = std::make_unique<Context>(opts.device, nullptr);
+    void build(Request& r, std::unique_ptr<Context>& ctx, std::unique_ptr<Solver>& solver) {
+        ctx = std::make_unique<Context>(opts.device, nullptr);
         Spaces S;
         S.nirrep = r.nirrep;
         for (int sp = 0; sp < 2; sp++)
@@ -241,8 +239,8 @@ private:
                     off += n;
                 }
             }
-        a.ctx->spaces = S;
-        a.ctx->spaces_set = true;
+        ctx->spaces = S;
+        ctx->spaces_set = true;
         if (r.synthetic) {
             int n = 0;
             for (int h = 0; h < r.nirrep; h++) n += r.occ[h] + r.vrt[h];
@@ -255,94 +253,66 @@ private:
             if (st != CCSD_OK) throw Error(st, "synthetic generator failed");
         }
         ccsd_hamiltonian H;
-        build_hamiltonian(*a.ctx, r.naux, r.B.data(), r.eps.data(),
+        build_hamiltonian(*ctx, r.naux, r.B.data(), r.eps.data(),
                           r.nirrep > 1 && !r.aux.empty() ? r.aux.data() : nullptr, opts.pack_vvvv != 0, &H);
         std::vector<double>().swap(r.B);   // the factor is on the device now
         ccsd_options o = opts.solve;
         if (o.precision == CCSD_PREC_SPLIT && !kern::split_supported()) o.precision = CCSD_PREC_FP64;
-        a.solver = std::make_unique<Solver>(*a.ctx, H, o);
-        CCSD_CUDA(cudaEventCreateWithFlags(&a.ev, cudaEventDisableTiming));
+        solver = std::make_unique<Solver>(*ctx, H, o);
     }
 
-    void release(Active& a) {
-        if (a.ev) cudaEventDestroy(a.ev);
-        a.ev = nullptr;
-        a.solver.reset();
-        a.ctx.reset();
+    // one active solve, start to finish, on this worker thread
+    void run_solve(std::shared_ptr<Request> r, double t_admit) {
+        cudaSetDevice(opts.device);
+        std::unique_ptr<Context> ctx;
+        std::unique_ptr<Solver> s;
+        cudaEvent_t ev = nullptr;
+        int status = CCSD_OK;
+        double e = 0, c = 0, mp2 = 0;
+        int it = 0;
+        try {
+            build(*r, ctx, s);
+            mp2 = s->mp2;
+            CCSD_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming | cudaEventBlockingSync));
+            while (true) {
+                s->iterate_async();
+                s->post_status();
+                CCSD_CUDA(cudaEventRecord(ev, ctx->stream));
+                CCSD_CUDA(cudaEventSynchronize(ev));
+                s->check_status();
+                if (s->conv < s->opts.conv_tol) break;
+                if (s->iterations >= s->opts.max_iter) {
+                    status = CCSD_NOT_CONVERGED;
+                    break;
+                }
+                if (stopping()) {
+                    status = CCSD_NOT_CONVERGED;
+                    break;
+                }
+            }
+            e = s->energy;
+            c = s->conv;
+            it = s->iterations;
+        } catch (const Error& err) {
+            status = err.code;
+            it = s ? s->iterations : 0;
+        } catch (const std::exception& err) {
+            status = CCSD_ERR_ARG;
+            it = s ? s->iterations : 0;
+        }
+        if (ev) cudaEventDestroy(ev);
+        try {
+            s.reset();
+            ctx.reset();
+        } catch (...) {
+        }
         {
             std::lock_guard<std::mutex> lk(mu);
-            used_bytes -= a.req->bytes;
+            used_bytes -= r->bytes;
             n_active--;
         }
         cv_admit.notify_all();
-    }
-
-    void fail(std::unique_ptr<Active> a, int status) {
-        const double mp2 = a->solver ? a->solver->mp2 : 0.0;
-        const int it = a->solver ? a->solver->iterations : 0;
-        try {
-            release(*a);
-        } catch (...) {
-        }
-        finish(*a->req, status, it, 0, mp2, 0, a->t_admit);
-    }
-
-    void iter_loop() {
-        cudaSetDevice(opts.device);
-        std::vector<std::unique_ptr<Active>> act;
-        while (true) {
-            {
-                std::unique_lock<std::mutex> lk(mu);
-                if (act.empty())
-                    cv_iter.wait_for(lk, std::chrono::milliseconds(5), [&] { return stop || !admitted.empty(); });
-                if (stop) break;
-                for (auto& a : admitted) act.push_back(std::move(a));
-                admitted.clear();
-            }
-            bool progressed = false;
-            for (auto& a : act) {
-                Solver& s = *a->solver;
-                try {
-                    if (!a->in_flight) {
-                        s.iterate_async();
-                        s.post_status();
-                        CCSD_CUDA(cudaEventRecord(a->ev, a->ctx->stream));
-                        a->in_flight = true;
-                        progressed = true;
-                        continue;
-                    }
-                    const cudaError_t q = cudaEventQuery(a->ev);
-                    if (q == cudaErrorNotReady) continue;
-                    CCSD_CUDA(q);
-                    a->in_flight = false;
-                    progressed = true;
-                    s.check_status();
-                    const bool conv = s.conv < s.opts.conv_tol;
-                    if (conv || s.iterations >= s.opts.max_iter) {
-                        const double e = s.energy, c = s.conv, mp2 = s.mp2;
-                        const int it = s.iterations;
-                        const double ta = a->t_admit;
-                        auto req = a->req;
-                        release(*a);
-                        finish(*req, conv ? CCSD_OK : CCSD_NOT_CONVERGED, it, e, mp2, c, ta);
-                        a.reset();
-                    }
-                } catch (const Error& e) {
-                    fail(std::move(a), e.code);
-                } catch (const std::exception& e) {
-                    fail(std::move(a), CCSD_ERR_ARG);
-                }
-            }
-            act.erase(std::remove(act.begin(), act.end(), nullptr), act.end());
-            if (!progressed && !act.empty()) std::this_thread::sleep_for(std::chrono::microseconds(50));
-        }
-        for (auto& a : act) {
-            if (!a) continue;
-            try {
-                release(*a);
-            } catch (...) {
-            }
-        }
+        finish(*r, status, it, status == CCSD_OK || status == CCSD_NOT_CONVERGED ? e : 0.0, mp2, c, t_admit);
     }
 };
 

@@ -38,6 +38,8 @@ void options_default(ccsd_options* o) {
 Solver::Solver(Context& c, const ccsd_hamiltonian& h, const ccsd_options& o) : ctx(c), H(h), opts(o) {
     if (opts.diis_damping != 0.0) throw Error(CCSD_ERR_UNSUPPORTED, "DIIS damping is not supported");
     if (opts.diis_order < 1 || opts.diis_order > 16) throw Error(CCSD_ERR_ARG, "diis_order must be in 1..16");
+    if (opts.slices != 0 && opts.slices != 3 && opts.slices != 4)
+        throw Error(CCSD_ERR_ARG, "slices must be 0 (default), 3 or 4");
     ctx.precision = opts.precision;
     ctx.slices = opts.slices;
     // constants: the H blocks never change, so their split slices can be cached
@@ -427,17 +429,29 @@ void Solver::diis_step() {
 }
 
 void Solver::iterate_async() {
-    // split-precision residuals bottom out near 1e-9; past refine_tol the contractions
-    // switch to native FP64 for the rest of the solve (graphs are recaptured)
+    // Refinement of the split precision.  Three BF16 slices leave a residual floor near
+    // 1e-9; once conv < refine_tol the contractions move to four slices (floor ~2^-8
+    // lower), and to native FP64 only if the residual then stalls (no halving over two
+    // iterations) above conv_tol.  Graphs are recaptured after a switch.
     if (opts.precision == CCSD_PREC_SPLIT && opts.refine_tol > 0 && conv < opts.refine_tol &&
         ctx.precision != CCSD_PREC_FP64) {
-        ctx.precision = CCSD_PREC_FP64;
-        refined = true;
-        if (graph_exec) cudaGraphExecDestroy(graph_exec);
-        if (graph) cudaGraphDestroy(graph);
-        graph_exec = nullptr;
-        graph = nullptr;
-        captured_once = false;
+        bool escalate = false;
+        if (ctx.split_slices() == 3) {
+            ctx.slices = 4;
+            escalate = true;
+        } else if (conv_hist.size() >= 3 && conv > 0.5 * conv_hist[conv_hist.size() - 3]) {
+            ctx.precision = CCSD_PREC_FP64;
+            escalate = true;
+        }
+        if (escalate) {
+            refined = true;
+            conv_hist.clear();
+            if (graph_exec) cudaGraphExecDestroy(graph_exec);
+            if (graph) cudaGraphDestroy(graph);
+            graph_exec = nullptr;
+            graph = nullptr;
+            captured_once = false;
+        }
     }
     if (opts.use_graph) {
         if (!graph_exec) {
@@ -485,6 +499,7 @@ void Solver::post_status() {
 void Solver::check_status() {
     energy = h_red[0];
     conv = h_red[1];
+    conv_hist.push_back(conv);
     if (opts.precision == CCSD_PREC_SPLIT) {
         int e = kern::split_error(true);
         if (e) throw Error(CCSD_ERR_TIMEOUT, "split GEMM wait " + std::to_string(e) + " expired");

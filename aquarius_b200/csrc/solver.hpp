@@ -38,7 +38,8 @@ public:
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t graph_exec = nullptr;
     bool captured_once = false;
-    bool refined = false;           // switched to FP64 contractions (refine_tol reached)
+    bool refined = false;           // moved to a more accurate contraction mode (refine_tol reached)
+    std::vector<double> conv_hist;  // residuals since the last mode switch (stall detection)
     std::vector<kern::TauArgs> tau_blocks;
 
     int iterations = 0;

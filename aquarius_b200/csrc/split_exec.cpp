@@ -15,17 +15,16 @@ namespace {
 // CCSD_SPLIT_ROUTE_ALL sends every contraction through the split kernel (coverage tests).
 bool use_split(const GemmStep& g, int routing) {
     if (routing == CCSD_SPLIT_ROUTE_ALL) return g.M > 0 && g.N > 0 && g.K > 0;
-    // Skinny (N of a few tens) or few-tile contractions stay on the FP64 kernel: the
-    // tensor kernel has no split-K, and re-slicing a large operand on every call costs
-    // more than the FP64 product when its slices cannot stay cached.
+    // Skinny contractions (N of a few tens) stay on the FP64 kernels; few-tile ones take
+    // the split kernel only when splitting K fills the machine (a 1024-k chunk per range).
     const int64_t tiles = (int64_t)((g.M + 127) / 128) * ((g.N + 127) / 128);
-    return g.M >= 128 && g.N >= 64 && g.K >= 256 && tiles >= 148 && g.flops() >= 5e8;
+    const int64_t ctas = tiles * kern::split_ksplit(g.M, g.N, g.K, 3);
+    return g.M >= 128 && g.N >= 64 && g.K >= 256 && ctas >= 148 && g.flops() >= 5e8;
 }
 
-// bytes of the three BF16 slices of a rows x K operand
-int64_t slice_bytes(int rows, int K) {
-    return (int64_t)kern::kDefaultSlices * kern::split_rows_pad(rows) * kern::split_k_pad(K) * 2 +
-           2 * (int64_t)kern::split_rows_pad(rows) * 8;
+// bytes of the ns BF16 slices (and row scales) of a rows x K operand
+int64_t slice_bytes(int rows, int K, int ns) {
+    return (int64_t)ns * kern::split_rows_pad(rows) * kern::split_k_pad(K) * 2 + 2 * (int64_t)kern::split_rows_pad(rows) * 8;
 }
 
 // device bytes the sliced constant operands may occupy (CCSD_SPLIT_CACHE_GB, default 56)
@@ -37,11 +36,15 @@ int64_t cache_budget() {
 
 }  // namespace
 
-kern::SlicedOperand Context::alloc_sliced(int rows, int K) {
+bool Context::routes_split(const GemmStep& g) const {
+    return precision == CCSD_PREC_SPLIT && kern::split_supported() && use_split(g, split_routing);
+}
+
+kern::SlicedOperand Context::alloc_sliced(int rows, int K, int ns) {
     kern::SlicedOperand s;
     s.rows = kern::split_rows_pad(rows);
     s.kpad = kern::split_k_pad(K);
-    s.nslices = kern::kDefaultSlices;
+    s.nslices = ns;
     const int64_t nd = (int64_t)s.nslices * s.rows * s.kpad;
     s.data = (uint16_t*)dmalloc(nd * sizeof(uint16_t));
     s.scale = (double*)dmalloc(s.rows * sizeof(double));
@@ -67,8 +70,9 @@ void Context::ensure_ws(kern::SlicedOperand& w, int rows, int K) {
     int keep_rows = std::max(rp, w.rows);
     int64_t keep_elems = std::max<int64_t>((int64_t)rp * kp, (int64_t)w.rows * w.kpad);
     if (w.data) free_sliced(w);
-    // capacity is tracked in elements; rows/kpad are set per call
-    w = alloc_sliced(keep_rows, (int)std::min<int64_t>((keep_elems + keep_rows - 1) / keep_rows, INT32_MAX));
+    // capacity is tracked in elements per slice, for the largest slice count (4); rows,
+    // kpad and the slice count of a view are set per call
+    w = alloc_sliced(keep_rows, (int)std::min<int64_t>((keep_elems + keep_rows - 1) / keep_rows, INT32_MAX), 4);
 }
 
 // Decide, for every split contraction of a plan, which constant operands keep cached
@@ -89,7 +93,7 @@ void Context::reserve_split(Plan& p) {
             bool& cache = side == 0 ? g->cache_a : g->cache_b;
             cache = false;
             if (h == kScratch || !is_constant(h)) continue;
-            const int64_t b = slice_bytes(rows, g->K);
+            const int64_t b = slice_bytes(rows, g->K, split_slices());
             if (used + b <= budget) {
                 cache = true;
                 used += b;
@@ -110,7 +114,7 @@ void Context::reserve_split(Plan& p) {
     if (host_only) {
         // account the cached slices and the workspace as if they were allocated
         dmalloc(used + 1);
-        dmalloc(6 * (need_a + need_b) + 16 * (rows_a + rows_b) + 1);
+        dmalloc(8 * (need_a + need_b) + 16 * (rows_a + rows_b) + 1);
         return;
     }
     for (GemmStep* g : order) {
@@ -125,7 +129,7 @@ void Context::run_split_gemm(GemmStep& g, kern::GemmArgs& a) {
         return;
     }
     split_launches++;
-    const int ns = kern::kDefaultSlices;
+    const int ns = split_slices();
     auto prepare = [&](bool is_a, int64_t& key, kern::SlicedOperand& ws) -> kern::SlicedOperand* {
         const int rows = is_a ? g.M : g.N;
         const double* X = is_a ? a.A : a.B;
@@ -133,10 +137,21 @@ void Context::run_split_gemm(GemmStep& g, kern::GemmArgs& a) {
         const int64_t* Kt = is_a ? a.Ak : a.Bk;
         const bool kc = is_a ? a.a_kcontig : a.b_kcontig;
         const int h = is_a ? g.tA : g.tB;
-        if (is_a ? g.cache_a : g.cache_b) {
+        bool& cached = is_a ? g.cache_a : g.cache_b;
+        if (cached && key >= 0 && split_cache[key].nslices != ns) {
+            // the slice count changed (refinement): re-slice within the budget, or stop caching
+            free_sliced(split_cache[key]);
+            split_cache.erase(key);
+            split_owner.erase(key);
+            key = -1;
+            int64_t used = 0;
+            for (auto& kv : split_cache) used += kv.second.bytes;
+            if (used + slice_bytes(rows, g.K, ns) > cache_budget()) cached = false;
+        }
+        if (cached) {
             if (key < 0) {
                 key = split_cache_next++;
-                split_cache[key] = alloc_sliced(rows, g.K);
+                split_cache[key] = alloc_sliced(rows, g.K, ns);
                 split_owner[key] = h;
                 kern::slice_rows(X, R, Kt, rows, g.K, kc, ns, split_cache[key], stream);
             }
@@ -146,13 +161,14 @@ void Context::run_split_gemm(GemmStep& g, kern::GemmArgs& a) {
         kern::SlicedOperand view = ws;
         view.rows = kern::split_rows_pad(rows);
         view.kpad = kern::split_k_pad(g.K);
+        view.nslices = ns;
         ws_view[is_a ? 0 : 1] = view;
         kern::slice_rows(X, R, Kt, rows, g.K, kc, ns, ws_view[is_a ? 0 : 1], stream);
         return &ws_view[is_a ? 0 : 1];
     };
     kern::SlicedOperand* sa = prepare(true, g.split_cache_a, split_ws.a);
     kern::SlicedOperand* sb = prepare(false, g.split_cache_b, split_ws.b);
-    kern::gemm_split(*sa, *sb, g.M, g.N, g.K, a, stream);
+    kern::gemm_split(*sa, *sb, g.M, g.N, g.K, a, stream, kern::split_ksplit(g.M, g.N, g.K, ns));
 }
 
 }  // namespace ccsd

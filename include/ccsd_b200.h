@@ -158,10 +158,11 @@ typedef struct {
     int    diis_start;    /* default 1     (ccsd.cxx:279-280) */
     double diis_damping;  /* default 0.0   (ccsd.cxx:277-278) */
     int    precision;     /* CCSD_PREC_FP64 or CCSD_PREC_SPLIT */
-    int    slices;        /* split-BF16 slice count; 0 = autotuned */
+    int    slices;        /* split-BF16 slices per operand: 3 (0 = default) or 4 */
     int    use_graph;     /* capture one iteration as a CUDA graph and replay it */
-    double refine_tol;    /* split precision only: once conv < refine_tol, the remaining
-                             iterations use native-FP64 contractions (0 = never) */
+    double refine_tol;    /* split precision only: once conv < refine_tol, 3-slice
+                             contractions move to 4 slices, and 4-slice ones to native
+                             FP64 if the residual then stalls (0 = never) */
 } ccsd_options;
 
 void ccsd_options_default(ccsd_options* opts);
@@ -233,6 +234,9 @@ int ccsd_solver_run(ccsd_solver s, double* energy, double* conv, int* iterations
 int ccsd_solver_amplitudes(ccsd_solver s, ccsd_tensor* T1, ccsd_tensor* T2);
 /* algorithmic FP64 flops of one iteration as planned (packed-pair counts) */
 int ccsd_solver_flops(ccsd_solver s, double* flops);
+/* contraction mode the next iteration uses (changes when refine_tol is reached):
+ * CCSD_PREC_* and, for the split precision, the BF16 slices per operand */
+int ccsd_solver_mode(ccsd_solver s, int* precision, int* slices);
 
 /* Planning query, host only (no device is touched): algorithmic FP64 flops of one
  * iteration (reference flop convention: packed same-spin pairs count once) and the
@@ -261,12 +265,13 @@ int ccsd_dot_batch_noalloc(void* stream, const double* x, const double* const* y
  * No counterpart in the reference (it runs one solve per job).  Requests of any size
  * are queued on submission; an admission thread takes them in arrival order as soon as
  * their planned device bytes (ccsd_plan_query) fit in the memory budget next to the
- * active solves and a slot is free, builds H on a context and stream of their own, and
- * hands them to the iteration thread.  That thread keeps one iteration of every active
- * solve in flight (stream-ordered, no host synchronisation), polls their completion
- * events, and retires a solve when its residual is below conv_tol or max_iter is
- * reached, freeing its memory for the next admission.  Every solve's kernels and
- * reductions are those of a lone solve, so its result does not depend on the mix. */
+ * active solves and a slot is free, and starts a worker thread for each.  The worker
+ * builds H on a context and stream of its own and runs the iterations back to back,
+ * sleeping on each iteration's completion event, until the residual is below conv_tol
+ * or max_iter is reached; then it frees the solve's memory for the next admission.  The
+ * iterations of all active solves overlap on the device through their streams.  Every
+ * solve's kernels and reductions are those of a lone solve, so its result does not
+ * depend on the mix. */
 typedef struct ccsd_server_s* ccsd_server;
 typedef struct {
     int device;

@@ -42,10 +42,31 @@ def test_unpacked_vvvv_matches_oracle():
     assert de < 1e-11 and dt2 < 1e-11
 
 
+@pytest.mark.parametrize("grouped", [True, False], ids=["grouped", "one-launch-per-block"])
 @pytest.mark.parametrize("nirrep", [2, 4, 8])
-def test_symmetry_blocked_matches_oracle(nirrep):
+def test_symmetry_blocked_matches_oracle(nirrep, grouped, monkeypatch):
+    """Symmetry-blocked statements run their small block contractions as grouped
+    launches by default; CCSD_GROUP_GEMMS=0 launches each block on its own."""
+    monkeypatch.setenv("CCSD_GROUP_GEMMS", "1" if grouped else "0")
     de, dt1, dt2 = _run_pair(8, 20, 5, nirrep=nirrep, iters=8)
     assert de < 1e-11 and dt2 < 1e-11
+
+
+def test_grouped_launches_cut_the_launch_count(monkeypatch):
+    counts = {}
+    for grouped in (True, False):
+        monkeypatch.setenv("CCSD_GROUP_GEMMS", "1" if grouped else "0")
+        eps, B, occ, vrt, aux = A.synth_problem(5, 8, 20, nirrep=8)
+        with A.Context(0) as ctx:
+            ctx.set_spaces(vrt=vrt, occ=occ)
+            H = ctx.hamiltonian_from_factor(B, eps, aux_per_irrep=aux)
+            s = ctx.solver(H, diis_order=8)
+            s.iterate()
+            n0 = ctx.launch_count()
+            s.iterate()
+            counts[grouped] = ctx.launch_count() - n0
+            s.close()
+    assert counts[True] * 5 < counts[False], counts
 
 
 def test_graph_replay_matches_eager():

@@ -11,7 +11,7 @@ import aquarius_b200 as A
 
 pytestmark = pytest.mark.gpu
 
-MIX = [(4, 24, 1, 11), (5, 30, 2, 12), (6, 36, 1, 13), (3, 20, 4, 14), (4, 28, 1, 15), (5, 26, 8, 16)]
+MIX = [(4, 24, 1, 11), (5, 30, 2, 12), (6, 36, 1, 13), (4, 20, 4, 14), (4, 28, 1, 15), (8, 26, 8, 16)]
 
 
 def _serve(reqs, **kw):
