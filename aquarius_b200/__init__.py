@@ -32,6 +32,7 @@ STATUS = {
 }
 PREC = {"fp64": 0, "split": 1}
 TENSOR_PACKED = 1
+TENSOR_PLAIN = 2
 
 # symbols declared in include/ccsd_b200.h
 EXPORTS = [
@@ -48,6 +49,8 @@ EXPORTS = [
     "ccsd_hamiltonian_from_fcidump", "ccsd_ctx_set_split_routing", "ccsd_ctx_split_launches",
     "ccsd_server_options_default", "ccsd_server_create", "ccsd_server_submit_synthetic", "ccsd_server_submit_factor",
     "ccsd_server_poll", "ccsd_server_wait", "ccsd_server_stats", "ccsd_server_destroy", "ccsd_solver_mode",
+    "ccsd_rhf_hamiltonian_from_factor", "ccsd_rhf_hamiltonian_from_integrals", "ccsd_rhf_hamiltonian_destroy",
+    "ccsd_rhf_solver_create", "ccsd_rhf_plan_query",
 ]
 
 
@@ -78,6 +81,19 @@ H_SHAPES = {
 
 class Hamiltonian(ctypes.Structure):
     _fields_ = [(f, ctypes.c_int32) for f in H_FIELDS]
+
+
+# closed-shell spatial blocks (rhfccsd.cxx:19-30); VAIJB holds <ai|jb> at [a, i, b, j]
+RHF_FIELDS = ["fAI", "fAB", "fIJ", "VABCD", "VABCI", "VABIJ", "VAIBJ", "VAIJB", "VAIJK", "VIJKL"]
+RHF_SHAPES = {
+    "fAI": ((1, 0), (0, 1)), "fAB": ((1, 0), (1, 0)), "fIJ": ((0, 1), (0, 1)), "VABCD": ((2, 0), (2, 0)),
+    "VABCI": ((2, 0), (1, 1)), "VABIJ": ((2, 0), (0, 2)), "VAIBJ": ((1, 1), (1, 1)), "VAIJB": ((1, 1), (1, 1)),
+    "VAIJK": ((1, 1), (0, 2)), "VIJKL": ((0, 2), (0, 2)),
+}
+
+
+class RHFHamiltonian(ctypes.Structure):
+    _fields_ = [(f, ctypes.c_int32) for f in RHF_FIELDS]
 
 
 class ServerOptions(ctypes.Structure):
@@ -159,6 +175,11 @@ def lib():
             "ccsd_solver_flops": [vp, P(dbl)],
             "ccsd_solver_mode": [vp, P(ctypes.c_int), P(ctypes.c_int)],
             "ccsd_plan_query": [ctypes.c_int, vp, vp, P(Options), ctypes.c_int, P(dbl), P(i64)],
+            "ccsd_rhf_plan_query": [ctypes.c_int, vp, vp, P(Options), P(dbl), P(i64)],
+            "ccsd_rhf_hamiltonian_from_factor": [vp, ctypes.c_int, vp, vp, vp, P(RHFHamiltonian)],
+            "ccsd_rhf_hamiltonian_from_integrals": [vp, ctypes.c_int, vp, vp, P(RHFHamiltonian)],
+            "ccsd_rhf_hamiltonian_destroy": [vp, P(RHFHamiltonian)],
+            "ccsd_rhf_solver_create": [vp, P(RHFHamiltonian), P(Options), P(vp)],
             "ccsd_dot_batch_noalloc": [vp, vp, vp, ctypes.c_int, i64, vp],
             "ccsd_synth_irreps": [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp],
             "ccsd_synth_problem": [ctypes.c_uint64, ctypes.c_int, vp, vp, vp, vp, vp],
@@ -235,6 +256,20 @@ def plan_query(vrt, occ, diis_order=8, pack_vvvv=True, precision="fp64"):
     return fl.value, by.value
 
 
+def rhf_plan_query(vrt, occ, diis_order=8, precision="fp64", refine_tol=0.0):
+    """Host-only planning of the closed-shell iteration: (flops per iteration, device bytes)."""
+    vrt, occ = _ints(vrt), _ints(occ)
+    o = Options()
+    lib().ccsd_options_default(ctypes.byref(o))
+    o.diis_order = diis_order
+    o.precision = PREC[precision]
+    o.refine_tol = refine_tol
+    fl, by = ctypes.c_double(), ctypes.c_int64()
+    _check(lib().ccsd_rhf_plan_query(len(vrt), _ptr(vrt), _ptr(occ), ctypes.byref(o), ctypes.byref(fl),
+                                     ctypes.byref(by)))
+    return fl.value, by.value
+
+
 FCIDUMP_FULL_FOCK = 1
 FCIDUMP_SEMICANONICAL = 2
 
@@ -260,8 +295,8 @@ def fcidump_read(path, full_fock=False):
 # ---------------------------------------------------------------------------
 
 class Tensor:
-    def __init__(self, ctx: "Context", handle: int, name: str, nout, nin, packed=False):
-        self.ctx, self.h, self.name, self.packed = ctx, handle, name, packed
+    def __init__(self, ctx: "Context", handle: int, name: str, nout, nin, packed=False, plain=False):
+        self.ctx, self.h, self.name, self.packed, self.plain = ctx, handle, name, packed, plain
         self.nout, self.nin = tuple(nout), tuple(nin)
         self.group = [0] * nout[0] + [1] * nout[1] + [2] * nin[0] + [3] * nin[1]
         self.ndim = len(self.group)
@@ -352,8 +387,23 @@ class Tensor:
     # -- full spin-orbital array (tests) -------------------------------------------------
     def to_full(self):
         """Dense full spin-orbital array: every index runs over [alpha | beta] of its space,
-        irrep-major inside a spin; antisymmetric images inside groups are filled in."""
+        irrep-major inside a spin; antisymmetric images inside groups are filled in.
+        A plain tensor gives its spatial array (irrep-major per index)."""
         ctx = self.ctx
+        if self.plain:
+            full = np.zeros([ctx.total(self.group[p] % 2) for p in range(self.ndim)])
+            alpha = self.spin_cases()[0]
+            for irr in itertools.product(range(ctx.nirrep), repeat=self.ndim):
+                x = 0
+                for h in irr:
+                    x ^= h
+                if x or self.block_size(alpha, irr) == 0:
+                    continue
+                shape = self.block_shape(alpha, irr)
+                sl = tuple(slice(ctx.offset(self.group[p] % 2, irr[p]), ctx.offset(self.group[p] % 2, irr[p]) + shape[p])
+                           for p in range(self.ndim))
+                full[sl] = self.read_block(alpha, irr).reshape(shape, order="F")
+            return full
         dims = []
         for p in range(self.ndim):
             sp = self.group[p] % 2
@@ -497,11 +547,13 @@ class Context:
         _check(lib().ccsd_ctx_split_launches(self.c, ctypes.byref(n)), self.c)
         return n.value
 
-    def tensor(self, name, nout, nin, packed=False):
+    def tensor(self, name, nout, nin, packed=False, plain=False):
+        """plain: a spatial tensor without antisymmetry or spin cases (closed-shell forms)"""
         h = ctypes.c_int32()
-        _check(lib().ccsd_tensor_create(self.c, name.encode(), _ptr(_ints(nout)), _ptr(_ints(nin)),
-                                        TENSOR_PACKED if packed else 0, ctypes.byref(h)), self.c)
-        return Tensor(self, h.value, name, nout, nin, packed)
+        flags = (TENSOR_PACKED if packed else 0) | (TENSOR_PLAIN if plain else 0)
+        _check(lib().ccsd_tensor_create(self.c, name.encode(), _ptr(_ints(nout)), _ptr(_ints(nin)), flags,
+                                        ctypes.byref(h)), self.c)
+        return Tensor(self, h.value, name, nout, nin, packed, plain)
 
     def contract(self, alpha, A, ia, B, ib, beta, C, ic):
         _check(lib().ccsd_contract(self.c, alpha, A.h, ia.encode(), B.h, ib.encode(), beta, C.h, ic.encode()), self.c)
@@ -594,6 +646,27 @@ class Context:
                                                   1 if pack_vvvv else 0, ctypes.byref(H)), self.c)
         return HamiltonianHandle(self, H, pack_vvvv)
 
+    def rhf_hamiltonian_from_factor(self, B, eps, aux_per_irrep=None):
+        """Closed-shell spatial blocks <pq|rs> from the factor B[P,p,q] and orbital energies."""
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        eps = np.ascontiguousarray(eps, dtype=np.float64)
+        H = RHFHamiltonian()
+        aux = _ints(aux_per_irrep) if aux_per_irrep is not None else None
+        _check(lib().ccsd_rhf_hamiltonian_from_factor(self.c, B.shape[0], _ptr(B), _ptr(eps), _ptr(aux),
+                                                      ctypes.byref(H)), self.c)
+        return RHFHamiltonianHandle(self, H)
+
+    def rhf_hamiltonian_from_integrals(self, fock, eri):
+        """Closed-shell spatial blocks from a Fock matrix and dense (pq|rs) (occupied first)."""
+        fock = np.ascontiguousarray(fock, dtype=np.float64)
+        eri = np.ascontiguousarray(eri, dtype=np.float64)
+        n = fock.shape[0]
+        if fock.shape != (n, n) or eri.shape != (n, n, n, n):
+            raise ValueError("fock must be (n, n) and eri (n, n, n, n)")
+        H = RHFHamiltonian()
+        _check(lib().ccsd_rhf_hamiltonian_from_integrals(self.c, n, _ptr(fock), _ptr(eri), ctypes.byref(H)), self.c)
+        return RHFHamiltonianHandle(self, H)
+
     def solver(self, H, **kw):
         return Solver(self, H, **kw)
 
@@ -612,8 +685,23 @@ class HamiltonianHandle:
             _check(lib().ccsd_hamiltonian_destroy(self.ctx.c, ctypes.byref(self.H)), self.ctx.c)
 
 
+class RHFHamiltonianHandle:
+    def __init__(self, ctx, H):
+        self.ctx, self.H = ctx, H
+        self.tensors = {f: Tensor(ctx, getattr(H, f), f, *RHF_SHAPES[f], plain=True) for f in RHF_FIELDS}
+
+    def __getitem__(self, name):
+        return self.tensors[name]
+
+    def destroy(self):
+        if self.ctx.c:
+            _check(lib().ccsd_rhf_hamiltonian_destroy(self.ctx.c, ctypes.byref(self.H)), self.ctx.c)
+
+
 class Solver:
-    def __init__(self, ctx, H: HamiltonianHandle, conv_tol=1e-9, max_iter=50, diis_order=5, diis_start=1,
+    """CCSD solver over a spin-orbital H (CCSD) or a closed-shell spatial H (RHFCCSD)."""
+
+    def __init__(self, ctx, H, conv_tol=1e-9, max_iter=50, diis_order=5, diis_start=1,
                  precision="fp64", slices=0, use_graph=False, refine_tol=0.0):
         self.ctx = ctx
         o = Options()
@@ -622,12 +710,14 @@ class Solver:
         o.precision, o.slices, o.use_graph = PREC[precision], slices, 1 if use_graph else 0
         o.refine_tol = refine_tol
         s = ctypes.c_void_p()
-        _check(lib().ccsd_solver_create(ctx.c, ctypes.byref(H.H), ctypes.byref(o), ctypes.byref(s)), ctx.c)
+        self.rhf = isinstance(H, RHFHamiltonianHandle)
+        create = lib().ccsd_rhf_solver_create if self.rhf else lib().ccsd_solver_create
+        _check(create(ctx.c, ctypes.byref(H.H), ctypes.byref(o), ctypes.byref(s)), ctx.c)
         self.s = s
         t1, t2 = ctypes.c_int32(), ctypes.c_int32()
         _check(lib().ccsd_solver_amplitudes(s, ctypes.byref(t1), ctypes.byref(t2)), ctx.c)
-        self.T1 = Tensor(ctx, t1.value, "T1", (1, 0), (0, 1))
-        self.T2 = Tensor(ctx, t2.value, "T2", (2, 0), (0, 2))
+        self.T1 = Tensor(ctx, t1.value, "T1", (1, 0), (0, 1), plain=self.rhf)
+        self.T2 = Tensor(ctx, t2.value, "T2", (2, 0), (0, 2), plain=self.rhf)
 
     def close(self):
         if self.s:

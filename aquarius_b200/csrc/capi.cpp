@@ -78,9 +78,10 @@ void key_images(const Tensor& T, int cs, const Block& b, int64_t key, std::vecto
     }
     if (r != 0) throw Error(CCSD_ERR_ARG, "key out of range");
     const SpinCase& sc = T.cases[cs];
-    // same-spin pairs inside a group with equal irreps can be swapped (AS symmetry)
+    // same-spin pairs inside a group with equal irreps can be swapped (AS symmetry);
+    // plain tensors have no antisymmetric images
     std::vector<std::pair<int, int>> swaps;
-    for (int p = 0; p + 1 < nd; p++)
+    for (int p = 0; p + 1 < nd && !T.plain(); p++)
         if (T.group[p] == T.group[p + 1] && sc.spin[p] == sc.spin[p + 1] && b.irrep[p] == b.irrep[p + 1])
             swaps.push_back({p, p + 1});
     const int ns = (int)swaps.size();
@@ -629,6 +630,103 @@ int ccsd_hamiltonian_destroy(ccsd_ctx ctx, ccsd_hamiltonian* H) {
             if (*t && c->tensors.count(*t)) c->destroy_tensor(*t);
             *t = 0;
         }
+    });
+}
+
+int ccsd_rhf_hamiltonian_from_factor(ccsd_ctx ctx, int naux, const double* B, const double* eps,
+                                     const int* aux_per_irrep, ccsd_rhf_hamiltonian* H) {
+    return guarded(ctx, [&] {
+        if (!B || !eps || !H || naux <= 0) throw Error(CCSD_ERR_ARG, "bad factor arguments");
+        Context* c = from_handle(ctx);
+        if (!c->spaces_set) throw Error(CCSD_ERR_ARG, "set the orbital spaces first");
+        build_rhf_hamiltonian(*c, naux, B, eps, aux_per_irrep, H);
+    });
+}
+
+int ccsd_rhf_hamiltonian_from_integrals(ccsd_ctx ctx, int n, const double* fock, const double* eri,
+                                        ccsd_rhf_hamiltonian* H) {
+    return guarded(ctx, [&] {
+        if (!fock || !eri || !H || n <= 0) throw Error(CCSD_ERR_ARG, "bad integral arguments");
+        Context* c = from_handle(ctx);
+        if (!c->spaces_set) throw Error(CCSD_ERR_ARG, "set the orbital spaces first");
+        build_rhf_hamiltonian_dense(*c, n, fock, eri, H);
+    });
+}
+
+int ccsd_rhf_hamiltonian_destroy(ccsd_ctx ctx, ccsd_rhf_hamiltonian* H) {
+    return guarded(ctx, [&] {
+        if (!H) throw Error(CCSD_ERR_ARG, "null hamiltonian");
+        Context* c = from_handle(ctx);
+        for (ccsd_tensor* t : {&H->fAI, &H->fAB, &H->fIJ, &H->VABCD, &H->VABCI, &H->VABIJ, &H->VAIBJ, &H->VAIJB,
+                               &H->VAIJK, &H->VIJKL}) {
+            if (*t && c->tensors.count(*t)) c->destroy_tensor(*t);
+            *t = 0;
+        }
+    });
+}
+
+int ccsd_rhf_solver_create(ccsd_ctx ctx, const ccsd_rhf_hamiltonian* H, const ccsd_options* opts, ccsd_solver* out) {
+    if (!out) return CCSD_ERR_ARG;
+    *out = nullptr;
+    return guarded(ctx, [&] {
+        if (!H) throw Error(CCSD_ERR_ARG, "null hamiltonian");
+        Context* c = from_handle(ctx);
+        ccsd_options o;
+        options_default(&o);
+        if (opts) o = *opts;
+        if (o.precision == CCSD_PREC_SPLIT && !kern::split_supported())
+            throw Error(CCSD_ERR_UNSUPPORTED, "split-BF16 GEMMs need an sm_100 device");
+        auto* h = new ccsd_solver_s;
+        h->ctx = ctx;
+        try {
+            h->s = new Solver(*c, *H, o);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+namespace {
+Spaces query_spaces(int nirrep, const int* vrt, const int* occ, int& n) {
+    if (nirrep != 1 && nirrep != 2 && nirrep != 4 && nirrep != 8) throw Error(CCSD_ERR_ARG, "nirrep must be 1,2,4,8");
+    if (!vrt || !occ) throw Error(CCSD_ERR_ARG, "null orbital counts");
+    Spaces S;
+    S.nirrep = nirrep;
+    n = 0;
+    for (int s = 0; s < 2; s++) {
+        int ov = 0, oo = 0;
+        for (int h = 0; h < nirrep; h++) {
+            S.n[VRT][s][h] = vrt[h];
+            S.n[OCC][s][h] = occ[h];
+            S.off[VRT][s][h] = ov;
+            S.off[OCC][s][h] = oo;
+            ov += vrt[h];
+            oo += occ[h];
+        }
+        n = ov + oo;
+    }
+    return S;
+}
+}  // namespace
+
+int ccsd_rhf_plan_query(int nirrep, const int* vrt, const int* occ, const ccsd_options* opts,
+                        double* flops_per_iter, int64_t* device_bytes) {
+    return guarded(nullptr, [&] {
+        Context host(-1, nullptr);
+        int n = 0;
+        host.spaces = query_spaces(nirrep, vrt, occ, n);
+        host.spaces_set = true;
+        ccsd_rhf_hamiltonian H;
+        create_rhf_hamiltonian_tensors(host, &H);
+        const int64_t build_peak = host.device_bytes + (int64_t)3 * n * n * n * 8;
+        ccsd_options o;
+        options_default(&o);
+        if (opts) o = *opts;
+        Solver s(host, H, o);
+        if (flops_per_iter) *flops_per_iter = s.flops_per_iter;
+        if (device_bytes) *device_bytes = std::max(host.peak_bytes, build_peak);
     });
 }
 

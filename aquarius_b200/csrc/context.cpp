@@ -114,14 +114,18 @@ int Context::create_tensor(const std::string& name, const int nout[2], const int
     if (T->ndim > 8) throw Error(CCSD_ERR_ARG, "tensor rank above 8");
     const int nouttot = nout[0] + nout[1], nintot = nin[0] + nin[1];
     if ((nintot - nouttot) % 2) throw Error(CCSD_ERR_ARG, "odd spin imbalance");
+    if (T->plain() && T->packed()) throw Error(CCSD_ERR_ARG, "a plain tensor has no antisymmetric pairs to pack");
+    if (T->plain() && nintot != nouttot) throw Error(CCSD_ERR_ARG, "plain tensors need as many lower as upper indices");
     const int nirr = spaces.nirrep;
     int64_t offset = 0;
-    // spin cases: #alpha(lower) = #alpha(upper) + (nin - nout)/2  (spinorbital_tensor.cxx:183)
+    // spin cases: #alpha(lower) = #alpha(upper) + (nin - nout)/2  (spinorbital_tensor.cxx:183);
+    // a plain tensor has the one all-alpha case (spatial orbitals)
     for (int a0 = 0; a0 <= gsize[0]; a0++)
         for (int a1 = 0; a1 <= gsize[1]; a1++)
             for (int a2 = 0; a2 <= gsize[2]; a2++)
                 for (int a3 = 0; a3 <= gsize[3]; a3++) {
                     if (a2 + a3 != a0 + a1 + (nintot - nouttot) / 2) continue;
+                    if (T->plain() && (a0 != gsize[0] || a1 != gsize[1] || a2 != gsize[2] || a3 != gsize[3])) continue;
                     SpinCase sc;
                     sc.alpha[0] = a0;
                     sc.alpha[1] = a1;

@@ -99,6 +99,7 @@ struct Tensor {
         return -1;
     }
     bool packed() const { return flags & CCSD_TENSOR_PACKED; }
+    bool plain() const { return flags & CCSD_TENSOR_PLAIN; }
 };
 
 // ---------------------------------------------------------------------------
@@ -241,6 +242,7 @@ public:
     int64_t launches = 0;
     int precision = CCSD_PREC_FP64;
     int slices = 0;
+    bool plan_refine = false;          // host-only plan of a split solve that may move to 4 slices
     int split_routing = CCSD_SPLIT_ROUTE_AUTO;  // which contractions take the split kernel
     bool fp64_tiled_only = false;      // keep skinny FP64 products on the tiled kernel
     bool group_gemms = true;           // batch small block contractions of a statement into grouped launches
@@ -296,6 +298,7 @@ public:
     double* data_of(Plan& p, int h);
     void run_split_gemm(GemmStep& g, kern::GemmArgs& a);
     bool routes_split(const GemmStep& g) const;   // would run_gemm send g to the split kernel
+    bool split_eligible(const GemmStep& g) const; // shape / operand rule of the split path
     kern::GemmArgs gemm_args(Plan& p, const GemmStep& g);
     RunSchedule& schedule(Plan& p);
     void build_run(Plan& p, RunSchedule& rs, int first, int end);

@@ -85,6 +85,7 @@ struct TensorRef {
         void operator-=(const IndexedMult& m) { Lhs{r, h, idx} -= m; }
         void operator=(const Proxy& x) { Lhs{r, h, idx} = Indexed(x); }
         void operator+=(const Proxy& x) { Lhs{r, h, idx} += Indexed(x); }
+        void operator-=(const Proxy& x) { Lhs{r, h, idx} -= Indexed(x); }
     };
     Proxy operator[](const char* idx) const { return Proxy{r, h, idx}; }
 };

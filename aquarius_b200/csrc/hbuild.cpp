@@ -186,6 +186,23 @@ struct Builder {
             }
     }
 
+    // every block of a plain (spatial) two-electron tensor as one Coulomb piece
+    // (x_pa x_pb | x_pc x_pd): the non-antisymmetrised <pq|rs> of the RHF integrals
+    void coulomb_plain(int h, int pa, int pb, int pc, int pd) {
+        Tensor& T = ctx.tensor(h);
+        for (auto& sc : T.cases)
+            for (auto& b : sc.blocks) {
+                if (b.size == 0) continue;
+                int space[4], irr[4], len[4];
+                for (int p = 0; p < 4; p++) {
+                    space[p] = group_space(T.group[p]);
+                    irr[p] = b.irrep[p];
+                    len[p] = b.len[p];
+                }
+                coulomb(T.data, b.offset, space, irr, len, b.stride.data(), pa, pb, pc, pd, 1.0);
+            }
+    }
+
     // packed V_abcd-type block: chunk over the first index, build (ac|bd) and (ad|bc)
     // unpacked for the chunk, then pack <ab||cd> for canonical pairs
     void packed_block(Tensor& T, const SpinCase& sc, const Block& b, const int* space, const int* irr,
@@ -299,6 +316,86 @@ void create_hamiltonian_tensors(Context& ctx, bool pack_vvvv, ccsd_hamiltonian* 
         int no[2] = {2, 0}, ni[2] = {1, 1};
         H->VABEJ = ctx.create_view("<ab||ci>", H->VAMEF, no, ni, perm);
     }
+}
+
+void create_rhf_hamiltonian_tensors(Context& ctx, ccsd_rhf_hamiltonian* H) {
+    const int P = CCSD_TENSOR_PLAIN;
+    H->fAI = mk(ctx, "fAI", 1, 0, 0, 1, P);
+    H->fAB = mk(ctx, "fAB", 1, 0, 1, 0, P);
+    H->fIJ = mk(ctx, "fIJ", 0, 1, 0, 1, P);
+    H->VABCD = mk(ctx, "<Ab|Cd>", 2, 0, 2, 0, P);
+    H->VABCI = mk(ctx, "<Ab|Ci>", 2, 0, 1, 1, P);
+    H->VABIJ = mk(ctx, "<Ab|Ij>", 2, 0, 0, 2, P);
+    H->VAIBJ = mk(ctx, "<Ai|Bj>", 1, 1, 1, 1, P);
+    H->VAIJB = mk(ctx, "<Ai|Jb>", 1, 1, 1, 1, P);
+    H->VAIJK = mk(ctx, "<Ai|Jk>", 1, 1, 0, 2, P);
+    H->VIJKL = mk(ctx, "<Ij|Kl>", 0, 2, 0, 2, P);
+}
+
+namespace {
+
+// <pq|rs> = (pr|qs): positions (0,2 | 1,3) of every block, except VAIJB whose element
+// <ai|jb> = (aj|ib) is stored at [a, i, b, j] (positions 0,3 | 1,2); the block list of
+// the reference's RHF integrals (rhfaomoints.cxx:59-66)
+void fill_rhf_two_electron(Builder& bld, const ccsd_rhf_hamiltonian* H) {
+    for (int h : {H->VABCD, H->VABCI, H->VABIJ, H->VAIBJ, H->VAIJK, H->VIJKL}) bld.coulomb_plain(h, 0, 2, 1, 3);
+    bld.coulomb_plain(H->VAIJB, 0, 3, 1, 2);
+}
+
+void require_closed_shell(const Spaces& S, const char* who) {
+    for (int h = 0; h < S.nirrep; h++)
+        for (int sp = 0; sp < 2; sp++)
+            if (S.n[sp][ALPHA][h] != S.n[sp][BETA][h])
+                throw Error(CCSD_ERR_ARG, std::string(who) + " needs a closed-shell (alpha = beta) space");
+}
+
+}  // namespace
+
+void build_rhf_hamiltonian(Context& ctx, int naux, const double* B, const double* eps, const int* aux_per_irrep,
+                           ccsd_rhf_hamiltonian* H) {
+    const Spaces& S = ctx.spaces;
+    require_closed_shell(S, "the RHF builder");
+    Builder bld{ctx, S.total(VRT, ALPHA) + S.total(OCC, ALPHA), naux, S.total(OCC, ALPHA)};
+    if (aux_per_irrep) {
+        bld.aux_known = true;
+        for (int h = 0; h < S.nirrep; h++)
+            for (int k = 0; k < aux_per_irrep[h]; k++) bld.aux_irrep.push_back(h);
+        if ((int)bld.aux_irrep.size() != naux) throw Error(CCSD_ERR_ARG, "aux_per_irrep does not sum to naux");
+    }
+    const int64_t nB = (int64_t)naux * bld.n * bld.n;
+    bld.dB = (double*)ctx.dmalloc(nB * sizeof(double));
+    CCSD_CUDA(cudaMemcpyAsync(bld.dB, B, nB * sizeof(double), cudaMemcpyHostToDevice, ctx.stream));
+    create_rhf_hamiltonian_tensors(ctx, H);
+    bld.one_electron(H->fAB, eps);
+    bld.one_electron(H->fIJ, eps);
+    fill_rhf_two_electron(bld, H);
+    CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
+    ctx.dfree(bld.dB, nB * sizeof(double));
+}
+
+void build_rhf_hamiltonian_dense(Context& ctx, int n, const double* fock, const double* eri, ccsd_rhf_hamiltonian* H) {
+    const Spaces& S = ctx.spaces;
+    require_closed_shell(S, "the RHF builder");
+    if (n != S.total(VRT, ALPHA) + S.total(OCC, ALPHA))
+        throw Error(CCSD_ERR_ARG, "orbital count differs from the context's spaces");
+    const int64_t ne = (int64_t)n * n * n * n;
+    Builder bld{ctx, n, 0, S.total(OCC, ALPHA)};
+    double* d = (double*)ctx.dmalloc(ne * sizeof(double));
+    struct Free {
+        Context& c;
+        double* p;
+        int64_t b;
+        ~Free() {
+            cudaStreamSynchronize(c.stream);
+            c.dfree(p, b);
+        }
+    } guard{ctx, d, ne * (int64_t)sizeof(double)};
+    CCSD_CUDA(cudaMemcpyAsync(d, eri, ne * sizeof(double), cudaMemcpyHostToDevice, ctx.stream));
+    bld.dEri = d;
+    create_rhf_hamiltonian_tensors(ctx, H);
+    for (int h : {H->fAI, H->fAB, H->fIJ}) bld.one_electron_full(h, fock);
+    fill_rhf_two_electron(bld, H);
+    CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
 }
 
 void build_hamiltonian(Context& ctx, int naux, const double* B, const double* eps, const int* aux_per_irrep,

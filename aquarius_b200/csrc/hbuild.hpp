@@ -12,6 +12,12 @@ void build_hamiltonian(Context& ctx, int naux, const double* B, const double* ep
 // fastest, orbitals ordered occupied first, irrep-major inside occ and vrt
 void build_hamiltonian_dense(Context& ctx, int n, const double* fock, const double* eri, bool pack_vvvv,
                              ccsd_hamiltonian* H);
+// the 10 plain spatial blocks of the closed-shell (RHF) Hamiltonian, zero-filled, and
+// their builders from the factor / the dense integrals (arguments as above)
+void create_rhf_hamiltonian_tensors(Context& ctx, ccsd_rhf_hamiltonian* H);
+void build_rhf_hamiltonian(Context& ctx, int naux, const double* B, const double* eps, const int* aux_per_irrep,
+                           ccsd_rhf_hamiltonian* H);
+void build_rhf_hamiltonian_dense(Context& ctx, int n, const double* fock, const double* eri, ccsd_rhf_hamiltonian* H);
 
 // FCIDUMP contents: h[n*n], eri[n^4] dense, core energy
 struct Fcidump {

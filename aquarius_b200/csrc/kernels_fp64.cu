@@ -187,6 +187,30 @@ __device__ __forceinline__ void fp64_tile(const GemmArgs& g, const int m0, const
         return;
     }
 
+    if (g.nvm == 1 && g.nvn == 1) {
+        // one destination per element: the 8 read-modify-writes of a row group are
+        // issued as 8 reads, then 8 writes (overlapped instead of one by one)
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int m = m0 + wm + i * 8 + (lane >> 2);
+            if (m >= g.M) continue;
+            const int64_t cm = g.Cm[0][m];
+            const double sc = g.alpha * g.vsign[0];
+            int64_t off[8];
+            double old[8];
+#pragma unroll
+            for (int t = 0; t < 8; t++) {
+                const int n = n0 + wn + (t >> 1) * 8 + 2 * (lane & 3) + (t & 1);
+                off[t] = n < g.N ? cm + g.Cn[0][n] : -1;
+            }
+#pragma unroll
+            for (int t = 0; t < 8; t++) old[t] = off[t] >= 0 ? g.C[off[t]] : 0.0;
+#pragma unroll
+            for (int t = 0; t < 8; t++)
+                if (off[t] >= 0) g.C[off[t]] = old[t] + sc * acc[i][t >> 1][t & 1];
+        }
+        return;
+    }
     // epilogue: scatter to every destination variant
 #pragma unroll
     for (int i = 0; i < 4; i++) {
@@ -390,6 +414,29 @@ __global__ void __launch_bounds__(SK_THREADS, 1) skinny_kernel(SkinnyArgs g) {
                 const int s = ty * 8 + j;
                 if (s < g.NS) wz[(int64_t)r * g.NS + s] = acc[i][j];
             }
+        }
+        return;
+    }
+    if (g.nvr == 1 && g.nvs == 1) {
+        // one destination per element: 8 reads, then 8 writes per row
+        const double sc = g.alpha * g.vsign[0];
+#pragma unroll
+        for (int i = 0; i < SK_RPT; i++) {
+            const int r = r0 + tx + i * Sh::TX;
+            if (r >= g.R) continue;
+            const int64_t cr = g.Cr[0][r];
+            int64_t off[8];
+            double old[8];
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                const int s = ty * 8 + j;
+                off[j] = s < g.NS ? cr + g.Cs[0][s] : -1;
+            }
+#pragma unroll
+            for (int j = 0; j < 8; j++) old[j] = off[j] >= 0 ? g.C[off[j]] : 0.0;
+#pragma unroll
+            for (int j = 0; j < 8; j++)
+                if (off[j] >= 0) g.C[off[j]] = old[j] + sc * acc[i][j];
         }
         return;
     }

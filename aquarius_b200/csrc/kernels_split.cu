@@ -344,6 +344,32 @@ __global__ void __launch_bounds__(THREADS, 1)
                     if (n < p.N) wz[n] = sa * p.scaleB[n] * acc[j];
                 }
             }
+        } else if (ok && p.nvm == 1 && p.nvn == 1) {
+            // one destination per element: read EB destinations, then write them, so that
+            // the read-modify-writes of a thread overlap instead of running one by one
+            constexpr int EB = 8;
+            const int m = m0 + q * 32 + lane;
+            if (m < p.M) {
+                const double sa = p.alpha * p.vsign[0] * p.scaleA[m];
+                const int64_t cm0 = p.Cm0[m];
+#pragma unroll
+                for (int j0 = 0; j0 < COLS; j0 += EB) {
+                    int64_t off[EB];
+                    double old[EB];
+#pragma unroll
+                    for (int t = 0; t < EB; t++) {
+                        const int n = n0 + h * COLS + j0 + t;
+                        off[t] = n < p.N ? cm0 + p.Cn0[n] : -1;
+                    }
+#pragma unroll
+                    for (int t = 0; t < EB; t++) old[t] = off[t] >= 0 ? p.C[off[t]] : 0.0;
+#pragma unroll
+                    for (int t = 0; t < EB; t++) {
+                        const int n = n0 + h * COLS + j0 + t;
+                        if (off[t] >= 0) p.C[off[t]] = old[t] + sa * p.scaleB[n] * acc[j0 + t];
+                    }
+                }
+            }
         } else if (ok) {
             const int m = m0 + q * 32 + lane;
             if (m < p.M) {

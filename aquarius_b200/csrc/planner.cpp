@@ -358,6 +358,7 @@ void lower_gemm(Context& ctx, Term& t, int hA, int hB, int hC, int cc, std::set<
     double factor = 1.0;
     auto find_pairs = [&](const std::vector<int>& vl, const Operand& op1, const Operand* op2,
                           std::vector<std::pair<int, int>>& out, bool external) {
+        if (op1.t->plain()) return;   // no antisymmetric pairs in plain tensors
         std::set<int> used;
         for (size_t i = 0; i < vl.size(); i++)
             for (size_t j = i + 1; j < vl.size(); j++) {
@@ -542,6 +543,11 @@ Plan plan_contract(Context& ctx, double alpha, int hA, const std::string& idxA, 
     Tensor& C = ctx.tensor(hC);
     if (hA == hC || hB == hC) fail(CCSD_ERR_ARG, "output tensor aliases an input");
     if (C.packed()) fail(CCSD_ERR_PLAN, "packed output tensors are not supported");
+    // plain (spatial, no antisymmetry) statements are plain einsums: no antisymmetriser,
+    // no spin cases beyond all-alpha, no pair restrictions
+    const bool plain = C.plain();
+    if (A.plain() != plain || B.plain() != plain)
+        fail(CCSD_ERR_PLAN, "plain and spin-orbital tensors mixed in one statement");
     Letters L;
     std::map<char, int> sp;
     index_check(A, idxA, "A", L.inA, sp);
@@ -567,7 +573,7 @@ Plan plan_contract(Context& ctx, double alpha, int hA, const std::string& idxA, 
     // antisymmetrisers per C group
     std::vector<std::vector<int>> grp_pos;
     std::vector<std::vector<Shuffle>> grp_sh;
-    for (int g = 0; g < 4; g++) {
+    for (int g = 0; g < 4 && !plain; g++) {
         std::vector<int> pos, sub;
         for (int p = 0; p < C.ndim; p++)
             if (C.group[p] == g) {
@@ -608,7 +614,7 @@ Plan plan_contract(Context& ctx, double alpha, int hA, const std::string& idxA, 
     // equal contributions, so only alpha-before-beta is kept, with weight 2 -- the merge
     // of equal terms done by the reference's spin integration (spinorbital_tensor.cxx:676-694).
     std::vector<std::pair<int, int>> sym_int;
-    {
+    if (!plain) {
         auto group_internal_count = [&](const Tensor& T, const std::map<char, int>& pos, int g) {
             int n = 0;
             for (char c : internal)
@@ -672,6 +678,8 @@ Plan plan_contract(Context& ctx, double alpha, int hA, const std::string& idxA, 
                         vars[p].irrep = bC.irrep[p];
                         vars[p].len = ctx.spaces.n[vars[p].space][vars[p].spin][vars[p].irrep];
                     }
+                    // external letters sit at their own C position unless the shuffle moves them
+                    for (char c : ext) var_of[c] = L.inC[c];
                     for (auto& kv : sh.first) var_of[kv.first] = kv.second;
                     for (int i = 0; i < nint; i++) {
                         var_of[internal[i]] = C.ndim + i;
@@ -877,6 +885,7 @@ Plan plan_sum(Context& ctx, double alpha, int hA, const std::string& idxA, doubl
     Tensor& C = ctx.tensor(hC);
     if (hA == hC) fail(CCSD_ERR_ARG, "sum with aliased input and output");
     if (C.packed() || A.packed()) fail(CCSD_ERR_PLAN, "sum over packed tensors is not supported");
+    if (A.plain() != C.plain()) fail(CCSD_ERR_PLAN, "plain and spin-orbital tensors mixed in one sum");
     Letters L;
     std::map<char, int> sp;
     index_check(A, idxA, "A", L.inA, sp);
@@ -950,6 +959,7 @@ Plan plan_dot(Context& ctx, int hA, const std::string& idxA, int hB, const std::
     Tensor& A = ctx.tensor(hA);
     Tensor& B = ctx.tensor(hB);
     if (A.packed() || B.packed()) fail(CCSD_ERR_PLAN, "dot over packed tensors is not supported");
+    if (A.plain() != B.plain()) fail(CCSD_ERR_PLAN, "plain and spin-orbital tensors mixed in one dot");
     Letters L;
     std::map<char, int> sp;
     index_check(A, idxA, "A", L.inA, sp);

@@ -36,17 +36,6 @@ void options_default(ccsd_options* o) {
 }
 
 Solver::Solver(Context& c, const ccsd_hamiltonian& h, const ccsd_options& o) : ctx(c), H(h), opts(o) {
-    if (opts.diis_damping != 0.0) throw Error(CCSD_ERR_UNSUPPORTED, "DIIS damping is not supported");
-    if (opts.diis_order < 1 || opts.diis_order > 16) throw Error(CCSD_ERR_ARG, "diis_order must be in 1..16");
-    if (opts.slices != 0 && opts.slices != 3 && opts.slices != 4)
-        throw Error(CCSD_ERR_ARG, "slices must be 0 (default), 3 or 4");
-    ctx.precision = opts.precision;
-    ctx.slices = opts.slices;
-    // constants: the H blocks never change, so their split slices can be cached
-    for (int t : {H.fAI, H.fME, H.fAE, H.fMI, H.VMNIJ, H.VAMIJ, H.VMNEJ, H.VABIJ, H.VMNEF, H.VAMEI, H.VAMEF,
-                  H.VABEJ, H.VABEF})
-        ctx.constant_tensors.push_back(t);
-
     // ccsd.cxx:37-48
     T1 = mk(ctx, "T(1)", 1, 0, 0, 1);
     T2 = mk(ctx, "T(2)", 2, 0, 0, 2);
@@ -60,16 +49,72 @@ Solver::Solver(Context& c, const ccsd_hamiltonian& h, const ccsd_options& o) : c
     WMNEJ = mk(ctx, "W(mn,ej)", 0, 2, 1, 1);
     WAMIJ = mk(ctx, "W~(am,ij)", 1, 1, 0, 2);
     WAMEI = mk(ctx, "W~(am,ei)", 1, 1, 1, 1);
+    setup();
+}
+
+// Closed-shell spin-adapted form (rhfccsd.cxx:44-110): plain spatial tensors, positions in
+// [upper vrt, upper occ, lower vrt, lower occ] order (VAIJBSA and W(Am,Ie) therefore hold
+// their [a, i, j, b] elements at [a, i, b, j]).
+Solver::Solver(Context& c, const ccsd_rhf_hamiltonian& h, const ccsd_options& o)
+    : ctx(c), HR(h), rhf(true), opts(o) {
+    const int P = CCSD_TENSOR_PLAIN;
+    T1 = mk(ctx, "T1", 1, 0, 0, 1, P);
+    T2 = mk(ctx, "T2", 2, 0, 0, 2, P);
+    Z1 = mk(ctx, "Z1", 1, 0, 0, 1, P);
+    Z2 = mk(ctx, "Z2", 2, 0, 0, 2, P);
+    Z2c = mk(ctx, "Z2 (copy)", 2, 0, 0, 2, P);
+    Tau = mk(ctx, "Tau", 2, 0, 0, 2, P);
+    T2SA = mk(ctx, "T2SA", 2, 0, 0, 2, P);
+    TauSA = mk(ctx, "TauSA", 2, 0, 0, 2, P);
+    VABIJSA = mk(ctx, "VABIJSA", 2, 0, 0, 2, P);
+    VAIJBSA = mk(ctx, "VAIJBSA", 1, 1, 1, 1, P);
+    FME = mk(ctx, "F(ME)", 0, 1, 1, 0, P);
+    FMI = mk(ctx, "F(MI)", 0, 1, 0, 1, P);
+    FAE = mk(ctx, "F(AE)", 1, 0, 1, 0, P);
+    WMNIJ = mk(ctx, "W(Mn,Ij)", 0, 2, 0, 2, P);
+    WMNIJc = mk(ctx, "W(Mn,Ij) (copy)", 0, 2, 0, 2, P);
+    WMNEJ = mk(ctx, "W(Mn,Ej)", 0, 2, 1, 1, P);
+    WAMIJ = mk(ctx, "W(Am,Ij)", 1, 1, 0, 2, P);
+    WAMEI = mk(ctx, "W(Am,Ei)", 1, 1, 1, 1, P);
+    WAMIE = mk(ctx, "W(Am,Ie)", 1, 1, 1, 1, P);
+    setup();
+}
+
+std::vector<int> Solver::constants() const {
+    if (rhf)
+        return {HR.fAI, HR.fAB, HR.fIJ, HR.VABCD, HR.VABCI, HR.VABIJ, HR.VAIBJ, HR.VAIJB, HR.VAIJK, HR.VIJKL,
+                VABIJSA, VAIJBSA};
+    return {H.fAI, H.fME, H.fAE, H.fMI, H.VMNIJ, H.VAMIJ, H.VMNEJ, H.VABIJ, H.VMNEF, H.VAMEI, H.VAMEF, H.VABEJ, H.VABEF};
+}
+
+std::vector<int> Solver::owned_tensors() const {
+    std::vector<int> t = {T1, T2, Z1, Z2, Tau, FME, FMI, FAE, WMNIJ, WMNEJ, WAMIJ, WAMEI};
+    if (rhf)
+        for (int x : {T2SA, TauSA, VABIJSA, VAIJBSA, WAMIE, WMNIJc, Z2c}) t.push_back(x);
+    return t;
+}
+
+void Solver::setup() {
+    if (opts.diis_damping != 0.0) throw Error(CCSD_ERR_UNSUPPORTED, "DIIS damping is not supported");
+    if (opts.diis_order < 1 || opts.diis_order > 16) throw Error(CCSD_ERR_ARG, "diis_order must be in 1..16");
+    if (opts.slices != 0 && opts.slices != 3 && opts.slices != 4)
+        throw Error(CCSD_ERR_ARG, "slices must be 0 (default), 3 or 4");
+    ctx.precision = opts.precision;
+    ctx.slices = opts.slices;
+    // constants: the H blocks never change, so their split slices can be cached
+    for (int t : constants()) ctx.constant_tensors.push_back(t);
 
     if (ctx.host_only) {
         // planning query: account every allocation and plan one iteration, launch nothing
+        ctx.plan_refine = opts.precision == CCSD_PREC_SPLIT && opts.refine_tol > 0;
         for (int sp = 0; sp < 2; sp++)
             for (int s = 0; s < 2; s++) den[sp][s] = (double*)alloc(std::max(ctx.spaces.total(sp, s), 1) * sizeof(double));
         build_diis();
         d_red = (double*)alloc(8 * sizeof(double));
         record_tau(tau_plan);
         record_energy(energy_plan);
-        record_iteration();
+        if (rhf) record_iteration_rhf();
+        else record_iteration();
         ctx.upload(iter_plan);
         ctx.upload(tau_plan);
         ctx.upload(energy_plan);
@@ -90,13 +135,25 @@ Solver::Solver(Context& c, const ccsd_hamiltonian& h, const ccsd_options& o) : c
     CCSD_CUDA(cudaMallocHost(&h_red, 8 * sizeof(double)));
     CCSD_CUDA(cudaMallocHost(&h_state, 8 * sizeof(int)));
 
-    // ---- initial guess and MP2 (ccsd.cxx:50-62) -------------------------------
+    // ---- initial guess and MP2 (ccsd.cxx:50-62; rhfccsd.cxx:72-86) -------------
     {
         Plan init;
         Recorder r{&ctx, &init};
-        TensorRef t1{&r, T1}, t2{&r, T2}, fai{&r, H.fAI}, vabij{&r, H.VABIJ};
-        t1["ai"] = fai["ai"];
-        t2["abij"] = vabij["abij"];
+        TensorRef t1{&r, T1}, t2{&r, T2};
+        if (rhf) {
+            TensorRef fai{&r, HR.fAI}, vabij{&r, HR.VABIJ}, vaijb{&r, HR.VAIJB}, vaibj{&r, HR.VAIBJ};
+            TensorRef sa{&r, VABIJSA}, sb{&r, VAIJBSA};
+            t1["ai"] = fai["ai"];
+            t2["abij"] = vabij["abij"];
+            sa["abij"] = 2.0 * vabij["abij"];
+            sa["abij"] -= vabij["abji"];
+            sb["aibj"] = 2.0 * vaijb["aibj"];
+            sb["aibj"] -= vaibj["aibj"];
+        } else {
+            TensorRef fai{&r, H.fAI}, vabij{&r, H.VABIJ};
+            t1["ai"] = fai["ai"];
+            t2["abij"] = vabij["abij"];
+        }
         ctx.run(init);
         weight_tensor(T1);
         weight_tensor(T2);
@@ -113,7 +170,8 @@ Solver::Solver(Context& c, const ccsd_hamiltonian& h, const ccsd_options& o) : c
     energy = mp2;
     conv = std::numeric_limits<double>::max();
 
-    record_iteration();
+    if (rhf) record_iteration_rhf();
+    else record_iteration();
     ctx.upload(iter_plan);
     ctx.upload(tau_plan);
     ctx.upload(energy_plan);
@@ -126,13 +184,13 @@ Solver::~Solver() {
     ctx.release(iter_plan);
     ctx.release(tau_plan);
     ctx.release(energy_plan);
-    for (int t : {T1, T2, Z1, Z2, Tau, FME, FMI, FAE, WMNIJ, WMNEJ, WAMIJ, WAMEI})
+    const std::vector<int> cons = constants();
+    for (int t : owned_tensors())
         if (ctx.tensors.count(t)) ctx.destroy_tensor(t);
     for (auto p : owned) ctx.dfree(p.first, p.second);
     if (h_red) cudaFreeHost(h_red);
     if (h_state) cudaFreeHost(h_state);
-    for (int t : {H.fAI, H.fME, H.fAE, H.fMI, H.VMNIJ, H.VAMIJ, H.VMNEJ, H.VABIJ, H.VMNEF, H.VAMEI, H.VAMEF,
-                  H.VABEJ, H.VABEF})
+    for (int t : cons)
         ctx.constant_tensors.erase(std::remove(ctx.constant_tensors.begin(), ctx.constant_tensors.end(), t),
                                    ctx.constant_tensors.end());
 }
@@ -152,8 +210,12 @@ void Solver::build_denominators() {
             int n = S.total(sp, s);
             den[sp][s] = (double*)alloc(std::max(n, 1) * sizeof(double));
             std::vector<double> host(std::max(n, 1), 0.0);
-            int tf = sp == VRT ? H.fAE : H.fMI;
+            const int tf = rhf ? (sp == VRT ? HR.fAB : HR.fIJ) : (sp == VRT ? H.fAE : H.fMI);
             Tensor& F = ctx.tensor(tf);
+            if (rhf && s == BETA) {   // spatial orbitals: one set of denominators
+                CCSD_CUDA(cudaMemcpy(den[sp][s], host.data(), std::max(n, 1) * sizeof(double), cudaMemcpyHostToDevice));
+                continue;
+            }
             int alpha[4] = {0, 0, 0, 0};
             if (s == ALPHA) {
                 if (sp == VRT) alpha[0] = alpha[2] = 1;
@@ -234,7 +296,7 @@ void Solver::build_tau_blocks() {
                     a.t1bj = t1.data + y->offset;
                 }
             }
-            if (sa == sj && sb == si && ha == hj && hb == hi) {
+            if (!rhf && sa == sj && sb == si && ha == hj && hb == hi) {
                 const Block* x = t1_block(sa, ha);
                 const Block* y = t1_block(sb, hb);
                 if (x && y && x->size && y->size) {
@@ -254,12 +316,21 @@ void Solver::launch_tau() {
 void Solver::record_tau(Plan& p) {
     Recorder r{&ctx, &p};
     TensorRef tau{&r, Tau}, t1{&r, T1}, t2{&r, T2};
-    // ccsd.cxx:123-124
+    // ccsd.cxx:123-124; rhfccsd.cxx:237-238 (no antisymmetriser: plain tensors)
     tau["abij"] = t2["abij"];
-    tau["abij"] += 0.5 * t1["ai"] * t1["bj"];
+    tau["abij"] += (rhf ? 1.0 : 0.5) * t1["ai"] * t1["bj"];
 }
 
 void Solver::record_energy(Plan& p) {
+    if (rhf) {
+        // energy = 2 <fAI|T1> + <VABIJSA|Tau>  (rhfccsd.cxx:320)
+        Plan a = plan_dot(ctx, HR.fAI, "ai", T1, "ai");
+        for (auto& d : a.dots) d.alpha *= 2.0;
+        Plan b = plan_dot(ctx, VABIJSA, "abij", Tau, "abij");
+        p.append(std::move(a));
+        p.append(std::move(b));
+        return;
+    }
     // energy = <fAI|T1> + 1/4 <VABIJ|Tau> over full spin-orbital ranges (ccsd.cxx:189)
     Plan a = plan_dot(ctx, H.fAI, "ai", T1, "ai");
     Plan b = plan_dot(ctx, H.VABIJ, "abij", Tau, "abij");
@@ -330,6 +401,95 @@ void Solver::record_iteration() {
     Z2r["abij"] += WAMEIr["amei"] * T2r["ebjm"];
 }
 
+// RHFCCSD<U>::iterate (rhfccsd.cxx:237-306) over plain tensors.  Index strings follow
+// each tensor's stored position order; for VAIJB, VAIJBSA and W(Am,Ie), whose elements
+// [a, i, j, b] sit at positions [a, i, b, j], the reference's "amie" reads "amei".
+// The two in-place symmetrisations (W(Mn,Ij) += W(Mn,Ij)[nmji], Z2 += Z2[baji]) are
+// accumulated in a second tensor and folded once.
+void Solver::record_iteration_rhf() {
+    Plan& p = iter_plan;
+    Recorder r{&ctx, &p};
+    TensorRef fAI{&r, HR.fAI}, fAB{&r, HR.fAB}, fIJ{&r, HR.fIJ};
+    TensorRef VABCD{&r, HR.VABCD}, VABCI{&r, HR.VABCI}, VABIJ{&r, HR.VABIJ}, VAIBJ{&r, HR.VAIBJ};
+    TensorRef VAIJB{&r, HR.VAIJB}, VAIJK{&r, HR.VAIJK}, VIJKL{&r, HR.VIJKL};
+    TensorRef VABIJSAr{&r, VABIJSA}, VAIJBSAr{&r, VAIJBSA};
+    TensorRef T1r{&r, T1}, T2r{&r, T2}, Z1r{&r, Z1}, Z2r{&r, Z2}, Z2cr{&r, Z2c}, Taur{&r, Tau};
+    TensorRef T2SAr{&r, T2SA}, TauSAr{&r, TauSA};
+    TensorRef FMEr{&r, FME}, FAEr{&r, FAE}, FMIr{&r, FMI};
+    TensorRef WMNIJr{&r, WMNIJ}, WMNIJcr{&r, WMNIJc}, WMNEJr{&r, WMNEJ}, WAMIJr{&r, WAMIJ};
+    TensorRef WAMEIr{&r, WAMEI}, WAMIEr{&r, WAMIE};
+
+    // Tau = T2 + t_ai t_bj comes from the fused Tau kernel before this plan runs
+    TauSAr["abij"] = 2.0 * Taur["abij"];
+    TauSAr["abij"] -= Taur["abji"];
+    T2SAr["abij"] = 2.0 * T2r["abij"];
+    T2SAr["abij"] -= T2r["abji"];
+
+    // intermediates (rhfccsd.cxx:249-288)
+    FMEr["me"] = fAI["em"];
+    FMEr["me"] += VABIJSAr["efmn"] * T1r["fn"];
+
+    FMIr["mi"] = fIJ["mi"];
+    FMIr["mi"] += VABIJSAr["efmn"] * T2r["efin"];
+    FMIr["mi"] += FMEr["me"] * T1r["ei"];
+    FMIr["mi"] += 2.0 * VAIJK["finm"] * T1r["fn"];
+    FMIr["mi"] -= VAIJK["fimn"] * T1r["fn"];
+
+    FAEr["ae"] = fAB["ae"];
+    FAEr["ae"] -= VABIJSAr["efmn"] * T2r["afmn"];
+    FAEr["ae"] -= FMEr["me"] * T1r["am"];
+    FAEr["ae"] += 2.0 * VABCI["efam"] * T1r["fm"];
+    FAEr["ae"] -= VABCI["feam"] * T1r["fm"];
+
+    WMNIJcr["mnij"] = 0.5 * VIJKL["mnij"];
+    WMNIJcr["mnij"] += 0.5 * VABIJ["efmn"] * Taur["efij"];
+    WMNIJcr["mnij"] += VAIJK["ejmn"] * T1r["ei"];
+    WMNIJr["mnij"] = WMNIJcr["mnij"];
+    WMNIJr["mnij"] += WMNIJcr["nmji"];
+
+    WMNEJr["mnej"] = VAIJK["ejmn"];
+    WMNEJr["mnej"] += VABIJ["efmn"] * T1r["fj"];
+
+    WAMIJr["amij"] = VAIJK["amij"];
+    WAMIJr["amij"] += VABCI["efam"] * Taur["efij"];
+    WAMIJr["amij"] += VAIBJ["amej"] * T1r["ei"];
+    WAMIJr["amij"] += VAIJB["amei"] * T1r["ej"];
+
+    WAMIEr["amei"] = VAIJBSAr["amei"];
+    WAMIEr["amei"] += 0.5 * VABIJSAr["efmn"] * T2SAr["afin"];
+    WAMIEr["amei"] += 2.0 * VABCI["feam"] * T1r["fi"];
+    WAMIEr["amei"] -= VABCI["efam"] * T1r["fi"];
+    WAMIEr["amei"] -= 2.0 * WMNEJr["mnei"] * T1r["an"];
+    WAMIEr["amei"] += WMNEJr["nmei"] * T1r["an"];
+
+    WAMEIr["amei"] = VAIBJ["amei"];
+    WAMEIr["amei"] -= 0.5 * VABIJ["efnm"] * T2r["afni"];
+    WAMEIr["amei"] += VABCI["efam"] * T1r["fi"];
+    WAMEIr["amei"] -= WMNEJr["nmei"] * T1r["an"];
+
+    // residual (rhfccsd.cxx:295-316)
+    Z1r["ai"] = fAI["ai"];
+    Z1r["ai"] += fAB["ae"] * T1r["ei"];
+    Z1r["ai"] -= FMIr["mi"] * T1r["am"];
+    Z1r["ai"] += VAIJBSAr["amei"] * T1r["em"];
+    Z1r["ai"] += FMEr["me"] * T2SAr["aeim"];
+    Z1r["ai"] += VABCI["efam"] * TauSAr["efim"];
+    Z1r["ai"] -= WMNEJr["mnei"] * T2SAr["eamn"];
+
+    Z2cr["abij"] = 0.5 * VABIJ["abij"];
+    Z2cr["abij"] += VABCI["abej"] * T1r["ei"];
+    Z2cr["abij"] -= WAMIJr["amij"] * T1r["bm"];
+    Z2cr["abij"] += FAEr["ae"] * T2r["ebij"];
+    Z2cr["abij"] -= FMIr["mi"] * T2r["abmj"];
+    Z2cr["abij"] += 0.5 * VABCD["abef"] * Taur["efij"];
+    Z2cr["abij"] += 0.5 * WMNIJr["mnij"] * Taur["abmn"];
+    Z2cr["abij"] += 0.5 * WAMIEr["amei"] * T2SAr["ebmj"];
+    Z2cr["abij"] -= 0.5 * WAMEIr["amei"] * T2r["ebjm"];
+    Z2cr["abij"] -= WAMEIr["amej"] * T2r["ebim"];
+    Z2r["abij"] = Z2cr["abij"];
+    Z2r["abij"] += Z2cr["baji"];
+}
+
 // ---- DIIS state ----------------------------------------------------------------------
 
 void Solver::build_diis() {
@@ -355,7 +515,8 @@ void Solver::build_diis() {
         }
     };
     add_segments(t1, 0, 1.0);
-    add_segments(t2, t1.total, 0.25);
+    // (the RHF DIIS takes the plain dot of the spatial amplitudes, rhfccsd.cxx:102)
+    add_segments(t2, t1.total, rhf ? 1.0 : 0.25);
     if (n <= 1) return;
     xs.resize(n);
     dxs.resize(n);
@@ -431,17 +592,25 @@ void Solver::diis_step() {
 void Solver::iterate_async() {
     // Refinement of the split precision.  Three BF16 slices leave a residual floor near
     // 1e-9; once conv < refine_tol the contractions move to four slices (floor ~2^-8
-    // lower), and to native FP64 only if the residual then stalls (no halving over two
-    // iterations) above conv_tol.  Graphs are recaptured after a switch.
+    // lower), and to native FP64 only if the residual then stalls above conv_tol.  Graphs
+    // are recaptured after a switch.
     if (opts.precision == CCSD_PREC_SPLIT && opts.refine_tol > 0 && conv < opts.refine_tol &&
         ctx.precision != CCSD_PREC_FP64) {
         bool escalate = false;
         if (ctx.split_slices() == 3) {
             ctx.slices = 4;
             escalate = true;
-        } else if (conv_hist.size() >= 3 && conv > 0.5 * conv_hist[conv_hist.size() - 3]) {
-            ctx.precision = CCSD_PREC_FP64;
-            escalate = true;
+        } else if (conv_hist.size() >= 5) {
+            // stalled: none of the last three residuals improves on the best one before
+            // them by 20% (DIIS makes single steps non-monotone; a slowly converging
+            // system still gains a factor ~2 over three iterations)
+            const size_t n = conv_hist.size();
+            const double before = *std::min_element(conv_hist.begin(), conv_hist.end() - 3);
+            const double recent = std::min({conv_hist[n - 3], conv_hist[n - 2], conv_hist[n - 1]});
+            if (recent > 0.8 * before) {
+                ctx.precision = CCSD_PREC_FP64;
+                escalate = true;
+            }
         }
         if (escalate) {
             refined = true;

@@ -17,10 +17,15 @@ struct DiisSegment {
 class Solver {
 public:
     Context& ctx;
-    ccsd_hamiltonian H;
+    ccsd_hamiltonian H{};              // spin-orbital blocks (ccsd.cxx)
+    ccsd_rhf_hamiltonian HR{};         // closed-shell spatial blocks (rhfccsd.cxx)
+    bool rhf = false;
     ccsd_options opts;
     int T1 = 0, T2 = 0, Z1 = 0, Z2 = 0, Tau = 0;
     int FME = 0, FMI = 0, FAE = 0, WMNIJ = 0, WMNEJ = 0, WAMIJ = 0, WAMEI = 0;
+    // RHF only: spin-adapted combinations, the extra ring intermediate, and the copies
+    // that the in-place symmetrisations WMNIJ += WMNIJ(nmji), Z2 += Z2(baji) read
+    int T2SA = 0, TauSA = 0, VABIJSA = 0, VAIJBSA = 0, WAMIE = 0, WMNIJc = 0, Z2c = 0;
     double* den[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [space][spin]
     Plan iter_plan, tau_plan, energy_plan;
     double* d_red = nullptr;    // [0] energy, [1] conv
@@ -48,6 +53,7 @@ public:
     std::vector<std::pair<void*, size_t>> owned;
 
     Solver(Context& c, const ccsd_hamiltonian& h, const ccsd_options& o);
+    Solver(Context& c, const ccsd_rhf_hamiltonian& h, const ccsd_options& o);
     ~Solver();
     void iterate(double* e, double* c);
     void iterate_async();
@@ -69,6 +75,10 @@ private:
     void launch_tau();
     void record_energy(Plan& p);
     void record_iteration();
+    void record_iteration_rhf();
+    void setup();
+    std::vector<int> constants() const;
+    std::vector<int> owned_tensors() const;
     void launch_iteration();
     void diis_step();
 };

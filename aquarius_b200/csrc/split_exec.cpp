@@ -8,26 +8,33 @@
 
 namespace ccsd {
 
-namespace {
-
-// Small contractions stay on the FP64 tensor-core kernel: a 128x128 tile would be mostly
-// padding and the slicing passes would cost more than the product.
-// CCSD_SPLIT_ROUTE_ALL sends every contraction through the split kernel (coverage tests).
-bool use_split(const GemmStep& g, int routing) {
-    if (routing == CCSD_SPLIT_ROUTE_ALL) return g.M > 0 && g.N > 0 && g.K > 0;
-    // Skinny contractions (N of a few tens) stay on the FP64 kernels; few-tile ones take
-    // the split kernel only when splitting K fills the machine (a 1024-k chunk per range).
+// Which block contractions take the split kernel.  Small contractions stay on the FP64
+// kernels: a 128x128 tile would be mostly padding and the slicing passes would cost more
+// than the product.  CCSD_SPLIT_ROUTE_ALL sends every contraction through the split
+// kernel (coverage tests).
+bool Context::split_eligible(const GemmStep& g) const {
+    if (split_routing == CCSD_SPLIT_ROUTE_ALL) return g.M > 0 && g.N > 0 && g.K > 0;
+    if (g.K < 256 || g.flops() < 5e8) return false;
+    // few-tile products take the split kernel only when splitting K fills the machine (a
+    // 1024-k chunk per range)
     const int64_t tiles = (int64_t)((g.M + 127) / 128) * ((g.N + 127) / 128);
     const int64_t ctas = tiles * kern::split_ksplit(g.M, g.N, g.K, 3);
-    return g.M >= 128 && g.N >= 64 && g.K >= 256 && ctas >= 148 && g.flops() >= 5e8;
+    if (ctas < 148) return false;
+    // Skinny products (an extent of a few tens) stay on the FP64 kernels even when the long
+    // operand is a constant H block: each statement gathers that block in its own row / k
+    // split, so its slices could not be shared, and slicing per call costs more than the
+    // FP64 product
+    return g.M >= 128 && g.N >= 64;
 }
+
+namespace {
 
 // bytes of the ns BF16 slices (and row scales) of a rows x K operand
 int64_t slice_bytes(int rows, int K, int ns) {
     return (int64_t)ns * kern::split_rows_pad(rows) * kern::split_k_pad(K) * 2 + 2 * (int64_t)kern::split_rows_pad(rows) * 8;
 }
 
-// device bytes the sliced constant operands may occupy (CCSD_SPLIT_CACHE_GB, default 56)
+// device bytes the sliced constant operands may occupy (CCSD_SPLIT_CACHE_GB, default 50)
 int64_t cache_budget() {
     const char* e = std::getenv("CCSD_SPLIT_CACHE_GB");
     double gb = e ? std::atof(e) : 50.0;
@@ -37,7 +44,7 @@ int64_t cache_budget() {
 }  // namespace
 
 bool Context::routes_split(const GemmStep& g) const {
-    return precision == CCSD_PREC_SPLIT && kern::split_supported() && use_split(g, split_routing);
+    return precision == CCSD_PREC_SPLIT && kern::split_supported() && split_eligible(g);
 }
 
 kern::SlicedOperand Context::alloc_sliced(int rows, int K, int ns) {
@@ -81,25 +88,33 @@ void Context::ensure_ws(kern::SlicedOperand& w, int rows, int K) {
 void Context::reserve_split(Plan& p) {
     std::vector<GemmStep*> order;
     for (auto& g : p.gemms)
-        if (use_split(g, split_routing)) order.push_back(&g);
+        if (split_eligible(g)) order.push_back(&g);
     std::stable_sort(order.begin(), order.end(), [](GemmStep* a, GemmStep* b) { return a->flops() > b->flops(); });
-    int64_t used = 0;
-    for (auto& kv : split_cache) used += kv.second.bytes;
+    int64_t base = 0;
+    for (auto& kv : split_cache) base += kv.second.bytes;
     const int64_t budget = cache_budget();
-    for (GemmStep* g : order) {
-        for (int side = 0; side < 2; side++) {
-            const int h = side == 0 ? g->tA : g->tB;
-            const int rows = side == 0 ? g->M : g->N;
-            bool& cache = side == 0 ? g->cache_a : g->cache_b;
-            cache = false;
-            if (h == kScratch || !is_constant(h)) continue;
-            const int64_t b = slice_bytes(rows, g->K, split_slices());
-            if (used + b <= budget) {
-                cache = true;
-                used += b;
+    auto choose = [&](int ns) {
+        int64_t used = base;
+        for (GemmStep* g : order) {
+            for (int side = 0; side < 2; side++) {
+                const int h = side == 0 ? g->tA : g->tB;
+                const int rows = side == 0 ? g->M : g->N;
+                bool& cache = side == 0 ? g->cache_a : g->cache_b;
+                cache = false;
+                if (h == kScratch || !is_constant(h)) continue;
+                const int64_t b = slice_bytes(rows, g->K, ns);
+                if (used + b <= budget) {
+                    cache = true;
+                    used += b;
+                }
             }
         }
-    }
+        return used;
+    };
+    // a solve that refines from 3 to 4 slices re-slices its cached operands within the
+    // same budget: a planning query accounts the larger of the two selections
+    int64_t used = plan_refine && host_only ? choose(4) : 0;
+    used = std::max(used, choose(split_slices()));
     int64_t need_a = 0, need_b = 0, rows_a = 0, rows_b = 0;
     for (GemmStep* g : order) {
         if (!g->cache_a) {
@@ -124,7 +139,7 @@ void Context::reserve_split(Plan& p) {
 }
 
 void Context::run_split_gemm(GemmStep& g, kern::GemmArgs& a) {
-    if (!use_split(g, split_routing)) {
+    if (!split_eligible(g)) {
         kern::gemm_fp64(a, stream);
         return;
     }

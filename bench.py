@@ -105,6 +105,18 @@ class Clocks:
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+def other_gpu_processes(device):
+    """Compute processes on the device other than this one (nvidia-smi), for the log: a
+    neighbour sharing the GPU time-slices every launch of the timed region."""
+    try:
+        out = subprocess.run(["nvidia-smi", "-i", str(device), "--query-compute-apps=pid,used_memory",
+                              "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=20).stdout
+    except Exception:
+        return None
+    rows = [r.split(",") for r in out.strip().splitlines() if r.strip()]
+    return [{"pid": int(r[0]), "mib": r[1].strip()} for r in rows if r[0].strip().isdigit() and int(r[0]) != os.getpid()]
+
+
 def fp64_gemm_peak(torch, device):
     """Measured cuBLAS DGEMM TFLOP/s (the FP64 roofline denominator; not in MEASURED_PEAKS)."""
     n = 8192
@@ -243,12 +255,15 @@ def timed_iterations(torch, ctx, s, stream, steps, warmup, profile):
         ctx.set_profiling(True)
     ctx.profile_report() if profile else None
     n0 = ctx.launch_count()
+    log(f"[bench] launches before the timed region: {n0}")
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("timed")   # launch-list captures filter on this range
     ev0.record(stream)
     for _ in range(steps):
         s.iterate_async()
     ev1.record(stream)
     ev1.synchronize()
+    torch.cuda.nvtx.range_pop()
     ms = ev0.elapsed_time(ev1)
     launches = ctx.launch_count() - n0
     prof = ctx.profile_report() if profile else {}
@@ -364,6 +379,7 @@ def main():
     H = ctx.hamiltonian_from_factor(B, eps, aux_per_irrep=aux if w["nirrep"] > 1 else None)
     ctx.synchronize()
     log(f"[bench] H built in {time.perf_counter() - t0:.1f}s, device bytes {ctx.device_bytes() / 1e9:.1f} GB")
+    log(f"[bench] other compute processes on the device: {other_gpu_processes(local)}")
 
     peaks, peak_kind = measured_peaks()
     results = {}

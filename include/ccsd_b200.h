@@ -66,7 +66,14 @@ enum {
 
 /* tensor creation flags */
 enum {
-    CCSD_TENSOR_PACKED = 1   /* store same-spin antisymmetric pairs once (i<j) */
+    CCSD_TENSOR_PACKED = 1,  /* store same-spin antisymmetric pairs once (i<j) */
+    /* a plain irrep-blocked tensor over spatial orbitals (the reference's
+     * SymmetryBlockedTensor with NS symmetry, src/tensor/symblocked_tensor.cxx): no
+     * spin cases, no antisymmetry; contractions among plain tensors are plain
+     * einsums.  Positions still follow [upper vrt, upper occ, lower vrt, lower occ],
+     * so an index string names the letters in that order; upper and lower counts must
+     * be equal. */
+    CCSD_TENSOR_PLAIN = 2
 };
 
 /* ---- context ------------------------------------------------------------ */
@@ -220,6 +227,30 @@ int ccsd_hamiltonian_from_fcidump(ccsd_ctx ctx, const char* path, int flags, int
  * MP1 guess and the MP2 energy (ccsd.cxx:37-62), and plans one iteration. */
 int ccsd_solver_create(ccsd_ctx ctx, const ccsd_hamiltonian* H, const ccsd_options* opts,
                        ccsd_solver* out);
+
+/* ---- closed-shell spin-adapted CCSD (RHFCCSD, src/cc/rhfccsd.cxx) --------------
+ * The same iteration driver over plain spatial tensors (CCSD_TENSOR_PLAIN): about
+ * half the flops of the spin-orbital form for a closed-shell reference.  The blocks
+ * are the non-antisymmetrised <pq|rs> of the reference's RHF integrals; positions
+ * follow the tensor layout [upper vrt, upper occ, lower vrt, lower occ], so VAIJB
+ * stores <ai|jb> at [a, i, b, j].  fAI, fAB and fIJ are the Fock blocks. */
+typedef struct {
+    ccsd_tensor fAI, fAB, fIJ, VABCD, VABCI, VABIJ, VAIBJ, VAIJB, VAIJK, VIJKL;
+} ccsd_rhf_hamiltonian;
+/* from a three-index factor (arguments as ccsd_hamiltonian_from_factor) */
+int ccsd_rhf_hamiltonian_from_factor(ccsd_ctx ctx, int naux, const double* B, const double* eps,
+                                     const int* aux_per_irrep, ccsd_rhf_hamiltonian* H);
+/* from a spatial Fock matrix and dense (pq|rs) (arguments as ccsd_hamiltonian_from_integrals) */
+int ccsd_rhf_hamiltonian_from_integrals(ccsd_ctx ctx, int n, const double* fock, const double* eri,
+                                        ccsd_rhf_hamiltonian* H);
+int ccsd_rhf_hamiltonian_destroy(ccsd_ctx ctx, ccsd_rhf_hamiltonian* H);
+/* Solver over the RHF blocks: RHFCCSD::run / iterate (rhfccsd.cxx:44-110, 193-327); the
+ * solver handle then works with every ccsd_solver_* call (amplitudes are plain tensors) */
+int ccsd_rhf_solver_create(ccsd_ctx ctx, const ccsd_rhf_hamiltonian* H, const ccsd_options* opts,
+                           ccsd_solver* out);
+/* host-only plan of one RHF iteration: flops and peak device bytes (as ccsd_plan_query) */
+int ccsd_rhf_plan_query(int nirrep, const int* vrt, const int* occ, const ccsd_options* opts,
+                        double* flops_per_iter, int64_t* device_bytes);
 int ccsd_solver_destroy(ccsd_solver s);
 int ccsd_solver_mp2(ccsd_solver s, double* mp2);
 /* one CCSD::iterate; energy and conv (max-abs of the weighted update) come back to the host */

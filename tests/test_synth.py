@@ -34,3 +34,18 @@ def test_different_seeds_differ(built_lib):
     _, B1, *_ = A.synth_problem(1, 3, 6)
     _, B2, *_ = A.synth_problem(2, 3, 6)
     assert not np.allclose(B1, B2)
+
+
+def test_rhf_plan_query_plans_every_statement():
+    """Host-only planning of the closed-shell iteration (no device): every RHFCCSD
+    statement plans, in C1 and with D2h blocks, at about half the spin-orbital flops."""
+    import aquarius_b200 as A
+    f_rhf, b_rhf = A.rhf_plan_query([256], [32], precision="split")
+    f_so, b_so = A.plan_query([256], [32], precision="split")
+    assert 0 < f_rhf < 0.5 * f_so
+    assert b_rhf > 8 * 256 ** 4   # the unpacked <Ab|Cd> block alone
+    f8, b8 = A.rhf_plan_query([6, 3, 4, 5, 2, 3, 4, 5], [2, 0, 1, 1, 1, 0, 1, 0])
+    assert f8 > 0 and b8 > 0
+    # a solve that may refine to 4 slices reserves the larger slice cache
+    _, b_ref = A.rhf_plan_query([256], [32], precision="split", refine_tol=1e-7)
+    assert b_ref >= b_rhf
