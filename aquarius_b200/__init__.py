@@ -22,7 +22,8 @@ from pathlib import Path
 import numpy as np
 
 _HERE = Path(__file__).resolve().parent
-LIB_PATH = _HERE / "libccsd_b200.so"
+# CCSD_B200_LIB points at another build of the library (e.g. a variant under test)
+LIB_PATH = Path(os.environ["CCSD_B200_LIB"]) if os.environ.get("CCSD_B200_LIB") else _HERE / "libccsd_b200.so"
 
 CCSD_OK = 0
 STATUS = {
@@ -105,7 +106,8 @@ class ServerResult(ctypes.Structure):
     _fields_ = [("id", ctypes.c_int64), ("status", ctypes.c_int), ("iterations", ctypes.c_int),
                 ("energy", ctypes.c_double), ("mp2", ctypes.c_double), ("conv", ctypes.c_double),
                 ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double),
-                ("device_bytes", ctypes.c_int64), ("flops_per_iter", ctypes.c_double)]
+                ("device_bytes", ctypes.c_int64), ("flops_per_iter", ctypes.c_double),
+                ("peak_bytes", ctypes.c_int64), ("message", ctypes.c_char * 160)]
 
 
 _lib = None
@@ -797,7 +799,10 @@ class Server:
         buf = (ServerResult * max_results)()
         n = ctypes.c_int()
         _check(lib().ccsd_server_poll(self.s, max_results, buf, ctypes.byref(n)))
-        return [{f: getattr(buf[k], f) for f, _ in ServerResult._fields_} for k in range(n.value)]
+        out = [{f: getattr(buf[k], f) for f, _ in ServerResult._fields_} for k in range(n.value)]
+        for r in out:
+            r["message"] = r["message"].decode(errors="replace")
+        return out
 
     def wait(self, timeout=3600.0):
         _check(lib().ccsd_server_wait(self.s, timeout))

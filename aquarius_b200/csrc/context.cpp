@@ -404,6 +404,8 @@ void Context::release(Plan& p) {
             fr(g.dCm[v], g.hCm[v].size());
             fr(g.dCn[v], g.hCn[v].size());
         }
+        // cached slices belong to the plan's contraction, not to the operand tensor alone
+        drop_split_cache(g);
     }
     for (auto& kv : p.schedules)
         for (auto& r : kv.second.runs)

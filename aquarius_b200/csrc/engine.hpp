@@ -260,6 +260,10 @@ public:
     void free_sliced(kern::SlicedOperand& s);
     void ensure_ws(kern::SlicedOperand& w, int rows, int K);
     void reserve_split(Plan& p);
+    // drop the plan's cached slices and choose again for the current slice count (after a
+    // 3 -> 4 slice switch), so that the cache is rebuilt within its budget largest-first
+    void refresh_split(Plan& p);
+    void drop_split_cache(GemmStep& g);
     std::map<std::string, std::unique_ptr<Plan>> plan_cache;
 
     // optional per-statement timing of GEMM steps with CUDA events on the stream

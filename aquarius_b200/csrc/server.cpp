@@ -14,6 +14,8 @@
 // Solves share nothing on the device but the memory pool; each one runs the same kernels
 // and reductions it would run alone, so its result does not depend on the mix.
 #include <algorithm>
+#include <cstdio>
+#include <cstring>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -143,8 +145,12 @@ private:
         r.flops = fl;
     }
 
-    void finish(const Request& r, int status, int iters, double e, double mp2, double conv, double t_admit) {
+    void finish(const Request& r, int status, int iters, double e, double mp2, double conv, double t_admit,
+                int64_t peak = 0, const std::string& msg = std::string()) {
         ccsd_server_result res;
+        std::memset(&res, 0, sizeof(res));
+        res.peak_bytes = peak;
+        std::snprintf(res.message, sizeof(res.message), "%s", msg.c_str());
         res.id = r.id;
         res.status = status;
         res.iterations = iters;
@@ -270,6 +276,7 @@ private:
         int status = CCSD_OK;
         double e = 0, c = 0, mp2 = 0;
         int it = 0;
+        std::string msg;
         try {
             build(*r, ctx, s);
             mp2 = s->mp2;
@@ -295,11 +302,14 @@ private:
             it = s->iterations;
         } catch (const Error& err) {
             status = err.code;
+            msg = err.what();
             it = s ? s->iterations : 0;
         } catch (const std::exception& err) {
             status = CCSD_ERR_ARG;
+            msg = err.what();
             it = s ? s->iterations : 0;
         }
+        const int64_t peak = ctx ? ctx->peak_bytes : 0;
         if (ev) cudaEventDestroy(ev);
         try {
             s.reset();
@@ -312,7 +322,7 @@ private:
             n_active--;
         }
         cv_admit.notify_all();
-        finish(*r, status, it, status == CCSD_OK || status == CCSD_NOT_CONVERGED ? e : 0.0, mp2, c, t_admit);
+        finish(*r, status, it, status == CCSD_OK || status == CCSD_NOT_CONVERGED ? e : 0.0, mp2, c, t_admit, peak, msg);
     }
 };
 

@@ -599,6 +599,7 @@ void Solver::iterate_async() {
         bool escalate = false;
         if (ctx.split_slices() == 3) {
             ctx.slices = 4;
+            ctx.refresh_split(iter_plan);
             escalate = true;
         } else if (conv_hist.size() >= 5) {
             // stalled: none of the last three residuals improves on the best one before

@@ -138,6 +138,24 @@ void Context::reserve_split(Plan& p) {
     }
 }
 
+void Context::drop_split_cache(GemmStep& g) {
+    for (int64_t* key : {&g.split_cache_a, &g.split_cache_b}) {
+        auto it = *key >= 0 ? split_cache.find(*key) : split_cache.end();
+        if (it != split_cache.end()) {
+            free_sliced(it->second);
+            split_owner.erase(it->first);
+            split_cache.erase(it);
+        }
+        *key = -1;
+    }
+}
+
+void Context::refresh_split(Plan& p) {
+    CCSD_CUDA(cudaStreamSynchronize(stream));
+    for (auto& g : p.gemms) drop_split_cache(g);
+    reserve_split(p);
+}
+
 void Context::run_split_gemm(GemmStep& g, kern::GemmArgs& a) {
     if (!split_eligible(g)) {
         kern::gemm_fp64(a, stream);

@@ -169,7 +169,9 @@ typedef struct {
     int    use_graph;     /* capture one iteration as a CUDA graph and replay it */
     double refine_tol;    /* split precision only: once conv < refine_tol, 3-slice
                              contractions move to 4 slices, and 4-slice ones to native
-                             FP64 if the residual then stalls (0 = never) */
+                             FP64 if the residual then stalls (0 = never).  About
+                             1000 x conv_tol: the 3-slice floor is near 1e-9, and a
+                             switch close to it leaves DIIS a history of 3-slice noise */
 } ccsd_options;
 
 void ccsd_options_default(ccsd_options* opts);
@@ -319,6 +321,8 @@ typedef struct {
     double t_submit, t_admit, t_done;   /* seconds since the server started */
     int64_t device_bytes;    /* planned bytes the solve was admitted with */
     double flops_per_iter;
+    int64_t peak_bytes;      /* device bytes the solve's context held at its peak */
+    char message[160];       /* the error message of a failed solve ("" otherwise) */
 } ccsd_server_result;
 void ccsd_server_options_default(ccsd_server_options* o);
 int ccsd_server_create(const ccsd_server_options* o, ccsd_server* out);
