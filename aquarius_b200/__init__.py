@@ -31,7 +31,7 @@ STATUS = {
     5: "CCSD_DIVERGED", 6: "CCSD_NOT_CONVERGED", 7: "CCSD_ERR_SINGULAR", 8: "CCSD_ERR_TIMEOUT",
     9: "CCSD_ERR_UNSUPPORTED",
 }
-PREC = {"fp64": 0, "split": 1}
+PREC = {"fp64": 0, "split": 1, "split_i8": 2}   # split: BF16 slices; split_i8: INT8 slices
 TENSOR_PACKED = 1
 TENSOR_PLAIN = 2
 
@@ -753,10 +753,11 @@ class Solver:
         return e.value, c.value, i.value
 
     def mode(self):
-        """contraction mode of the next iteration: "fp64", "split3" or "split4\""""
+        """contraction mode of the next iteration: "fp64", "split3", "split4" (BF16 slices) or
+        "i8split3" .. "i8split5" (INT8 slices)"""
         p, n = ctypes.c_int(), ctypes.c_int()
         _check(lib().ccsd_solver_mode(self.s, ctypes.byref(p), ctypes.byref(n)), self.ctx.c)
-        return "fp64" if p.value == 0 else f"split{n.value}"
+        return "fp64" if p.value == 0 else (f"split{n.value}" if p.value == 1 else f"i8split{n.value}")
 
     def flops(self):
         x = ctypes.c_double()

@@ -176,10 +176,13 @@ int ccsd_ctx_launch_count(ccsd_ctx ctx, int64_t* count) {
 int ccsd_ctx_set_precision(ccsd_ctx ctx, int precision, int slices) {
     return guarded(ctx, [&] {
         Context* c = from_handle(ctx);
-        if (precision != CCSD_PREC_FP64 && precision != CCSD_PREC_SPLIT) throw Error(CCSD_ERR_ARG, "bad precision");
-        if (precision == CCSD_PREC_SPLIT && !kern::split_supported())
-            throw Error(CCSD_ERR_UNSUPPORTED, "split-BF16 GEMMs need an sm_100 device");
-        if (slices != 0 && slices != 3 && slices != 4) throw Error(CCSD_ERR_ARG, "slices must be 0 (default), 3 or 4");
+        if (precision != CCSD_PREC_FP64 && precision != CCSD_PREC_SPLIT && precision != CCSD_PREC_SPLIT_I8)
+            throw Error(CCSD_ERR_ARG, "bad precision");
+        if (precision != CCSD_PREC_FP64 && !kern::split_supported())
+            throw Error(CCSD_ERR_UNSUPPORTED, "split GEMMs need an sm_100 device");
+        const int kind = precision == CCSD_PREC_SPLIT_I8 ? kern::SLICE_INT8 : kern::SLICE_BF16;
+        if (slices != 0 && !kern::slice_scheme_ok(kind, slices))
+            throw Error(CCSD_ERR_ARG, "slices must be 0 (default) or 3, 4 (BF16) / 3, 4, 5 (INT8)");
         c->precision = precision;
         c->slices = slices;
     });
@@ -674,8 +677,8 @@ int ccsd_rhf_solver_create(ccsd_ctx ctx, const ccsd_rhf_hamiltonian* H, const cc
         ccsd_options o;
         options_default(&o);
         if (opts) o = *opts;
-        if (o.precision == CCSD_PREC_SPLIT && !kern::split_supported())
-            throw Error(CCSD_ERR_UNSUPPORTED, "split-BF16 GEMMs need an sm_100 device");
+        if (o.precision != CCSD_PREC_FP64 && !kern::split_supported())
+            throw Error(CCSD_ERR_UNSUPPORTED, "split GEMMs need an sm_100 device");
         auto* h = new ccsd_solver_s;
         h->ctx = ctx;
         try {
@@ -774,8 +777,8 @@ int ccsd_solver_create(ccsd_ctx ctx, const ccsd_hamiltonian* H, const ccsd_optio
         ccsd_options o;
         options_default(&o);
         if (opts) o = *opts;
-        if (o.precision == CCSD_PREC_SPLIT && !kern::split_supported())
-            throw Error(CCSD_ERR_UNSUPPORTED, "split-BF16 GEMMs need an sm_100 device");
+        if (o.precision != CCSD_PREC_FP64 && !kern::split_supported())
+            throw Error(CCSD_ERR_UNSUPPORTED, "split GEMMs need an sm_100 device");
         auto* h = new ccsd_solver_s;
         h->ctx = ctx;
         try {

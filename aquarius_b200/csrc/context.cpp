@@ -348,10 +348,13 @@ void Context::upload(Plan& p) {
     for (auto& g : p.gemms) {
         int ks = kern::fp64_ksplit(g.M, g.N, g.K, !fp64_tiled_only);
         if (ks > 1) need = std::max<int64_t>(need, (int64_t)ks * g.M * g.N);
-        for (int ns : {3, 4}) {   // split-precision GEMMs share the space
-            const int kss = kern::split_ksplit(g.M, g.N, g.K, ns);
-            if (kss > 1) need = std::max<int64_t>(need, (int64_t)kss * g.M * g.N);
-        }
+        // split-precision GEMMs share the space (every scheme a refinement may reach)
+        for (int kind : {kern::SLICE_BF16, kern::SLICE_INT8})
+            for (int ns = 3; ns <= 5; ns++) {
+                if (!kern::slice_scheme_ok(kind, ns)) continue;
+                const int kss = kern::split_ksplit(g.M, g.N, g.K, ns, kind);
+                if (kss > 1) need = std::max<int64_t>(need, (int64_t)kss * g.M * g.N);
+            }
     }
     if (need > splitk_elems) {
         if (splitk_ws) dfree(splitk_ws, splitk_elems * sizeof(double));
@@ -381,7 +384,7 @@ void Context::upload(Plan& p) {
     }
     // tables are uploaded from pageable host memory; make sure the copies have been
     // staged before the host vectors could change
-    if (precision == CCSD_PREC_SPLIT && !p.split_reserved && (host_only || kern::split_supported())) {
+    if (split_precision() && !p.split_reserved && (host_only || kern::split_supported())) {
         reserve_split(p);
         p.split_reserved = true;
     }
@@ -428,7 +431,7 @@ double* Context::data_of(Plan& p, int h) {
 
 void Context::run_gemm(Plan& p, GemmStep& g) {
     kern::GemmArgs a = gemm_args(p, g);
-    if (precision == CCSD_PREC_SPLIT && kern::split_supported()) {
+    if (split_precision() && kern::split_supported()) {
         run_split_gemm(g, a);
     } else {
         kern::gemm_fp64(a, stream);
@@ -479,8 +482,8 @@ kern::GemmArgs Context::gemm_args(Plan& p, const GemmStep& g) {
 // sums (antisymmetriser images, copies) and of block scalings of one statement are
 // batched the same way, one launch per level.
 RunSchedule& Context::schedule(Plan& p) {
-    const int key = (precision == CCSD_PREC_SPLIT ? 1 : 0) | (split_routing << 1) | (fp64_tiled_only ? 4 : 0) |
-                    (group_gemms ? 8 : 0);
+    const int key = (split_precision() ? 1 : 0) | (split_routing << 1) | (fp64_tiled_only ? 4 : 0) |
+                    (group_gemms ? 8 : 0) | (precision == CCSD_PREC_SPLIT_I8 ? 16 : 0);
     auto it = p.schedules.find(key);
     if (it != p.schedules.end()) return it->second;
     RunSchedule& rs = p.schedules[key];

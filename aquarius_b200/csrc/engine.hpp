@@ -255,8 +255,11 @@ public:
     kern::SlicedOperand ws_view[2];                        // workspace views of the current call
     double* splitk_ws = nullptr;                           // FP64 split-K partials
     int64_t splitk_elems = 0;
-    kern::SlicedOperand alloc_sliced(int rows, int K, int nslices);
-    int split_slices() const { return slices == 4 ? 4 : 3; }   // BF16 slices per operand
+    kern::SlicedOperand alloc_sliced(int rows, int K, int nslices, int kind);
+    // slices per operand of the split path (3 unless set) and their kind
+    int split_slices() const { return slices >= 3 ? slices : 3; }
+    int slice_kind() const { return precision == CCSD_PREC_SPLIT_I8 ? kern::SLICE_INT8 : kern::SLICE_BF16; }
+    bool split_precision() const { return precision == CCSD_PREC_SPLIT || precision == CCSD_PREC_SPLIT_I8; }
     void free_sliced(kern::SlicedOperand& s);
     void ensure_ws(kern::SlicedOperand& w, int rows, int K);
     void reserve_split(Plan& p);

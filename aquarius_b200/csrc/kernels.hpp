@@ -45,15 +45,25 @@ int fp64_tiles(int M, int N);
 void gemm_fp64_grouped(const GemmArgs* probs, const int* tile_start, int nprob, int total_tiles, bool a_kcontig,
                        bool b_kcontig, cudaStream_t s);
 
-// ---- split-BF16 (Ozaki-style) path ------------------------------------------------
-// An operand sliced for the tcgen05 GEMM: rows x kpad bf16 values per slice, K-major,
-// row scale 2^e per row.  rows is padded to a multiple of 128, kpad to a multiple of 64.
+// ---- split (Ozaki-style) path ----------------------------------------------------
+// Slice kinds: BF16 slices of 8 significant bits (3 or 4 per operand, FP32 tensor
+// accumulation) or INT8 slices of 7 bits (3, 4 or 5 per operand, exact INT32 tensor
+// accumulation at twice the BF16 rate).
+enum SliceKind { SLICE_BF16 = 0, SLICE_INT8 = 1 };
+inline int slice_elem_bytes(int kind) { return kind == SLICE_INT8 ? 1 : 2; }
+inline bool slice_scheme_ok(int kind, int ns) {
+    return kind == SLICE_INT8 ? (ns >= 3 && ns <= 5) : (ns == 3 || ns == 4);
+}
+
+// An operand sliced for the tcgen05 GEMM: rows x kpad values per slice, K-major, row
+// scale 2^e per row.  rows is padded to a multiple of 128, kpad to one 128-byte k-block
+// (64 BF16 or 128 INT8 values).
 struct SlicedOperand {
-    uint16_t* data = nullptr;   // [nslices][rows][kpad]
-    double* scale = nullptr;    // [rows]  value = scale * (s1 + s2 + s3)
+    uint8_t* data = nullptr;    // [nslices][rows][kpad] elements of the kind
+    double* scale = nullptr;    // [rows]  value = scale * sum_t w_t s_t
     double* rowmax = nullptr;   // [rows]  scratch of the slicing pass
-    int rows = 0, kpad = 0, nslices = 0;
-    int64_t bytes = 0;
+    int rows = 0, kpad = 0, nslices = 0, kind = SLICE_BF16;
+    int64_t bytes = 0;          // allocated slice bytes (capacity of a workspace)
 };
 
 struct SplitWorkspace {
@@ -63,19 +73,23 @@ struct SplitWorkspace {
 // number of bf16 slices of the split path
 constexpr int kDefaultSlices = 3;
 int split_rows_pad(int rows);
-int split_k_pad(int k);
+int split_k_pad(int k, int kind);
+// slice bytes of a rows x K operand in a scheme (without the row scales)
+inline int64_t split_slice_bytes(int rows, int K, int ns, int kind) {
+    return (int64_t)ns * split_rows_pad(rows) * split_k_pad(K, kind) * slice_elem_bytes(kind);
+}
 
 // slice rows of X(r,k) = X[R[r] + Kt[k]] (r < nrows, k < K) into `out` (allocated by caller
-// with out.rows >= nrows padded, out.kpad >= K padded)
+// with out.rows >= nrows padded, out.kpad >= K padded; out.kind and out.nslices say how)
 void slice_rows(const double* X, const int64_t* R, const int64_t* Kt, int nrows, int K, bool kcontig,
-                int nslices, SlicedOperand& out, cudaStream_t s);
+                SlicedOperand& out, cudaStream_t s);
 // tcgen05 GEMM over slices; epilogue scatters into C like gemm_fp64.  ks > 1 splits K
 // into ks ranges whose partials go to g.ws (ks * M * N doubles) and are folded into C.
 void gemm_split(const SlicedOperand& a, const SlicedOperand& b, int M, int N, int K,
                 const GemmArgs& g, cudaStream_t s, int ks = 1);
 // K-ranges for a split GEMM: enough CTAs for about two waves when the output has few
-// tiles, each range at least one exact 1024-k chunk (1 = none)
-int split_ksplit(int M, int N, int K, int nslices = 3);
+// tiles (1 = none)
+int split_ksplit(int M, int N, int K, int nslices = 3, int kind = SLICE_BF16);
 // alpha * sum_z ws[z][m][n] scattered into every destination variant of g (fixed order)
 void splitk_fold(const GemmArgs& g, int ks, cudaStream_t s);
 bool split_supported();

@@ -1,28 +1,35 @@
-// Split-BF16 (Ozaki-style) contraction path on the sm_100a tensor cores.
+// Split (Ozaki-style) contraction path on the sm_100a tensor cores.
 //
 // Each FP64 operand row x (a row of A(m,:) or a column of B(:,n), gathered through
-// the planner's offset tables) is written as
-//     x = 2^(e-6) * (s1 + s2 + s3),   2^e <= max|x| < 2^(e+1),
-// with s1 an integer in [-128,128], s2 = integer/2^8, s3 = integer/2^16, all exact in
-// BF16 (round-to-nearest at each step, so the truncation error is unbiased and below
-// 2^-23 of the row maximum).  The tcgen05 GEMM keeps two FP32 accumulators in TMEM:
-//     L2  = sum_k s1a*s1b                          (products <= 2^14: a chunk of 1024 k
-//                                                     sums exactly in FP32)
-//     L34 = sum_k (s1a*s2b + s2a*s1b + s1a*s3b + s2a*s2b + s3a*s1b)   (2^-8 smaller)
-// and every 1024-k chunk is drained into FP64 registers, so the leading term is exact
-// and the FP32 rounding of the rest sits ~2^-32 below the result.  The dropped
-// products (s2*s3, s3*s2, s3*s3) are below 2^-23 of the row maxima.
+// the planner's offset tables) is scaled by a power of two from its max-abs and cut
+// into slices, round-to-nearest at each step (so the truncation error is unbiased):
 //
-// Kernel structure (one 128x128 output tile per CTA, 320 threads):
-//   warp 0      TMA producer: 3 A-slice + 3 B-slice tiles of 128x64 BF16 per stage
-//               (128-byte swizzle), 2 stages of 96 KiB, mbarrier full/empty ring;
-//   warp 1      TMEM allocation (512 columns) and the single-thread MMA issuer:
-//               tcgen05.mma kind::f16 M128 N128 K16, 6 MMAs per k-step, commit to
-//               release smem stages and to publish a finished chunk;
-//   warps 2..9  epilogue: TMEM accumulator sets are double-buffered across chunks;
-//               each warp drains its 32 lanes x 64 columns into FP64 registers and
-//               scatters the scaled result into the destination through the planner's
-//               offset tables at the end.
+// BF16 slices (3 or 4):   x = 2^(e-6) * (s1 + s2 + s3 [+ s4]),  2^e <= max|x| < 2^(e+1),
+//   s1 an integer in [-128,128], s2 = integer/2^8, s3 = integer/2^16, all exact in BF16.
+//   The tcgen05 GEMM (kind::f16) keeps FP32 accumulators in TMEM:
+//     L2  = sum_k s1a*s1b                         (products <= 2^14: a chunk of 1024 k
+//                                                    sums exactly in FP32)
+//     L34 = the other products with i+j < NS      (2^-8 smaller)
+//   and every chunk is drained into FP64 registers, so the leading term is exact and the
+//   FP32 rounding of the rest sits ~2^-32 below the result (3 slices; 4 slices also keep
+//   s1*s2 + s2*s1 apart, exact over 512 k).
+//
+// INT8 slices (3, 4 or 5):  x = 2^(e-5) * (q1 + 2^-7 q2 + 2^-14 q3 ...),  q_t in [-64,64].
+//   The tcgen05 GEMM (kind::i8, twice the BF16 rate) accumulates every level
+//   t = i+j of the kept products q_i*q_j (i+j < NS) in its own INT32 accumulator, which
+//   is exact (|q_i q_j| <= 2^12, at most 5 products per level: a drained chunk of 65536 k
+//   stays below 2^31); the epilogue weights level t by 2^-7t in FP64.  Per product the
+//   error is ~2^-(7 NS - 1) of row max x column max (2^-20, 2^-27, 2^-34).
+//
+// Kernel structure (one 128 x TBN output tile per CTA, 320 threads):
+//   warp 0      TMA producer: NS A-slice + NS B-slice tiles of 128-byte k-blocks per
+//               stage (128-byte swizzle), 2 stages, mbarrier full/empty ring;
+//   warp 1      TMEM allocation and the single-thread MMA issuer: one MMA per kept slice
+//               product per k-step, commit to release smem stages and to publish a
+//               finished chunk;
+//   warps 2..9  epilogue: TMEM accumulator sets (double-buffered where two fit) are
+//               drained per chunk into FP64 registers; the scaled result is scattered
+//               into the destination through the planner's offset tables at the end.
 // Every mbarrier wait is bounded (about 2 s); on expiry the kernel records an error
 // code, stops issuing work and returns after releasing its TMEM.
 #include <atomic>
@@ -48,33 +55,40 @@ void set_smem_once(const void* kernel, int bytes);
 
 namespace split {
 
-constexpr int BM = 128, BN = 128, BK = 64;           // BN: tile width of the 3-slice kernel
+constexpr int BM = 128;
+constexpr int KB_BYTES = 128;                       // one k-block: a 128-byte row segment
 constexpr int STAGES = 2;
-constexpr int CHUNK_KB = 16;                       // 16 x 64 = 1024 k: the 3-slice exact FP32 chunk
 constexpr int EPI_WARPS = 8;
 constexpr int THREADS = 32 * (2 + EPI_WARPS);
-constexpr int TILE_A_BYTES = BM * BK * 2;           // 16 KiB
+constexpr int TILE_A_BYTES = BM * KB_BYTES;         // 16 KiB
 constexpr long long WAIT_CYCLES = 4000000000ll;     // ~2 s at 1.9 GHz
 
-// Kernel shape per slice count: 3 slices on 128x128 tiles, 4 slices on 128x64 tiles, so
-// that a stage (NS A tiles + NS B tiles) is 96 KiB either way.
-template <int NS>
+// Kernel shape per scheme.  A stage holds NS A tiles and NS B tiles of one k-block;
+// the tile width keeps a stage near 96 KiB (two stages fit in shared memory).
+template <int NS, bool I8>
 struct Shape {
-    static constexpr int TBN = NS == 3 ? 128 : 64;
-    static constexpr int TILE_B = TBN * BK * 2;
+    static constexpr int BKE = I8 ? 128 : 64;                       // k elements per k-block
+    static constexpr int TBN = NS == 3 ? 128 : NS == 4 ? 64 : 32;
+    static constexpr int TILE_B = TBN * KB_BYTES;
     static constexpr int STAGE = NS * (TILE_A_BYTES + TILE_B);
-    // TMEM accumulators per buffer: 3 slices keep s1*s1 (exact over 1024 k) and the rest;
-    // 4 slices also keep s1*s2 + s2*s1 apart (exact over 512 k), so that the FP32 rounding
-    // of the remaining terms sits below the 4-slice truncation
-    static constexpr int NACC = NS == 4 ? 3 : 2;
-    static constexpr int CHUNK = NS == 4 ? 8 : CHUNK_KB;   // K blocks per drained chunk
-    static constexpr int BUF = NACC * TBN;                 // TMEM columns per buffer
-    static constexpr int TMEM_COLS = 2 * BUF <= 256 ? 256 : 512;
-    static constexpr int COLS = TBN / 2;             // columns per epilogue warp
+    // accumulators per buffer.  BF16: s1*s1 (exact over 1024 k) and the rest; 4 slices
+    // also keep s1*s2 + s2*s1 apart (exact over 512 k).  INT8: one exact INT32
+    // accumulator per level i+j.
+    static constexpr int NACC = I8 ? NS : (NS == 4 ? 3 : 2);
+    static constexpr int CHUNK = I8 ? 512 : (NS == 4 ? 8 : 16);     // k-blocks per drained chunk
+    // split-K ranges: whole exact chunks (BF16), any 8 k-blocks (INT8: exact per range)
+    static constexpr int KSPLIT_GRAIN = I8 ? 8 : CHUNK;
+    static constexpr int BUF = NACC * TBN;                          // TMEM columns per buffer
+    static constexpr int NBUF = 2 * BUF <= 512 ? 2 : 1;             // double-buffered if two fit
+    static constexpr int TMEM_COLS = NBUF * BUF <= 256 ? 256 : 512;
+    static constexpr int COLS = TBN / 2;                            // columns per epilogue warp
     static constexpr size_t SMEM = 1024 + (size_t)STAGES * STAGE + 256;
-    // instruction descriptor: D=F32, A=B=BF16, K-major both, N=TBN, M=128
-    static constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TBN >> 3) << 17) |
-                                      ((uint32_t)(BM >> 4) << 24);
+    // instruction descriptor: D = F32 / S32, A = B = BF16 / signed 8-bit, K-major both,
+    // N = TBN, M = 128
+    static constexpr uint32_t IDESC = (I8 ? (2u << 4) : (1u << 4)) | (1u << 7) | (1u << 10) |
+                                      ((uint32_t)(TBN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+    static_assert(STAGE * STAGES + 1024 + 256 <= 227 * 1024, "stages exceed shared memory");
+    static_assert(TBN % 16 == 0 && TBN >= 16 && TBN <= 256, "MMA N");
 };
 
 struct Params {
@@ -161,12 +175,21 @@ __device__ __forceinline__ uint64_t sdesc(const void* p) {
     return d;
 }
 
+template <bool I8>
 __device__ __forceinline__ void umma(uint32_t dtmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(dtmem),
-        "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+    if constexpr (I8) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(dtmem),
+            "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "setp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(dtmem),
+            "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0), "r"(0), "r"(0), "r"(0));
+    }
 }
 
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
@@ -186,10 +209,11 @@ __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 
-template <int NS>
+template <int NS, bool I8>
 __global__ void __launch_bounds__(THREADS, 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params p) {
-    using Sh = Shape<NS>;
+    using Sh = Shape<NS, I8>;
+    constexpr int NBUF = Sh::NBUF;
     constexpr int TBN = Sh::TBN, COLS = Sh::COLS;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -208,7 +232,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int m0 = tm * BM, n0 = tn * TBN;
     // this CTA's K blocks [kb0, kb0 + nkb)
     const int kb0 = blockIdx.y * p.kb_per;
-    const int nkb = max(0, min(p.Kp / BK, kb0 + p.kb_per) - kb0);
+    const int nkb = max(0, min(p.Kp / Sh::BKE, kb0 + p.kb_per) - kb0);
     const int nchunks = (nkb + Sh::CHUNK - 1) / Sh::CHUNK;
 
     if (threadIdx.x == 0) {
@@ -241,11 +265,12 @@ __global__ void __launch_bounds__(THREADS, 1)
                 if (kb >= STAGES && !mbar_wait(&empty[s], ((kb / STAGES) - 1) & 1, abort_flag, p.err, 1)) break;
                 mbar_expect_tx(&full[s], Sh::STAGE);
                 uint8_t* base = stages + (size_t)s * Sh::STAGE;
+                // x = k-block start in elements: a multiple of 128 bytes
                 for (int i = 0; i < NS; i++)
-                    tma_load_2d(base + i * TILE_A_BYTES, &tmA, (kb0 + kb) * BK, i * p.Mp + m0, &full[s]);
+                    tma_load_2d(base + i * TILE_A_BYTES, &tmA, (kb0 + kb) * Sh::BKE, i * p.Mp + m0, &full[s]);
                 for (int i = 0; i < NS; i++)
-                    tma_load_2d(base + NS * TILE_A_BYTES + i * Sh::TILE_B, &tmB, (kb0 + kb) * BK, i * p.Np + n0,
-                                &full[s]);
+                    tma_load_2d(base + NS * TILE_A_BYTES + i * Sh::TILE_B, &tmB, (kb0 + kb) * Sh::BKE,
+                                i * p.Np + n0, &full[s]);
             }
         }
     } else if (warp == 1) {
@@ -253,8 +278,8 @@ __global__ void __launch_bounds__(THREADS, 1)
             // ---------------- MMA issuer ----------------
             int kb = 0;
             for (int c = 0; c < nchunks && !*abort_flag; c++) {
-                const int b = c & 1;
-                if (c >= 2 && !mbar_wait(&tempty[b], ((c >> 1) - 1) & 1, abort_flag, p.err, 2)) break;
+                const int b = c % NBUF;
+                if (c >= NBUF && !mbar_wait(&tempty[b], ((c / NBUF) - 1) & 1, abort_flag, p.err, 2)) break;
                 tc_fence_after();
                 const uint32_t dbase = tmem + b * Sh::BUF;
                 const int kb_end = min(nkb, (c + 1) * Sh::CHUNK);
@@ -275,10 +300,11 @@ __global__ void __launch_bounds__(THREADS, 1)
                         bd[i] = sdesc(base + NS * TILE_A_BYTES + i * Sh::TILE_B);
                     }
 #pragma unroll
-                    for (int kk = 0; kk < BK / 16; kk++) {
-                        const uint64_t o = (uint64_t)(kk * 32) >> 4;   // 16 bf16 = 32 bytes along K
-                        // slice products (i, t - i) with t < NS: t = 0 into accumulator 0,
-                        // the rest into accumulator min(t, NACC - 1)
+                    for (int kk = 0; kk < 4; kk++) {
+                        // one MMA covers 32 bytes of K (16 BF16 or 32 INT8 values)
+                        const uint64_t o = (uint64_t)(kk * 32) >> 4;
+                        // slice products (i, t - i) with t < NS into accumulator t (INT8) or
+                        // min(t, NACC - 1) (BF16)
                         bool fresh[Sh::NACC];
 #pragma unroll
                         for (int j = 0; j < Sh::NACC; j++) fresh[j] = first;
@@ -287,7 +313,7 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
                             for (int i = 0; i <= t; i++) {
                                 const int j = t < Sh::NACC - 1 ? t : Sh::NACC - 1;
-                                umma(dbase + j * TBN, ad[i] + o, bd[t - i] + o, Sh::IDESC, fresh[j] ? 0u : 1u);
+                                umma<I8>(dbase + j * TBN, ad[i] + o, bd[t - i] + o, Sh::IDESC, fresh[j] ? 0u : 1u);
                                 fresh[j] = false;
                             }
                         first = false;
@@ -308,8 +334,8 @@ __global__ void __launch_bounds__(THREADS, 1)
         for (int j = 0; j < COLS; j++) acc[j] = 0.0;
         bool ok = true;
         for (int c = 0; c < nchunks; c++) {
-            const int b = c & 1;
-            if (!mbar_wait(&tfull[b], (c >> 1) & 1, abort_flag, p.err, 4)) {
+            const int b = c % NBUF;
+            if (!mbar_wait(&tfull[b], (c / NBUF) & 1, abort_flag, p.err, 4)) {
                 ok = false;
                 break;
             }
@@ -317,16 +343,30 @@ __global__ void __launch_bounds__(THREADS, 1)
             const uint32_t base = tmem + ((uint32_t)(q * 32) << 16) + b * Sh::BUF + h * COLS;
 #pragma unroll
             for (int j4 = 0; j4 < COLS / 16; j4++) {
-                uint32_t r[Sh::NACC][16];
+                if constexpr (I8) {
+                    // one level at a time (fewer live registers): level j weighs 2^-7j, each
+                    // term exact in FP64
 #pragma unroll
-                for (int j = 0; j < Sh::NACC; j++) tmem_ld16(base + j * TBN + j4 * 16, r[j]);
-                tmem_wait_ld();
+                    for (int j = 0; j < Sh::NACC; j++) {
+                        uint32_t r[16];
+                        tmem_ld16(base + j * TBN + j4 * 16, r);
+                        tmem_wait_ld();
+                        const double w = 1.0 / (double)(1ll << (7 * j));
 #pragma unroll
-                for (int t = 0; t < 16; t++) {
-                    double v = 0.0;
+                        for (int t = 0; t < 16; t++) acc[j4 * 16 + t] += (double)(int)r[t] * w;
+                    }
+                } else {
+                    uint32_t r[Sh::NACC][16];
 #pragma unroll
-                    for (int j = 0; j < Sh::NACC; j++) v += (double)__uint_as_float(r[j][t]);
-                    acc[j4 * 16 + t] += v;
+                    for (int j = 0; j < Sh::NACC; j++) tmem_ld16(base + j * TBN + j4 * 16, r[j]);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int t = 0; t < 16; t++) {
+                        double v = 0.0;
+#pragma unroll
+                        for (int j = 0; j < Sh::NACC; j++) v += (double)__uint_as_float(r[j][t]);
+                        acc[j4 * 16 + t] += v;
+                    }
                 }
             }
             tc_fence_before();
@@ -452,41 +492,55 @@ __device__ __forceinline__ unsigned short bf16_bits(double v) {
     return *reinterpret_cast<unsigned short*>(&b);
 }
 
-template <bool KC, int NS>
+template <bool KC, int NS, bool I8>
 __global__ void __launch_bounds__(STHREADS)
     slice_kernel(const double* __restrict__ X, const int64_t* __restrict__ R, const int64_t* __restrict__ Kt, int nrows,
                  int K, const unsigned long long* __restrict__ rowmax, int rows_p, int kpad,
-                 unsigned short* __restrict__ out, double* __restrict__ scale) {
+                 uint8_t* __restrict__ out_bytes, double* __restrict__ scale) {
     __shared__ double tile[SR][SK + 1];
     __shared__ int64_t sR[SR], sK[SK];
     const int r0 = blockIdx.x * SR, k0 = blockIdx.y * SK;   // rows on x: up to 2^31 tiles
     load_tile<KC>(X, R, Kt, nrows, K, r0, k0, tile, sR, sK);
     const size_t plane = (size_t)rows_p * kpad;
+    // BF16: x = 2^(ex-6) (s1 + s2 + ...), s1 in [-128,128], slice t carries weight 2^-8t
+    // INT8: x = 2^(ex-5) (q1 + 2^-7 q2 + ...), q_t in [-64,64]
+    constexpr int SHIFT = I8 ? 5 : 6;
 #pragma unroll
     for (int i = 0; i < (SR * SK) / STHREADS; i++) {
         const int e = threadIdx.x + i * STHREADS;
         const int k = e % SK, r = e / SK;
         const int row = r0 + r;
         double mx = row < nrows ? __longlong_as_double((long long)rowmax[row]) : 0.0;
-        unsigned short bits[NS];
+        uint16_t bits[NS];
 #pragma unroll
         for (int t = 0; t < NS; t++) bits[t] = 0;
         if (mx > 0.0) {
-            const int ex = ilogb(mx);                // mx in [2^ex, 2^(ex+1))
-            double y = ldexp(tile[r][k], 6 - ex);    // |y| < 128
-            double w = 1.0;                          // weight of slice t: 2^(-8t)
+            const int ex = ilogb(mx);                    // mx in [2^ex, 2^(ex+1))
+            double y = ldexp(tile[r][k], SHIFT - ex);    // |y| < 2^SHIFT+1
+            double w = 1.0;                              // BF16 weight of slice t: 2^(-8t)
 #pragma unroll
             for (int t = 0; t < NS; t++) {
-                const double st = rint(y);           // an integer of at most 8 significant bits
-                bits[t] = bf16_bits(st * w);
-                y = (y - st) * 256.0;
-                w *= 0.00390625;
+                const double st = rint(y);               // an integer of at most 8 (7) significant bits
+                if constexpr (I8) {
+                    bits[t] = (uint16_t)(uint8_t)(int8_t)(int)st;
+                    y = (y - st) * 128.0;
+                } else {
+                    bits[t] = bf16_bits(st * w);
+                    y = (y - st) * 256.0;
+                    w *= 0.00390625;
+                }
             }
         }
         const size_t o = (size_t)row * kpad + (k0 + k);
+        if constexpr (I8) {
 #pragma unroll
-        for (int t = 0; t < NS; t++) out[t * plane + o] = bits[t];
-        if (blockIdx.y == 0 && k == 0) scale[row] = mx > 0.0 ? ldexp(1.0, ilogb(mx) - 6) : 0.0;
+            for (int t = 0; t < NS; t++) out_bytes[t * plane + o] = (uint8_t)bits[t];
+        } else {
+            uint16_t* out = reinterpret_cast<uint16_t*>(out_bytes);
+#pragma unroll
+            for (int t = 0; t < NS; t++) out[t * plane + o] = bits[t];
+        }
+        if (blockIdx.y == 0 && k == 0) scale[row] = mx > 0.0 ? ldexp(1.0, ilogb(mx) - SHIFT) : 0.0;
     }
 }
 
@@ -510,14 +564,16 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 
-void make_map(CUtensorMap* map, const uint16_t* base, int rows_total, int kpad, int box_rows) {
+void make_map(CUtensorMap* map, const uint8_t* base, int kind, int rows_total, int kpad, int box_rows) {
     EncodeTiledFn enc = encode_fn();
     if (!enc) throw std::runtime_error("cuTensorMapEncodeTiled is not available");
+    const int eb = slice_elem_bytes(kind);
     cuuint64_t dims[2] = {(cuuint64_t)kpad, (cuuint64_t)rows_total};
-    cuuint64_t strides[1] = {(cuuint64_t)kpad * 2};
-    cuuint32_t box[2] = {BK, (cuuint32_t)box_rows};
+    cuuint64_t strides[1] = {(cuuint64_t)kpad * eb};
+    cuuint32_t box[2] = {(cuuint32_t)(KB_BYTES / eb), (cuuint32_t)box_rows};   // 128 bytes of k
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)base, dims, strides, box, estr,
+    CUresult r = enc(map, kind == SLICE_INT8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                     (void*)base, dims, strides, box, estr,
                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
@@ -551,39 +607,83 @@ bool split_supported() {
 }
 
 int split_rows_pad(int rows) { return (rows + split::BM - 1) / split::BM * split::BM; }
-int split_k_pad(int k) { return (k + split::BK - 1) / split::BK * split::BK; }
+int split_k_pad(int k, int kind) {
+    const int bke = split::KB_BYTES / slice_elem_bytes(kind);
+    return (k + bke - 1) / bke * bke;
+}
 
-void slice_rows(const double* X, const int64_t* R, const int64_t* Kt, int nrows, int K, bool kcontig, int nslices,
+namespace {
+template <int NS, bool I8>
+void launch_slice(dim3 grid, bool kcontig, const double* X, const int64_t* R, const int64_t* Kt, int nrows, int K,
+                  const unsigned long long* rowmax, SlicedOperand& out, cudaStream_t s) {
+    using namespace split;
+    if (kcontig)
+        slice_kernel<true, NS, I8><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax, out.rows, out.kpad, out.data,
+                                                             out.scale);
+    else
+        slice_kernel<false, NS, I8><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax, out.rows, out.kpad, out.data,
+                                                              out.scale);
+}
+}  // namespace
+
+void slice_rows(const double* X, const int64_t* R, const int64_t* Kt, int nrows, int K, bool kcontig,
                 SlicedOperand& out, cudaStream_t s) {
     using namespace split;
-    if (nslices != 3 && nslices != 4) throw std::runtime_error("3 or 4 slices are built");
-    if (out.nslices != nslices) throw std::runtime_error("sliced operand allocated for another slice count");
+    const int ns = out.nslices;
+    if (!slice_scheme_ok(out.kind, ns)) throw std::runtime_error("unsupported slice scheme");
+    if ((int64_t)ns * out.rows * out.kpad * slice_elem_bytes(out.kind) > out.bytes)
+        throw std::runtime_error("sliced operand smaller than its scheme needs");
     unsigned long long* rowmax = reinterpret_cast<unsigned long long*>(out.rowmax);
     cudaMemsetAsync(rowmax, 0, sizeof(double) * out.rows, s);
     if (out.kpad / SK > 65535) throw std::runtime_error("split operand K too long for the slicing grid");
     dim3 grid(out.rows / SR, out.kpad / SK);
     if (kcontig) rowmax_kernel<true><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax);
     else rowmax_kernel<false><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax);
-    auto* d = out.data;
-    if (nslices == 3) {
-        if (kcontig) slice_kernel<true, 3><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax, out.rows, out.kpad, d, out.scale);
-        else slice_kernel<false, 3><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax, out.rows, out.kpad, d, out.scale);
+    if (out.kind == SLICE_INT8) {
+        if (ns == 3) launch_slice<3, true>(grid, kcontig, X, R, Kt, nrows, K, rowmax, out, s);
+        else if (ns == 4) launch_slice<4, true>(grid, kcontig, X, R, Kt, nrows, K, rowmax, out, s);
+        else launch_slice<5, true>(grid, kcontig, X, R, Kt, nrows, K, rowmax, out, s);
     } else {
-        if (kcontig) slice_kernel<true, 4><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax, out.rows, out.kpad, d, out.scale);
-        else slice_kernel<false, 4><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax, out.rows, out.kpad, d, out.scale);
+        if (ns == 3) launch_slice<3, false>(grid, kcontig, X, R, Kt, nrows, K, rowmax, out, s);
+        else launch_slice<4, false>(grid, kcontig, X, R, Kt, nrows, K, rowmax, out, s);
     }
     g_launches += 2;
 }
 
-int split_ksplit(int M, int N, int K, int nslices) {
+namespace {
+struct SchemeInfo {
+    int tbn, bke, chunk, grain;
+    size_t smem;
+    const void* kfn;
+};
+
+template <int NS, bool I8>
+SchemeInfo scheme_info() {
+    using Sh = split::Shape<NS, I8>;
+    return {Sh::TBN, Sh::BKE, Sh::CHUNK, Sh::KSPLIT_GRAIN, Sh::SMEM, (const void*)split::split_gemm_kernel<NS, I8>};
+}
+
+SchemeInfo scheme(int kind, int ns) {
+    if (kind == SLICE_INT8) {
+        if (ns == 3) return scheme_info<3, true>();
+        if (ns == 4) return scheme_info<4, true>();
+        if (ns == 5) return scheme_info<5, true>();
+    } else {
+        if (ns == 3) return scheme_info<3, false>();
+        if (ns == 4) return scheme_info<4, false>();
+    }
+    throw std::runtime_error("unsupported slice scheme");
+}
+}  // namespace
+
+int split_ksplit(int M, int N, int K, int nslices, int kind) {
     using namespace split;
-    const int tbn = nslices == 4 ? Shape<4>::TBN : Shape<3>::TBN;
-    const int64_t tiles = (int64_t)((M + BM - 1) / BM) * ((N + tbn - 1) / tbn);
+    const SchemeInfo si = scheme(kind, nslices);
+    const int64_t tiles = (int64_t)((M + BM - 1) / BM) * ((N + si.tbn - 1) / si.tbn);
     if (tiles >= 148) return 1;
-    const int chunk = nslices == 4 ? Shape<4>::CHUNK : Shape<3>::CHUNK;
-    const int64_t chunks = (split_k_pad(K) / BK + chunk - 1) / chunk;
+    const int64_t grains = (split_k_pad(K, kind) / si.bke + si.grain - 1) / si.grain;
     int64_t ks = (2 * 148 + tiles - 1) / tiles;
-    ks = std::min<int64_t>(ks, chunks);
+    ks = std::min<int64_t>(ks, grains);
     ks = std::min<int64_t>(ks, 256);
     return (int)std::max<int64_t>(ks, 1);
 }
@@ -592,15 +692,14 @@ void gemm_split(const SlicedOperand& a, const SlicedOperand& b, int M, int N, in
                 cudaStream_t s, int ks) {
     using namespace split;
     (void)K;
-    const int ns = a.nslices;
-    if ((ns != 3 && ns != 4) || b.nslices != ns) throw std::runtime_error("split GEMM operands with different slice counts");
-    const int tbn = ns == 4 ? Shape<4>::TBN : Shape<3>::TBN;
-    const size_t smem = ns == 4 ? Shape<4>::SMEM : Shape<3>::SMEM;
-    const void* kfn = ns == 4 ? (const void*)split_gemm_kernel<4> : (const void*)split_gemm_kernel<3>;
-    set_smem_once(kfn, (int)smem);
+    const int ns = a.nslices, kind = a.kind;
+    if (b.nslices != ns || b.kind != kind || a.kpad != b.kpad)
+        throw std::runtime_error("split GEMM operands sliced differently");
+    const SchemeInfo si = scheme(kind, ns);
+    set_smem_once(si.kfn, (int)si.smem);
     CUtensorMap ma, mb;
-    make_map(&ma, a.data, ns * a.rows, a.kpad, BM);
-    make_map(&mb, b.data, ns * b.rows, b.kpad, tbn);
+    make_map(&ma, a.data, kind, ns * a.rows, a.kpad, BM);
+    make_map(&mb, b.data, kind, ns * b.rows, b.kpad, si.tbn);
     Params p;
     p.M = M;
     p.N = N;
@@ -608,7 +707,7 @@ void gemm_split(const SlicedOperand& a, const SlicedOperand& b, int M, int N, in
     p.Mp = a.rows;
     p.Np = b.rows;
     p.Kp = a.kpad;
-    p.tiles_n = b.rows / tbn;
+    p.tiles_n = b.rows / si.tbn;
     p.alpha = g.alpha;
     p.scaleA = a.scale;
     p.scaleB = b.scale;
@@ -621,18 +720,24 @@ void gemm_split(const SlicedOperand& a, const SlicedOperand& b, int M, int N, in
     p.nvn = g.nvn;
     for (int i = 0; i < 4; i++) p.vsign[i] = g.vsign[i];
     p.err = error_flag();
-    const int nkb = a.kpad / BK;
+    const int nkb = a.kpad / si.bke;
     if (ks > 1 && (!g.ws || (int64_t)ks * M * N > g.ws_elems)) ks = 1;
     if (ks > 65535) ks = 65535;
-    // K blocks per range: whole exact chunks
-    const int chunk = ns == 4 ? Shape<4>::CHUNK : Shape<3>::CHUNK;
-    const int per_chunks = ((nkb + chunk - 1) / chunk + ks - 1) / ks;
+    // K blocks per range: whole grains
+    const int per_grains = ((nkb + si.grain - 1) / si.grain + ks - 1) / ks;
     p.ks = ks;
-    p.kb_per = ks > 1 ? per_chunks * chunk : nkb;
+    p.kb_per = ks > 1 ? per_grains * si.grain : nkb;
     p.ws = g.ws;
     const int tiles = (a.rows / BM) * p.tiles_n;
-    if (ns == 4) split_gemm_kernel<4><<<dim3(tiles, ks), THREADS, smem, s>>>(ma, mb, p);
-    else split_gemm_kernel<3><<<dim3(tiles, ks), THREADS, smem, s>>>(ma, mb, p);
+    const dim3 grid(tiles, ks);
+    if (kind == SLICE_INT8) {
+        if (ns == 3) split_gemm_kernel<3, true><<<grid, THREADS, si.smem, s>>>(ma, mb, p);
+        else if (ns == 4) split_gemm_kernel<4, true><<<grid, THREADS, si.smem, s>>>(ma, mb, p);
+        else split_gemm_kernel<5, true><<<grid, THREADS, si.smem, s>>>(ma, mb, p);
+    } else {
+        if (ns == 3) split_gemm_kernel<3, false><<<grid, THREADS, si.smem, s>>>(ma, mb, p);
+        else split_gemm_kernel<4, false><<<grid, THREADS, si.smem, s>>>(ma, mb, p);
+    }
     g_launches++;
     if (ks > 1) splitk_fold(g, ks, s);
 }

@@ -263,7 +263,7 @@ private:
                           r.nirrep > 1 && !r.aux.empty() ? r.aux.data() : nullptr, opts.pack_vvvv != 0, &H);
         std::vector<double>().swap(r.B);   // the factor is on the device now
         ccsd_options o = opts.solve;
-        if (o.precision == CCSD_PREC_SPLIT && !kern::split_supported()) o.precision = CCSD_PREC_FP64;
+        if (o.precision != CCSD_PREC_FP64 && !kern::split_supported()) o.precision = CCSD_PREC_FP64;
         solver = std::make_unique<Solver>(*ctx, H, o);
     }
 

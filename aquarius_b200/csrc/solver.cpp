@@ -97,8 +97,11 @@ std::vector<int> Solver::owned_tensors() const {
 void Solver::setup() {
     if (opts.diis_damping != 0.0) throw Error(CCSD_ERR_UNSUPPORTED, "DIIS damping is not supported");
     if (opts.diis_order < 1 || opts.diis_order > 16) throw Error(CCSD_ERR_ARG, "diis_order must be in 1..16");
-    if (opts.slices != 0 && opts.slices != 3 && opts.slices != 4)
-        throw Error(CCSD_ERR_ARG, "slices must be 0 (default), 3 or 4");
+    if (opts.precision != CCSD_PREC_FP64 && opts.precision != CCSD_PREC_SPLIT && opts.precision != CCSD_PREC_SPLIT_I8)
+        throw Error(CCSD_ERR_ARG, "bad precision");
+    if (opts.slices != 0 &&
+        !kern::slice_scheme_ok(opts.precision == CCSD_PREC_SPLIT_I8 ? kern::SLICE_INT8 : kern::SLICE_BF16, opts.slices))
+        throw Error(CCSD_ERR_ARG, "slices must be 0 (default) or 3, 4 (BF16) / 3, 4, 5 (INT8)");
     ctx.precision = opts.precision;
     ctx.slices = opts.slices;
     // constants: the H blocks never change, so their split slices can be cached
@@ -106,7 +109,8 @@ void Solver::setup() {
 
     if (ctx.host_only) {
         // planning query: account every allocation and plan one iteration, launch nothing
-        ctx.plan_refine = opts.precision == CCSD_PREC_SPLIT && opts.refine_tol > 0;
+        ctx.plan_refine = (opts.precision == CCSD_PREC_SPLIT || opts.precision == CCSD_PREC_SPLIT_I8) &&
+                          opts.refine_tol > 0;
         for (int sp = 0; sp < 2; sp++)
             for (int s = 0; s < 2; s++) den[sp][s] = (double*)alloc(std::max(ctx.spaces.total(sp, s), 1) * sizeof(double));
         build_diis();
@@ -590,12 +594,12 @@ void Solver::diis_step() {
 }
 
 void Solver::iterate_async() {
-    // Refinement of the split precision.  Three BF16 slices leave a residual floor near
-    // 1e-9; once conv < refine_tol the contractions move to four slices (floor ~2^-8
-    // lower), and to native FP64 only if the residual then stalls above conv_tol.  Graphs
-    // are recaptured after a switch.
-    if (opts.precision == CCSD_PREC_SPLIT && opts.refine_tol > 0 && conv < opts.refine_tol &&
-        ctx.precision != CCSD_PREC_FP64) {
+    // Refinement of the split precision.  Three slices leave a residual floor (near 1e-9
+    // for BF16, ~8x higher for INT8); once conv < refine_tol the contractions move to four
+    // slices, and on a stall above conv_tol to five (INT8) and then to native FP64.
+    // Graphs are recaptured after a switch.
+    const bool split_opts = opts.precision == CCSD_PREC_SPLIT || opts.precision == CCSD_PREC_SPLIT_I8;
+    if (split_opts && opts.refine_tol > 0 && conv < opts.refine_tol && ctx.precision != CCSD_PREC_FP64) {
         bool escalate = false;
         if (ctx.split_slices() == 3) {
             ctx.slices = 4;
@@ -609,13 +613,22 @@ void Solver::iterate_async() {
             const double before = *std::min_element(conv_hist.begin(), conv_hist.end() - 3);
             const double recent = std::min({conv_hist[n - 3], conv_hist[n - 2], conv_hist[n - 1]});
             if (recent > 0.8 * before) {
-                ctx.precision = CCSD_PREC_FP64;
+                if (kern::slice_scheme_ok(ctx.slice_kind(), ctx.split_slices() + 1)) {
+                    ctx.slices = ctx.split_slices() + 1;
+                    ctx.refresh_split(iter_plan);
+                } else {
+                    ctx.precision = CCSD_PREC_FP64;
+                }
                 escalate = true;
             }
         }
         if (escalate) {
             refined = true;
             conv_hist.clear();
+            // the stored vectors carry the previous mode's contraction noise, which would
+            // hold the extrapolated residual at that mode's floor until they age out of the
+            // ring: restart the subspace from the current amplitudes
+            if (opts.diis_order > 1) CCSD_CUDA(cudaMemsetAsync(d_state + 1, 0, sizeof(int), ctx.stream));
             if (graph_exec) cudaGraphExecDestroy(graph_exec);
             if (graph) cudaGraphDestroy(graph);
             graph_exec = nullptr;
@@ -670,7 +683,7 @@ void Solver::check_status() {
     energy = h_red[0];
     conv = h_red[1];
     conv_hist.push_back(conv);
-    if (opts.precision == CCSD_PREC_SPLIT) {
+    if (opts.precision == CCSD_PREC_SPLIT || opts.precision == CCSD_PREC_SPLIT_I8) {
         int e = kern::split_error(true);
         if (e) throw Error(CCSD_ERR_TIMEOUT, "split GEMM wait " + std::to_string(e) + " expired");
     }

@@ -18,7 +18,7 @@ bool Context::split_eligible(const GemmStep& g) const {
     // few-tile products take the split kernel only when splitting K fills the machine (a
     // 1024-k chunk per range)
     const int64_t tiles = (int64_t)((g.M + 127) / 128) * ((g.N + 127) / 128);
-    const int64_t ctas = tiles * kern::split_ksplit(g.M, g.N, g.K, 3);
+    const int64_t ctas = tiles * kern::split_ksplit(g.M, g.N, g.K, 3, slice_kind());
     if (ctas < 148) return false;
     // Skinny products (an extent of a few tens) stay on the FP64 kernels even when the long
     // operand is a constant H block: each statement gathers that block in its own row / k
@@ -29,10 +29,15 @@ bool Context::split_eligible(const GemmStep& g) const {
 
 namespace {
 
-// bytes of the ns BF16 slices (and row scales) of a rows x K operand
-int64_t slice_bytes(int rows, int K, int ns) {
-    return (int64_t)ns * kern::split_rows_pad(rows) * kern::split_k_pad(K) * 2 + 2 * (int64_t)kern::split_rows_pad(rows) * 8;
+// bytes of the ns slices (and row scales) of a rows x K operand
+int64_t slice_bytes(int rows, int K, int ns, int kind) {
+    return kern::split_slice_bytes(rows, K, ns, kind) + 2 * (int64_t)kern::split_rows_pad(rows) * 8;
 }
+
+// workspace bytes per padded row x k element: enough for any scheme (4 BF16 slices at
+// 2 bytes, or 5 INT8 slices at 1 byte over a k padded to 128)
+constexpr int64_t kWsBytesPerElem = 8;
+int64_t ws_k_pad(int K) { return kern::split_k_pad(K, kern::SLICE_INT8); }   // the wider padding
 
 // device bytes the sliced constant operands may occupy (CCSD_SPLIT_CACHE_GB, default 50)
 int64_t cache_budget() {
@@ -44,42 +49,43 @@ int64_t cache_budget() {
 }  // namespace
 
 bool Context::routes_split(const GemmStep& g) const {
-    return precision == CCSD_PREC_SPLIT && kern::split_supported() && split_eligible(g);
+    return split_precision() && kern::split_supported() && split_eligible(g);
 }
 
-kern::SlicedOperand Context::alloc_sliced(int rows, int K, int ns) {
+kern::SlicedOperand Context::alloc_sliced(int rows, int K, int ns, int kind) {
     kern::SlicedOperand s;
     s.rows = kern::split_rows_pad(rows);
-    s.kpad = kern::split_k_pad(K);
+    s.kpad = kern::split_k_pad(K, kind);
     s.nslices = ns;
-    const int64_t nd = (int64_t)s.nslices * s.rows * s.kpad;
-    s.data = (uint16_t*)dmalloc(nd * sizeof(uint16_t));
+    s.kind = kind;
+    s.bytes = kern::split_slice_bytes(rows, K, ns, kind);
+    s.data = (uint8_t*)dmalloc(s.bytes);
     s.scale = (double*)dmalloc(s.rows * sizeof(double));
     s.rowmax = (double*)dmalloc(s.rows * sizeof(double));
-    s.bytes = nd * (int64_t)sizeof(uint16_t) + 2 * (int64_t)s.rows * (int64_t)sizeof(double);
     return s;
 }
 
 void Context::free_sliced(kern::SlicedOperand& s) {
-    const int64_t nd = (int64_t)s.nslices * s.rows * s.kpad;
-    dfree(s.data, nd * sizeof(uint16_t));
+    dfree(s.data, s.bytes);
     dfree(s.scale, s.rows * sizeof(double));
     dfree(s.rowmax, s.rows * sizeof(double));
     s = kern::SlicedOperand();
 }
 
-// make the per-call workspace hold a rows x K operand (never shrinks)
+// make the per-call workspace hold a rows x K operand in any scheme (never shrinks); the
+// rows, kpad, kind and slice count of a view are set per call
 void Context::ensure_ws(kern::SlicedOperand& w, int rows, int K) {
-    const int rp = kern::split_rows_pad(rows), kp = kern::split_k_pad(K);
-    if (w.data && (int64_t)w.rows * w.kpad >= (int64_t)rp * kp && w.rows >= rp) {
-        return;
-    }
-    int keep_rows = std::max(rp, w.rows);
-    int64_t keep_elems = std::max<int64_t>((int64_t)rp * kp, (int64_t)w.rows * w.kpad);
+    const int rp = kern::split_rows_pad(rows);
+    const int64_t need = (int64_t)rp * ws_k_pad(K) * kWsBytesPerElem;
+    if (w.data && w.bytes >= need && w.rows >= rp) return;
+    const int keep_rows = std::max(rp, w.rows);
+    const int64_t keep_bytes = std::max(need, w.bytes);
     if (w.data) free_sliced(w);
-    // capacity is tracked in elements per slice, for the largest slice count (4); rows,
-    // kpad and the slice count of a view are set per call
-    w = alloc_sliced(keep_rows, (int)std::min<int64_t>((keep_elems + keep_rows - 1) / keep_rows, INT32_MAX), 4);
+    w.rows = keep_rows;
+    w.bytes = keep_bytes;
+    w.data = (uint8_t*)dmalloc(keep_bytes);
+    w.scale = (double*)dmalloc(keep_rows * sizeof(double));
+    w.rowmax = (double*)dmalloc(keep_rows * sizeof(double));
 }
 
 // Decide, for every split contraction of a plan, which constant operands keep cached
@@ -102,7 +108,7 @@ void Context::reserve_split(Plan& p) {
                 bool& cache = side == 0 ? g->cache_a : g->cache_b;
                 cache = false;
                 if (h == kScratch || !is_constant(h)) continue;
-                const int64_t b = slice_bytes(rows, g->K, ns);
+                const int64_t b = slice_bytes(rows, g->K, ns, slice_kind());
                 if (used + b <= budget) {
                     cache = true;
                     used += b;
@@ -111,25 +117,28 @@ void Context::reserve_split(Plan& p) {
         }
         return used;
     };
-    // a solve that refines from 3 to 4 slices re-slices its cached operands within the
-    // same budget: a planning query accounts the larger of the two selections
-    int64_t used = plan_refine && host_only ? choose(4) : 0;
+    // a solve that refines to more slices re-slices its cached operands within the same
+    // budget: a planning query accounts the largest selection the refinement can reach
+    // (the flags of the current slice count are chosen last)
+    int64_t used = 0;
+    if (plan_refine && host_only)
+        for (int ns = split_slices() + 1; kern::slice_scheme_ok(slice_kind(), ns); ns++) used = std::max(used, choose(ns));
     used = std::max(used, choose(split_slices()));
     int64_t need_a = 0, need_b = 0, rows_a = 0, rows_b = 0;
     for (GemmStep* g : order) {
         if (!g->cache_a) {
-            need_a = std::max<int64_t>(need_a, (int64_t)kern::split_rows_pad(g->M) * kern::split_k_pad(g->K));
+            need_a = std::max<int64_t>(need_a, (int64_t)kern::split_rows_pad(g->M) * ws_k_pad(g->K));
             rows_a = std::max<int64_t>(rows_a, kern::split_rows_pad(g->M));
         }
         if (!g->cache_b) {
-            need_b = std::max<int64_t>(need_b, (int64_t)kern::split_rows_pad(g->N) * kern::split_k_pad(g->K));
+            need_b = std::max<int64_t>(need_b, (int64_t)kern::split_rows_pad(g->N) * ws_k_pad(g->K));
             rows_b = std::max<int64_t>(rows_b, kern::split_rows_pad(g->N));
         }
     }
     if (host_only) {
         // account the cached slices and the workspace as if they were allocated
         dmalloc(used + 1);
-        dmalloc(8 * (need_a + need_b) + 16 * (rows_a + rows_b) + 1);
+        dmalloc(kWsBytesPerElem * (need_a + need_b) + 16 * (rows_a + rows_b) + 1);
         return;
     }
     for (GemmStep* g : order) {
@@ -162,7 +171,7 @@ void Context::run_split_gemm(GemmStep& g, kern::GemmArgs& a) {
         return;
     }
     split_launches++;
-    const int ns = split_slices();
+    const int ns = split_slices(), kind = slice_kind();
     auto prepare = [&](bool is_a, int64_t& key, kern::SlicedOperand& ws) -> kern::SlicedOperand* {
         const int rows = is_a ? g.M : g.N;
         const double* X = is_a ? a.A : a.B;
@@ -171,37 +180,38 @@ void Context::run_split_gemm(GemmStep& g, kern::GemmArgs& a) {
         const bool kc = is_a ? a.a_kcontig : a.b_kcontig;
         const int h = is_a ? g.tA : g.tB;
         bool& cached = is_a ? g.cache_a : g.cache_b;
-        if (cached && key >= 0 && split_cache[key].nslices != ns) {
-            // the slice count changed (refinement): re-slice within the budget, or stop caching
+        if (cached && key >= 0 && (split_cache[key].nslices != ns || split_cache[key].kind != kind)) {
+            // the scheme changed (refinement): re-slice within the budget, or stop caching
             free_sliced(split_cache[key]);
             split_cache.erase(key);
             split_owner.erase(key);
             key = -1;
             int64_t used = 0;
             for (auto& kv : split_cache) used += kv.second.bytes;
-            if (used + slice_bytes(rows, g.K, ns) > cache_budget()) cached = false;
+            if (used + slice_bytes(rows, g.K, ns, kind) > cache_budget()) cached = false;
         }
         if (cached) {
             if (key < 0) {
                 key = split_cache_next++;
-                split_cache[key] = alloc_sliced(rows, g.K, ns);
+                split_cache[key] = alloc_sliced(rows, g.K, ns, kind);
                 split_owner[key] = h;
-                kern::slice_rows(X, R, Kt, rows, g.K, kc, ns, split_cache[key], stream);
+                kern::slice_rows(X, R, Kt, rows, g.K, kc, split_cache[key], stream);
             }
             return &split_cache[key];
         }
         ensure_ws(ws, rows, g.K);
         kern::SlicedOperand view = ws;
         view.rows = kern::split_rows_pad(rows);
-        view.kpad = kern::split_k_pad(g.K);
+        view.kpad = kern::split_k_pad(g.K, kind);
         view.nslices = ns;
+        view.kind = kind;
         ws_view[is_a ? 0 : 1] = view;
-        kern::slice_rows(X, R, Kt, rows, g.K, kc, ns, ws_view[is_a ? 0 : 1], stream);
+        kern::slice_rows(X, R, Kt, rows, g.K, kc, ws_view[is_a ? 0 : 1], stream);
         return &ws_view[is_a ? 0 : 1];
     };
     kern::SlicedOperand* sa = prepare(true, g.split_cache_a, split_ws.a);
     kern::SlicedOperand* sb = prepare(false, g.split_cache_b, split_ws.b);
-    kern::gemm_split(*sa, *sb, g.M, g.N, g.K, a, stream, kern::split_ksplit(g.M, g.N, g.K, ns));
+    kern::gemm_split(*sa, *sb, g.M, g.N, g.K, a, stream, kern::split_ksplit(g.M, g.N, g.K, ns, kind));
 }
 
 }  // namespace ccsd

@@ -44,6 +44,9 @@ WORKLOADS = {
 CPU_SAMPLE = {"cfg2": (16, 64), "cfg3": (32, 80), "cfg4": (24, 80), "small": (8, 48)}
 LADDER = "Z(2)[abij] += <ab||cd>[abef]*Tau[efij]"
 DIIS_ORDER = 8
+# residual at which a split solve moves from 3 to 4 slices: above the 3-slice floor
+# (~2e-9 for BF16 slices, ~4e-7 for INT8 slices at o=32 v=256)
+REFINE_TOL = {"split": 1e-6, "split_i8": 1e-5}
 
 
 def log(*a):
@@ -201,7 +204,7 @@ def serve(A, n_req, rate, seed, precision, log_each=False):
     reqs = serve_requests(n_req, seed)
     gaps = np.random.default_rng(seed + 1).exponential(1.0 / rate, size=n_req)
     srv = A.Server(0, max_active=16, precision=precision, conv_tol=1e-9, max_iter=100, diis_order=DIIS_ORDER,
-                   refine_tol=1e-6 if precision == "split" else 0.0)
+                   refine_tol=REFINE_TOL.get(precision, 0.0))
     t0 = time.perf_counter()
     t = 0.0
     ids = {}
@@ -293,8 +296,8 @@ def run_kernel(args):
     stream = torch.cuda.Stream()
     ctx = A.Context(0, stream.cuda_stream)
     ctx.set_spaces(vrt=[w["v"]], occ=[w["o"]])
-    if args.precision == "split":
-        ctx.set_precision("split")
+    if args.precision in ("split", "split_i8"):
+        ctx.set_precision(args.precision)
     V = ctx.tensor("A", *sa, packed=packed)
     T = ctx.tensor("B", *sb)
     Z = ctx.tensor("C", *sc)
@@ -334,7 +337,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--workload", default="cfg3", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="auto", choices=["auto", "split", "fp64"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "split", "split_i8", "fp64"])
+    ap.add_argument("--slices", type=int, default=0,
+                    help="slices per operand of the timed split mode (0: the default of the precision)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64-ref", action="store_true", help="skip the native-FP64 comparison run")
@@ -384,9 +389,10 @@ def main():
 
     peaks, peak_kind = measured_peaks()
     results = {}
-    order = ["fp64", prec] if (prec == "split" and not args.no_fp64_ref) else [prec]
+    order = ["fp64", prec] if (prec != "fp64" and not args.no_fp64_ref) else [prec]
     for p in order:
-        s = ctx.solver(H, diis_order=DIIS_ORDER, precision=p, conv_tol=1e-9, max_iter=1000)
+        s = ctx.solver(H, diis_order=DIIS_ORDER, precision=p, conv_tol=1e-9, max_iter=1000,
+                       slices=args.slices if p != "fp64" else 0)
         flops = s.flops()
         with Clocks(local) as clk:
             if dist:
@@ -426,6 +432,11 @@ def main():
     if prec == "split" and peak:
         # three BF16 slices per operand: six tcgen05 products per FP64-equivalent product
         roofline["tensor_pipe_frac"] = 6 * achieved / peak
+    elif prec == "split_i8" and peak:
+        # three INT8 slices: six products on the INT8 pipe, taken as twice the measured BF16
+        # rate (the nominal ratio; the INT8 rate itself is not in MEASURED_PEAKS.json)
+        roofline["tensor_pipe_frac"] = 6 * achieved / (2 * peak)
+        roofline["tensor_pipe_peak_kind"] = "int8 = 2 x measured bf16 (nominal ratio)"
 
     # end to end through the public API: host factor -> H on device -> solve -> energy
     e2e = None
@@ -439,11 +450,10 @@ def main():
         t0 = time.perf_counter()
         H2 = ctx.hamiltonian_from_factor(Bp, epsp, aux_per_irrep=aux if w["nirrep"] > 1 else None)
         t_h = time.perf_counter() - t0
-        # 3-slice residuals bottom out near 1e-9: past 1e-6 (1000 x conv_tol) the contractions
-        # move to 4 slices, early enough that the DIIS history is not dominated by 3-slice
-        # noise (a switch at 1e-7 stalled here and fell back to FP64)
+        # the contractions move to 4 slices once the residual passes REFINE_TOL (the DIIS
+        # subspace restarts there), to 5 INT8 slices and then FP64 only on a stall
         s = ctx.solver(H2, diis_order=DIIS_ORDER, precision=prec, conv_tol=1e-9, max_iter=80,
-                       refine_tol=1e-6 if prec == "split" else 0.0)
+                       refine_tol=REFINE_TOL.get(prec, 0.0))
         # Iterative::run, one iteration per call (the loop of ccsd_solver_run), recording
         # which contraction mode each iteration used
         phases, c_fin, iters, trace = {}, float("inf"), 0, []
@@ -487,7 +497,8 @@ def main():
         line = {
             "metric": "CCSD iterations/s", "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "bf16x3-split->f64",
+            "vs_baseline": None,
+            "dtype": {"fp64": "f64", "split": "bf16x3-split->f64", "split_i8": "i8x3-split->f64"}[prec],
             "data": "synthetic (seeded generator, B[P,p,q] factor, eps occ U[-1.2,-0.4] vrt U[0.3,4.0])",
             "config": {"workload": w["desc"], "o": w["o"], "v": w["v"], "nirrep": w["nirrep"], "precision": prec,
                        "diis_order": DIIS_ORDER, "parallelism": f"replicas x{world}",

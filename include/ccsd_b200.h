@@ -60,8 +60,10 @@ typedef struct ccsd_solver_s* ccsd_solver;
 
 /* precision of the contraction layer */
 enum {
-    CCSD_PREC_FP64  = 0,   /* native FP64 GEMMs (plain path) */
-    CCSD_PREC_SPLIT = 1    /* split BF16 slices on tcgen05, FP32 accumulate, summed in FP64 */
+    CCSD_PREC_FP64     = 0,   /* native FP64 GEMMs (plain path) */
+    CCSD_PREC_SPLIT    = 1,   /* split BF16 slices on tcgen05, FP32 accumulate, summed in FP64 */
+    CCSD_PREC_SPLIT_I8 = 2    /* split INT8 slices on tcgen05 (twice the BF16 rate), exact INT32
+                                 accumulate per slice level, summed in FP64 */
 };
 
 /* tensor creation flags */
@@ -164,7 +166,7 @@ typedef struct {
     int    diis_order;    /* default 5     (ccsd.cxx:281-282) */
     int    diis_start;    /* default 1     (ccsd.cxx:279-280) */
     double diis_damping;  /* default 0.0   (ccsd.cxx:277-278) */
-    int    precision;     /* CCSD_PREC_FP64 or CCSD_PREC_SPLIT */
+    int    precision;     /* CCSD_PREC_FP64, CCSD_PREC_SPLIT or CCSD_PREC_SPLIT_I8 */
     int    slices;        /* split-BF16 slices per operand: 3 (0 = default) or 4 */
     int    use_graph;     /* capture one iteration as a CUDA graph and replay it */
     double refine_tol;    /* split precision only: once conv < refine_tol, 3-slice
