@@ -56,28 +56,33 @@ void set_smem_once(const void* kernel, int bytes);
 namespace split {
 
 constexpr int BM = 128;
-constexpr int KB_BYTES = 128;                       // one k-block: a 128-byte row segment
-constexpr int STAGES = 2;
 constexpr int EPI_WARPS = 8;
 constexpr int THREADS = 32 * (2 + EPI_WARPS);
-constexpr int TILE_A_BYTES = BM * KB_BYTES;         // 16 KiB
 constexpr long long WAIT_CYCLES = 4000000000ll;     // ~2 s at 1.9 GHz
+constexpr int SMEM_LIMIT = 227 * 1024;
 
-// Kernel shape per scheme.  A stage holds NS A tiles and NS B tiles of one k-block;
-// the tile width keeps a stage near 96 KiB (two stages fit in shared memory).
+// Kernel shape per scheme.  A stage holds NS A tiles and NS B tiles of one k-block (a
+// 128- or 64-byte row segment); as many stages as fit in shared memory (at most 4).
 template <int NS, bool I8>
 struct Shape {
-    static constexpr int BKE = I8 ? 128 : 64;                       // k elements per k-block
-    static constexpr int TBN = NS == 3 ? 128 : NS == 4 ? 64 : 32;
-    static constexpr int TILE_B = TBN * KB_BYTES;
-    static constexpr int STAGE = NS * (TILE_A_BYTES + TILE_B);
+    // 4 and 5 INT8 slices use 64-byte k-blocks so that wider tiles still fit
+    static constexpr int KBB = (I8 && NS >= 4) ? 64 : 128;          // bytes per k-block row
+    static constexpr int BKE = KBB / (I8 ? 1 : 2);                  // k elements per k-block
+    static constexpr int TBN = I8 ? (NS <= 4 ? 128 : 64) : (NS == 3 ? 128 : 64);
+    static constexpr int TILE_A = BM * KBB;
+    static constexpr int TILE_B = TBN * KBB;
+    static constexpr int STAGE = NS * (TILE_A + TILE_B);
+    static constexpr int STAGES_FIT = (SMEM_LIMIT - 1024 - 256) / STAGE;
+    static constexpr int STAGES = STAGES_FIT < 4 ? STAGES_FIT : 4;
+    static constexpr int KSTEPS = KBB / 32;                         // MMAs of 32 bytes of K per k-block
     // accumulators per buffer.  BF16: s1*s1 (exact over 1024 k) and the rest; 4 slices
     // also keep s1*s2 + s2*s1 apart (exact over 512 k).  INT8: one exact INT32
     // accumulator per level i+j.
     static constexpr int NACC = I8 ? NS : (NS == 4 ? 3 : 2);
-    static constexpr int CHUNK = I8 ? 512 : (NS == 4 ? 8 : 16);     // k-blocks per drained chunk
-    // split-K ranges: whole exact chunks (BF16), any 8 k-blocks (INT8: exact per range)
-    static constexpr int KSPLIT_GRAIN = I8 ? 8 : CHUNK;
+    // k-blocks per drained chunk: 1024 / 512 k (BF16), 65536 k (INT8: |level| < 2^31)
+    static constexpr int CHUNK = I8 ? 65536 / BKE : (NS == 4 ? 8 : 16);
+    // split-K ranges: whole exact chunks (BF16), any 1024 k (INT8: exact per range)
+    static constexpr int KSPLIT_GRAIN = I8 ? 1024 / BKE : CHUNK;
     static constexpr int BUF = NACC * TBN;                          // TMEM columns per buffer
     static constexpr int NBUF = 2 * BUF <= 512 ? 2 : 1;             // double-buffered if two fit
     static constexpr int TMEM_COLS = NBUF * BUF <= 256 ? 256 : 512;
@@ -87,7 +92,9 @@ struct Shape {
     // N = TBN, M = 128
     static constexpr uint32_t IDESC = (I8 ? (2u << 4) : (1u << 4)) | (1u << 7) | (1u << 10) |
                                       ((uint32_t)(TBN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
-    static_assert(STAGE * STAGES + 1024 + 256 <= 227 * 1024, "stages exceed shared memory");
+    static_assert(STAGES >= 2, "two stages must fit");
+    static_assert(SMEM <= SMEM_LIMIT, "stages exceed shared memory");
+    static_assert(BUF <= 512, "accumulators exceed TMEM");
     static_assert(TBN % 16 == 0 && TBN >= 16 && TBN <= 256, "MMA N");
 };
 
@@ -164,14 +171,16 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
         : "memory");
 }
 
-// K-major, 128-byte swizzled tile descriptor (rows of 128 B, 8-row groups 1024 B apart)
+// K-major swizzled tile descriptor: rows of KBB (128 or 64) bytes, 8-row groups 8*KBB
+// bytes apart, swizzle of the row width
+template <int KBB>
 __device__ __forceinline__ uint64_t sdesc(const void* p) {
     uint64_t d = 0;
     d |= (uint64_t)((smem_u32(p) >> 4) & 0x3FFF);
-    d |= (uint64_t)1 << 16;                 // leading byte offset (unused for swizzled K-major)
-    d |= (uint64_t)(1024 >> 4) << 32;       // stride byte offset
-    d |= (uint64_t)1 << 46;                 // descriptor version (sm_100)
-    d |= (uint64_t)2 << 61;                 // SWIZZLE_128B
+    d |= (uint64_t)1 << 16;                           // leading byte offset (unused for swizzled K-major)
+    d |= (uint64_t)((8 * KBB) >> 4) << 32;            // stride byte offset
+    d |= (uint64_t)1 << 46;                           // descriptor version (sm_100)
+    d |= (uint64_t)(KBB == 128 ? 2 : 4) << 61;        // SWIZZLE_128B / SWIZZLE_64B
     return d;
 }
 
@@ -213,17 +222,17 @@ template <int NS, bool I8>
 __global__ void __launch_bounds__(THREADS, 1)
     split_gemm_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, Params p) {
     using Sh = Shape<NS, I8>;
-    constexpr int NBUF = Sh::NBUF;
+    constexpr int NBUF = Sh::NBUF, STAGES = Sh::STAGES;
     constexpr int TBN = Sh::TBN, COLS = Sh::COLS;
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
     uint8_t* stages = smem;
     uint64_t* bars = (uint64_t*)(smem + (size_t)STAGES * Sh::STAGE);
-    uint64_t* full = bars;          // [STAGES]
-    uint64_t* empty = bars + 2;     // [STAGES]
-    uint64_t* tfull = bars + 4;     // [2]
-    uint64_t* tempty = bars + 6;    // [2]
-    uint32_t* tmem_slot = (uint32_t*)(bars + 8);
+    uint64_t* full = bars;                   // [STAGES]
+    uint64_t* empty = bars + STAGES;         // [STAGES]
+    uint64_t* tfull = bars + 2 * STAGES;     // [2]
+    uint64_t* tempty = bars + 2 * STAGES + 2;   // [2]
+    uint32_t* tmem_slot = (uint32_t*)(bars + 2 * STAGES + 4);
     volatile int* abort_flag = (volatile int*)(tmem_slot + 1);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -267,9 +276,9 @@ __global__ void __launch_bounds__(THREADS, 1)
                 uint8_t* base = stages + (size_t)s * Sh::STAGE;
                 // x = k-block start in elements: a multiple of 128 bytes
                 for (int i = 0; i < NS; i++)
-                    tma_load_2d(base + i * TILE_A_BYTES, &tmA, (kb0 + kb) * Sh::BKE, i * p.Mp + m0, &full[s]);
+                    tma_load_2d(base + i * Sh::TILE_A, &tmA, (kb0 + kb) * Sh::BKE, i * p.Mp + m0, &full[s]);
                 for (int i = 0; i < NS; i++)
-                    tma_load_2d(base + NS * TILE_A_BYTES + i * Sh::TILE_B, &tmB, (kb0 + kb) * Sh::BKE,
+                    tma_load_2d(base + NS * Sh::TILE_A + i * Sh::TILE_B, &tmB, (kb0 + kb) * Sh::BKE,
                                 i * p.Np + n0, &full[s]);
             }
         }
@@ -296,11 +305,11 @@ __global__ void __launch_bounds__(THREADS, 1)
                     uint64_t ad[NS], bd[NS];
 #pragma unroll
                     for (int i = 0; i < NS; i++) {
-                        ad[i] = sdesc(base + i * TILE_A_BYTES);
-                        bd[i] = sdesc(base + NS * TILE_A_BYTES + i * Sh::TILE_B);
+                        ad[i] = sdesc<Sh::KBB>(base + i * Sh::TILE_A);
+                        bd[i] = sdesc<Sh::KBB>(base + NS * Sh::TILE_A + i * Sh::TILE_B);
                     }
 #pragma unroll
-                    for (int kk = 0; kk < 4; kk++) {
+                    for (int kk = 0; kk < Sh::KSTEPS; kk++) {
                         // one MMA covers 32 bytes of K (16 BF16 or 32 INT8 values)
                         const uint64_t o = (uint64_t)(kk * 32) >> 4;
                         // slice products (i, t - i) with t < NS into accumulator t (INT8) or
@@ -564,17 +573,18 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 
-void make_map(CUtensorMap* map, const uint8_t* base, int kind, int rows_total, int kpad, int box_rows) {
+void make_map(CUtensorMap* map, const uint8_t* base, int kind, int rows_total, int kpad, int box_rows, int kbb) {
     EncodeTiledFn enc = encode_fn();
     if (!enc) throw std::runtime_error("cuTensorMapEncodeTiled is not available");
     const int eb = slice_elem_bytes(kind);
     cuuint64_t dims[2] = {(cuuint64_t)kpad, (cuuint64_t)rows_total};
     cuuint64_t strides[1] = {(cuuint64_t)kpad * eb};
-    cuuint32_t box[2] = {(cuuint32_t)(KB_BYTES / eb), (cuuint32_t)box_rows};   // 128 bytes of k
+    cuuint32_t box[2] = {(cuuint32_t)(kbb / eb), (cuuint32_t)box_rows};   // one k-block of kbb bytes
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(map, kind == SLICE_INT8 ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
                      (void*)base, dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, kbb == 128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) throw std::runtime_error("cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
 }
@@ -608,7 +618,7 @@ bool split_supported() {
 
 int split_rows_pad(int rows) { return (rows + split::BM - 1) / split::BM * split::BM; }
 int split_k_pad(int k, int kind) {
-    const int bke = split::KB_BYTES / slice_elem_bytes(kind);
+    const int bke = 128 / slice_elem_bytes(kind);   // a multiple of every scheme's k-block
     return (k + bke - 1) / bke * bke;
 }
 
@@ -652,7 +662,7 @@ void slice_rows(const double* X, const int64_t* R, const int64_t* Kt, int nrows,
 
 namespace {
 struct SchemeInfo {
-    int tbn, bke, chunk, grain;
+    int tbn, bke, kbb, chunk, grain;
     size_t smem;
     const void* kfn;
 };
@@ -660,7 +670,8 @@ struct SchemeInfo {
 template <int NS, bool I8>
 SchemeInfo scheme_info() {
     using Sh = split::Shape<NS, I8>;
-    return {Sh::TBN, Sh::BKE, Sh::CHUNK, Sh::KSPLIT_GRAIN, Sh::SMEM, (const void*)split::split_gemm_kernel<NS, I8>};
+    return {Sh::TBN, Sh::BKE, Sh::KBB, Sh::CHUNK, Sh::KSPLIT_GRAIN, Sh::SMEM,
+            (const void*)split::split_gemm_kernel<NS, I8>};
 }
 
 SchemeInfo scheme(int kind, int ns) {
@@ -698,8 +709,8 @@ void gemm_split(const SlicedOperand& a, const SlicedOperand& b, int M, int N, in
     const SchemeInfo si = scheme(kind, ns);
     set_smem_once(si.kfn, (int)si.smem);
     CUtensorMap ma, mb;
-    make_map(&ma, a.data, kind, ns * a.rows, a.kpad, BM);
-    make_map(&mb, b.data, kind, ns * b.rows, b.kpad, si.tbn);
+    make_map(&ma, a.data, kind, ns * a.rows, a.kpad, BM, si.kbb);
+    make_map(&mb, b.data, kind, ns * b.rows, b.kpad, si.tbn, si.kbb);
     Params p;
     p.M = M;
     p.N = N;

@@ -8,7 +8,12 @@ resident in HBM.  Inputs are far larger than L2 (V_abcd alone is ~51 GB), so no 
 flush is needed between steps.
 
   python bench.py [--steps K] [--warmup W] [--gpus N] [--workload cfg3|cfg2|...]
-                  [--precision split|fp64] [--impl engine|reference]
+                  [--precision split_i8|split|fp64] [--slices N] [--impl engine|reference]
+
+The default timed mode is the split path with four INT8 slices per operand (the fewest
+whose iterations hold |dE| <= 1e-8 Eh against the FP64 plain path here); the line also
+carries the FP64 plain path of the same iterations, the end-to-end solve (3 -> 4 slice
+refinement to conv 1e-9) and a bounded serving run.
 
 For N>1 (torchrun, one rank per GPU) every rank runs an independent replica of the
 workload (the north star fixes one GPU per solve: "replicas only"); the value is the
@@ -240,7 +245,7 @@ def serve(A, n_req, rate, seed, precision, log_each=False):
 
 def run_serve(args):
     import aquarius_b200 as A
-    prec = args.precision if args.precision != "auto" else "split"
+    prec = args.precision if args.precision != "auto" else "split_i8"
     lines = []
     for rate in args.rates:
         r = serve(A, args.requests, rate, args.serve_seed, prec, log_each=True)
@@ -375,7 +380,11 @@ def main():
 
     w = WORKLOADS[args.workload]
     split_ok = A.lib() is not None and _split_available(A)
-    prec = args.precision if args.precision != "auto" else ("split" if split_ok else "fp64")
+    prec = args.precision if args.precision != "auto" else ("split_i8" if split_ok else "fp64")
+    if prec == "split_i8" and args.slices == 0:
+        # the timed mode: the fewest INT8 slices whose iterations hold |dE| <= 1e-8 Eh against
+        # the FP64 plain path at this workload (3 slices drift to ~3e-7, 4 to ~2e-9)
+        args.slices = 4
 
     stream = torch.cuda.Stream(device=local)
     ctx = A.Context(local, stream.cuda_stream)
@@ -429,13 +438,16 @@ def main():
                 "frac": achieved / peak if peak else None, "traffic": None, "peak_kind": unit_kind,
                 "launches_per_step": lad["launches"] / args.steps,
                 "share_of_step": lad["ms"] / head["ms"] if head["ms"] else None}
+    ns = args.slices or 3
+    products = ns * (ns + 1) // 2     # kept slice products (i + j < ns) per FP64-equivalent product
     if prec == "split" and peak:
-        # three BF16 slices per operand: six tcgen05 products per FP64-equivalent product
-        roofline["tensor_pipe_frac"] = 6 * achieved / peak
+        roofline["tensor_pipe_frac"] = products * achieved / peak
+        roofline["slice_products"] = products
     elif prec == "split_i8" and peak:
-        # three INT8 slices: six products on the INT8 pipe, taken as twice the measured BF16
-        # rate (the nominal ratio; the INT8 rate itself is not in MEASURED_PEAKS.json)
-        roofline["tensor_pipe_frac"] = 6 * achieved / (2 * peak)
+        # products on the INT8 pipe, taken as twice the measured BF16 rate (the nominal
+        # ratio; the INT8 rate itself is not in MEASURED_PEAKS.json)
+        roofline["tensor_pipe_frac"] = products * achieved / (2 * peak)
+        roofline["slice_products"] = products
         roofline["tensor_pipe_peak_kind"] = "int8 = 2 x measured bf16 (nominal ratio)"
 
     # end to end through the public API: host factor -> H on device -> solve -> energy
@@ -498,7 +510,8 @@ def main():
             "metric": "CCSD iterations/s", "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
-            "dtype": {"fp64": "f64", "split": "bf16x3-split->f64", "split_i8": "i8x3-split->f64"}[prec],
+            "dtype": "f64" if prec == "fp64" else
+                     f"{'i8' if prec == 'split_i8' else 'bf16'}x{args.slices or 3}-split->f64",
             "data": "synthetic (seeded generator, B[P,p,q] factor, eps occ U[-1.2,-0.4] vrt U[0.3,4.0])",
             "config": {"workload": w["desc"], "o": w["o"], "v": w["v"], "nirrep": w["nirrep"], "precision": prec,
                        "diis_order": DIIS_ORDER, "parallelism": f"replicas x{world}",
