@@ -14,6 +14,7 @@
 // Solves share nothing on the device but the memory pool; each one runs the same kernels
 // and reductions it would run alone, so its result does not depend on the mix.
 #include <algorithm>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <atomic>
@@ -231,8 +232,22 @@ private:
         finish(r, status, 0, 0, 0, 0, now());
     }
 
-    void build(Request& r, std::unique_ptr<Context>& ctx, std::unique_ptr<Solver>& solver) {
-        ctx = std::make_unique<Context>(opts.device, nullptr);
+    // Stream priority of a solve: the fewer flops per iteration, the higher.  A small
+    // (e.g. symmetry-blocked) solve is a chain of short dependent launches; at equal
+    // priority each waits behind the long GEMM waves of the large solves sharing the GPU.
+    static cudaStream_t priority_stream(double flops) {
+        int least = 0, greatest = 0;
+        CCSD_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        double f = (std::log10(std::max(flops, 1.0)) - 10.0) / 4.0;   // 1e10 -> 0, 1e14 -> 1
+        f = std::min(1.0, std::max(0.0, f));
+        const int prio = greatest + (int)std::lround(f * (least - greatest));
+        cudaStream_t st = nullptr;
+        CCSD_CUDA(cudaStreamCreateWithPriority(&st, cudaStreamNonBlocking, prio));
+        return st;
+    }
+
+    void build(Request& r, cudaStream_t stream, std::unique_ptr<Context>& ctx, std::unique_ptr<Solver>& solver) {
+        ctx = std::make_unique<Context>(opts.device, stream);
         Spaces S;
         S.nirrep = r.nirrep;
         for (int sp = 0; sp < 2; sp++)
@@ -273,12 +288,14 @@ private:
         std::unique_ptr<Context> ctx;
         std::unique_ptr<Solver> s;
         cudaEvent_t ev = nullptr;
+        cudaStream_t stream = nullptr;
         int status = CCSD_OK;
         double e = 0, c = 0, mp2 = 0;
         int it = 0;
         std::string msg;
         try {
-            build(*r, ctx, s);
+            stream = priority_stream(r->flops);
+            build(*r, stream, ctx, s);
             mp2 = s->mp2;
             CCSD_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming | cudaEventBlockingSync));
             while (true) {
@@ -316,6 +333,7 @@ private:
             ctx.reset();
         } catch (...) {
         }
+        if (stream) cudaStreamDestroy(stream);
         {
             std::lock_guard<std::mutex> lk(mu);
             used_bytes -= r->bytes;

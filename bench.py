@@ -204,12 +204,12 @@ def serve_requests(n, seed):
     return out
 
 
-def serve(A, n_req, rate, seed, precision, log_each=False):
+def serve(A, n_req, rate, seed, precision, log_each=False, graph=False):
     """Poisson arrivals at `rate` req/s into the serving loop; time-to-converged per request."""
     reqs = serve_requests(n_req, seed)
     gaps = np.random.default_rng(seed + 1).exponential(1.0 / rate, size=n_req)
     srv = A.Server(0, max_active=16, precision=precision, conv_tol=1e-9, max_iter=100, diis_order=DIIS_ORDER,
-                   refine_tol=REFINE_TOL.get(precision, 0.0))
+                   refine_tol=REFINE_TOL.get(precision, 0.0), use_graph=graph)
     t0 = time.perf_counter()
     t = 0.0
     ids = {}
@@ -248,7 +248,7 @@ def run_serve(args):
     prec = args.precision if args.precision != "auto" else "split_i8"
     lines = []
     for rate in args.rates:
-        r = serve(A, args.requests, rate, args.serve_seed, prec, log_each=True)
+        r = serve(A, args.requests, rate, args.serve_seed, prec, log_each=True, graph=args.graph)
         line = {"metric": "CCSD serving time-to-converged", "value": r["p50_s"], "unit": "s",
                 "higher_is_better": False, "n_gpus": 1, "data": "synthetic", **r}
         print(json.dumps(line), flush=True)
@@ -345,6 +345,8 @@ def main():
     ap.add_argument("--precision", default="auto", choices=["auto", "split", "split_i8", "fp64"])
     ap.add_argument("--slices", type=int, default=0,
                     help="slices per operand of the timed split mode (0: the default of the precision)")
+    ap.add_argument("--graph", action="store_true",
+                    help="end-to-end solve and serving replay each iteration as a CUDA graph")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64-ref", action="store_true", help="skip the native-FP64 comparison run")
@@ -465,7 +467,7 @@ def main():
         # the contractions move to 4 slices once the residual passes REFINE_TOL (the DIIS
         # subspace restarts there), to 5 INT8 slices and then FP64 only on a stall
         s = ctx.solver(H2, diis_order=DIIS_ORDER, precision=prec, conv_tol=1e-9, max_iter=80,
-                       refine_tol=REFINE_TOL.get(prec, 0.0))
+                       refine_tol=REFINE_TOL.get(prec, 0.0), use_graph=args.graph)
         # Iterative::run, one iteration per call (the loop of ccsd_solver_run), recording
         # which contraction mode each iteration used
         phases, c_fin, iters, trace = {}, float("inf"), 0, []
@@ -493,7 +495,7 @@ def main():
     # bounded serving run (the full sweep is `--serve`): Poisson arrivals at 2 req/s
     serving = None
     if args.serve_sample > 0 and rank == 0:
-        serving = serve(A, args.serve_sample, 2.0, args.serve_seed, prec, log_each=True)
+        serving = serve(A, args.serve_sample, 2.0, args.serve_seed, prec, log_each=True, graph=args.graph)
         log(f"[bench] serving: p50 {serving['p50_s']:.2f}s p99 {serving['p99_s']:.2f}s, "
             f"{serving['aggregate_iters_per_s']:.1f} iter/s aggregate, peak {serving['peak_active']} active")
 
