@@ -414,7 +414,9 @@ void Context::release(Plan& p) {
         for (auto& r : kv.second.runs)
             for (auto& l : r.launches) {
                 if (l.d_probs) dfree(l.d_probs, l.nprob * sizeof(kern::GemmArgs));
-                if (l.d_tile_start) dfree(l.d_tile_start, l.nprob * sizeof(int));
+                if (l.d_part) dfree(l.d_part, l.part_elems * sizeof(double));
+                if (l.d_tile_start)
+                    dfree(l.d_tile_start, (l.kind == GemmLaunch::FOLD_GROUPS ? l.ngroups + 1 : l.nprob) * sizeof(int));
                 if (l.d_desc) dfree(l.d_desc, l.desc_bytes);
                 if (l.d_chunks) dfree(l.d_chunks, l.nprob * sizeof(int64_t));
             }
@@ -504,7 +506,10 @@ RunSchedule& Context::schedule(Plan& p) {
     while (s < p.steps.size()) {
         const Step::Kind kind = p.steps[s].kind;
         if (kind == Step::DOT) {
-            s++;
+            size_t e = s;
+            while (e < p.steps.size() && p.steps[e].kind == Step::DOT) e++;
+            if (e - s >= 2) build_dot_run(p, rs, (int)s, (int)e);
+            s = e;
             continue;
         }
         const std::string& lab = label_of(p.steps[s]);
@@ -544,6 +549,7 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
     };
     std::map<std::pair<int, int64_t>, int> last;
     std::vector<int> level(end - first, 0);
+    std::vector<std::pair<int, int64_t>> key1(end - first, {0, -1});   // the block of a one-destination step
     int maxlvl = 0;
     int ngroupable = 0;
     for (int i = first; i < end; i++) {
@@ -563,6 +569,7 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
         }
         for (auto& k : keys) last[k] = lvl;
         level[i - first] = lvl;
+        if (keys.size() == 1) key1[i - first] = keys[0];
         maxlvl = std::max(maxlvl, lvl);
         if (groupable(g)) ngroupable++;
     }
@@ -571,10 +578,112 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
     run.first = first;
     run.end = end;
     bool any_group = false;
+
+    // Shared-output groups.  Small one-destination products that several levels would
+    // serialise (block contractions of a symmetry-blocked statement summing into the same
+    // output blocks over their internal irreps) run as one grouped launch per operand
+    // contiguity writing dense partial products, then one fold launch: a CTA per output
+    // block adds its products in plan order (deterministic).
+    std::vector<char> in_fold(end - first, 0);
+    {
+        int nfold = 0;
+        bool multi = false;
+        int64_t part = 0;
+        for (int i = first; i < end; i++) {
+            const GemmStep& g = p.gemms[p.steps[i].idx];
+            if (!groupable(g) || g.nvm != 1 || g.nvn != 1 || key1[i - first].second < 0) continue;
+            if ((int64_t)g.M * g.N > 65536) continue;
+            in_fold[i - first] = 1;
+            nfold++;
+            multi |= level[i - first] > 0;
+            part += (int64_t)g.M * g.N;
+        }
+        if (nfold < 2 || !multi || part > (32ll << 20)) std::fill(in_fold.begin(), in_fold.end(), 0);
+        else {
+            double* d_part = (double*)dmalloc(part * sizeof(double));
+            int64_t off = 0;
+            std::vector<kern::GemmArgs> probs[4];
+            std::vector<int> tstart[4];
+            int tiles[4] = {0, 0, 0, 0};
+            double fl[4] = {0, 0, 0, 0};
+            std::map<std::pair<int, int64_t>, std::vector<kern::FoldDesc>> groups;
+            std::vector<std::pair<int, int64_t>> group_order;
+            for (int i = first; i < end; i++) {
+                if (!in_fold[i - first]) continue;
+                const GemmStep& g = p.gemms[p.steps[i].idx];
+                kern::GemmArgs a = gemm_args(p, g);
+                kern::FoldDesc f;
+                f.part = d_part + off;
+                f.C = a.C;
+                f.Cm = a.Cm[0];
+                f.Cn = a.Cn[0];
+                f.M = g.M;
+                f.N = g.N;
+                f.scale = a.alpha * a.vsign[0];
+                a.ws = d_part + off;
+                a.ws_elems = (int64_t)g.M * g.N;
+                a.partial_out = true;
+                off += (int64_t)g.M * g.N;
+                const int c = (g.a_kcontig ? 2 : 0) + (g.b_kcontig ? 1 : 0);
+                probs[c].push_back(a);
+                tstart[c].push_back(tiles[c]);
+                tiles[c] += kern::fp64_tiles(g.M, g.N);
+                fl[c] += g.flops();
+                auto k = key1[i - first];
+                if (!groups.count(k)) group_order.push_back(k);
+                groups[k].push_back(f);
+            }
+            bool first_launch = true;
+            for (int c = 0; c < 4; c++) {
+                if (probs[c].empty()) continue;
+                GemmLaunch l;
+                l.kind = GemmLaunch::GEMM_GROUPED;
+                l.ak = (c & 2) != 0;
+                l.bk = (c & 1) != 0;
+                l.nprob = (int)probs[c].size();
+                l.tiles = tiles[c];
+                l.flops = fl[c];
+                if (first_launch) {   // the partial buffer is owned by the first launch
+                    l.d_part = d_part;
+                    l.part_elems = part;
+                    first_launch = false;
+                }
+                l.d_probs = (kern::GemmArgs*)dmalloc(probs[c].size() * sizeof(kern::GemmArgs));
+                l.d_tile_start = (int*)dmalloc(tstart[c].size() * sizeof(int));
+                CCSD_CUDA(cudaMemcpyAsync(l.d_probs, probs[c].data(), probs[c].size() * sizeof(kern::GemmArgs),
+                                          cudaMemcpyHostToDevice, stream));
+                CCSD_CUDA(cudaMemcpyAsync(l.d_tile_start, tstart[c].data(), tstart[c].size() * sizeof(int),
+                                          cudaMemcpyHostToDevice, stream));
+                CCSD_CUDA(cudaStreamSynchronize(stream));
+                run.launches.push_back(l);
+            }
+            std::vector<kern::FoldDesc> descs;
+            std::vector<int> gstart;
+            for (auto& k : group_order) {
+                gstart.push_back((int)descs.size());
+                for (auto& f : groups[k]) descs.push_back(f);
+            }
+            gstart.push_back((int)descs.size());
+            GemmLaunch fl_l;
+            fl_l.kind = GemmLaunch::FOLD_GROUPS;
+            fl_l.nprob = (int)descs.size();
+            fl_l.ngroups = (int)group_order.size();
+            fl_l.desc_bytes = descs.size() * sizeof(kern::FoldDesc);
+            fl_l.d_desc = dmalloc(fl_l.desc_bytes);
+            fl_l.d_tile_start = (int*)dmalloc(gstart.size() * sizeof(int));
+            CCSD_CUDA(cudaMemcpyAsync(fl_l.d_desc, descs.data(), fl_l.desc_bytes, cudaMemcpyHostToDevice, stream));
+            CCSD_CUDA(cudaMemcpyAsync(fl_l.d_tile_start, gstart.data(), gstart.size() * sizeof(int),
+                                      cudaMemcpyHostToDevice, stream));
+            CCSD_CUDA(cudaStreamSynchronize(stream));
+            run.launches.push_back(fl_l);
+            any_group = true;
+        }
+    }
+
     for (int L = 0; L <= maxlvl; L++) {
         std::vector<int> grp[4];
         for (int i = first; i < end; i++) {
-            if (level[i - first] != L) continue;
+            if (level[i - first] != L || in_fold[i - first]) continue;
             const int gi = p.steps[i].idx;
             const GemmStep& g = p.gemms[gi];
             if (groupable(g)) {
@@ -732,12 +841,64 @@ void Context::build_elementwise_run(Plan& p, RunSchedule& rs, int first, int end
     rs.runs.push_back(std::move(run));
 }
 
-void Context::launch(Plan& p, const GemmLaunch& l, const std::string& label) {
+// A run of dots (the energy and other scalars): one launch of per-chunk partial dots and
+// one fixed-order fold into the run's accumulator.
+void Context::build_dot_run(Plan& p, RunSchedule& rs, int first, int end) {
+    std::vector<kern::DotDesc> descs;
+    std::vector<int64_t> cs;
+    int64_t chunks = 0;
+    for (int i = first; i < end; i++) {
+        const DotStep& d = p.dots[p.steps[i].idx];
+        kern::DotDesc x;
+        x.A = tensor(d.tA).data + d.offA;
+        x.B = tensor(d.tB).data + d.offB;
+        x.ndim = d.ndim;
+        x.total = 1;
+        for (int k = 0; k < d.ndim; k++) {
+            x.len[k] = d.len[k];
+            x.sA[k] = d.sA[k];
+            x.sB[k] = d.sB[k];
+            x.total *= d.len[k];
+        }
+        x.alpha = d.alpha;
+        if (x.total <= 0) continue;
+        descs.push_back(x);
+        cs.push_back(chunks);
+        chunks += (x.total + kern::kBatchChunk - 1) / kern::kBatchChunk;
+    }
+    if (descs.size() < 2) return;
+    GemmLaunch l;
+    l.kind = GemmLaunch::DOT_BATCHED;
+    l.nprob = (int)descs.size();
+    l.chunks = chunks;
+    l.desc_bytes = descs.size() * sizeof(kern::DotDesc);
+    l.d_desc = dmalloc(l.desc_bytes);
+    l.d_chunks = (int64_t*)dmalloc(cs.size() * sizeof(int64_t));
+    l.d_part = (double*)dmalloc(chunks * sizeof(double));
+    l.part_elems = chunks;
+    CCSD_CUDA(cudaMemcpyAsync(l.d_desc, descs.data(), l.desc_bytes, cudaMemcpyHostToDevice, stream));
+    CCSD_CUDA(cudaMemcpyAsync(l.d_chunks, cs.data(), cs.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream));
+    CCSD_CUDA(cudaStreamSynchronize(stream));
+    GemmRun run;
+    run.first = first;
+    run.end = end;
+    run.launches.push_back(l);
+    rs.run_at[first] = (int)rs.runs.size();
+    rs.runs.push_back(std::move(run));
+}
+
+void Context::launch(Plan& p, const GemmLaunch& l, const std::string& label, double* dot_acc) {
     auto ev = profiling ? prof_begin() : std::make_pair((cudaEvent_t) nullptr, (cudaEvent_t) nullptr);
     switch (l.kind) {
         case GemmLaunch::GEMM: run_gemm(p, p.gemms[l.gemm]); break;
         case GemmLaunch::GEMM_GROUPED:
             kern::gemm_fp64_grouped(l.d_probs, l.d_tile_start, l.nprob, l.tiles, l.ak, l.bk, stream);
+            break;
+        case GemmLaunch::DOT_BATCHED:
+            kern::dot_batched((const kern::DotDesc*)l.d_desc, l.d_chunks, l.nprob, l.chunks, l.d_part, dot_acc, stream);
+            break;
+        case GemmLaunch::FOLD_GROUPS:
+            kern::fold_groups((const kern::FoldDesc*)l.d_desc, l.d_tile_start, l.ngroups, stream);
             break;
         case GemmLaunch::SUM_BATCHED:
             kern::sum_batched((const kern::SumDesc*)l.d_desc, l.d_chunks, l.nprob, l.chunks, stream);
@@ -763,9 +924,14 @@ void Context::run(Plan& p, double* scalar_out, double* dot_target) {
             switch (st.kind) {
                 case Step::GEMM: lab = p.gemms[st.idx].label.empty() ? "gemm" : p.gemms[st.idx].label; break;
                 case Step::SUM: lab = p.sums[st.idx].label.empty() ? "sum" : p.sums[st.idx].label; break;
+                case Step::DOT: lab = "dot"; break;
                 default: lab = p.scales[st.idx].label.empty() ? "scale" : p.scales[st.idx].label; break;
             }
-            for (auto& l : r.launches) launch(p, l, lab);
+            if (st.kind == Step::DOT && !zeroed) {
+                CCSD_CUDA(cudaMemsetAsync(d_scalar, 0, sizeof(double), stream));
+                zeroed = true;
+            }
+            for (auto& l : r.launches) launch(p, l, lab, acc);
             si = r.end - 1;
             continue;
         }

@@ -171,7 +171,7 @@ constexpr int kScratch = -1;
 // step, or one batched launch over several steps whose outputs are disjoint (GEMMs on the
 // grouped tiled-FP64 kernel, permuted sums, block scalings).
 struct GemmLaunch {
-    enum Kind { GEMM, GEMM_GROUPED, SUM, SUM_BATCHED, SCALE, SCALE_BATCHED };
+    enum Kind { GEMM, GEMM_GROUPED, FOLD_GROUPS, SUM, SUM_BATCHED, SCALE, SCALE_BATCHED, DOT_BATCHED };
     Kind kind = GEMM;
     int gemm = -1;                     // single GEMM: index into Plan::gemms
     int step = -1;                     // single SUM / SCALE: index into Plan::sums / scales
@@ -179,6 +179,9 @@ struct GemmLaunch {
     int nprob = 0, tiles = 0;
     kern::GemmArgs* d_probs = nullptr;
     int* d_tile_start = nullptr;
+    double* d_part = nullptr;          // shared-output group: partial products (part_elems doubles)
+    int64_t part_elems = 0;
+    int ngroups = 0;                   // fold: output blocks (d_desc: FoldDesc[nprob], d_tile_start: group starts)
     void* d_desc = nullptr;            // batched sums / scalings: descriptors
     int64_t* d_chunks = nullptr;       // ... and their first chunks
     size_t desc_bytes = 0;
@@ -310,7 +313,8 @@ public:
     RunSchedule& schedule(Plan& p);
     void build_run(Plan& p, RunSchedule& rs, int first, int end);
     void build_elementwise_run(Plan& p, RunSchedule& rs, int first, int end);
-    void launch(Plan& p, const GemmLaunch& l, const std::string& label);
+    void build_dot_run(Plan& p, RunSchedule& rs, int first, int end);
+    void launch(Plan& p, const GemmLaunch& l, const std::string& label, double* dot_acc = nullptr);
     std::vector<int> constant_tensors;  // handles whose contents never change (sliced once)
     bool is_constant(int h) const;
 };

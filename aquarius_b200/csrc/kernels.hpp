@@ -30,7 +30,23 @@ struct GemmArgs {
     // kernels' address path (the tables stay valid for the other users)
     bool ak_affine = false, bk_affine = false;
     int64_t ak0 = 0, ak_step = 0, bk0 = 0, bk_step = 0;
+    // grouped launches with shared outputs: write the raw product to ws[m][n] (no alpha,
+    // no scatter); a fold applies it to C
+    bool partial_out = false;
 };
+
+// Fold of dense partial products into C: C[Cm[m] + Cn[n]] += scale * part[m*N + n], the
+// problems of one output block in order (one destination per element).
+struct FoldDesc {
+    const double* part = nullptr;
+    double* C = nullptr;
+    const int64_t* Cm = nullptr;
+    const int64_t* Cn = nullptr;
+    int M = 0, N = 0;
+    double scale = 0;
+};
+// one CTA per group: problems [group_start[g], group_start[g + 1]) of d, in order
+void fold_groups(const FoldDesc* d, const int* group_start, int ngroups, cudaStream_t s);
 
 // K-ranges the FP64 GEMM splits a contraction into (1 = none); ws needs ksplit*M*N doubles
 int fp64_ksplit(int M, int N, int K, bool skinny_ok = true);
@@ -174,6 +190,31 @@ struct TauArgs {
     int64_t len[4] = {0, 0, 0, 0};
 };
 void tau_block(const TauArgs& a, cudaStream_t s);
+// every block of Tau in one launch: chunks of kBatchChunk elements, chunk_start[p] the
+// first chunk of block p (device arrays)
+void tau_batched(const TauArgs* d, const int64_t* chunk_start, int n, int64_t chunks, cudaStream_t s);
+
+// Jacobi update of many blocks in one launch: z = z / den, t += z, red_max = max |z|
+struct UpdateDesc {
+    double* Z = nullptr;
+    double* T = nullptr;
+    WeightArgs w;
+};
+void update_batched(const UpdateDesc* d, const int64_t* chunk_start, int n, int64_t chunks, double* red_max,
+                    cudaStream_t s);
+
+// Dots of many strided blocks in one launch: part[c] = partial sum of chunk c, then one
+// CTA adds sum_c part[c] (fixed order) to out[0]
+struct DotDesc {
+    const double* A = nullptr;
+    const double* B = nullptr;
+    int ndim = 0;
+    int64_t len[8], sA[8], sB[8];
+    int64_t total = 0;
+    double alpha = 0;
+};
+void dot_batched(const DotDesc* d, const int64_t* chunk_start, int n, int64_t chunks, double* part, double* out,
+                 cudaStream_t s);
 
 // Gather of a dense spatial (pq|rs) array (n^4, last index fastest) into a block:
 //   C[off + sum_p st[p] x_p] += sign * eri[((g0 n + g1) n + g2) n + g3],

@@ -169,8 +169,9 @@ __device__ __forceinline__ void fp64_tile(const GemmArgs& g, const int m0, const
     }
     cp_wait<0>();
 
-    if (nz > 1) {
-        // split-K: raw partial sums, folded by splitk_fold_kernel
+    if (nz > 1 || g.partial_out) {
+        // split-K (or a shared-output group): raw partial sums, folded by splitk_fold_kernel
+        // (fold_groups_kernel)
         double* wz = g.ws + (int64_t)kz * g.M * g.N;
 #pragma unroll
         for (int i = 0; i < 4; i++) {
@@ -265,6 +266,21 @@ __global__ void __launch_bounds__(THREADS, 1)
     const int local = t - tile_start[sp];
     const int tn = (sg.N + BN - 1) / BN;
     fp64_tile<AK, BKc>(sg, (local / tn) * BM, (local % tn) * BN, 0, 1, smem_raw);
+}
+
+// shared-output groups: each CTA folds the partial products of one output block, its
+// problems one after another (fixed order; one destination per element)
+__global__ void fold_groups_kernel(const FoldDesc* __restrict__ d, const int* __restrict__ gstart) {
+    const int g = blockIdx.x;
+    for (int p = gstart[g]; p < gstart[g + 1]; p++) {
+        const FoldDesc f = d[p];
+        const int64_t mn = (int64_t)f.M * f.N;
+        for (int64_t l = threadIdx.x; l < mn; l += blockDim.x) {
+            const int m = (int)(l / f.N), n = (int)(l % f.N);
+            f.C[f.Cm[m] + f.Cn[n]] += f.scale * f.part[l];
+        }
+        __syncthreads();
+    }
 }
 
 // fold split-K partials in a fixed order and scatter alpha * sum into every variant
@@ -626,6 +642,12 @@ void gemm_fp64_grouped(const GemmArgs* probs, const int* tile_start, int nprob, 
     COUNT_LAUNCH();
 }
 
+void fold_groups(const FoldDesc* d, const int* group_start, int ngroups, cudaStream_t s) {
+    if (ngroups <= 0) return;
+    fold_groups_kernel<<<ngroups, 256, 0, s>>>(d, group_start);
+    COUNT_LAUNCH();
+}
+
 // ---------------------------------------------------------------------------
 // elementwise and reductions
 // ---------------------------------------------------------------------------
@@ -899,11 +921,112 @@ __global__ void __launch_bounds__(256) scale_batched_kernel(const ScaleDesc* __r
     }
 }
 
+// Tau of one chunk of one block (tau_kernel's arithmetic)
+__global__ void __launch_bounds__(256) tau_batched_kernel(const TauArgs* __restrict__ d, const int64_t* __restrict__ cs,
+                                                          int n) {
+    __shared__ int sp;
+    const int64_t c = blockIdx.x;
+    if (threadIdx.x == 0) sp = find_problem(cs, n, c);
+    __syncthreads();
+    const TauArgs& a = d[sp];
+    const int64_t la = a.len[0], lb = a.len[1], li = a.len[2], lj = a.len[3];
+    const int64_t total = la * lb * li * lj;
+    const int64_t base = (c - cs[sp]) * kBatchChunk;
+    for (int i = threadIdx.x; i < kBatchChunk; i += blockDim.x) {
+        const int64_t l = base + i;
+        if (l >= total) break;
+        int64_t r = l;
+        const int64_t x = r % la;
+        r /= la;
+        const int64_t y = r % lb;
+        r /= lb;
+        const int64_t ii = r % li;
+        const int64_t j = r / li;
+        double v = a.t2[l];
+        if (a.t1ai) v += a.t1ai[x + la * ii] * a.t1bj[y + lb * j];
+        if (a.t1aj) v -= a.t1aj[x + la * j] * a.t1bi[y + lb * ii];
+        a.tau[l] = v;
+    }
+}
+
+// Jacobi update of one chunk of one block; the residual max goes to red_max through an
+// atomic max on the bits of non-negative doubles (order-independent)
+__global__ void __launch_bounds__(256) update_batched_kernel(const UpdateDesc* __restrict__ d,
+                                                             const int64_t* __restrict__ cs, int n, double* red_max) {
+    __shared__ int sp;
+    const int64_t c = blockIdx.x;
+    if (threadIdx.x == 0) sp = find_problem(cs, n, c);
+    __syncthreads();
+    const UpdateDesc& D = d[sp];
+    const int64_t base = (c - cs[sp]) * kBatchChunk;
+    double mx = 0;
+    for (int i = threadIdx.x; i < kBatchChunk; i += blockDim.x) {
+        const int64_t l = base + i;
+        if (l >= D.w.total) break;
+        const double den = den_of(D.w, l);
+        const double z = fabs(den) < 1e-4 ? 0.0 : D.Z[l] / den;
+        D.Z[l] = z;
+        D.T[l] += z;
+        mx = fmax(mx, fabs(z));
+    }
+    mx = block_max(mx);
+    if (threadIdx.x == 0 && mx > 0.0)
+        atomicMax(reinterpret_cast<unsigned long long*>(red_max), (unsigned long long)__double_as_longlong(mx));
+}
+
+// dot of one chunk of one block into part[c]
+__global__ void __launch_bounds__(256) dot_batched_kernel(const DotDesc* __restrict__ d, const int64_t* __restrict__ cs,
+                                                          int n, double* part) {
+    __shared__ int sp;
+    const int64_t c = blockIdx.x;
+    if (threadIdx.x == 0) sp = find_problem(cs, n, c);
+    __syncthreads();
+    const DotDesc& D = d[sp];
+    const int64_t base = (c - cs[sp]) * kBatchChunk;
+    double acc = 0;
+    for (int i = threadIdx.x; i < kBatchChunk; i += blockDim.x) {
+        const int64_t l = base + i;
+        if (l >= D.total) break;
+        int64_t r = l, oa = 0, ob = 0;
+        for (int k = 0; k < D.ndim; k++) {
+            const int64_t x = r % D.len[k];
+            r /= D.len[k];
+            oa += x * D.sA[k];
+            ob += x * D.sB[k];
+        }
+        acc += D.A[oa] * D.B[ob];
+    }
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) part[c] = D.alpha * acc;
+}
+
 }  // namespace
 
 void sum_batched(const SumDesc* d, const int64_t* chunk_start, int n, int64_t chunks, cudaStream_t s) {
     if (n <= 0 || chunks <= 0) return;
     sum_batched_kernel<<<(unsigned)chunks, 256, 0, s>>>(d, chunk_start, n);
+    COUNT_LAUNCH();
+}
+
+void tau_batched(const TauArgs* d, const int64_t* chunk_start, int n, int64_t chunks, cudaStream_t s) {
+    if (n <= 0 || chunks <= 0) return;
+    tau_batched_kernel<<<(unsigned)chunks, 256, 0, s>>>(d, chunk_start, n);
+    COUNT_LAUNCH();
+}
+
+void update_batched(const UpdateDesc* d, const int64_t* chunk_start, int n, int64_t chunks, double* red_max,
+                    cudaStream_t s) {
+    if (n <= 0 || chunks <= 0) return;
+    update_batched_kernel<<<(unsigned)chunks, 256, 0, s>>>(d, chunk_start, n, red_max);
+    COUNT_LAUNCH();
+}
+
+void dot_batched(const DotDesc* d, const int64_t* chunk_start, int n, int64_t chunks, double* part, double* out,
+                 cudaStream_t s) {
+    if (n <= 0 || chunks <= 0) return;
+    dot_batched_kernel<<<(unsigned)chunks, 256, 0, s>>>(d, chunk_start, n, part);
+    fold_sum_kernel<<<1, 1024, 0, s>>>(part, (int)chunks, 1.0, out);
+    COUNT_LAUNCH();
     COUNT_LAUNCH();
 }
 

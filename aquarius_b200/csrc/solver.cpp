@@ -165,6 +165,7 @@ void Solver::setup() {
     record_tau(tau_plan);
     record_energy(energy_plan);
     build_tau_blocks();
+    build_update();
     launch_tau();
     CCSD_CUDA(cudaMemsetAsync(d_red, 0, sizeof(double), ctx.stream));
     ctx.run(energy_plan, nullptr, d_red + 0);
@@ -311,10 +312,56 @@ void Solver::build_tau_blocks() {
             tau_blocks.push_back(a);
         }
     }
+    // descriptors of the one-launch form
+    std::vector<int64_t> cs;
+    tau_chunks = 0;
+    for (auto& a : tau_blocks) {
+        cs.push_back(tau_chunks);
+        tau_chunks += (a.len[0] * a.len[1] * a.len[2] * a.len[3] + kern::kBatchChunk - 1) / kern::kBatchChunk;
+    }
+    if (tau_blocks.size() > 1) {
+        d_tau = (kern::TauArgs*)alloc(tau_blocks.size() * sizeof(kern::TauArgs));
+        d_tau_cs = (int64_t*)alloc(cs.size() * sizeof(int64_t));
+        CCSD_CUDA(cudaMemcpyAsync(d_tau, tau_blocks.data(), tau_blocks.size() * sizeof(kern::TauArgs),
+                                  cudaMemcpyHostToDevice, ctx.stream));
+        CCSD_CUDA(cudaMemcpyAsync(d_tau_cs, cs.data(), cs.size() * sizeof(int64_t), cudaMemcpyHostToDevice, ctx.stream));
+        CCSD_CUDA(cudaStreamSynchronize(ctx.stream));   // the host arrays go out of scope
+    }
 }
 
 void Solver::launch_tau() {
-    for (auto& a : tau_blocks) kern::tau_block(a, ctx.stream);
+    if (d_tau) kern::tau_batched(d_tau, d_tau_cs, (int)tau_blocks.size(), tau_chunks, ctx.stream);
+    else
+        for (auto& a : tau_blocks) kern::tau_block(a, ctx.stream);
+}
+
+// Z.weight(D); T += Z; conv = Z.norm(00) over every block of Z1 and Z2, one launch
+void Solver::build_update() {
+    std::vector<kern::UpdateDesc> descs;
+    std::vector<int64_t> cs;
+    upd_chunks = 0;
+    for (int pair = 0; pair < 2; pair++) {
+        Tensor& Z = ctx.tensor(pair == 0 ? Z1 : Z2);
+        Tensor& T = ctx.tensor(pair == 0 ? T1 : T2);
+        for (size_t c = 0; c < Z.cases.size(); c++)
+            for (auto& b : Z.cases[c].blocks) {
+                if (b.size == 0) continue;
+                kern::UpdateDesc u;
+                u.Z = Z.data + b.offset;
+                u.T = T.data + b.offset;
+                u.w = weight_args(Z, (int)c, b);
+                descs.push_back(u);
+                cs.push_back(upd_chunks);
+                upd_chunks += (b.size + kern::kBatchChunk - 1) / kern::kBatchChunk;
+            }
+    }
+    n_upd = (int)descs.size();
+    d_upd = (kern::UpdateDesc*)alloc(std::max<size_t>(descs.size(), 1) * sizeof(kern::UpdateDesc));
+    d_upd_cs = (int64_t*)alloc(std::max<size_t>(cs.size(), 1) * sizeof(int64_t));
+    CCSD_CUDA(cudaMemcpyAsync(d_upd, descs.data(), descs.size() * sizeof(kern::UpdateDesc), cudaMemcpyHostToDevice,
+                              ctx.stream));
+    CCSD_CUDA(cudaMemcpyAsync(d_upd_cs, cs.data(), cs.size() * sizeof(int64_t), cudaMemcpyHostToDevice, ctx.stream));
+    CCSD_CUDA(cudaStreamSynchronize(ctx.stream));   // the host arrays go out of scope
 }
 
 void Solver::record_tau(Plan& p) {
@@ -554,17 +601,9 @@ void Solver::launch_iteration() {
     // contractions (ccsd.cxx:123-180)
     launch_tau();
     ctx.run(iter_plan);
-    // Z.weight(D); T += Z; conv = Z.norm(00)  (ccsd.cxx:184-185,190), fused
+    // Z.weight(D); T += Z; conv = Z.norm(00)  (ccsd.cxx:184-185,190), fused, one launch
     CCSD_CUDA(cudaMemsetAsync(d_red, 0, 2 * sizeof(double), s));
-    for (int pair = 0; pair < 2; pair++) {
-        Tensor& Z = ctx.tensor(pair == 0 ? Z1 : Z2);
-        Tensor& T = ctx.tensor(pair == 0 ? T1 : T2);
-        for (size_t c = 0; c < Z.cases.size(); c++)
-            for (auto& b : Z.cases[c].blocks) {
-                if (b.size == 0) continue;
-                kern::update_block(Z.data + b.offset, T.data + b.offset, weight_args(Z, (int)c, b), d_red + 1, s);
-            }
-    }
+    kern::update_batched(d_upd, d_upd_cs, n_upd, upd_chunks, d_red + 1, s);
     // Tau from the updated T, energy (ccsd.cxx:187-189)
     launch_tau();
     ctx.run(energy_plan, nullptr, d_red + 0);

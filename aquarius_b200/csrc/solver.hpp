@@ -46,6 +46,14 @@ public:
     bool refined = false;           // moved to a more accurate contraction mode (refine_tol reached)
     std::vector<double> conv_hist;  // residuals since the last mode switch (stall detection)
     std::vector<kern::TauArgs> tau_blocks;
+    // one-launch Tau and Jacobi update over all blocks: device descriptors and chunk starts
+    kern::TauArgs* d_tau = nullptr;
+    int64_t* d_tau_cs = nullptr;
+    int64_t tau_chunks = 0;
+    kern::UpdateDesc* d_upd = nullptr;
+    int64_t* d_upd_cs = nullptr;
+    int64_t upd_chunks = 0;
+    int n_upd = 0;
 
     int iterations = 0;
     double energy = 0, conv = 0, mp2 = 0;
@@ -73,6 +81,7 @@ private:
     void record_tau(Plan& p);
     void build_tau_blocks();
     void launch_tau();
+    void build_update();
     void record_energy(Plan& p);
     void record_iteration();
     void record_iteration_rhf();
