@@ -302,7 +302,7 @@ def run_kernel(args):
     ctx = A.Context(0, stream.cuda_stream)
     ctx.set_spaces(vrt=[w["v"]], occ=[w["o"]])
     if args.precision in ("split", "split_i8"):
-        ctx.set_precision(args.precision)
+        ctx.set_precision(args.precision, slices=args.slices)
     V = ctx.tensor("A", *sa, packed=packed)
     T = ctx.tensor("B", *sb)
     Z = ctx.tensor("C", *sc)
