@@ -801,9 +801,10 @@ void Context::build_elementwise_run(Plan& p, RunSchedule& rs, int first, int end
                     x.total *= s.len[q];
                 }
                 if (x.total <= 0) continue;
+                kern::sum_plan_tiles(x);
                 d.push_back(x);
                 cs.push_back(chunks);
-                chunks += nchunks(x.total);
+                chunks += kern::sum_chunks(x);
             }
             if (d.empty()) continue;
             l.desc_bytes = d.size() * sizeof(kern::SumDesc);

@@ -249,7 +249,18 @@ struct SumDesc {
     int ndim = 0;
     int64_t len[8], sA[8], sC[8];
     int64_t total = 0;
+    // permuted sums whose fastest A and C positions differ go through 32 x 32 shared-memory
+    // tiles over those two positions (coalesced reads of A and writes of C); a chunk is
+    // two tiles
+    int tiled = 0, p0 = 0, pc = 0;
+    int64_t ntiles = 0;
 };
+// chunks of kBatchChunk elements (or two 32 x 32 tiles) a sum descriptor takes
+inline int64_t sum_chunks(const SumDesc& d) {
+    return d.tiled ? (d.ntiles + 1) / 2 : (d.total + kBatchChunk - 1) / kBatchChunk;
+}
+// fill the tiling fields of a descriptor (after len / sA / sC / total)
+void sum_plan_tiles(SumDesc& d);
 struct ScaleDesc {
     double* X = nullptr;
     int64_t n = 0;

@@ -887,10 +887,49 @@ __device__ __forceinline__ int find_problem(const int64_t* __restrict__ cs, int 
 __global__ void __launch_bounds__(256) sum_batched_kernel(const SumDesc* __restrict__ d, const int64_t* __restrict__ cs,
                                                           int n) {
     __shared__ int sp;
+    __shared__ double tile[32][33];
     const int64_t c = blockIdx.x;
     if (threadIdx.x == 0) sp = find_problem(cs, n, c);
     __syncthreads();
     const SumDesc& D = d[sp];
+    if (D.tiled) {
+        // two 32 x 32 tiles over (p0, pc): read along p0 (A-contiguous), write along pc
+        const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8 threads
+        const int64_t l0 = D.len[D.p0], lc = D.len[D.pc];
+        const int64_t t0n = (l0 + 31) / 32, tcn = (lc + 31) / 32;
+        for (int tt = 0; tt < 2; tt++) {
+            const int64_t t = (c - cs[sp]) * 2 + tt;
+            if (t >= D.ntiles) break;   // uniform across the CTA
+            int64_t r = t;
+            const int64_t t0 = r % t0n;
+            r /= t0n;
+            const int64_t tc = r % tcn;
+            r /= tcn;
+            int64_t oa = 0, oc = 0;
+            for (int k = 0; k < D.ndim; k++) {
+                if (k == D.p0 || k == D.pc) continue;
+                const int64_t x = r % D.len[k];
+                r /= D.len[k];
+                oa += x * D.sA[k];
+                oc += x * D.sC[k];
+            }
+            const int64_t x0 = t0 * 32 + tx;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int64_t xc = tc * 32 + ty + 8 * q;
+                tile[ty + 8 * q][tx] = (x0 < l0 && xc < lc) ? D.A[oa + x0 * D.sA[D.p0] + xc * D.sA[D.pc]] : 0.0;
+            }
+            __syncthreads();
+            const int64_t xc = tc * 32 + tx;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                const int64_t y0 = t0 * 32 + ty + 8 * q;
+                if (y0 < l0 && xc < lc) D.C[oc + y0 * D.sC[D.p0] + xc * D.sC[D.pc]] += D.alpha * tile[tx][ty + 8 * q];
+            }
+            __syncthreads();
+        }
+        return;
+    }
     const int64_t base = (c - cs[sp]) * kBatchChunk;
     for (int i = threadIdx.x; i < kBatchChunk; i += blockDim.x) {
         const int64_t l = base + i;
@@ -1001,6 +1040,23 @@ __global__ void __launch_bounds__(256) dot_batched_kernel(const DotDesc* __restr
 }
 
 }  // namespace
+
+void sum_plan_tiles(SumDesc& d) {
+    d.tiled = 0;
+    if (d.ndim < 2) return;
+    int p0 = 0, pc = 0;
+    for (int k = 1; k < d.ndim; k++) {
+        if (d.sA[k] < d.sA[p0]) p0 = k;
+        if (d.sC[k] < d.sC[pc]) pc = k;
+    }
+    if (p0 == pc || d.len[p0] < 8 || d.len[pc] < 8) return;
+    d.tiled = 1;
+    d.p0 = p0;
+    d.pc = pc;
+    d.ntiles = ((d.len[p0] + 31) / 32) * ((d.len[pc] + 31) / 32);
+    for (int k = 0; k < d.ndim; k++)
+        if (k != p0 && k != pc) d.ntiles *= d.len[k];
+}
 
 void sum_batched(const SumDesc* d, const int64_t* chunk_start, int n, int64_t chunks, cudaStream_t s) {
     if (n <= 0 || chunks <= 0) return;
