@@ -51,7 +51,7 @@ EXPORTS = [
     "ccsd_server_options_default", "ccsd_server_create", "ccsd_server_submit_synthetic", "ccsd_server_submit_factor",
     "ccsd_server_poll", "ccsd_server_wait", "ccsd_server_stats", "ccsd_server_destroy", "ccsd_solver_mode",
     "ccsd_rhf_hamiltonian_from_factor", "ccsd_rhf_hamiltonian_from_integrals", "ccsd_rhf_hamiltonian_destroy",
-    "ccsd_rhf_solver_create", "ccsd_rhf_plan_query",
+    "ccsd_rhf_solver_create", "ccsd_rhf_plan_query", "ccsd_hamiltonian_from_ao", "ccsd_rhf_hamiltonian_from_ao",
 ]
 
 
@@ -182,6 +182,10 @@ def lib():
             "ccsd_rhf_hamiltonian_from_integrals": [vp, ctypes.c_int, vp, vp, P(RHFHamiltonian)],
             "ccsd_rhf_hamiltonian_destroy": [vp, P(RHFHamiltonian)],
             "ccsd_rhf_solver_create": [vp, P(RHFHamiltonian), P(Options), P(vp)],
+            "ccsd_hamiltonian_from_ao": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp, ctypes.c_int,
+                                         P(Hamiltonian), P(dbl)],
+            "ccsd_rhf_hamiltonian_from_ao": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp,
+                                             P(RHFHamiltonian), P(dbl)],
             "ccsd_dot_batch_noalloc": [vp, vp, vp, ctypes.c_int, i64, vp],
             "ccsd_synth_irreps": [ctypes.c_uint64, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp],
             "ccsd_synth_problem": [ctypes.c_uint64, ctypes.c_int, vp, vp, vp, vp, vp],
@@ -668,6 +672,37 @@ class Context:
         H = RHFHamiltonian()
         _check(lib().ccsd_rhf_hamiltonian_from_integrals(self.c, n, _ptr(fock), _ptr(eri), ctypes.byref(H)), self.c)
         return RHFHamiltonianHandle(self, H)
+
+    def _ao_args(self, hcore, eri_ao, C, nocc):
+        hcore = np.ascontiguousarray(hcore, dtype=np.float64)
+        eri_ao = np.ascontiguousarray(eri_ao, dtype=np.float64)
+        C = np.ascontiguousarray(C, dtype=np.float64)
+        nao, nmo = C.shape
+        if hcore.shape != (nao, nao) or eri_ao.shape != (nao, nao, nao, nao):
+            raise ValueError("hcore must be (nao, nao), eri_ao (nao,)*4 and C (nao, nmo)")
+        self.nirrep = 1
+        self._counts = {(0, 0): _ints([nmo - nocc]), (0, 1): _ints([nmo - nocc]), (1, 0): _ints([nocc]),
+                        (1, 1): _ints([nocc])}
+        return hcore, eri_ao, C, nao, nmo
+
+    def hamiltonian_from_ao(self, hcore, eri_ao, C, nocc, pack_vvvv=True):
+        """Closed-shell H from AO quantities; the MO integrals are formed on the device.
+        Returns (handle, SCF electronic energy of C)."""
+        hcore, eri_ao, C, nao, nmo = self._ao_args(hcore, eri_ao, C, nocc)
+        H = Hamiltonian()
+        e = ctypes.c_double()
+        _check(lib().ccsd_hamiltonian_from_ao(self.c, nao, nmo, nocc, _ptr(hcore), _ptr(eri_ao), _ptr(C),
+                                              1 if pack_vvvv else 0, ctypes.byref(H), ctypes.byref(e)), self.c)
+        return HamiltonianHandle(self, H, pack_vvvv), e.value
+
+    def rhf_hamiltonian_from_ao(self, hcore, eri_ao, C, nocc):
+        """Closed-shell spatial blocks from AO quantities (MO integrals formed on the device)."""
+        hcore, eri_ao, C, nao, nmo = self._ao_args(hcore, eri_ao, C, nocc)
+        H = RHFHamiltonian()
+        e = ctypes.c_double()
+        _check(lib().ccsd_rhf_hamiltonian_from_ao(self.c, nao, nmo, nocc, _ptr(hcore), _ptr(eri_ao), _ptr(C),
+                                                  ctypes.byref(H), ctypes.byref(e)), self.c)
+        return RHFHamiltonianHandle(self, H), e.value
 
     def solver(self, H, **kw):
         return Solver(self, H, **kw)

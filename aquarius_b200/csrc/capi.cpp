@@ -624,6 +624,67 @@ int ccsd_hamiltonian_from_fcidump(ccsd_ctx ctx, const char* path, int flags, int
     });
 }
 
+namespace {
+// C1 closed-shell spaces for nocc of nmo orbitals on a context without tensors (or check them)
+void set_closed_shell_spaces(ccsd_ctx ctx, Context* c, int nmo, int nocc) {
+    const int nv = nmo - nocc;
+    if (!c->tensors.empty() || c->spaces_set) {
+        const Spaces& S = c->spaces;
+        bool same = c->spaces_set && S.nirrep == 1;
+        for (int s = 0; s < 2 && same; s++) same = S.n[VRT][s][0] == nv && S.n[OCC][s][0] == nocc;
+        if (!same) throw Error(CCSD_ERR_ARG, "context spaces differ from the AO problem's (C1, nocc, nmo - nocc)");
+        return;
+    }
+    int v[1] = {nv}, o[1] = {nocc};
+    const int st = ccsd_ctx_set_spaces(ctx, 1, v, v, o, o);
+    if (st != CCSD_OK) throw Error(st, "setting the AO problem's spaces failed");
+}
+
+// device MO integrals of an AO problem, freed with the object
+struct MoIntegrals {
+    Context& c;
+    double* d = nullptr;
+    int64_t bytes = 0;
+    std::vector<double> fock;
+    double e = 0;
+    MoIntegrals(Context& ctx, int nao, int nmo, int nocc, const double* hcore, const double* eri, const double* C)
+        : c(ctx) {
+        bytes = (int64_t)nmo * nmo * nmo * nmo * (int64_t)sizeof(double);
+        d = (double*)c.dmalloc(bytes);
+        fock.resize((size_t)nmo * nmo);
+        e = ao_to_mo(c, nao, nmo, nocc, hcore, eri, C, d, fock.data());
+    }
+    ~MoIntegrals() {
+        cudaStreamSynchronize(c.stream);
+        c.dfree(d, bytes);
+    }
+};
+}  // namespace
+
+int ccsd_hamiltonian_from_ao(ccsd_ctx ctx, int nao, int nmo, int nocc, const double* hcore, const double* eri_ao,
+                             const double* C, int pack_vvvv, ccsd_hamiltonian* H, double* e_elec) {
+    return guarded(ctx, [&] {
+        if (!hcore || !eri_ao || !C || !H) throw Error(CCSD_ERR_ARG, "bad AO arguments");
+        Context* c = from_handle(ctx);
+        set_closed_shell_spaces(ctx, c, nmo, nocc);
+        MoIntegrals mo(*c, nao, nmo, nocc, hcore, eri_ao, C);
+        build_hamiltonian_device(*c, nmo, mo.fock.data(), mo.d, pack_vvvv != 0, H);
+        if (e_elec) *e_elec = mo.e;
+    });
+}
+
+int ccsd_rhf_hamiltonian_from_ao(ccsd_ctx ctx, int nao, int nmo, int nocc, const double* hcore,
+                                 const double* eri_ao, const double* C, ccsd_rhf_hamiltonian* H, double* e_elec) {
+    return guarded(ctx, [&] {
+        if (!hcore || !eri_ao || !C || !H) throw Error(CCSD_ERR_ARG, "bad AO arguments");
+        Context* c = from_handle(ctx);
+        set_closed_shell_spaces(ctx, c, nmo, nocc);
+        MoIntegrals mo(*c, nao, nmo, nocc, hcore, eri_ao, C);
+        build_rhf_hamiltonian_device(*c, nmo, mo.fock.data(), mo.d, H);
+        if (e_elec) *e_elec = mo.e;
+    });
+}
+
 int ccsd_hamiltonian_destroy(ccsd_ctx ctx, ccsd_hamiltonian* H) {
     return guarded(ctx, [&] {
         Context* c = from_handle(ctx);

@@ -373,29 +373,44 @@ void build_rhf_hamiltonian(Context& ctx, int naux, const double* B, const double
     ctx.dfree(bld.dB, nB * sizeof(double));
 }
 
-void build_rhf_hamiltonian_dense(Context& ctx, int n, const double* fock, const double* eri, ccsd_rhf_hamiltonian* H) {
+void build_rhf_hamiltonian_device(Context& ctx, int n, const double* fock, const double* d_eri,
+                                  ccsd_rhf_hamiltonian* H) {
     const Spaces& S = ctx.spaces;
     require_closed_shell(S, "the RHF builder");
     if (n != S.total(VRT, ALPHA) + S.total(OCC, ALPHA))
         throw Error(CCSD_ERR_ARG, "orbital count differs from the context's spaces");
-    const int64_t ne = (int64_t)n * n * n * n;
     Builder bld{ctx, n, 0, S.total(OCC, ALPHA)};
-    double* d = (double*)ctx.dmalloc(ne * sizeof(double));
-    struct Free {
-        Context& c;
-        double* p;
-        int64_t b;
-        ~Free() {
-            cudaStreamSynchronize(c.stream);
-            c.dfree(p, b);
-        }
-    } guard{ctx, d, ne * (int64_t)sizeof(double)};
-    CCSD_CUDA(cudaMemcpyAsync(d, eri, ne * sizeof(double), cudaMemcpyHostToDevice, ctx.stream));
-    bld.dEri = d;
+    bld.dEri = d_eri;
     create_rhf_hamiltonian_tensors(ctx, H);
     for (int h : {H->fAI, H->fAB, H->fIJ}) bld.one_electron_full(h, fock);
     fill_rhf_two_electron(bld, H);
     CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+namespace {
+// a dense (pq|rs) copied to the device for the lifetime of a build
+struct DeviceEri {
+    Context& c;
+    double* p = nullptr;
+    int64_t bytes = 0;
+    DeviceEri(Context& ctx, int n, const double* eri) : c(ctx) {
+        const int64_t ne = (int64_t)n * n * n * n;
+        bytes = ne * (int64_t)sizeof(double);
+        p = (double*)c.dmalloc(bytes);
+        CCSD_CUDA(cudaMemcpyAsync(p, eri, bytes, cudaMemcpyHostToDevice, c.stream));
+    }
+    ~DeviceEri() {
+        cudaStreamSynchronize(c.stream);
+        c.dfree(p, bytes);
+    }
+};
+}  // namespace
+
+void build_rhf_hamiltonian_dense(Context& ctx, int n, const double* fock, const double* eri, ccsd_rhf_hamiltonian* H) {
+    if (n != ctx.spaces.total(VRT, ALPHA) + ctx.spaces.total(OCC, ALPHA))
+        throw Error(CCSD_ERR_ARG, "orbital count differs from the context's spaces");
+    DeviceEri d(ctx, n, eri);
+    build_rhf_hamiltonian_device(ctx, n, fock, d.p, H);
 }
 
 void build_hamiltonian(Context& ctx, int naux, const double* B, const double* eps, const int* aux_per_irrep,
@@ -425,8 +440,8 @@ void build_hamiltonian(Context& ctx, int naux, const double* B, const double* ep
     ctx.dfree(bld.dB, nB * sizeof(double));
 }
 
-void build_hamiltonian_dense(Context& ctx, int n, const double* fock, const double* eri, bool pack_vvvv,
-                             ccsd_hamiltonian* H) {
+void build_hamiltonian_device(Context& ctx, int n, const double* fock, const double* d_eri, bool pack_vvvv,
+                              ccsd_hamiltonian* H) {
     const Spaces& S = ctx.spaces;
     for (int h = 0; h < S.nirrep; h++)
         for (int sp = 0; sp < 2; sp++)
@@ -434,24 +449,20 @@ void build_hamiltonian_dense(Context& ctx, int n, const double* fock, const doub
                 throw Error(CCSD_ERR_ARG, "the dense-integral builder needs a closed-shell (alpha = beta) space");
     if (n != S.total(VRT, ALPHA) + S.total(OCC, ALPHA))
         throw Error(CCSD_ERR_ARG, "orbital count differs from the context's spaces");
-    const int64_t ne = (int64_t)n * n * n * n;
     Builder bld{ctx, n, 0, S.total(OCC, ALPHA)};
-    double* d = (double*)ctx.dmalloc(ne * sizeof(double));
-    struct Free {
-        Context& c;
-        double* p;
-        int64_t b;
-        ~Free() {
-            cudaStreamSynchronize(c.stream);
-            c.dfree(p, b);
-        }
-    } guard{ctx, d, ne * (int64_t)sizeof(double)};
-    CCSD_CUDA(cudaMemcpyAsync(d, eri, ne * sizeof(double), cudaMemcpyHostToDevice, ctx.stream));
-    bld.dEri = d;
+    bld.dEri = d_eri;
     create_hamiltonian_tensors(ctx, pack_vvvv, H);
     for (int h : {H->fAI, H->fME, H->fAE, H->fMI}) bld.one_electron_full(h, fock);
     for (int h : {H->VMNIJ, H->VAMIJ, H->VMNEF, H->VAMEI, H->VAMEF, H->VABEF}) bld.two_electron(h);
     CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+void build_hamiltonian_dense(Context& ctx, int n, const double* fock, const double* eri, bool pack_vvvv,
+                             ccsd_hamiltonian* H) {
+    if (n != ctx.spaces.total(VRT, ALPHA) + ctx.spaces.total(OCC, ALPHA))
+        throw Error(CCSD_ERR_ARG, "orbital count differs from the context's spaces");
+    DeviceEri d(ctx, n, eri);
+    build_hamiltonian_device(ctx, n, fock, d.p, pack_vvvv, H);
 }
 
 }  // namespace ccsd

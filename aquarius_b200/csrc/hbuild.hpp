@@ -18,6 +18,16 @@ void create_rhf_hamiltonian_tensors(Context& ctx, ccsd_rhf_hamiltonian* H);
 void build_rhf_hamiltonian(Context& ctx, int naux, const double* B, const double* eps, const int* aux_per_irrep,
                            ccsd_rhf_hamiltonian* H);
 void build_rhf_hamiltonian_dense(Context& ctx, int n, const double* fock, const double* eri, ccsd_rhf_hamiltonian* H);
+// the same from a (pq|rs) array already on the device (host Fock matrix)
+void build_hamiltonian_device(Context& ctx, int n, const double* fock, const double* d_eri, bool pack_vvvv,
+                              ccsd_hamiltonian* H);
+void build_rhf_hamiltonian_device(Context& ctx, int n, const double* fock, const double* d_eri,
+                                  ccsd_rhf_hamiltonian* H);
+// AO -> MO on the device for a closed-shell reference: d_mo[p,q,r,s] = (pq|rs) over the
+// nmo columns of C (nao x nmo, row-major), the MO Fock matrix f = C^T h C + sum_i 2(pq|ii)
+// - (pi|iq) over the first nocc orbitals (host, nmo x nmo); returns sum_i (h_ii + f_ii)
+double ao_to_mo(Context& ctx, int nao, int nmo, int nocc, const double* hcore, const double* eri_ao,
+                const double* C, double* d_mo, double* fock);
 
 // FCIDUMP contents: h[n*n], eri[n^4] dense, core energy
 struct Fcidump {

@@ -190,6 +190,9 @@ struct TauArgs {
     int64_t len[4] = {0, 0, 0, 0};
 };
 void tau_block(const TauArgs& a, cudaStream_t s);
+// closed-shell two-electron Fock part from dense (pq|rs) (last index fastest):
+// F[p*n + q] = sum_{i < nocc} 2 (pq|ii) - (pi|iq)
+void closed_shell_jk(const double* eri, int n, int nocc, double* F, cudaStream_t s);
 // every block of Tau in one launch: chunks of kBatchChunk elements, chunk_start[p] the
 // first chunk of block p (device arrays)
 void tau_batched(const TauArgs* d, const int64_t* chunk_start, int n, int64_t chunks, cudaStream_t s);

@@ -1408,6 +1408,24 @@ void eri_gather(const EriGatherArgs& a, const double* eri, cudaStream_t s) {
     COUNT_LAUNCH();
 }
 
+namespace {
+__global__ void closed_shell_jk_kernel(const double* __restrict__ eri, int n, int nocc, double* __restrict__ F) {
+    const int64_t pq = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (pq >= (int64_t)n * n) return;
+    const int64_t p = pq / n, q = pq % n, n2 = (int64_t)n * n, n3 = n2 * n;
+    double v = 0;
+    for (int i = 0; i < nocc; i++) v += 2.0 * eri[p * n3 + q * n2 + (int64_t)i * n + i] - eri[p * n3 + (int64_t)i * n2 + (int64_t)i * n + q];
+    F[pq] = v;
+}
+}  // namespace
+
+void closed_shell_jk(const double* eri, int n, int nocc, double* F, cudaStream_t s) {
+    const int64_t nn = (int64_t)n * n;
+    if (nn <= 0) return;
+    closed_shell_jk_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(eri, n, nocc, F);
+    COUNT_LAUNCH();
+}
+
 void tau_block(const TauArgs& a, cudaStream_t s) {
     const int64_t n = a.len[0] * a.len[1] * a.len[2] * a.len[3];
     if (n <= 0) return;

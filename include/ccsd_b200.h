@@ -224,6 +224,16 @@ enum {
 int ccsd_fcidump_read(const char* path, int flags, int* norb, int* nelec, double* ecore, double* h, double* eri);
 /* Read a file, set the context's spaces (C1, NELEC/2 occupied, closed shell), build the
  * Fock matrix and H on the device; escf (may be NULL) receives E_core + sum_i (h_ii + f_ii). */
+/* Closed shell from AO quantities (the integral transformation of aomoints.cxx:1017-1450 /
+ * rhfaomoints.cxx:37-180): hcore[nao*nao] and the AO integrals eri_ao[nao^4] = (mu nu|la si)
+ * (last index fastest), MO coefficients C[nao*nmo] (row-major, column p = MO p, occupied
+ * first).  The MO integrals are formed on the device (four quarter transformations on the
+ * FP64 GEMM kernels), the MO Fock matrix from them, then H as ccsd_hamiltonian_from_integrals
+ * does.  Sets C1 spaces (nocc occupied, nmo - nocc virtual) on a context without tensors.
+ * *e_elec (optional) receives sum_i (h_ii + f_ii), the SCF electronic energy of C.  The AO
+ * array is held on the device (nao^4 + nmo nao^3 doubles); nao^3 must stay below 2^23. */
+int ccsd_hamiltonian_from_ao(ccsd_ctx ctx, int nao, int nmo, int nocc, const double* hcore, const double* eri_ao,
+                             const double* C, int pack_vvvv, ccsd_hamiltonian* H, double* e_elec);
 int ccsd_hamiltonian_from_fcidump(ccsd_ctx ctx, const char* path, int flags, int pack_vvvv, ccsd_hamiltonian* H,
                                   double* escf);
 
@@ -247,6 +257,9 @@ int ccsd_rhf_hamiltonian_from_factor(ccsd_ctx ctx, int naux, const double* B, co
 /* from a spatial Fock matrix and dense (pq|rs) (arguments as ccsd_hamiltonian_from_integrals) */
 int ccsd_rhf_hamiltonian_from_integrals(ccsd_ctx ctx, int n, const double* fock, const double* eri,
                                         ccsd_rhf_hamiltonian* H);
+/* from AO quantities (arguments as ccsd_hamiltonian_from_ao) */
+int ccsd_rhf_hamiltonian_from_ao(ccsd_ctx ctx, int nao, int nmo, int nocc, const double* hcore,
+                                 const double* eri_ao, const double* C, ccsd_rhf_hamiltonian* H, double* e_elec);
 int ccsd_rhf_hamiltonian_destroy(ccsd_ctx ctx, ccsd_rhf_hamiltonian* H);
 /* Solver over the RHF blocks: RHFCCSD::run / iterate (rhfccsd.cxx:44-110, 193-327); the
  * solver handle then works with every ccsd_solver_* call (amplitudes are plain tensors) */
