@@ -627,9 +627,10 @@ void Solver::diis_step() {
     for (auto& sg : segs) kern::diis_dots(d_state, d_dxs, n, sg.off, sg.len, sg.w, d_dots, s);
     // bordered system, solve, coefficients by slot
     kern::diis_solve(d_state, d_e, d_c, d_dots, n, s);
-    // x = sum c_j x_j, dx = sum c_j dx_j  (diis.hpp:205-226)
+    // x = sum c_j x_j (diis.hpp:205-226).  The reference also extrapolates dx into Z; every
+    // iteration assigns Z afresh before reading it and the energy and residual are taken
+    // before DIIS, so that second combination (nine full-vector passes) is not formed
     kern::lincomb(t1.data, t1.total, t2.data, t2.total, d_xs, d_c, n, s);
-    kern::lincomb(z1.data, z1.total, z2.data, z2.total, d_dxs, d_c, n, s);
 }
 
 void Solver::iterate_async() {

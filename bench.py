@@ -541,7 +541,8 @@ def main():
     # bounded serving run (the full sweep is `--serve`): Poisson arrivals at 2 req/s
     serving = None
     if args.serve_sample > 0 and rank == 0:
-        serving = serve(A, args.serve_sample, 2.0, args.serve_seed, prec, log_each=True, graph=args.graph)
+        # served solves replay their iterations as CUDA graphs (fewer host launches per solve)
+        serving = serve(A, args.serve_sample, 2.0, args.serve_seed, prec, log_each=True, graph=True)
         log(f"[bench] serving: p50 {serving['p50_s']:.2f}s p99 {serving['p99_s']:.2f}s, "
             f"{serving['aggregate_iters_per_s']:.1f} iter/s aggregate, peak {serving['peak_active']} active")
 
