@@ -52,6 +52,7 @@ EXPORTS = [
     "ccsd_server_poll", "ccsd_server_wait", "ccsd_server_stats", "ccsd_server_destroy", "ccsd_solver_mode",
     "ccsd_rhf_hamiltonian_from_factor", "ccsd_rhf_hamiltonian_from_integrals", "ccsd_rhf_hamiltonian_destroy",
     "ccsd_rhf_solver_create", "ccsd_rhf_plan_query", "ccsd_hamiltonian_from_ao", "ccsd_rhf_hamiltonian_from_ao",
+    "ccsd_rhf_solver_hbar",
 ]
 
 
@@ -95,6 +96,18 @@ RHF_SHAPES = {
 
 class RHFHamiltonian(ctypes.Structure):
     _fields_ = [(f, ctypes.c_int32) for f in RHF_FIELDS]
+
+
+# closed-shell Hbar intermediates (rhfccsd.cxx:110-186); W(Am,Ie) holds (a,m,i,e) at [a,m,e,i]
+HBAR_SHAPES = {
+    "FME": ((0, 1), (1, 0)), "FMI": ((0, 1), (0, 1)), "FAE": ((1, 0), (1, 0)), "WMNIJ": ((0, 2), (0, 2)),
+    "WMNEJ": ((0, 2), (1, 1)), "WAMIJ": ((1, 1), (0, 2)), "WAMIE": ((1, 1), (1, 1)), "WAMEI": ((1, 1), (1, 1)),
+    "WABEJ": ((2, 0), (1, 1)),
+}
+
+
+class RHFHbar(ctypes.Structure):
+    _fields_ = [(f, ctypes.c_int32) for f in HBAR_SHAPES]
 
 
 class ServerOptions(ctypes.Structure):
@@ -182,6 +195,7 @@ def lib():
             "ccsd_rhf_hamiltonian_from_integrals": [vp, ctypes.c_int, vp, vp, P(RHFHamiltonian)],
             "ccsd_rhf_hamiltonian_destroy": [vp, P(RHFHamiltonian)],
             "ccsd_rhf_solver_create": [vp, P(RHFHamiltonian), P(Options), P(vp)],
+            "ccsd_rhf_solver_hbar": [vp, P(RHFHbar)],
             "ccsd_hamiltonian_from_ao": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp, ctypes.c_int,
                                          P(Hamiltonian), P(dbl)],
             "ccsd_rhf_hamiltonian_from_ao": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp,
@@ -798,6 +812,13 @@ class Solver:
         x = ctypes.c_double()
         _check(lib().ccsd_solver_flops(self.s, ctypes.byref(x)), self.ctx.c)
         return x.value
+
+    def hbar(self):
+        """Closed-shell solver: the Hbar intermediates from the current amplitudes (dict of
+        plain tensors owned by the solver)."""
+        h = RHFHbar()
+        _check(lib().ccsd_rhf_solver_hbar(self.s, ctypes.byref(h)), self.ctx.c)
+        return {f: Tensor(self.ctx, getattr(h, f), f, *HBAR_SHAPES[f], plain=True) for f in HBAR_SHAPES}
 
 
 class Server:

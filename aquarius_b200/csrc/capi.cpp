@@ -899,6 +899,23 @@ int ccsd_solver_amplitudes(ccsd_solver s, ccsd_tensor* T1, ccsd_tensor* T2) {
     });
 }
 
+int ccsd_rhf_solver_hbar(ccsd_solver s, ccsd_rhf_hbar* out) {
+    if (!s || !out) return CCSD_ERR_ARG;
+    return guarded(s->ctx, [&] {
+        Solver& v = *s->s;
+        v.hbar_rhf();
+        out->FME = v.FME;
+        out->FMI = v.FMI;
+        out->FAE = v.FAE;
+        out->WMNIJ = v.WMNIJ;
+        out->WMNEJ = v.WMNEJ;
+        out->WAMIJ = v.WAMIJ;
+        out->WAMIE = v.WAMIE;
+        out->WAMEI = v.WAMEI;
+        out->WABEJ = v.WABEJ;
+    });
+}
+
 int ccsd_solver_flops(ccsd_solver s, double* flops) {
     if (!s) return CCSD_ERR_ARG;
     return guarded(s->ctx, [&] { *flops = s->s->flops_per_iter; });

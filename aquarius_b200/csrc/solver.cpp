@@ -91,6 +91,7 @@ std::vector<int> Solver::owned_tensors() const {
     std::vector<int> t = {T1, T2, Z1, Z2, Tau, FME, FMI, FAE, WMNIJ, WMNEJ, WAMIJ, WAMEI};
     if (rhf)
         for (int x : {T2SA, TauSA, VABIJSA, VAIJBSA, WAMIE, WMNIJc, Z2c}) t.push_back(x);
+    if (WABEJ) t.push_back(WABEJ);
     return t;
 }
 
@@ -189,6 +190,7 @@ Solver::~Solver() {
     ctx.release(iter_plan);
     ctx.release(tau_plan);
     ctx.release(energy_plan);
+    ctx.release(hbar_plan);
     const std::vector<int> cons = constants();
     for (int t : owned_tensors())
         if (ctx.tensors.count(t)) ctx.destroy_tensor(t);
@@ -539,6 +541,94 @@ void Solver::record_iteration_rhf() {
     Z2cr["abij"] -= WAMEIr["amej"] * T2r["ebim"];
     Z2r["abij"] = Z2cr["abij"];
     Z2r["abij"] += Z2cr["baji"];
+}
+
+// "Form Hbar" of RHFCCSD<U>::run (rhfccsd.cxx:110-186): the intermediates again, with the
+// terms the iteration leaves out, and W(Ab,Ej), from the converged amplitudes.  Index
+// strings as in record_iteration_rhf (W(Am,Ie), VAIJB: "amie" reads "amei").
+void Solver::hbar_rhf() {
+    if (!rhf) throw Error(CCSD_ERR_UNSUPPORTED, "Hbar intermediates are formed for the closed-shell solver");
+    if (ctx.host_only) return;
+    if (!WABEJ) {
+        WABEJ = mk(ctx, "W(Ab,Ej)", 2, 0, 1, 1, CCSD_TENSOR_PLAIN);
+        Plan& p = hbar_plan;
+        Recorder r{&ctx, &p};
+        TensorRef fAI{&r, HR.fAI}, fAB{&r, HR.fAB}, fIJ{&r, HR.fIJ};
+        TensorRef VABCD{&r, HR.VABCD}, VABCI{&r, HR.VABCI}, VABIJ{&r, HR.VABIJ}, VAIBJ{&r, HR.VAIBJ};
+        TensorRef VAIJB{&r, HR.VAIJB}, VAIJK{&r, HR.VAIJK}, VIJKL{&r, HR.VIJKL};
+        TensorRef VABIJSAr{&r, VABIJSA}, VAIJBSAr{&r, VAIJBSA};
+        TensorRef T1r{&r, T1}, T2r{&r, T2}, Taur{&r, Tau}, T2SAr{&r, T2SA};
+        TensorRef FMEr{&r, FME}, FAEr{&r, FAE}, FMIr{&r, FMI};
+        TensorRef WMNIJr{&r, WMNIJ}, WMNIJcr{&r, WMNIJc}, WMNEJr{&r, WMNEJ}, WAMIJr{&r, WAMIJ};
+        TensorRef WAMEIr{&r, WAMEI}, WAMIEr{&r, WAMIE}, WABEJr{&r, WABEJ};
+
+        Taur["abij"] = T2r["abij"];
+        Taur["abij"] += T1r["ai"] * T1r["bj"];
+        T2SAr["abij"] = 2.0 * T2r["abij"];
+        T2SAr["abij"] -= T2r["abji"];
+
+        FMEr["me"] = fAI["em"];
+        FMEr["me"] += VABIJSAr["efmn"] * T1r["fn"];
+
+        FMIr["mi"] = fIJ["mi"];
+        FMIr["mi"] += VABIJSAr["efmn"] * T2r["efin"];
+        FMIr["mi"] += FMEr["me"] * T1r["ei"];
+        FMIr["mi"] += 2.0 * VAIJK["finm"] * T1r["fn"];
+        FMIr["mi"] -= VAIJK["fimn"] * T1r["fn"];
+
+        FAEr["ae"] = fAB["ae"];
+        FAEr["ae"] -= VABIJSAr["efmn"] * T2r["afmn"];
+        FAEr["ae"] -= FMEr["me"] * T1r["am"];
+        FAEr["ae"] += 2.0 * VABCI["efam"] * T1r["fm"];
+        FAEr["ae"] -= VABCI["feam"] * T1r["fm"];
+
+        WMNIJcr["mnij"] = 0.5 * VIJKL["mnij"];
+        WMNIJcr["mnij"] += 0.5 * VABIJ["efmn"] * Taur["efij"];
+        WMNIJcr["mnij"] += VAIJK["ejmn"] * T1r["ei"];
+        WMNIJr["mnij"] = WMNIJcr["mnij"];
+        WMNIJr["mnij"] += WMNIJcr["nmji"];
+
+        WMNEJr["mnej"] = VAIJK["ejmn"];
+        WMNEJr["mnej"] += VABIJ["efmn"] * T1r["fj"];
+
+        WAMIJr["amij"] = VAIJK["amij"];
+        WAMIJr["amij"] += VABCI["efam"] * Taur["efij"];
+        WAMIJr["amij"] += VAIBJ["amej"] * T1r["ei"];
+        WAMIJr["amij"] += VAIJB["amei"] * T1r["ej"];
+        WAMIJr["amij"] -= WMNIJr["nmij"] * T1r["an"];
+        WAMIJr["amij"] += WMNEJr["nmej"] * T2SAr["aein"];
+        WAMIJr["amij"] -= WMNEJr["mnej"] * T2r["aein"];
+        WAMIJr["amij"] -= WMNEJr["mnei"] * T2r["aenj"];
+        WAMIJr["amij"] += FMEr["me"] * T2r["aeij"];
+
+        WAMIEr["amei"] = VAIJBSAr["amei"];
+        WAMIEr["amei"] += VABIJSAr["efmn"] * T2SAr["afin"];
+        WAMIEr["amei"] += 2.0 * VABCI["feam"] * T1r["fi"];
+        WAMIEr["amei"] -= VABCI["efam"] * T1r["fi"];
+
+        WAMEIr["amei"] = VAIBJ["amei"];
+        WAMEIr["amei"] -= VABIJ["efnm"] * T2r["afni"];
+        WAMEIr["amei"] += VABCI["efam"] * T1r["fi"];
+
+        WABEJr["abej"] = VABCI["abej"];
+        WABEJr["abej"] += WMNEJr["mnej"] * Taur["abmn"];
+        WABEJr["abej"] -= 0.5 * WAMIEr["bmej"] * T1r["am"];
+        WABEJr["abej"] -= 0.5 * WAMEIr["bmej"] * T1r["am"];
+        WABEJr["abej"] -= WAMEIr["amej"] * T1r["bm"];
+        WABEJr["abej"] += VABCD["abef"] * T1r["fj"];
+        WABEJr["abej"] += VABCI["efam"] * T2SAr["fbmj"];
+        WABEJr["abej"] -= VABCI["feam"] * T2r["fbmj"];
+        WABEJr["abej"] -= VABCI["febm"] * T2r["afmj"];
+        WABEJr["abej"] -= FMEr["me"] * T2r["abmj"];
+
+        WAMIEr["amei"] -= 2.0 * WMNEJr["mnei"] * T1r["an"];
+        WAMIEr["amei"] += WMNEJr["nmei"] * T1r["an"];
+
+        WAMEIr["amei"] -= WMNEJr["nmei"] * T1r["an"];
+        ctx.upload(hbar_plan);
+    }
+    ctx.run(hbar_plan);
+    CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
 }
 
 // ---- DIIS state ----------------------------------------------------------------------

@@ -26,6 +26,8 @@ public:
     // RHF only: spin-adapted combinations, the extra ring intermediate, and the copies
     // that the in-place symmetrisations WMNIJ += WMNIJ(nmji), Z2 += Z2(baji) read
     int T2SA = 0, TauSA = 0, VABIJSA = 0, VAIJBSA = 0, WAMIE = 0, WMNIJc = 0, Z2c = 0;
+    int WABEJ = 0;                     // RHF Hbar only (created on the first hbar())
+    Plan hbar_plan;
     double* den[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [space][spin]
     Plan iter_plan, tau_plan, energy_plan;
     double* d_red = nullptr;    // [0] energy, [1] conv
@@ -71,6 +73,8 @@ public:
     void post_status();
     void check_status();
     int run(double* e, double* c, int* it);
+    // closed-shell Hbar intermediates from the current amplitudes (rhfccsd.cxx:110-186)
+    void hbar_rhf();
 
 private:
     void* alloc(size_t bytes);

@@ -280,6 +280,14 @@ int ccsd_solver_status(ccsd_solver s, double* energy, double* conv, int* iterati
 int ccsd_solver_run(ccsd_solver s, double* energy, double* conv, int* iterations);
 /* amplitudes T1 / T2 as tensors of the solver (for reading) */
 int ccsd_solver_amplitudes(ccsd_solver s, ccsd_tensor* T1, ccsd_tensor* T2);
+/* Closed-shell similarity-transformed Hamiltonian intermediates after convergence
+ * (RHFCCSD::run "Form Hbar", rhfccsd.cxx:110-186) from the solver's current T1, T2: plain
+ * tensors owned by the solver (valid until it is destroyed; recomputed on every call).
+ * WAMIE keeps the engine's [a, m, e, i] position order for the reference's (a, m, i, e). */
+typedef struct {
+    ccsd_tensor FME, FMI, FAE, WMNIJ, WMNEJ, WAMIJ, WAMIE, WAMEI, WABEJ;
+} ccsd_rhf_hbar;
+int ccsd_rhf_solver_hbar(ccsd_solver s, ccsd_rhf_hbar* out);
 /* algorithmic FP64 flops of one iteration as planned (packed-pair counts) */
 int ccsd_solver_flops(ccsd_solver s, double* flops);
 /* contraction mode the next iteration uses (changes when refine_tol is reached):

@@ -127,6 +127,40 @@ class RHFCCSD:
         T2 = sum(sol[i] * self.xs[i][1] for i in range(k))
         return T1, T2
 
+    def hbar(self):
+        """"Form Hbar" of RHFCCSD<U>::run (rhfccsd.cxx:110-186) from the current T1, T2, in
+        the reference's index orders (W(Am,Ie) as [a, m, i, e])."""
+        T1, T2 = self.T1, self.T2
+        fAI, fAB, fIJ = self.fAI, self.fAB, self.fIJ
+        VABIJ, VAIBJ, VAIJB, VABCI = self.VABIJ, self.VAIBJ, self.VAIJB, self.VABCI
+        VAIJK, VIJKL, VABCD = self.VAIJK, self.VIJKL, self.VABCD
+        VABIJSA, VAIJBSA = self.VABIJSA, self.VAIJBSA
+        Tau = T2 + es('ai,bj->abij', T1, T1)
+        T2SA = 2 * T2 - T2.transpose(0, 1, 3, 2)
+        FME = fAI.T + es('efmn,fn->me', VABIJSA, T1)
+        FMI = fIJ + es('efmn,efin->mi', VABIJSA, T2) + es('me,ei->mi', FME, T1) \
+            + 2 * es('finm,fn->mi', VAIJK, T1) - es('fimn,fn->mi', VAIJK, T1)
+        FAE = fAB - es('efmn,afmn->ae', VABIJSA, T2) - es('me,am->ae', FME, T1) \
+            + 2 * es('efam,fm->ae', VABCI, T1) - es('feam,fm->ae', VABCI, T1)
+        WMNIJ = 0.5 * VIJKL + 0.5 * es('efmn,efij->mnij', VABIJ, Tau) + es('ejmn,ei->mnij', VAIJK, T1)
+        WMNIJ = WMNIJ + WMNIJ.transpose(1, 0, 3, 2)
+        WMNEJ = VAIJK.transpose(2, 3, 0, 1) + es('efmn,fj->mnej', VABIJ, T1)
+        WAMIJ = VAIJK + es('efam,efij->amij', VABCI, Tau) + es('amej,ei->amij', VAIBJ, T1) \
+            + es('amie,ej->amij', VAIJB, T1) - es('nmij,an->amij', WMNIJ, T1) \
+            + es('nmej,aein->amij', WMNEJ, T2SA) - es('mnej,aein->amij', WMNEJ, T2) \
+            - es('mnei,aenj->amij', WMNEJ, T2) + es('me,aeij->amij', FME, T2)
+        WAMIE = VAIJBSA + es('efmn,afin->amie', VABIJSA, T2SA) + 2 * es('feam,fi->amie', VABCI, T1) \
+            - es('efam,fi->amie', VABCI, T1)
+        WAMEI = VAIBJ - es('efnm,afni->amei', VABIJ, T2) + es('efam,fi->amei', VABCI, T1)
+        WABEJ = VABCI + es('mnej,abmn->abej', WMNEJ, Tau) - 0.5 * es('bmje,am->abej', WAMIE, T1) \
+            - 0.5 * es('bmej,am->abej', WAMEI, T1) - es('amej,bm->abej', WAMEI, T1) \
+            + es('abef,fj->abej', VABCD, T1) + es('efam,fbmj->abej', VABCI, T2SA) \
+            - es('feam,fbmj->abej', VABCI, T2) - es('febm,afmj->abej', VABCI, T2) - es('me,abmj->abej', FME, T2)
+        WAMIE = WAMIE - 2 * es('mnei,an->amie', WMNEJ, T1) + es('nmei,an->amie', WMNEJ, T1)
+        WAMEI = WAMEI - es('nmei,an->amei', WMNEJ, T1)
+        return {"FME": FME, "FMI": FMI, "FAE": FAE, "WMNIJ": WMNIJ, "WMNEJ": WMNEJ, "WAMIJ": WAMIJ,
+                "WAMIE": WAMIE, "WAMEI": WAMEI, "WABEJ": WABEJ}
+
     def run(self, conv_tol=1e-9, max_iter=50):
         it = 1
         while it <= max_iter and not (self.conv < conv_tol):

@@ -148,3 +148,27 @@ def test_rhf_h2o_known_answers():
         assert abs(e - known["ccsd"]) < known["tolerance"], (e, iters)
         s.close()
         H.destroy()
+
+
+@pytest.mark.parametrize("nirrep", [1, 4])
+def test_rhf_hbar_matches_oracle(nirrep):
+    """The closed-shell Hbar intermediates (rhfccsd.cxx:110-186) after a converged solve."""
+    o, v = (4, 12) if nirrep == 1 else (8, 20)
+    eps, B, occ, vrt, aux, eri = _factor_problem(17, o, v, nirrep)
+    ref = R.RHFCCSD(np.diag(eps), eri, o, diis_order=8)
+    ref.run(1e-11, 100)
+    with A.Context(0) as ctx:
+        ctx.set_spaces(vrt=vrt, occ=occ)
+        H = ctx.rhf_hamiltonian_from_factor(B, eps, aux_per_irrep=aux if nirrep > 1 else None)
+        s = ctx.solver(H, diis_order=8, conv_tol=1e-11, max_iter=100)
+        e, c, it = s.run()
+        assert c < 1e-11 and abs(e - ref.energy) < 1e-10
+        got = s.hbar()
+        want = ref.hbar()
+        want["WAMIE"] = want["WAMIE"].transpose(0, 1, 3, 2)   # engine order [a, m, e, i]
+        for name, w in want.items():
+            g = got[name].to_full()
+            assert g.shape == w.shape, name
+            assert np.abs(g - w).max() < 1e-9 * max(1.0, np.abs(w).max()), (name, np.abs(g - w).max())
+        s.close()
+        H.destroy()
