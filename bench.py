@@ -37,6 +37,10 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
+# The serving loop runs one stream per active solve; with the default 8 hardware work
+# queues, streams share queues and a small solve's launches wait behind a large solve's
+# GEMMs in the same queue.  32 queues (the maximum) for this process, set before CUDA starts.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 WORKLOADS = {
     "cfg2": dict(o=16, v=128, nirrep=1, seed=2, desc="synthetic closed-shell spin-orbital CCSD, C1, o=16 v=128"),
