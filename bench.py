@@ -37,10 +37,7 @@ import numpy as np
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
-# The serving loop runs one stream per active solve; with the default 8 hardware work
-# queues, streams share queues and a small solve's launches wait behind a large solve's
-# GEMMs in the same queue.  32 queues (the maximum) for this process, set before CUDA starts.
-os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 
 WORKLOADS = {
     "cfg2": dict(o=16, v=128, nirrep=1, seed=2, desc="synthetic closed-shell spin-orbital CCSD, C1, o=16 v=128"),
@@ -252,7 +249,7 @@ def run_serve(args):
     prec = args.precision if args.precision != "auto" else "split_i8"
     lines = []
     for rate in args.rates:
-        r = serve(A, args.requests, rate, args.serve_seed, prec, log_each=True, graph=args.graph)
+        r = serve(A, args.requests, rate, args.serve_seed, prec, log_each=True, graph=True)
         line = {"metric": "CCSD serving time-to-converged", "value": r["p50_s"], "unit": "s",
                 "higher_is_better": False, "n_gpus": 1, "data": "synthetic", **r}
         print(json.dumps(line), flush=True)
