@@ -38,9 +38,11 @@ def test_ao_path_blocks_equal_host_transformed_blocks(h2o):
         assert abs(e_elec + res.enuc - known["scf"]) < known["tolerance"]
         c2.set_spaces(vrt=[res.Ca.shape[1] - no], occ=[no])
         Hh = c2.hamiltonian_from_integrals(fock, mo, pack_vvvv=False)
+        # the host integrals are averaged over their 8-fold symmetry, the device ones are not:
+        # they differ at the rounding level of four transformations (~3e-12 measured)
         for name in ["fAI", "fAE", "fMI", "VMNIJ", "VAMIJ", "VMNEF", "VAMEI", "VAMEF", "VABEF"]:
             d = np.abs(Hd[name].to_full() - Hh[name].to_full()).max()
-            assert d < 1e-12, (name, d)
+            assert d < 1e-10, (name, d)
 
 
 def test_ao_path_known_answers_spin_orbital(h2o):
