@@ -120,7 +120,7 @@ class ServerResult(ctypes.Structure):
                 ("energy", ctypes.c_double), ("mp2", ctypes.c_double), ("conv", ctypes.c_double),
                 ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double), ("t_done", ctypes.c_double),
                 ("device_bytes", ctypes.c_int64), ("flops_per_iter", ctypes.c_double),
-                ("peak_bytes", ctypes.c_int64), ("message", ctypes.c_char * 160)]
+                ("peak_bytes", ctypes.c_int64), ("t_built", ctypes.c_double), ("message", ctypes.c_char * 160)]
 
 
 _lib = None

@@ -147,10 +147,11 @@ private:
     }
 
     void finish(const Request& r, int status, int iters, double e, double mp2, double conv, double t_admit,
-                int64_t peak = 0, const std::string& msg = std::string()) {
+                int64_t peak = 0, const std::string& msg = std::string(), double t_built = 0) {
         ccsd_server_result res;
         std::memset(&res, 0, sizeof(res));
         res.peak_bytes = peak;
+        res.t_built = t_built;
         std::snprintf(res.message, sizeof(res.message), "%s", msg.c_str());
         res.id = r.id;
         res.status = status;
@@ -293,9 +294,11 @@ private:
         double e = 0, c = 0, mp2 = 0;
         int it = 0;
         std::string msg;
+        double t_built = 0;
         try {
             stream = priority_stream(r->flops);
             build(*r, stream, ctx, s);
+            t_built = now();
             mp2 = s->mp2;
             CCSD_CUDA(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming | cudaEventBlockingSync));
             while (true) {
@@ -340,7 +343,8 @@ private:
             n_active--;
         }
         cv_admit.notify_all();
-        finish(*r, status, it, status == CCSD_OK || status == CCSD_NOT_CONVERGED ? e : 0.0, mp2, c, t_admit, peak, msg);
+        finish(*r, status, it, status == CCSD_OK || status == CCSD_NOT_CONVERGED ? e : 0.0, mp2, c, t_admit, peak, msg,
+               t_built);
     }
 };
 

@@ -234,6 +234,7 @@ def serve(A, n_req, rate, seed, precision, log_each=False, graph=False):
             o, v, h, s = ids[r["id"]]
             log(f"[serve] id={r['id']:3d} o={o:2d} v={v:3d} nirrep={h} status={r['status']} it={r['iterations']:3d} "
                 f"wait={r['t_admit'] - r['t_submit']:6.2f}s ttc={r['t_done'] - r['t_submit']:6.2f}s "
+                f"build={r['t_built'] - r['t_admit']:6.2f}s iterate={r['t_done'] - r['t_built']:6.2f}s "
                 f"bytes={r['device_bytes'] / 1e9:6.1f}GB peak={r['peak_bytes'] / 1e9:6.1f}GB"
                 + (f" error: {r['message']}" if r["message"] else ""))
     return {"requests": n_req, "rate_req_s": rate, "precision": precision,

@@ -345,6 +345,7 @@ typedef struct {
     int64_t device_bytes;    /* planned bytes the solve was admitted with */
     double flops_per_iter;
     int64_t peak_bytes;      /* device bytes the solve's context held at its peak */
+    double t_built;          /* when its H and solver were ready (seconds since the server started) */
     char message[160];       /* the error message of a failed solve ("" otherwise) */
 } ccsd_server_result;
 void ccsd_server_options_default(ccsd_server_options* o);
