@@ -25,13 +25,12 @@ struct DeviceTables {
     T* up(const std::vector<T>& h) {
         const size_t b = std::max<size_t>(h.size(), 1) * sizeof(T);
         T* d = (T*)ctx.dmalloc(b);
-        CCSD_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, ctx.stream));
+        ctx.stage_h2d(d, h.data(), h.size() * sizeof(T));
         held.push_back({d, b});
         return d;
     }
     ~DeviceTables() {
-        cudaStreamSynchronize(ctx.stream);
-        for (auto& p : held) ctx.dfree(p.first, p.second);
+        for (auto& p : held) ctx.dfree(p.first, p.second);   // stream-ordered
     }
 };
 

@@ -57,7 +57,29 @@ Context::~Context() {
     }
     for (auto e : event_pool) cudaEventDestroy(e);
     kern::release_stream_buffers(stream);
+    if (pin_buf) cudaFreeHost(pin_buf);
     if (own_stream) cudaStreamDestroy(stream);
+}
+
+void Context::stage_h2d(void* dst, const void* src, size_t bytes) {
+    if (host_only || bytes == 0) return;
+    constexpr size_t kArena = 64ull << 20;
+    if (bytes > kArena / 4) {   // large copies go direct (pageable: the driver stages them)
+        CCSD_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
+        return;
+    }
+    if (!pin_buf) {
+        CCSD_CUDA(cudaMallocHost((void**)&pin_buf, kArena));
+        pin_cap = kArena;
+        pin_off = 0;
+    }
+    if (pin_off + bytes > pin_cap) {
+        CCSD_CUDA(cudaStreamSynchronize(stream));   // every staged copy has left the arena
+        pin_off = 0;
+    }
+    std::memcpy(pin_buf + pin_off, src, bytes);
+    CCSD_CUDA(cudaMemcpyAsync(dst, pin_buf + pin_off, bytes, cudaMemcpyHostToDevice, stream));
+    pin_off += (bytes + 255) & ~(size_t)255;
 }
 
 void* Context::dmalloc(size_t bytes) {
@@ -297,8 +319,7 @@ int Context::create_view(const std::string& name, int hb, const int nout[2], con
 static int64_t* upload_table(Context& ctx, const std::vector<int64_t>& h) {
     if (h.empty()) return nullptr;
     int64_t* d = (int64_t*)ctx.dmalloc(h.size() * sizeof(int64_t));
-    if (ctx.host_only) return d;
-    CCSD_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(int64_t), cudaMemcpyHostToDevice, ctx.stream));
+    ctx.stage_h2d(d, h.data(), h.size() * sizeof(int64_t));
     return d;
 }
 
@@ -388,7 +409,7 @@ void Context::upload(Plan& p) {
         reserve_split(p);
         p.split_reserved = true;
     }
-    if (any && !host_only) CCSD_CUDA(cudaStreamSynchronize(stream));
+    (void)any;   // staged copies need no synchronisation (the host tables stay with the plan)
 }
 
 void Context::release(Plan& p) {
@@ -650,11 +671,8 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
                 }
                 l.d_probs = (kern::GemmArgs*)dmalloc(probs[c].size() * sizeof(kern::GemmArgs));
                 l.d_tile_start = (int*)dmalloc(tstart[c].size() * sizeof(int));
-                CCSD_CUDA(cudaMemcpyAsync(l.d_probs, probs[c].data(), probs[c].size() * sizeof(kern::GemmArgs),
-                                          cudaMemcpyHostToDevice, stream));
-                CCSD_CUDA(cudaMemcpyAsync(l.d_tile_start, tstart[c].data(), tstart[c].size() * sizeof(int),
-                                          cudaMemcpyHostToDevice, stream));
-                CCSD_CUDA(cudaStreamSynchronize(stream));
+                stage_h2d(l.d_probs, probs[c].data(), probs[c].size() * sizeof(kern::GemmArgs));
+                stage_h2d(l.d_tile_start, tstart[c].data(), tstart[c].size() * sizeof(int));
                 run.launches.push_back(l);
             }
             std::vector<kern::FoldDesc> descs;
@@ -671,10 +689,8 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
             fl_l.desc_bytes = descs.size() * sizeof(kern::FoldDesc);
             fl_l.d_desc = dmalloc(fl_l.desc_bytes);
             fl_l.d_tile_start = (int*)dmalloc(gstart.size() * sizeof(int));
-            CCSD_CUDA(cudaMemcpyAsync(fl_l.d_desc, descs.data(), fl_l.desc_bytes, cudaMemcpyHostToDevice, stream));
-            CCSD_CUDA(cudaMemcpyAsync(fl_l.d_tile_start, gstart.data(), gstart.size() * sizeof(int),
-                                      cudaMemcpyHostToDevice, stream));
-            CCSD_CUDA(cudaStreamSynchronize(stream));
+            stage_h2d(fl_l.d_desc, descs.data(), fl_l.desc_bytes);
+            stage_h2d(fl_l.d_tile_start, gstart.data(), gstart.size() * sizeof(int));
             run.launches.push_back(fl_l);
             any_group = true;
         }
@@ -725,11 +741,8 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
             l.tiles = tiles;
             l.d_probs = (kern::GemmArgs*)dmalloc(probs.size() * sizeof(kern::GemmArgs));
             l.d_tile_start = (int*)dmalloc(tstart.size() * sizeof(int));
-            CCSD_CUDA(cudaMemcpyAsync(l.d_probs, probs.data(), probs.size() * sizeof(kern::GemmArgs),
-                                      cudaMemcpyHostToDevice, stream));
-            CCSD_CUDA(cudaMemcpyAsync(l.d_tile_start, tstart.data(), tstart.size() * sizeof(int),
-                                      cudaMemcpyHostToDevice, stream));
-            CCSD_CUDA(cudaStreamSynchronize(stream));   // the host vectors go out of scope
+            stage_h2d(l.d_probs, probs.data(), probs.size() * sizeof(kern::GemmArgs));
+            stage_h2d(l.d_tile_start, tstart.data(), tstart.size() * sizeof(int));
             run.launches.push_back(l);
             any_group = true;
         }
@@ -809,7 +822,7 @@ void Context::build_elementwise_run(Plan& p, RunSchedule& rs, int first, int end
             if (d.empty()) continue;
             l.desc_bytes = d.size() * sizeof(kern::SumDesc);
             l.d_desc = dmalloc(l.desc_bytes);
-            CCSD_CUDA(cudaMemcpyAsync(l.d_desc, d.data(), l.desc_bytes, cudaMemcpyHostToDevice, stream));
+            stage_h2d(l.d_desc, d.data(), l.desc_bytes);
             l.nprob = (int)d.size();
         } else {
             l.kind = GemmLaunch::SCALE_BATCHED;
@@ -828,14 +841,13 @@ void Context::build_elementwise_run(Plan& p, RunSchedule& rs, int first, int end
             if (d.empty()) continue;
             l.desc_bytes = d.size() * sizeof(kern::ScaleDesc);
             l.d_desc = dmalloc(l.desc_bytes);
-            CCSD_CUDA(cudaMemcpyAsync(l.d_desc, d.data(), l.desc_bytes, cudaMemcpyHostToDevice, stream));
+            stage_h2d(l.d_desc, d.data(), l.desc_bytes);
             l.nprob = (int)d.size();
         }
         if (chunks > INT32_MAX) throw Error(CCSD_ERR_PLAN, "batched launch too large");
         l.chunks = chunks;
         l.d_chunks = (int64_t*)dmalloc(cs.size() * sizeof(int64_t));
-        CCSD_CUDA(cudaMemcpyAsync(l.d_chunks, cs.data(), cs.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream));
-        CCSD_CUDA(cudaStreamSynchronize(stream));   // the host vectors go out of scope
+        stage_h2d(l.d_chunks, cs.data(), cs.size() * sizeof(int64_t));
         run.launches.push_back(l);
     }
     rs.run_at[first] = (int)rs.runs.size();
@@ -877,9 +889,8 @@ void Context::build_dot_run(Plan& p, RunSchedule& rs, int first, int end) {
     l.d_chunks = (int64_t*)dmalloc(cs.size() * sizeof(int64_t));
     l.d_part = (double*)dmalloc(chunks * sizeof(double));
     l.part_elems = chunks;
-    CCSD_CUDA(cudaMemcpyAsync(l.d_desc, descs.data(), l.desc_bytes, cudaMemcpyHostToDevice, stream));
-    CCSD_CUDA(cudaMemcpyAsync(l.d_chunks, cs.data(), cs.size() * sizeof(int64_t), cudaMemcpyHostToDevice, stream));
-    CCSD_CUDA(cudaStreamSynchronize(stream));
+    stage_h2d(l.d_desc, descs.data(), l.desc_bytes);
+    stage_h2d(l.d_chunks, cs.data(), cs.size() * sizeof(int64_t));
     GemmRun run;
     run.first = first;
     run.end = end;

@@ -296,6 +296,12 @@ public:
     int create_view(const std::string& name, int base, const int nout[2], const int nin[2], const int* perm);
     void destroy_tensor(int h);
     void* dmalloc(size_t bytes);
+    // Host -> device copy of plan tables and descriptors through a pinned staging arena:
+    // stream-ordered, no implicit synchronisation (a copy from pageable memory waits for
+    // the stream first); the arena is reused only after a stream synchronisation.
+    void stage_h2d(void* dst, const void* src, size_t bytes);
+    char* pin_buf = nullptr;
+    size_t pin_cap = 0, pin_off = 0;
     void dfree(void* p, size_t bytes);
 
     // execute a plan on the stream (device tables uploaded lazily)

@@ -21,19 +21,19 @@ namespace ccsd {
 
 namespace {
 
-// device copies of host index tables, freed together
+// device copies of host index tables, freed together (staged and freed in stream order:
+// no host synchronisation per block product)
 struct Tables {
     Context& ctx;
     std::vector<std::pair<void*, size_t>> held;
     template <class T>
     T* up(const std::vector<T>& h) {
         T* d = (T*)ctx.dmalloc(std::max<size_t>(h.size(), 1) * sizeof(T));
-        CCSD_CUDA(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, ctx.stream));
+        ctx.stage_h2d(d, h.data(), h.size() * sizeof(T));
         held.push_back({d, std::max<size_t>(h.size(), 1) * sizeof(T)});
         return d;
     }
     ~Tables() {
-        cudaStreamSynchronize(ctx.stream);
         for (auto& p : held) ctx.dfree(p.first, p.second);
     }
 };
@@ -141,7 +141,7 @@ struct Builder {
                 if (sp0 != sp1 || b.irrep[0] != b.irrep[1] || sc.spin[0] != sc.spin[1]) continue;
                 std::vector<double> host(b.size, 0.0);
                 for (int x = 0; x < b.len[0]; x++) host[x + (int64_t)x * b.len[0]] = eps[gidx(sp0, b.irrep[0], x)];
-                CCSD_CUDA(cudaMemcpy(T.data + b.offset, host.data(), b.size * sizeof(double), cudaMemcpyHostToDevice));
+                ctx.stage_h2d(T.data + b.offset, host.data(), b.size * sizeof(double));
             }
     }
 
@@ -159,7 +159,7 @@ struct Builder {
                     for (int x = 0; x < b.len[0]; x++)
                         host[b.stride[0] * x + b.stride[1] * y] =
                             f[(int64_t)gidx(sp0, b.irrep[0], x) * n + gidx(sp1, b.irrep[1], y)];
-                CCSD_CUDA(cudaMemcpy(T.data + b.offset, host.data(), b.size * sizeof(double), cudaMemcpyHostToDevice));
+                ctx.stage_h2d(T.data + b.offset, host.data(), b.size * sizeof(double));
             }
     }
 
@@ -234,8 +234,7 @@ struct Builder {
             kern::pack_vvvv(T.data + b.offset, b.pairs[0].kind, b.pairs[1].kind, len[0], len[1], len[2], len[3],
                             b.pairs[1].stride, tJ, tK, a0, a1, J, K, ctx.stream);
         }
-        CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
-        ctx.dfree(tJ, chunk * per_a * sizeof(double));
+        ctx.dfree(tJ, chunk * per_a * sizeof(double));   // stream-ordered
         ctx.dfree(tK, chunk * per_a * sizeof(double));
     }
 

@@ -324,10 +324,8 @@ void Solver::build_tau_blocks() {
     if (tau_blocks.size() > 1) {
         d_tau = (kern::TauArgs*)alloc(tau_blocks.size() * sizeof(kern::TauArgs));
         d_tau_cs = (int64_t*)alloc(cs.size() * sizeof(int64_t));
-        CCSD_CUDA(cudaMemcpyAsync(d_tau, tau_blocks.data(), tau_blocks.size() * sizeof(kern::TauArgs),
-                                  cudaMemcpyHostToDevice, ctx.stream));
-        CCSD_CUDA(cudaMemcpyAsync(d_tau_cs, cs.data(), cs.size() * sizeof(int64_t), cudaMemcpyHostToDevice, ctx.stream));
-        CCSD_CUDA(cudaStreamSynchronize(ctx.stream));   // the host arrays go out of scope
+        ctx.stage_h2d(d_tau, tau_blocks.data(), tau_blocks.size() * sizeof(kern::TauArgs));
+        ctx.stage_h2d(d_tau_cs, cs.data(), cs.size() * sizeof(int64_t));
     }
 }
 
@@ -360,10 +358,8 @@ void Solver::build_update() {
     n_upd = (int)descs.size();
     d_upd = (kern::UpdateDesc*)alloc(std::max<size_t>(descs.size(), 1) * sizeof(kern::UpdateDesc));
     d_upd_cs = (int64_t*)alloc(std::max<size_t>(cs.size(), 1) * sizeof(int64_t));
-    CCSD_CUDA(cudaMemcpyAsync(d_upd, descs.data(), descs.size() * sizeof(kern::UpdateDesc), cudaMemcpyHostToDevice,
-                              ctx.stream));
-    CCSD_CUDA(cudaMemcpyAsync(d_upd_cs, cs.data(), cs.size() * sizeof(int64_t), cudaMemcpyHostToDevice, ctx.stream));
-    CCSD_CUDA(cudaStreamSynchronize(ctx.stream));   // the host arrays go out of scope
+    ctx.stage_h2d(d_upd, descs.data(), descs.size() * sizeof(kern::UpdateDesc));
+    ctx.stage_h2d(d_upd_cs, cs.data(), cs.size() * sizeof(int64_t));
 }
 
 void Solver::record_tau(Plan& p) {
