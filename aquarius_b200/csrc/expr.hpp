@@ -6,16 +6,41 @@
 // Each statement is planned once (spin cases, irrep blocks, gather tables) and
 // appended to a Plan that the solver replays every iteration.
 #pragma once
+#include <exception>
+#include <functional>
 #include <string>
+#include <vector>
 
 #include "engine.hpp"
 
 namespace ccsd {
 
+// With `defer` set, statements are collected and planned by run_deferred(), in parallel
+// (planning reads the context's tensors only), and appended to the plan in statement order.
 struct Recorder {
     Context* ctx;
     Plan* plan;
+    std::vector<std::function<Plan()>>* defer = nullptr;
 };
+
+inline void run_deferred(Recorder& r) {
+    if (!r.defer) return;
+    auto& jobs = *r.defer;
+    std::vector<Plan> out(jobs.size());
+    std::vector<std::exception_ptr> err(jobs.size());
+#pragma omp parallel for schedule(dynamic, 1)
+    for (long i = 0; i < (long)jobs.size(); i++) {
+        try {
+            out[i] = jobs[i]();
+        } catch (...) {
+            err[i] = std::current_exception();
+        }
+    }
+    for (auto& e : err)
+        if (e) std::rethrow_exception(e);
+    for (auto& p : out) r.plan->append(std::move(p));
+    jobs.clear();
+}
 
 struct Indexed {
     Recorder* r = nullptr;
@@ -44,20 +69,34 @@ struct Lhs {
     int h;
     std::string idx;
     void sum(double alpha, const Indexed& x, double beta) {
-        Plan p = plan_sum(*r->ctx, alpha, x.h, x.idx, beta, h, idx);
-        std::string label = r->ctx->tensor(h).name + "[" + idx + "] += " + r->ctx->tensor(x.h).name + "[" + x.idx + "]";
-        for (auto& g : p.sums) g.label = label;
-        for (auto& g : p.scales) g.label = label + " (scale)";
-        r->plan->append(std::move(p));
+        Context* ctx = r->ctx;
+        const int hc = h, ha = x.h;
+        const std::string ic = idx, ia = x.idx;
+        auto job = [=]() {
+            Plan p = plan_sum(*ctx, alpha, ha, ia, beta, hc, ic);
+            std::string label = ctx->tensor(hc).name + "[" + ic + "] += " + ctx->tensor(ha).name + "[" + ia + "]";
+            for (auto& g : p.sums) g.label = label;
+            for (auto& g : p.scales) g.label = label + " (scale)";
+            return p;
+        };
+        if (r->defer) r->defer->push_back(job);
+        else r->plan->append(job());
     }
     void mult(double alpha, const IndexedMult& m, double beta) {
-        Plan p = plan_contract(*r->ctx, alpha, m.a.h, m.a.idx, m.b.h, m.b.idx, beta, h, idx);
-        std::string label = r->ctx->tensor(h).name + "[" + idx + "] += " + r->ctx->tensor(m.a.h).name + "[" + m.a.idx +
-                            "]*" + r->ctx->tensor(m.b.h).name + "[" + m.b.idx + "]";
-        for (auto& g : p.gemms) g.label = label;
-        for (auto& g : p.sums) g.label = label + " (images)";
-        for (auto& g : p.scales) g.label = label + " (scale)";
-        r->plan->append(std::move(p));
+        Context* ctx = r->ctx;
+        const int hc = h, ha = m.a.h, hb = m.b.h;
+        const std::string ic = idx, ia = m.a.idx, ib = m.b.idx;
+        auto job = [=]() {
+            Plan p = plan_contract(*ctx, alpha, ha, ia, hb, ib, beta, hc, ic);
+            std::string label = ctx->tensor(hc).name + "[" + ic + "] += " + ctx->tensor(ha).name + "[" + ia + "]*" +
+                                ctx->tensor(hb).name + "[" + ib + "]";
+            for (auto& g : p.gemms) g.label = label;
+            for (auto& g : p.sums) g.label = label + " (images)";
+            for (auto& g : p.scales) g.label = label + " (scale)";
+            return p;
+        };
+        if (r->defer) r->defer->push_back(job);
+        else r->plan->append(job());
     }
     void operator=(const Indexed& x) { sum(x.f, x, 0.0); }
     void operator+=(const Indexed& x) { sum(x.f, x, 1.0); }

@@ -368,7 +368,7 @@ void lower_gemm(Context& ctx, Term& t, int hA, int hB, int hC, int cc, std::set<
                 if (op2 && !same_group_spin(*op2, a, b, vars)) continue;
                 if (external) {
                     // C positions a,b must be in the same group of C with equal spin
-                    const Tensor& C = *ctx.tensors[hC];
+                    const Tensor& C = *ctx.tensors.at(hC);
                     int pa = -1, pb = -1;
                     for (size_t p = 0; p < t.cvar.size(); p++) {
                         if (t.cvar[p] == a) pa = (int)p;
@@ -467,7 +467,7 @@ void lower_gemm(Context& ctx, Term& t, int hA, int hB, int hC, int cc, std::set<
     } else {
         // C destinations (C unpacked): variants swap the values (and irreps) of restricted pairs;
         // a swapped pair with unequal irreps lands in the C block with those irreps exchanged.
-        const Tensor& Ct = *ctx.tensors[hC];
+        const Tensor& Ct = *ctx.tensors.at(hC);
         g.nvm = mpairs.empty() ? 1 : 2;
         g.nvn = npairs.empty() ? 1 : 2;
         if (mpairs.size() > 1 || npairs.size() > 1) fail(CCSD_ERR_PLAN, "more than one restricted output pair per factor");

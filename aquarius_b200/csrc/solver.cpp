@@ -390,7 +390,8 @@ void Solver::record_energy(Plan& p) {
 
 void Solver::record_iteration() {
     Plan& p = iter_plan;
-    Recorder r{&ctx, &p};
+    std::vector<std::function<Plan()>> jobs;
+    Recorder r{&ctx, &p, &jobs};
     TensorRef fAI{&r, H.fAI}, fME{&r, H.fME}, fAE{&r, H.fAE}, fMI{&r, H.fMI};
     TensorRef VABIJ{&r, H.VABIJ}, VMNEF{&r, H.VMNEF}, VAMEF{&r, H.VAMEF}, VABEJ{&r, H.VABEJ}, VABEF{&r, H.VABEF};
     TensorRef VMNIJ{&r, H.VMNIJ}, VMNEJ{&r, H.VMNEJ}, VAMIJ{&r, H.VAMIJ}, VAMEI{&r, H.VAMEI};
@@ -448,6 +449,7 @@ void Solver::record_iteration() {
     Z2r["abij"] += 0.5 * VABEF["abef"] * Taur["efij"];
     Z2r["abij"] += 0.5 * WMNIJr["mnij"] * Taur["abmn"];
     Z2r["abij"] += WAMEIr["amei"] * T2r["ebjm"];
+    run_deferred(r);
 }
 
 // RHFCCSD<U>::iterate (rhfccsd.cxx:237-306) over plain tensors.  Index strings follow
@@ -457,7 +459,8 @@ void Solver::record_iteration() {
 // accumulated in a second tensor and folded once.
 void Solver::record_iteration_rhf() {
     Plan& p = iter_plan;
-    Recorder r{&ctx, &p};
+    std::vector<std::function<Plan()>> jobs;
+    Recorder r{&ctx, &p, &jobs};
     TensorRef fAI{&r, HR.fAI}, fAB{&r, HR.fAB}, fIJ{&r, HR.fIJ};
     TensorRef VABCD{&r, HR.VABCD}, VABCI{&r, HR.VABCI}, VABIJ{&r, HR.VABIJ}, VAIBJ{&r, HR.VAIBJ};
     TensorRef VAIJB{&r, HR.VAIJB}, VAIJK{&r, HR.VAIJK}, VIJKL{&r, HR.VIJKL};
@@ -537,6 +540,7 @@ void Solver::record_iteration_rhf() {
     Z2cr["abij"] -= WAMEIr["amej"] * T2r["ebim"];
     Z2r["abij"] = Z2cr["abij"];
     Z2r["abij"] += Z2cr["baji"];
+    run_deferred(r);
 }
 
 // "Form Hbar" of RHFCCSD<U>::run (rhfccsd.cxx:110-186): the intermediates again, with the
@@ -548,7 +552,8 @@ void Solver::hbar_rhf() {
     if (!WABEJ) {
         WABEJ = mk(ctx, "W(Ab,Ej)", 2, 0, 1, 1, CCSD_TENSOR_PLAIN);
         Plan& p = hbar_plan;
-        Recorder r{&ctx, &p};
+        std::vector<std::function<Plan()>> jobs;
+        Recorder r{&ctx, &p, &jobs};
         TensorRef fAI{&r, HR.fAI}, fAB{&r, HR.fAB}, fIJ{&r, HR.fIJ};
         TensorRef VABCD{&r, HR.VABCD}, VABCI{&r, HR.VABCI}, VABIJ{&r, HR.VABIJ}, VAIBJ{&r, HR.VAIBJ};
         TensorRef VAIJB{&r, HR.VAIJB}, VAIJK{&r, HR.VAIJK}, VIJKL{&r, HR.VIJKL};
@@ -621,6 +626,7 @@ void Solver::hbar_rhf() {
         WAMIEr["amei"] += WMNEJr["nmei"] * T1r["an"];
 
         WAMEIr["amei"] -= WMNEJr["nmei"] * T1r["an"];
+        run_deferred(r);
         ctx.upload(hbar_plan);
     }
     ctx.run(hbar_plan);
