@@ -246,6 +246,7 @@ public:
     int precision = CCSD_PREC_FP64;
     int slices = 0;
     bool plan_refine = false;          // host-only plan of a split solve that may move to 4 slices
+    int plan_threads = 8;              // host threads that plan the statements of an iteration
     int split_routing = CCSD_SPLIT_ROUTE_AUTO;  // which contractions take the split kernel
     bool fp64_tiled_only = false;      // keep skinny FP64 products on the tiled kernel
     bool group_gemms = true;           // batch small block contractions of a statement into grouped launches

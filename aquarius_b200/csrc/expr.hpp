@@ -28,7 +28,8 @@ inline void run_deferred(Recorder& r) {
     auto& jobs = *r.defer;
     std::vector<Plan> out(jobs.size());
     std::vector<std::exception_ptr> err(jobs.size());
-#pragma omp parallel for schedule(dynamic, 1)
+    const int nt = r.ctx->plan_threads > 0 ? r.ctx->plan_threads : 1;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
     for (long i = 0; i < (long)jobs.size(); i++) {
         try {
             out[i] = jobs[i]();

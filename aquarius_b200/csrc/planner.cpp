@@ -251,11 +251,13 @@ void enumerate_dim(const std::vector<Unit>& units, const std::vector<Var>& vars,
     }
 }
 
+constexpr int kMaxVars = 32;   // C positions + internal letters of one statement (at most 8 + 8)
+
 int64_t operand_offset(const Operand& op, const std::vector<int64_t>& val, const std::vector<int>& only_vars) {
     // offset of the operand element for the subset of variables `only_vars` (others 0)
     const Block& b = *op.blk;
     int64_t off = 0;
-    std::vector<char> use(val.size(), 0);
+    char use[kMaxVars] = {0};   // per element: no heap allocation on the planning hot path
     for (int v : only_vars) use[v] = 1;
     int np = (int)op.var.size();
     for (int q = 0; q < np; q++) {
@@ -353,6 +355,7 @@ struct Dest {
 void lower_gemm(Context& ctx, Term& t, int hA, int hB, int hC, int cc, std::set<std::pair<int, int>>& touched,
                 Plan& plan, const Dest* dest_x = nullptr) {
     const auto& vars = t.vars;
+    if ((int)vars.size() > kMaxVars) fail(CCSD_ERR_PLAN, "too many index letters in one statement");
     // pair restrictions
     std::vector<std::pair<int, int>> kpairs, mpairs, npairs;
     double factor = 1.0;
@@ -485,14 +488,16 @@ void lower_gemm(Context& ctx, Term& t, int hA, int hB, int hC, int cc, std::set<
             fail(CCSD_ERR_PLAN, "restricted pairs in both dimensions across irrep blocks");
         auto c_off = [&](const std::vector<int64_t>& val, const std::vector<int>& vl, int swapmask,
                          const std::vector<std::pair<int, int>>& prs, const Block& blk) {
-            std::vector<int64_t> v2 = val;
+            // variable whose value each variable takes (a restricted pair swapped in variant 1)
+            int src[kMaxVars];
+            char use[kMaxVars] = {0};
+            for (size_t v = 0; v < vars.size(); v++) src[v] = (int)v;
             if (swapmask)
-                for (auto& pr : prs) std::swap(v2[pr.first], v2[pr.second]);
-            int64_t off = 0;
-            std::vector<char> use(vars.size(), 0);
+                for (auto& pr : prs) std::swap(src[pr.first], src[pr.second]);
             for (int v : vl) use[v] = 1;
+            int64_t off = 0;
             for (size_t p = 0; p < t.cvar.size(); p++)
-                if (use[t.cvar[p]]) off += blk.stride[p] * v2[t.cvar[p]];
+                if (use[t.cvar[p]]) off += blk.stride[p] * val[src[t.cvar[p]]];
             return off;
         };
         for (int v = 0; v < g.nvm; v++) {

@@ -249,6 +249,7 @@ private:
 
     void build(Request& r, cudaStream_t stream, std::unique_ptr<Context>& ctx, std::unique_ptr<Solver>& solver) {
         ctx = std::make_unique<Context>(opts.device, stream);
+        ctx->plan_threads = 2;   // several solves build at once: keep the host from oversubscription
         Spaces S;
         S.nirrep = r.nirrep;
         for (int sp = 0; sp < 2; sp++)
