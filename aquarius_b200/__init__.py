@@ -52,7 +52,7 @@ EXPORTS = [
     "ccsd_server_poll", "ccsd_server_wait", "ccsd_server_stats", "ccsd_server_destroy", "ccsd_solver_mode",
     "ccsd_rhf_hamiltonian_from_factor", "ccsd_rhf_hamiltonian_from_integrals", "ccsd_rhf_hamiltonian_destroy",
     "ccsd_rhf_solver_create", "ccsd_rhf_plan_query", "ccsd_hamiltonian_from_ao", "ccsd_rhf_hamiltonian_from_ao",
-    "ccsd_rhf_solver_hbar",
+    "ccsd_rhf_solver_hbar", "ccsd_ctx_plan_flops",
 ]
 
 
@@ -141,6 +141,7 @@ def lib():
             "ccsd_ctx_synchronize": [vp],
             "ccsd_ctx_device_bytes": [vp, P(i64)],
             "ccsd_ctx_launch_count": [vp, P(i64)],
+            "ccsd_ctx_plan_flops": [vp, P(dbl)],
             "ccsd_ctx_set_precision": [vp, ctypes.c_int, ctypes.c_int],
             "ccsd_ctx_set_profiling": [vp, ctypes.c_int],
             "ccsd_ctx_set_split_routing": [vp, ctypes.c_int],
@@ -510,6 +511,9 @@ def _assign(t, idx, expr, beta):
 
 
 class Context:
+    """device < 0: a planning-only context (no GPU): statements plan and account bytes and
+    flops, nothing runs, tensor data cannot be read or written."""
+
     def __init__(self, device: int = 0, stream: int | None = None):
         c = ctypes.c_void_p()
         _check(lib().ccsd_ctx_create(device, stream, ctypes.byref(c)))
@@ -616,6 +620,12 @@ class Context:
         buf = ctypes.create_string_buffer(int(need.value) + 16)
         _check(lib().ccsd_ctx_profile_report(self.c, buf, len(buf), ctypes.byref(need)), self.c)
         return json.loads(buf.value.decode())
+
+    def plan_flops(self):
+        """algorithmic flops of the last contraction statement (planner count)"""
+        x = ctypes.c_double()
+        _check(lib().ccsd_ctx_plan_flops(self.c, ctypes.byref(x)), self.c)
+        return x.value
 
     def launch_count(self):
         n = ctypes.c_int64()

@@ -27,6 +27,12 @@ Context* from_handle(ccsd_ctx c) {
     if (!c || !c->c) throw Error(CCSD_ERR_ARG, "null context");
     return c->c;
 }
+// a context whose tensors have device data (not a planning-only context)
+Context* device_handle(ccsd_ctx c) {
+    Context* x = from_handle(c);
+    if (x->host_only) throw Error(CCSD_ERR_UNSUPPORTED, "planning-only context: tensors hold no data");
+    return x;
+}
 // message for entry points that have no context (ccsd_last_error(NULL))
 void set_global_error(const std::string& msg) { g_global_error = msg; }
 }  // namespace ccsd
@@ -38,7 +44,7 @@ namespace {
 template <class F>
 int guarded(ccsd_ctx ctx, F f) {
     try {
-        if (ctx && ctx->c) CCSD_CUDA(cudaSetDevice(ctx->c->device));
+        if (ctx && ctx->c && ctx->c->device >= 0) CCSD_CUDA(cudaSetDevice(ctx->c->device));
         f();
         return CCSD_OK;
     } catch (const Error& e) {
@@ -133,7 +139,7 @@ int ccsd_ctx_create(int device, void* stream, ccsd_ctx* out) {
     if (!out) return CCSD_ERR_ARG;
     *out = nullptr;
     return guarded(nullptr, [&] {
-        CCSD_CUDA(cudaSetDevice(device));
+        if (device >= 0) CCSD_CUDA(cudaSetDevice(device));   // < 0: planning only
         auto* h = new ccsd_ctx_s;
         try {
             h->c = new Context(device, (cudaStream_t)stream);
@@ -156,6 +162,13 @@ int ccsd_ctx_destroy(ccsd_ctx ctx) {
 const char* ccsd_last_error(ccsd_ctx ctx) {
     if (ctx && ctx->c) return ctx->c->last_error.c_str();
     return g_global_error.c_str();
+}
+
+int ccsd_ctx_plan_flops(ccsd_ctx ctx, double* flops) {
+    return guarded(ctx, [&] {
+        if (!flops) throw Error(CCSD_ERR_ARG, "null output");
+        *flops = from_handle(ctx)->last_plan_flops;
+    });
 }
 
 int ccsd_ctx_synchronize(ccsd_ctx ctx) {
@@ -322,7 +335,7 @@ static std::vector<int64_t> block_order(const Block& b) {
 
 int ccsd_tensor_write_block(ccsd_ctx ctx, ccsd_tensor t, const int alpha[4], const int* irreps, const double* host) {
     return guarded(ctx, [&] {
-        Context* c = from_handle(ctx);
+        Context* c = device_handle(ctx);
         Tensor& T = c->tensor(t);
         int cs;
         const Block& b = block_at(T, alpha, irreps, cs);
@@ -340,7 +353,7 @@ int ccsd_tensor_write_block(ccsd_ctx ctx, ccsd_tensor t, const int alpha[4], con
 
 int ccsd_tensor_read_block(ccsd_ctx ctx, ccsd_tensor t, const int alpha[4], const int* irreps, double* host) {
     return guarded(ctx, [&] {
-        Context* c = from_handle(ctx);
+        Context* c = device_handle(ctx);
         Tensor& T = c->tensor(t);
         int cs;
         const Block& b = block_at(T, alpha, irreps, cs);
@@ -360,7 +373,7 @@ int ccsd_tensor_read_block(ccsd_ctx ctx, ccsd_tensor t, const int alpha[4], cons
 int ccsd_tensor_write(ccsd_ctx ctx, ccsd_tensor t, const int alpha_spin[4], const int* irreps, int64_t n,
                       const int64_t* keys, const double* vals, double alpha, double beta) {
     return guarded(ctx, [&] {
-        Context* c = from_handle(ctx);
+        Context* c = device_handle(ctx);
         Tensor& T = c->tensor(t);
         int cs;
         const Block& b = block_at(T, alpha_spin, irreps, cs);
@@ -389,7 +402,7 @@ int ccsd_tensor_write(ccsd_ctx ctx, ccsd_tensor t, const int alpha_spin[4], cons
 int ccsd_tensor_read(ccsd_ctx ctx, ccsd_tensor t, const int alpha_spin[4], const int* irreps, int64_t n,
                      const int64_t* keys, double* vals) {
     return guarded(ctx, [&] {
-        Context* c = from_handle(ctx);
+        Context* c = device_handle(ctx);
         Tensor& T = c->tensor(t);
         int cs;
         const Block& b = block_at(T, alpha_spin, irreps, cs);
@@ -417,7 +430,7 @@ int ccsd_tensor_read(ccsd_ctx ctx, ccsd_tensor t, const int alpha_spin[4], const
 
 int ccsd_tensor_fill(ccsd_ctx ctx, ccsd_tensor t, double val) {
     return guarded(ctx, [&] {
-        Context* c = from_handle(ctx);
+        Context* c = device_handle(ctx);
         Tensor& T = c->tensor(t);
         kern::fill(T.data, T.total, val, c->stream);
     });
@@ -443,6 +456,7 @@ int ccsd_contract(ccsd_ctx ctx, double alpha, ccsd_tensor A, const char* idxA, c
             auto p = std::make_unique<Plan>(plan_contract(*c, alpha, A, idxA, B, idxB, beta, C, idxC));
             it = c->plan_cache.emplace(key, std::move(p)).first;
         }
+        c->last_plan_flops = it->second->flops();
         c->run(*it->second);
     });
 }
@@ -464,7 +478,7 @@ int ccsd_sum(ccsd_ctx ctx, double alpha, ccsd_tensor A, const char* idxA, double
 
 int ccsd_scale(ccsd_ctx ctx, ccsd_tensor A, double alpha) {
     return guarded(ctx, [&] {
-        Context* c = from_handle(ctx);
+        Context* c = device_handle(ctx);
         Tensor& T = c->tensor(A);
         kern::scale(T.data, T.total, alpha, c->stream);
     });
@@ -472,7 +486,7 @@ int ccsd_scale(ccsd_ctx ctx, ccsd_tensor A, double alpha) {
 
 int ccsd_dot(ccsd_ctx ctx, ccsd_tensor A, const char* idxA, ccsd_tensor B, const char* idxB, double* out) {
     return guarded(ctx, [&] {
-        Context* c = from_handle(ctx);
+        Context* c = device_handle(ctx);
         if (!idxA || !idxB || !out) throw Error(CCSD_ERR_ARG, "null argument");
         std::string key = plan_key("dot", 1.0, A, idxA, B, idxB, 0.0, 0, nullptr, 0);
         auto it = c->plan_cache.find(key);
@@ -489,7 +503,7 @@ int ccsd_dot(ccsd_ctx ctx, ccsd_tensor A, const char* idxA, ccsd_tensor B, const
 // Inside a case each antisymmetric same-spin element counts once (packed semantics).
 int ccsd_norm(ccsd_ctx ctx, ccsd_tensor A, int p, double* out) {
     return guarded(ctx, [&] {
-        Context* c = from_handle(ctx);
+        Context* c = device_handle(ctx);
         if (p != 0 && p != 1 && p != 2) throw Error(CCSD_ERR_ARG, "p must be 0, 1 or 2");
         Tensor& T = c->tensor(A);
         CCSD_CUDA(cudaMemsetAsync(c->d_scalar, 0, sizeof(double), c->stream));
@@ -522,7 +536,7 @@ int ccsd_norm(ccsd_ctx ctx, ccsd_tensor A, int p, double* out) {
 int ccsd_weight(ccsd_ctx ctx, ccsd_tensor A, const double* dvrt_a, const double* dvrt_b, const double* docc_a,
                 const double* docc_b, double shift) {
     return guarded(ctx, [&] {
-        Context* c = from_handle(ctx);
+        Context* c = device_handle(ctx);
         Tensor& T = c->tensor(A);
         const Spaces& S = c->spaces;
         const double* src[2][2] = {{dvrt_a, dvrt_b}, {docc_a, docc_b}};
@@ -564,7 +578,7 @@ int ccsd_hamiltonian_from_factor(ccsd_ctx ctx, int naux, const double* B, const 
                                  const int* aux_per_irrep, int pack_vvvv, ccsd_hamiltonian* H) {
     return guarded(ctx, [&] {
         if (!B || !eps || !H || naux <= 0) throw Error(CCSD_ERR_ARG, "bad factor arguments");
-        build_hamiltonian(*from_handle(ctx), naux, B, eps, aux_per_irrep, pack_vvvv != 0, H);
+        build_hamiltonian(*device_handle(ctx), naux, B, eps, aux_per_irrep, pack_vvvv != 0, H);
     });
 }
 
@@ -581,7 +595,7 @@ int ccsd_hamiltonian_from_integrals(ccsd_ctx ctx, int n, const double* fock, con
                                     ccsd_hamiltonian* H) {
     return guarded(ctx, [&] {
         if (!fock || !eri || !H || n <= 0) throw Error(CCSD_ERR_ARG, "bad integral arguments");
-        Context* c = from_handle(ctx);
+        Context* c = device_handle(ctx);
         if (!c->spaces_set) throw Error(CCSD_ERR_ARG, "set the orbital spaces first");
         build_hamiltonian_dense(*c, n, fock, eri, pack_vvvv != 0, H);
     });
@@ -603,7 +617,7 @@ int ccsd_hamiltonian_from_fcidump(ccsd_ctx ctx, const char* path, int flags, int
                                   double* escf) {
     return guarded(ctx, [&] {
         if (!path || !H) throw Error(CCSD_ERR_ARG, "bad FCIDUMP arguments");
-        Context* c = from_handle(ctx);
+        Context* c = device_handle(ctx);
         Fcidump d = read_fcidump(path, (flags & CCSD_FCIDUMP_FULL_FOCK) != 0, false);
         const int n = d.norb, no = d.nelec / 2, nv = n - no;
         if (!c->tensors.empty()) {
@@ -665,7 +679,7 @@ int ccsd_hamiltonian_from_ao(ccsd_ctx ctx, int nao, int nmo, int nocc, const dou
                              const double* C, int pack_vvvv, ccsd_hamiltonian* H, double* e_elec) {
     return guarded(ctx, [&] {
         if (!hcore || !eri_ao || !C || !H) throw Error(CCSD_ERR_ARG, "bad AO arguments");
-        Context* c = from_handle(ctx);
+        Context* c = device_handle(ctx);
         set_closed_shell_spaces(ctx, c, nmo, nocc);
         MoIntegrals mo(*c, nao, nmo, nocc, hcore, eri_ao, C);
         build_hamiltonian_device(*c, nmo, mo.fock.data(), mo.d, pack_vvvv != 0, H);
@@ -677,7 +691,7 @@ int ccsd_rhf_hamiltonian_from_ao(ccsd_ctx ctx, int nao, int nmo, int nocc, const
                                  const double* eri_ao, const double* C, ccsd_rhf_hamiltonian* H, double* e_elec) {
     return guarded(ctx, [&] {
         if (!hcore || !eri_ao || !C || !H) throw Error(CCSD_ERR_ARG, "bad AO arguments");
-        Context* c = from_handle(ctx);
+        Context* c = device_handle(ctx);
         set_closed_shell_spaces(ctx, c, nmo, nocc);
         MoIntegrals mo(*c, nao, nmo, nocc, hcore, eri_ao, C);
         build_rhf_hamiltonian_device(*c, nmo, mo.fock.data(), mo.d, H);
@@ -701,7 +715,7 @@ int ccsd_rhf_hamiltonian_from_factor(ccsd_ctx ctx, int naux, const double* B, co
                                      const int* aux_per_irrep, ccsd_rhf_hamiltonian* H) {
     return guarded(ctx, [&] {
         if (!B || !eps || !H || naux <= 0) throw Error(CCSD_ERR_ARG, "bad factor arguments");
-        Context* c = from_handle(ctx);
+        Context* c = device_handle(ctx);
         if (!c->spaces_set) throw Error(CCSD_ERR_ARG, "set the orbital spaces first");
         build_rhf_hamiltonian(*c, naux, B, eps, aux_per_irrep, H);
     });
@@ -711,7 +725,7 @@ int ccsd_rhf_hamiltonian_from_integrals(ccsd_ctx ctx, int n, const double* fock,
                                         ccsd_rhf_hamiltonian* H) {
     return guarded(ctx, [&] {
         if (!fock || !eri || !H || n <= 0) throw Error(CCSD_ERR_ARG, "bad integral arguments");
-        Context* c = from_handle(ctx);
+        Context* c = device_handle(ctx);
         if (!c->spaces_set) throw Error(CCSD_ERR_ARG, "set the orbital spaces first");
         build_rhf_hamiltonian_dense(*c, n, fock, eri, H);
     });
@@ -734,7 +748,7 @@ int ccsd_rhf_solver_create(ccsd_ctx ctx, const ccsd_rhf_hamiltonian* H, const cc
     *out = nullptr;
     return guarded(ctx, [&] {
         if (!H) throw Error(CCSD_ERR_ARG, "null hamiltonian");
-        Context* c = from_handle(ctx);
+        Context* c = device_handle(ctx);
         ccsd_options o;
         options_default(&o);
         if (opts) o = *opts;
@@ -834,7 +848,7 @@ int ccsd_solver_create(ccsd_ctx ctx, const ccsd_hamiltonian* H, const ccsd_optio
     if (!out) return CCSD_ERR_ARG;
     *out = nullptr;
     return guarded(ctx, [&] {
-        Context* c = from_handle(ctx);
+        Context* c = device_handle(ctx);
         ccsd_options o;
         options_default(&o);
         if (opts) o = *opts;

@@ -925,6 +925,7 @@ void Context::launch(Plan& p, const GemmLaunch& l, const std::string& label, dou
 
 void Context::run(Plan& p, double* scalar_out, double* dot_target) {
     upload(p);
+    if (host_only) return;   // planning only: account the tables, launch nothing
     bool zeroed = dot_target != nullptr;
     double* acc = dot_target ? dot_target : d_scalar;
     RunSchedule* rs = host_only ? nullptr : &schedule(p);

@@ -247,6 +247,7 @@ public:
     int slices = 0;
     bool plan_refine = false;          // host-only plan of a split solve that may move to 4 slices
     int plan_threads = 8;              // host threads that plan the statements of an iteration
+    double last_plan_flops = 0;        // algorithmic flops of the last ccsd_contract statement
     int split_routing = CCSD_SPLIT_ROUTE_AUTO;  // which contractions take the split kernel
     bool fp64_tiled_only = false;      // keep skinny FP64 products on the tiled kernel
     bool group_gemms = true;           // batch small block contractions of a statement into grouped launches

@@ -79,8 +79,14 @@ enum {
 };
 
 /* ---- context ------------------------------------------------------------ */
-/* stream: a cudaStream_t, or NULL to let the context create its own */
+/* stream: a cudaStream_t, or NULL to let the context create its own.  device < 0 makes a
+ * planning-only context (no GPU needed): tensors are created and contractions planned and
+ * accounted (ccsd_ctx_device_bytes, ccsd_ctx_plan_flops), nothing is launched, and calls
+ * that read or write tensor data fail with CCSD_ERR_UNSUPPORTED. */
 int ccsd_ctx_create(int device, void* stream, ccsd_ctx* out);
+/* algorithmic flops of the last ccsd_contract statement, as the planner counts them
+ * (block products 2*M*N*K, packed pairs counted once) */
+int ccsd_ctx_plan_flops(ccsd_ctx ctx, double* flops);
 int ccsd_ctx_destroy(ccsd_ctx ctx);
 const char* ccsd_last_error(ccsd_ctx ctx);
 int ccsd_ctx_synchronize(ccsd_ctx ctx);
