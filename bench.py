@@ -258,6 +258,21 @@ def run_serve(args):
     return 0
 
 
+def max_over_ranks(ms, dist, device="cuda"):
+    """The job's time is the slowest rank's (replicas time the same steps)."""
+    if not dist:
+        return ms
+    import torch
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world, steps, ms_max):
+    """Iterations per second of the whole job: every replica did `steps` iterations."""
+    return world * steps / (ms_max * 1e-3)
+
+
 def timed_iterations(torch, ctx, s, stream, steps, warmup, profile):
     for _ in range(warmup):
         s.iterate()
@@ -459,10 +474,7 @@ def main():
             torch.cuda.synchronize()
             ms, launches, prof, e, c = timed_iterations(torch, ctx, s, stream, args.steps, args.warmup, True)
             torch.cuda.synchronize()
-        if dist:
-            t = torch.tensor([ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, dist)
         results[p] = dict(ms=ms, launches=launches, prof=prof, energy=e, conv=c, flops=flops,
                           clocks=clk.summary(), energies=None)
         log(f"[bench] {p}: {ms / args.steps:.1f} ms/iter, E={e:.12f}, conv={c:.3e}, launches={launches}")
@@ -474,7 +486,7 @@ def main():
         s.close()
     head = results[prec]
     ms_step = head["ms"] / args.steps
-    value = world * args.steps / (head["ms"] * 1e-3)
+    value = whole_job_rate(world, args.steps, head["ms"])
 
     # roofline of the dominant kernel (the particle-ladder contraction)
     lad = head["prof"].get(LADDER, {"ms": 0, "flops": 0, "launches": 0})
