@@ -29,7 +29,7 @@ def _rank(rank, world, port, out):
 
 def test_two_replicas_take_the_slowest_rank():
     world, port = 2, _free_port()
-    out = mp.Manager().dict()
+    out = mp.get_context("spawn").Manager().dict()
     mp.spawn(_rank, args=(world, port, out), nprocs=world, join=True)
     for r in range(world):
         m, rate = out[r]
