@@ -4,7 +4,7 @@ Reads, from a checkout of the reference (path given as the first argument):
   * test/input.aq     -- the sections whose CCSD energy the reference checks
                          (h2o-pvdz: lines 1-24, ch2-pvdz: lines 47-71): geometry (bohr),
                          multiplicity, basis-set name and the compared SCF / MP2 / CCSD
-                         energies with their tolerance;
+                         and Lambda-CCSD energies with their tolerance;
   * basis/<name>      -- the contracted shells of every element used.
 Writes a small JSON fixture so that the tests never read the reference at run time.
 
@@ -23,7 +23,7 @@ sys.path.insert(0, str(HERE.parent.parent))
 from oracle import scf  # noqa: E402
 
 SECTIONS = ["h2o-pvdz", "ch2-pvdz"]
-KEYS = {"localaoscf:energy": "scf", "ccsd:mp2": "mp2", "ccsd:energy": "ccsd"}
+KEYS = {"localaoscf:energy": "scf", "ccsd:mp2": "mp2", "ccsd:energy": "ccsd", "lambdaccsd:energy": "lambda"}
 
 
 def parse_sections(text):

@@ -68,3 +68,37 @@ def test_diis_coefficients_sum_to_one(built_lib):
         n = sum(x is not None for x in c.diis.old_dx)
         if n > 1:
             assert abs(c.diis.c[:n].sum() - 1.0) < 1e-10
+
+
+def test_implicit_antisymmetrisation_helper():
+    """The general helper of the Hbar/Lambda oracle gives the CCSD oracle's explicit
+    P(ab)P(ij) forms: Tau and the ring term P(ab)P(ij) W_amei t_ebjm."""
+    from oracle import lambda_ccsd as LC
+    rng = np.random.default_rng(5)
+    v, o = 6, 4
+    T1 = rng.standard_normal((v, o))
+    T2 = rng.standard_normal((v, v, o, o))
+    T2 = T2 - T2.transpose(1, 0, 2, 3)
+    T2 = T2 - T2.transpose(0, 1, 3, 2)
+    W = rng.standard_normal((v, o, v, o))
+    tau = O.CCSD.make_tau(O.Amplitudes(T1, T2))
+    assert np.abs(T2 + LC.contract(0.5, T1, "ai", T1, "bj", "abij", LC.SHAPES["abij"]) - tau).max() < 1e-14
+    ring = O.P23(O.P01(np.einsum("amei,ebjm->abij", W, T2)))
+    assert np.abs(LC.contract(1.0, W, "amei", T2, "ebjm", "abij", LC.SHAPES["abij"]) - ring).max() < 1e-13
+
+
+def test_hbar_without_amplitudes_is_the_bare_hamiltonian(built_lib):
+    """With T = 0 every Hbar block is the bare block, except those the isHbar form
+    assigns: the occupied-virtual Fock block and <ab||ij> and f_ai set to zero."""
+    from oracle import lambda_ccsd as LC
+    F, eri = _problem(4, 3, 5)
+    H = O.Hamiltonian(F, eri, 3, ladder_literal=True)
+    T1 = np.zeros_like(H.fAI)
+    T2 = np.zeros_like(H.VABIJ)
+    X = LC.hbar(H, T1, T2)
+    bare = {"ij": H.fMI, "ab": H.fAE, "ijkl": H.VMNIJ, "aijk": H.VAMIJ, "ijak": H.VMNEJ, "ijab": H.VMNEF,
+            "aibj": H.VAMEI, "aibc": H.VAMEF, "abci": H.VABEJ, "abcd": H.VABEF}
+    for k, b in bare.items():
+        assert np.array_equal(X[k], b), k
+    for k in ("ia", "ai", "abij"):
+        assert not X[k].any(), k

@@ -1,7 +1,7 @@
 """The CPU oracle against the reference's own end-to-end known answers.
 
 test/input.aq:1-24 (H2O/cc-pVDZ, closed shell) and test/input.aq:47-71 (CH2/cc-pVDZ,
-triplet, UHF) compare the SCF, MP2 and CCSD energies to 1e-9 Eh.  The fixture
+triplet, UHF) compare the SCF, MP2, CCSD and Lambda-CCSD energies to 1e-9 Eh.  The fixture
 (tests/golden/molecules.json) holds the geometries, basis sets and those energies;
 the integrals, the SCF and the CCSD iterations are the oracle's own.
 """
@@ -12,6 +12,7 @@ import numpy as np
 import pytest
 
 from oracle import ccsd_oracle as O
+from oracle import lambda_ccsd as LC
 from oracle import scf
 
 FIXTURE = json.loads((Path(__file__).parent / "golden" / "molecules.json").read_text())
@@ -38,6 +39,23 @@ def test_mp2_and_ccsd_energies(system):
     e = cc.run(conv_tol=1e-11, max_iter=100)
     assert cc.conv < 1e-11
     assert abs(e - known["ccsd"]) < known["tolerance"], (e, known["ccsd"])
+
+
+def test_lambda_energy(system):
+    """Hbar of the converged T (st2eoperator.hpp, isHbar) and the Lambda iteration
+    (lambdaccsd.cxx): 1/4 <mn||ef> l_mn^ef at convergence."""
+    name, res, Hso = system
+    known = FIXTURE["molecules"][name]["known"]
+    cc = O.CCSD(Hso, diis_order=5)
+    cc.run(conv_tol=1e-11, max_iter=100)
+    Hb, lam = LC.lambda_from_ccsd(cc)
+    e = lam.run(conv_tol=1e-11, max_iter=100)
+    assert lam.conv < 1e-11
+    assert abs(e - known["lambda"]) < known["tolerance"], (e, known["lambda"])
+    # L2 keeps the antisymmetry of its upper and lower pairs
+    L2 = lam.L.T2
+    assert np.abs(L2 + L2.transpose(1, 0, 2, 3)).max() < 1e-13
+    assert np.abs(L2 + L2.transpose(0, 1, 3, 2)).max() < 1e-13
 
 
 def test_spin_orbital_hamiltonian_symmetries(system):
