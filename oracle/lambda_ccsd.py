@@ -13,8 +13,11 @@ It restates, statement for statement and in the reference's order:
   residual, weight, update, energy, convergence
   and DIIS:                                       src/cc/lambdaccsd.cxx:27-133
 * weight and norm of a de-excitation operator
-  (same denominators and dot weights 1, 1/4 as
-  the excitation operator):                       src/operator/deexcitationoperator.hpp:63-102
+  (dot weights 1, 1/4 as the excitation
+  operator):                                      src/operator/deexcitationoperator.hpp:63-102
+* denominators from the diagonals of Hbar's
+  F_ae and F_mi (Denominator of H = Hbar):        src/cc/lambdaccsd.cxx:40,
+                                                  src/operator/denominator.hpp:22-73
 
 Every statement is an einsum over the full index ranges with the written factor, followed
 by the implicit antisymmetrisation of output lines that come from both factors, separately
@@ -155,8 +158,10 @@ def hbar(H, T1, T2):
 class LambdaCCSD:
     """LambdaCCSD::run / iterate (lambdaccsd.cxx:27-133) on an Hbar from hbar()."""
 
-    def __init__(self, Hb, T1, T2, dv, do, diis_order=5, diis_start=1):
+    def __init__(self, Hb, T1, T2, diis_order=5, diis_start=1):
         self.Hb, self.T1, self.T2 = Hb, T1, T2
+        dv = -np.diag(Hb["ab"]).copy()
+        do = np.diag(Hb["ij"]).copy()
         self.D1 = do[:, None] + dv[None, :]                                      # [i, a]
         self.D2 = (do[:, None, None, None] + do[None, :, None, None]
                    + dv[None, None, :, None] + dv[None, None, None, :])         # [i, j, a, b]
@@ -224,4 +229,4 @@ class LambdaCCSD:
 def lambda_from_ccsd(cc, diis_order=5):
     """Hbar of a converged ccsd_oracle.CCSD and a Lambda solver on it."""
     Hb = hbar(cc.H, cc.T.T1, cc.T.T2)
-    return Hb, LambdaCCSD(Hb, cc.T.T1, cc.T.T2, cc.H.dv, cc.H.do, diis_order=diis_order)
+    return Hb, LambdaCCSD(Hb, cc.T.T1, cc.T.T2, diis_order=diis_order)
