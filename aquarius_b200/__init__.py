@@ -52,7 +52,8 @@ EXPORTS = [
     "ccsd_server_poll", "ccsd_server_wait", "ccsd_server_stats", "ccsd_server_destroy", "ccsd_solver_mode",
     "ccsd_rhf_hamiltonian_from_factor", "ccsd_rhf_hamiltonian_from_integrals", "ccsd_rhf_hamiltonian_destroy",
     "ccsd_rhf_solver_create", "ccsd_rhf_plan_query", "ccsd_hamiltonian_from_ao", "ccsd_rhf_hamiltonian_from_ao",
-    "ccsd_rhf_solver_hbar", "ccsd_ctx_plan_flops",
+    "ccsd_rhf_solver_hbar", "ccsd_ctx_plan_flops", "ccsd_solver_hbar", "ccsd_lambda_solver_create",
+    "ccsd_lambda_plan_query",
 ]
 
 
@@ -197,6 +198,9 @@ def lib():
             "ccsd_rhf_hamiltonian_destroy": [vp, P(RHFHamiltonian)],
             "ccsd_rhf_solver_create": [vp, P(RHFHamiltonian), P(Options), P(vp)],
             "ccsd_rhf_solver_hbar": [vp, P(RHFHbar)],
+            "ccsd_solver_hbar": [vp, P(Hamiltonian)],
+            "ccsd_lambda_solver_create": [vp, P(Hamiltonian), vp, P(Options), P(vp)],
+            "ccsd_lambda_plan_query": [ctypes.c_int, vp, vp, P(Options), P(dbl), P(dbl), P(i64)],
             "ccsd_hamiltonian_from_ao": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp, ctypes.c_int,
                                          P(Hamiltonian), P(dbl)],
             "ccsd_rhf_hamiltonian_from_ao": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp,
@@ -275,6 +279,20 @@ def plan_query(vrt, occ, diis_order=8, pack_vvvv=True, precision="fp64"):
     _check(lib().ccsd_plan_query(len(vrt), _ptr(vrt), _ptr(occ), ctypes.byref(o), 1 if pack_vvvv else 0,
                                  ctypes.byref(fl), ctypes.byref(by)))
     return fl.value, by.value
+
+
+def lambda_plan_query(vrt, occ, diis_order=8, precision="fp64"):
+    """Host-only planning of CCSD + Hbar + Lambda-CCSD (unpacked <ab||ef>): (flops of forming
+    Hbar, flops per Lambda iteration, peak device bytes)."""
+    vrt, occ = _ints(vrt), _ints(occ)
+    o = Options()
+    lib().ccsd_options_default(ctypes.byref(o))
+    o.diis_order = diis_order
+    o.precision = PREC[precision]
+    hf, fl, by = ctypes.c_double(), ctypes.c_double(), ctypes.c_int64()
+    _check(lib().ccsd_lambda_plan_query(len(vrt), _ptr(vrt), _ptr(occ), ctypes.byref(o), ctypes.byref(hf),
+                                        ctypes.byref(fl), ctypes.byref(by)))
+    return hf.value, fl.value, by.value
 
 
 def rhf_plan_query(vrt, occ, diis_order=8, precision="fp64", refine_tol=0.0):
@@ -759,26 +777,46 @@ class RHFHamiltonianHandle:
             _check(lib().ccsd_rhf_hamiltonian_destroy(self.ctx.c, ctypes.byref(self.H)), self.ctx.c)
 
 
+def _options(conv_tol=1e-9, max_iter=50, diis_order=5, diis_start=1, precision="fp64", slices=0,
+             use_graph=False, refine_tol=0.0):
+    o = Options()
+    lib().ccsd_options_default(ctypes.byref(o))
+    o.conv_tol, o.max_iter, o.diis_order, o.diis_start = conv_tol, max_iter, diis_order, diis_start
+    o.precision, o.slices, o.use_graph = PREC[precision], slices, 1 if use_graph else 0
+    o.refine_tol = refine_tol
+    return o
+
+
+class HbarHandle:
+    """Spin-orbital Hbar blocks (ccsd_solver_hbar), keyed like the H blocks; owned by the
+    CCSD solver that formed them."""
+
+    def __init__(self, ctx, H):
+        self.ctx, self.H = ctx, H
+        self.tensors = {f: Tensor(ctx, getattr(H, f), f, *H_SHAPES[f]) for f in H_FIELDS}
+
+    def __getitem__(self, name):
+        return self.tensors[name]
+
+
 class Solver:
     """CCSD solver over a spin-orbital H (CCSD) or a closed-shell spatial H (RHFCCSD)."""
 
-    def __init__(self, ctx, H, conv_tol=1e-9, max_iter=50, diis_order=5, diis_start=1,
-                 precision="fp64", slices=0, use_graph=False, refine_tol=0.0):
+    def __init__(self, ctx, H, **kw):
         self.ctx = ctx
-        o = Options()
-        lib().ccsd_options_default(ctypes.byref(o))
-        o.conv_tol, o.max_iter, o.diis_order, o.diis_start = conv_tol, max_iter, diis_order, diis_start
-        o.precision, o.slices, o.use_graph = PREC[precision], slices, 1 if use_graph else 0
-        o.refine_tol = refine_tol
+        o = _options(**kw)
         s = ctypes.c_void_p()
         self.rhf = isinstance(H, RHFHamiltonianHandle)
         create = lib().ccsd_rhf_solver_create if self.rhf else lib().ccsd_solver_create
         _check(create(ctx.c, ctypes.byref(H.H), ctypes.byref(o), ctypes.byref(s)), ctx.c)
         self.s = s
+        self._amplitudes(((1, 0), (0, 1)), ((2, 0), (0, 2)), "T")
+
+    def _amplitudes(self, shape1, shape2, name):
         t1, t2 = ctypes.c_int32(), ctypes.c_int32()
-        _check(lib().ccsd_solver_amplitudes(s, ctypes.byref(t1), ctypes.byref(t2)), ctx.c)
-        self.T1 = Tensor(ctx, t1.value, "T1", (1, 0), (0, 1), plain=self.rhf)
-        self.T2 = Tensor(ctx, t2.value, "T2", (2, 0), (0, 2), plain=self.rhf)
+        _check(lib().ccsd_solver_amplitudes(self.s, ctypes.byref(t1), ctypes.byref(t2)), self.ctx.c)
+        self.T1 = Tensor(self.ctx, t1.value, name + "1", *shape1, plain=self.rhf)
+        self.T2 = Tensor(self.ctx, t2.value, name + "2", *shape2, plain=self.rhf)
 
     def close(self):
         if self.s:
@@ -824,11 +862,39 @@ class Solver:
         return x.value
 
     def hbar(self):
-        """Closed-shell solver: the Hbar intermediates from the current amplitudes (dict of
-        plain tensors owned by the solver)."""
+        """Hbar from the current amplitudes, as tensors owned by the solver.  Closed-shell
+        solver: dict of the RHF intermediates (rhfccsd.cxx:110-186).  Spin-orbital solver: an
+        HbarHandle with the 13 blocks of STTwoElectronOperator(H, T, isHbar)."""
+        if not self.rhf:
+            h = Hamiltonian()
+            _check(lib().ccsd_solver_hbar(self.s, ctypes.byref(h)), self.ctx.c)
+            return HbarHandle(self.ctx, h)
         h = RHFHbar()
         _check(lib().ccsd_rhf_solver_hbar(self.s, ctypes.byref(h)), self.ctx.c)
         return {f: Tensor(self.ctx, getattr(h, f), f, *HBAR_SHAPES[f], plain=True) for f in HBAR_SHAPES}
+
+    def lambda_solver(self, hbar=None, **kw):
+        """Lambda-CCSD on `hbar` (default: this solver's Hbar, formed now) and this solver's T."""
+        return LambdaSolver(self, self.hbar() if hbar is None else hbar, **kw)
+
+
+class LambdaSolver(Solver):
+    """Lambda-CCSD (LambdaCCSD, lambdaccsd.cxx) on an Hbar and a spin-orbital CCSD solver's
+    amplitudes.  L1 is [i, a] and L2 [i, j, a, b]; energy() is 1/4 <mn||ef> l_mn^ef."""
+
+    def __init__(self, ccsd, hbar, **kw):
+        self.ctx, self.rhf = ccsd.ctx, False
+        self.ccsd, self.hbar_blocks = ccsd, hbar
+        o = _options(**kw)
+        s = ctypes.c_void_p()
+        _check(lib().ccsd_lambda_solver_create(self.ctx.c, ctypes.byref(hbar.H), ccsd.s, ctypes.byref(o),
+                                               ctypes.byref(s)), self.ctx.c)
+        self.s = s
+        self._amplitudes(((0, 1), (1, 0)), ((0, 2), (2, 0)), "L")
+        self.L1, self.L2 = self.T1, self.T2
+
+    def hbar(self):
+        raise CcsdError(9, "a Lambda solver forms no Hbar")
 
 
 class Server:

@@ -844,10 +844,32 @@ int ccsd_plan_query(int nirrep, const int* vrt, const int* occ, const ccsd_optio
     });
 }
 
+int ccsd_lambda_plan_query(int nirrep, const int* vrt, const int* occ, const ccsd_options* opts,
+                           double* hbar_flops, double* flops_per_iter, int64_t* device_bytes) {
+    return guarded(nullptr, [&] {
+        Context host(-1, nullptr);
+        int n = 0;
+        host.spaces = query_spaces(nirrep, vrt, occ, n);
+        host.spaces_set = true;
+        ccsd_hamiltonian H;
+        create_hamiltonian_tensors(host, false, &H);
+        ccsd_options o;
+        options_default(&o);
+        if (opts) o = *opts;
+        Solver cc(host, H, o);
+        cc.hbar_so();
+        Solver lam(host, cc, cc.HB, o);
+        if (hbar_flops) *hbar_flops = cc.hbar_plan.flops();
+        if (flops_per_iter) *flops_per_iter = lam.flops_per_iter;
+        if (device_bytes) *device_bytes = host.peak_bytes;
+    });
+}
+
 int ccsd_solver_create(ccsd_ctx ctx, const ccsd_hamiltonian* H, const ccsd_options* opts, ccsd_solver* out) {
     if (!out) return CCSD_ERR_ARG;
     *out = nullptr;
     return guarded(ctx, [&] {
+        if (!H) throw Error(CCSD_ERR_ARG, "null hamiltonian");
         Context* c = device_handle(ctx);
         ccsd_options o;
         options_default(&o);
@@ -866,8 +888,37 @@ int ccsd_solver_create(ccsd_ctx ctx, const ccsd_hamiltonian* H, const ccsd_optio
     });
 }
 
+int ccsd_lambda_solver_create(ccsd_ctx ctx, const ccsd_hamiltonian* hbar, ccsd_solver ccsd, const ccsd_options* opts,
+                              ccsd_solver* out) {
+    if (!out) return CCSD_ERR_ARG;
+    *out = nullptr;
+    return guarded(ctx, [&] {
+        if (!hbar || !ccsd || !ccsd->s) throw Error(CCSD_ERR_ARG, "null Hbar or CCSD solver");
+        Context* c = device_handle(ctx);
+        if (ccsd->ctx != ctx) throw Error(CCSD_ERR_ARG, "the CCSD solver belongs to another context");
+        ccsd_options o;
+        options_default(&o);
+        if (opts) o = *opts;
+        if (o.precision != CCSD_PREC_FP64 && !kern::split_supported())
+            throw Error(CCSD_ERR_UNSUPPORTED, "split GEMMs need an sm_100 device");
+        auto* h = new ccsd_solver_s;
+        h->ctx = ctx;
+        try {
+            h->s = new Solver(*c, *ccsd->s, *hbar, o);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
 int ccsd_solver_destroy(ccsd_solver s) {
     if (!s) return CCSD_ERR_ARG;
+    if (s->s && s->s->lambda_users > 0)
+        return guarded(s->ctx, [&] {
+            throw Error(CCSD_ERR_ARG, "a Lambda solver still reads this solver's amplitudes and Hbar: destroy it first");
+        });
     int st = guarded(s->ctx, [&] { delete s->s; });
     delete s;
     return st;
@@ -927,6 +978,14 @@ int ccsd_rhf_solver_hbar(ccsd_solver s, ccsd_rhf_hbar* out) {
         out->WAMIE = v.WAMIE;
         out->WAMEI = v.WAMEI;
         out->WABEJ = v.WABEJ;
+    });
+}
+
+int ccsd_solver_hbar(ccsd_solver s, ccsd_hamiltonian* out) {
+    if (!s || !out) return CCSD_ERR_ARG;
+    return guarded(s->ctx, [&] {
+        s->s->hbar_so();
+        *out = s->s->HB;
     });
 }
 

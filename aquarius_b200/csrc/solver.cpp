@@ -80,6 +80,46 @@ Solver::Solver(Context& c, const ccsd_rhf_hamiltonian& h, const ccsd_options& o)
     setup();
 }
 
+// LambdaCCSD<U>::run (lambdaccsd.cxx:27-58): L(1), L(2) in the reference's layout (upper
+// occupied, lower virtual), Z of the same shapes and the two G intermediates.  The Hbar
+// blocks take the place of H, so the denominators come from the diagonals of its F(ae) and
+// F(mi), as Denominator(Hbar) reads them (denominator.hpp:22-73).
+Solver::Solver(Context& c, Solver& ccsd, const ccsd_hamiltonian& hbar, const ccsd_options& o)
+    : ctx(c), H(hbar), opts(o), lambda(true), source(&ccsd) {
+    if (ccsd.rhf || ccsd.lambda) throw Error(CCSD_ERR_ARG, "Lambda-CCSD needs a spin-orbital CCSD solver");
+    if (&ccsd.ctx != &ctx) throw Error(CCSD_ERR_ARG, "the CCSD solver belongs to another context");
+    struct Want {
+        int h;
+        int o0, o1, i0, i1;
+        const char* name;
+    };
+    const Want want[] = {{H.fAI, 1, 0, 0, 1, "fAI"},     {H.fME, 0, 1, 1, 0, "fME"},     {H.fAE, 1, 0, 1, 0, "fAE"},
+                         {H.fMI, 0, 1, 0, 1, "fMI"},     {H.VMNIJ, 0, 2, 0, 2, "VMNIJ"}, {H.VAMIJ, 1, 1, 0, 2, "VAMIJ"},
+                         {H.VMNEJ, 0, 2, 1, 1, "VMNEJ"}, {H.VABIJ, 2, 0, 0, 2, "VABIJ"}, {H.VMNEF, 0, 2, 2, 0, "VMNEF"},
+                         {H.VAMEI, 1, 1, 1, 1, "VAMEI"}, {H.VAMEF, 1, 1, 2, 0, "VAMEF"}, {H.VABEJ, 2, 0, 1, 1, "VABEJ"},
+                         {H.VABEF, 2, 0, 2, 0, "VABEF"}};
+    for (const Want& w : want) {
+        if (!ctx.tensors.count(w.h)) throw Error(CCSD_ERR_ARG, std::string("Hbar block ") + w.name + " is not a tensor");
+        const Tensor& t = ctx.tensor(w.h);
+        if (t.plain() || t.nout[0] != w.o0 || t.nout[1] != w.o1 || t.nin[0] != w.i0 || t.nin[1] != w.i1)
+            throw Error(CCSD_ERR_ARG, std::string("Hbar block ") + w.name + " has the wrong shape");
+    }
+    T1 = mk(ctx, "L(1)", 0, 1, 1, 0);
+    T2 = mk(ctx, "L(2)", 0, 2, 2, 0);
+    Z1 = mk(ctx, "Z(1)", 0, 1, 1, 0);
+    Z2 = mk(ctx, "Z(2)", 0, 2, 2, 0);
+    GIM = mk(ctx, "G(im)", 0, 1, 0, 1);
+    GEA = mk(ctx, "G(ea)", 1, 0, 1, 0);
+    source->lambda_users++;
+    try {
+        setup();
+    } catch (...) {
+        source->lambda_users--;
+        source = nullptr;
+        throw;
+    }
+}
+
 std::vector<int> Solver::constants() const {
     if (rhf)
         return {HR.fAI, HR.fAB, HR.fIJ, HR.VABCD, HR.VABCI, HR.VABIJ, HR.VAIBJ, HR.VAIJB, HR.VAIJK, HR.VIJKL,
@@ -92,6 +132,11 @@ std::vector<int> Solver::owned_tensors() const {
     if (rhf)
         for (int x : {T2SA, TauSA, VABIJSA, VAIJBSA, WAMIE, WMNIJc, Z2c}) t.push_back(x);
     if (WABEJ) t.push_back(WABEJ);
+    for (int x : {GIM, GEA}) t.push_back(x);
+    if (hbar_formed)
+        for (int x : {HB.fAI, HB.fME, HB.fAE, HB.fMI, HB.VMNIJ, HB.VAMIJ, HB.VMNEJ, HB.VABIJ, HB.VMNEF, HB.VAMEI,
+                      HB.VAMEF, HB.VABEJ, HB.VABEF})
+            t.push_back(x);
     return t;
 }
 
@@ -116,9 +161,10 @@ void Solver::setup() {
             for (int s = 0; s < 2; s++) den[sp][s] = (double*)alloc(std::max(ctx.spaces.total(sp, s), 1) * sizeof(double));
         build_diis();
         d_red = (double*)alloc(8 * sizeof(double));
-        record_tau(tau_plan);
+        if (!lambda) record_tau(tau_plan);
         record_energy(energy_plan);
         if (rhf) record_iteration_rhf();
+        else if (lambda) record_iteration_lambda();
         else record_iteration();
         ctx.upload(iter_plan);
         ctx.upload(tau_plan);
@@ -145,7 +191,12 @@ void Solver::setup() {
         Plan init;
         Recorder r{&ctx, &init};
         TensorRef t1{&r, T1}, t2{&r, T2};
-        if (rhf) {
+        if (lambda) {
+            // L(0) = 1, L(1)[ia] = T(1)[ai], L(2)[ijab] = T(2)[abij]  (lambdaccsd.cxx:52-55)
+            TensorRef s1{&r, source->T1}, s2{&r, source->T2};
+            t1["ia"] = s1["ai"];
+            t2["ijab"] = s2["abij"];
+        } else if (rhf) {
             TensorRef fai{&r, HR.fAI}, vabij{&r, HR.VABIJ}, vaijb{&r, HR.VAIJB}, vaibj{&r, HR.VAIBJ};
             TensorRef sa{&r, VABIJSA}, sb{&r, VAIJBSA};
             t1["ai"] = fai["ai"];
@@ -160,12 +211,14 @@ void Solver::setup() {
             t2["abij"] = vabij["abij"];
         }
         ctx.run(init);
-        weight_tensor(T1);
-        weight_tensor(T2);
+        if (!lambda) {
+            weight_tensor(T1);
+            weight_tensor(T2);
+        }
     }
-    record_tau(tau_plan);
+    if (!lambda) record_tau(tau_plan);
     record_energy(energy_plan);
-    build_tau_blocks();
+    if (!lambda) build_tau_blocks();
     build_update();
     launch_tau();
     CCSD_CUDA(cudaMemsetAsync(d_red, 0, sizeof(double), ctx.stream));
@@ -177,6 +230,7 @@ void Solver::setup() {
     conv = std::numeric_limits<double>::max();
 
     if (rhf) record_iteration_rhf();
+    else if (lambda) record_iteration_lambda();
     else record_iteration();
     ctx.upload(iter_plan);
     ctx.upload(tau_plan);
@@ -185,6 +239,7 @@ void Solver::setup() {
 }
 
 Solver::~Solver() {
+    if (source) source->lambda_users--;
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
     ctx.release(iter_plan);
@@ -377,6 +432,13 @@ void Solver::record_energy(Plan& p) {
         for (auto& d : a.dots) d.alpha *= 2.0;
         Plan b = plan_dot(ctx, VABIJSA, "abij", Tau, "abij");
         p.append(std::move(a));
+        p.append(std::move(b));
+        return;
+    }
+    if (lambda) {
+        // energy = 1/4 <WMNEF|L(2)>  (lambdaccsd.cxx:129)
+        Plan b = plan_dot(ctx, H.VMNEF, "ijab", T2, "ijab");
+        for (auto& d : b.dots) d.alpha *= 0.25;
         p.append(std::move(b));
         return;
     }
@@ -629,6 +691,150 @@ void Solver::hbar_rhf() {
         run_deferred(r);
         ctx.upload(hbar_plan);
     }
+    ctx.run(hbar_plan);
+    CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
+}
+
+// LambdaCCSD<U>::iterate (lambdaccsd.cxx:60-133): the G intermediates and the residual,
+// statement for statement; weight, update, energy, norm and DIIS are the shared driver's.
+void Solver::record_iteration_lambda() {
+    Plan& p = iter_plan;
+    std::vector<std::function<Plan()>> jobs;
+    Recorder r{&ctx, &p, &jobs};
+    TensorRef FME{&r, H.fME}, FAE{&r, H.fAE}, FMI{&r, H.fMI}, WMNEF{&r, H.VMNEF}, WAMEF{&r, H.VAMEF};
+    TensorRef WABEJ{&r, H.VABEJ}, WABEF{&r, H.VABEF}, WMNIJ{&r, H.VMNIJ}, WMNEJ{&r, H.VMNEJ};
+    TensorRef WAMIJ{&r, H.VAMIJ}, WAMEI{&r, H.VAMEI};
+    TensorRef T2r{&r, source->T2}, L1{&r, T1}, L2{&r, T2}, Z1r{&r, Z1}, Z2r{&r, Z2};
+    TensorRef GIMr{&r, GIM}, GEAr{&r, GEA};
+
+    GIMr["mn"] = 0.5 * T2r["efno"] * L2["moef"];
+    GEAr["ef"] = -0.5 * T2r["egmn"] * L2["mnfg"];
+
+    Z1r["ia"] = FME["ia"];
+    Z1r["ia"] += FAE["ea"] * L1["ie"];
+    Z1r["ia"] -= FMI["im"] * L1["ma"];
+    Z1r["ia"] -= WAMEI["eiam"] * L1["me"];
+    Z1r["ia"] += 0.5 * WABEJ["efam"] * L2["imef"];
+    Z1r["ia"] -= 0.5 * WAMIJ["eimn"] * L2["mnea"];
+    Z1r["ia"] -= WMNEJ["inam"] * GIMr["mn"];
+    Z1r["ia"] -= WAMEF["fiea"] * GEAr["ef"];
+
+    Z2r["ijab"] = WMNEF["ijab"];
+    Z2r["ijab"] += FME["ia"] * L1["jb"];
+    Z2r["ijab"] += WAMEF["ejab"] * L1["ie"];
+    Z2r["ijab"] -= WMNEJ["ijam"] * L1["mb"];
+    Z2r["ijab"] += FAE["ea"] * L2["ijeb"];
+    Z2r["ijab"] -= FMI["im"] * L2["mjab"];
+    Z2r["ijab"] += 0.5 * WABEF["efab"] * L2["ijef"];
+    Z2r["ijab"] += 0.5 * WMNIJ["ijmn"] * L2["mnab"];
+    Z2r["ijab"] += WAMEI["eiam"] * L2["mjbe"];
+    Z2r["ijab"] -= WMNEF["mjab"] * GIMr["im"];
+    Z2r["ijab"] += WMNEF["ijeb"] * GEAr["ea"];
+    run_deferred(r);
+}
+
+// The "Hbar" product of CCSD::run (ccsd.cxx:83-86): STTwoElectronOperator(H, T, isHbar =
+// true) for T truncated at doubles (st2eoperator.hpp:59-130), statement for statement and
+// in the reference's order (later statements read blocks that earlier ones updated).  The
+// blocks start as copies of H; the occupied-virtual Fock block is assigned by the first
+// statement (the bare f_me does not survive) and f(ai), <ab||ij> stay zero.
+void Solver::record_hbar_so() {
+    Plan& p = hbar_plan;
+    std::vector<std::function<Plan()>> jobs;
+    Recorder r{&ctx, &p, &jobs};
+    TensorRef fME{&r, H.fME}, fAE{&r, H.fAE}, fMI{&r, H.fMI};
+    TensorRef VMNIJ{&r, H.VMNIJ}, VAMIJ{&r, H.VAMIJ}, VMNEJ{&r, H.VMNEJ}, VMNEF{&r, H.VMNEF};
+    TensorRef VAMEI{&r, H.VAMEI}, VAMEF{&r, H.VAMEF}, VABEJ{&r, H.VABEJ}, VABEF{&r, H.VABEF};
+    TensorRef T1r{&r, T1}, T2r{&r, T2}, Taur{&r, Tau};
+    TensorRef ia{&r, HB.fME}, ij{&r, HB.fMI}, ab{&r, HB.fAE}, ijkl{&r, HB.VMNIJ}, aijk{&r, HB.VAMIJ};
+    TensorRef ijak{&r, HB.VMNEJ}, ijab{&r, HB.VMNEF}, aibj{&r, HB.VAMEI}, aibc{&r, HB.VAMEF};
+    TensorRef abci{&r, HB.VABEJ}, abcd{&r, HB.VABEF};
+
+    // TwoElectronOperator(name, X): the blocks of H
+    ij["mi"] = fMI["mi"];
+    ab["ae"] = fAE["ae"];
+    ijkl["mnij"] = VMNIJ["mnij"];
+    aijk["amij"] = VAMIJ["amij"];
+    ijak["mnej"] = VMNEJ["mnej"];
+    ijab["mnef"] = VMNEF["mnef"];
+    aibj["amei"] = VAMEI["amei"];
+    aibc["amef"] = VAMEF["amef"];
+    abci["abej"] = VABEJ["abej"];
+    abcd["abef"] = VABEF["abef"];
+
+    // Tau = T2 + 1/2 P(ab)P(ij) t_ai t_bj from the current amplitudes
+    Taur["abij"] = T2r["abij"];
+    Taur["abij"] += 0.5 * T1r["ai"] * T1r["bj"];
+
+    ia["me"] = ijab["mnef"] * T1r["fn"];
+
+    ij["mi"] += 0.5 * ijab["nmef"] * T2r["efni"];
+    ij["mi"] += ia["me"] * T1r["ei"];
+    ij["mi"] += ijak["nmfi"] * T1r["fn"];
+
+    ijkl["mnij"] += 0.5 * ijab["mnef"] * Taur["efij"];
+    ijkl["mnij"] += ijak["nmei"] * T1r["ej"];
+
+    ijak["mnej"] += ijab["mnef"] * T1r["fj"];
+
+    ab["ae"] -= 0.5 * ijab["mnfe"] * T2r["famn"];
+    ab["ae"] -= ia["me"] * T1r["am"];
+    ab["ae"] += aibc["anef"] * T1r["fn"];
+
+    aijk["amij"] += 0.5 * aibc["amef"] * Taur["efij"];
+    aijk["amij"] += aibj["amej"] * T1r["ei"];
+
+    aibj["amei"] -= 0.5 * ijab["mnef"] * T2r["afin"];
+    aibj["amei"] -= aibc["amfe"] * T1r["fi"];
+    aibj["amei"] -= ijak["nmei"] * T1r["an"];
+
+    aijk["amij"] += ijak["nmej"] * T2r["aein"];
+    aijk["amij"] -= ijkl["nmij"] * T1r["an"];
+    aijk["amij"] += ia["me"] * T2r["aeij"];
+
+    aibj["amei"] -= 0.5 * ijab["mnef"] * T2r["afin"];
+    aibj["amei"] += 0.5 * ijak["nmei"] * T1r["an"];
+
+    abci["abej"] += 0.5 * ijak["mnej"] * T2r["abmn"];
+    abci["abej"] -= aibj["amej"] * T1r["bm"];
+    abci["abej"] += aibc["amef"] * T2r["fbmj"];
+    abci["abej"] += abcd["abef"] * T1r["fj"];
+    abci["abej"] -= ia["me"] * T2r["abmj"];
+
+    aibj["amei"] -= 0.5 * ijak["nmei"] * T1r["an"];
+
+    abcd["abef"] += 0.5 * ijab["mnef"] * Taur["abmn"];
+    abcd["abef"] -= aibc["amef"] * T1r["bm"];
+
+    aibc["amef"] -= ijab["nmef"] * T1r["an"];
+    run_deferred(r);
+}
+
+void Solver::hbar_so() {
+    if (rhf || lambda) throw Error(CCSD_ERR_UNSUPPORTED, "the spin-orbital Hbar is formed by a spin-orbital CCSD solver");
+    if (lambda_users > 0)
+        throw Error(CCSD_ERR_ARG, "a Lambda solver reads this Hbar: destroy it before forming Hbar again");
+    if (ctx.tensor(H.VABEF).packed())
+        throw Error(CCSD_ERR_UNSUPPORTED, "the spin-orbital Hbar needs <ab||ef> stored unpacked (pack_vvvv = 0)");
+    if (!hbar_formed) {
+        HB.fAI = mk(ctx, "Hbar f(ai)", 1, 0, 0, 1);
+        HB.fME = mk(ctx, "Hbar F(me)", 0, 1, 1, 0);
+        HB.fAE = mk(ctx, "Hbar F(ae)", 1, 0, 1, 0);
+        HB.fMI = mk(ctx, "Hbar F(mi)", 0, 1, 0, 1);
+        HB.VMNIJ = mk(ctx, "Hbar W(mn,ij)", 0, 2, 0, 2);
+        HB.VAMIJ = mk(ctx, "Hbar W(am,ij)", 1, 1, 0, 2);
+        HB.VMNEJ = mk(ctx, "Hbar W(mn,ej)", 0, 2, 1, 1);
+        HB.VABIJ = mk(ctx, "Hbar W(ab,ij)", 2, 0, 0, 2);
+        HB.VMNEF = mk(ctx, "Hbar W(mn,ef)", 0, 2, 2, 0);
+        HB.VAMEI = mk(ctx, "Hbar W(am,ei)", 1, 1, 1, 1);
+        HB.VAMEF = mk(ctx, "Hbar W(am,ef)", 1, 1, 2, 0);
+        HB.VABEJ = mk(ctx, "Hbar W(ab,ej)", 2, 0, 1, 1);
+        HB.VABEF = mk(ctx, "Hbar W(ab,ef)", 2, 0, 2, 0);
+        hbar_formed = true;
+        record_hbar_so();
+        ctx.upload(hbar_plan);
+    }
+    if (ctx.host_only) return;
     ctx.run(hbar_plan);
     CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
 }

@@ -27,6 +27,16 @@ public:
     // that the in-place symmetrisations WMNIJ += WMNIJ(nmji), Z2 += Z2(baji) read
     int T2SA = 0, TauSA = 0, VABIJSA = 0, VAIJBSA = 0, WAMIE = 0, WMNIJc = 0, Z2c = 0;
     int WABEJ = 0;                     // RHF Hbar only (created on the first hbar())
+    // Spin-orbital Hbar (STTwoElectronOperator with isHbar, st2eoperator.hpp:59-130): 13
+    // blocks of the solver's own, created on the first hbar_so()
+    ccsd_hamiltonian HB{};
+    bool hbar_formed = false;
+    // Lambda-CCSD (lambdaccsd.cxx): H holds the Hbar blocks, T1/T2/Z1/Z2 are L(1)[ia],
+    // L(2)[ijab] and their updates, `source` is the CCSD solver whose T2 G(im)/G(ea) read
+    bool lambda = false;
+    int GIM = 0, GEA = 0;
+    Solver* source = nullptr;
+    int lambda_users = 0;              // Lambda solvers reading this solver's T and Hbar
     Plan hbar_plan;
     double* den[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};   // [space][spin]
     Plan iter_plan, tau_plan, energy_plan;
@@ -64,6 +74,8 @@ public:
 
     Solver(Context& c, const ccsd_hamiltonian& h, const ccsd_options& o);
     Solver(Context& c, const ccsd_rhf_hamiltonian& h, const ccsd_options& o);
+    // Lambda-CCSD on an Hbar and the amplitudes of a spin-orbital CCSD solver
+    Solver(Context& c, Solver& ccsd, const ccsd_hamiltonian& hbar, const ccsd_options& o);
     ~Solver();
     void iterate(double* e, double* c);
     void iterate_async();
@@ -75,6 +87,8 @@ public:
     int run(double* e, double* c, int* it);
     // closed-shell Hbar intermediates from the current amplitudes (rhfccsd.cxx:110-186)
     void hbar_rhf();
+    // spin-orbital Hbar from the current amplitudes into HB
+    void hbar_so();
 
 private:
     void* alloc(size_t bytes);
@@ -89,6 +103,8 @@ private:
     void record_energy(Plan& p);
     void record_iteration();
     void record_iteration_rhf();
+    void record_iteration_lambda();
+    void record_hbar_so();
     void setup();
     std::vector<int> constants() const;
     std::vector<int> owned_tensors() const;

@@ -294,6 +294,30 @@ typedef struct {
     ccsd_tensor FME, FMI, FAE, WMNIJ, WMNEJ, WAMIJ, WAMIE, WAMEI, WABEJ;
 } ccsd_rhf_hbar;
 int ccsd_rhf_solver_hbar(ccsd_solver s, ccsd_rhf_hbar* out);
+/* Spin-orbital similarity-transformed Hamiltonian after convergence: the "Hbar" product of
+ * CCSD::run (ccsd.cxx:83-86), STTwoElectronOperator(H, T, isHbar) for T truncated at doubles
+ * (st2eoperator.hpp:59-130), from the solver's current T1, T2.  Thirteen blocks of the
+ * solver's own (valid until it is destroyed; recomputed on every call, which fails while a
+ * Lambda solver reads them).  As in the reference: fAI and VABIJ are zero, fME holds only
+ * sum_nf <mn||ef> t_fn (the bare f_me is replaced: zero for an SCF reference), and no block
+ * is a view of another.  Needs the solver's <ab||ef> stored unpacked (pack_vvvv = 0):
+ * otherwise CCSD_ERR_UNSUPPORTED.  Replaces LambdaCCSD's requirement "ccsd.Hbar". */
+int ccsd_solver_hbar(ccsd_solver s, ccsd_hamiltonian* out);
+
+/* Lambda-CCSD (LambdaCCSD<U>::run / iterate, src/cc/lambdaccsd.cxx:27-133) on an Hbar
+ * (normally from ccsd_solver_hbar) and the amplitudes of the spin-orbital CCSD solver
+ * `ccsd` (T2 is read every iteration by G(im), G(ea); destroying `ccsd` first fails).
+ * The returned handle works with ccsd_solver_iterate / _iterate_async / _status / _run /
+ * _destroy: the energy is 1/4 <mn||ef> l_mn^ef (lambdaccsd.cxx:129), conv the max-abs of
+ * the weighted update, ccsd_solver_amplitudes gives L1 [i, a] and L2 [i, j, a, b] (upper
+ * occupied, lower virtual), and ccsd_solver_mp2 the energy of the initial guess L = T.
+ * The denominators are the diagonals of Hbar's fAE and fMI (Denominator(Hbar)). */
+int ccsd_lambda_solver_create(ccsd_ctx ctx, const ccsd_hamiltonian* hbar, ccsd_solver ccsd,
+                              const ccsd_options* opts, ccsd_solver* out);
+/* host-only plan of CCSD + Hbar + Lambda in C1 or D2h sizes: flops of forming Hbar, flops
+ * of one Lambda iteration and the peak device bytes with all three alive */
+int ccsd_lambda_plan_query(int nirrep, const int* vrt, const int* occ, const ccsd_options* opts,
+                           double* hbar_flops, double* flops_per_iter, int64_t* device_bytes);
 /* algorithmic FP64 flops of one iteration as planned (packed-pair counts) */
 int ccsd_solver_flops(ccsd_solver s, double* flops);
 /* contraction mode the next iteration uses (changes when refine_tol is reached):

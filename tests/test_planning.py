@@ -102,3 +102,29 @@ def test_closed_shell_iteration_plans_in_every_point_group():
         occ, vrt, _ = A.synth_irreps(5, nirrep, 10, 40)
         f, b = A.rhf_plan_query(vrt, occ)
         assert f > 0 and b > 0
+
+
+@pytest.mark.parametrize("o,v", [(2, 6), (4, 20)])
+def test_lambda_ladder_flops(o, v):
+    """Lambda's Z2[ijab] += 1/2 WABEF[efab] L2[ijef] (lambdaccsd.cxx:122) over an unpacked
+    W: the same restricted-pair count as the CCSD ladder."""
+    with _ctx([v], [o]) as c:
+        W = c.tensor("W", (2, 0), (2, 0))
+        L2 = c.tensor("L2", (0, 2), (2, 0))
+        Z = c.tensor("Z", (0, 2), (2, 0))
+        Z["ijab"] += 0.5 * W["efab"] * L2["ijef"]
+        assert c.plan_flops() == 4 * comb(v, 2) ** 2 * comb(o, 2) + 2 * v ** 4 * o ** 2
+
+
+def test_lambda_plan_query():
+    """CCSD + spin-orbital Hbar + Lambda plan on the host: every Hbar and Lambda statement
+    plans, one Lambda iteration costs more than its ladder, forming Hbar more than one
+    Lambda iteration, and D2h blocks cost less than C1 over the same orbitals."""
+    o, v = 4, 20
+    hf, fl, by = A.lambda_plan_query([v], [o])
+    ladder = 4 * comb(v, 2) ** 2 * comb(o, 2) + 2 * v ** 4 * o ** 2
+    assert fl > ladder and hf > fl and by > 0
+    occ, vrt = [2, 1, 1, 0, 1, 1, 0, 1], [4, 3, 2, 3, 3, 2, 3, 2]
+    hf8, fl8, by8 = A.lambda_plan_query(vrt, occ)
+    hf1, fl1, by1 = A.lambda_plan_query([sum(vrt)], [sum(occ)])
+    assert 0 < fl8 < fl1 / 4 and 0 < hf8 < hf1 / 4 and by8 < by1
