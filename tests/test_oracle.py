@@ -102,3 +102,35 @@ def test_hbar_without_amplitudes_is_the_bare_hamiltonian(built_lib):
         assert np.array_equal(X[k], b), k
     for k in ("ia", "ai", "abij"):
         assert not X[k].any(), k
+
+
+@pytest.mark.parametrize("o,v,seed", [(3, 7, 4), (4, 9, 6)])
+def test_spin_orbital_hbar_matches_spin_adapted(built_lib, o, v, seed):
+    """Two restatements that share no code: the spin-orbital Hbar (st2eoperator.hpp:59-130)
+    of the converged spin-orbital T and the closed-shell "Form Hbar" (rhfccsd.cxx:110-186)
+    of the converged spatial T give the same intermediates.  The spatial ones are spin blocks
+    (A, I alpha; m, j beta): F = alpha-alpha blocks, W(Mn,Ij) = ijkl[AbAb]-type blocks, and
+    W(Am,Ie) = -2 W[Am,eI]_(alpha beta beta alpha) - W[Am,Ei]_(alpha beta alpha beta)."""
+    from oracle import lambda_ccsd as LC
+    F, eri = _problem(seed, o, v)
+    rhf = R.RHFCCSD(F, eri, o, diis_order=8)
+    rhf.run(1e-12, 100)
+    H = O.Hamiltonian(F, eri, o, ladder_literal=True)
+    cc = O.CCSD(H, diis_order=8)
+    cc.run(1e-12, 100)
+    assert abs(rhf.energy - cc.energy) < 1e-12
+    Hr = rhf.hbar()
+    Hs = LC.hbar(H, cc.T.T1, cc.T.T2)
+
+    def blk(x, spins, dims):
+        return x[tuple(slice(s * d, (s + 1) * d) for s, d in zip(spins, dims))]
+
+    pairs = {"FME": ("ia", (0, 0), (o, v)), "FMI": ("ij", (0, 0), (o, o)), "FAE": ("ab", (0, 0), (v, v)),
+             "WMNIJ": ("ijkl", (0, 1, 0, 1), (o, o, o, o)), "WMNEJ": ("ijak", (0, 1, 0, 1), (o, o, v, o)),
+             "WAMIJ": ("aijk", (0, 1, 0, 1), (v, o, o, o)), "WAMEI": ("aibj", (0, 1, 0, 1), (v, o, v, o)),
+             "WABEJ": ("abci", (0, 1, 0, 1), (v, v, v, o))}
+    for name, (key, spins, dims) in pairs.items():
+        r = Hr[name]
+        assert np.abs(r - blk(Hs[key], spins, dims)).max() < 1e-12 * max(1.0, np.abs(r).max()), name
+    ring = -2 * blk(Hs["aibj"], (0, 1, 1, 0), (v, o, v, o)) - blk(Hs["aibj"], (0, 1, 0, 1), (v, o, v, o))
+    assert np.abs(Hr["WAMIE"].transpose(0, 1, 3, 2) - ring).max() < 1e-12
