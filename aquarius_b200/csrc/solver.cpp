@@ -49,7 +49,7 @@ Solver::Solver(Context& c, const ccsd_hamiltonian& h, const ccsd_options& o) : c
     WMNEJ = mk(ctx, "W(mn,ej)", 0, 2, 1, 1);
     WAMIJ = mk(ctx, "W~(am,ij)", 1, 1, 0, 2);
     WAMEI = mk(ctx, "W~(am,ei)", 1, 1, 1, 1);
-    setup();
+    setup_or_teardown();
 }
 
 // Closed-shell spin-adapted form (rhfccsd.cxx:44-110): plain spatial tensors, positions in
@@ -77,7 +77,7 @@ Solver::Solver(Context& c, const ccsd_rhf_hamiltonian& h, const ccsd_options& o)
     WAMIJ = mk(ctx, "W(Am,Ij)", 1, 1, 0, 2, P);
     WAMEI = mk(ctx, "W(Am,Ei)", 1, 1, 1, 1, P);
     WAMIE = mk(ctx, "W(Am,Ie)", 1, 1, 1, 1, P);
-    setup();
+    setup_or_teardown();
 }
 
 // LambdaCCSD<U>::run (lambdaccsd.cxx:27-58): L(1), L(2) in the reference's layout (upper
@@ -111,13 +111,7 @@ Solver::Solver(Context& c, Solver& ccsd, const ccsd_hamiltonian& hbar, const ccs
     GIM = mk(ctx, "G(im)", 0, 1, 0, 1);
     GEA = mk(ctx, "G(ea)", 1, 0, 1, 0);
     source->lambda_users++;
-    try {
-        setup();
-    } catch (...) {
-        source->lambda_users--;
-        source = nullptr;
-        throw;
-    }
+    setup_or_teardown();
 }
 
 std::vector<int> Solver::constants() const {
@@ -152,6 +146,7 @@ void Solver::setup() {
     ctx.slices = opts.slices;
     // constants: the H blocks never change, so their split slices can be cached
     for (int t : constants()) ctx.constant_tensors.push_back(t);
+    constants_registered = true;
 
     if (ctx.host_only) {
         // planning query: account every allocation and plan one iteration, launch nothing
@@ -238,23 +233,43 @@ void Solver::setup() {
     flops_per_iter = iter_plan.flops() + tau_plan.flops();
 }
 
-Solver::~Solver() {
+// A constructor that fails gives back what it took (tensors, device memory, plans) before
+// the exception leaves it: the destructor does not run for a half-built object.
+void Solver::setup_or_teardown() {
+    try {
+        setup();
+    } catch (...) {
+        teardown();
+        throw;
+    }
+}
+
+Solver::~Solver() { teardown(); }
+
+void Solver::teardown() {
     if (source) source->lambda_users--;
+    source = nullptr;
     if (graph_exec) cudaGraphExecDestroy(graph_exec);
     if (graph) cudaGraphDestroy(graph);
     ctx.release(iter_plan);
     ctx.release(tau_plan);
     ctx.release(energy_plan);
     ctx.release(hbar_plan);
-    const std::vector<int> cons = constants();
+    const std::vector<int> cons = constants_registered ? constants() : std::vector<int>{};
+    constants_registered = false;
     for (int t : owned_tensors())
         if (ctx.tensors.count(t)) ctx.destroy_tensor(t);
     for (auto p : owned) ctx.dfree(p.first, p.second);
+    owned.clear();
     if (h_red) cudaFreeHost(h_red);
     if (h_state) cudaFreeHost(h_state);
-    for (int t : cons)
-        ctx.constant_tensors.erase(std::remove(ctx.constant_tensors.begin(), ctx.constant_tensors.end(), t),
-                                   ctx.constant_tensors.end());
+    h_red = nullptr;
+    h_state = nullptr;
+    // one registration each: another solver on the same H keeps its own
+    for (int t : cons) {
+        auto it = std::find(ctx.constant_tensors.begin(), ctx.constant_tensors.end(), t);
+        if (it != ctx.constant_tensors.end()) ctx.constant_tensors.erase(it);
+    }
 }
 
 void* Solver::alloc(size_t bytes) {
@@ -830,9 +845,20 @@ void Solver::hbar_so() {
         HB.VAMEF = mk(ctx, "Hbar W(am,ef)", 1, 1, 2, 0);
         HB.VABEJ = mk(ctx, "Hbar W(ab,ej)", 2, 0, 1, 1);
         HB.VABEF = mk(ctx, "Hbar W(ab,ef)", 2, 0, 2, 0);
+        try {
+            record_hbar_so();
+            ctx.upload(hbar_plan);
+        } catch (...) {
+            // leave no half-recorded plan and no blocks behind: a later call starts afresh
+            ctx.release(hbar_plan);
+            hbar_plan = Plan();
+            for (int t : {HB.fAI, HB.fME, HB.fAE, HB.fMI, HB.VMNIJ, HB.VAMIJ, HB.VMNEJ, HB.VABIJ, HB.VMNEF, HB.VAMEI,
+                          HB.VAMEF, HB.VABEJ, HB.VABEF})
+                if (ctx.tensors.count(t)) ctx.destroy_tensor(t);
+            HB = ccsd_hamiltonian{};
+            throw;
+        }
         hbar_formed = true;
-        record_hbar_so();
-        ctx.upload(hbar_plan);
     }
     if (ctx.host_only) return;
     ctx.run(hbar_plan);

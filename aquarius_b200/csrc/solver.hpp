@@ -71,6 +71,7 @@ public:
     double energy = 0, conv = 0, mp2 = 0;
     double flops_per_iter = 0;
     std::vector<std::pair<void*, size_t>> owned;
+    bool constants_registered = false;   // setup() marked constants() as constant tensors
 
     Solver(Context& c, const ccsd_hamiltonian& h, const ccsd_options& o);
     Solver(Context& c, const ccsd_rhf_hamiltonian& h, const ccsd_options& o);
@@ -106,6 +107,8 @@ private:
     void record_iteration_lambda();
     void record_hbar_so();
     void setup();
+    void setup_or_teardown();
+    void teardown();
     std::vector<int> constants() const;
     std::vector<int> owned_tensors() const;
     void launch_iteration();

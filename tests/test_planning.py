@@ -128,3 +128,15 @@ def test_lambda_plan_query():
     hf8, fl8, by8 = A.lambda_plan_query(vrt, occ)
     hf1, fl1, by1 = A.lambda_plan_query([sum(vrt)], [sum(occ)])
     assert 0 < fl8 < fl1 / 4 and 0 < hf8 < hf1 / 4 and by8 < by1
+
+
+def test_rejected_options_leave_no_state():
+    """A solver whose options are rejected gives back what its constructor took; the
+    same query then succeeds."""
+    for bad in ({"diis_order": 20}, {"precision": "split", "diis_order": 0}):
+        with pytest.raises(A.CcsdError) as e:
+            A.plan_query([6], [2], **bad)
+        assert e.value.code == 1   # CCSD_ERR_ARG
+        with pytest.raises(A.CcsdError):
+            A.lambda_plan_query([6], [2], **bad)
+    assert A.lambda_plan_query([6], [2])[1] > 0
