@@ -53,7 +53,7 @@ EXPORTS = [
     "ccsd_rhf_hamiltonian_from_factor", "ccsd_rhf_hamiltonian_from_integrals", "ccsd_rhf_hamiltonian_destroy",
     "ccsd_rhf_solver_create", "ccsd_rhf_plan_query", "ccsd_hamiltonian_from_ao", "ccsd_rhf_hamiltonian_from_ao",
     "ccsd_rhf_solver_hbar", "ccsd_ctx_plan_flops", "ccsd_solver_hbar", "ccsd_lambda_solver_create",
-    "ccsd_lambda_plan_query",
+    "ccsd_lambda_plan_query", "ccsd_ctx_plan_export",
 ]
 
 
@@ -199,6 +199,7 @@ def lib():
             "ccsd_rhf_solver_create": [vp, P(RHFHamiltonian), P(Options), P(vp)],
             "ccsd_rhf_solver_hbar": [vp, P(RHFHbar)],
             "ccsd_solver_hbar": [vp, P(Hamiltonian)],
+            "ccsd_ctx_plan_export": [vp, ctypes.c_char_p],
             "ccsd_lambda_solver_create": [vp, P(Hamiltonian), vp, P(Options), P(vp)],
             "ccsd_lambda_plan_query": [ctypes.c_int, vp, vp, P(Options), P(dbl), P(dbl), P(i64)],
             "ccsd_hamiltonian_from_ao": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp, ctypes.c_int,
@@ -644,6 +645,10 @@ class Context:
         x = ctypes.c_double()
         _check(lib().ccsd_ctx_plan_flops(self.c, ctypes.byref(x)), self.c)
         return x.value
+
+    def plan_export(self, path):
+        """write the plan of the last contraction / sum statement as text (ccsd_ctx_plan_export)"""
+        _check(lib().ccsd_ctx_plan_export(self.c, str(path).encode()), self.c)
 
     def launch_count(self):
         n = ctypes.c_int64()

@@ -171,6 +171,17 @@ int ccsd_ctx_plan_flops(ccsd_ctx ctx, double* flops) {
     });
 }
 
+int ccsd_ctx_plan_export(ccsd_ctx ctx, const char* path) {
+    return guarded(ctx, [&] {
+        if (!path) throw Error(CCSD_ERR_ARG, "null path");
+        Context* c = from_handle(ctx);
+        auto it = c->plan_cache.find(c->last_plan_key);
+        if (c->last_plan_key.empty() || it == c->plan_cache.end())
+            throw Error(CCSD_ERR_ARG, "no statement planned on this context");
+        export_plan(*c, *it->second, path);
+    });
+}
+
 int ccsd_ctx_synchronize(ccsd_ctx ctx) {
     return guarded(ctx, [&] { CCSD_CUDA(cudaStreamSynchronize(from_handle(ctx)->stream)); });
 }
@@ -457,6 +468,7 @@ int ccsd_contract(ccsd_ctx ctx, double alpha, ccsd_tensor A, const char* idxA, c
             it = c->plan_cache.emplace(key, std::move(p)).first;
         }
         c->last_plan_flops = it->second->flops();
+        c->last_plan_key = key;
         c->run(*it->second);
     });
 }
@@ -472,6 +484,7 @@ int ccsd_sum(ccsd_ctx ctx, double alpha, ccsd_tensor A, const char* idxA, double
             auto p = std::make_unique<Plan>(plan_sum(*c, alpha, A, idxA, beta, B, idxB));
             it = c->plan_cache.emplace(key, std::move(p)).first;
         }
+        c->last_plan_key = key;
         c->run(*it->second);
     });
 }

@@ -224,6 +224,8 @@ Plan plan_contract(Context& ctx, double alpha, int A, const std::string& idxA, i
 Plan plan_sum(Context& ctx, double alpha, int A, const std::string& idxA, double beta, int C,
               const std::string& idxC);
 Plan plan_dot(Context& ctx, int A, const std::string& idxA, int B, const std::string& idxB);
+// text export of a plan and of the layout of the tensors it touches (plan_export.cpp)
+void export_plan(const Context& ctx, const Plan& p, const char* path);
 
 // ---------------------------------------------------------------------------
 // context
@@ -248,6 +250,7 @@ public:
     bool plan_refine = false;          // host-only plan of a split solve that may move to 4 slices
     int plan_threads = 8;              // host threads that plan the statements of an iteration
     double last_plan_flops = 0;        // algorithmic flops of the last ccsd_contract statement
+    std::string last_plan_key;         // plan-cache key of the last ccsd_contract / ccsd_sum statement
     int split_routing = CCSD_SPLIT_ROUTE_AUTO;  // which contractions take the split kernel
     bool fp64_tiled_only = false;      // keep skinny FP64 products on the tiled kernel
     bool group_gemms = true;           // batch small block contractions of a statement into grouped launches

@@ -87,6 +87,12 @@ int ccsd_ctx_create(int device, void* stream, ccsd_ctx* out);
 /* algorithmic flops of the last ccsd_contract statement, as the planner counts them
  * (block products 2*M*N*K, packed pairs counted once) */
 int ccsd_ctx_plan_flops(ccsd_ctx ctx, double* flops);
+/* Diagnostic: write the plan of the last ccsd_contract / ccsd_sum statement on this context
+ * (its block GEMMs with their offset tables, permuted sums, block scalings, in execution
+ * order) and the block layout of the tensors it touches to a text file, so that a host-side
+ * checker can replay the planner's expansion of a statement.  Record format: the header of
+ * aquarius_b200/csrc/plan_export.cpp.  Works on planning-only contexts. */
+int ccsd_ctx_plan_export(ccsd_ctx ctx, const char* path);
 int ccsd_ctx_destroy(ccsd_ctx ctx);
 const char* ccsd_last_error(ccsd_ctx ctx);
 int ccsd_ctx_synchronize(ccsd_ctx ctx);
