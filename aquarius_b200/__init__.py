@@ -53,7 +53,7 @@ EXPORTS = [
     "ccsd_rhf_hamiltonian_from_factor", "ccsd_rhf_hamiltonian_from_integrals", "ccsd_rhf_hamiltonian_destroy",
     "ccsd_rhf_solver_create", "ccsd_rhf_plan_query", "ccsd_hamiltonian_from_ao", "ccsd_rhf_hamiltonian_from_ao",
     "ccsd_rhf_solver_hbar", "ccsd_ctx_plan_flops", "ccsd_solver_hbar", "ccsd_lambda_solver_create",
-    "ccsd_lambda_plan_query", "ccsd_ctx_plan_export",
+    "ccsd_lambda_plan_query", "ccsd_ctx_plan_export", "ccsd_plan_export_solver",
 ]
 
 
@@ -200,6 +200,7 @@ def lib():
             "ccsd_rhf_solver_hbar": [vp, P(RHFHbar)],
             "ccsd_solver_hbar": [vp, P(Hamiltonian)],
             "ccsd_ctx_plan_export": [vp, ctypes.c_char_p],
+            "ccsd_plan_export_solver": [ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_char_p],
             "ccsd_lambda_solver_create": [vp, P(Hamiltonian), vp, P(Options), P(vp)],
             "ccsd_lambda_plan_query": [ctypes.c_int, vp, vp, P(Options), P(dbl), P(dbl), P(i64)],
             "ccsd_hamiltonian_from_ao": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp, ctypes.c_int,
@@ -294,6 +295,18 @@ def lambda_plan_query(vrt, occ, diis_order=8, precision="fp64"):
     _check(lib().ccsd_lambda_plan_query(len(vrt), _ptr(vrt), _ptr(occ), ctypes.byref(o), ctypes.byref(hf),
                                         ctypes.byref(fl), ctypes.byref(by)))
     return hf.value, fl.value, by.value
+
+
+METHODS = {"ccsd": 0, "rhf": 1, "lambda": 2}
+PLANS = {"iteration": 0, "hbar": 1, "energy": 2}
+
+
+def plan_export_solver(method, vrt, occ, which, path):
+    """Host-only: write one recorded plan of a CCSD / RHF / Lambda solver for these sizes
+    (ccsd_plan_export_solver), for replay by a host-side checker."""
+    vrt, occ = _ints(vrt), _ints(occ)
+    _check(lib().ccsd_plan_export_solver(METHODS[method], len(vrt), _ptr(vrt), _ptr(occ), PLANS[which],
+                                         str(path).encode()))
 
 
 def rhf_plan_query(vrt, occ, diis_order=8, precision="fp64", refine_tol=0.0):

@@ -878,6 +878,60 @@ int ccsd_lambda_plan_query(int nirrep, const int* vrt, const int* occ, const ccs
     });
 }
 
+int ccsd_plan_export_solver(int method, int nirrep, const int* vrt, const int* occ, int which, const char* path) {
+    return guarded(nullptr, [&] {
+        if (!path) throw Error(CCSD_ERR_ARG, "null path");
+        if (method < CCSD_METHOD_CCSD || method > CCSD_METHOD_LAMBDA) throw Error(CCSD_ERR_ARG, "bad method");
+        if (which < CCSD_PLAN_ITERATION || which > CCSD_PLAN_ENERGY) throw Error(CCSD_ERR_ARG, "bad plan");
+        if (which == CCSD_PLAN_HBAR && method == CCSD_METHOD_LAMBDA) throw Error(CCSD_ERR_ARG, "Lambda forms no Hbar");
+        Context host(-1, nullptr);
+        int n = 0;
+        host.spaces = query_spaces(nirrep, vrt, occ, n);
+        host.spaces_set = true;
+        ccsd_options o;
+        options_default(&o);
+        Plan out;
+        auto take = [&](const Plan& p) {
+            Plan c = p;
+            out.append(std::move(c));
+        };
+        // the iteration plan starts from Tau = T2 + 1/2 P(ab)P(ij) t t, which the fused Tau
+        // kernel forms on the device; its statement form (the Tau plan) is exported first
+        auto pick = [&](Solver& s) {
+            if (which == CCSD_PLAN_ITERATION) {
+                take(s.tau_plan);
+                take(s.iter_plan);
+            } else if (which == CCSD_PLAN_ENERGY) {
+                take(s.energy_plan);
+            } else {
+                take(s.hbar_plan);
+            }
+        };
+        if (method == CCSD_METHOD_RHF) {
+            ccsd_rhf_hamiltonian H;
+            create_rhf_hamiltonian_tensors(host, &H);
+            Solver s(host, H, o);
+            if (which == CCSD_PLAN_HBAR) s.hbar_rhf();
+            pick(s);
+            export_plan(host, out, path);
+            return;
+        }
+        ccsd_hamiltonian H;
+        create_hamiltonian_tensors(host, false, &H);
+        Solver cc(host, H, o);
+        if (method == CCSD_METHOD_CCSD) {
+            if (which == CCSD_PLAN_HBAR) cc.hbar_so();
+            pick(cc);
+            export_plan(host, out, path);
+            return;
+        }
+        cc.hbar_so();
+        Solver lam(host, cc, cc.HB, o);
+        pick(lam);
+        export_plan(host, out, path);
+    });
+}
+
 int ccsd_solver_create(ccsd_ctx ctx, const ccsd_hamiltonian* H, const ccsd_options* opts, ccsd_solver* out) {
     if (!out) return CCSD_ERR_ARG;
     *out = nullptr;

@@ -625,7 +625,6 @@ void Solver::record_iteration_rhf() {
 // strings as in record_iteration_rhf (W(Am,Ie), VAIJB: "amie" reads "amei").
 void Solver::hbar_rhf() {
     if (!rhf) throw Error(CCSD_ERR_UNSUPPORTED, "Hbar intermediates are formed for the closed-shell solver");
-    if (ctx.host_only) return;
     if (!WABEJ) {
         WABEJ = mk(ctx, "W(Ab,Ej)", 2, 0, 1, 1, CCSD_TENSOR_PLAIN);
         Plan& p = hbar_plan;
@@ -706,6 +705,7 @@ void Solver::hbar_rhf() {
         run_deferred(r);
         ctx.upload(hbar_plan);
     }
+    if (ctx.host_only) return;
     ctx.run(hbar_plan);
     CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
 }

@@ -1,0 +1,123 @@
+"""The solvers' own recorded statement lists, replayed on the CPU against the oracles.
+
+One CCSD iteration (ccsd.cxx:123-180), the spin-orbital Hbar (st2eoperator.hpp:59-130,
+isHbar), one Lambda-CCSD iteration (lambdaccsd.cxx:80-124) and the energy reductions are
+planned on the host for C1 and D2h sizes (ccsd_plan_export_solver), executed with numpy
+over the engine's block layout (tests/plan_replay.py) and compared with oracle/ccsd_oracle.py
+and oracle/lambda_ccsd.py.  This checks the statement lists in csrc/solver.cpp -- their
+order, assignments, factors and signs -- with the planner's expansion, without a device.
+"""
+import numpy as np
+import pytest
+
+import aquarius_b200 as A
+from oracle import ccsd_oracle as O
+from oracle import lambda_ccsd as LC
+from tests import plan_replay as R
+
+H_NAMES = {"f(ai)": "fAI", "f(ia)": "fME", "f(ab)": "fAE", "f(ij)": "fMI", "<ij||kl>": "VMNIJ",
+           "<ai||jk>": "VAMIJ", "<ij||ab>": "VMNEF", "<ai||bj>": "VAMEI", "<ai||bc>": "VAMEF",
+           "<ab||cd>": "VABEF"}
+HBAR_NAMES = {"Hbar f(ai)": "ai", "Hbar F(me)": "ia", "Hbar F(ae)": "ab", "Hbar F(mi)": "ij",
+              "Hbar W(mn,ij)": "ijkl", "Hbar W(am,ij)": "aijk", "Hbar W(mn,ej)": "ijak",
+              "Hbar W(ab,ij)": "abij", "Hbar W(mn,ef)": "ijab", "Hbar W(am,ei)": "aibj",
+              "Hbar W(am,ef)": "aibc", "Hbar W(ab,ej)": "abci", "Hbar W(ab,ef)": "abcd"}
+SIZES = {1: (3, 6), 4: (5, 12)}
+
+
+@pytest.fixture(scope="module", params=[1, 4], ids=["C1", "D2h-4"])
+def problem(request):
+    nirrep = request.param
+    o, v = SIZES[nirrep]
+    eps, B, occ, vrt, _ = A.synth_problem(31 + nirrep, o, v, nirrep=nirrep)
+    H = O.hamiltonian_from_factor(B, eps, o, ladder_literal=True)
+    cc = O.CCSD(H, diis_order=8)
+    for _ in range(3):
+        cc.iterate()                     # amplitudes away from the MP1 guess
+    Hb = LC.hbar(H, cc.T.T1, cc.T.T2)
+    lam = LC.LambdaCCSD(Hb, cc.T.T1, cc.T.T2, diis_order=8)
+    lam.iterate()                        # Lambda amplitudes away from L = T
+    return occ, vrt, H, cc, Hb, lam
+
+
+def _replay(problem, method, which, arrays, tmp_path):
+    occ, vrt = problem[0], problem[1]
+    path = tmp_path / f"{method}-{which}.txt"
+    A.plan_export_solver(method, vrt, occ, which, path)
+    dump = R.load(path)
+    ctx = A.Context(-1)
+    ctx.set_spaces(vrt=vrt, occ=occ)
+    store = {}
+    for h, t in dump.tensors.items():
+        if t.view_of:
+            continue
+        full = arrays.get(t.name)
+        store[h] = R.to_storage(ctx, t, full) if full is not None else np.zeros(max(t.total, 1))
+    acc = R.replay(dump, store)
+    by_name = {t.name: (t, store[h]) for h, t in dump.tensors.items() if not t.view_of}
+
+    def check(name, want, tol=1e-12):
+        t, got = by_name[name]
+        w = R.to_storage(ctx, t, want)
+        err = np.abs(got - w).max()
+        assert err < tol * max(1.0, np.abs(w).max()), (name, err)
+
+    return check, acc, by_name, ctx
+
+
+def _h_arrays(H):
+    return {n: getattr(H, k) for n, k in H_NAMES.items()}
+
+
+def test_ccsd_iteration_plan(problem, tmp_path):
+    _, _, H, cc, _, _ = problem
+    arrays = _h_arrays(H)
+    arrays.update({"T(1)": cc.T.T1, "T(2)": cc.T.T2})
+    check, _, _, ctx = _replay(problem, "ccsd", "iteration", arrays, tmp_path)
+    Z1, Z2 = cc.residual(cc.T)
+    check("Tau", O.CCSD.make_tau(cc.T))
+    check("Z(1)", Z1)
+    check("Z(2)", Z2)
+    ctx.close()
+
+
+def test_ccsd_energy_plan(problem, tmp_path):
+    _, _, H, cc, _, _ = problem
+    arrays = _h_arrays(H)
+    arrays.update({"T(1)": cc.T.T1, "Tau": O.CCSD.make_tau(cc.T)})
+    _, e, _, ctx = _replay(problem, "ccsd", "energy", arrays, tmp_path)
+    assert abs(e - cc.energy_of(cc.T)) < 1e-13
+    ctx.close()
+
+
+def test_hbar_plan(problem, tmp_path):
+    _, _, H, cc, Hb, _ = problem
+    arrays = _h_arrays(H)
+    arrays.update({"T(1)": cc.T.T1, "T(2)": cc.T.T2})
+    check, _, by_name, ctx = _replay(problem, "ccsd", "hbar", arrays, tmp_path)
+    written = [n for n in HBAR_NAMES if n in by_name]
+    # f(ai) and <ab||ij> of Hbar are zero and no statement writes them
+    assert sorted(set(HBAR_NAMES) - set(written)) == ["Hbar W(ab,ij)", "Hbar f(ai)"]
+    for name in written:
+        check(name, Hb[HBAR_NAMES[name]])
+    ctx.close()
+
+
+def test_lambda_iteration_plan(problem, tmp_path):
+    _, _, _, cc, Hb, lam = problem
+    arrays = {n: Hb[k] for n, k in HBAR_NAMES.items()}
+    arrays.update({"T(2)": cc.T.T2, "L(1)": lam.L.T1, "L(2)": lam.L.T2})
+    check, _, _, ctx = _replay(problem, "lambda", "iteration", arrays, tmp_path)
+    Z1, Z2 = lam.residual(lam.L.T1, lam.L.T2)
+    check("Z(1)", Z1)
+    check("Z(2)", Z2)
+    ctx.close()
+
+
+def test_lambda_energy_plan(problem, tmp_path):
+    _, _, _, _, Hb, lam = problem
+    arrays = {n: Hb[k] for n, k in HBAR_NAMES.items()}
+    arrays.update({"L(2)": lam.L.T2})
+    _, e, _, ctx = _replay(problem, "lambda", "energy", arrays, tmp_path)
+    assert abs(e - 0.25 * float(np.vdot(Hb["ijab"], lam.L.T2))) < 1e-13
+    ctx.close()
