@@ -56,7 +56,20 @@ class RHFCCSD:
         self.conv = np.finfo(float).max
 
     def iterate(self):
-        T1, T2 = self.T1, self.T2
+        Z1, Z2 = self.residual(self.T1, self.T2)
+        fAI, VABIJSA = self.fAI, self.VABIJSA
+        Z1 = weight(Z1, self.D1)
+        Z2 = weight(Z2, self.D2)
+        T1 = self.T1 + Z1
+        T2 = self.T2 + Z2
+        Tau = T2 + es('ai,bj->abij', T1, T1)
+        self.energy = 2 * float(np.vdot(fAI, T1)) + float(np.vdot(VABIJSA, Tau))
+        self.conv = max(np.abs(Z1).max(), np.abs(Z2).max())
+        self.T1, self.T2 = self._diis(T1, T2, Z1, Z2)
+        return self.energy, self.conv
+
+    def residual(self, T1, T2):
+        """The intermediates and the unweighted residual (rhfccsd.cxx:237-316)."""
         fAI, fAB, fIJ = self.fAI, self.fAB, self.fIJ
         VABIJ, VAIBJ, VAIJB, VABCI = self.VABIJ, self.VAIBJ, self.VAIJB, self.VABCI
         VAIJK, VIJKL, VABCD = self.VAIJK, self.VIJKL, self.VABCD
@@ -94,16 +107,7 @@ class RHFCCSD:
             + 0.5 * es('mnij,abmn->abij', WMNIJ, Tau) + 0.5 * es('amie,ebmj->abij', WAMIE, T2SA) \
             - 0.5 * es('amei,ebjm->abij', WAMEI, T2) - es('amej,ebim->abij', WAMEI, T2)
         Z2 = Z2 + Z2.transpose(1, 0, 3, 2)
-
-        Z1 = weight(Z1, self.D1)
-        Z2 = weight(Z2, self.D2)
-        T1 = T1 + Z1
-        T2 = T2 + Z2
-        Tau = T2 + es('ai,bj->abij', T1, T1)
-        self.energy = 2 * float(np.vdot(fAI, T1)) + float(np.vdot(VABIJSA, Tau))
-        self.conv = max(np.abs(Z1).max(), np.abs(Z2).max())
-        self.T1, self.T2 = self._diis(T1, T2, Z1, Z2)
-        return self.energy, self.conv
+        return Z1, Z2
 
     def _diis(self, T1, T2, Z1, Z2):
         # diis.hpp:70-227 with two x and two dx; inner product sum_j <dx_j, dx'_j>

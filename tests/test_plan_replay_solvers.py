@@ -1,10 +1,11 @@
 """The solvers' own recorded statement lists, replayed on the CPU against the oracles.
 
 One CCSD iteration (ccsd.cxx:123-180), the spin-orbital Hbar (st2eoperator.hpp:59-130,
-isHbar), one Lambda-CCSD iteration (lambdaccsd.cxx:80-124) and the energy reductions are
-planned on the host for C1 and D2h sizes (ccsd_plan_export_solver), executed with numpy
-over the engine's block layout (tests/plan_replay.py) and compared with oracle/ccsd_oracle.py
-and oracle/lambda_ccsd.py.  This checks the statement lists in csrc/solver.cpp -- their
+isHbar), one Lambda-CCSD iteration (lambdaccsd.cxx:80-124), the energy reductions, and the
+closed-shell iteration and Hbar (rhfccsd.cxx:110-186, 237-316) are planned on the host for C1
+and D2h sizes (ccsd_plan_export_solver), executed with numpy over the engine's block layout
+(tests/plan_replay.py) and compared with oracle/ccsd_oracle.py, oracle/lambda_ccsd.py and
+oracle/rhf_ccsd.py.  This checks the statement lists in csrc/solver.cpp -- their
 order, assignments, factors and signs -- with the planner's expansion, without a device.
 """
 import numpy as np
@@ -120,4 +121,52 @@ def test_lambda_energy_plan(problem, tmp_path):
     arrays.update({"L(2)": lam.L.T2})
     _, e, _, ctx = _replay(problem, "lambda", "energy", arrays, tmp_path)
     assert abs(e - 0.25 * float(np.vdot(Hb["ijab"], lam.L.T2))) < 1e-13
+    ctx.close()
+
+
+# closed shell (rhfccsd.cxx): plain spatial tensors; VAIJB, VAIJBSA and W(Am,Ie) hold their
+# [a, i, j, b] elements at [a, i, b, j]
+RHF_NAMES = {"fAI": "fAI", "fAB": "fAB", "fIJ": "fIJ", "<Ab|Cd>": "VABCD", "<Ab|Ci>": "VABCI", "<Ab|Ij>": "VABIJ",
+             "<Ai|Bj>": "VAIBJ", "<Ai|Jk>": "VAIJK", "<Ij|Kl>": "VIJKL", "VABIJSA": "VABIJSA"}
+RHF_HBAR = {"F(ME)": "FME", "F(MI)": "FMI", "F(AE)": "FAE", "W(Mn,Ij)": "WMNIJ", "W(Mn,Ej)": "WMNEJ",
+            "W(Am,Ij)": "WAMIJ", "W(Am,Ei)": "WAMEI", "W(Ab,Ej)": "WABEJ"}
+
+
+@pytest.fixture(scope="module", params=[1, 4], ids=["C1", "D2h-4"])
+def rhf_problem(request):
+    from oracle import rhf_ccsd as RH
+    nirrep = request.param
+    o, v = SIZES[nirrep]
+    eps, B, occ, vrt, _ = A.synth_problem(41 + nirrep, o, v, nirrep=nirrep)
+    ref = RH.RHFCCSD(np.diag(eps), O.eri_from_factor(B), o, diis_order=8)
+    for _ in range(3):
+        ref.iterate()
+    return occ, vrt, ref
+
+
+def _rhf_arrays(ref):
+    arrays = {n: getattr(ref, k) for n, k in RHF_NAMES.items()}
+    arrays["<Ai|Jb>"] = ref.VAIJB.transpose(0, 1, 3, 2)
+    arrays["VAIJBSA"] = ref.VAIJBSA.transpose(0, 1, 3, 2)
+    arrays.update({"T1": ref.T1, "T2": ref.T2})
+    return arrays
+
+
+def test_rhf_iteration_plan(rhf_problem, tmp_path):
+    occ, vrt, ref = rhf_problem
+    check, _, _, ctx = _replay(rhf_problem, "rhf", "iteration", _rhf_arrays(ref), tmp_path)
+    Z1, Z2 = ref.residual(ref.T1, ref.T2)
+    check("Tau", ref.T2 + np.einsum("ai,bj->abij", ref.T1, ref.T1))
+    check("Z1", Z1)
+    check("Z2", Z2)
+    ctx.close()
+
+
+def test_rhf_hbar_plan(rhf_problem, tmp_path):
+    occ, vrt, ref = rhf_problem
+    check, _, _, ctx = _replay(rhf_problem, "rhf", "hbar", _rhf_arrays(ref), tmp_path)
+    want = ref.hbar()
+    for name, key in RHF_HBAR.items():
+        check(name, want[key])
+    check("W(Am,Ie)", want["WAMIE"].transpose(0, 1, 3, 2))
     ctx.close()
