@@ -23,10 +23,10 @@ HBAR_NAMES = {"Hbar f(ai)": "ai", "Hbar F(me)": "ia", "Hbar F(ae)": "ab", "Hbar 
               "Hbar W(mn,ij)": "ijkl", "Hbar W(am,ij)": "aijk", "Hbar W(mn,ej)": "ijak",
               "Hbar W(ab,ij)": "abij", "Hbar W(mn,ef)": "ijab", "Hbar W(am,ei)": "aibj",
               "Hbar W(am,ef)": "aibc", "Hbar W(ab,ej)": "abci", "Hbar W(ab,ef)": "abcd"}
-SIZES = {1: (3, 6), 4: (5, 12)}
+SIZES = {1: (3, 6), 4: (5, 12), 8: (8, 16)}
 
 
-@pytest.fixture(scope="module", params=[1, 4], ids=["C1", "D2h-4"])
+@pytest.fixture(scope="module", params=[1, 4, 8], ids=["C1", "4-irreps", "D2h"])
 def problem(request):
     nirrep = request.param
     o, v = SIZES[nirrep]
@@ -132,7 +132,7 @@ RHF_HBAR = {"F(ME)": "FME", "F(MI)": "FMI", "F(AE)": "FAE", "W(Mn,Ij)": "WMNIJ",
             "W(Am,Ij)": "WAMIJ", "W(Am,Ei)": "WAMEI", "W(Ab,Ej)": "WABEJ"}
 
 
-@pytest.fixture(scope="module", params=[1, 4], ids=["C1", "D2h-4"])
+@pytest.fixture(scope="module", params=[1, 4, 8], ids=["C1", "4-irreps", "D2h"])
 def rhf_problem(request):
     from oracle import rhf_ccsd as RH
     nirrep = request.param
