@@ -39,6 +39,21 @@ inline void run_deferred(Recorder& r) {
     }
     for (auto& e : err)
         if (e) std::rethrow_exception(e);
+    // one allocation per step list for the merged plan (a D2h iteration has ~10^5 GEMMs)
+    size_t ng = r.plan->gemms.size(), nsu = r.plan->sums.size(), nsc = r.plan->scales.size(),
+           nd = r.plan->dots.size(), nst = r.plan->steps.size();
+    for (auto& p : out) {
+        ng += p.gemms.size();
+        nsu += p.sums.size();
+        nsc += p.scales.size();
+        nd += p.dots.size();
+        nst += p.steps.size();
+    }
+    r.plan->gemms.reserve(ng);
+    r.plan->sums.reserve(nsu);
+    r.plan->scales.reserve(nsc);
+    r.plan->dots.reserve(nd);
+    r.plan->steps.reserve(nst);
     for (auto& p : out) r.plan->append(std::move(p));
     jobs.clear();
 }

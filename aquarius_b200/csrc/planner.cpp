@@ -253,6 +253,56 @@ void enumerate_dim(const std::vector<Unit>& units, const std::vector<Var>& vars,
 
 constexpr int kMaxVars = 32;   // C positions + internal letters of one statement (at most 8 + 8)
 
+// Offset table of a GEMM dimension: out[k] = base + f(values at point k), points ordered as
+// enumerate_dim orders them (first unit fastest).  Every offset this planner tabulates is a
+// sum of one term per unit: an operand position depends on one variable, and a packed or
+// swapped pair on the two variables of one restricted-pair unit.  So each unit's terms are
+// evaluated once (f at that unit's values, all other variables 0, minus f at all zeros) and
+// the table is their Kronecker sum: O(points) additions instead of O(points x positions).
+template <class F>
+void fill_table(std::vector<int64_t>& out, const std::vector<Unit>& units, const std::vector<Var>& vars, int64_t base,
+                F f) {
+    // per-thread scratch: planning runs statements on several threads, and the tables of a
+    // large plan are filled a few million times
+    thread_local std::vector<int64_t> val, cur, next, term;
+    val.assign(vars.size(), 0);
+    const int64_t f0 = f(val);
+    cur.assign(1, base + f0);
+    for (const Unit& u : units) {
+        term.resize(u.size);
+        // the unit's points in enumerate_dim's order: a value, a rectangle pair (first
+        // variable fastest) or a triangle pair x < y (y outer, x inner)
+        if (u.v1 < 0) {
+            for (int64_t c = 0; c < u.size; c++) {
+                val[u.v0] = c;
+                term[c] = f(val) - f0;
+            }
+        } else if (u.tri) {
+            int64_t c = 0;
+            for (int64_t y = 0; y < vars[u.v0].len; y++)
+                for (int64_t x = 0; x < y; x++) {
+                    val[u.v0] = x;
+                    val[u.v1] = y;
+                    term[c++] = f(val) - f0;
+                }
+        } else {
+            const int64_t n0 = vars[u.v0].len;
+            for (int64_t c = 0; c < u.size; c++) {
+                val[u.v0] = c % n0;
+                val[u.v1] = c / n0;
+                term[c] = f(val) - f0;
+            }
+        }
+        val[u.v0] = 0;
+        if (u.v1 >= 0) val[u.v1] = 0;
+        next.resize(cur.size() * term.size());
+        for (size_t j = 0; j < term.size(); j++)
+            for (size_t t = 0; t < cur.size(); t++) next[j * cur.size() + t] = cur[t] + term[j];
+        cur.swap(next);
+    }
+    out.assign(cur.begin(), cur.end());
+}
+
 int64_t operand_offset(const Operand& op, const std::vector<int64_t>& val, const std::vector<int>& only_vars) {
     // offset of the operand element for the subset of variables `only_vars` (others 0)
     const Block& b = *op.blk;
@@ -430,42 +480,30 @@ void lower_gemm(Context& ctx, Term& t, int hA, int hB, int hC, int cc, std::set<
     g.alpha = t.coef * factor;
 
     std::vector<int> all_m = t.mvars, all_n = t.nvars, all_k = t.kvars;
-    g.hAm.resize(M);
-    g.hAk.resize(K);
-    g.hBk.resize(K);
-    g.hBn.resize(N);
     const Block& bA = *t.A.blk;
     const Block& bB = *t.B.blk;
     const Block& bC = *t.bC;
-    enumerate_dim(mu, vars, [&](int64_t k, const std::vector<int64_t>& val) {
-        g.hAm[k] = bA.offset + operand_offset(t.A, val, all_m);
-    });
-    enumerate_dim(ku, vars, [&](int64_t k, const std::vector<int64_t>& val) {
-        g.hAk[k] = operand_offset(t.A, val, all_k);
-        g.hBk[k] = operand_offset(t.B, val, all_k);
-    });
-    enumerate_dim(nu, vars, [&](int64_t k, const std::vector<int64_t>& val) {
-        g.hBn[k] = bB.offset + operand_offset(t.B, val, all_n);
-    });
+    fill_table(g.hAm, mu, vars, bA.offset, [&](const std::vector<int64_t>& val) { return operand_offset(t.A, val, all_m); });
+    fill_table(g.hAk, ku, vars, 0, [&](const std::vector<int64_t>& val) { return operand_offset(t.A, val, all_k); });
+    fill_table(g.hBk, ku, vars, 0, [&](const std::vector<int64_t>& val) { return operand_offset(t.B, val, all_k); });
+    fill_table(g.hBn, nu, vars, bB.offset, [&](const std::vector<int64_t>& val) { return operand_offset(t.B, val, all_n); });
     if (dest_x) {
         // plain column-major scratch product: no variants
         g.nvm = g.nvn = 1;
         std::vector<char> um(vars.size(), 0), un(vars.size(), 0);
         for (int v : all_m) um[v] = 1;
         for (int v : all_n) un[v] = 1;
-        g.hCm[0].resize(M);
-        g.hCn[0].resize(N);
-        enumerate_dim(mu, vars, [&](int64_t k, const std::vector<int64_t>& val) {
+        fill_table(g.hCm[0], mu, vars, 0, [&](const std::vector<int64_t>& val) {
             int64_t off = 0;
             for (size_t p = 0; p < t.cvar.size(); p++)
                 if (um[t.cvar[p]]) off += dest_x->stride[p] * val[t.cvar[p]];
-            g.hCm[0][k] = off;
+            return off;
         });
-        enumerate_dim(nu, vars, [&](int64_t k, const std::vector<int64_t>& val) {
+        fill_table(g.hCn[0], nu, vars, 0, [&](const std::vector<int64_t>& val) {
             int64_t off = 0;
             for (size_t p = 0; p < t.cvar.size(); p++)
                 if (un[t.cvar[p]]) off += dest_x->stride[p] * val[t.cvar[p]];
-            g.hCn[0][k] = off;
+            return off;
         });
     } else {
         // C destinations (C unpacked): variants swap the values (and irreps) of restricted pairs;
@@ -501,19 +539,15 @@ void lower_gemm(Context& ctx, Term& t, int hA, int hB, int hC, int cc, std::set<
             return off;
         };
         for (int v = 0; v < g.nvm; v++) {
-            g.hCm[v].resize(M);
             const Block& blk = *dest[v][0];
-            enumerate_dim(mu, vars, [&](int64_t k, const std::vector<int64_t>& val) {
-                g.hCm[v][k] = blk.offset + c_off(val, all_m, v, mpairs, blk);
-            });
+            fill_table(g.hCm[v], mu, vars, blk.offset,
+                       [&](const std::vector<int64_t>& val) { return c_off(val, all_m, v, mpairs, blk); });
         }
         for (int v = 0; v < g.nvn; v++) {
-            g.hCn[v].resize(N);
             const Block& blk = *dest[0][v];
             const int64_t shift = dest[0][v]->offset - dest[0][0]->offset;
-            enumerate_dim(nu, vars, [&](int64_t k, const std::vector<int64_t>& val) {
-                g.hCn[v][k] = shift + c_off(val, all_n, v, npairs, blk);
-            });
+            fill_table(g.hCn[v], nu, vars, shift,
+                       [&](const std::vector<int64_t>& val) { return c_off(val, all_n, v, npairs, blk); });
         }
         for (int a = 0; a < g.nvm; a++)
             for (int b = 0; b < g.nvn; b++) g.vsign[a * g.nvn + b] = ((a + b) % 2) ? -1.0 : 1.0;
