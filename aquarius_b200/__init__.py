@@ -200,7 +200,7 @@ def lib():
             "ccsd_rhf_solver_hbar": [vp, P(RHFHbar)],
             "ccsd_solver_hbar": [vp, P(Hamiltonian)],
             "ccsd_ctx_plan_export": [vp, ctypes.c_char_p],
-            "ccsd_plan_export_solver": [ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_char_p],
+            "ccsd_plan_export_solver": [ctypes.c_int, ctypes.c_int, vp, vp, vp, vp, ctypes.c_int, ctypes.c_char_p],
             "ccsd_lambda_solver_create": [vp, P(Hamiltonian), vp, P(Options), P(vp)],
             "ccsd_lambda_plan_query": [ctypes.c_int, vp, vp, P(Options), P(dbl), P(dbl), P(i64)],
             "ccsd_hamiltonian_from_ao": [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp, ctypes.c_int,
@@ -301,12 +301,15 @@ METHODS = {"ccsd": 0, "rhf": 1, "lambda": 2}
 PLANS = {"iteration": 0, "hbar": 1, "energy": 2}
 
 
-def plan_export_solver(method, vrt, occ, which, path):
+def plan_export_solver(method, vrt, occ, which, path, vrt_beta=None, occ_beta=None):
     """Host-only: write one recorded plan of a CCSD / RHF / Lambda solver for these sizes
     (ccsd_plan_export_solver), for replay by a host-side checker."""
     vrt, occ = _ints(vrt), _ints(occ)
-    _check(lib().ccsd_plan_export_solver(METHODS[method], len(vrt), _ptr(vrt), _ptr(occ), PLANS[which],
-                                         str(path).encode()))
+    vb = _ints(vrt_beta) if vrt_beta is not None else None
+    ob = _ints(occ_beta) if occ_beta is not None else None
+    _check(lib().ccsd_plan_export_solver(METHODS[method], len(vrt), _ptr(vrt), _ptr(occ),
+                                         _ptr(vb) if vb is not None else None, _ptr(ob) if ob is not None else None,
+                                         PLANS[which], str(path).encode()))
 
 
 def rhf_plan_query(vrt, occ, diis_order=8, precision="fp64", refine_tol=0.0):

@@ -780,21 +780,25 @@ int ccsd_rhf_solver_create(ccsd_ctx ctx, const ccsd_rhf_hamiltonian* H, const cc
 }
 
 namespace {
-Spaces query_spaces(int nirrep, const int* vrt, const int* occ, int& n) {
+// orbital counts per irrep; the beta counts default to the alpha ones (closed shell)
+Spaces query_spaces(int nirrep, const int* vrt, const int* occ, int& n, const int* vrt_b = nullptr,
+                    const int* occ_b = nullptr) {
     if (nirrep != 1 && nirrep != 2 && nirrep != 4 && nirrep != 8) throw Error(CCSD_ERR_ARG, "nirrep must be 1,2,4,8");
     if (!vrt || !occ) throw Error(CCSD_ERR_ARG, "null orbital counts");
     Spaces S;
     S.nirrep = nirrep;
     n = 0;
     for (int s = 0; s < 2; s++) {
+        const int* v = (s == 1 && vrt_b) ? vrt_b : vrt;
+        const int* o = (s == 1 && occ_b) ? occ_b : occ;
         int ov = 0, oo = 0;
         for (int h = 0; h < nirrep; h++) {
-            S.n[VRT][s][h] = vrt[h];
-            S.n[OCC][s][h] = occ[h];
+            S.n[VRT][s][h] = v[h];
+            S.n[OCC][s][h] = o[h];
             S.off[VRT][s][h] = ov;
             S.off[OCC][s][h] = oo;
-            ov += vrt[h];
-            oo += occ[h];
+            ov += v[h];
+            oo += o[h];
         }
         n = ov + oo;
     }
@@ -878,15 +882,18 @@ int ccsd_lambda_plan_query(int nirrep, const int* vrt, const int* occ, const ccs
     });
 }
 
-int ccsd_plan_export_solver(int method, int nirrep, const int* vrt, const int* occ, int which, const char* path) {
+int ccsd_plan_export_solver(int method, int nirrep, const int* vrt, const int* occ, const int* vrt_beta,
+                            const int* occ_beta, int which, const char* path) {
     return guarded(nullptr, [&] {
         if (!path) throw Error(CCSD_ERR_ARG, "null path");
+        if (method == CCSD_METHOD_RHF && (vrt_beta || occ_beta))
+            throw Error(CCSD_ERR_ARG, "the closed-shell solver has one set of spatial orbitals");
         if (method < CCSD_METHOD_CCSD || method > CCSD_METHOD_LAMBDA) throw Error(CCSD_ERR_ARG, "bad method");
         if (which < CCSD_PLAN_ITERATION || which > CCSD_PLAN_ENERGY) throw Error(CCSD_ERR_ARG, "bad plan");
         if (which == CCSD_PLAN_HBAR && method == CCSD_METHOD_LAMBDA) throw Error(CCSD_ERR_ARG, "Lambda forms no Hbar");
         Context host(-1, nullptr);
         int n = 0;
-        host.spaces = query_spaces(nirrep, vrt, occ, n);
+        host.spaces = query_spaces(nirrep, vrt, occ, n, vrt_beta, occ_beta);
         host.spaces_set = true;
         ccsd_options o;
         options_default(&o);

@@ -326,12 +326,14 @@ int ccsd_lambda_plan_query(int nirrep, const int* vrt, const int* occ, const ccs
                            double* hbar_flops, double* flops_per_iter, int64_t* device_bytes);
 /* Diagnostic: plan a solver on the host for C1 or D2h sizes (unpacked <ab||ef>) and write
  * one of its recorded plans in the format of ccsd_ctx_plan_export, so that a host-side
- * checker can replay the solver's statement list.  method: CCSD_METHOD_*; which:
+ * checker can replay the solver's statement list.  vrt_beta / occ_beta may be NULL (closed
+ * shell; must be NULL for CCSD_METHOD_RHF).  method: CCSD_METHOD_*; which:
  * CCSD_PLAN_ITERATION (the Tau statements, then one iteration's intermediates and
  * residual), CCSD_PLAN_HBAR (CCSD and RHF only) or CCSD_PLAN_ENERGY. */
 enum { CCSD_METHOD_CCSD = 0, CCSD_METHOD_RHF = 1, CCSD_METHOD_LAMBDA = 2 };
 enum { CCSD_PLAN_ITERATION = 0, CCSD_PLAN_HBAR = 1, CCSD_PLAN_ENERGY = 2 };
-int ccsd_plan_export_solver(int method, int nirrep, const int* vrt, const int* occ, int which, const char* path);
+int ccsd_plan_export_solver(int method, int nirrep, const int* vrt, const int* occ, const int* vrt_beta,
+                            const int* occ_beta, int which, const char* path);
 /* algorithmic FP64 flops of one iteration as planned (packed-pair counts) */
 int ccsd_solver_flops(ccsd_solver s, double* flops);
 /* contraction mode the next iteration uses (changes when refine_tol is reached):

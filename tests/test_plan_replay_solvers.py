@@ -3,7 +3,7 @@
 One CCSD iteration (ccsd.cxx:123-180), the spin-orbital Hbar (st2eoperator.hpp:59-130,
 isHbar), one Lambda-CCSD iteration (lambdaccsd.cxx:80-124), the energy reductions, and the
 closed-shell iteration and Hbar (rhfccsd.cxx:110-186, 237-316) are planned on the host for C1
-and D2h sizes (ccsd_plan_export_solver), executed with numpy over the engine's block layout
+and D2h sizes and for the UHF triplet CH2 (alpha and beta spaces differ) (ccsd_plan_export_solver), executed with numpy over the engine's block layout
 (tests/plan_replay.py) and compared with oracle/ccsd_oracle.py, oracle/lambda_ccsd.py and
 oracle/rhf_ccsd.py.  This checks the statement lists in csrc/solver.cpp -- their
 order, assignments, factors and signs -- with the planner's expansion, without a device.
@@ -42,12 +42,16 @@ def problem(request):
 
 
 def _replay(problem, method, which, arrays, tmp_path):
-    occ, vrt = problem[0], problem[1]
+    return _replay_spaces(dict(vrt=problem[1], occ=problem[0]), method, which, arrays, tmp_path)
+
+
+def _replay_spaces(spaces, method, which, arrays, tmp_path):
     path = tmp_path / f"{method}-{which}.txt"
-    A.plan_export_solver(method, vrt, occ, which, path)
+    A.plan_export_solver(method, spaces["vrt"], spaces["occ"], which, path, spaces.get("vrt_beta"),
+                         spaces.get("occ_beta"))
     dump = R.load(path)
     ctx = A.Context(-1)
-    ctx.set_spaces(vrt=vrt, occ=occ)
+    ctx.set_spaces(**spaces)
     store = {}
     for h, t in dump.tensors.items():
         if t.view_of:
@@ -170,3 +174,56 @@ def test_rhf_hbar_plan(rhf_problem, tmp_path):
         check(name, want[key])
     check("W(Am,Ie)", want["WAMIE"].transpose(0, 1, 3, 2))
     ctx.close()
+
+
+@pytest.fixture(scope="module")
+def uhf_problem():
+    """CH2/cc-pVDZ triplet (test/input.aq:47-71): UHF, alpha and beta spaces differ."""
+    import json
+    from pathlib import Path
+    from oracle import scf
+    fixture = json.loads((Path(__file__).parent / "golden" / "molecules.json").read_text())
+    res, Hao, eri = scf.solve_scf(fixture, "ch2-pvdz")
+    H = scf.SpinOrbitalHamiltonian(res, Hao, eri)
+    (na, nb), (va, vb) = H.nocc, H.nvrt
+    cc = O.CCSD(H, diis_order=8)
+    for _ in range(3):
+        cc.iterate()
+    Hb = LC.hbar(H, cc.T.T1, cc.T.T2)
+    lam = LC.LambdaCCSD(Hb, cc.T.T1, cc.T.T2, diis_order=8)
+    lam.iterate()
+    return dict(vrt=[va], occ=[na], vrt_beta=[vb], occ_beta=[nb]), H, cc, Hb, lam
+
+
+def test_uhf_ccsd_iteration_plan(uhf_problem, tmp_path):
+    spaces, H, cc, _, _ = uhf_problem
+    arrays = _h_arrays(H)
+    arrays.update({"T(1)": cc.T.T1, "T(2)": cc.T.T2})
+    check, _, _, ctx = _replay_spaces(spaces, "ccsd", "iteration", arrays, tmp_path)
+    Z1, Z2 = cc.residual(cc.T)
+    check("Z(1)", Z1)
+    check("Z(2)", Z2)
+    ctx.close()
+
+
+def test_uhf_hbar_and_lambda_plans(uhf_problem, tmp_path):
+    spaces, H, cc, Hb, lam = uhf_problem
+    arrays = _h_arrays(H)
+    arrays.update({"T(1)": cc.T.T1, "T(2)": cc.T.T2})
+    check, _, by_name, ctx = _replay_spaces(spaces, "ccsd", "hbar", arrays, tmp_path)
+    for name in HBAR_NAMES:
+        if name in by_name:
+            check(name, Hb[HBAR_NAMES[name]])
+    ctx.close()
+    arrays = {n: Hb[k] for n, k in HBAR_NAMES.items()}
+    arrays.update({"T(2)": cc.T.T2, "L(1)": lam.L.T1, "L(2)": lam.L.T2})
+    check, _, _, ctx = _replay_spaces(spaces, "lambda", "iteration", arrays, tmp_path)
+    Z1, Z2 = lam.residual(lam.L.T1, lam.L.T2)
+    check("Z(1)", Z1)
+    check("Z(2)", Z2)
+    ctx.close()
+
+
+def test_rhf_export_refuses_beta_spaces(tmp_path):
+    with pytest.raises(A.CcsdError):
+        A.plan_export_solver("rhf", [4], [2], "iteration", tmp_path / "p.txt", vrt_beta=[5], occ_beta=[1])
