@@ -35,6 +35,12 @@ Context* device_handle(ccsd_ctx c) {
 }
 // message for entry points that have no context (ccsd_last_error(NULL))
 void set_global_error(const std::string& msg) { g_global_error = msg; }
+// an output argument of the ABI: NULL is a caller error, reported as CCSD_ERR_ARG
+template <class T>
+T& need(T* p) {
+    if (!p) throw Error(CCSD_ERR_ARG, "null output argument");
+    return *p;
+}
 }  // namespace ccsd
 
 using namespace ccsd;
@@ -187,13 +193,13 @@ int ccsd_ctx_synchronize(ccsd_ctx ctx) {
 }
 
 int ccsd_ctx_device_bytes(ccsd_ctx ctx, int64_t* bytes) {
-    return guarded(ctx, [&] { *bytes = from_handle(ctx)->device_bytes; });
+    return guarded(ctx, [&] { need(bytes) = from_handle(ctx)->device_bytes; });
 }
 
 int ccsd_ctx_launch_count(ccsd_ctx ctx, int64_t* count) {
     return guarded(ctx, [&] {
         from_handle(ctx);
-        *count = kern::launch_count();
+        need(count) = kern::launch_count();
     });
 }
 
@@ -271,9 +277,11 @@ int ccsd_ctx_set_spaces(ccsd_ctx ctx, int nirrep, const int* vrt_alpha, const in
         Context* c = from_handle(ctx);
         if (nirrep != 1 && nirrep != 2 && nirrep != 4 && nirrep != 8) throw Error(CCSD_ERR_ARG, "nirrep must be 1,2,4,8");
         if (!c->tensors.empty()) throw Error(CCSD_ERR_ARG, "spaces cannot change while tensors exist");
+        if (!vrt_alpha || !occ_alpha) throw Error(CCSD_ERR_ARG, "null alpha orbital counts");
         Spaces S;
         S.nirrep = nirrep;
-        const int* src[2][2] = {{vrt_alpha, vrt_beta}, {occ_alpha, occ_beta}};
+        // NULL beta counts: closed shell, the same orbitals for both spins
+        const int* src[2][2] = {{vrt_alpha, vrt_beta ? vrt_beta : vrt_alpha}, {occ_alpha, occ_beta ? occ_beta : occ_alpha}};
         for (int sp = 0; sp < 2; sp++)
             for (int s = 0; s < 2; s++) {
                 int off = 0;
@@ -292,7 +300,10 @@ int ccsd_ctx_set_spaces(ccsd_ctx ctx, int nirrep, const int* vrt_alpha, const in
 
 int ccsd_tensor_create(ccsd_ctx ctx, const char* name, const int nout[2], const int nin[2], int flags,
                        ccsd_tensor* out) {
-    return guarded(ctx, [&] { *out = from_handle(ctx)->create_tensor(name ? name : "", nout, nin, flags); });
+    return guarded(ctx, [&] {
+        if (!nout || !nin || !out) throw Error(CCSD_ERR_ARG, "null argument");
+        *out = from_handle(ctx)->create_tensor(name ? name : "", nout, nin, flags);
+    });
 }
 
 int ccsd_tensor_destroy(ccsd_ctx ctx, ccsd_tensor t) {
@@ -300,13 +311,13 @@ int ccsd_tensor_destroy(ccsd_ctx ctx, ccsd_tensor t) {
 }
 
 int ccsd_tensor_ndim(ccsd_ctx ctx, ccsd_tensor t, int* ndim) {
-    return guarded(ctx, [&] { *ndim = from_handle(ctx)->tensor(t).ndim; });
+    return guarded(ctx, [&] { need(ndim) = from_handle(ctx)->tensor(t).ndim; });
 }
 
 int ccsd_tensor_spin_cases(ccsd_ctx ctx, ccsd_tensor t, int* ncases, int* alpha) {
     return guarded(ctx, [&] {
         Tensor& T = from_handle(ctx)->tensor(t);
-        *ncases = (int)T.cases.size();
+        need(ncases) = (int)T.cases.size();
         if (alpha)
             for (size_t c = 0; c < T.cases.size(); c++)
                 for (int g = 0; g < 4; g++) alpha[4 * c + g] = T.cases[c].alpha[g];
@@ -316,8 +327,9 @@ int ccsd_tensor_spin_cases(ccsd_ctx ctx, ccsd_tensor t, int* ncases, int* alpha)
 int ccsd_tensor_block_size(ccsd_ctx ctx, ccsd_tensor t, const int alpha[4], const int* irreps, int64_t* n) {
     return guarded(ctx, [&] {
         Tensor& T = from_handle(ctx)->tensor(t);
+        if (!alpha) throw Error(CCSD_ERR_ARG, "null spin case");
         int cs = T.find_case(alpha);
-        *n = 0;
+        need(n) = 0;
         if (cs < 0) return;
         std::vector<int> irr(T.ndim, 0);
         if (irreps)
@@ -517,6 +529,7 @@ int ccsd_dot(ccsd_ctx ctx, ccsd_tensor A, const char* idxA, ccsd_tensor B, const
 int ccsd_norm(ccsd_ctx ctx, ccsd_tensor A, int p, double* out) {
     return guarded(ctx, [&] {
         Context* c = device_handle(ctx);
+        need(out);
         if (p != 0 && p != 1 && p != 2) throw Error(CCSD_ERR_ARG, "p must be 0, 1 or 2");
         Tensor& T = c->tensor(A);
         CCSD_CUDA(cudaMemsetAsync(c->d_scalar, 0, sizeof(double), c->stream));
@@ -542,7 +555,7 @@ int ccsd_norm(ccsd_ctx ctx, ccsd_tensor A, int p, double* out) {
         double h = 0;
         CCSD_CUDA(cudaMemcpyAsync(&h, c->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
         CCSD_CUDA(cudaStreamSynchronize(c->stream));
-        *out = p == 2 ? std::sqrt(h) : h;
+        need(out) = p == 2 ? std::sqrt(h) : h;
     });
 }
 
@@ -1000,7 +1013,7 @@ int ccsd_solver_destroy(ccsd_solver s) {
 
 int ccsd_solver_mp2(ccsd_solver s, double* mp2) {
     if (!s) return CCSD_ERR_ARG;
-    return guarded(s->ctx, [&] { *mp2 = s->s->mp2; });
+    return guarded(s->ctx, [&] { need(mp2) = s->s->mp2; });
 }
 
 int ccsd_solver_iterate(ccsd_solver s, double* energy, double* conv) {
@@ -1065,7 +1078,7 @@ int ccsd_solver_hbar(ccsd_solver s, ccsd_hamiltonian* out) {
 
 int ccsd_solver_flops(ccsd_solver s, double* flops) {
     if (!s) return CCSD_ERR_ARG;
-    return guarded(s->ctx, [&] { *flops = s->s->flops_per_iter; });
+    return guarded(s->ctx, [&] { need(flops) = s->s->flops_per_iter; });
 }
 
 int ccsd_solver_mode(ccsd_solver s, int* precision, int* slices) {

@@ -118,7 +118,8 @@ int ccsd_ctx_set_profiling(ccsd_ctx ctx, int on);
 int ccsd_ctx_profile_report(ccsd_ctx ctx, char* buf, int64_t buflen, int64_t* needed);
 
 /* Orbital spaces (Space of src/operator/space.hpp): per-irrep counts of
- * alpha/beta virtual and occupied orbitals.  nirrep in {1,2,4,8}. */
+ * alpha/beta virtual and occupied orbitals.  nirrep in {1,2,4,8}.  vrt_beta and
+ * occ_beta may be NULL: closed shell, the alpha counts for both spins. */
 int ccsd_ctx_set_spaces(ccsd_ctx ctx, int nirrep,
                         const int* vrt_alpha, const int* vrt_beta,
                         const int* occ_alpha, const int* occ_beta);
