@@ -16,7 +16,7 @@ carries the FP64 plain path of the same iterations, the end-to-end solve (3 -> 4
 refinement to conv 1e-9) and a bounded serving run.
 
 For N>1 (torchrun, one rank per GPU) every rank runs an independent replica of the
-workload (the north star fixes one GPU per solve: "replicas only"); the value is the
+workload (a solve is not sharded across GPUs: "replicas only"); the value is the
 sum over ranks, timed as the max over ranks.
 
 --impl reference times the reference algorithm's CPU restatement (the oracle, numpy
