@@ -227,3 +227,19 @@ def test_uhf_hbar_and_lambda_plans(uhf_problem, tmp_path):
 def test_rhf_export_refuses_beta_spaces(tmp_path):
     with pytest.raises(A.CcsdError):
         A.plan_export_solver("rhf", [4], [2], "iteration", tmp_path / "p.txt", vrt_beta=[5], occ_beta=[1])
+
+
+def test_replay_tells_a_changed_statement_apart(problem, tmp_path):
+    """The replayed Lambda plan against an oracle residual with one statement's sign
+    flipped (the ring term W(am,ei) L2, lambdaccsd.cxx:124) no longer matches."""
+    _, _, _, cc, Hb, lam = problem
+    arrays = {n: Hb[k] for n, k in HBAR_NAMES.items()}
+    arrays.update({"T(2)": cc.T.T2, "L(1)": lam.L.T1, "L(2)": lam.L.T2})
+    check, _, _, ctx = _replay(problem, "lambda", "iteration", arrays, tmp_path)
+    _, Z2 = lam.residual(lam.L.T1, lam.L.T2)
+    ring = LC.contract(1.0, Hb["aibj"], "eiam", lam.L.T2, "mjbe", "ijab", LC.SHAPES["ijab"])
+    assert np.abs(ring).max() > 1e-6
+    check("Z(2)", Z2)
+    with pytest.raises(AssertionError):
+        check("Z(2)", Z2 - 2.0 * ring)
+    ctx.close()
