@@ -3,9 +3,10 @@
 // The regular reductions of the engine keep their per-block partial sums in scratch
 // that the library allocates itself (a buffer per stream, created on first use).  Some
 // callers cannot allow that: an application that owns every byte of device memory
-// through its own arena and forbids allocations by libraries, or code that issues the
-// call while a CUDA stream is being captured into a graph, where a cudaMalloc is not
-// permitted.  ccsd_dot_batch_noalloc gives them the same computation as the DIIS
+// through its own arena (a memory pool sized at start-up, or a framework's caching
+// allocator) and forbids libraries to allocate behind its back, because an allocation
+// it does not know of can push its own pool out of memory or make its accounting
+// wrong.  ccsd_dot_batch_noalloc gives them the same computation as the DIIS
 // error-matrix row (out[j] = <x, y_j>) with the scratch placed in a fixed file-scope
 // device array instead: the caller passes inputs and outputs, the library allocates
 // nothing.
@@ -18,7 +19,12 @@
 //    streams, or two threads) race; serialise them on one stream;
 //  * the first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress (no allocation); make that first call before any stream
-//    capture begins.
+//    capture begins;
+//  * that address is kept per device number for the life of the process: it does not
+//    survive cudaDeviceReset (or a reset of the primary context by other code), after
+//    which the entry point must not be called again in this process;
+//  * a CUDA error left pending by earlier work on the calling thread is reported and
+//    left in place for its owner: the call then launches nothing.
 #include <cstdint>
 #include <cstdio>
 #include <mutex>
@@ -136,11 +142,26 @@ extern "C" int ccsd_dot_batch_noalloc(void* stream, const double* x, const doubl
     int64_t want = (n + kThreads - 1) / kThreads;
     const int nblocks = (int)(want < 1 ? 1 : (want > kBlocks ? kBlocks : want));
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // an error pending from earlier, unrelated work belongs to that work: report it without
+    // consuming it, and launch nothing
+    e = cudaPeekAtLastError();
+    if (e != cudaSuccess) {
+        ccsd::set_global_error(std::string("ccsd_dot_batch_noalloc: a CUDA error from earlier work is pending: ") +
+                               cudaGetErrorString(e));
+        return CCSD_ERR_CUDA;
+    }
     dot_partials<<<nblocks, kThreads, 0, s>>>(x, v, ny, n, scratch);
+    e = cudaGetLastError();   // nothing was pending, so an error here is this launch's
+    if (e != cudaSuccess) {
+        ccsd::set_global_error(std::string("ccsd_dot_batch_noalloc: launch of the partial sums failed: ") +
+                               cudaGetErrorString(e));
+        return CCSD_ERR_CUDA;
+    }
     dot_fold<<<1, kThreads, 0, s>>>(scratch, nblocks, ny, out);
     e = cudaGetLastError();
     if (e != cudaSuccess) {
-        ccsd::set_global_error(std::string("ccsd_dot_batch_noalloc: launch failed: ") + cudaGetErrorString(e));
+        ccsd::set_global_error(std::string("ccsd_dot_batch_noalloc: launch of the fold failed: ") +
+                               cudaGetErrorString(e));
         return CCSD_ERR_CUDA;
     }
     return CCSD_OK;

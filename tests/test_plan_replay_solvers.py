@@ -231,7 +231,10 @@ def test_rhf_export_refuses_beta_spaces(tmp_path):
 
 def test_replay_tells_a_changed_statement_apart(problem, tmp_path):
     """The replayed Lambda plan against an oracle residual with one statement's sign
-    flipped (the ring term W(am,ei) L2, lambdaccsd.cxx:124) no longer matches."""
+    flipped (the ring term W(am,ei) L2, lambdaccsd.cxx:124) no longer matches.  `ring` is
+    the statement's full contribution: LC.contract applies the statement's implicit
+    antisymmetriser P(ij)P(ab) to the output lines that come from both factors, so
+    Z2 - 2 * ring is the residual with that term's sign flipped."""
     _, _, _, cc, Hb, lam = problem
     arrays = {n: Hb[k] for n, k in HBAR_NAMES.items()}
     arrays.update({"T(2)": cc.T.T2, "L(1)": lam.L.T1, "L(2)": lam.L.T2})
