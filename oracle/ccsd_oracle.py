@@ -133,6 +133,21 @@ def P23(x):
 
 
 def es(spec, *ops):
+    """einsum of the statements.  A two-factor contraction without batch (Hadamard) indices
+    goes through one tensordot (a BLAS GEMM after transposes); numpy's einsum path search
+    left some of the iteration's terms (e.g. 'amef,efim->ai') off BLAS, 10x slower."""
+    if len(ops) == 2:
+        ins, out = spec.split('->')
+        ia, ib = ins.split(',')
+        con = [c for c in ia if c in ib and c not in out]
+        plain = (len(set(ia)) == len(ia) and len(set(ib)) == len(ib)
+                 and all((c in out) != (c in con) for c in ia + ib))
+        if plain:
+            fa = [c for c in ia if c not in con]
+            fb = [c for c in ib if c not in con]
+            r = np.tensordot(ops[0], ops[1], axes=([ia.index(c) for c in con], [ib.index(c) for c in con]))
+            cur = fa + fb
+            return r.transpose([cur.index(c) for c in out])
     return np.einsum(spec, *ops, optimize=True)
 
 
@@ -249,6 +264,8 @@ class CCSD:
         self.energy = self.mp2
         self.conv = np.finfo(float).max
         self.iter = 0
+        self.keep_intermediates = False   # residual() keeps its intermediates (CPU tests)
+        self.intermediates = None
 
     @staticmethod
     def make_tau(T):
@@ -261,12 +278,14 @@ class CCSD:
         if H.VABEF is not None:
             return 0.5 * es('abef,efij->abij', H.VABEF, Tau)
         v, o2 = H.v, 2 * H.o
-        tr = Tau.reshape(2, v, 2, v, o2, o2)
-        out = np.zeros((2, v, 2, v, o2, o2))
-        for sa in (0, 1):
-            for sb in (0, 1):
-                out[sa, :, sb, :] = np.tensordot(H.eri_vvvv, tr[sa, :, sb, :], axes=((1, 3), (0, 1)))
-        return out.reshape(2 * v, 2 * v, o2, o2)
+        if getattr(H, "_vvvv_ab_ef", None) is None:
+            # (ae|bf) as a [ab, ef] matrix, formed once: each spin case is then one GEMM
+            H._vvvv_ab_ef = np.ascontiguousarray(H.eri_vvvv.transpose(0, 2, 1, 3)).reshape(v * v, v * v)
+        tr = Tau.reshape(2, v, 2, v, o2 * o2)
+        # the four (sa, sb) spin cases side by side: [ef, (sa, sb, ij)]
+        rhs = np.ascontiguousarray(tr.transpose(1, 3, 0, 2, 4)).reshape(v * v, 4 * o2 * o2)
+        out = (H._vvvv_ab_ef @ rhs).reshape(v, v, 2, 2, o2, o2)
+        return np.ascontiguousarray(out.transpose(2, 0, 3, 1, 4, 5)).reshape(2 * v, 2 * v, o2, o2)
 
     def residual(self, T: Amplitudes):
         """ccsd.cxx:123-180: intermediates and the unweighted Z(1), Z(2)."""
@@ -317,6 +336,9 @@ class CCSD:
         Z2 += self.ladder(Tau)
         Z2 += 0.5 * es('mnij,abmn->abij', WMNIJ, Tau)
         Z2 += P23(P01(es('amei,ebjm->abij', WAMEI, T2)))
+        if self.keep_intermediates:
+            self.intermediates = dict(Tau=Tau, FME=FME, FMI=FMI, FAE=FAE, WMNIJ=WMNIJ, WMNEJ=WMNEJ, WAMIJ=WAMIJ,
+                                      WAMEI=WAMEI, Z1=Z1, Z2=Z2)
         return Z1, Z2
 
     def energy_of(self, T: Amplitudes):

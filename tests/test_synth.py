@@ -49,3 +49,28 @@ def test_rhf_plan_query_plans_every_statement():
     # a solve that may refine to 4 slices reserves the larger slice cache
     _, b_ref = A.rhf_plan_query([256], [32], precision="split", refine_tol=1e-7)
     assert b_ref >= b_rhf
+
+
+import pytest
+
+
+@pytest.mark.parametrize("seed,o,v,nirrep", [(2, 16, 128, 1), (6, 16, 96, 8), (3, 5, 19, 4), (11, 12, 40, 2)])
+def test_numpy_restatement_is_bit_identical(built_lib, seed, o, v, nirrep):
+    """oracle/synth.py (which the CPU benchmark legs use, loading no engine library) gives
+    the same bits as ccsd_synth_problem: orbital energies, irrep counts and the factor."""
+    from oracle import synth as S
+    e1, B1, occ1, vrt1, aux1 = A.synth_problem(seed, o, v, nirrep=nirrep)
+    e2, B2, occ2, vrt2, aux2 = S.synth_problem(seed, o, v, nirrep=nirrep)
+    for x, y in ((occ1, occ2), (vrt1, vrt2), (aux1, aux2)):
+        assert np.array_equal(x, y)
+    assert np.array_equal(e1.view(np.uint64), e2.view(np.uint64))
+    assert np.array_equal(B1.view(np.uint64), B2.view(np.uint64))
+
+
+def test_numpy_restatement_irrep_counts_at_the_d2h_benchmark_size(built_lib):
+    from oracle import synth as S
+    for seed in (4, 5, 1000, 1001):
+        got = S.synth_irreps(seed, 8, 48, 336)
+        ref = A.synth_irreps(seed, 8, 48, 336)
+        for x, y in zip(got, ref):
+            assert np.array_equal(x, y)
