@@ -34,6 +34,26 @@ def test_result_alone_equals_result_in_mix():
         assert a["conv"] < 1e-10
 
 
+# large enough that natural routing puts the particle ladder and other big products on the
+# tcgen05 split kernel (o=12 v=96: ladder blocks M = K = v^2, N = o^2)
+MIX_SPLIT = [(12, 96, 1, 21), (4, 24, 1, 11), (10, 70, 1, 22), (8, 26, 8, 16), (6, 36, 1, 13)]
+
+
+def test_split_graph_result_alone_equals_result_in_mix():
+    """The precision the benchmark serves with: INT8 split slices with the 3 -> 4 slice
+    refinement, every iteration replayed as a CUDA graph."""
+    kw = dict(precision="split_i8", refine_tol=1e-5, use_graph=True)
+    mixed, st = _serve(MIX_SPLIT, max_active=8, **kw)
+    assert st["peak_active"] >= 2
+    for key in MIX_SPLIT:
+        alone, _ = _serve([key], max_active=1, **kw)
+        a, m = alone[key], mixed[key]
+        assert a["status"] == 0 and m["status"] == 0, (key, a["message"], m["message"])
+        assert a["iterations"] == m["iterations"]
+        assert abs(a["energy"] - m["energy"]) <= 1e-12, (key, a["energy"], m["energy"])
+        assert a["conv"] < 1e-10
+
+
 def test_served_solve_matches_direct_solver():
     o, v, h, s = MIX[1]
     res, _ = _serve([MIX[1]], max_active=1)
