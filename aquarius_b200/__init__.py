@@ -54,6 +54,7 @@ EXPORTS = [
     "ccsd_rhf_solver_create", "ccsd_rhf_plan_query", "ccsd_hamiltonian_from_ao", "ccsd_rhf_hamiltonian_from_ao",
     "ccsd_rhf_solver_hbar", "ccsd_ctx_plan_flops", "ccsd_solver_hbar", "ccsd_lambda_solver_create",
     "ccsd_lambda_plan_query", "ccsd_ctx_plan_export", "ccsd_plan_export_solver",
+    "ccsd_diis_create", "ccsd_diis_extrapolate", "ccsd_diis_coefficients", "ccsd_diis_destroy",
 ]
 
 
@@ -183,6 +184,10 @@ def lib():
                                               P(dbl)],
             "ccsd_solver_create": [vp, P(Hamiltonian), P(Options), P(vp)],
             "ccsd_solver_destroy": [vp],
+            "ccsd_diis_create": [vp, ctypes.c_int, ctypes.c_int, dbl, P(vp)],
+            "ccsd_diis_extrapolate": [vp, ctypes.c_int, vp, vp, vp],
+            "ccsd_diis_coefficients": [vp, P(ctypes.c_int), vp],
+            "ccsd_diis_destroy": [vp],
             "ccsd_solver_mp2": [vp, P(dbl)],
             "ccsd_solver_iterate": [vp, P(dbl), P(dbl)],
             "ccsd_solver_iterate_async": [vp],
@@ -769,6 +774,41 @@ class Context:
 
     def solver(self, H, **kw):
         return Solver(self, H, **kw)
+
+    def diis(self, order=5, start=1, damping=0.0):
+        """DIIS over caller tensors (ccsd_diis_*), the reference's DIIS<T>."""
+        return Diis(self, order, start, damping)
+
+
+class Diis:
+    """DIIS<T>::extrapolate (src/convergence/diis.hpp:70-227) on the device over engine
+    tensors: extrapolate([T1, T2], [Z1, Z2]) overwrites both lists with the combinations."""
+
+    def __init__(self, ctx, order, start, damping):
+        self.ctx, self.order = ctx, order
+        d = ctypes.c_void_p()
+        _check(lib().ccsd_diis_create(ctx.c, order, start, float(damping), ctypes.byref(d)), ctx.c)
+        self.d = d
+
+    def extrapolate(self, x, dx, weights=None):
+        n = len(x)
+        xa = np.array([t.h for t in x], dtype=np.int32)
+        da = np.array([t.h for t in dx], dtype=np.int32)
+        w = None if weights is None else np.ascontiguousarray(np.asarray(weights, dtype=np.float64))
+        _check(lib().ccsd_diis_extrapolate(self.d, n, _ptr(xa), _ptr(da), None if w is None else _ptr(w)),
+               self.ctx.c)
+
+    def coefficients(self):
+        """(stored pairs, coefficients by age: c[0] for the pair just stored)"""
+        n = ctypes.c_int()
+        c = np.zeros(max(self.order, 1))
+        _check(lib().ccsd_diis_coefficients(self.d, ctypes.byref(n), _ptr(c)), self.ctx.c)
+        return n.value, c
+
+    def close(self):
+        if self.d:
+            _check(lib().ccsd_diis_destroy(self.d), self.ctx.c)
+            self.d = None
 
 
 class HamiltonianHandle:

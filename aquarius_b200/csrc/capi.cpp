@@ -5,6 +5,7 @@
 #include <cstring>
 #include <sstream>
 
+#include "diis.hpp"
 #include "engine.hpp"
 #include "hbuild.hpp"
 #include "solver.hpp"
@@ -998,6 +999,50 @@ int ccsd_lambda_solver_create(ccsd_ctx ctx, const ccsd_hamiltonian* hbar, ccsd_s
         }
         *out = h;
     });
+}
+
+// ---- DIIS over caller tensors (diis.hpp:36-228) ----------------------------------------
+
+struct ccsd_diis_s {
+    ccsd_ctx ctx = nullptr;
+    DiisRing* d = nullptr;
+};
+
+int ccsd_diis_create(ccsd_ctx ctx, int order, int start, double damping, ccsd_diis* out) {
+    if (!out) return CCSD_ERR_ARG;
+    *out = nullptr;
+    return guarded(ctx, [&] {
+        Context* c = device_handle(ctx);
+        auto* h = new ccsd_diis_s;
+        h->ctx = ctx;
+        try {
+            h->d = new DiisRing(*c, order, start, damping);
+        } catch (...) {
+            delete h;
+            throw;
+        }
+        *out = h;
+    });
+}
+
+int ccsd_diis_extrapolate(ccsd_diis d, int n, const ccsd_tensor* x, const ccsd_tensor* dx, const double* weights) {
+    if (!d) return CCSD_ERR_ARG;
+    return guarded(d->ctx, [&] {
+        if (n < 1 || !x || !dx) throw Error(CCSD_ERR_ARG, "DIIS: n >= 1 pieces and non-null x, dx needed");
+        d->d->extrapolate(std::vector<int>(x, x + n), std::vector<int>(dx, dx + n), weights);
+    });
+}
+
+int ccsd_diis_coefficients(ccsd_diis d, int* nvec, double* c) {
+    if (!d) return CCSD_ERR_ARG;
+    return guarded(d->ctx, [&] { need(nvec) = d->d->coefficients(c); });
+}
+
+int ccsd_diis_destroy(ccsd_diis d) {
+    if (!d) return CCSD_ERR_ARG;
+    int st = guarded(d->ctx, [&] { delete d->d; });
+    delete d;
+    return st;
 }
 
 int ccsd_solver_destroy(ccsd_solver s) {

@@ -172,6 +172,14 @@ void diis_dots(const int* state, const double* const* dxs, int order, int64_t of
 // update the error matrix with the new row, solve the bordered system and write the
 // coefficients by slot into c (unit vector at head when no extrapolation happens)
 void diis_solve(int* state, double* e, double* c, const double* dots, int order, cudaStream_t s);
+// standalone DIIS over caller tensors: one (x, dx) piece into the head slot at `off`
+void diis_store_segment(const int* state, const double* const* xs, const double* const* dxs, int64_t off,
+                        const double* x, const double* dx, int64_t len, cudaStream_t s);
+// out[i] = sum_j c[j] * xs[j][off + i], i < len
+void lincomb_segment(double* out, int64_t len, const double* const* xs, int64_t off, const double* c, int nx,
+                     cudaStream_t s);
+// the damping branch of diis.hpp:155-161 on the stored newest x (after diis_solve)
+void diis_damp(const int* state, const double* const* xs, int order, int64_t len, double damping, cudaStream_t s);
 
 // Pack <ab||cd> = J - K for canonical pairs of a packed block, a in [a0,a1):
 //   J = tJ[a-a0, c, b, d] = (ac|bd),  K = tK[a-a0, d, b, c] = (ad|bc)

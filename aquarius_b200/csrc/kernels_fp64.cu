@@ -1321,6 +1321,43 @@ __global__ void diis_solve_kernel(int* st, double* e, double* c, const double* d
     for (int i = 0; i < cnt; i++) c[slot(i)] = b[i];
 }
 
+// one piece of a caller's (x, dx) pair into the head slot at offset `off`
+__global__ void diis_store_segment_kernel(const int* st, const double* const* xs, const double* const* dxs,
+                                          int64_t off, const double* __restrict__ x, const double* __restrict__ dx,
+                                          int64_t len) {
+    const int h = st[0];
+    double* rx = const_cast<double*>(xs[h]) + off;
+    double* rdx = const_cast<double*>(dxs[h]) + off;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x) {
+        rx[i] = x[i];
+        rdx[i] = dx[i];
+    }
+}
+
+// out[i] = sum_j c[j] * xs[j][off + i]
+__global__ void lincomb_segment_kernel(double* __restrict__ out, int64_t len, const double* const* xs, int64_t off,
+                                       const double* c, int nx) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x) {
+        double s = 0;
+        for (int j = 0; j < nx; j++) {
+            double cj = c[j];
+            if (cj != 0.0) s += cj * xs[j][off + i];
+        }
+        out[i] = s;
+    }
+}
+
+// diis.hpp:155-161: while the start counter is above 1 (and two vectors are stored), the
+// stored newest x becomes (damping - 1) x_0 + damping x_1
+__global__ void diis_damp_kernel(const int* st, const double* const* xs, int order, int64_t len, double damping) {
+    if (st[1] < 2 || st[2] <= 1) return;
+    const int h = st[0], p = (st[0] - 1 + order) % order;
+    double* x0 = const_cast<double*>(xs[h]);
+    const double* x1 = xs[p];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < len; i += (int64_t)gridDim.x * blockDim.x)
+        x0[i] = (damping - 1.0) * x0[i] + damping * x1[i];
+}
+
 }  // namespace
 
 namespace {
@@ -1467,6 +1504,26 @@ void diis_dots(const int* state, const double* const* dxs, int order, int64_t of
 
 void diis_solve(int* state, double* e, double* c, const double* dots, int order, cudaStream_t s) {
     diis_solve_kernel<<<1, 32, 0, s>>>(state, e, c, dots, order);
+    COUNT_LAUNCH();
+}
+
+void diis_store_segment(const int* state, const double* const* xs, const double* const* dxs, int64_t off,
+                        const double* x, const double* dx, int64_t len, cudaStream_t s) {
+    if (len <= 0) return;
+    diis_store_segment_kernel<<<ew_blocks(len), EW_THREADS, 0, s>>>(state, xs, dxs, off, x, dx, len);
+    COUNT_LAUNCH();
+}
+
+void lincomb_segment(double* out, int64_t len, const double* const* xs, int64_t off, const double* c, int nx,
+                     cudaStream_t s) {
+    if (len <= 0) return;
+    lincomb_segment_kernel<<<ew_blocks(len), EW_THREADS, 0, s>>>(out, len, xs, off, c, nx);
+    COUNT_LAUNCH();
+}
+
+void diis_damp(const int* state, const double* const* xs, int order, int64_t len, double damping, cudaStream_t s) {
+    if (len <= 0 || damping <= 0.0) return;
+    diis_damp_kernel<<<ew_blocks(len), EW_THREADS, 0, s>>>(state, xs, order, len, damping);
     COUNT_LAUNCH();
 }
 

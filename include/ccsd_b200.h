@@ -349,18 +349,45 @@ int ccsd_solver_mode(ccsd_solver s, int* precision, int* slices);
 int ccsd_plan_query(int nirrep, const int* vrt_per_irrep, const int* occ_per_irrep, const ccsd_options* opts,
                     int pack_vvvv, double* flops_per_iter, int64_t* device_bytes);
 
+/* ---- DIIS over caller tensors ------------------------------------------------
+ * DIIS<T> of src/convergence/diis.hpp:36-228: its constructor (order, start, damping) and
+ * extrapolate(x, dx) (:70-227), which CCSD<U>::iterate calls at src/cc/ccsd.cxx:192; for
+ * a caller that keeps its own iteration (the solvers run the same DIIS internally).
+ * A vector is the concatenation of n tensor pieces (e.g. {T1, T2}): x[k] and dx[k] have
+ * the same shape, and every call passes pieces of the first call's shapes.  The inner
+ * product is sum_k w_k <a_k, b_k> over full spin-orbital ranges, with w_k = weights[k],
+ * or, for weights NULL, 1 / (upper! lower!) of piece k: 1 for T1 and 1/4 for T2, as
+ * ExcitationOperator::dot (src/operator/excitationoperator.hpp:77-87); plain tensors 1.
+ * Each call stores copies of x and dx in a device ring of `order` pairs, adds the new
+ * error-matrix row, and once two pairs are stored and the start counter allows it solves
+ * the bordered system (Lagrange row -1, an eps-shifted retry when singular) and overwrites
+ * x and dx with sum c_i x_i and sum c_i dx_i; otherwise x and dx keep their values.
+ * damping > 0 applies the reference's damping of the stored newest x while the start
+ * counter is above 1.  The call synchronises the context's stream and returns
+ * CCSD_ERR_SINGULAR if the system stays singular.  Packed tensors are refused.  Destroy
+ * the DIIS object before its context. */
+typedef struct ccsd_diis_s* ccsd_diis;
+int ccsd_diis_create(ccsd_ctx ctx, int order, int start, double damping, ccsd_diis* out);
+int ccsd_diis_extrapolate(ccsd_diis d, int n, const ccsd_tensor* x, const ccsd_tensor* dx, const double* weights);
+/* coefficients of the last extrapolation by age (c[0]: the pair just stored), `order`
+ * entries; *nvec = stored pairs (c is a unit vector when no extrapolation happened) */
+int ccsd_diis_coefficients(ccsd_diis d, int* nvec, double* c);
+int ccsd_diis_destroy(ccsd_diis d);
+
 /* ---- allocation-free variant -------------------------------------------------
  * No counterpart in the reference.  out[j] = <x, ys[j]> for j < ny, the batched dot of
  * the DIIS error-matrix row, for callers that must not have the library allocate device
- * memory (an application owning all device memory through its own arena, or a call
- * issued while a stream is being captured).  x, every ys[j] (n doubles each) and out
+ * memory (an application that owns all device memory through its own arena or pool and
+ * forbids libraries to allocate behind its back).  x, every ys[j] (n doubles each) and out
  * (ny doubles) are caller-owned device buffers on the current device; ys itself is a
  * HOST array of ny device pointers; work is ordered on `stream` (a cudaStream_t, NULL
  * for the default stream) and the call does not synchronise.  The partial sums live in
  * a fixed 32 KiB device array inside the library: ny is limited to 1..16 (else
  * CCSD_ERR_ARG, message in ccsd_last_error(NULL)); calls whose kernels overlap on the
  * GPU share that array and race, so serialise them; the first call on a device looks
- * the array up with cudaGetSymbolAddress and should precede any stream capture. */
+ * the array up with cudaGetSymbolAddress and should precede any stream capture; that
+ * address does not survive cudaDeviceReset.  A CUDA error pending from earlier work is
+ * reported (CCSD_ERR_CUDA) and left in place, and nothing is launched. */
 int ccsd_dot_batch_noalloc(void* stream, const double* x, const double* const* ys, int ny, int64_t n,
                            double* out);
 

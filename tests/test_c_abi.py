@@ -1,7 +1,7 @@
 """The C-ABI from plain C: include/ccsd_b200.h compiles as C11 with warnings as errors, and a
 C program drives the library on a planning-only context (no device): spaces, tensors, one
-contraction statement and its flop count, the CCSD and Lambda plan queries, error codes and
-messages.  This is the binding surface a cgo / JNI / ctypes caller sees."""
+contraction statement and its flop count, the CCSD and Lambda plan queries, the DIIS entry
+points' argument checks, error codes and messages.  This is the binding surface a cgo / JNI / ctypes caller sees."""
 import os
 import shutil
 import subprocess
@@ -52,6 +52,14 @@ int main(void) {
     CHECK(ccsd_tensor_block_size(ctx, T, alpha, irr, &nb));
     if (nd != 4 || nb != 6 * 6 * 2 * 2) return 1;
     (void)none;
+    /* DIIS over caller tensors needs tensors with data: refused on a planning context;
+       NULL handles and outputs are argument errors */
+    ccsd_diis d = NULL;
+    if (ccsd_diis_create(ctx, 8, 1, 0.0, &d) != CCSD_ERR_UNSUPPORTED || d != NULL) return 1;
+    if (ccsd_diis_create(ctx, 8, 1, 0.0, NULL) != CCSD_ERR_ARG) return 1;
+    if (ccsd_diis_extrapolate(NULL, 1, &T, &Z, NULL) != CCSD_ERR_ARG) return 1;
+    if (ccsd_diis_coefficients(NULL, &nd, NULL) != CCSD_ERR_ARG) return 1;
+    if (ccsd_diis_destroy(NULL) != CCSD_ERR_ARG) return 1;
     CHECK(ccsd_ctx_destroy(ctx));
 
     ccsd_options o;
