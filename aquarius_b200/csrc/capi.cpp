@@ -1129,8 +1129,8 @@ int ccsd_solver_flops(ccsd_solver s, double* flops) {
 int ccsd_solver_mode(ccsd_solver s, int* precision, int* slices) {
     if (!s) return CCSD_ERR_ARG;
     return guarded(s->ctx, [&] {
-        if (precision) *precision = s->s->ctx.precision;
-        if (slices) *slices = s->s->ctx.split_slices();
+        if (precision) *precision = s->s->mode_precision;
+        if (slices) *slices = s->s->mode_slices >= 3 ? s->s->mode_slices : 3;
     });
 }
 

@@ -142,8 +142,9 @@ void Solver::setup() {
     if (opts.slices != 0 &&
         !kern::slice_scheme_ok(opts.precision == CCSD_PREC_SPLIT_I8 ? kern::SLICE_INT8 : kern::SLICE_BF16, opts.slices))
         throw Error(CCSD_ERR_ARG, "slices must be 0 (default) or 3, 4 (BF16) / 3, 4, 5 (INT8)");
-    ctx.precision = opts.precision;
-    ctx.slices = opts.slices;
+    mode_precision = opts.precision;
+    mode_slices = opts.slices;
+    use_mode();
     // constants: the H blocks never change, so their split slices can be cached
     for (int t : constants()) ctx.constant_tensors.push_back(t);
     constants_registered = true;
@@ -706,6 +707,7 @@ void Solver::hbar_rhf() {
         ctx.upload(hbar_plan);
     }
     if (ctx.host_only) return;
+    use_mode();
     ctx.run(hbar_plan);
     CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
 }
@@ -861,6 +863,7 @@ void Solver::hbar_so() {
         hbar_formed = true;
     }
     if (ctx.host_only) return;
+    use_mode();
     ctx.run(hbar_plan);
     CCSD_CUDA(cudaStreamSynchronize(ctx.stream));
 }
@@ -962,6 +965,7 @@ void Solver::iterate_async() {
     // for BF16, ~8x higher for INT8); once conv < refine_tol the contractions move to four
     // slices, and on a stall above conv_tol to five (INT8) and then to native FP64.
     // Graphs are recaptured after a switch.
+    use_mode();
     const bool split_opts = opts.precision == CCSD_PREC_SPLIT || opts.precision == CCSD_PREC_SPLIT_I8;
     if (split_opts && opts.refine_tol > 0 && conv < opts.refine_tol && ctx.precision != CCSD_PREC_FP64) {
         bool escalate = false;
@@ -987,6 +991,8 @@ void Solver::iterate_async() {
             }
         }
         if (escalate) {
+            mode_precision = ctx.precision;
+            mode_slices = ctx.slices;
             refined = true;
             conv_hist.clear();
             // the stored vectors carry the previous mode's contraction noise, which would

@@ -56,6 +56,14 @@ public:
     cudaGraphExec_t graph_exec = nullptr;
     bool captured_once = false;
     bool refined = false;           // moved to a more accurate contraction mode (refine_tol reached)
+    // this solver's contraction mode (precision, slices): the context's routing fields are
+    // shared by every solver on it, so each entry point that launches contractions first
+    // puts the solver's own mode in place (use_mode) and a refinement switch updates it
+    int mode_precision = CCSD_PREC_FP64, mode_slices = 0;
+    void use_mode() {
+        ctx.precision = mode_precision;
+        ctx.slices = mode_slices;
+    }
     std::vector<double> conv_hist;  // residuals since the last mode switch (stall detection)
     std::vector<kern::TauArgs> tau_blocks;
     // one-launch Tau and Jacobi update over all blocks: device descriptors and chunk starts

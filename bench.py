@@ -428,6 +428,8 @@ KERNELS = {
     "ladder": (((2, 0), (2, 0)), True, "abef", ((2, 0), (0, 2)), "efij", ((2, 0), (0, 2)), "abij"),
     # skinny ring piece  W(am,ei) += 1/2 VAMEF["amef"] * T1["fi"]  (N = o)
     "skinny": (((1, 1), (2, 0)), False, "amef", ((1, 0), (0, 1)), "fi", ((1, 1), (1, 1)), "amei"),
+    # matrix-vector product  F(ae) += 1/2 VAMEF["amef"] * T1["fm"]  (N = 1)
+    "fae": (((1, 1), (2, 0)), False, "amef", ((1, 0), (0, 1)), "fm", ((1, 0), (1, 0)), "ae"),
 }
 
 
@@ -519,7 +521,7 @@ def run_kernel(args):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--kernel", default=None, choices=[None, "ladder", "skinny", "aomo"],
+    ap.add_argument("--kernel", default=None, choices=[None, "ladder", "skinny", "fae", "aomo"],
                     help="micro-benchmark one contraction kernel instead of the iteration")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
