@@ -564,6 +564,11 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
     auto groupable = [&](const GemmStep& g) {
         if (routes_split(g) || g.M <= 0 || g.N <= 0 || g.K <= 0) return false;
         if (kern::fp64_tiles(g.M, g.N) >= 148) return false;
+        // a skinny product (one extent <= 32) with a long operand of 4M elements or more is
+        // bandwidth work for the skinny kernel: on a 128 x 64 tile it would use 1/64 to 1/2
+        // of every tile (F(ae) += <am||ef> t(fm) at o=16 v=128: 2.3 ms grouped)
+        if (!fp64_tiled_only && std::min(g.M, g.N) <= 32 && (int64_t)std::max(g.M, g.N) * g.K >= (int64_t)1 << 22)
+            return false;
         // a grouped tile walks the whole K range: long-K products keep their split-K launch
         if (g.flops() < 4e8 && g.K <= 4096) return true;
         return kern::fp64_ksplit(g.M, g.N, g.K, !fp64_tiled_only) == 1 && kern::fp64_ksplit(g.M, g.N, g.K, false) == 1;

@@ -265,6 +265,10 @@ struct SumDesc {
     // two tiles
     int tiled = 0, p0 = 0, pc = 0;
     int64_t ntiles = 0;
+    // every index below 2^31: the element index splits into positions by multiply-shift
+    // (x / len = (umulhi(x, mul) + x) >> shr) instead of 64-bit divisions
+    int fast = 0;
+    uint32_t dmul[8], dshr[8];
 };
 // chunks of kBatchChunk elements (or two 32 x 32 tiles) a sum descriptor takes
 inline int64_t sum_chunks(const SumDesc& d) {

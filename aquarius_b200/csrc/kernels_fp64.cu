@@ -299,12 +299,15 @@ __global__ void splitk_fold_kernel(GemmArgs g, int ks) {
 // ---------------------------------------------------------------------------
 // Skinny FP64 product: one small extent (<= 32) against a long operand.
 //   C[Cr_v[r] + Cs_w[s]] += sign_vw * alpha * sum_k L[Lr[r] + Lk[k]] * S[Sk[k] + Sn[s]]
-// The long operand L streams through shared memory in TM x KC tiles (cp.async, three
-// stages, coalesced along whichever of r / k is contiguous); the small operand's KC x 8*NT
-// tile is read by every thread as a broadcast.  Each thread keeps 4 rows x 8 columns in
-// registers (CUDA-core FP64 FMA: on this part the FP64 tensor rate is no higher, and a
-// 128x64 tensor tile would be mostly padding).  A short long-extent splits K over
-// gridDim.z into ws[z][r][s], folded in a fixed order.
+// A CTA owns SK_TM rows of the long operand L and one K range.  L streams through shared
+// memory in SK_TM x SK_KC tiles (cp.async, SK_STAGES stages, 16-byte copies where two
+// neighbouring elements are contiguous and aligned; coalesced along whichever of r / k is
+// contiguous); the small operand's SK_KC x 8*NT tile sits beside it.  The k offsets of
+// both operands for a stage are staged in shared memory one stage ahead, so no copy
+// waits on a table load.  Each warp computes 32 rows x 8*NT columns on the FP64 tensor
+// cores (mma.m8n8k4: 4 x NT tiles per warp, 32 accumulators per thread), so the issue
+// slots go to the loads and not to one FMA per element pair.  A short long-extent splits
+// K over gridDim.z into ws[z][r][s], folded in a fixed order.
 // ---------------------------------------------------------------------------
 struct SkinnyArgs {
     const double* L = nullptr;
@@ -321,158 +324,213 @@ struct SkinnyArgs {
     double* ws = nullptr;
 };
 
-constexpr int SK_THREADS = 256, SK_STAGES = 3, SK_RPT = 4, SK_TILE = 4096;   // TM * KC doubles per stage
-
-template <int NT>
-struct SkinnyShape {
-    static constexpr int TX = SK_THREADS / NT;     // threads along r
-    static constexpr int TM = SK_RPT * TX;         // rows per CTA
-    static constexpr int KC = SK_TILE / TM;        // k per stage
-    static constexpr int LDA = TM + 1;             // As[k][r], odd pitch
-    static constexpr int LDB = 8 * NT;             // Bs[k][s]
-    static constexpr size_t bytes =
-        (size_t)SK_STAGES * (KC * LDA + KC * LDB) * sizeof(double) + (TM + LDB) * sizeof(int64_t);
-};
+constexpr int SK_THREADS = 256, SK_STAGES = 4, SK_TM = 256, SK_KC = 8;
 
 template <int NT, bool LK>
-// two CTAs per SM (128 registers, 2 x ~111 KB shared): 16 warps hide the cp.async and
-// shared-memory latencies that 8 could not (10.2 -> 14.2 TFLOP/s on the o=32 v=256 ring piece)
+struct SkinnyShape {
+    static constexpr int MT = 4;                          // m-tiles of 8 rows per warp (8 warps x 32 rows)
+    static constexpr int LDA = SK_TM + 8;                 // [k][r] (r contiguous): 8 mod 16 doubles
+    static constexpr int A_ELEMS = LK ? SK_TM * SK_KC : SK_KC * LDA;
+    static constexpr int LDB = 8 * NT + (NT > 1 ? 8 : 0); // [k][s]: 8 mod 16 doubles
+    static constexpr int B_ELEMS = SK_KC * LDB;
+    static constexpr size_t bytes = (size_t)SK_STAGES * (A_ELEMS + B_ELEMS) * sizeof(double) +
+                                    (SK_TM + 8 * NT + 2 * SK_STAGES * SK_KC) * sizeof(int64_t);
+};
+
+// [r][k] tiles (k contiguous, 8 per row): k XOR 4 on every other pair of rows, so that the
+// eight rows x four k of an A fragment fall on 16 different double banks
+__device__ __forceinline__ int lk_index(int r, int k) { return r * SK_KC + (k ^ (((r >> 1) & 1) << 2)); }
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
+}
+
+template <int NT, bool LK>
+// two CTAs per SM (about 80 KB of shared memory each): 16 warps keep four stages of the
+// long operand in flight per CTA
 __global__ void __launch_bounds__(SK_THREADS, 2) skinny_kernel(SkinnyArgs g) {
-    using Sh = SkinnyShape<NT>;
+    using Sh = SkinnyShape<NT, LK>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* As = reinterpret_cast<double*>(smem_raw);
-    double* Bs = As + SK_STAGES * Sh::KC * Sh::LDA;
-    int64_t* sLr = reinterpret_cast<int64_t*>(Bs + SK_STAGES * Sh::KC * Sh::LDB);
-    int64_t* sSn = sLr + Sh::TM;
+    double* Bs = As + SK_STAGES * Sh::A_ELEMS;
+    int64_t* sLr = reinterpret_cast<int64_t*>(Bs + SK_STAGES * Sh::B_ELEMS);
+    int64_t* sSn = sLr + SK_TM;
+    int64_t* sLk = sSn + 8 * NT;                 // [stage][k]: offsets of L, -1 past K
+    int64_t* sSk = sLk + SK_STAGES * SK_KC;      // [stage][k]: offsets of S
 
-    const int tid = threadIdx.x;
-    const int tx = tid % Sh::TX, ty = tid / Sh::TX;
-    const int r0 = blockIdx.x * Sh::TM;
-    for (int i = tid; i < Sh::TM; i += SK_THREADS) sLr[i] = (r0 + i < g.R) ? g.Lr[r0 + i] : 0;
-    for (int i = tid; i < Sh::LDB; i += SK_THREADS) sSn[i] = (i < g.NS) ? g.Sn[i] : 0;
-    __syncthreads();
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int r0 = blockIdx.x * SK_TM;
+    for (int i = tid; i < SK_TM; i += SK_THREADS) sLr[i] = (r0 + i < g.R) ? g.Lr[r0 + i] : -1;
+    for (int i = tid; i < 8 * NT; i += SK_THREADS) sSn[i] = (i < g.NS) ? g.Sn[i] : -1;
 
-    const int kchunks_all = (g.K + Sh::KC - 1) / Sh::KC;
+    const int kchunks_all = (g.K + SK_KC - 1) / SK_KC;
     const int per_split = (kchunks_all + gridDim.z - 1) / gridDim.z;
     const int kc0 = blockIdx.z * per_split;
     const int kchunks = max(0, min(kchunks_all, kc0 + per_split) - kc0);
 
-    auto load_stage = [&](int stage, int kc) {
-        const int k0 = kc * Sh::KC;
-        double* as = As + stage * Sh::KC * Sh::LDA;
-        double* bs = Bs + stage * Sh::KC * Sh::LDB;
-#pragma unroll
-        for (int i = 0; i < SK_TILE / SK_THREADS; i++) {
-            const int e = tid + i * SK_THREADS;
-            int r, k;
-            if (LK) { k = e % Sh::KC; r = e / Sh::KC; }
-            else    { r = e % Sh::TM; k = e / Sh::TM; }
-            const bool ok = (r0 + r < g.R) && (k0 + k < g.K);
-            const double* src =
-                ok ? g.L + sLr[r] + (g.lk_affine ? g.lk0 + g.lk_step * (k0 + k) : __ldg(g.Lk + k0 + k)) : g.L;
-            cp_async8(as + k * Sh::LDA + r, src, ok);
+    // the k offsets of chunk c (relative to this CTA's range) into table slot c % stages
+    auto load_table = [&](int c) {
+        if (tid < 2 * SK_KC && c < kchunks) {
+            const int k = (kc0 + c) * SK_KC + (tid % SK_KC);
+            int64_t v = -1;
+            if (k < g.K) {
+                if (tid < SK_KC) v = g.lk_affine ? g.lk0 + g.lk_step * k : __ldg(g.Lk + k);
+                else v = g.sk_affine ? g.sk0 + g.sk_step * k : __ldg(g.Sk + k);
+            }
+            (tid < SK_KC ? sLk : sSk)[(c % SK_STAGES) * SK_KC + (tid % SK_KC)] = v;
         }
-        for (int e = tid; e < Sh::KC * Sh::LDB; e += SK_THREADS) {
-            const int s = e % Sh::LDB, k = e / Sh::LDB;
-            const bool ok = (s < g.NS) && (k0 + k < g.K);
-            const double* src =
-                ok ? g.S + sSn[s] + (g.sk_affine ? g.sk0 + g.sk_step * (k0 + k) : __ldg(g.Sk + k0 + k)) : g.S;
-            cp_async8(bs + k * Sh::LDB + s, src, ok);
+    };
+    auto load_stage = [&](int c) {
+        const int st = c % SK_STAGES;
+        double* as = As + st * Sh::A_ELEMS;
+        double* bs = Bs + st * Sh::B_ELEMS;
+        const int64_t* lk = sLk + st * SK_KC;
+        const int64_t* sk = sSk + st * SK_KC;
+        // the long operand in pairs of neighbours (rows for [k][r], k for [r][k])
+#pragma unroll
+        for (int i = 0; i < (SK_TM * SK_KC / 2) / SK_THREADS; i++) {
+            const int e = tid + i * SK_THREADS;
+            int r, k, r1, k1;
+            double *d0, *d1;
+            if (LK) {
+                r = e / (SK_KC / 2);
+                k = 2 * (e % (SK_KC / 2));
+                r1 = r;
+                k1 = k + 1;
+                d0 = as + lk_index(r, k);
+                d1 = d0 + 1;
+            } else {
+                k = e / (SK_TM / 2);
+                r = 2 * (e % (SK_TM / 2));
+                r1 = r + 1;
+                k1 = k;
+                d0 = as + k * Sh::LDA + r;
+                d1 = d0 + 1;
+            }
+            const int64_t o0r = sLr[r], o1r = sLr[r1], o0k = lk[k], o1k = lk[k1];
+            const bool ok0 = o0r >= 0 && o0k >= 0, ok1 = o1r >= 0 && o1k >= 0;
+            const int64_t o0 = o0r + o0k, o1 = o1r + o1k;
+            if (ok0 && ok1 && o1 == o0 + 1 && !(o0 & 1) && !((reinterpret_cast<uintptr_t>(g.L)) & 15)) {
+                cp_async16(d0, g.L + o0);
+            } else {
+                cp_async8(d0, ok0 ? g.L + o0 : g.L, ok0);
+                cp_async8(d1, ok1 ? g.L + o1 : g.L, ok1);
+            }
+        }
+        for (int e = tid; e < SK_KC * 8 * NT; e += SK_THREADS) {
+            const int sidx = e % (8 * NT), k = e / (8 * NT);
+            const bool ok = sSn[sidx] >= 0 && sk[k] >= 0;
+            cp_async8(bs + k * Sh::LDB + sidx, ok ? g.S + sSn[sidx] + sk[k] : g.S, ok);
         }
     };
 
-    double acc[SK_RPT][8];
+    double acc[Sh::MT][NT][2];
 #pragma unroll
-    for (int i = 0; i < SK_RPT; i++)
+    for (int i = 0; i < Sh::MT; i++)
 #pragma unroll
-        for (int j = 0; j < 8; j++) acc[i][j] = 0.0;
+        for (int j = 0; j < NT; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
 
+    for (int c = 0; c < SK_STAGES; c++) load_table(c);
+    __syncthreads();
 #pragma unroll
-    for (int st = 0; st < SK_STAGES - 1; st++) {
-        if (st < kchunks) load_stage(st, kc0 + st);
+    for (int c = 0; c < SK_STAGES - 1; c++) {
+        if (c < kchunks) load_stage(c);
         cp_commit();
     }
+    const int wr = warp * 8 * Sh::MT;            // first row of this warp in the tile
+    const int fr = lane >> 2, fk = lane & 3;      // fragment row / k of this lane
     for (int c = 0; c < kchunks; c++) {
         cp_wait<SK_STAGES - 2>();
         __syncthreads();
         {
             const int nc = c + SK_STAGES - 1;
-            if (nc < kchunks) load_stage(nc % SK_STAGES, kc0 + nc);
+            if (nc < kchunks) load_stage(nc);
             cp_commit();
+            load_table(c + SK_STAGES);           // the slot of chunk c, whose copies are issued
         }
-        const double* as = As + (c % SK_STAGES) * Sh::KC * Sh::LDA;
-        const double* bs = Bs + (c % SK_STAGES) * Sh::KC * Sh::LDB + ty * 8;
-#pragma unroll 4
-        for (int k = 0; k < Sh::KC; k++) {
-            double a[SK_RPT], b[8];
+        const double* as = As + (c % SK_STAGES) * Sh::A_ELEMS;
+        const double* bs = Bs + (c % SK_STAGES) * Sh::B_ELEMS;
 #pragma unroll
-            for (int i = 0; i < SK_RPT; i++) a[i] = as[k * Sh::LDA + tx + i * Sh::TX];
+        for (int ks = 0; ks < SK_KC / 4; ks++) {
+            double a[Sh::MT], b[NT];
+            const int k = 4 * ks + fk;
 #pragma unroll
-            for (int j = 0; j < 8; j += 2) {
-                const double2 v = *reinterpret_cast<const double2*>(bs + k * Sh::LDB + j);
-                b[j] = v.x;
-                b[j + 1] = v.y;
+            for (int i = 0; i < Sh::MT; i++) {
+                const int r = wr + 8 * i + fr;
+                a[i] = LK ? as[lk_index(r, k)] : as[k * Sh::LDA + r];
             }
 #pragma unroll
-            for (int i = 0; i < SK_RPT; i++)
+            for (int j = 0; j < NT; j++) b[j] = bs[k * Sh::LDB + 8 * j + fr];
 #pragma unroll
-                for (int j = 0; j < 8; j++) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+            for (int i = 0; i < Sh::MT; i++)
+#pragma unroll
+                for (int j = 0; j < NT; j++) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
         }
     }
     cp_wait<0>();
 
+    // lane holds rows wr + 8i + fr, columns 8j + 2 fk + {0, 1}
     if (gridDim.z > 1) {
         double* wz = g.ws + (int64_t)blockIdx.z * g.R * g.NS;
 #pragma unroll
-        for (int i = 0; i < SK_RPT; i++) {
-            const int r = r0 + tx + i * Sh::TX;
+        for (int i = 0; i < Sh::MT; i++) {
+            const int r = r0 + wr + 8 * i + fr;
             if (r >= g.R) continue;
 #pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const int s = ty * 8 + j;
-                if (s < g.NS) wz[(int64_t)r * g.NS + s] = acc[i][j];
-            }
+            for (int j = 0; j < NT; j++)
+#pragma unroll
+                for (int h = 0; h < 2; h++) {
+                    const int sidx = 8 * j + 2 * fk + h;
+                    if (sidx < g.NS) wz[(int64_t)r * g.NS + sidx] = acc[i][j][h];
+                }
         }
         return;
     }
     if (g.nvr == 1 && g.nvs == 1) {
-        // one destination per element: 8 reads, then 8 writes per row
+        // one destination per element: the reads of a row batch first, then the writes
         const double sc = g.alpha * g.vsign[0];
 #pragma unroll
-        for (int i = 0; i < SK_RPT; i++) {
-            const int r = r0 + tx + i * Sh::TX;
+        for (int i = 0; i < Sh::MT; i++) {
+            const int r = r0 + wr + 8 * i + fr;
             if (r >= g.R) continue;
             const int64_t cr = g.Cr[0][r];
-            int64_t off[8];
-            double old[8];
+            int64_t off[2 * NT];
+            double old[2 * NT];
 #pragma unroll
-            for (int j = 0; j < 8; j++) {
-                const int s = ty * 8 + j;
-                off[j] = s < g.NS ? cr + g.Cs[0][s] : -1;
-            }
+            for (int j = 0; j < NT; j++)
 #pragma unroll
-            for (int j = 0; j < 8; j++) old[j] = off[j] >= 0 ? g.C[off[j]] : 0.0;
+                for (int h = 0; h < 2; h++) {
+                    const int sidx = 8 * j + 2 * fk + h;
+                    off[2 * j + h] = sidx < g.NS ? cr + g.Cs[0][sidx] : -1;
+                }
 #pragma unroll
-            for (int j = 0; j < 8; j++)
-                if (off[j] >= 0) g.C[off[j]] = old[j] + sc * acc[i][j];
+            for (int q = 0; q < 2 * NT; q++) old[q] = off[q] >= 0 ? g.C[off[q]] : 0.0;
+#pragma unroll
+            for (int j = 0; j < NT; j++)
+#pragma unroll
+                for (int h = 0; h < 2; h++)
+                    if (off[2 * j + h] >= 0) g.C[off[2 * j + h]] = old[2 * j + h] + sc * acc[i][j][h];
         }
         return;
     }
 #pragma unroll
-    for (int i = 0; i < SK_RPT; i++) {
-        const int r = r0 + tx + i * Sh::TX;
+    for (int i = 0; i < Sh::MT; i++) {
+        const int r = r0 + wr + 8 * i + fr;
         if (r >= g.R) continue;
         int64_t cr[2];
         cr[0] = g.Cr[0][r];
         cr[1] = g.nvr > 1 ? g.Cr[1][r] : 0;
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-            const int s = ty * 8 + j;
-            if (s >= g.NS) continue;
-            const double v = g.alpha * acc[i][j];
-            for (int a = 0; a < g.nvr; a++)
-                for (int b = 0; b < g.nvs; b++) g.C[cr[a] + g.Cs[b][s]] += g.vsign[a * g.nvs + b] * v;
-        }
+        for (int j = 0; j < NT; j++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) {
+                const int sidx = 8 * j + 2 * fk + h;
+                if (sidx >= g.NS) continue;
+                const double v = g.alpha * acc[i][j][h];
+                for (int a = 0; a < g.nvr; a++)
+                    for (int b = 0; b < g.nvs; b++) g.C[cr[a] + g.Cs[b][sidx]] += g.vsign[a * g.nvs + b] * v;
+            }
     }
 }
 
@@ -495,11 +553,10 @@ int skinny_groups(int M, int N) {
     return small <= 8 ? 1 : (small <= 16 ? 2 : 4);
 }
 
-int skinny_tm(int nt) { return SK_RPT * (SK_THREADS / nt); }
-
 // K-ranges for the skinny kernel: about two waves of CTAs, at least 16 k-chunks each
 int skinny_ksplit(int R, int K, int nt) {
-    const int tm = skinny_tm(nt), kc = SK_TILE / tm;
+    (void)nt;
+    const int tm = SK_TM, kc = SK_KC;
     const int64_t tiles = (R + tm - 1) / tm;
     if (tiles >= 2 * 148) return 1;
     const int64_t kchunks = (K + kc - 1) / kc;
@@ -511,9 +568,9 @@ int skinny_ksplit(int R, int K, int nt) {
 
 template <int NT, bool LK>
 void launch_skinny_t(const SkinnyArgs& a, int ks, cudaStream_t s) {
-    using Sh = SkinnyShape<NT>;
+    using Sh = SkinnyShape<NT, LK>;
     set_smem_once((const void*)skinny_kernel<NT, LK>, (int)Sh::bytes);
-    dim3 grid((a.R + Sh::TM - 1) / Sh::TM, 1, ks);
+    dim3 grid((a.R + SK_TM - 1) / SK_TM, 1, ks);
     skinny_kernel<NT, LK><<<grid, SK_THREADS, Sh::bytes, s>>>(a);
 }
 
@@ -930,19 +987,48 @@ __global__ void __launch_bounds__(256) sum_batched_kernel(const SumDesc* __restr
         }
         return;
     }
+    // a thread's elements: all offsets first, then all loads, then the stores, so that
+    // the loads of a thread are in flight together
+    constexpr int PER = kBatchChunk / 256;
     const int64_t base = (c - cs[sp]) * kBatchChunk;
-    for (int i = threadIdx.x; i < kBatchChunk; i += blockDim.x) {
-        const int64_t l = base + i;
-        if (l >= D.total) break;
-        int64_t r = l, oa = 0, oc = 0;
-        for (int k = 0; k < D.ndim; k++) {
-            const int64_t x = r % D.len[k];
-            r /= D.len[k];
-            oa += x * D.sA[k];
-            oc += x * D.sC[k];
+    int64_t oa[PER], oc[PER];
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+        const int64_t l = base + threadIdx.x + q * 256;
+        oa[q] = -1;
+        oc[q] = 0;
+        if (l >= D.total) continue;
+        int64_t a = 0, cc = 0;
+        if (D.fast) {
+            uint32_t r = (uint32_t)l;
+            for (int k = 0; k < D.ndim; k++) {
+                const uint32_t qq = (uint32_t)(((uint64_t)__umulhi(r, D.dmul[k]) + r) >> D.dshr[k]);
+                const uint32_t x = r - qq * (uint32_t)D.len[k];
+                a += (int64_t)x * D.sA[k];
+                cc += (int64_t)x * D.sC[k];
+                r = qq;
+            }
+        } else {
+            int64_t r = l;
+            for (int k = 0; k < D.ndim; k++) {
+                const int64_t x = r % D.len[k];
+                r /= D.len[k];
+                a += x * D.sA[k];
+                cc += x * D.sC[k];
+            }
         }
-        D.C[oc] += D.alpha * D.A[oa];
+        oa[q] = a;
+        oc[q] = cc;
     }
+    double va[PER], vc[PER];
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+        va[q] = oa[q] >= 0 ? D.A[oa[q]] : 0.0;
+        vc[q] = oa[q] >= 0 ? D.C[oc[q]] : 0.0;
+    }
+#pragma unroll
+    for (int q = 0; q < PER; q++)
+        if (oa[q] >= 0) D.C[oc[q]] = vc[q] + D.alpha * va[q];
 }
 
 __global__ void __launch_bounds__(256) scale_batched_kernel(const ScaleDesc* __restrict__ d,
@@ -1043,6 +1129,21 @@ __global__ void __launch_bounds__(256) dot_batched_kernel(const DotDesc* __restr
 
 void sum_plan_tiles(SumDesc& d) {
     d.tiled = 0;
+    // multiply-shift division by every extent (Granlund-Montgomery, round-up variant): for
+    // 1 <= len < 2^31, shr = ceil(log2 len), mul = floor(2^32 (2^shr - len) / len) + 1 gives
+    // x / len = (umulhi(x, mul) + x) >> shr for every x < 2^32
+    d.fast = d.total < ((int64_t)1 << 31) ? 1 : 0;
+    for (int k = 0; k < d.ndim && d.fast; k++) {
+        const uint64_t len = (uint64_t)d.len[k];
+        if (len < 1 || len >= ((uint64_t)1 << 31)) {
+            d.fast = 0;
+            break;
+        }
+        uint32_t l = 0;
+        while (((uint64_t)1 << l) < len) l++;
+        d.dshr[k] = l;
+        d.dmul[k] = (uint32_t)((((uint64_t)1 << 32) * (((uint64_t)1 << l) - len)) / len + 1);
+    }
     if (d.ndim < 2) return;
     int p0 = 0, pc = 0;
     for (int k = 1; k < d.ndim; k++) {

@@ -24,10 +24,12 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("o,v", [(6, 40), (8, 64), (12, 31)], ids=["o6v40", "o8v64", "o12v31"])
 @pytest.mark.parametrize("case", CASES, ids=[f"{c[0]}+={c[2]}*{c[4]}" for c in CASES])
-def test_skinny_matches_reference_and_tiled(case, monkeypatch):
+def test_skinny_matches_reference_and_tiled(case, o, v, monkeypatch):
+    """o8v64: hundreds of row tiles with 16-byte copies; o12v31: odd extents, so that
+    neighbouring elements are often misaligned and take the 8-byte path."""
     cs, ic, as_, ia, bs, ib = case
-    o, v = 6, 40
     out = {}
     for path in ("auto", "tiled"):
         monkeypatch.setenv("CCSD_FP64_TILED", "1" if path == "tiled" else "0")
