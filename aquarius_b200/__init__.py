@@ -55,6 +55,7 @@ EXPORTS = [
     "ccsd_rhf_solver_hbar", "ccsd_ctx_plan_flops", "ccsd_solver_hbar", "ccsd_lambda_solver_create",
     "ccsd_lambda_plan_query", "ccsd_ctx_plan_export", "ccsd_plan_export_solver",
     "ccsd_diis_create", "ccsd_diis_extrapolate", "ccsd_diis_coefficients", "ccsd_diis_destroy",
+    "ccsd_slice_choice", "ccsd_solver_slice_report",
 ]
 
 
@@ -69,6 +70,7 @@ class Options(ctypes.Structure):
         ("conv_tol", ctypes.c_double), ("max_iter", ctypes.c_int), ("diis_order", ctypes.c_int),
         ("diis_start", ctypes.c_int), ("diis_damping", ctypes.c_double), ("precision", ctypes.c_int),
         ("slices", ctypes.c_int), ("use_graph", ctypes.c_int), ("refine_tol", ctypes.c_double),
+        ("autotune_de", ctypes.c_double),
     ]
 
 
@@ -188,6 +190,8 @@ def lib():
             "ccsd_diis_extrapolate": [vp, ctypes.c_int, vp, vp, vp],
             "ccsd_diis_coefficients": [vp, P(ctypes.c_int), vp],
             "ccsd_diis_destroy": [vp],
+            "ccsd_slice_choice": [ctypes.c_int, vp, dbl, vp],
+            "ccsd_solver_slice_report": [vp, ctypes.c_char_p, i64, P(i64)],
             "ccsd_solver_mp2": [vp, P(dbl)],
             "ccsd_solver_iterate": [vp, P(dbl), P(dbl)],
             "ccsd_solver_iterate_async": [vp],
@@ -839,13 +843,22 @@ class RHFHamiltonianHandle:
 
 
 def _options(conv_tol=1e-9, max_iter=50, diis_order=5, diis_start=1, precision="fp64", slices=0,
-             use_graph=False, refine_tol=0.0):
+             use_graph=False, refine_tol=0.0, autotune_de=0.0):
     o = Options()
     lib().ccsd_options_default(ctypes.byref(o))
     o.conv_tol, o.max_iter, o.diis_order, o.diis_start = conv_tol, max_iter, diis_order, diis_start
     o.precision, o.slices, o.use_graph = PREC[precision], slices, 1 if use_graph else 0
     o.refine_tol = refine_tol
+    o.autotune_de = autotune_de
     return o
+
+
+def slice_choice(dE, budget):
+    """The slice autotuner's rule (ccsd_slice_choice): which statements take one slice fewer."""
+    d = np.ascontiguousarray(np.asarray(dE, dtype=np.float64))
+    out = np.zeros(len(d), np.int32)
+    _check(lib().ccsd_slice_choice(len(d), _ptr(d), float(budget), _ptr(out)))
+    return out.astype(bool)
 
 
 class HbarHandle:
@@ -894,6 +907,19 @@ class Solver:
         e, c = ctypes.c_double(), ctypes.c_double()
         _check(lib().ccsd_solver_iterate(self.s, ctypes.byref(e), ctypes.byref(c)), self.ctx.c)
         return e.value, c.value
+
+    def slice_report(self):
+        """[(slices, measured dE, statement label)] of the split statements (the autotuner's
+        choice once it has run)."""
+        need = ctypes.c_int64()
+        _check(lib().ccsd_solver_slice_report(self.s, None, 0, ctypes.byref(need)), self.ctx.c)
+        buf = ctypes.create_string_buffer(max(need.value, 1))
+        _check(lib().ccsd_solver_slice_report(self.s, buf, need.value, ctypes.byref(need)), self.ctx.c)
+        out = []
+        for line in buf.value.decode().splitlines():
+            ns, de, label = line.split("\t", 2)
+            out.append((int(ns), float(de), label))
+        return out
 
     def iterate_async(self):
         _check(lib().ccsd_solver_iterate_async(self.s), self.ctx.c)

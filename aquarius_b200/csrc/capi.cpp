@@ -2,6 +2,7 @@
 // engine exceptions into status codes; nothing throws across the ABI.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <sstream>
 
@@ -1124,6 +1125,48 @@ int ccsd_solver_hbar(ccsd_solver s, ccsd_hamiltonian* out) {
 int ccsd_solver_flops(ccsd_solver s, double* flops) {
     if (!s) return CCSD_ERR_ARG;
     return guarded(s->ctx, [&] { need(flops) = s->s->flops_per_iter; });
+}
+
+int ccsd_slice_choice(int n, const double* dE, double budget, int* drop) {
+    return guarded(nullptr, [&] {
+        if (n < 0 || (n > 0 && (!dE || !drop))) throw Error(CCSD_ERR_ARG, "ccsd_slice_choice: bad arguments");
+        const std::vector<int> d = slice_choice(std::vector<double>(dE, dE + n), budget);
+        for (int i = 0; i < n; i++) drop[i] = d[i];
+    });
+}
+
+int ccsd_solver_slice_report(ccsd_solver s, char* buf, int64_t len, int64_t* needed) {
+    if (!s) return CCSD_ERR_ARG;
+    return guarded(s->ctx, [&] {
+        Solver& v = *s->s;
+        const int base = v.mode_slices >= 3 ? v.mode_slices : 3;
+        std::string out;
+        std::vector<std::string> seen;
+        auto line = [&](const std::string& label, int slices, double dE) {
+            char head[64];
+            std::snprintf(head, sizeof(head), "%d\t%.6e\t", slices, dE);
+            out += head + label + "\n";
+        };
+        if (!v.tune_report.empty()) {
+            for (auto& e : v.tune_report) line(e.label, std::max(3, base + e.delta), e.dE);
+        } else if (v.ctx.split_precision() || v.mode_precision != CCSD_PREC_FP64) {
+            const int saved_p = v.ctx.precision, saved_s = v.ctx.slices;
+            v.use_mode();
+            for (auto& g : v.iter_plan.gemms)
+                if (v.ctx.routes_split(g) && std::find(seen.begin(), seen.end(), g.label) == seen.end()) {
+                    seen.push_back(g.label);
+                    line(g.label, base, 0.0);
+                }
+            v.ctx.precision = saved_p;
+            v.ctx.slices = saved_s;
+        }
+        need(needed) = (int64_t)out.size() + 1;
+        if (buf && len > 0) {
+            const size_t n = std::min<size_t>(out.size(), (size_t)len - 1);
+            std::memcpy(buf, out.data(), n);
+            buf[n] = 0;
+        }
+    });
 }
 
 int ccsd_solver_mode(ccsd_solver s, int* precision, int* slices) {

@@ -880,6 +880,7 @@ void Context::build_dot_run(Plan& p, RunSchedule& rs, int first, int end) {
         }
         x.alpha = d.alpha;
         if (x.total <= 0) continue;
+        kern::plan_divisors(x.len, x.ndim, x.total, x.fast, x.dmul, x.dshr);
         descs.push_back(x);
         cs.push_back(chunks);
         chunks += (x.total + kern::kBatchChunk - 1) / kern::kBatchChunk;

@@ -125,6 +125,7 @@ struct GemmStep {
     int64_t ak0 = 0, ak_step = 0, bk0 = 0, bk_step = 0;
     double flops() const { return 2.0 * M * N * (double)K; }
     std::string label;                 // statement this block contraction came from
+    int slice_delta = 0;               // split path: slices relative to the context's count (autotuner)
     int64_t split_cache_a = -1;        // keys of cached slices of constant operands
     int64_t split_cache_b = -1;
     bool cache_a = false, cache_b = false;   // operand slices kept across calls (set at reserve)
@@ -266,6 +267,8 @@ public:
     kern::SlicedOperand alloc_sliced(int rows, int K, int nslices, int kind);
     // slices per operand of the split path (3 unless set) and their kind
     int split_slices() const { return slices >= 3 ? slices : 3; }
+    // slices of one split contraction: the context's count plus its autotuned delta
+    int step_slices(const GemmStep& g) const { return std::max(3, split_slices() + g.slice_delta); }
     int slice_kind() const { return precision == CCSD_PREC_SPLIT_I8 ? kern::SLICE_INT8 : kern::SLICE_BF16; }
     bool split_precision() const { return precision == CCSD_PREC_SPLIT || precision == CCSD_PREC_SPLIT_I8; }
     void free_sliced(kern::SlicedOperand& s);

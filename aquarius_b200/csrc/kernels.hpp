@@ -223,7 +223,12 @@ struct DotDesc {
     int64_t len[8], sA[8], sB[8];
     int64_t total = 0;
     double alpha = 0;
+    int fast = 0;                      // multiply-shift index split, as SumDesc
+    uint32_t dmul[8], dshr[8];
 };
+// fill the multiply-shift divisors of a sum / dot descriptor (fast = 0 when an index may
+// reach 2^31)
+void plan_divisors(const int64_t* len, int ndim, int64_t total, int& fast, uint32_t* dmul, uint32_t* dshr);
 void dot_batched(const DotDesc* d, const int64_t* chunk_start, int n, int64_t chunks, double* part, double* out,
                  cudaStream_t s);
 

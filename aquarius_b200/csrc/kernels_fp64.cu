@@ -987,10 +987,12 @@ __global__ void __launch_bounds__(256) sum_batched_kernel(const SumDesc* __restr
         }
         return;
     }
-    // a thread's elements: all offsets first, then all loads, then the stores, so that
-    // the loads of a thread are in flight together
-    constexpr int PER = kBatchChunk / 256;
-    const int64_t base = (c - cs[sp]) * kBatchChunk;
+    // a thread's elements in batches of four: the offsets, then the loads, then the stores,
+    // so that the loads of a batch are in flight together (batches of four keep the
+    // registers, and with them the occupancy of the tiled path of this kernel, low)
+    constexpr int PER = 4;
+    for (int half = 0; half < kBatchChunk / (256 * PER); half++) {
+    const int64_t base = (c - cs[sp]) * kBatchChunk + half * 256 * PER;
     int64_t oa[PER], oc[PER];
 #pragma unroll
     for (int q = 0; q < PER; q++) {
@@ -1029,6 +1031,7 @@ __global__ void __launch_bounds__(256) sum_batched_kernel(const SumDesc* __restr
 #pragma unroll
     for (int q = 0; q < PER; q++)
         if (oa[q] >= 0) D.C[oc[q]] = vc[q] + D.alpha * va[q];
+    }
 }
 
 __global__ void __launch_bounds__(256) scale_batched_kernel(const ScaleDesc* __restrict__ d,
@@ -1109,17 +1112,41 @@ __global__ void __launch_bounds__(256) dot_batched_kernel(const DotDesc* __restr
     const DotDesc& D = d[sp];
     const int64_t base = (c - cs[sp]) * kBatchChunk;
     double acc = 0;
-    for (int i = threadIdx.x; i < kBatchChunk; i += blockDim.x) {
-        const int64_t l = base + i;
-        if (l >= D.total) break;
-        int64_t r = l, oa = 0, ob = 0;
-        for (int k = 0; k < D.ndim; k++) {
-            const int64_t x = r % D.len[k];
-            r /= D.len[k];
-            oa += x * D.sA[k];
-            ob += x * D.sB[k];
+    // batches of four elements: the offsets first, then the loads (in flight together)
+    constexpr int PER = 4;
+    for (int half = 0; half < kBatchChunk / (256 * PER); half++) {
+    int64_t oa[PER], ob[PER];
+#pragma unroll
+    for (int q = 0; q < PER; q++) {
+        const int64_t l = base + half * 256 * PER + threadIdx.x + q * 256;
+        oa[q] = -1;
+        ob[q] = 0;
+        if (l >= D.total) continue;
+        int64_t a = 0, b = 0;
+        if (D.fast) {
+            uint32_t r = (uint32_t)l;
+            for (int k = 0; k < D.ndim; k++) {
+                const uint32_t qq = (uint32_t)(((uint64_t)__umulhi(r, D.dmul[k]) + r) >> D.dshr[k]);
+                const uint32_t x = r - qq * (uint32_t)D.len[k];
+                a += (int64_t)x * D.sA[k];
+                b += (int64_t)x * D.sB[k];
+                r = qq;
+            }
+        } else {
+            int64_t r = l;
+            for (int k = 0; k < D.ndim; k++) {
+                const int64_t x = r % D.len[k];
+                r /= D.len[k];
+                a += x * D.sA[k];
+                b += x * D.sB[k];
+            }
         }
-        acc += D.A[oa] * D.B[ob];
+        oa[q] = a;
+        ob[q] = b;
+    }
+#pragma unroll
+    for (int q = 0; q < PER; q++)
+        if (oa[q] >= 0) acc += D.A[oa[q]] * D.B[ob[q]];
     }
     acc = block_sum(acc);
     if (threadIdx.x == 0) part[c] = D.alpha * acc;
@@ -1127,23 +1154,27 @@ __global__ void __launch_bounds__(256) dot_batched_kernel(const DotDesc* __restr
 
 }  // namespace
 
-void sum_plan_tiles(SumDesc& d) {
-    d.tiled = 0;
-    // multiply-shift division by every extent (Granlund-Montgomery, round-up variant): for
-    // 1 <= len < 2^31, shr = ceil(log2 len), mul = floor(2^32 (2^shr - len) / len) + 1 gives
-    // x / len = (umulhi(x, mul) + x) >> shr for every x < 2^32
-    d.fast = d.total < ((int64_t)1 << 31) ? 1 : 0;
-    for (int k = 0; k < d.ndim && d.fast; k++) {
-        const uint64_t len = (uint64_t)d.len[k];
+// multiply-shift division by every extent (Granlund-Montgomery, round-up variant): for
+// 1 <= len < 2^31, shr = ceil(log2 len), mul = floor(2^32 (2^shr - len) / len) + 1 gives
+// x / len = (umulhi(x, mul) + x) >> shr for every x < 2^32
+void plan_divisors(const int64_t* lens, int ndim, int64_t total, int& fast, uint32_t* dmul, uint32_t* dshr) {
+    fast = total < ((int64_t)1 << 31) ? 1 : 0;
+    for (int k = 0; k < ndim && fast; k++) {
+        const uint64_t len = (uint64_t)lens[k];
         if (len < 1 || len >= ((uint64_t)1 << 31)) {
-            d.fast = 0;
+            fast = 0;
             break;
         }
         uint32_t l = 0;
         while (((uint64_t)1 << l) < len) l++;
-        d.dshr[k] = l;
-        d.dmul[k] = (uint32_t)((((uint64_t)1 << 32) * (((uint64_t)1 << l) - len)) / len + 1);
+        dshr[k] = l;
+        dmul[k] = (uint32_t)((((uint64_t)1 << 32) * (((uint64_t)1 << l) - len)) / len + 1);
     }
+}
+
+void sum_plan_tiles(SumDesc& d) {
+    d.tiled = 0;
+    plan_divisors(d.len, d.ndim, d.total, d.fast, d.dmul, d.dshr);
     if (d.ndim < 2) return;
     int p0 = 0, pc = 0;
     for (int k = 1; k < d.ndim; k++) {

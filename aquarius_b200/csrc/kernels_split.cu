@@ -14,12 +14,15 @@
 //   FP32 rounding of the rest sits ~2^-32 below the result (3 slices; 4 slices also keep
 //   s1*s2 + s2*s1 apart, exact over 512 k).
 //
-// INT8 slices (3, 4 or 5):  x = 2^(e-5) * (q1 + 2^-7 q2 + 2^-14 q3 ...),  q_t in [-64,64].
-//   The tcgen05 GEMM (kind::i8, twice the BF16 rate) accumulates every level
-//   t = i+j of the kept products q_i*q_j (i+j < NS) in its own INT32 accumulator, which
-//   is exact (|q_i q_j| <= 2^12, at most 5 products per level: a drained chunk of 65536 k
-//   stays below 2^31); the epilogue weights level t by 2^-7t in FP64.  Per product the
-//   error is ~2^-(7 NS - 1) of row max x column max (2^-20, 2^-27, 2^-34).
+// INT8 slices (3, 4 or 5):  x = (max/127) * (q1 + q2/254 + q3/254^2 ...),  q_t in [-127,127],
+//   the whole signed 8-bit range: y = x * 127/max lies in [-127,127]; q1 = rint(y) and each
+//   further slice is rint of the remainder (in [-1/2,1/2]) times 254, so every slice
+//   carries log2(254) = 7.99 bits.  The tcgen05 GEMM (kind::i8, twice the BF16 rate)
+//   accumulates every level t = i+j of the kept products q_i*q_j (i+j < NS) in its own
+//   INT32 accumulator, which is exact (|q_i q_j| <= 127^2 < 2^14, at most 5 products per
+//   level: a drained chunk of 16384 k stays below 2^31); the epilogue weights level t by
+//   254^-t in FP64.  Per product the error is ~254^-NS / 2 of row max x column max
+//   (3.7e-8, 1.5e-10, 5.7e-13 for 3, 4, 5 slices).
 //
 // Kernel structure (one 128 x TBN output tile per CTA, 320 threads):
 //   warp 0      TMA producer: NS A-slice + NS B-slice tiles of 128-byte k-blocks per
@@ -32,6 +35,7 @@
 //               into the destination through the planner's offset tables at the end.
 // Every mbarrier wait is bounded (about 2 s); on expiry the kernel records an error
 // code, stops issuing work and returns after releasing its TMEM.
+#include <algorithm>
 #include <atomic>
 #include <cstdint>
 #include <cstdio>
@@ -79,8 +83,8 @@ struct Shape {
     // also keep s1*s2 + s2*s1 apart (exact over 512 k).  INT8: one exact INT32
     // accumulator per level i+j.
     static constexpr int NACC = I8 ? NS : (NS == 4 ? 3 : 2);
-    // k-blocks per drained chunk: 1024 / 512 k (BF16), 65536 k (INT8: |level| < 2^31)
-    static constexpr int CHUNK = I8 ? 65536 / BKE : (NS == 4 ? 8 : 16);
+    // k-blocks per drained chunk: 1024 / 512 k (BF16), 16384 k (INT8: |level| < 2^31)
+    static constexpr int CHUNK = I8 ? 16384 / BKE : (NS == 4 ? 8 : 16);
     // split-K ranges: whole exact chunks (BF16), any 1024 k (INT8: exact per range)
     static constexpr int KSPLIT_GRAIN = I8 ? 1024 / BKE : CHUNK;
     static constexpr int BUF = NACC * TBN;                          // TMEM columns per buffer
@@ -353,14 +357,14 @@ __global__ void __launch_bounds__(THREADS, 1)
 #pragma unroll
             for (int j4 = 0; j4 < COLS / 16; j4++) {
                 if constexpr (I8) {
-                    // one level at a time (fewer live registers): level j weighs 2^-7j, each
-                    // term exact in FP64
+                    // one level at a time (fewer live registers): level j weighs 254^-j
 #pragma unroll
                     for (int j = 0; j < Sh::NACC; j++) {
                         uint32_t r[16];
                         tmem_ld16(base + j * TBN + j4 * 16, r);
                         tmem_wait_ld();
-                        const double w = 1.0 / (double)(1ll << (7 * j));
+                        const double w = j == 0 ? 1.0 : j == 1 ? 1.0 / 254.0 : j == 2 ? 1.0 / 64516.0
+                                       : j == 3 ? 1.0 / 16387064.0 : 1.0 / 4162314256.0;
 #pragma unroll
                         for (int t = 0; t < 16; t++) acc[j4 * 16 + t] += (double)(int)r[t] * w;
                     }
@@ -451,48 +455,93 @@ __global__ void __launch_bounds__(THREADS, 1)
 }
 
 // ---------------------------------------------------------------------------
-// slicing: two passes over 32-row x 64-k tiles of the gathered operand
+// slicing: two passes over 32-row x 64-k tiles of the gathered operand.  A CTA walks
+// tiles t = blockIdx.x, + gridDim.x, ... (t = row tile + tiles_r * k tile); the offset
+// tables of the next tile load while the current tile's elements are in flight.
 // ---------------------------------------------------------------------------
-constexpr int SR = 32, SK = 64, STHREADS = 256;
+constexpr int SR = 32, SK = 64, STHREADS = 256, SPER = (SR * SK) / STHREADS;
+constexpr int SLICE_CTAS = 148 * 6;   // resident at 6 CTAs per SM (40 registers, 18 KB)
 
+// offset tables of tile t into buffer b (-1 past the operand)
+__device__ __forceinline__ void slice_tables(const int64_t* __restrict__ R, const int64_t* __restrict__ Kt, int nrows,
+                                             int K, int tiles_r, int64_t t, int64_t (*sR)[SR], int64_t (*sK)[SK],
+                                             int b) {
+    const int r0 = (int)(t % tiles_r) * SR;
+    const int64_t k0 = (t / tiles_r) * SK;
+    for (int i = threadIdx.x; i < SR; i += STHREADS) sR[b][i] = (r0 + i < nrows) ? R[r0 + i] : -1;
+    for (int i = threadIdx.x; i < SK; i += STHREADS) sK[b][i] = (k0 + i < K) ? Kt[k0 + i] : -1;
+}
+
+// element i of this thread in a tile: KC (k contiguous) walks k fastest, else r
 template <bool KC>
-__device__ __forceinline__ void load_tile(const double* __restrict__ X, const int64_t* __restrict__ R,
-                                          const int64_t* __restrict__ Kt, int nrows, int K, int r0, int k0,
-                                          double (*tile)[SK + 1], int64_t* sR, int64_t* sK) {
-    for (int i = threadIdx.x; i < SR; i += STHREADS) sR[i] = (r0 + i < nrows) ? R[r0 + i] : -1;
-    for (int i = threadIdx.x; i < SK; i += STHREADS) sK[i] = (k0 + i < K) ? Kt[k0 + i] : -1;
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < (SR * SK) / STHREADS; i++) {
-        const int e = threadIdx.x + i * STHREADS;
-        int r, k;
-        if (KC) {
-            k = e % SK;
-            r = e / SK;
-        } else {
-            r = e % SR;
-            k = e / SR;
-        }
-        double v = 0.0;
-        if (sR[r] >= 0 && sK[k] >= 0) v = X[sR[r] + sK[k]];
-        tile[r][k] = v;
+__device__ __forceinline__ void slice_rk(int i, int& r, int& k) {
+    const int e = threadIdx.x + i * STHREADS;
+    if (KC) {
+        k = e % SK;
+        r = e / SK;
+    } else {
+        r = e % SR;
+        k = e / SR;
     }
+}
+
+// Tiles are handed out in order: the first to CTA blockIdx.x, then the next free tile
+// from a counter (ctr, zeroed with the row maxima) to whichever CTA asks, so that the tiles
+// in flight stay a compact range of the operand, as with one CTA per tile.
+__device__ __forceinline__ int64_t next_tile(unsigned long long* ctr, int64_t* s_next) {
+    if (threadIdx.x == 0) *s_next = (int64_t)gridDim.x + (int64_t)atomicAdd(ctr, 1ull);
     __syncthreads();
+    return *s_next;
 }
 
 template <bool KC>
-__global__ void __launch_bounds__(STHREADS) rowmax_kernel(const double* __restrict__ X, const int64_t* __restrict__ R,
-                                                          const int64_t* __restrict__ Kt, int nrows, int K,
-                                                          unsigned long long* rowmax) {
-    __shared__ double tile[SR][SK + 1];
-    __shared__ int64_t sR[SR], sK[SK];
-    const int r0 = blockIdx.x * SR, k0 = blockIdx.y * SK;   // rows on x: up to 2^31 tiles
-    load_tile<KC>(X, R, Kt, nrows, K, r0, k0, tile, sR, sK);
+__global__ void __launch_bounds__(STHREADS, 6) rowmax_kernel(const double* __restrict__ X, const int64_t* __restrict__ R,
+                                                          const int64_t* __restrict__ Kt, int nrows, int K, int tiles_r,
+                                                          int64_t ntiles, unsigned long long* rowmax,
+                                                          unsigned long long* ctr) {
+    __shared__ int64_t sR[2][SR], sK[2][SK];
+    __shared__ double red[STHREADS / 32][SR];
+    __shared__ int64_t s_next;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int r = warp; r < SR; r += STHREADS / 32) {
-        double m = fmax(fabs(tile[r][lane]), fabs(tile[r][lane + 32]));
-        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-        if (lane == 0 && r0 + r < nrows && m > 0.0) atomicMax(&rowmax[r0 + r], (unsigned long long)__double_as_longlong(m));
+    int b = 0;
+    if ((int64_t)blockIdx.x < ntiles) slice_tables(R, Kt, nrows, K, tiles_r, blockIdx.x, sR, sK, 0);
+    __syncthreads();
+    for (int64_t t = blockIdx.x, tn; t < ntiles; t = tn, b ^= 1) {
+        double v[SPER];
+#pragma unroll
+        for (int i = 0; i < SPER; i++) {
+            int r, k;
+            slice_rk<KC>(i, r, k);
+            const int64_t orr = sR[b][r], ok = sK[b][k];
+            v[i] = (orr >= 0 && ok >= 0) ? fabs(X[orr + ok]) : 0.0;
+        }
+        tn = next_tile(ctr, &s_next);
+        if (tn < ntiles) slice_tables(R, Kt, nrows, K, tiles_r, tn, sR, sK, b ^ 1);
+        const int r0 = (int)(t % tiles_r) * SR;
+        if (KC) {
+            // element i of a warp: one row (warp / 2 + 4 i), 32 consecutive k
+#pragma unroll
+            for (int i = 0; i < SPER; i++) {
+                double m = v[i];
+                for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+                const int row = r0 + (warp >> 1) + 4 * i;
+                if (lane == 0 && row < nrows && m > 0.0)
+                    atomicMax(&rowmax[row], (unsigned long long)__double_as_longlong(m));
+            }
+        } else {
+            // every element of a thread sits in row `lane`: fold them, then across the warps
+            double m = 0.0;
+#pragma unroll
+            for (int i = 0; i < SPER; i++) m = fmax(m, v[i]);
+            red[warp][lane] = m;
+            __syncthreads();
+            if (warp == 0) {
+                for (int w = 1; w < STHREADS / 32; w++) m = fmax(m, red[w][lane]);
+                const int row = r0 + lane;
+                if (row < nrows && m > 0.0) atomicMax(&rowmax[row], (unsigned long long)__double_as_longlong(m));
+            }
+        }
+        __syncthreads();   // next tables visible, red free again
     }
 }
 
@@ -502,54 +551,92 @@ __device__ __forceinline__ unsigned short bf16_bits(double v) {
 }
 
 template <bool KC, int NS, bool I8>
-__global__ void __launch_bounds__(STHREADS)
+__global__ void __launch_bounds__(STHREADS, 6)
     slice_kernel(const double* __restrict__ X, const int64_t* __restrict__ R, const int64_t* __restrict__ Kt, int nrows,
-                 int K, const unsigned long long* __restrict__ rowmax, int rows_p, int kpad,
-                 uint8_t* __restrict__ out_bytes, double* __restrict__ scale) {
+                 int K, int tiles_r, int64_t ntiles, const unsigned long long* __restrict__ rowmax, int rows_p, int kpad,
+                 uint8_t* __restrict__ out_bytes, double* __restrict__ scale, unsigned long long* ctr) {
     __shared__ double tile[SR][SK + 1];
-    __shared__ int64_t sR[SR], sK[SK];
-    const int r0 = blockIdx.x * SR, k0 = blockIdx.y * SK;   // rows on x: up to 2^31 tiles
-    load_tile<KC>(X, R, Kt, nrows, K, r0, k0, tile, sR, sK);
+    __shared__ int64_t sR[2][SR], sK[2][SK];
+    __shared__ double sMul[SR];      // per row: 127 / max (INT8) or 2^(6 - e) (BF16); 0 for a zero row
+    __shared__ int64_t s_next;
     const size_t plane = (size_t)rows_p * kpad;
-    // BF16: x = 2^(ex-6) (s1 + s2 + ...), s1 in [-128,128], slice t carries weight 2^-8t
-    // INT8: x = 2^(ex-5) (q1 + 2^-7 q2 + ...), q_t in [-64,64]
-    constexpr int SHIFT = I8 ? 5 : 6;
+    int b = 0;
+    if ((int64_t)blockIdx.x < ntiles) slice_tables(R, Kt, nrows, K, tiles_r, blockIdx.x, sR, sK, 0);
+    __syncthreads();
+    for (int64_t t = blockIdx.x, tn; t < ntiles; t = tn, b ^= 1) {
+        const int r0 = (int)(t % tiles_r) * SR;
+        const int64_t k0 = (t / tiles_r) * SK;
+        double v[SPER];
 #pragma unroll
-    for (int i = 0; i < (SR * SK) / STHREADS; i++) {
-        const int e = threadIdx.x + i * STHREADS;
-        const int k = e % SK, r = e / SK;
-        const int row = r0 + r;
-        double mx = row < nrows ? __longlong_as_double((long long)rowmax[row]) : 0.0;
-        uint16_t bits[NS];
-#pragma unroll
-        for (int t = 0; t < NS; t++) bits[t] = 0;
-        if (mx > 0.0) {
-            const int ex = ilogb(mx);                    // mx in [2^ex, 2^(ex+1))
-            double y = ldexp(tile[r][k], SHIFT - ex);    // |y| < 2^SHIFT+1
-            double w = 1.0;                              // BF16 weight of slice t: 2^(-8t)
-#pragma unroll
-            for (int t = 0; t < NS; t++) {
-                const double st = rint(y);               // an integer of at most 8 (7) significant bits
+        for (int i = 0; i < SPER; i++) {
+            int r, k;
+            slice_rk<KC>(i, r, k);
+            const int64_t orr = sR[b][r], ok = sK[b][k];
+            v[i] = (orr >= 0 && ok >= 0) ? X[orr + ok] : 0.0;
+        }
+        if (threadIdx.x < SR) {
+            const int row = r0 + threadIdx.x;
+            const double mx = row < nrows ? __longlong_as_double((long long)rowmax[row]) : 0.0;
+            double mul = 0.0, sc = 0.0;
+            if (mx > 1e-290) {   // below that a row counts as zero (127 / max would overflow)
                 if constexpr (I8) {
-                    bits[t] = (uint16_t)(uint8_t)(int8_t)(int)st;
-                    y = (y - st) * 128.0;
+                    mul = 127.0 / mx;
+                    sc = mx / 127.0;
                 } else {
-                    bits[t] = bf16_bits(st * w);
-                    y = (y - st) * 256.0;
-                    w *= 0.00390625;
+                    mul = ldexp(1.0, 6 - ilogb(mx));          // mx in [2^e, 2^(e+1))
+                    sc = ldexp(1.0, ilogb(mx) - 6);
                 }
             }
+            sMul[threadIdx.x] = mul;
+            if (k0 == 0 && row < rows_p) scale[row] = sc;
         }
-        const size_t o = (size_t)row * kpad + (k0 + k);
-        if constexpr (I8) {
+        tn = next_tile(ctr, &s_next);
+        if (tn < ntiles) slice_tables(R, Kt, nrows, K, tiles_r, tn, sR, sK, b ^ 1);
 #pragma unroll
-            for (int t = 0; t < NS; t++) out_bytes[t * plane + o] = (uint8_t)bits[t];
-        } else {
-            uint16_t* out = reinterpret_cast<uint16_t*>(out_bytes);
-#pragma unroll
-            for (int t = 0; t < NS; t++) out[t * plane + o] = bits[t];
+        for (int i = 0; i < SPER; i++) {
+            int r, k;
+            slice_rk<KC>(i, r, k);
+            tile[r][k] = v[i];
         }
-        if (blockIdx.y == 0 && k == 0) scale[row] = mx > 0.0 ? ldexp(1.0, ilogb(mx) - SHIFT) : 0.0;
+        __syncthreads();
+        // BF16: x = 2^(e-6) (s1 + s2 + ...), s1 in [-128,128], slice t carries weight 2^-8t
+        // INT8: x = (max/127) (q1 + q2/254 + ...), q_t in [-127,127]
+#pragma unroll
+        for (int i = 0; i < SPER; i++) {
+            const int e = threadIdx.x + i * STHREADS;
+            const int k = e % SK, r = e / SK;
+            const int row = r0 + r;
+            const double mul = sMul[r];
+            uint16_t bits[NS];
+#pragma unroll
+            for (int q = 0; q < NS; q++) bits[q] = 0;
+            if (mul > 0.0) {
+                double y = tile[r][k] * mul;                 // |y| <= 127 (INT8), < 2^7 + 1 (BF16)
+                double w = 1.0;                              // BF16 weight of slice q: 2^(-8q)
+#pragma unroll
+                for (int q = 0; q < NS; q++) {
+                    const double st = rint(y);               // an integer of at most 8 significant bits
+                    if constexpr (I8) {
+                        bits[q] = (uint16_t)(uint8_t)(int8_t)(int)st;
+                        y = (y - st) * 254.0;                // remainder in [-1/2, 1/2] -> [-127, 127]
+                    } else {
+                        bits[q] = bf16_bits(st * w);
+                        y = (y - st) * 256.0;
+                        w *= 0.00390625;
+                    }
+                }
+            }
+            const size_t o = (size_t)row * kpad + (size_t)(k0 + k);
+            if constexpr (I8) {
+#pragma unroll
+                for (int q = 0; q < NS; q++) out_bytes[q * plane + o] = (uint8_t)bits[q];
+            } else {
+                uint16_t* out = reinterpret_cast<uint16_t*>(out_bytes);
+#pragma unroll
+                for (int q = 0; q < NS; q++) out[q * plane + o] = bits[q];
+            }
+        }
+        __syncthreads();   // the tile, sMul and the next tables
     }
 }
 
@@ -624,15 +711,17 @@ int split_k_pad(int k, int kind) {
 
 namespace {
 template <int NS, bool I8>
-void launch_slice(dim3 grid, bool kcontig, const double* X, const int64_t* R, const int64_t* Kt, int nrows, int K,
-                  const unsigned long long* rowmax, SlicedOperand& out, cudaStream_t s) {
+void launch_slice(int grid, int tiles_r, int64_t ntiles, bool kcontig, const double* X, const int64_t* R,
+                  const int64_t* Kt, int nrows, int K, const unsigned long long* rowmax, SlicedOperand& out,
+                  cudaStream_t s) {
     using namespace split;
+    unsigned long long* ctr = const_cast<unsigned long long*>(rowmax) + out.rows + 1;
     if (kcontig)
-        slice_kernel<true, NS, I8><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax, out.rows, out.kpad, out.data,
-                                                             out.scale);
+        slice_kernel<true, NS, I8><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, tiles_r, ntiles, rowmax, out.rows,
+                                                             out.kpad, out.data, out.scale, ctr);
     else
-        slice_kernel<false, NS, I8><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax, out.rows, out.kpad, out.data,
-                                                              out.scale);
+        slice_kernel<false, NS, I8><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, tiles_r, ntiles, rowmax, out.rows,
+                                                              out.kpad, out.data, out.scale, ctr);
 }
 }  // namespace
 
@@ -644,18 +733,20 @@ void slice_rows(const double* X, const int64_t* R, const int64_t* Kt, int nrows,
     if ((int64_t)ns * out.rows * out.kpad * slice_elem_bytes(out.kind) > out.bytes)
         throw std::runtime_error("sliced operand smaller than its scheme needs");
     unsigned long long* rowmax = reinterpret_cast<unsigned long long*>(out.rowmax);
-    cudaMemsetAsync(rowmax, 0, sizeof(double) * out.rows, s);
-    if (out.kpad / SK > 65535) throw std::runtime_error("split operand K too long for the slicing grid");
-    dim3 grid(out.rows / SR, out.kpad / SK);
-    if (kcontig) rowmax_kernel<true><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax);
-    else rowmax_kernel<false><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, rowmax);
+    // the row maxima and, after them, the tile counters of the two passes
+    cudaMemsetAsync(rowmax, 0, sizeof(double) * (out.rows + 2), s);
+    const int tiles_r = out.rows / SR;
+    const int64_t ntiles = (int64_t)tiles_r * (out.kpad / SK);
+    const int grid = (int)std::min<int64_t>(ntiles, SLICE_CTAS);
+    if (kcontig) rowmax_kernel<true><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, tiles_r, ntiles, rowmax, rowmax + out.rows);
+    else rowmax_kernel<false><<<grid, STHREADS, 0, s>>>(X, R, Kt, nrows, K, tiles_r, ntiles, rowmax, rowmax + out.rows);
     if (out.kind == SLICE_INT8) {
-        if (ns == 3) launch_slice<3, true>(grid, kcontig, X, R, Kt, nrows, K, rowmax, out, s);
-        else if (ns == 4) launch_slice<4, true>(grid, kcontig, X, R, Kt, nrows, K, rowmax, out, s);
-        else launch_slice<5, true>(grid, kcontig, X, R, Kt, nrows, K, rowmax, out, s);
+        if (ns == 3) launch_slice<3, true>(grid, tiles_r, ntiles, kcontig, X, R, Kt, nrows, K, rowmax, out, s);
+        else if (ns == 4) launch_slice<4, true>(grid, tiles_r, ntiles, kcontig, X, R, Kt, nrows, K, rowmax, out, s);
+        else launch_slice<5, true>(grid, tiles_r, ntiles, kcontig, X, R, Kt, nrows, K, rowmax, out, s);
     } else {
-        if (ns == 3) launch_slice<3, false>(grid, kcontig, X, R, Kt, nrows, K, rowmax, out, s);
-        else launch_slice<4, false>(grid, kcontig, X, R, Kt, nrows, K, rowmax, out, s);
+        if (ns == 3) launch_slice<3, false>(grid, tiles_r, ntiles, kcontig, X, R, Kt, nrows, K, rowmax, out, s);
+        else launch_slice<4, false>(grid, tiles_r, ntiles, kcontig, X, R, Kt, nrows, K, rowmax, out, s);
     }
     g_launches += 2;
 }

@@ -3,6 +3,7 @@
 // the device so that one iteration is a fixed sequence of kernel launches (and can be
 // captured as a CUDA graph).
 #include <algorithm>
+#include <map>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -33,6 +34,25 @@ void options_default(ccsd_options* o) {
     o->slices = 0;
     o->use_graph = 0;
     o->refine_tol = 0.0;
+    o->autotune_de = 0.0;
+}
+
+// The slice autotuner's rule: smallest |dE| first while the running sum stays within the
+// budget (a stable order keeps ties in statement order).
+std::vector<int> slice_choice(const std::vector<double>& dE, double budget) {
+    std::vector<int> order(dE.size()), drop(dE.size(), 0);
+    for (size_t i = 0; i < order.size(); i++) order[i] = (int)i;
+    // a change that is not finite never takes a slice away (sorted last)
+    auto key = [&](int i) { return std::isfinite(dE[i]) ? std::fabs(dE[i]) : std::numeric_limits<double>::infinity(); };
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return key(a) < key(b); });
+    double used = 0.0;
+    for (int i : order) {
+        const double d = std::fabs(dE[i]);
+        if (!std::isfinite(d) || used + d > budget) break;
+        used += d;
+        drop[i] = 1;
+    }
+    return drop;
 }
 
 Solver::Solver(Context& c, const ccsd_hamiltonian& h, const ccsd_options& o) : ctx(c), H(h), opts(o) {
@@ -960,6 +980,61 @@ void Solver::diis_step() {
     kern::lincomb(t1.data, t1.total, t2.data, t2.total, d_xs, d_c, n, s);
 }
 
+// Slice count per contraction (the autotuner).  From the current amplitudes, one trial
+// evaluates the iteration's contractions, the Jacobi update and the energy (DIIS left out)
+// with every contraction at the solver's slice count; then one trial per statement with
+// split contractions, that statement one slice fewer.  The difference of each trial's
+// energy from the first is that statement's measured energy change; slice_choice picks
+// the statements that keep one slice fewer.  The amplitudes are restored after every
+// trial, so the solve continues from where it was.
+void Solver::autotune_slices() {
+    tuned = true;
+    cudaStream_t s = ctx.stream;
+    Tensor& t1 = ctx.tensor(T1);
+    Tensor& t2 = ctx.tensor(T2);
+    const int64_t n1 = t1.total, n2 = t2.total;
+    double* save = (double*)ctx.dmalloc((n1 + n2) * sizeof(double));
+    CCSD_CUDA(cudaMemcpyAsync(save, t1.data, n1 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CCSD_CUDA(cudaMemcpyAsync(save + n1, t2.data, n2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    std::vector<std::string> labels;
+    std::map<std::string, std::vector<GemmStep*>> steps;
+    for (auto& g : iter_plan.gemms) {
+        if (!ctx.routes_split(g)) continue;
+        if (!steps.count(g.label)) labels.push_back(g.label);
+        steps[g.label].push_back(&g);
+    }
+    auto trial = [&]() {
+        CCSD_CUDA(cudaMemsetAsync(d_red, 0, 2 * sizeof(double), s));
+        launch_tau();
+        ctx.run(iter_plan);
+        kern::update_batched(d_upd, d_upd_cs, n_upd, upd_chunks, d_red + 1, s);
+        launch_tau();
+        ctx.run(energy_plan, nullptr, d_red + 0);
+        CCSD_CUDA(cudaMemcpyAsync(h_red, d_red, sizeof(double), cudaMemcpyDeviceToHost, s));
+        CCSD_CUDA(cudaMemcpyAsync(t1.data, save, n1 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        CCSD_CUDA(cudaMemcpyAsync(t2.data, save + n1, n2 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        CCSD_CUDA(cudaStreamSynchronize(s));
+        return h_red[0];
+    };
+    const double e0 = trial();
+    std::vector<double> dE;
+    for (auto& l : labels) {
+        for (GemmStep* g : steps[l]) g->slice_delta = -1;
+        const double e = trial();
+        for (GemmStep* g : steps[l]) g->slice_delta = 0;
+        dE.push_back(e - e0);
+    }
+    const std::vector<int> drop = slice_choice(dE, opts.autotune_de);
+    tune_report.clear();
+    for (size_t i = 0; i < labels.size(); i++) {
+        if (drop[i])
+            for (GemmStep* g : steps[labels[i]]) g->slice_delta = -1;
+        tune_report.push_back({labels[i], dE[i], drop[i] ? -1 : 0});
+    }
+    ctx.dfree(save, (n1 + n2) * sizeof(double));
+    if (kern::split_error(true)) throw Error(CCSD_ERR_TIMEOUT, "split GEMM wait expired while tuning");
+}
+
 void Solver::iterate_async() {
     // Refinement of the split precision.  Three slices leave a residual floor (near 1e-9
     // for BF16, ~8x higher for INT8); once conv < refine_tol the contractions move to four
@@ -1006,6 +1081,11 @@ void Solver::iterate_async() {
             captured_once = false;
         }
     }
+    // the autotuner runs once, on the first iteration at 4 or more slices after the first
+    // (the amplitudes have left the MP2 guess), before any graph is captured
+    if (opts.autotune_de > 0 && !tuned && iterations >= 1 && ctx.split_precision() && ctx.split_slices() >= 4 &&
+        !ctx.host_only)
+        autotune_slices();
     if (opts.use_graph) {
         if (!graph_exec) {
             // the first iteration runs eagerly (it also warms every kernel), the graph is

@@ -8,6 +8,8 @@
 namespace ccsd {
 
 void options_default(ccsd_options* o);
+// the slice autotuner's rule: 1 for the statements that take one slice fewer
+std::vector<int> slice_choice(const std::vector<double>& dE, double budget);
 
 struct DiisSegment {
     int64_t off, len;
@@ -60,6 +62,16 @@ public:
     // shared by every solver on it, so each entry point that launches contractions first
     // puts the solver's own mode in place (use_mode) and a refinement switch updates it
     int mode_precision = CCSD_PREC_FP64, mode_slices = 0;
+    // slice autotuner (opts.autotune_de): per statement label, measured energy change and
+    // the slice delta chosen
+    struct TuneEntry {
+        std::string label;
+        double dE;
+        int delta;
+    };
+    bool tuned = false;
+    std::vector<TuneEntry> tune_report;
+    void autotune_slices();
     void use_mode() {
         ctx.precision = mode_precision;
         ctx.slices = mode_slices;

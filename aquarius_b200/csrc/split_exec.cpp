@@ -61,14 +61,14 @@ kern::SlicedOperand Context::alloc_sliced(int rows, int K, int ns, int kind) {
     s.bytes = kern::split_slice_bytes(rows, K, ns, kind);
     s.data = (uint8_t*)dmalloc(s.bytes);
     s.scale = (double*)dmalloc(s.rows * sizeof(double));
-    s.rowmax = (double*)dmalloc(s.rows * sizeof(double));
+    s.rowmax = (double*)dmalloc((s.rows + 2) * sizeof(double));   // + the slicing kernels' tile counters
     return s;
 }
 
 void Context::free_sliced(kern::SlicedOperand& s) {
     dfree(s.data, s.bytes);
     dfree(s.scale, s.rows * sizeof(double));
-    dfree(s.rowmax, s.rows * sizeof(double));
+    dfree(s.rowmax, (s.rows + 2) * sizeof(double));
     s = kern::SlicedOperand();
 }
 
@@ -85,7 +85,7 @@ void Context::ensure_ws(kern::SlicedOperand& w, int rows, int K) {
     w.bytes = keep_bytes;
     w.data = (uint8_t*)dmalloc(keep_bytes);
     w.scale = (double*)dmalloc(keep_rows * sizeof(double));
-    w.rowmax = (double*)dmalloc(keep_rows * sizeof(double));
+    w.rowmax = (double*)dmalloc((keep_rows + 2) * sizeof(double));
 }
 
 // Decide, for every split contraction of a plan, which constant operands keep cached
@@ -171,7 +171,7 @@ void Context::run_split_gemm(GemmStep& g, kern::GemmArgs& a) {
         return;
     }
     split_launches++;
-    const int ns = split_slices(), kind = slice_kind();
+    const int ns = step_slices(g), kind = slice_kind();
     auto prepare = [&](bool is_a, int64_t& key, kern::SlicedOperand& ws) -> kern::SlicedOperand* {
         const int rows = is_a ? g.M : g.N;
         const double* X = is_a ? a.A : a.B;
@@ -180,6 +180,15 @@ void Context::run_split_gemm(GemmStep& g, kern::GemmArgs& a) {
         const bool kc = is_a ? a.a_kcontig : a.b_kcontig;
         const int h = is_a ? g.tA : g.tB;
         bool& cached = is_a ? g.cache_a : g.cache_b;
+        // the first ns slices of a deeper slicing are the ns-slice slicing (each slice is the
+        // rounded remainder of the ones before): a cached operand with more slices serves
+        // a contraction that the autotuner runs with fewer
+        if (cached && key >= 0 && split_cache[key].kind == kind && split_cache[key].nslices > ns) {
+            kern::SlicedOperand& v = ws_view[is_a ? 0 : 1];
+            v = split_cache[key];
+            v.nslices = ns;
+            return &v;
+        }
         if (cached && key >= 0 && (split_cache[key].nslices != ns || split_cache[key].kind != kind)) {
             // the scheme changed (refinement): re-slice within the budget, or stop caching
             free_sliced(split_cache[key]);

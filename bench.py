@@ -58,6 +58,10 @@ DIIS_ORDER = 8
 # residual at which a split solve moves from 3 to 4 slices: above the 3-slice floor
 # (~2e-9 for BF16 slices, ~4e-7 for INT8 slices at o=32 v=256)
 REFINE_TOL = {"split": 1e-6, "split_i8": 1e-5}
+# energy budget (Eh) of the slice autotuner in the timed split mode: statements whose
+# one-slice-fewer trials change the next energy by at most this much in total keep one
+# slice fewer (the per-iteration parity vs FP64 in the line checks the outcome)
+AUTOTUNE_DE = 1e-9
 
 
 def log(*a):
@@ -149,9 +153,9 @@ def fp64_gemm_peak(torch, device):
     return best
 
 
-# rows of the bounded CPU sample: spin-orbital virtuals (a of Z2, FAE, W(am..)) and occupied
-# (m of F(mi), W(mn..)); the first and the last spin-orbital, one alpha and one beta
-CPU_SLAB_VIRTUALS = 2
+# rows of the bounded CPU sample: spin-orbital virtuals (a of Z2, FAE, W(am..)), spread evenly
+# over alpha and beta, and one occupied (m of F(mi), W(mn..))
+CPU_SLAB_VIRTUALS = 4
 
 
 def cpu_slab_sample(workload, warmup, steps):
@@ -357,7 +361,7 @@ def amplitude_blocks(T):
     return out
 
 
-def parity_vs_fp64(ctx, H, prec, slices, iters):
+def parity_vs_fp64(ctx, H, prec, slices, iters, autotune=0.0):
     """The split solver against the native-FP64 solver on the same H, iteration by iteration
     (each from the MP2 guess, DIIS order 8): |dE| and max|dT1|, max|dT2| over every stored
     amplitude element, the FP64 amplitudes kept on the host between the two runs."""
@@ -367,7 +371,8 @@ def parity_vs_fp64(ctx, H, prec, slices, iters):
         e, _ = s.iterate()
         snaps.append((e, amplitude_blocks(s.T1), amplitude_blocks(s.T2)))
     s.close()
-    s = ctx.solver(H, diis_order=DIIS_ORDER, precision=prec, conv_tol=1e-9, max_iter=1000, slices=slices)
+    s = ctx.solver(H, diis_order=DIIS_ORDER, precision=prec, conv_tol=1e-9, max_iter=1000, slices=slices,
+                   autotune_de=autotune)
     n0 = ctx.split_launches()
     rows = []
     for k in range(iters):
@@ -382,7 +387,7 @@ def parity_vs_fp64(ctx, H, prec, slices, iters):
             "max_abs_dT2": max(r[3] for r in rows), "split_gemm_launches": split,
             "per_iter": [[r[0], float(f"{r[1]:.3e}"), float(f"{r[2]:.3e}"), float(f"{r[3]:.3e}")] for r in rows],
             "per_iter_columns": ["iteration", "abs_dE", "max_abs_dT1", "max_abs_dT2"],
-            "routing": "natural (the timed mode's)"}
+            "routing": "natural (the timed mode's)", "slice_autotune_de": autotune}
 
 
 def int8_peak(torch, device, secs=3.0):
@@ -542,6 +547,9 @@ def main():
     ap.add_argument("--serve-seed", type=int, default=5)
     ap.add_argument("--validate-sample", action="store_true",
                     help="--impl reference: also time whole oracle iterations and compare with the estimate")
+    ap.add_argument("--autotune", type=float, default=None,
+                    help="slice autotuner energy budget in Eh for the split modes (default 1e-9 for 4 INT8 "
+                         "slices, 0 = off)")
     ap.add_argument("--parity-iters", type=int, default=8,
                     help="iterations of the split-vs-FP64 comparison before the timed runs (0: none)")
     ap.add_argument("--serve-sample", type=int, default=24,
@@ -577,8 +585,11 @@ def main():
     prec = args.precision if args.precision != "auto" else ("split_i8" if split_ok else "fp64")
     if prec == "split_i8" and args.slices == 0:
         # the timed mode: the fewest INT8 slices whose iterations hold |dE| <= 1e-8 Eh against
-        # the FP64 plain path at this workload (3 slices drift to ~3e-7, 4 to ~2e-9)
+        # the FP64 plain path at this workload (3 slices drift to ~1e-7, 4 stay near 1e-9),
+        # with the autotuner taking a slice away where the measured energy change allows
         args.slices = 4
+    if args.autotune is None:
+        args.autotune = AUTOTUNE_DE if (prec == "split_i8" and args.slices >= 4) else 0.0
 
     stream = torch.cuda.Stream(device=local)
     ctx = A.Context(local, stream.cuda_stream)
@@ -592,9 +603,9 @@ def main():
 
     peaks, peak_kind = measured_peaks()
     parity = None
-    if prec != "fp64" and not args.no_fp64_ref and args.parity_iters > 0:
+    if prec != "fp64" and args.parity_iters > 0:
         t0 = time.perf_counter()
-        parity = parity_vs_fp64(ctx, H, prec, args.slices, args.parity_iters)
+        parity = parity_vs_fp64(ctx, H, prec, args.slices, args.parity_iters, args.autotune)
         log(f"[bench] parity vs FP64 over {args.parity_iters} iterations ({time.perf_counter() - t0:.0f}s): "
             f"max|dE| {parity['max_abs_dE']:.2e}, max|dT1| {parity['max_abs_dT1']:.2e}, "
             f"max|dT2| {parity['max_abs_dT2']:.2e}, split GEMMs {parity['split_gemm_launches']}")
@@ -602,7 +613,7 @@ def main():
     order = ["fp64", prec] if (prec != "fp64" and not args.no_fp64_ref) else [prec]
     for p in order:
         s = ctx.solver(H, diis_order=DIIS_ORDER, precision=p, conv_tol=1e-9, max_iter=1000,
-                       slices=args.slices if p != "fp64" else 0)
+                       slices=args.slices if p != "fp64" else 0, autotune_de=args.autotune if p != "fp64" else 0.0)
         flops = s.flops()
         # the FP64 comparison path is stable from iteration to iteration: a few steps suffice
         steps = args.steps if p == prec else min(args.steps, 6)
@@ -614,7 +625,8 @@ def main():
             torch.cuda.synchronize()
         ms = max_over_ranks(ms, dist)
         results[p] = dict(ms=ms, steps=steps, launches=launches, prof=prof, energy=e, conv=c, flops=flops,
-                          clocks=clk.summary(), energies=None)
+                          clocks=clk.summary(), energies=None,
+                          slices=s.slice_report() if p != "fp64" else None)
         log(f"[bench] {p}: {ms / steps:.1f} ms/iter, E={e:.12f}, conv={c:.3e}, launches={launches}")
         log(f"[bench]   profiled contraction/sum steps: {sum(e['ms'] for e in prof.values()) / steps:.1f} ms/iter")
         for k, ent in sorted(prof.items(), key=lambda kv: -kv[1]["ms"])[:14]:
@@ -742,6 +754,9 @@ def main():
             line["speedup_vs_fp64_plain"] = (f["ms"] / f["steps"]) / (head["ms"] / head["steps"])
             line["fp64_dgemm_tflops"] = fp64_peak
         line["parity_vs_fp64"] = parity
+        if head.get("slices"):
+            line["slices_per_statement"] = [{"slices": ns, "dE": de, "statement": lab} for ns, de, lab in head["slices"]]
+            line["config"]["slice_autotune_de"] = args.autotune
         print(json.dumps(line), flush=True)
     if dist:
         dist.barrier()

@@ -187,9 +187,27 @@ typedef struct {
                              FP64 if the residual then stalls (0 = never).  About
                              1000 x conv_tol: the 3-slice floor is near 1e-9, and a
                              switch close to it leaves DIIS a history of 3-slice noise */
+    double autotune_de;   /* split precision only, > 0: slice count per contraction.  On
+                             the first iteration run at 4 or more slices, every statement
+                             with split contractions is evaluated once with one slice
+                             fewer, from the same amplitudes, and the change of the next
+                             energy is measured; statements whose changes add up to at
+                             most autotune_de (in Eh, smallest first) keep one slice fewer
+                             from then on (0 = every contraction at the solver's count) */
 } ccsd_options;
 
 void ccsd_options_default(ccsd_options* opts);
+
+/* The slice autotuner's rule, host only (no counterpart in the reference): given the
+ * measured energy changes dE[0..n) of dropping one slice in each of n statements, set
+ * drop[i] = 1 for the statements that take one slice fewer: smallest |dE| first, while
+ * the sum of the chosen |dE| stays <= budget (ties keep statement order). */
+int ccsd_slice_choice(int n, const double* dE, double budget, int* drop);
+/* Per statement of the solver's iteration with split contractions: its label, the slices
+ * it runs with and the energy change measured by the autotuner (0 if it did not run),
+ * as text lines "slices<TAB>dE<TAB>label\n" into buf (len bytes, NUL-terminated; the
+ * needed size is returned in *needed). */
+int ccsd_solver_slice_report(ccsd_solver s, char* buf, int64_t len, int64_t* needed);
 
 /* The 13 blocks of H in the order of TwoElectronOperator
  * (2eoperator.cxx:13-21, 1eoperator.hpp:39-44):
