@@ -86,10 +86,71 @@ struct Builder {
         kern::eri_gather(g, dEri, ctx.stream);
     }
 
+    // Symmetry-blocked H: thousands of small block products.  With `batch` set the Coulomb
+    // pieces are collected per level (a block's J piece in level 0, its K piece in level 1,
+    // so that every launch writes disjoint blocks) and flush() runs each level as one
+    // grouped FP64 launch with its tables uploaded in one copy, instead of one launch and
+    // five table uploads per piece: in the serving mix, where every launch of a small solve
+    // waits for a free SM behind the tiles of the large ones, this is the build's cost.
+    struct Piece {
+        double* C;
+        double sign;
+        int M, N, K;
+        std::vector<int64_t> Am, Ak, Bn, Cm, Cn;
+    };
+    bool batch = false;
+    std::vector<Piece> level[2];
+
+    void flush() {
+        for (auto& lv : level) {
+            if (lv.empty()) continue;
+            std::vector<int64_t> all;
+            std::vector<size_t> at;
+            for (auto& pc : lv)
+                for (auto* t : {&pc.Am, &pc.Ak, &pc.Bn, &pc.Cm, &pc.Cn}) {
+                    at.push_back(all.size());
+                    all.insert(all.end(), t->begin(), t->end());
+                }
+            Tables tb{ctx, {}};
+            const int64_t* d = tb.up(all);
+            std::vector<kern::GemmArgs> probs;
+            std::vector<int> tstart;
+            int tiles = 0;
+            size_t q = 0;
+            for (auto& pc : lv) {
+                kern::GemmArgs a;
+                a.A = dB;
+                a.B = dB;
+                a.C = pc.C;
+                a.M = pc.M;
+                a.N = pc.N;
+                a.K = pc.K;
+                a.alpha = pc.sign;
+                a.Am = d + at[q++];
+                a.Ak = d + at[q++];
+                a.Bk = a.Ak;
+                a.Bn = d + at[q++];
+                a.Cm[0] = d + at[q++];
+                a.Cn[0] = d + at[q++];
+                probs.push_back(a);
+                tstart.push_back(tiles);
+                tiles += kern::fp64_tiles(pc.M, pc.N);
+            }
+            kern::GemmArgs* dp = (kern::GemmArgs*)ctx.dmalloc(probs.size() * sizeof(kern::GemmArgs));
+            int* dt = (int*)ctx.dmalloc(tstart.size() * sizeof(int));
+            ctx.stage_h2d(dp, probs.data(), probs.size() * sizeof(kern::GemmArgs));
+            ctx.stage_h2d(dt, tstart.data(), tstart.size() * sizeof(int));
+            kern::gemm_fp64_grouped(dp, dt, (int)probs.size(), tiles, false, false, ctx.stream);
+            ctx.dfree(dp, probs.size() * sizeof(kern::GemmArgs));
+            ctx.dfree(dt, tstart.size() * sizeof(int));
+            lv.clear();
+        }
+    }
+
     // (x0 x1 | x2 x3) pieces over positions (pa, pb | pc, pd) of a block, scattered into
     // C with sign: C[off + sum stride*x] += sign * sum_P B[P,a,b] B[P,c,d]
     void coulomb(double* C, int64_t off, const int* space, const int* irrep, const int* len,
-                 const int64_t* stride, int pa, int pb, int pc, int pd, double sign) {
+                 const int64_t* stride, int pa, int pb, int pc, int pd, double sign, int lvl = 0) {
         if (dEri) {
             gather(C, off, space, irrep, len, stride, pa, pb, pc, pd, sign);
             return;
@@ -112,6 +173,11 @@ struct Builder {
                 Bn[m] = (int64_t)gidx(space[pc], irrep[pc], x) * n + gidx(space[pd], irrep[pd], y);
                 Cn[m] = stride[pc] * x + stride[pd] * y;
             }
+        if (batch) {
+            level[lvl].push_back({C, sign, (int)M, (int)N, (int)k.size(), std::move(Am), std::move(k), std::move(Bn),
+                                  std::move(Cm), std::move(Cn)});
+            return;
+        }
         Tables tb{ctx, {}};
         int64_t *dAm = tb.up(Am), *dK = tb.up(k), *dBn = tb.up(Bn), *dCm = tb.up(Cm), *dCn = tb.up(Cn);
         a.A = dB;
@@ -178,12 +244,16 @@ struct Builder {
                 bool J = s[0] == s[2] && s[1] == s[3];
                 bool K = s[0] == s[3] && s[1] == s[2];
                 if (b.pairs.empty()) {
-                    if (J) coulomb(T.data, b.offset, space, irr, len, b.stride.data(), 0, 2, 1, 3, 1.0);
-                    if (K) coulomb(T.data, b.offset, space, irr, len, b.stride.data(), 0, 3, 1, 2, -1.0);
+                    if (J) coulomb(T.data, b.offset, space, irr, len, b.stride.data(), 0, 2, 1, 3, 1.0, 0);
+                    if (K) coulomb(T.data, b.offset, space, irr, len, b.stride.data(), 0, 3, 1, 2, -1.0, 1);
                 } else {
+                    const bool was = batch;   // a packed block's pieces feed the pack kernel at once
+                    batch = false;
                     packed_block(T, sc, b, space, irr, len, J, K);
+                    batch = was;
                 }
             }
+        flush();
     }
 
     // every block of a plain (spatial) two-electron tensor as one Coulomb piece
@@ -201,6 +271,7 @@ struct Builder {
                 }
                 coulomb(T.data, b.offset, space, irr, len, b.stride.data(), pa, pb, pc, pd, 1.0);
             }
+        flush();
     }
 
     // packed V_abcd-type block: chunk over the first index, build (ac|bd) and (ad|bc)
@@ -365,6 +436,7 @@ void build_rhf_hamiltonian(Context& ctx, int naux, const double* B, const double
     bld.dB = (double*)ctx.dmalloc(nB * sizeof(double));
     CCSD_CUDA(cudaMemcpyAsync(bld.dB, B, nB * sizeof(double), cudaMemcpyHostToDevice, ctx.stream));
     create_rhf_hamiltonian_tensors(ctx, H);
+    bld.batch = S.nirrep > 1;
     bld.one_electron(H->fAB, eps);
     bld.one_electron(H->fIJ, eps);
     fill_rhf_two_electron(bld, H);
@@ -431,6 +503,7 @@ void build_hamiltonian(Context& ctx, int naux, const double* B, const double* ep
     CCSD_CUDA(cudaMemcpyAsync(bld.dB, B, nB * sizeof(double), cudaMemcpyHostToDevice, ctx.stream));
 
     create_hamiltonian_tensors(ctx, pack_vvvv, H);
+    bld.batch = S.nirrep > 1;
 
     bld.one_electron(H->fAE, eps);
     bld.one_electron(H->fMI, eps);

@@ -51,9 +51,15 @@ WORKLOADS = {
     "mid": dict(o=16, v=96, nirrep=1, seed=6, desc="synthetic closed-shell spin-orbital CCSD, C1, o=16 v=96"),
 }
 LADDER = "Z(2)[abij] += <ab||cd>[abef]*Tau[efij]"
-# DRAM bytes (read + write) per ladder launch from an ncu capture, per workload (filled in
-# from the committed summary under profiles/; None where no capture exists)
-LADDER_TRAFFIC = {}
+# DRAM bytes (read + write) per ladder launch from an ncu capture of the full-size workload
+# (one-pass metrics, so no scaling), per workload; the capture and its command are in
+# profiles/launches_split_o32v256.md
+LADDER_TRAFFIC = {
+    "cfg3": {"bytes_per_launch": 18.6e9,
+             "note": "mean of the three ladder launches (AA 5.4 GB, Ab 44.0 GB, bb 5.4 GB read + write) in one "
+                     "ncu capture of the timed iteration at o=32 v=256 (dram__bytes_read.sum + "
+                     "dram__bytes_write.sum); the Ab launch re-reads its 17.2 GB of cached slices ~2.5x"},
+}
 DIIS_ORDER = 8
 # residual at which a split solve moves from 3 to 4 slices: above the 3-slice floor
 # (~2e-9 for BF16 slices, ~4e-7 for INT8 slices at o=32 v=256)
