@@ -17,7 +17,7 @@ BUILD = HERE / "_build"
 
 CU = ["kernels_fp64.cu", "kernels_split.cu", "noalloc.cu"]
 CPP = ["context.cpp", "planner.cpp", "solver.cpp", "hbuild.cpp", "fcidump.cpp", "capi.cpp", "synth.cpp", "split_exec.cpp",
-       "server.cpp", "aomo.cpp", "plan_export.cpp", "diis.cpp"]
+       "server.cpp", "aomo.cpp", "plan_export.cpp", "diis.cpp", "merged.cpp"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -51,6 +51,8 @@ Context::~Context() {
         if (!kv.second->view_of) cudaFree(kv.second->data);   // views alias their base
     cudaFree(d_scalar);
     cudaFree(splitk_ws);
+    cudaFree(merged_ws);
+    for (double* q : merged_retired) cudaFree(q);
     for (auto& p : pending) {
         cudaEventDestroy(p.second.first);
         cudaEventDestroy(p.second.second);
@@ -316,13 +318,6 @@ int Context::create_view(const std::string& name, int hb, const int nout[2], con
 // executor
 // ---------------------------------------------------------------------------
 
-static int64_t* upload_table(Context& ctx, const std::vector<int64_t>& h) {
-    if (h.empty()) return nullptr;
-    int64_t* d = (int64_t*)ctx.dmalloc(h.size() * sizeof(int64_t));
-    ctx.stage_h2d(d, h.data(), h.size() * sizeof(int64_t));
-    return d;
-}
-
 std::pair<cudaEvent_t, cudaEvent_t> Context::prof_begin() {
     cudaEvent_t e0, e1;
     if (event_pool.size() >= 2) {
@@ -382,15 +377,51 @@ void Context::upload(Plan& p) {
         splitk_ws = (double*)dmalloc(need * sizeof(double));
         splitk_elems = need;
     }
+    // every table of the steps not yet uploaded goes into ONE device buffer with one copy:
+    // a symmetry-blocked plan has hundreds of thousands of tables, and an allocation and a
+    // copy per table cost seconds alone and minutes when several solves share the driver
+    {
+        int64_t total = 0;
+        auto count = [&](const std::vector<int64_t>& h) { total += (int64_t)h.size(); };
+        for (auto& g : p.gemms) {
+            if (g.dAm) continue;
+            count(g.hAm);
+            count(g.hAk);
+            count(g.hBk);
+            count(g.hBn);
+            for (int v = 0; v < g.nvm; v++) count(g.hCm[v]);
+            for (int v = 0; v < g.nvn; v++) count(g.hCn[v]);
+        }
+        if (total > 0) {
+            int64_t* d = (int64_t*)dmalloc(total * sizeof(int64_t));
+            p.table_pool.push_back({d, total * sizeof(int64_t)});
+            std::vector<int64_t> host;
+            host.reserve(total);
+            auto place = [&](const std::vector<int64_t>& h) -> int64_t* {
+                if (h.empty()) return nullptr;
+                int64_t* at = d + host.size();
+                host.insert(host.end(), h.begin(), h.end());
+                return at;
+            };
+            for (auto& g : p.gemms) {
+                if (g.dAm) continue;
+                g.dAm = place(g.hAm);
+                g.dAk = place(g.hAk);
+                g.dBk = place(g.hBk);
+                g.dBn = place(g.hBn);
+                for (int v = 0; v < g.nvm; v++) g.dCm[v] = place(g.hCm[v]);
+                for (int v = 0; v < g.nvn; v++) g.dCn[v] = place(g.hCn[v]);
+            }
+            if (!host_only) {
+                CCSD_CUDA(cudaMemcpyAsync(d, host.data(), total * sizeof(int64_t), cudaMemcpyHostToDevice, stream));
+                CCSD_CUDA(cudaStreamSynchronize(stream));   // the staging vector goes out of scope
+            }
+        }
+    }
     for (auto& g : p.gemms) {
-        if (g.dAm) continue;
+        if (g.uploaded) continue;
+        g.uploaded = true;
         any = true;
-        g.dAm = upload_table(*this, g.hAm);
-        g.dAk = upload_table(*this, g.hAk);
-        g.dBk = upload_table(*this, g.hBk);
-        g.dBn = upload_table(*this, g.hBn);
-        for (int v = 0; v < g.nvm; v++) g.dCm[v] = upload_table(*this, g.hCm[v]);
-        for (int v = 0; v < g.nvn; v++) g.dCn[v] = upload_table(*this, g.hCn[v]);
         // k tables that are arithmetic progressions let the kernels compute the offsets
         auto affine = [](const std::vector<int64_t>& t, int64_t& b0, int64_t& st) {
             if (t.empty()) return false;
@@ -415,19 +446,12 @@ void Context::upload(Plan& p) {
 void Context::release(Plan& p) {
     if (p.scratch) dfree(p.scratch, p.scratch_elems * sizeof(double));
     p.scratch = nullptr;
+    for (auto& t : p.table_pool) dfree(t.first, t.second);
+    p.table_pool.clear();
     for (auto& g : p.gemms) {
-        auto fr = [&](int64_t*& d, size_t n) {
-            if (d) dfree(d, n * sizeof(int64_t));
-            d = nullptr;
-        };
-        fr(g.dAm, g.hAm.size());
-        fr(g.dAk, g.hAk.size());
-        fr(g.dBk, g.hBk.size());
-        fr(g.dBn, g.hBn.size());
-        for (int v = 0; v < 2; v++) {
-            fr(g.dCm[v], g.hCm[v].size());
-            fr(g.dCn[v], g.hCn[v].size());
-        }
+        g.dAm = g.dAk = g.dBk = g.dBn = nullptr;
+        for (int v = 0; v < 2; v++) g.dCm[v] = g.dCn[v] = nullptr;
+        g.uploaded = false;
         // cached slices belong to the plan's contraction, not to the operand tensor alone
         drop_split_cache(g);
     }
@@ -440,6 +464,7 @@ void Context::release(Plan& p) {
                     dfree(l.d_tile_start, (l.kind == GemmLaunch::FOLD_GROUPS ? l.ngroups + 1 : l.nprob) * sizeof(int));
                 if (l.d_desc) dfree(l.d_desc, l.desc_bytes);
                 if (l.d_chunks) dfree(l.d_chunks, l.nprob * sizeof(int64_t));
+                if (l.merged) free_merged(*l.merged);
             }
     p.schedules.clear();
 }
@@ -599,11 +624,23 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
         maxlvl = std::max(maxlvl, lvl);
         if (groupable(g)) ngroupable++;
     }
-    if (ngroupable < 2) return;
     GemmRun run;
     run.first = first;
     run.end = end;
     bool any_group = false;
+    // the block products of one irrep class as one split GEMM (symmetry-blocked statements)
+    std::vector<char> merged(end - first, 0);
+    // CCSD_MERGED=0: no merged products (coverage tests)
+    const bool merge_on = !std::getenv("CCSD_MERGED") || std::getenv("CCSD_MERGED")[0] != '0';
+    if (merge_on && precision == CCSD_PREC_SPLIT_I8 && kern::split_supported() && spaces.nirrep > 1 &&
+        split_routing != CCSD_SPLIT_ROUTE_ALL) {
+        build_merged(p, run, first, end, merged, block_of);
+        any_group = !run.launches.empty();
+        ngroupable = 0;
+        for (int i = first; i < end; i++)
+            if (!merged[i - first] && groupable(p.gemms[p.steps[i].idx])) ngroupable++;
+    }
+    if (!any_group && ngroupable < 2) return;
 
     // Shared-output groups.  Small one-destination products that several levels would
     // serialise (block contractions of a symmetry-blocked statement summing into the same
@@ -617,7 +654,7 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
         int64_t part = 0;
         for (int i = first; i < end; i++) {
             const GemmStep& g = p.gemms[p.steps[i].idx];
-            if (!groupable(g) || g.nvm != 1 || g.nvn != 1 || key1[i - first].second < 0) continue;
+            if (merged[i - first] || !groupable(g) || g.nvm != 1 || g.nvn != 1 || key1[i - first].second < 0) continue;
             if ((int64_t)g.M * g.N > 65536) continue;
             in_fold[i - first] = 1;
             nfold++;
@@ -704,7 +741,7 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
     for (int L = 0; L <= maxlvl; L++) {
         std::vector<int> grp[4];
         for (int i = first; i < end; i++) {
-            if (level[i - first] != L || in_fold[i - first]) continue;
+            if (level[i - first] != L || in_fold[i - first] || merged[i - first]) continue;
             const int gi = p.steps[i].idx;
             const GemmStep& g = p.gemms[gi];
             if (groupable(g)) {
@@ -908,6 +945,7 @@ void Context::build_dot_run(Plan& p, RunSchedule& rs, int first, int end) {
 void Context::launch(Plan& p, const GemmLaunch& l, const std::string& label, double* dot_acc) {
     auto ev = profiling ? prof_begin() : std::make_pair((cudaEvent_t) nullptr, (cudaEvent_t) nullptr);
     switch (l.kind) {
+        case GemmLaunch::MERGED_SPLIT: run_merged(p, *l.merged); break;
         case GemmLaunch::GEMM: run_gemm(p, p.gemms[l.gemm]); break;
         case GemmLaunch::GEMM_GROUPED:
             kern::gemm_fp64_grouped(l.d_probs, l.d_tile_start, l.nprob, l.tiles, l.ak, l.bk, stream);

@@ -11,7 +11,9 @@
 #include <cstdint>
 #include <string>
 #include <vector>
+#include <functional>
 #include <map>
+#include <memory>
 #include <memory>
 #include <stdexcept>
 
@@ -126,6 +128,11 @@ struct GemmStep {
     double flops() const { return 2.0 * M * N * (double)K; }
     std::string label;                 // statement this block contraction came from
     int slice_delta = 0;               // split path: slices relative to the context's count (autotuner)
+    bool uploaded = false;             // device tables placed (Context::upload)
+    // what the rows, columns and k range of this block product are (operand, spin and irrep
+    // of every index, restricted pairs): block products of one statement that share a key
+    // along a dimension share those rows / columns / k (merged symmetry-blocked products)
+    std::string mkey, nkey, kkey;
     int64_t split_cache_a = -1;        // keys of cached slices of constant operands
     int64_t split_cache_b = -1;
     bool cache_a = false, cache_b = false;   // operand slices kept across calls (set at reserve)
@@ -172,7 +179,7 @@ constexpr int kScratch = -1;
 // step, or one batched launch over several steps whose outputs are disjoint (GEMMs on the
 // grouped tiled-FP64 kernel, permuted sums, block scalings).
 struct GemmLaunch {
-    enum Kind { GEMM, GEMM_GROUPED, FOLD_GROUPS, SUM, SUM_BATCHED, SCALE, SCALE_BATCHED, DOT_BATCHED };
+    enum Kind { GEMM, GEMM_GROUPED, FOLD_GROUPS, SUM, SUM_BATCHED, SCALE, SCALE_BATCHED, DOT_BATCHED, MERGED_SPLIT };
     Kind kind = GEMM;
     int gemm = -1;                     // single GEMM: index into Plan::gemms
     int step = -1;                     // single SUM / SCALE: index into Plan::sums / scales
@@ -188,6 +195,28 @@ struct GemmLaunch {
     size_t desc_bytes = 0;
     int64_t chunks = 0;
     double flops = 0;
+    std::shared_ptr<struct MergedProduct> merged;   // MERGED_SPLIT
+};
+// The block products of one irrep class of a symmetry-blocked statement as one dense split
+// GEMM: rectangles of A (rows x k), of B (columns x k) and of C (rows x columns) placed in
+// the merged operands; the scatter of C runs in levels so that no two rectangles of one
+// launch write the same block.
+struct MergedProduct {
+    int M = 0, N = 0, K = 0;
+    int first_gemm = -1;               // a member (slice count)
+    int nA = 0, nB = 0;
+    int64_t tilesA = 0, tilesB = 0;
+    kern::RectDesc* dA = nullptr;
+    kern::RectDesc* dB = nullptr;
+    int64_t *dA_ts = nullptr, *dB_ts = nullptr;
+    struct Level {
+        kern::ScatterDesc* d = nullptr;
+        int64_t* cs = nullptr;
+        int n = 0;
+        int64_t chunks = 0;
+    };
+    std::vector<Level> levels;
+    int members = 0;
 };
 struct GemmRun {
     int first = 0, end = 0;            // steps [first, end)
@@ -203,6 +232,7 @@ struct Plan {
     int64_t scratch_elems = 0;         // doubles of scratch the steps need (products X)
     double* scratch = nullptr;         // allocated at upload
     bool split_reserved = false;       // split-path workspace sized for this plan
+    std::vector<std::pair<void*, size_t>> table_pool;   // device buffers holding the steps' tables
     std::vector<Step> steps;
     std::vector<GemmStep> gemms;
     std::vector<SumStep> sums;
@@ -262,6 +292,13 @@ public:
     std::map<int64_t, int> split_owner;                    // cache key -> tensor handle
     int64_t split_cache_next = 1;
     kern::SlicedOperand ws_view[2];                        // workspace views of the current call
+    double* merged_ws = nullptr;                           // dense products of merged launches
+    int64_t merged_ws_elems = 0;
+    std::vector<double*> merged_retired;                   // outgrown, kept until the context goes
+    void build_merged(Plan& p, GemmRun& run, int first, int end, std::vector<char>& merged,
+                      const std::function<std::pair<int, int64_t>(int, int64_t)>& block_of);
+    void run_merged(Plan& p, const MergedProduct& m);
+    void free_merged(MergedProduct& m);
     double* splitk_ws = nullptr;                           // FP64 split-K partials
     int64_t splitk_elems = 0;
     kern::SlicedOperand alloc_sliced(int rows, int K, int nslices, int kind);

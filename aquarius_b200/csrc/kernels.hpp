@@ -33,6 +33,9 @@ struct GemmArgs {
     // grouped launches with shared outputs: write the raw product to ws[m][n] (no alpha,
     // no scatter); a fold applies it to C
     bool partial_out = false;
+    // split path: write the scaled product to ws[z][m][n] (dense, no alpha, no fold) for a
+    // scatter by the caller (merged symmetry-blocked products)
+    bool dense_out = false;
 };
 
 // Fold of dense partial products into C: C[Cm[m] + Cn[n]] += scale * part[m*N + n], the
@@ -108,6 +111,39 @@ void gemm_split(const SlicedOperand& a, const SlicedOperand& b, int M, int N, in
 int split_ksplit(int M, int N, int K, int nslices = 3, int kind = SLICE_BF16);
 // alpha * sum_z ws[z][m][n] scattered into every destination variant of g (fixed order)
 void splitk_fold(const GemmArgs& g, int ks, cudaStream_t s);
+
+// Merged products of a symmetry-blocked statement: the block products of one irrep class
+// form one dense GEMM.  Its operands are rectangles (a block product's rows x its k range)
+// placed at (row0, k0) of a merged operand; its result goes to a dense workspace and is
+// scattered into the C blocks rectangle by rectangle.
+struct RectDesc {
+    const double* X = nullptr;     // storage the rectangle's offsets index
+    const int64_t* R = nullptr;    // row offsets (nrows)
+    const int64_t* Kt = nullptr;   // k offsets (nk)
+    int nrows = 0, nk = 0;
+    int row0 = 0, k0 = 0;          // position in the merged operand
+    int kc = 0;                    // neighbouring k adjacent in memory (lanes along k)
+    int tiles_r = 0;               // 32-row tiles of the rectangle
+    double mul = 1.0;              // factor of the rectangle's values (its product's coefficient
+                                   // relative to the class's, folded into the B operand)
+};
+// row maxima over all rectangles of a row, then INT8 slices of every rectangle into out
+// (its rows, scales and slices zeroed first); tile_start[i] = first 32 x 64 tile of
+// rectangle i, ntiles in all
+void rect_slice(const RectDesc* d, const int64_t* tile_start, int n, int64_t ntiles, int ns, SlicedOperand& out,
+                cudaStream_t s);
+struct ScatterDesc {
+    double* C = nullptr;
+    const int64_t* Cm[2] = {nullptr, nullptr};
+    const int64_t* Cn[2] = {nullptr, nullptr};
+    int nvm = 1, nvn = 1;
+    double vsign[4] = {1, 1, 1, 1};
+    double alpha = 0;
+    int nrows = 0, ncols = 0, row0 = 0, col0 = 0;
+};
+// C += alpha * sum_z ws[z] over each rectangle (chunks of kBatchChunk elements)
+void rect_scatter(const ScatterDesc* d, const int64_t* chunk_start, int n, int64_t chunks, const double* ws, int ldn,
+                  int64_t zstride, int ks, cudaStream_t s);
 bool split_supported();
 // nonzero if a split-GEMM wait expired (1..4 = which wait); reset clears it
 int split_error(bool reset);

@@ -122,6 +122,7 @@ struct Params {
     int ks;
     int kb_per;                    // K blocks per range (a multiple of the exact chunk)
     double* ws;
+    int dense;                     // write ws[z][m][n] even without split-K (merged products)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -386,7 +387,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             __syncwarp();
             if (lane == 0) mbar_arrive(&tempty[b]);
         }
-        if (ok && p.ks > 1) {
+        if (ok && (p.ks > 1 || p.dense)) {
             const int m = m0 + q * 32 + lane;
             if (m < p.M) {
                 const double sa = p.scaleA[m];
@@ -830,6 +831,9 @@ void gemm_split(const SlicedOperand& a, const SlicedOperand& b, int M, int N, in
     p.ks = ks;
     p.kb_per = ks > 1 ? per_grains * si.grain : nkb;
     p.ws = g.ws;
+    p.dense = g.dense_out ? 1 : 0;
+    if (g.dense_out && (!g.ws || (int64_t)ks * M * N > g.ws_elems))
+        throw std::runtime_error("merged split product: dense output workspace too small");
     const int tiles = (a.rows / BM) * p.tiles_n;
     const dim3 grid(tiles, ks);
     if (kind == SLICE_INT8) {
@@ -841,7 +845,178 @@ void gemm_split(const SlicedOperand& a, const SlicedOperand& b, int M, int N, in
         else split_gemm_kernel<4, false><<<grid, THREADS, si.smem, s>>>(ma, mb, p);
     }
     g_launches++;
-    if (ks > 1) splitk_fold(g, ks, s);
+    if (ks > 1 && !g.dense_out) splitk_fold(g, ks, s);
+}
+
+// ---------------------------------------------------------------------------
+// merged symmetry-blocked products: slicing of rectangles of a merged operand, and the
+// scatter of the merged dense product into the blocks of C
+// ---------------------------------------------------------------------------
+namespace {
+
+__device__ __forceinline__ int find_rect(const int64_t* __restrict__ ts, int n, int64_t t) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (ts[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// one 32 x 64 tile of one rectangle per CTA: element (r, k) of the rectangle into v (0
+// outside), lanes along k where the rectangle's k are contiguous, else along the rows
+__device__ __forceinline__ void rect_tile(const RectDesc& d, int64_t lt, int& r0, int& k0, double* v, int64_t* sR,
+                                          int64_t* sK) {
+    using namespace split;
+    r0 = (int)(lt % d.tiles_r) * SR;
+    k0 = (int)(lt / d.tiles_r) * SK;
+    for (int i = threadIdx.x; i < SR; i += STHREADS) sR[i] = (r0 + i < d.nrows) ? d.R[r0 + i] : -1;
+    for (int i = threadIdx.x; i < SK; i += STHREADS) sK[i] = (k0 + i < d.nk) ? d.Kt[k0 + i] : -1;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < SPER; i++) {
+        const int e = threadIdx.x + i * STHREADS;
+        const int r = d.kc ? e / SK : e % SR, k = d.kc ? e % SK : e / SR;
+        v[i] = (sR[r] >= 0 && sK[k] >= 0) ? d.mul * d.X[sR[r] + sK[k]] : 0.0;
+    }
+}
+
+__global__ void __launch_bounds__(split::STHREADS) rect_rowmax_kernel(const RectDesc* __restrict__ rd,
+                                                                      const int64_t* __restrict__ ts, int n,
+                                                                      unsigned long long* rowmax) {
+    using namespace split;
+    __shared__ int64_t sR[SR], sK[SK];
+    __shared__ double red[STHREADS / 32][SR];
+    __shared__ int sp;
+    if (threadIdx.x == 0) sp = find_rect(ts, n, blockIdx.x);
+    __syncthreads();
+    const RectDesc& d = rd[sp];
+    int r0, k0;
+    double v[SPER];
+    rect_tile(d, blockIdx.x - ts[sp], r0, k0, v, sR, sK);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (d.kc) {
+#pragma unroll
+        for (int i = 0; i < SPER; i++) {
+            double m = fabs(v[i]);
+            for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+            const int r = (warp >> 1) + 4 * i;
+            if (lane == 0 && r0 + r < d.nrows && m > 0.0)
+                atomicMax(&rowmax[d.row0 + r0 + r], (unsigned long long)__double_as_longlong(m));
+        }
+    } else {
+        double m = 0.0;
+#pragma unroll
+        for (int i = 0; i < SPER; i++) m = fmax(m, fabs(v[i]));
+        red[warp][lane] = m;
+        __syncthreads();
+        if (warp == 0) {
+            for (int w = 1; w < STHREADS / 32; w++) m = fmax(m, red[w][lane]);
+            if (r0 + lane < d.nrows && m > 0.0)
+                atomicMax(&rowmax[d.row0 + r0 + lane], (unsigned long long)__double_as_longlong(m));
+        }
+    }
+}
+
+template <int NS>
+__global__ void __launch_bounds__(split::STHREADS) rect_slice_kernel(const RectDesc* __restrict__ rd,
+                                                                     const int64_t* __restrict__ ts, int n,
+                                                                     const unsigned long long* __restrict__ rowmax,
+                                                                     int rows_p, int kpad, uint8_t* __restrict__ out,
+                                                                     double* __restrict__ scale) {
+    using namespace split;
+    __shared__ double tile[SR][SK + 1];
+    __shared__ int64_t sR[SR], sK[SK];
+    __shared__ double sMul[SR];
+    __shared__ int sp;
+    if (threadIdx.x == 0) sp = find_rect(ts, n, blockIdx.x);
+    __syncthreads();
+    const RectDesc& d = rd[sp];
+    int r0, k0;
+    double v[SPER];
+    rect_tile(d, blockIdx.x - ts[sp], r0, k0, v, sR, sK);
+    if (threadIdx.x < SR) {
+        const int row = d.row0 + r0 + threadIdx.x;
+        const bool in = r0 + (int)threadIdx.x < d.nrows;
+        const double mx = in ? __longlong_as_double((long long)rowmax[row]) : 0.0;
+        const bool nz = mx > 1e-290;
+        sMul[threadIdx.x] = nz ? 127.0 / mx : 0.0;
+        if (in && d.k0 == 0 && k0 == 0) scale[row] = nz ? mx / 127.0 : 0.0;   // the row's first rectangle
+    }
+#pragma unroll
+    for (int i = 0; i < SPER; i++) {
+        const int e = threadIdx.x + i * STHREADS;
+        const int r = d.kc ? e / SK : e % SR, k = d.kc ? e % SK : e / SR;
+        tile[r][k] = v[i];
+    }
+    __syncthreads();
+    const size_t plane = (size_t)rows_p * kpad;
+#pragma unroll
+    for (int i = 0; i < SPER; i++) {
+        const int e = threadIdx.x + i * STHREADS;
+        const int k = e % SK, r = e / SK;
+        if (r0 + r >= d.nrows || k0 + k >= d.nk) continue;
+        const double mul = sMul[r];
+        const size_t o = (size_t)(d.row0 + r0 + r) * kpad + (size_t)(d.k0 + k0 + k);
+        double y = tile[r][k] * mul;
+#pragma unroll
+        for (int q = 0; q < NS; q++) {
+            const double st = mul > 0.0 ? rint(y) : 0.0;
+            out[q * plane + o] = (uint8_t)(int8_t)(int)st;
+            y = (y - st) * 254.0;
+        }
+    }
+}
+
+// C[Cm_a[m] + Cn_b[n]] += vsign_ab * alpha * sum_z ws[z][row0 + m][col0 + n] for one
+// rectangle's chunk of kBatchChunk elements per CTA
+__global__ void __launch_bounds__(256) rect_scatter_kernel(const ScatterDesc* __restrict__ sd,
+                                                           const int64_t* __restrict__ cs, int n,
+                                                           const double* __restrict__ ws, int ldn, int64_t zstride,
+                                                           int ks) {
+    __shared__ int sp;
+    if (threadIdx.x == 0) sp = find_rect(cs, n, blockIdx.x);
+    __syncthreads();
+    const ScatterDesc& d = sd[sp];
+    const int64_t base = (blockIdx.x - cs[sp]) * (int64_t)kBatchChunk;
+    const int64_t total = (int64_t)d.nrows * d.ncols;
+    for (int i = threadIdx.x; i < kBatchChunk; i += blockDim.x) {
+        const int64_t l = base + i;
+        if (l >= total) break;
+        const int m = (int)(l / d.ncols), c = (int)(l % d.ncols);
+        const int64_t w = (int64_t)(d.row0 + m) * ldn + d.col0 + c;
+        double v = 0.0;
+        for (int z = 0; z < ks; z++) v += ws[z * zstride + w];
+        v *= d.alpha;
+        for (int a = 0; a < d.nvm; a++)
+            for (int b = 0; b < d.nvn; b++) d.C[d.Cm[a][m] + d.Cn[b][c]] += d.vsign[a * d.nvn + b] * v;
+    }
+}
+
+}  // namespace
+
+void rect_slice(const RectDesc* d, const int64_t* tile_start, int n, int64_t ntiles, int ns, SlicedOperand& out,
+                cudaStream_t s) {
+    using namespace split;
+    if (n <= 0 || ntiles <= 0) return;
+    if (out.kind != SLICE_INT8) throw std::runtime_error("merged products slice to INT8 only");
+    unsigned long long* rowmax = reinterpret_cast<unsigned long long*>(out.rowmax);
+    cudaMemsetAsync(rowmax, 0, sizeof(double) * out.rows, s);
+    cudaMemsetAsync(out.scale, 0, sizeof(double) * out.rows, s);
+    cudaMemsetAsync(out.data, 0, (size_t)ns * out.rows * out.kpad, s);
+    rect_rowmax_kernel<<<(unsigned)ntiles, STHREADS, 0, s>>>(d, tile_start, n, rowmax);
+    if (ns == 3) rect_slice_kernel<3><<<(unsigned)ntiles, STHREADS, 0, s>>>(d, tile_start, n, rowmax, out.rows, out.kpad, out.data, out.scale);
+    else if (ns == 4) rect_slice_kernel<4><<<(unsigned)ntiles, STHREADS, 0, s>>>(d, tile_start, n, rowmax, out.rows, out.kpad, out.data, out.scale);
+    else rect_slice_kernel<5><<<(unsigned)ntiles, STHREADS, 0, s>>>(d, tile_start, n, rowmax, out.rows, out.kpad, out.data, out.scale);
+    g_launches += 2;
+}
+
+void rect_scatter(const ScatterDesc* d, const int64_t* chunk_start, int n, int64_t chunks, const double* ws, int ldn,
+                  int64_t zstride, int ks, cudaStream_t s) {
+    if (n <= 0 || chunks <= 0) return;
+    rect_scatter_kernel<<<(unsigned)chunks, 256, 0, s>>>(d, chunk_start, n, ws, ldn, zstride, ks);
+    g_launches++;
 }
 
 int split_error(bool reset) {

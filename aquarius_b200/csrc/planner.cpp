@@ -479,6 +479,19 @@ void lower_gemm(Context& ctx, Term& t, int hA, int hB, int hC, int cc, std::set<
     g.K = (int)K;
     g.alpha = t.coef * factor;
 
+    {
+        auto key_of = [&](const std::vector<int>& vl, const std::vector<std::pair<int, int>>& prs) {
+            std::string s;
+            for (int v : vl)
+                s += std::to_string(v) + ':' + std::to_string(vars[v].space) + std::to_string(vars[v].spin) + ':' +
+                     std::to_string(vars[v].irrep) + ',';
+            for (auto& pr : prs) s += 'p' + std::to_string(pr.first) + '-' + std::to_string(pr.second) + ',';
+            return s;
+        };
+        g.mkey = std::to_string(hA) + '|' + std::to_string(g.tC) + '|' + key_of(t.mvars, mpairs);
+        g.nkey = std::to_string(hB) + '|' + key_of(t.nvars, npairs);
+        g.kkey = key_of(t.kvars, kpairs);
+    }
     std::vector<int> all_m = t.mvars, all_n = t.nvars, all_k = t.kvars;
     const Block& bA = *t.A.blk;
     const Block& bB = *t.B.blk;
