@@ -598,9 +598,24 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
         if (g.flops() < 4e8 && g.K <= 4096) return true;
         return kern::fp64_ksplit(g.M, g.N, g.K, !fp64_tiled_only) == 1 && kern::fp64_ksplit(g.M, g.N, g.K, false) == 1;
     };
+    // short products (both extents <= 64, long K) compute partials on the short kernel and
+    // join the fold below, whatever their levels
+    // (CCSD_SHORT_MIN_K: the shortest K that takes them, default 512; coverage tests lower it)
+    const int short_min_k = std::getenv("CCSD_SHORT_MIN_K") ? std::atoi(std::getenv("CCSD_SHORT_MIN_K")) : 512;
+    auto shortable = [&](const GemmStep& g) {
+        return !fp64_tiled_only && !routes_split(g) && g.K >= short_min_k && kern::short_shape(g.M, g.N).first > 0;
+    };
+    // skinny products without a K split share one launch per level and shape
+    auto skinny_groupable = [&](const GemmStep& g) {
+        return !fp64_tiled_only && !routes_split(g) && !groupable(g) && kern::skinny_groups(g.M, g.N) > 0 &&
+               kern::fp64_ksplit(g.M, g.N, g.K, true) == 1;
+    };
+    int nskinny = 0;
     std::map<std::pair<int, int64_t>, int> last;
     std::vector<int> level(end - first, 0);
     std::vector<std::pair<int, int64_t>> key1(end - first, {0, -1});   // the block of a one-destination step
+    std::vector<std::vector<std::pair<int, int64_t>>> keys_of(end - first);   // every output block of a step
+    int nshort = 0;
     int maxlvl = 0;
     int ngroupable = 0;
     for (int i = first; i < end; i++) {
@@ -621,8 +636,11 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
         for (auto& k : keys) last[k] = lvl;
         level[i - first] = lvl;
         if (keys.size() == 1) key1[i - first] = keys[0];
+        keys_of[i - first] = keys;
         maxlvl = std::max(maxlvl, lvl);
         if (groupable(g)) ngroupable++;
+        if (shortable(g)) nshort++;
+        if (skinny_groupable(g)) nskinny++;
     }
     GemmRun run;
     run.first = first;
@@ -640,63 +658,117 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
         for (int i = first; i < end; i++)
             if (!merged[i - first] && groupable(p.gemms[p.steps[i].idx])) ngroupable++;
     }
-    if (!any_group && ngroupable < 2) return;
+    if (!any_group && ngroupable < 2 && nshort == 0 && nskinny < 2) return;
 
     // Shared-output groups.  Small one-destination products that several levels would
     // serialise (block contractions of a symmetry-blocked statement summing into the same
     // output blocks over their internal irreps) run as one grouped launch per operand
-    // contiguity writing dense partial products, then one fold launch: a CTA per output
-    // block adds its products in plan order (deterministic).
-    std::vector<char> in_fold(end - first, 0);
+    // contiguity writing dense partial products, and the short products as one launch per
+    // fragment shape writing a partial per CTA; then one fold launch: a CTA per group of
+    // output blocks (products that share a block, antisymmetriser variants included, fall in
+    // one group) adds its products in plan order (deterministic).
+    std::vector<char> in_fold(end - first, 0);   // 1: tile partial, 2: short partials
     {
         int nfold = 0;
         bool multi = false;
         int64_t part = 0;
         for (int i = first; i < end; i++) {
             const GemmStep& g = p.gemms[p.steps[i].idx];
-            if (merged[i - first] || !groupable(g) || g.nvm != 1 || g.nvn != 1 || key1[i - first].second < 0) continue;
+            if (merged[i - first] || shortable(g) || !groupable(g) || g.nvm != 1 || g.nvn != 1 ||
+                key1[i - first].second < 0)
+                continue;
             if ((int64_t)g.M * g.N > 65536) continue;
             in_fold[i - first] = 1;
             nfold++;
             multi |= level[i - first] > 0;
             part += (int64_t)g.M * g.N;
         }
-        if (nfold < 2 || !multi || part > (32ll << 20)) std::fill(in_fold.begin(), in_fold.end(), 0);
-        else {
-            double* d_part = (double*)dmalloc(part * sizeof(double));
+        if (nfold < 2 || !multi || part > (32ll << 20)) {
+            std::fill(in_fold.begin(), in_fold.end(), 0);
+            part = 0;
+        }
+        std::vector<int> sctas(end - first, 0), skper(end - first, 0);
+        for (int i = first; i < end; i++) {
+            const GemmStep& g = p.gemms[p.steps[i].idx];
+            if (merged[i - first] || !shortable(g) || keys_of[i - first].empty()) continue;
+            in_fold[i - first] = 2;
+            sctas[i - first] = kern::short_ctas(g.K, &skper[i - first]);
+            part += (int64_t)sctas[i - first] * g.M * g.N;
+        }
+        if (std::any_of(in_fold.begin(), in_fold.end(), [](char c) { return c != 0; })) {
+            double* d_part = (double*)dmalloc(std::max<int64_t>(part, 1) * sizeof(double));
+            bool owner = true;   // the partial buffer is owned by the first launch
+            auto own = [&](GemmLaunch& l) {
+                if (!owner) return;
+                l.d_part = d_part;
+                l.part_elems = std::max<int64_t>(part, 1);
+                owner = false;
+            };
             int64_t off = 0;
             std::vector<kern::GemmArgs> probs[4];
             std::vector<int> tstart[4];
             int tiles[4] = {0, 0, 0, 0};
             double fl[4] = {0, 0, 0, 0};
-            std::map<std::pair<int, int64_t>, std::vector<kern::FoldDesc>> groups;
-            std::vector<std::pair<int, int64_t>> group_order;
+            std::map<std::pair<int, int>, std::vector<kern::ShortDesc>> sprobs;
+            std::map<std::pair<int, int>, std::vector<int>> sstart;
+            std::map<std::pair<int, int>, int> sctas_total;
+            std::map<std::pair<int, int>, double> sfl;
+            std::vector<kern::FoldDesc> fdesc(end - first);
             for (int i = first; i < end; i++) {
                 if (!in_fold[i - first]) continue;
                 const GemmStep& g = p.gemms[p.steps[i].idx];
                 kern::GemmArgs a = gemm_args(p, g);
-                kern::FoldDesc f;
+                kern::FoldDesc& f = fdesc[i - first];
                 f.part = d_part + off;
                 f.C = a.C;
-                f.Cm = a.Cm[0];
-                f.Cn = a.Cn[0];
+                for (int v = 0; v < 2; v++) {
+                    f.Cm[v] = a.Cm[v];
+                    f.Cn[v] = a.Cn[v];
+                }
+                f.nvm = a.nvm;
+                f.nvn = a.nvn;
+                for (int v = 0; v < 4; v++) f.vsign[v] = a.vsign[v];
                 f.M = g.M;
                 f.N = g.N;
-                f.scale = a.alpha * a.vsign[0];
-                a.ws = d_part + off;
-                a.ws_elems = (int64_t)g.M * g.N;
-                a.partial_out = true;
-                off += (int64_t)g.M * g.N;
-                const int c = (g.a_kcontig ? 2 : 0) + (g.b_kcontig ? 1 : 0);
-                probs[c].push_back(a);
-                tstart[c].push_back(tiles[c]);
-                tiles[c] += kern::fp64_tiles(g.M, g.N);
-                fl[c] += g.flops();
-                auto k = key1[i - first];
-                if (!groups.count(k)) group_order.push_back(k);
-                groups[k].push_back(f);
+                f.scale = a.alpha;
+                if (in_fold[i - first] == 1) {
+                    a.ws = d_part + off;
+                    a.ws_elems = (int64_t)g.M * g.N;
+                    a.partial_out = true;
+                    off += (int64_t)g.M * g.N;
+                    const int c = (g.a_kcontig ? 2 : 0) + (g.b_kcontig ? 1 : 0);
+                    probs[c].push_back(a);
+                    tstart[c].push_back(tiles[c]);
+                    tiles[c] += kern::fp64_tiles(g.M, g.N);
+                    fl[c] += g.flops();
+                } else {
+                    const auto shape = kern::short_shape(g.M, g.N);
+                    kern::ShortDesc d;
+                    d.A = a.A;
+                    d.B = a.B;
+                    d.Am = a.Am;
+                    d.Ak = a.Ak;
+                    d.Bk = a.Bk;
+                    d.Bn = a.Bn;
+                    d.ak_affine = a.ak_affine;
+                    d.bk_affine = a.bk_affine;
+                    d.ak0 = a.ak0;
+                    d.ak_step = a.ak_step;
+                    d.bk0 = a.bk0;
+                    d.bk_step = a.bk_step;
+                    d.M = g.M;
+                    d.N = g.N;
+                    d.K = g.K;
+                    d.kper = skper[i - first];
+                    d.part = d_part + off;
+                    f.ks = sctas[i - first];
+                    off += (int64_t)f.ks * g.M * g.N;
+                    sstart[shape].push_back(sctas_total[shape]);
+                    sctas_total[shape] += f.ks;
+                    sprobs[shape].push_back(d);
+                    sfl[shape] += g.flops();
+                }
             }
-            bool first_launch = true;
             for (int c = 0; c < 4; c++) {
                 if (probs[c].empty()) continue;
                 GemmLaunch l;
@@ -706,22 +778,69 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
                 l.nprob = (int)probs[c].size();
                 l.tiles = tiles[c];
                 l.flops = fl[c];
-                if (first_launch) {   // the partial buffer is owned by the first launch
-                    l.d_part = d_part;
-                    l.part_elems = part;
-                    first_launch = false;
-                }
+                own(l);
                 l.d_probs = (kern::GemmArgs*)dmalloc(probs[c].size() * sizeof(kern::GemmArgs));
                 l.d_tile_start = (int*)dmalloc(tstart[c].size() * sizeof(int));
                 stage_h2d(l.d_probs, probs[c].data(), probs[c].size() * sizeof(kern::GemmArgs));
                 stage_h2d(l.d_tile_start, tstart[c].data(), tstart[c].size() * sizeof(int));
                 run.launches.push_back(l);
             }
+            for (auto& kv : sprobs) {
+                GemmLaunch l;
+                l.kind = GemmLaunch::SHORT_GROUPED;
+                l.mt = kv.first.first;
+                l.nt = kv.first.second;
+                l.nprob = (int)kv.second.size();
+                l.tiles = sctas_total[kv.first];
+                l.flops = sfl[kv.first];
+                own(l);
+                l.desc_bytes = kv.second.size() * sizeof(kern::ShortDesc);
+                l.d_desc = dmalloc(l.desc_bytes);
+                l.d_tile_start = (int*)dmalloc(kv.second.size() * sizeof(int));
+                stage_h2d(l.d_desc, kv.second.data(), l.desc_bytes);
+                stage_h2d(l.d_tile_start, sstart[kv.first].data(), kv.second.size() * sizeof(int));
+                run.launches.push_back(l);
+            }
+            // groups: products connected through a shared output block, in plan order
+            std::map<std::pair<int, int64_t>, int> bid;
+            std::vector<int> par;
+            auto find = [&](int x) {
+                while (par[x] != x) x = par[x] = par[par[x]];
+                return x;
+            };
+            for (int i = first; i < end; i++) {
+                if (!in_fold[i - first]) continue;
+                int root = -1;
+                for (auto& k : keys_of[i - first]) {
+                    auto it = bid.find(k);
+                    int b;
+                    if (it == bid.end()) {
+                        b = (int)par.size();
+                        par.push_back(b);
+                        bid.emplace(k, b);
+                    } else {
+                        b = it->second;
+                    }
+                    if (root < 0) root = find(b);
+                    else {
+                        const int rb = find(b);
+                        if (rb != root) par[rb] = root;
+                    }
+                }
+            }
+            std::map<int, std::vector<int>> members;
+            std::vector<int> group_order;
+            for (int i = first; i < end; i++) {
+                if (!in_fold[i - first]) continue;
+                const int r = find(bid.at(keys_of[i - first][0]));
+                if (!members.count(r)) group_order.push_back(r);
+                members[r].push_back(i - first);
+            }
             std::vector<kern::FoldDesc> descs;
             std::vector<int> gstart;
-            for (auto& k : group_order) {
+            for (int r : group_order) {
                 gstart.push_back((int)descs.size());
-                for (auto& f : groups[k]) descs.push_back(f);
+                for (int j : members[r]) descs.push_back(fdesc[j]);
             }
             gstart.push_back((int)descs.size());
             GemmLaunch fl_l;
@@ -740,12 +859,16 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
 
     for (int L = 0; L <= maxlvl; L++) {
         std::vector<int> grp[4];
+        std::map<std::pair<int, bool>, std::vector<int>> sk;
         for (int i = first; i < end; i++) {
             if (level[i - first] != L || in_fold[i - first] || merged[i - first]) continue;
             const int gi = p.steps[i].idx;
             const GemmStep& g = p.gemms[gi];
             if (groupable(g)) {
                 grp[(g.a_kcontig ? 2 : 0) + (g.b_kcontig ? 1 : 0)].push_back(gi);
+            } else if (skinny_groupable(g)) {
+                const bool lk = g.M >= g.N ? g.a_kcontig : g.b_kcontig;
+                sk[{kern::skinny_groups(g.M, g.N), lk}].push_back(gi);
             } else {
                 GemmLaunch l;
                 l.gemm = gi;
@@ -784,6 +907,41 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
             l.d_probs = (kern::GemmArgs*)dmalloc(probs.size() * sizeof(kern::GemmArgs));
             l.d_tile_start = (int*)dmalloc(tstart.size() * sizeof(int));
             stage_h2d(l.d_probs, probs.data(), probs.size() * sizeof(kern::GemmArgs));
+            stage_h2d(l.d_tile_start, tstart.data(), tstart.size() * sizeof(int));
+            run.launches.push_back(l);
+            any_group = true;
+        }
+        for (auto& kv : sk) {
+            if (kv.second.size() == 1) {
+                GemmLaunch l;
+                l.gemm = kv.second[0];
+                l.flops = p.gemms[kv.second[0]].flops();
+                run.launches.push_back(l);
+                continue;
+            }
+            GemmLaunch l;
+            l.kind = GemmLaunch::SKINNY_GROUPED;
+            l.nt = kv.first.first;
+            l.ak = kv.first.second;
+            std::vector<kern::SkinnyArgs> probs;
+            std::vector<int> tstart;
+            int tiles = 0;
+            for (int gi : kv.second) {
+                const GemmStep& g = p.gemms[gi];
+                bool lk;
+                kern::SkinnyArgs a = kern::skinny_args(gemm_args(p, g), &lk);
+                a.ws = nullptr;
+                probs.push_back(a);
+                tstart.push_back(tiles);
+                tiles += kern::skinny_tiles(a.R);
+                l.flops += g.flops();
+            }
+            l.nprob = (int)probs.size();
+            l.tiles = tiles;
+            l.desc_bytes = probs.size() * sizeof(kern::SkinnyArgs);
+            l.d_desc = dmalloc(l.desc_bytes);
+            l.d_tile_start = (int*)dmalloc(tstart.size() * sizeof(int));
+            stage_h2d(l.d_desc, probs.data(), l.desc_bytes);
             stage_h2d(l.d_tile_start, tstart.data(), tstart.size() * sizeof(int));
             run.launches.push_back(l);
             any_group = true;
@@ -952,6 +1110,12 @@ void Context::launch(Plan& p, const GemmLaunch& l, const std::string& label, dou
             break;
         case GemmLaunch::DOT_BATCHED:
             kern::dot_batched((const kern::DotDesc*)l.d_desc, l.d_chunks, l.nprob, l.chunks, l.d_part, dot_acc, stream);
+            break;
+        case GemmLaunch::SKINNY_GROUPED:
+            kern::skinny_grouped((const kern::SkinnyArgs*)l.d_desc, l.d_tile_start, l.nprob, l.tiles, l.nt, l.ak, stream);
+            break;
+        case GemmLaunch::SHORT_GROUPED:
+            kern::short_grouped((const kern::ShortDesc*)l.d_desc, l.d_tile_start, l.nprob, l.tiles, l.mt, l.nt, stream);
             break;
         case GemmLaunch::FOLD_GROUPS:
             kern::fold_groups((const kern::FoldDesc*)l.d_desc, l.d_tile_start, l.ngroups, stream);

@@ -24,6 +24,9 @@
 
 namespace ccsd {
 
+// device bytes the sliced constant operands may occupy (CCSD_SPLIT_CACHE_GB, default 50)
+int64_t split_cache_budget();
+
 struct Error : std::runtime_error {
     int code;
     Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
@@ -179,11 +182,15 @@ constexpr int kScratch = -1;
 // step, or one batched launch over several steps whose outputs are disjoint (GEMMs on the
 // grouped tiled-FP64 kernel, permuted sums, block scalings).
 struct GemmLaunch {
-    enum Kind { GEMM, GEMM_GROUPED, FOLD_GROUPS, SUM, SUM_BATCHED, SCALE, SCALE_BATCHED, DOT_BATCHED, MERGED_SPLIT };
+    enum Kind { GEMM, GEMM_GROUPED, FOLD_GROUPS, SUM, SUM_BATCHED, SCALE, SCALE_BATCHED, DOT_BATCHED, MERGED_SPLIT,
+                SHORT_GROUPED, SKINNY_GROUPED };
     Kind kind = GEMM;
     int gemm = -1;                     // single GEMM: index into Plan::gemms
     int step = -1;                     // single SUM / SCALE: index into Plan::sums / scales
     bool ak = false, bk = false;       // grouped GEMM: operand contiguity
+    int mt = 0, nt = 0;                // short products: fragment shape (d_desc: ShortDesc[nprob]);
+                                       // grouped skinny: nt n-groups, ak = L contiguous along k
+                                       // (d_desc: SkinnyArgs[nprob])
     int nprob = 0, tiles = 0;
     kern::GemmArgs* d_probs = nullptr;
     int* d_tile_start = nullptr;
@@ -217,6 +224,11 @@ struct MergedProduct {
     };
     std::vector<Level> levels;
     int members = 0;
+    // constant operands (the H blocks) keep their sliced rectangles from call to call
+    // within the split cache budget; a deeper cached slicing serves fewer slices
+    bool cache_a = false, cache_b = false;
+    int64_t cache_bytes = 0;           // reserved for both at build
+    kern::SlicedOperand sA, sB;
 };
 struct GemmRun {
     int first = 0, end = 0;            // steps [first, end)
@@ -297,7 +309,8 @@ public:
     std::vector<double*> merged_retired;                   // outgrown, kept until the context goes
     void build_merged(Plan& p, GemmRun& run, int first, int end, std::vector<char>& merged,
                       const std::function<std::pair<int, int64_t>(int, int64_t)>& block_of);
-    void run_merged(Plan& p, const MergedProduct& m);
+    void run_merged(Plan& p, MergedProduct& m);
+    int64_t merged_cache_bytes = 0;                        // reserved by merged products' cached slices
     void free_merged(MergedProduct& m);
     double* splitk_ws = nullptr;                           // FP64 split-K partials
     int64_t splitk_elems = 0;

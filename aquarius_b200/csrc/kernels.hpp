@@ -1,6 +1,7 @@
 // Launch wrappers for the engine's CUDA kernels (implemented in *.cu).
 #pragma once
 #include <cstdint>
+#include <utility>
 #include <cuda_runtime.h>
 
 namespace ccsd {
@@ -38,18 +39,67 @@ struct GemmArgs {
     bool dense_out = false;
 };
 
-// Fold of dense partial products into C: C[Cm[m] + Cn[n]] += scale * part[m*N + n], the
-// problems of one output block in order (one destination per element).
+// Fold of dense partial products into C: with p = sum over z < ks of part[z*M*N + m*N + n]
+// (the partials in order), C[Cm[a][m] + Cn[b][n]] += scale * vsign[a*nvn + b] * p for every
+// variant (a, b); the problems of one group of output blocks in order.
 struct FoldDesc {
     const double* part = nullptr;
     double* C = nullptr;
-    const int64_t* Cm = nullptr;
-    const int64_t* Cn = nullptr;
-    int M = 0, N = 0;
+    const int64_t* Cm[2] = {nullptr, nullptr};
+    const int64_t* Cn[2] = {nullptr, nullptr};
+    int M = 0, N = 0, ks = 1, nvm = 1, nvn = 1;
+    double vsign[4] = {1, 1, 1, 1};
     double scale = 0;
 };
 // one CTA per group: problems [group_start[g], group_start[g + 1]) of d, in order
 void fold_groups(const FoldDesc* d, const int* group_start, int ngroups, cudaStream_t s);
+
+// Skinny FP64 product: one small extent (<= 32) against a long operand L:
+//   C[Cr_v[r] + Cs_w[s]] += sign_vw * alpha * sum_k L[Lr[r] + Lk[k]] * S[Sk[k] + Sn[s]]
+struct SkinnyArgs {
+    const double* L = nullptr;
+    const double* S = nullptr;
+    double* C = nullptr;
+    const int64_t *Lr = nullptr, *Lk = nullptr, *Sk = nullptr, *Sn = nullptr;
+    bool lk_affine = false, sk_affine = false;     // Lk / Sk as offset0 + k * step
+    int64_t lk0 = 0, lk_step = 0, sk0 = 0, sk_step = 0;
+    const int64_t* Cr[2] = {nullptr, nullptr};
+    const int64_t* Cs[2] = {nullptr, nullptr};
+    int R = 0, NS = 0, K = 0, nvr = 1, nvs = 1;
+    double vsign[4] = {1, 1, 1, 1};   // [vr * nvs + vs]
+    double alpha = 0;
+    double* ws = nullptr;
+};
+// a contraction as a skinny product (the longer of M, N as the rows of L); *lk: L is
+// contiguous along k
+SkinnyArgs skinny_args(const GemmArgs& g, bool* lk);
+// n-groups of 8 for a small extent (0: not a skinny product), and the row tiles of R rows
+int skinny_groups(int M, int N);
+int skinny_tiles(int R);
+// many skinny products of one level (disjoint outputs, no K split) in one launch
+void skinny_grouped(const SkinnyArgs* d, const int* tile_start, int nprob, int tiles, int nt, bool lk,
+                    cudaStream_t s);
+
+// Short products: both extents <= 64 with (M/8) * (N/8) <= 8 fragments and a long K
+// (F(mi) += <mn||ef> t(ef,in) per irrep block).  The CTAs of a problem split its K range
+// (kper k each) and write their M x N partial products to part[cta][m][n]; a fold adds
+// them (FoldDesc, ks = the problem's CTAs).  One launch covers every problem of one
+// fragment shape, cta_start[p] being the first CTA of problem p.
+struct ShortDesc {
+    const double* A = nullptr;
+    const double* B = nullptr;
+    const int64_t *Am = nullptr, *Ak = nullptr, *Bk = nullptr, *Bn = nullptr;
+    bool ak_affine = false, bk_affine = false;
+    int64_t ak0 = 0, ak_step = 0, bk0 = 0, bk_step = 0;
+    int M = 0, N = 0, K = 0, kper = 0;
+    double* part = nullptr;
+};
+// fragment shape (m-fragments, n-fragments) of a short product, {0, 0} if it is not one
+std::pair<int, int> short_shape(int M, int N);
+// CTAs of a short product (its K range split in kper-multiples of 128)
+int short_ctas(int K, int* kper);
+void short_grouped(const ShortDesc* d, const int* cta_start, int nprob, int total_ctas, int mt, int nt,
+                   cudaStream_t s);
 
 // K-ranges the FP64 GEMM splits a contraction into (1 = none); ws needs ksplit*M*N doubles
 int fp64_ksplit(int M, int N, int K, bool skinny_ok = true);

@@ -268,16 +268,20 @@ __global__ void __launch_bounds__(THREADS, 1)
     fp64_tile<AK, BKc>(sg, (local / tn) * BM, (local % tn) * BN, 0, 1, smem_raw);
 }
 
-// shared-output groups: each CTA folds the partial products of one output block, its
-// problems one after another (fixed order; one destination per element)
+// shared-output groups: each CTA folds the partial products of one group of output blocks,
+// its problems one after another and each problem's partials in order (fixed order)
 __global__ void fold_groups_kernel(const FoldDesc* __restrict__ d, const int* __restrict__ gstart) {
     const int g = blockIdx.x;
     for (int p = gstart[g]; p < gstart[g + 1]; p++) {
         const FoldDesc f = d[p];
         const int64_t mn = (int64_t)f.M * f.N;
         for (int64_t l = threadIdx.x; l < mn; l += blockDim.x) {
+            double s = 0.0;
+            for (int z = 0; z < f.ks; z++) s += f.part[z * mn + l];
             const int m = (int)(l / f.N), n = (int)(l % f.N);
-            f.C[f.Cm[m] + f.Cn[n]] += f.scale * f.part[l];
+            const double v = f.scale * s;
+            for (int a = 0; a < f.nvm; a++)
+                for (int b = 0; b < f.nvn; b++) f.C[f.Cm[a][m] + f.Cn[b][n]] += f.vsign[a * f.nvn + b] * v;
         }
         __syncthreads();
     }
@@ -309,21 +313,6 @@ __global__ void splitk_fold_kernel(GemmArgs g, int ks) {
 // slots go to the loads and not to one FMA per element pair.  A short long-extent splits
 // K over gridDim.z into ws[z][r][s], folded in a fixed order.
 // ---------------------------------------------------------------------------
-struct SkinnyArgs {
-    const double* L = nullptr;
-    const double* S = nullptr;
-    double* C = nullptr;
-    const int64_t *Lr = nullptr, *Lk = nullptr, *Sk = nullptr, *Sn = nullptr;
-    bool lk_affine = false, sk_affine = false;     // Lk / Sk as offset0 + k * step
-    int64_t lk0 = 0, lk_step = 0, sk0 = 0, sk_step = 0;
-    const int64_t* Cr[2] = {nullptr, nullptr};
-    const int64_t* Cs[2] = {nullptr, nullptr};
-    int R = 0, NS = 0, K = 0, nvr = 1, nvs = 1;
-    double vsign[4] = {1, 1, 1, 1};   // [vr * nvs + vs]
-    double alpha = 0;
-    double* ws = nullptr;
-};
-
 constexpr int SK_THREADS = 256, SK_STAGES = 4, SK_TM = 256, SK_KC = 8;
 
 template <int NT, bool LK>
@@ -346,12 +335,10 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem));
 }
 
+// one CTA: rows [rtile * SK_TM, +SK_TM) of the long operand over K range z of nz
 template <int NT, bool LK>
-// two CTAs per SM (about 80 KB of shared memory each): 16 warps keep four stages of the
-// long operand in flight per CTA
-__global__ void __launch_bounds__(SK_THREADS, 2) skinny_kernel(SkinnyArgs g) {
+__device__ __forceinline__ void skinny_body(const SkinnyArgs& g, int rtile, int z, int nz, unsigned char* smem_raw) {
     using Sh = SkinnyShape<NT, LK>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
     double* As = reinterpret_cast<double*>(smem_raw);
     double* Bs = As + SK_STAGES * Sh::A_ELEMS;
     int64_t* sLr = reinterpret_cast<int64_t*>(Bs + SK_STAGES * Sh::B_ELEMS);
@@ -360,13 +347,13 @@ __global__ void __launch_bounds__(SK_THREADS, 2) skinny_kernel(SkinnyArgs g) {
     int64_t* sSk = sLk + SK_STAGES * SK_KC;      // [stage][k]: offsets of S
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int r0 = blockIdx.x * SK_TM;
+    const int r0 = rtile * SK_TM;
     for (int i = tid; i < SK_TM; i += SK_THREADS) sLr[i] = (r0 + i < g.R) ? g.Lr[r0 + i] : -1;
     for (int i = tid; i < 8 * NT; i += SK_THREADS) sSn[i] = (i < g.NS) ? g.Sn[i] : -1;
 
     const int kchunks_all = (g.K + SK_KC - 1) / SK_KC;
-    const int per_split = (kchunks_all + gridDim.z - 1) / gridDim.z;
-    const int kc0 = blockIdx.z * per_split;
+    const int per_split = (kchunks_all + nz - 1) / nz;
+    const int kc0 = z * per_split;
     const int kchunks = max(0, min(kchunks_all, kc0 + per_split) - kc0);
 
     // the k offsets of chunk c (relative to this CTA's range) into table slot c % stages
@@ -471,8 +458,8 @@ __global__ void __launch_bounds__(SK_THREADS, 2) skinny_kernel(SkinnyArgs g) {
     cp_wait<0>();
 
     // lane holds rows wr + 8i + fr, columns 8j + 2 fk + {0, 1}
-    if (gridDim.z > 1) {
-        double* wz = g.ws + (int64_t)blockIdx.z * g.R * g.NS;
+    if (nz > 1) {
+        double* wz = g.ws + (int64_t)z * g.R * g.NS;
 #pragma unroll
         for (int i = 0; i < Sh::MT; i++) {
             const int r = r0 + wr + 8 * i + fr;
@@ -534,6 +521,37 @@ __global__ void __launch_bounds__(SK_THREADS, 2) skinny_kernel(SkinnyArgs g) {
     }
 }
 
+// two CTAs per SM (about 80 KB of shared memory each): 16 warps keep four stages of the
+// long operand in flight per CTA
+template <int NT, bool LK>
+__global__ void __launch_bounds__(SK_THREADS, 2) skinny_kernel(SkinnyArgs g) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    skinny_body<NT, LK>(g, blockIdx.x, blockIdx.z, gridDim.z, smem_raw);
+}
+
+// Grouped launch: the row tiles of many skinny products of one level (disjoint outputs, no
+// K split), tile_start[p] being the first tile of problem p
+template <int NT, bool LK>
+__global__ void __launch_bounds__(SK_THREADS, 2)
+    skinny_grouped_kernel(const SkinnyArgs* __restrict__ probs, const int* __restrict__ tile_start, int nprob) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ SkinnyArgs sg;
+    __shared__ int sp;
+    const int t = blockIdx.x;
+    if (threadIdx.x == 0) {
+        int lo = 0, hi = nprob - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (tile_start[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        sp = lo;
+        sg = probs[lo];
+    }
+    __syncthreads();
+    skinny_body<NT, LK>(sg, t - tile_start[sp], 0, 1, smem_raw);
+}
+
 __global__ void skinny_fold_kernel(SkinnyArgs g, int ks) {
     const int64_t rs = (int64_t)g.R * g.NS;
     for (int64_t l = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; l < rs; l += (int64_t)gridDim.x * blockDim.x) {
@@ -546,12 +564,118 @@ __global__ void skinny_fold_kernel(SkinnyArgs g, int ks) {
     }
 }
 
+// ---------------------------------------------------------------------------
+// Short products: M, N <= 64, long K.  Each warp of a CTA walks its own part of the CTA's
+// K range, 16 k per step (8 for the widest shapes), loading the m8n8k4 fragments straight
+// from global memory (a lane reads A[m = lane/4 + 8i][k] and B[k][n = lane/4 + 8j] for
+// k = 4u + lane%4: 32-byte runs along k, or 64-byte runs along m / n, both whole
+// sectors); the k offsets of the next step are fetched while the current step's data
+// loads are in flight.  The eight warps' fragments are added in warp order in shared
+// memory and the CTA writes one partial M x N product.
+// ---------------------------------------------------------------------------
+constexpr int SH_THREADS = 256;
+constexpr int SH_KGRAN = 16 * (SH_THREADS / 32);   // kper is a multiple of this (128)
+
+template <int MT, int NT>
+__global__ void __launch_bounds__(SH_THREADS, 2)
+    short_grouped_kernel(const ShortDesc* __restrict__ descs, const int* __restrict__ cta_start, int nprob) {
+    // steps of 16 k (8 for the widest shapes, whose loads of a step would not fit the registers)
+    constexpr int SH_U = MT + NT <= 6 ? 4 : 2, SH_KSTEP = 4 * SH_U;
+    __shared__ ShortDesc sd;
+    __shared__ int sp;
+    __shared__ double red[SH_THREADS / 32][MT * 8 * NT * 8];
+    const int t = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        int lo = 0, hi = nprob - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (cta_start[mid] <= t) lo = mid;
+            else hi = mid - 1;
+        }
+        sp = lo;
+        sd = descs[lo];
+    }
+    __syncthreads();
+    const ShortDesc& g = sd;
+    const int local = t - cta_start[sp];
+    const int fr = lane >> 2, fk = lane & 3;
+    int64_t am[MT], bn[NT];
+#pragma unroll
+    for (int i = 0; i < MT; i++) am[i] = (8 * i + fr < g.M) ? __ldg(g.Am + 8 * i + fr) : -1;
+#pragma unroll
+    for (int j = 0; j < NT; j++) bn[j] = (8 * j + fr < g.N) ? __ldg(g.Bn + 8 * j + fr) : -1;
+
+    const int kw = g.kper / (SH_THREADS / 32);               // k per warp (a multiple of 16)
+    const int kb = local * g.kper + warp * kw;
+    const int ke = min(g.K, kb + kw);
+    double acc[MT][NT][2];
+#pragma unroll
+    for (int i = 0; i < MT; i++)
+#pragma unroll
+        for (int j = 0; j < NT; j++) acc[i][j][0] = acc[i][j][1] = 0.0;
+
+    auto offsets = [&](int k0, int64_t* ak, int64_t* bk) {
+#pragma unroll
+        for (int u = 0; u < SH_U; u++) {
+            const int k = k0 + 4 * u + fk;
+            const bool ok = k < ke;
+            ak[u] = !ok ? -1 : (g.ak_affine ? g.ak0 + g.ak_step * k : __ldg(g.Ak + k));
+            bk[u] = !ok ? -1 : (g.bk_affine ? g.bk0 + g.bk_step * k : __ldg(g.Bk + k));
+        }
+    };
+    int64_t ak[SH_U], bk[SH_U];
+    if (kb < ke) offsets(kb, ak, bk);
+    for (int k0 = kb; k0 < ke; k0 += SH_KSTEP) {
+        double a[SH_U][MT], b[SH_U][NT];
+#pragma unroll
+        for (int u = 0; u < SH_U; u++) {
+#pragma unroll
+            for (int i = 0; i < MT; i++) a[u][i] = (ak[u] >= 0 && am[i] >= 0) ? __ldg(g.A + am[i] + ak[u]) : 0.0;
+#pragma unroll
+            for (int j = 0; j < NT; j++) b[u][j] = (bk[u] >= 0 && bn[j] >= 0) ? __ldg(g.B + bk[u] + bn[j]) : 0.0;
+        }
+        if (k0 + SH_KSTEP < ke) offsets(k0 + SH_KSTEP, ak, bk);
+#pragma unroll
+        for (int u = 0; u < SH_U; u++)
+#pragma unroll
+            for (int i = 0; i < MT; i++)
+#pragma unroll
+                for (int j = 0; j < NT; j++) dmma(acc[i][j][0], acc[i][j][1], a[u][i], b[u][j]);
+    }
+    // lane holds rows 8i + fr, columns 8j + 2 fk + {0, 1}
+    constexpr int LDR = NT * 8;
+#pragma unroll
+    for (int i = 0; i < MT; i++)
+#pragma unroll
+        for (int j = 0; j < NT; j++)
+#pragma unroll
+            for (int h = 0; h < 2; h++) red[warp][(8 * i + fr) * LDR + 8 * j + 2 * fk + h] = acc[i][j][h];
+    __syncthreads();
+    double* out = g.part + (int64_t)local * g.M * g.N;
+    for (int e = tid; e < g.M * g.N; e += SH_THREADS) {
+        const int m = e / g.N, n = e % g.N;
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < SH_THREADS / 32; w++) s += red[w][m * LDR + n];
+        out[e] = s;
+    }
+}
+
+template <int MT, int NT>
+void launch_short_t(const ShortDesc* d, const int* cta_start, int nprob, int total, cudaStream_t s) {
+    short_grouped_kernel<MT, NT><<<total, SH_THREADS, 0, s>>>(d, cta_start, nprob);
+}
+
+}  // namespace
+
 // n-groups of 8 for a small extent (0: not a skinny product)
 int skinny_groups(int M, int N) {
     const int small = std::min(M, N);
     if (small > 32) return 0;
     return small <= 8 ? 1 : (small <= 16 ? 2 : 4);
 }
+
+namespace {
 
 // K-ranges for the skinny kernel: about two waves of CTAs, at least 16 k-chunks each
 int skinny_ksplit(int R, int K, int nt) {
@@ -574,7 +698,39 @@ void launch_skinny_t(const SkinnyArgs& a, int ks, cudaStream_t s) {
     skinny_kernel<NT, LK><<<grid, SK_THREADS, Sh::bytes, s>>>(a);
 }
 
+template <int NT, bool LK>
+void launch_skinny_grouped_t(const SkinnyArgs* d, const int* tile_start, int nprob, int tiles, cudaStream_t s) {
+    using Sh = SkinnyShape<NT, LK>;
+    set_smem_once((const void*)skinny_grouped_kernel<NT, LK>, (int)Sh::bytes);
+    skinny_grouped_kernel<NT, LK><<<tiles, SK_THREADS, Sh::bytes, s>>>(d, tile_start, nprob);
+}
+
 void launch_skinny(const GemmArgs& g, int nt, cudaStream_t s) {
+    bool lk;
+    SkinnyArgs a = skinny_args(g, &lk);
+    int ks = skinny_ksplit(a.R, a.K, nt);
+    if (!g.ws || (int64_t)ks * a.R * a.NS > g.ws_elems) ks = 1;
+    a.ws = g.ws;
+    switch (nt * 2 + (lk ? 1 : 0)) {
+        case 2: launch_skinny_t<1, false>(a, ks, s); break;
+        case 3: launch_skinny_t<1, true>(a, ks, s); break;
+        case 4: launch_skinny_t<2, false>(a, ks, s); break;
+        case 5: launch_skinny_t<2, true>(a, ks, s); break;
+        case 8: launch_skinny_t<4, false>(a, ks, s); break;
+        default: launch_skinny_t<4, true>(a, ks, s); break;
+    }
+    COUNT_LAUNCH();
+    if (ks > 1) {
+        const int64_t rs = (int64_t)a.R * a.NS;
+        const int nb = (int)std::min<int64_t>((rs + 255) / 256, 148 * 16);
+        skinny_fold_kernel<<<nb, 256, 0, s>>>(a, ks);
+        COUNT_LAUNCH();
+    }
+}
+
+}  // namespace
+
+SkinnyArgs skinny_args(const GemmArgs& g, bool* lk_out) {
     SkinnyArgs a;
     const bool long_a = g.M >= g.N;
     bool lk;
@@ -599,25 +755,26 @@ void launch_skinny(const GemmArgs& g, int nt, cudaStream_t s) {
         a.lk_affine = g.bk_affine; a.lk0 = g.bk0; a.lk_step = g.bk_step;
         a.sk_affine = g.ak_affine; a.sk0 = g.ak0; a.sk_step = g.ak_step;
     }
-    int ks = skinny_ksplit(a.R, a.K, nt);
-    if (!g.ws || (int64_t)ks * a.R * a.NS > g.ws_elems) ks = 1;
-    a.ws = g.ws;
+    *lk_out = lk;
+    return a;
+}
+
+int skinny_tiles(int R) { return (R + SK_TM - 1) / SK_TM; }
+
+void skinny_grouped(const SkinnyArgs* d, const int* tile_start, int nprob, int tiles, int nt, bool lk, cudaStream_t s) {
+    if (nprob <= 0 || tiles <= 0) return;
     switch (nt * 2 + (lk ? 1 : 0)) {
-        case 2: launch_skinny_t<1, false>(a, ks, s); break;
-        case 3: launch_skinny_t<1, true>(a, ks, s); break;
-        case 4: launch_skinny_t<2, false>(a, ks, s); break;
-        case 5: launch_skinny_t<2, true>(a, ks, s); break;
-        case 8: launch_skinny_t<4, false>(a, ks, s); break;
-        default: launch_skinny_t<4, true>(a, ks, s); break;
+        case 2: launch_skinny_grouped_t<1, false>(d, tile_start, nprob, tiles, s); break;
+        case 3: launch_skinny_grouped_t<1, true>(d, tile_start, nprob, tiles, s); break;
+        case 4: launch_skinny_grouped_t<2, false>(d, tile_start, nprob, tiles, s); break;
+        case 5: launch_skinny_grouped_t<2, true>(d, tile_start, nprob, tiles, s); break;
+        case 8: launch_skinny_grouped_t<4, false>(d, tile_start, nprob, tiles, s); break;
+        default: launch_skinny_grouped_t<4, true>(d, tile_start, nprob, tiles, s); break;
     }
     COUNT_LAUNCH();
-    if (ks > 1) {
-        const int64_t rs = (int64_t)a.R * a.NS;
-        const int nb = (int)std::min<int64_t>((rs + 255) / 256, 148 * 16);
-        skinny_fold_kernel<<<nb, 256, 0, s>>>(a, ks);
-        COUNT_LAUNCH();
-    }
 }
+
+namespace {
 
 template <bool AK, bool BKc>
 void launch_fp64(const GemmArgs& g, cudaStream_t s) {
@@ -695,6 +852,43 @@ void gemm_fp64_grouped(const GemmArgs* probs, const int* tile_start, int nprob, 
     } else {
         if (b_kcontig) launch_grouped_t<false, true>(probs, tile_start, nprob, total_tiles, s);
         else launch_grouped_t<false, false>(probs, tile_start, nprob, total_tiles, s);
+    }
+    COUNT_LAUNCH();
+}
+
+std::pair<int, int> short_shape(int M, int N) {
+    if (M <= 0 || N <= 0 || M > 64 || N > 64) return {0, 0};
+    auto frag = [](int x) { return x <= 8 ? 1 : (x <= 16 ? 2 : (x <= 32 ? 4 : 8)); };
+    const int mt = frag(M), nt = frag(N);
+    if (mt * nt > 8) return {0, 0};
+    return {mt, nt};
+}
+
+int short_ctas(int K, int* kper) {
+    // about 2048 k per CTA (eight warps, 16 steps of 16 k each), at most 512 CTAs
+    int ctas = std::max(1, std::min(512, (K + 2047) / 2048));
+    int per = (K + ctas - 1) / ctas;
+    per = (per + SH_KGRAN - 1) / SH_KGRAN * SH_KGRAN;
+    ctas = (K + per - 1) / per;
+    *kper = per;
+    return ctas;
+}
+
+void short_grouped(const ShortDesc* d, const int* cta_start, int nprob, int total_ctas, int mt, int nt,
+                   cudaStream_t s) {
+    if (nprob <= 0 || total_ctas <= 0) return;
+    switch (mt * 16 + nt) {
+        case 0x11: launch_short_t<1, 1>(d, cta_start, nprob, total_ctas, s); break;
+        case 0x12: launch_short_t<1, 2>(d, cta_start, nprob, total_ctas, s); break;
+        case 0x14: launch_short_t<1, 4>(d, cta_start, nprob, total_ctas, s); break;
+        case 0x18: launch_short_t<1, 8>(d, cta_start, nprob, total_ctas, s); break;
+        case 0x21: launch_short_t<2, 1>(d, cta_start, nprob, total_ctas, s); break;
+        case 0x22: launch_short_t<2, 2>(d, cta_start, nprob, total_ctas, s); break;
+        case 0x24: launch_short_t<2, 4>(d, cta_start, nprob, total_ctas, s); break;
+        case 0x41: launch_short_t<4, 1>(d, cta_start, nprob, total_ctas, s); break;
+        case 0x42: launch_short_t<4, 2>(d, cta_start, nprob, total_ctas, s); break;
+        case 0x81: launch_short_t<8, 1>(d, cta_start, nprob, total_ctas, s); break;
+        default: throw std::runtime_error("short product: unsupported fragment shape");
     }
     COUNT_LAUNCH();
 }

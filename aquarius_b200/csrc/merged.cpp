@@ -17,6 +17,7 @@
 #include <cstdlib>
 #include <map>
 #include <numeric>
+#include <set>
 #include <tuple>
 
 #include "engine.hpp"
@@ -43,6 +44,13 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
         if (g.mkey.empty() || routes_split(g) || std::min(g.M, g.N) <= 8 || g.K <= 0) continue;
         cands.push_back({i, id(rid, g.mkey), id(cid, g.nkey), id(kid, g.kkey)});
     }
+    if (std::getenv("CCSD_MERGE_REPORT")) {
+        double all = 0, in = 0;
+        for (int i = first; i < end; i++) all += p.gemms[p.steps[i].idx].flops();
+        for (auto& c : cands) in += p.gemms[p.steps[c.i].idx].flops();
+        std::fprintf(stderr, "[merge-run] %-48s %5d products %.3e flop, candidates %zu with %.3e flop\n",
+                     p.gemms[p.steps[first].idx].label.c_str(), end - first, all, cands.size(), in);
+    }
     if (cands.size() < 2) return;
     const int NR = (int)rid.size(), NK = (int)kid.size(), NC = (int)cid.size();
     std::vector<int> par(NR + NK + NC);
@@ -64,9 +72,53 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
     for (size_t j = 0; j < cands.size(); j++) comp[find(cands[j].r)].push_back((int)j);
     auto G = [&](int j) -> const GemmStep& { return p.gemms[p.steps[cands[j].i].idx]; };
 
+    const bool report = std::getenv("CCSD_MERGE_REPORT") != nullptr;
+    auto reject = [&](const std::vector<int>& js, const char* why, size_t nr, size_t nc, size_t nk) {
+        if (!report) return;
+        double fl = 0;
+        for (int j : js) fl += G(j).flops();
+        std::fprintf(stderr, "[merge-skip] %-48s %5zu products %.3e flop  R=%zu C=%zu K=%zu  %s\n",
+                     G(js[0]).label.c_str(), js.size(), fl, nr, nc, nk, why);
+    };
+    // the grids to merge: a component that is a full grid, else the row classes of it (rows
+    // that meet the same column blocks over the same k blocks) that are.  A ring statement's
+    // component joins rows of several spin sectors and antisymmetriser terms through shared
+    // k and column blocks; each sector alone is a full grid.
+    std::vector<std::vector<int>> grids;
     for (auto& kv : comp) {
         const std::vector<int>& js = kv.second;
         if (js.size() < 2) continue;
+        std::set<int> Rs, Cs, Ks;
+        std::set<std::tuple<int, int, int>> cells;
+        for (int j : js) {
+            Rs.insert(cands[j].r);
+            Cs.insert(cands[j].c);
+            Ks.insert(cands[j].k);
+            cells.insert(std::make_tuple(cands[j].r, cands[j].c, cands[j].k));
+        }
+        if (cells.size() == js.size() && cells.size() == Rs.size() * Cs.size() * Ks.size()) {
+            grids.push_back(js);
+            continue;
+        }
+        std::map<int, std::pair<std::set<int>, std::set<int>>> sig;   // row -> (column blocks, k blocks)
+        std::map<int, std::vector<int>> of_row;
+        for (int j : js) {
+            sig[cands[j].r].first.insert(cands[j].c);
+            sig[cands[j].r].second.insert(cands[j].k);
+            of_row[cands[j].r].push_back(j);
+        }
+        std::map<std::pair<std::set<int>, std::set<int>>, std::vector<int>> cls;
+        for (auto& rs : sig) cls[rs.second].push_back(rs.first);
+        for (auto& cl : cls) {
+            std::vector<int> sub;
+            for (int r : cl.second) sub.insert(sub.end(), of_row[r].begin(), of_row[r].end());
+            if (sub.size() < 2) continue;
+            std::sort(sub.begin(), sub.end());   // plan order
+            if (sub.size() == cl.second.size() * cl.first.first.size() * cl.first.second.size()) grids.push_back(sub);
+            else reject(sub, "row class not a full grid", cl.second.size(), cl.first.first.size(), cl.first.second.size());
+        }
+    }
+    for (const std::vector<int>& js : grids) {
         std::vector<int> R, C, Kb;
         std::map<std::tuple<int, int, int>, int> at;
         std::map<int, int> Mr, Nc, Kl;
@@ -86,7 +138,10 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
             ok &= Mr[c.r] == g.M && Nc[c.c] == g.N && Kl[c.k] == g.K;
         }
         // a full grid only: every row block with every column block over every k block
-        if (!ok || at.size() != R.size() * C.size() * Kb.size()) continue;
+        if (!ok || at.size() != R.size() * C.size() * Kb.size()) {
+            reject(js, !ok ? "repeated or mismatched extents" : "not a full grid", R.size(), C.size(), Kb.size());
+            continue;
+        }
         auto J = [&](int r, int c, int k) { return at.at(std::make_tuple(r, c, k)); };
         // the rectangles of A depend on (rows, k) only, of B on (k, columns), of C on (rows,
         // columns): the products that share them must agree on their tables
@@ -98,6 +153,10 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
                     ok &= b.tA == a.tA && b.hAm == a.hAm && b.hAk == a.hAk && b.a_kcontig == a.a_kcontig;
                 }
             }
+        if (!ok) {
+            reject(js, "A tables differ", R.size(), C.size(), Kb.size());
+            continue;
+        }
         for (int k : Kb)
             for (int c : C) {
                 const GemmStep& a = G(J(R[0], c, k));
@@ -106,6 +165,10 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
                     ok &= b.tB == a.tB && b.hBk == a.hBk && b.hBn == a.hBn && b.b_kcontig == a.b_kcontig;
                 }
             }
+        if (!ok) {
+            reject(js, "B tables differ", R.size(), C.size(), Kb.size());
+            continue;
+        }
         // coefficients: alpha(r, c, k) = alpha(r, c, k0) * ratio(k), the ratio (spin weights and
         // reordering signs of the k block) folded into the k block's rectangles of B
         std::map<int, double> ratio;
@@ -121,7 +184,10 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
                     for (int v = 0; v < 4 && ok; v++) ok &= b.vsign[v] == a.vsign[v];
                 }
             }
-        if (!ok) continue;
+        if (!ok) {
+            reject(js, "coefficients or C tables differ", R.size(), C.size(), Kb.size());
+            continue;
+        }
         int64_t M = 0, N = 0, K = 0;
         std::map<int, int> roff, coff, koff;
         for (int r : R) roff[r] = (int)M, M += Mr[r];
@@ -129,9 +195,11 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
         for (int k : Kb) koff[k] = (int)K, K += Kl[k];
         // a class worth one tensor-core GEMM (its slicing reads the operands once; below this
         // the grouped FP64 launch is cheaper)
-        if (M < 64 || N < 32 || K < 128 || 2.0 * M * N * K < 2e7 || M > (1 << 28) || N > (1 << 28) || K > (1 << 28))
+        if (M < 64 || N < 32 || K < 128 || 2.0 * M * N * K < 2e7 || M > (1 << 28) || N > (1 << 28) || K > (1 << 28)) {
+            reject(js, "below the size bar", R.size(), C.size(), Kb.size());
             continue;
-        if (std::getenv("CCSD_MERGE_REPORT"))
+        }
+        if (report)
             std::fprintf(stderr, "[merged] %-48s %5zu products  M=%-6lld N=%-6lld K=%-6lld\n", G(js[0]).label.c_str(),
                          js.size(), (long long)M, (long long)N, (long long)K);
 
@@ -219,6 +287,31 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
                 if ((int)lv.size() <= L) lv.resize(L + 1);
                 lv[L].push_back(s);
             }
+        // cached slices of constant operands, within the split cache budget
+        {
+            bool constA = true, constB = true;
+            for (int r : R)
+                for (int k : Kb) constA &= G(J(r, C[0], k)).tA != kScratch && is_constant(G(J(r, C[0], k)).tA);
+            for (int c : C)
+                for (int k : Kb) constB &= G(J(R[0], c, k)).tB != kScratch && is_constant(G(J(R[0], c, k)).tB);
+            int64_t used = merged_cache_bytes;
+            for (auto& kv : split_cache) used += kv.second.bytes;
+            const int deepest = 5;   // any slice count a refinement reaches
+            const int64_t ba = kern::split_slice_bytes((int)M, (int)K, deepest, kern::SLICE_INT8) +
+                               3 * (int64_t)kern::split_rows_pad((int)M) * 8;
+            const int64_t bb = kern::split_slice_bytes((int)N, (int)K, deepest, kern::SLICE_INT8) +
+                               3 * (int64_t)kern::split_rows_pad((int)N) * 8;
+            if (constA && used + ba <= split_cache_budget()) {
+                mp->cache_a = true;
+                used += ba;
+                mp->cache_bytes += ba;
+            }
+            if (constB && used + bb <= split_cache_budget()) {
+                mp->cache_b = true;
+                mp->cache_bytes += bb;
+            }
+            merged_cache_bytes += mp->cache_bytes;
+        }
         mp->nA = (int)A.size();
         mp->nB = (int)B.size();
         mp->dA = (kern::RectDesc*)dmalloc(A.size() * sizeof(kern::RectDesc));
@@ -267,19 +360,39 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
     }
 }
 
-void Context::run_merged(Plan& p, const MergedProduct& m) {
+void Context::run_merged(Plan& p, MergedProduct& m) {
     const int ns = step_slices(p.gemms[m.first_gemm]), kind = slice_kind();
     split_launches++;
-    ensure_ws(split_ws.a, m.M, m.K);
-    ensure_ws(split_ws.b, m.N, m.K);
-    kern::SlicedOperand va = split_ws.a, vb = split_ws.b;
-    va.rows = kern::split_rows_pad(m.M);
-    vb.rows = kern::split_rows_pad(m.N);
-    va.kpad = vb.kpad = kern::split_k_pad(m.K, kind);
-    va.nslices = vb.nslices = ns;
-    va.kind = vb.kind = kind;
-    kern::rect_slice(m.dA, m.dA_ts, m.nA, m.tilesA, ns, va, stream);
-    kern::rect_slice(m.dB, m.dB_ts, m.nB, m.tilesB, ns, vb, stream);
+    auto operand = [&](bool is_a) {
+        const int rows = is_a ? m.M : m.N;
+        const kern::RectDesc* d = is_a ? m.dA : m.dB;
+        const int64_t* ts = is_a ? m.dA_ts : m.dB_ts;
+        const int n = is_a ? m.nA : m.nB;
+        const int64_t tiles = is_a ? m.tilesA : m.tilesB;
+        if (is_a ? m.cache_a : m.cache_b) {
+            kern::SlicedOperand& c = is_a ? m.sA : m.sB;
+            if (!c.data || c.kind != kind || c.nslices < ns) {
+                if (c.data) free_sliced(c);
+                c = alloc_sliced(rows, m.K, ns, kind);
+                kern::rect_slice(d, ts, n, tiles, ns, c, stream);
+            }
+            // the first ns slices of a deeper slicing are the ns-slice slicing
+            kern::SlicedOperand v = c;
+            v.nslices = ns;
+            return v;
+        }
+        kern::SlicedOperand& w = is_a ? split_ws.a : split_ws.b;
+        ensure_ws(w, rows, m.K);
+        kern::SlicedOperand v = w;
+        v.rows = kern::split_rows_pad(rows);
+        v.kpad = kern::split_k_pad(m.K, kind);
+        v.nslices = ns;
+        v.kind = kind;
+        kern::rect_slice(d, ts, n, tiles, ns, v, stream);
+        return v;
+    };
+    const kern::SlicedOperand va = operand(true);
+    const kern::SlicedOperand vb = operand(false);
     kern::GemmArgs a;
     a.ws = merged_ws;
     a.ws_elems = merged_ws_elems;
@@ -292,6 +405,11 @@ void Context::run_merged(Plan& p, const MergedProduct& m) {
 }
 
 void Context::free_merged(MergedProduct& m) {
+    if (m.sA.data) free_sliced(m.sA);
+    if (m.sB.data) free_sliced(m.sB);
+    merged_cache_bytes -= m.cache_bytes;
+    m.cache_bytes = 0;
+    m.cache_a = m.cache_b = false;
     dfree(m.dA, m.nA * sizeof(kern::RectDesc));
     dfree(m.dB, m.nB * sizeof(kern::RectDesc));
     dfree(m.dA_ts, m.nA * sizeof(int64_t));

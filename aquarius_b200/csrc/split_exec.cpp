@@ -39,14 +39,14 @@ int64_t slice_bytes(int rows, int K, int ns, int kind) {
 constexpr int64_t kWsBytesPerElem = 8;
 int64_t ws_k_pad(int K) { return kern::split_k_pad(K, kern::SLICE_INT8); }   // the wider padding
 
+}  // namespace
+
 // device bytes the sliced constant operands may occupy (CCSD_SPLIT_CACHE_GB, default 50)
-int64_t cache_budget() {
+int64_t split_cache_budget() {
     const char* e = std::getenv("CCSD_SPLIT_CACHE_GB");
     double gb = e ? std::atof(e) : 50.0;
     return (int64_t)(gb * 1e9);
 }
-
-}  // namespace
 
 bool Context::routes_split(const GemmStep& g) const {
     return split_precision() && kern::split_supported() && split_eligible(g);
@@ -96,9 +96,9 @@ void Context::reserve_split(Plan& p) {
     for (auto& g : p.gemms)
         if (split_eligible(g)) order.push_back(&g);
     std::stable_sort(order.begin(), order.end(), [](GemmStep* a, GemmStep* b) { return a->flops() > b->flops(); });
-    int64_t base = 0;
+    int64_t base = merged_cache_bytes;
     for (auto& kv : split_cache) base += kv.second.bytes;
-    const int64_t budget = cache_budget();
+    const int64_t budget = split_cache_budget();
     auto choose = [&](int ns) {
         int64_t used = base;
         for (GemmStep* g : order) {
@@ -197,7 +197,7 @@ void Context::run_split_gemm(GemmStep& g, kern::GemmArgs& a) {
             key = -1;
             int64_t used = 0;
             for (auto& kv : split_cache) used += kv.second.bytes;
-            if (used + slice_bytes(rows, g.K, ns, kind) > cache_budget()) cached = false;
+            if (used + slice_bytes(rows, g.K, ns, kind) > split_cache_budget()) cached = false;
         }
         if (cached) {
             if (key < 0) {
