@@ -594,6 +594,10 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
         // of every tile (F(ae) += <am||ef> t(fm) at o=16 v=128: 2.3 ms grouped)
         if (!fp64_tiled_only && std::min(g.M, g.N) <= 32 && (int64_t)std::max(g.M, g.N) * g.K >= (int64_t)1 << 22)
             return false;
+        // and so is a skinny product with a long side of a tile or more: the grouped skinny
+        // launch streams it (the tiles would stay 1/8 to 1/2 empty and walk it at a fraction
+        // of the rate: W~(am,ei) += <am||ef> t(fi) at o=48 v=336 D2h took 16 ms on tiles)
+        if (!fp64_tiled_only && std::min(g.M, g.N) <= 32 && std::max(g.M, g.N) >= 128) return false;
         // a grouped tile walks the whole K range: long-K products keep their split-K launch
         if (g.flops() < 4e8 && g.K <= 4096) return true;
         return kern::fp64_ksplit(g.M, g.N, g.K, !fp64_tiled_only) == 1 && kern::fp64_ksplit(g.M, g.N, g.K, false) == 1;
@@ -640,7 +644,7 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
         maxlvl = std::max(maxlvl, lvl);
         if (groupable(g)) ngroupable++;
         if (shortable(g)) nshort++;
-        if (skinny_groupable(g)) nskinny++;
+        if (!fp64_tiled_only && !routes_split(g) && kern::skinny_groups(g.M, g.N) > 0) nskinny++;
     }
     GemmRun run;
     run.first = first;
@@ -695,6 +699,25 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
             sctas[i - first] = kern::short_ctas(g.K, &skper[i - first]);
             part += (int64_t)sctas[i - first] * g.M * g.N;
         }
+        // skinny products that split K write their K ranges' partials for the fold too (one
+        // grouped launch instead of a skinny launch and a fold launch per product), within a
+        // partial buffer of 64M elements
+        int64_t skpart = 0;
+        for (int i = first; i < end; i++) {
+            const GemmStep& g = p.gemms[p.steps[i].idx];
+            if (in_fold[i - first] || merged[i - first] || fp64_tiled_only || routes_split(g) ||
+                kern::skinny_groups(g.M, g.N) == 0 || keys_of[i - first].empty())
+                continue;
+            // (small outputs only: one CTA folds a group, so a large partial stays with the
+            // product's own launch and its parallel fold)
+            const int ks = kern::fp64_ksplit(g.M, g.N, g.K, true);
+            const int64_t mn = (int64_t)g.M * g.N;
+            if (ks < 2 || mn > 16384 || ks * mn > 262144 || skpart + ks * mn > (64ll << 20)) continue;
+            in_fold[i - first] = 3;
+            sctas[i - first] = ks;
+            skpart += (int64_t)ks * g.M * g.N;
+        }
+        part += skpart;
         if (std::any_of(in_fold.begin(), in_fold.end(), [](char c) { return c != 0; })) {
             double* d_part = (double*)dmalloc(std::max<int64_t>(part, 1) * sizeof(double));
             bool owner = true;   // the partial buffer is owned by the first launch
@@ -713,6 +736,10 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
             std::map<std::pair<int, int>, std::vector<int>> sstart;
             std::map<std::pair<int, int>, int> sctas_total;
             std::map<std::pair<int, int>, double> sfl;
+            std::map<std::pair<int, bool>, std::vector<kern::SkinnyArgs>> kprobs;
+            std::map<std::pair<int, bool>, std::vector<int>> kstart;
+            std::map<std::pair<int, bool>, int> ktiles;
+            std::map<std::pair<int, bool>, double> kfl;
             std::vector<kern::FoldDesc> fdesc(end - first);
             for (int i = first; i < end; i++) {
                 if (!in_fold[i - first]) continue;
@@ -741,6 +768,30 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
                     tstart[c].push_back(tiles[c]);
                     tiles[c] += kern::fp64_tiles(g.M, g.N);
                     fl[c] += g.flops();
+                } else if (in_fold[i - first] == 3) {
+                    bool lk;
+                    kern::SkinnyArgs k = kern::skinny_args(a, &lk);
+                    k.nz = sctas[i - first];
+                    k.partial = true;
+                    k.ws = d_part + off;
+                    // the partials are [z][long extent][short extent]: fold in that orientation
+                    f.M = k.R;
+                    f.N = k.NS;
+                    for (int v = 0; v < 2; v++) {
+                        f.Cm[v] = k.Cr[v];
+                        f.Cn[v] = k.Cs[v];
+                    }
+                    f.nvm = k.nvr;
+                    f.nvn = k.nvs;
+                    for (int v = 0; v < 4; v++) f.vsign[v] = k.vsign[v];
+                    f.scale = k.alpha;
+                    f.ks = k.nz;
+                    off += (int64_t)k.nz * k.R * k.NS;
+                    const std::pair<int, bool> cls{kern::skinny_groups(g.M, g.N), lk};
+                    kstart[cls].push_back(ktiles[cls]);
+                    ktiles[cls] += kern::skinny_tiles(k.R) * k.nz;
+                    kprobs[cls].push_back(k);
+                    kfl[cls] += g.flops();
                 } else {
                     const auto shape = kern::short_shape(g.M, g.N);
                     kern::ShortDesc d;
@@ -799,6 +850,22 @@ void Context::build_run(Plan& p, RunSchedule& rs, int first, int end) {
                 l.d_tile_start = (int*)dmalloc(kv.second.size() * sizeof(int));
                 stage_h2d(l.d_desc, kv.second.data(), l.desc_bytes);
                 stage_h2d(l.d_tile_start, sstart[kv.first].data(), kv.second.size() * sizeof(int));
+                run.launches.push_back(l);
+            }
+            for (auto& kv : kprobs) {
+                GemmLaunch l;
+                l.kind = GemmLaunch::SKINNY_GROUPED;
+                l.nt = kv.first.first;
+                l.ak = kv.first.second;
+                l.nprob = (int)kv.second.size();
+                l.tiles = ktiles[kv.first];
+                l.flops = kfl[kv.first];
+                own(l);
+                l.desc_bytes = kv.second.size() * sizeof(kern::SkinnyArgs);
+                l.d_desc = dmalloc(l.desc_bytes);
+                l.d_tile_start = (int*)dmalloc(kv.second.size() * sizeof(int));
+                stage_h2d(l.d_desc, kv.second.data(), l.desc_bytes);
+                stage_h2d(l.d_tile_start, kstart[kv.first].data(), kv.second.size() * sizeof(int));
                 run.launches.push_back(l);
             }
             // groups: products connected through a shared output block, in plan order
@@ -1103,7 +1170,7 @@ void Context::build_dot_run(Plan& p, RunSchedule& rs, int first, int end) {
 void Context::launch(Plan& p, const GemmLaunch& l, const std::string& label, double* dot_acc) {
     auto ev = profiling ? prof_begin() : std::make_pair((cudaEvent_t) nullptr, (cudaEvent_t) nullptr);
     switch (l.kind) {
-        case GemmLaunch::MERGED_SPLIT: run_merged(p, *l.merged); break;
+        case GemmLaunch::MERGED_SPLIT: run_merged(p, *l.merged, label); break;
         case GemmLaunch::GEMM: run_gemm(p, p.gemms[l.gemm]); break;
         case GemmLaunch::GEMM_GROUPED:
             kern::gemm_fp64_grouped(l.d_probs, l.d_tile_start, l.nprob, l.tiles, l.ak, l.bk, stream);
@@ -1128,7 +1195,19 @@ void Context::launch(Plan& p, const GemmLaunch& l, const std::string& label, dou
             break;
         default: throw Error(CCSD_ERR_PLAN, "bad launch record");
     }
-    if (profiling) prof_end(ev, label, l.flops);
+    if (profiling) {
+        // CCSD_PROFILE_KINDS=1: totals per statement and launch kind
+        static const bool kinds = std::getenv("CCSD_PROFILE_KINDS") != nullptr;
+        static const char* names[] = {"gemm", "grouped", "fold", "sum", "sum-batched", "scale", "scale-batched",
+                                      "dot-batched", "merged", "short", "skinny-grouped"};
+        if (kinds) {
+            std::string k = names[l.kind];
+            if (l.kind == GemmLaunch::GEMM) k = routes_split(p.gemms[l.gemm]) ? "gemm-split" : "gemm-fp64";
+            prof_end(ev, label + " {" + k + "}", l.flops);
+        } else {
+            prof_end(ev, label, l.flops);
+        }
+    }
 }
 
 void Context::run(Plan& p, double* scalar_out, double* dot_target) {

@@ -309,7 +309,7 @@ public:
     std::vector<double*> merged_retired;                   // outgrown, kept until the context goes
     void build_merged(Plan& p, GemmRun& run, int first, int end, std::vector<char>& merged,
                       const std::function<std::pair<int, int64_t>(int, int64_t)>& block_of);
-    void run_merged(Plan& p, MergedProduct& m);
+    void run_merged(Plan& p, MergedProduct& m, const std::string& label);
     int64_t merged_cache_bytes = 0;                        // reserved by merged products' cached slices
     void free_merged(MergedProduct& m);
     double* splitk_ws = nullptr;                           // FP64 split-K partials

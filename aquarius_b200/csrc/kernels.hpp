@@ -69,6 +69,10 @@ struct SkinnyArgs {
     double vsign[4] = {1, 1, 1, 1};   // [vr * nvs + vs]
     double alpha = 0;
     double* ws = nullptr;
+    // grouped launches: nz K ranges per row tile; partial: every K range writes its raw
+    // product to ws[z][r][s] for a fold (FoldDesc with ks = nz), even with nz = 1
+    int nz = 1;
+    bool partial = false;
 };
 // a contraction as a skinny product (the longer of M, N as the rows of L); *lk: L is
 // contiguous along k
@@ -76,11 +80,12 @@ SkinnyArgs skinny_args(const GemmArgs& g, bool* lk);
 // n-groups of 8 for a small extent (0: not a skinny product), and the row tiles of R rows
 int skinny_groups(int M, int N);
 int skinny_tiles(int R);
-// many skinny products of one level (disjoint outputs, no K split) in one launch
+// many skinny products in one launch: tile_start[p] is the first of problem p's
+// skinny_tiles(R) * nz CTAs; products writing C directly must have disjoint outputs
 void skinny_grouped(const SkinnyArgs* d, const int* tile_start, int nprob, int tiles, int nt, bool lk,
                     cudaStream_t s);
 
-// Short products: both extents <= 64 with (M/8) * (N/8) <= 8 fragments and a long K
+// Short products: both extents <= 64 with (M/8) * (N/8) <= 16 fragments and a long K
 // (F(mi) += <mn||ef> t(ef,in) per irrep block).  The CTAs of a problem split its K range
 // (kper k each) and write their M x N partial products to part[cta][m][n]; a fold adds
 // them (FoldDesc, ks = the problem's CTAs).  One launch covers every problem of one

@@ -458,7 +458,7 @@ __device__ __forceinline__ void skinny_body(const SkinnyArgs& g, int rtile, int 
     cp_wait<0>();
 
     // lane holds rows wr + 8i + fr, columns 8j + 2 fk + {0, 1}
-    if (nz > 1) {
+    if (nz > 1 || g.partial) {
         double* wz = g.ws + (int64_t)z * g.R * g.NS;
 #pragma unroll
         for (int i = 0; i < Sh::MT; i++) {
@@ -529,8 +529,8 @@ __global__ void __launch_bounds__(SK_THREADS, 2) skinny_kernel(SkinnyArgs g) {
     skinny_body<NT, LK>(g, blockIdx.x, blockIdx.z, gridDim.z, smem_raw);
 }
 
-// Grouped launch: the row tiles of many skinny products of one level (disjoint outputs, no
-// K split), tile_start[p] being the first tile of problem p
+// Grouped launch: the row tiles (times K ranges) of many skinny products, tile_start[p]
+// being the first CTA of problem p
 template <int NT, bool LK>
 __global__ void __launch_bounds__(SK_THREADS, 2)
     skinny_grouped_kernel(const SkinnyArgs* __restrict__ probs, const int* __restrict__ tile_start, int nprob) {
@@ -549,7 +549,8 @@ __global__ void __launch_bounds__(SK_THREADS, 2)
         sg = probs[lo];
     }
     __syncthreads();
-    skinny_body<NT, LK>(sg, t - tile_start[sp], 0, 1, smem_raw);
+    const int local = t - tile_start[sp], rt = (sg.R + SK_TM - 1) / SK_TM;
+    skinny_body<NT, LK>(sg, local % rt, local / rt, sg.nz, smem_raw);
 }
 
 __global__ void skinny_fold_kernel(SkinnyArgs g, int ks) {
@@ -577,13 +578,15 @@ constexpr int SH_THREADS = 256;
 constexpr int SH_KGRAN = 16 * (SH_THREADS / 32);   // kper is a multiple of this (128)
 
 template <int MT, int NT>
-__global__ void __launch_bounds__(SH_THREADS, 2)
+__global__ void __launch_bounds__(SH_THREADS, MT * NT > 8 ? 1 : 2)
     short_grouped_kernel(const ShortDesc* __restrict__ descs, const int* __restrict__ cta_start, int nprob) {
     // steps of 16 k (8 for the widest shapes, whose loads of a step would not fit the registers)
     constexpr int SH_U = MT + NT <= 6 ? 4 : 2, SH_KSTEP = 4 * SH_U;
     __shared__ ShortDesc sd;
     __shared__ int sp;
-    __shared__ double red[SH_THREADS / 32][MT * 8 * NT * 8];
+    // the warps' fragments for the reduction (dynamic: 64 KB for 16 fragments)
+    extern __shared__ __align__(16) unsigned char short_smem[];
+    auto red = reinterpret_cast<double(*)[MT * 8 * NT * 8]>(short_smem);
     const int t = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) {
         int lo = 0, hi = nprob - 1;
@@ -663,7 +666,9 @@ __global__ void __launch_bounds__(SH_THREADS, 2)
 
 template <int MT, int NT>
 void launch_short_t(const ShortDesc* d, const int* cta_start, int nprob, int total, cudaStream_t s) {
-    short_grouped_kernel<MT, NT><<<total, SH_THREADS, 0, s>>>(d, cta_start, nprob);
+    constexpr int bytes = (SH_THREADS / 32) * MT * 8 * NT * 8 * (int)sizeof(double);
+    set_smem_once((const void*)short_grouped_kernel<MT, NT>, bytes);
+    short_grouped_kernel<MT, NT><<<total, SH_THREADS, bytes, s>>>(d, cta_start, nprob);
 }
 
 }  // namespace
@@ -860,7 +865,7 @@ std::pair<int, int> short_shape(int M, int N) {
     if (M <= 0 || N <= 0 || M > 64 || N > 64) return {0, 0};
     auto frag = [](int x) { return x <= 8 ? 1 : (x <= 16 ? 2 : (x <= 32 ? 4 : 8)); };
     const int mt = frag(M), nt = frag(N);
-    if (mt * nt > 8) return {0, 0};
+    if (mt * nt > 16) return {0, 0};
     return {mt, nt};
 }
 
@@ -888,6 +893,9 @@ void short_grouped(const ShortDesc* d, const int* cta_start, int nprob, int tota
         case 0x41: launch_short_t<4, 1>(d, cta_start, nprob, total_ctas, s); break;
         case 0x42: launch_short_t<4, 2>(d, cta_start, nprob, total_ctas, s); break;
         case 0x81: launch_short_t<8, 1>(d, cta_start, nprob, total_ctas, s); break;
+        case 0x28: launch_short_t<2, 8>(d, cta_start, nprob, total_ctas, s); break;
+        case 0x44: launch_short_t<4, 4>(d, cta_start, nprob, total_ctas, s); break;
+        case 0x82: launch_short_t<8, 2>(d, cta_start, nprob, total_ctas, s); break;
         default: throw std::runtime_error("short product: unsupported fragment shape");
     }
     COUNT_LAUNCH();

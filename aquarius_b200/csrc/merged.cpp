@@ -37,11 +37,12 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
         m.emplace(key, v);
         return v;
     };
-    // block products that would run on the FP64 kernels, GEMM-shaped
+    // GEMM-shaped block products (those large enough for the split kernel alone too: a hole
+    // they left would break the grid of their class)
     std::vector<Cand> cands;
     for (int i = first; i < end; i++) {
         const GemmStep& g = p.gemms[p.steps[i].idx];
-        if (g.mkey.empty() || routes_split(g) || std::min(g.M, g.N) <= 8 || g.K <= 0) continue;
+        if (g.mkey.empty() || std::min(g.M, g.N) <= 8 || g.K <= 0) continue;
         cands.push_back({i, id(rid, g.mkey), id(cid, g.nkey), id(kid, g.kkey)});
     }
     if (std::getenv("CCSD_MERGE_REPORT")) {
@@ -80,48 +81,95 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
         std::fprintf(stderr, "[merge-skip] %-48s %5zu products %.3e flop  R=%zu C=%zu K=%zu  %s\n",
                      G(js[0]).label.c_str(), js.size(), fl, nr, nc, nk, why);
     };
-    // the grids to merge: a component that is a full grid, else the row classes of it (rows
-    // that meet the same column blocks over the same k blocks) that are.  A ring statement's
-    // component joins rows of several spin sectors and antisymmetriser terms through shared
-    // k and column blocks; each sector alone is a full grid.
-    std::vector<std::vector<int>> grids;
+    // The grids to merge.  The rows of a component that meet the same k blocks form a class;
+    // the rows and columns of a class that are linked through present (row, column) pairs
+    // form a grid whose columns are every column block its rows meet.  Each present pair
+    // must run over all of the grid's k blocks; the merged GEMM computes every pair and
+    // scatters the present ones, which is worth it while they hold at least half of the
+    // product, and otherwise the rows that meet the same columns form exact grids.  A
+    // ring statement's component joins rows of several spin sectors and antisymmetriser
+    // terms, each linked to its own columns, and the planner's canonical images leave
+    // same-spin sectors triangular.
+    struct Grid {
+        std::vector<int> js, R, C, Kb;
+    };
+    std::vector<Grid> grids;
+    auto add_grid = [&](const std::vector<int>& rows, const std::map<int, std::vector<int>>& of_row,
+                        const std::vector<int>& kb) {
+        Grid gr;
+        std::set<int> cs;
+        for (int r : rows) {
+            gr.js.insert(gr.js.end(), of_row.at(r).begin(), of_row.at(r).end());
+            for (int j : of_row.at(r)) cs.insert(cands[j].c);
+        }
+        if (gr.js.size() < 2) return;
+        std::sort(gr.js.begin(), gr.js.end());   // plan order
+        gr.R = rows;
+        gr.C.assign(cs.begin(), cs.end());
+        gr.Kb = kb;
+        grids.push_back(std::move(gr));
+    };
     for (auto& kv : comp) {
         const std::vector<int>& js = kv.second;
         if (js.size() < 2) continue;
-        std::set<int> Rs, Cs, Ks;
-        std::set<std::tuple<int, int, int>> cells;
-        for (int j : js) {
-            Rs.insert(cands[j].r);
-            Cs.insert(cands[j].c);
-            Ks.insert(cands[j].k);
-            cells.insert(std::make_tuple(cands[j].r, cands[j].c, cands[j].k));
-        }
-        if (cells.size() == js.size() && cells.size() == Rs.size() * Cs.size() * Ks.size()) {
-            grids.push_back(js);
-            continue;
-        }
-        std::map<int, std::pair<std::set<int>, std::set<int>>> sig;   // row -> (column blocks, k blocks)
+        std::map<int, std::set<int>> kset, cset;
         std::map<int, std::vector<int>> of_row;
+        std::map<int, int64_t> rlen, clen;
         for (int j : js) {
-            sig[cands[j].r].first.insert(cands[j].c);
-            sig[cands[j].r].second.insert(cands[j].k);
+            kset[cands[j].r].insert(cands[j].k);
+            cset[cands[j].r].insert(cands[j].c);
             of_row[cands[j].r].push_back(j);
+            rlen[cands[j].r] = G(j).M;
+            clen[cands[j].c] = G(j).N;
         }
-        std::map<std::pair<std::set<int>, std::set<int>>, std::vector<int>> cls;
-        for (auto& rs : sig) cls[rs.second].push_back(rs.first);
+        std::map<std::set<int>, std::vector<int>> cls;   // k blocks -> rows
+        for (auto& rk : kset) cls[rk.second].push_back(rk.first);
         for (auto& cl : cls) {
-            std::vector<int> sub;
-            for (int r : cl.second) sub.insert(sub.end(), of_row[r].begin(), of_row[r].end());
-            if (sub.size() < 2) continue;
-            std::sort(sub.begin(), sub.end());   // plan order
-            if (sub.size() == cl.second.size() * cl.first.first.size() * cl.first.second.size()) grids.push_back(sub);
-            else reject(sub, "row class not a full grid", cl.second.size(), cl.first.first.size(), cl.first.second.size());
+            const std::vector<int> kb(cl.first.begin(), cl.first.end());
+            // rows linked through shared columns
+            std::map<int, int> up;   // union-find over rows (r) and columns (-1 - c)
+            std::function<int(int)> root = [&](int x) {
+                auto it = up.find(x);
+                if (it == up.end() || it->second == x) return x;
+                return it->second = root(it->second);
+            };
+            for (int r : cl.second) {
+                up.emplace(r, r);
+                for (int c : cset[r]) {
+                    up.emplace(-1 - c, -1 - c);
+                    const int a = root(r), b = root(-1 - c);
+                    if (a != b) up[a] = b;
+                }
+            }
+            std::map<int, std::vector<int>> linked;
+            for (int r : cl.second) linked[root(r)].push_back(r);
+            for (auto& lk : linked) {
+                const std::vector<int>& rows = lk.second;
+                std::set<int> cs;
+                double present = 0, mr = 0, nc = 0;
+                for (int r : rows) {
+                    mr += rlen[r];
+                    for (int c : cset[r]) present += (double)rlen[r] * clen[c], cs.insert(c);
+                }
+                for (int c : cs) nc += clen[c];
+                if (present >= 0.5 * mr * nc) {
+                    add_grid(rows, of_row, kb);
+                    continue;
+                }
+                std::map<std::set<int>, std::vector<int>> exact;   // columns -> rows
+                for (int r : rows) exact[cset[r]].push_back(r);
+                for (auto& ex : exact) add_grid(ex.second, of_row, kb);
+            }
         }
     }
-    for (const std::vector<int>& js : grids) {
-        std::vector<int> R, C, Kb;
+    for (const Grid& gr : grids) {
+        const std::vector<int>& js = gr.js;
+        const std::vector<int>& R = gr.R;
+        const std::vector<int>& C = gr.C;
+        const std::vector<int>& Kb = gr.Kb;
         std::map<std::tuple<int, int, int>, int> at;
         std::map<int, int> Mr, Nc, Kl;
+        std::set<std::pair<int, int>> present;
         bool ok = true;
         for (int j : js) {
             const Cand& c = cands[j];
@@ -132,23 +180,29 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
                 break;
             }
             at[t] = j;
-            if (!Mr.count(c.r)) R.push_back(c.r), Mr[c.r] = g.M;
-            if (!Nc.count(c.c)) C.push_back(c.c), Nc[c.c] = g.N;
-            if (!Kl.count(c.k)) Kb.push_back(c.k), Kl[c.k] = g.K;
+            present.insert({c.r, c.c});
+            if (!Mr.count(c.r)) Mr[c.r] = g.M;
+            if (!Nc.count(c.c)) Nc[c.c] = g.N;
+            if (!Kl.count(c.k)) Kl[c.k] = g.K;
             ok &= Mr[c.r] == g.M && Nc[c.c] == g.N && Kl[c.k] == g.K;
         }
-        // a full grid only: every row block with every column block over every k block
-        if (!ok || at.size() != R.size() * C.size() * Kb.size()) {
-            reject(js, !ok ? "repeated or mismatched extents" : "not a full grid", R.size(), C.size(), Kb.size());
+        // every present pair over every k block
+        if (!ok || at.size() != present.size() * Kb.size()) {
+            reject(js, !ok ? "repeated or mismatched extents" : "a pair misses k blocks", R.size(), C.size(), Kb.size());
             continue;
         }
         auto J = [&](int r, int c, int k) { return at.at(std::make_tuple(r, c, k)); };
+        std::map<int, std::vector<int>> cols_of, rows_of;   // present pairs by row / by column
+        for (auto& rc : present) {
+            cols_of[rc.first].push_back(rc.second);
+            rows_of[rc.second].push_back(rc.first);
+        }
         // the rectangles of A depend on (rows, k) only, of B on (k, columns), of C on (rows,
         // columns): the products that share them must agree on their tables
         for (int r : R)
             for (int k : Kb) {
-                const GemmStep& a = G(J(r, C[0], k));
-                for (int c : C) {
+                const GemmStep& a = G(J(r, cols_of[r][0], k));
+                for (int c : cols_of[r]) {
                     const GemmStep& b = G(J(r, c, k));
                     ok &= b.tA == a.tA && b.hAm == a.hAm && b.hAk == a.hAk && b.a_kcontig == a.a_kcontig;
                 }
@@ -159,8 +213,8 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
         }
         for (int k : Kb)
             for (int c : C) {
-                const GemmStep& a = G(J(R[0], c, k));
-                for (int r : R) {
+                const GemmStep& a = G(J(rows_of[c][0], c, k));
+                for (int r : rows_of[c]) {
                     const GemmStep& b = G(J(r, c, k));
                     ok &= b.tB == a.tB && b.hBk == a.hBk && b.hBn == a.hBn && b.b_kcontig == a.b_kcontig;
                 }
@@ -172,18 +226,19 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
         // coefficients: alpha(r, c, k) = alpha(r, c, k0) * ratio(k), the ratio (spin weights and
         // reordering signs of the k block) folded into the k block's rectangles of B
         std::map<int, double> ratio;
-        for (int k : Kb) ratio[k] = G(J(R[0], C[0], k)).alpha / G(J(R[0], C[0], Kb[0])).alpha;
-        for (int r : R)
-            for (int c : C) {
-                const GemmStep& a = G(J(r, c, Kb[0]));
-                for (int k : Kb) {
-                    const GemmStep& b = G(J(r, c, k));
-                    ok &= b.alpha == a.alpha * ratio[k];
-                    ok &= b.tC == a.tC && b.nvm == a.nvm && b.nvn == a.nvn;
-                    for (int v = 0; v < 2 && ok; v++) ok &= b.hCm[v] == a.hCm[v] && b.hCn[v] == a.hCn[v];
-                    for (int v = 0; v < 4 && ok; v++) ok &= b.vsign[v] == a.vsign[v];
-                }
+        const int r0 = present.begin()->first, c0 = present.begin()->second;
+        for (int k : Kb) ratio[k] = G(J(r0, c0, k)).alpha / G(J(r0, c0, Kb[0])).alpha;
+        for (auto& rc : present) {
+            const int r = rc.first, c = rc.second;
+            const GemmStep& a = G(J(r, c, Kb[0]));
+            for (int k : Kb) {
+                const GemmStep& b = G(J(r, c, k));
+                ok &= b.alpha == a.alpha * ratio[k];
+                ok &= b.tC == a.tC && b.nvm == a.nvm && b.nvn == a.nvn;
+                for (int v = 0; v < 2 && ok; v++) ok &= b.hCm[v] == a.hCm[v] && b.hCn[v] == a.hCn[v];
+                for (int v = 0; v < 4 && ok; v++) ok &= b.vsign[v] == a.vsign[v];
             }
+        }
         if (!ok) {
             reject(js, "coefficients or C tables differ", R.size(), C.size(), Kb.size());
             continue;
@@ -193,15 +248,23 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
         for (int r : R) roff[r] = (int)M, M += Mr[r];
         for (int c : C) coff[c] = (int)N, N += Nc[c];
         for (int k : Kb) koff[k] = (int)K, K += Kl[k];
-        // a class worth one tensor-core GEMM (its slicing reads the operands once; below this
-        // the grouped FP64 launch is cheaper)
-        if (M < 64 || N < 32 || K < 128 || 2.0 * M * N * K < 2e7 || M > (1 << 28) || N > (1 << 28) || K > (1 << 28)) {
+        double used = 0;
+        for (auto& rc : present) used += (double)Mr[rc.first] * Nc[rc.second];
+        if (used < 0.5 * (double)M * N) {
+            reject(js, "present pairs under half of the product", R.size(), C.size(), Kb.size());
+            continue;
+        }
+        // a class worth one tensor-core GEMM and its four or more launches (slicing reads each
+        // operand twice, the scatter the product once); below this the grouped FP64 launches
+        // are cheaper
+        if (M < 32 || N < 32 || K < 32 || 2.0 * M * N * K < 1e8 || M > (1 << 28) || N > (1 << 28) || K > (1 << 28)) {
             reject(js, "below the size bar", R.size(), C.size(), Kb.size());
             continue;
         }
         if (report)
-            std::fprintf(stderr, "[merged] %-48s %5zu products  M=%-6lld N=%-6lld K=%-6lld\n", G(js[0]).label.c_str(),
-                         js.size(), (long long)M, (long long)N, (long long)K);
+            std::fprintf(stderr, "[merged] %-48s %5zu products  M=%-6lld N=%-6lld K=%-6lld ks=%d present %.2f\n",
+                         G(js[0]).label.c_str(), js.size(), (long long)M, (long long)N, (long long)K,
+                         kern::split_ksplit((int)M, (int)N, (int)K, 4, kern::SLICE_INT8), used / ((double)M * N));
 
         auto mp = std::make_shared<MergedProduct>();
         mp->M = (int)M;
@@ -213,7 +276,7 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
         std::vector<int64_t> tsA, tsB;
         for (int r : R)
             for (int k : Kb) {
-                const GemmStep& g = G(J(r, C[0], k));
+                const GemmStep& g = G(J(r, cols_of[r][0], k));
                 const kern::GemmArgs a = gemm_args(p, g);
                 kern::RectDesc d;
                 d.X = a.A;
@@ -231,7 +294,7 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
             }
         for (int c : C)
             for (int k : Kb) {
-                const GemmStep& g = G(J(R[0], c, k));
+                const GemmStep& g = G(J(rows_of[c][0], c, k));
                 const kern::GemmArgs a = gemm_args(p, g);
                 kern::RectDesc d;
                 d.X = a.B;
@@ -253,47 +316,53 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
         std::vector<std::vector<kern::ScatterDesc>> lv;
         double flops = 0;
         for (int j : js) flops += G(j).flops();
-        for (int r : R)
-            for (int c : C) {
-                const GemmStep& g = G(J(r, c, Kb[0]));
-                const kern::GemmArgs a = gemm_args(p, g);
-                kern::ScatterDesc s;
-                s.C = a.C;
-                for (int v = 0; v < 2; v++) {
-                    s.Cm[v] = a.Cm[v];
-                    s.Cn[v] = a.Cn[v];
-                }
-                s.nvm = g.nvm;
-                s.nvn = g.nvn;
-                for (int v = 0; v < 4; v++) s.vsign[v] = a.vsign[v];
-                s.alpha = a.alpha;
-                s.nrows = g.M;
-                s.ncols = g.N;
-                s.row0 = roff[r];
-                s.col0 = coff[c];
-                std::vector<std::pair<int, int64_t>> keys;
-                for (int v = 0; v < g.nvm; v++)
-                    for (int w = 0; w < g.nvn; w++) {
-                        if (g.hCm[v].empty() || g.hCn[w].empty()) continue;
-                        keys.push_back(block_of(g.tC, *std::min_element(g.hCm[v].begin(), g.hCm[v].end()) +
-                                                          *std::min_element(g.hCn[w].begin(), g.hCn[w].end())));
-                    }
-                int L = 0;
-                for (auto& key : keys) {
-                    auto f = last.find(key);
-                    if (f != last.end()) L = std::max(L, f->second + 1);
-                }
-                for (auto& key : keys) last[key] = L;
-                if ((int)lv.size() <= L) lv.resize(L + 1);
-                lv[L].push_back(s);
+        for (auto& rc : present) {
+            const int r = rc.first, c = rc.second;
+            const GemmStep& g = G(J(r, c, Kb[0]));
+            const kern::GemmArgs a = gemm_args(p, g);
+            kern::ScatterDesc s;
+            s.C = a.C;
+            for (int v = 0; v < 2; v++) {
+                s.Cm[v] = a.Cm[v];
+                s.Cn[v] = a.Cn[v];
             }
+            s.nvm = g.nvm;
+            s.nvn = g.nvn;
+            for (int v = 0; v < 4; v++) s.vsign[v] = a.vsign[v];
+            s.alpha = a.alpha;
+            s.nrows = g.M;
+            s.ncols = g.N;
+            s.row0 = roff[r];
+            s.col0 = coff[c];
+            std::vector<std::pair<int, int64_t>> keys;
+            for (int v = 0; v < g.nvm; v++)
+                for (int w = 0; w < g.nvn; w++) {
+                    if (g.hCm[v].empty() || g.hCn[w].empty()) continue;
+                    keys.push_back(block_of(g.tC, *std::min_element(g.hCm[v].begin(), g.hCm[v].end()) +
+                                                      *std::min_element(g.hCn[w].begin(), g.hCn[w].end())));
+                }
+            int L = 0;
+            for (auto& key : keys) {
+                auto f = last.find(key);
+                if (f != last.end()) L = std::max(L, f->second + 1);
+            }
+            for (auto& key : keys) last[key] = L;
+            if ((int)lv.size() <= L) lv.resize(L + 1);
+            lv[L].push_back(s);
+        }
         // cached slices of constant operands, within the split cache budget
         {
             bool constA = true, constB = true;
             for (int r : R)
-                for (int k : Kb) constA &= G(J(r, C[0], k)).tA != kScratch && is_constant(G(J(r, C[0], k)).tA);
+                for (int k : Kb) {
+                    const int h = G(J(r, cols_of[r][0], k)).tA;
+                    constA &= h != kScratch && is_constant(h);
+                }
             for (int c : C)
-                for (int k : Kb) constB &= G(J(R[0], c, k)).tB != kScratch && is_constant(G(J(R[0], c, k)).tB);
+                for (int k : Kb) {
+                    const int h = G(J(rows_of[c][0], c, k)).tB;
+                    constB &= h != kScratch && is_constant(h);
+                }
             int64_t used = merged_cache_bytes;
             for (auto& kv : split_cache) used += kv.second.bytes;
             const int deepest = 5;   // any slice count a refinement reaches
@@ -360,9 +429,18 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
     }
 }
 
-void Context::run_merged(Plan& p, MergedProduct& m) {
+void Context::run_merged(Plan& p, MergedProduct& m, const std::string& label) {
     const int ns = step_slices(p.gemms[m.first_gemm]), kind = slice_kind();
     split_launches++;
+    // CCSD_PROFILE_KINDS=1: the phases of a merged product timed apart
+    static const bool phases = std::getenv("CCSD_PROFILE_KINDS") != nullptr;
+    const bool timed = profiling && phases;
+    auto phase = [&](const char* name, const std::function<void()>& f) {
+        if (!timed) return f();
+        auto ev = prof_begin();
+        f();
+        prof_end(ev, label + " {merged:" + name + "}", 0.0);
+    };
     auto operand = [&](bool is_a) {
         const int rows = is_a ? m.M : m.N;
         const kern::RectDesc* d = is_a ? m.dA : m.dB;
@@ -374,7 +452,7 @@ void Context::run_merged(Plan& p, MergedProduct& m) {
             if (!c.data || c.kind != kind || c.nslices < ns) {
                 if (c.data) free_sliced(c);
                 c = alloc_sliced(rows, m.K, ns, kind);
-                kern::rect_slice(d, ts, n, tiles, ns, c, stream);
+                phase("slice-cached", [&] { kern::rect_slice(d, ts, n, tiles, ns, c, stream); });
             }
             // the first ns slices of a deeper slicing are the ns-slice slicing
             kern::SlicedOperand v = c;
@@ -388,7 +466,7 @@ void Context::run_merged(Plan& p, MergedProduct& m) {
         v.kpad = kern::split_k_pad(m.K, kind);
         v.nslices = ns;
         v.kind = kind;
-        kern::rect_slice(d, ts, n, tiles, ns, v, stream);
+        phase(is_a ? "slice-a" : "slice-b", [&] { kern::rect_slice(d, ts, n, tiles, ns, v, stream); });
         return v;
     };
     const kern::SlicedOperand va = operand(true);
@@ -399,9 +477,11 @@ void Context::run_merged(Plan& p, MergedProduct& m) {
     a.dense_out = true;
     a.alpha = 1.0;
     const int ks = kern::split_ksplit(m.M, m.N, m.K, ns, kind);
-    kern::gemm_split(va, vb, m.M, m.N, m.K, a, stream, ks);
-    for (auto& L : m.levels)
-        kern::rect_scatter(L.d, L.cs, L.n, L.chunks, merged_ws, m.N, (int64_t)m.M * m.N, ks, stream);
+    phase("gemm", [&] { kern::gemm_split(va, vb, m.M, m.N, m.K, a, stream, ks); });
+    phase("scatter", [&] {
+        for (auto& L : m.levels)
+            kern::rect_scatter(L.d, L.cs, L.n, L.chunks, merged_ws, m.N, (int64_t)m.M * m.N, ks, stream);
+    });
 }
 
 void Context::free_merged(MergedProduct& m) {
