@@ -464,6 +464,8 @@ void Context::release(Plan& p) {
                     dfree(l.d_tile_start, (l.kind == GemmLaunch::FOLD_GROUPS ? l.ngroups + 1 : l.nprob) * sizeof(int));
                 if (l.d_desc) dfree(l.d_desc, l.desc_bytes);
                 if (l.d_chunks) dfree(l.d_chunks, l.nprob * sizeof(int64_t));
+                if (l.arena) dfree(l.arena, l.arena_bytes);
+                if (l.aux) dfree(l.aux, l.aux_bytes);
                 if (l.merged) free_merged(*l.merged);
             }
     p.schedules.clear();
@@ -1178,6 +1180,11 @@ void Context::launch(Plan& p, const GemmLaunch& l, const std::string& label, dou
         case GemmLaunch::DOT_BATCHED:
             kern::dot_batched((const kern::DotDesc*)l.d_desc, l.d_chunks, l.nprob, l.chunks, l.d_part, dot_acc, stream);
             break;
+        case GemmLaunch::MERGED_SLICE:
+            kern::rect_slice_batched((const kern::RectDesc*)l.d_desc, l.d_chunks, l.nprob, l.chunks,
+                                     step_slices(p.gemms[l.gemm]), (uint8_t*)l.aux + l.aux_bytes / 2, l.aux_bytes / 2,
+                                     stream);
+            break;
         case GemmLaunch::SKINNY_GROUPED:
             kern::skinny_grouped((const kern::SkinnyArgs*)l.d_desc, l.d_tile_start, l.nprob, l.tiles, l.nt, l.ak, stream);
             break;
@@ -1199,7 +1206,7 @@ void Context::launch(Plan& p, const GemmLaunch& l, const std::string& label, dou
         // CCSD_PROFILE_KINDS=1: totals per statement and launch kind
         static const bool kinds = std::getenv("CCSD_PROFILE_KINDS") != nullptr;
         static const char* names[] = {"gemm", "grouped", "fold", "sum", "sum-batched", "scale", "scale-batched",
-                                      "dot-batched", "merged", "short", "skinny-grouped"};
+                                      "dot-batched", "merged", "short", "skinny-grouped", "merged-slice"};
         if (kinds) {
             std::string k = names[l.kind];
             if (l.kind == GemmLaunch::GEMM) k = routes_split(p.gemms[l.gemm]) ? "gemm-split" : "gemm-fp64";

@@ -183,7 +183,7 @@ constexpr int kScratch = -1;
 // grouped tiled-FP64 kernel, permuted sums, block scalings).
 struct GemmLaunch {
     enum Kind { GEMM, GEMM_GROUPED, FOLD_GROUPS, SUM, SUM_BATCHED, SCALE, SCALE_BATCHED, DOT_BATCHED, MERGED_SPLIT,
-                SHORT_GROUPED, SKINNY_GROUPED };
+                SHORT_GROUPED, SKINNY_GROUPED, MERGED_SLICE };
     Kind kind = GEMM;
     int gemm = -1;                     // single GEMM: index into Plan::gemms
     int step = -1;                     // single SUM / SCALE: index into Plan::sums / scales
@@ -203,6 +203,10 @@ struct GemmLaunch {
     int64_t chunks = 0;
     double flops = 0;
     std::shared_ptr<struct MergedProduct> merged;   // MERGED_SPLIT
+    void* arena = nullptr;             // batched slicing of merged products: their operands'
+    size_t arena_bytes = 0;            // slices, scales and row maxima (aux: the row maxima)
+    void* aux = nullptr;
+    size_t aux_bytes = 0;
 };
 // The block products of one irrep class of a symmetry-blocked statement as one dense split
 // GEMM: rectangles of A (rows x k), of B (columns x k) and of C (rows x columns) placed in
@@ -229,6 +233,14 @@ struct MergedProduct {
     bool cache_a = false, cache_b = false;
     int64_t cache_bytes = 0;           // reserved for both at build
     kern::SlicedOperand sA, sB;
+    // the other operands are sliced by one batched launch for all merged products of the
+    // statement (MERGED_SLICE, before the first of them) into their own operand buffers
+    std::vector<kern::RectDesc> hA, hB;   // host copies of the rectangles
+    // each rectangle's host row and k tables (its block product's), to find equal operands
+    std::vector<std::pair<const std::vector<int64_t>*, const std::vector<int64_t>*>> srcA, srcB;
+    bool self_read = false;            // an operand is the statement's output (no batching)
+    bool batched_a = false, batched_b = false;
+    kern::SlicedOperand pa, pb;
 };
 struct GemmRun {
     int first = 0, end = 0;            // steps [first, end)
@@ -310,6 +322,7 @@ public:
     void build_merged(Plan& p, GemmRun& run, int first, int end, std::vector<char>& merged,
                       const std::function<std::pair<int, int64_t>(int, int64_t)>& block_of);
     void run_merged(Plan& p, MergedProduct& m, const std::string& label);
+    void batch_merged_slicing(GemmRun& run, size_t launch0);
     int64_t merged_cache_bytes = 0;                        // reserved by merged products' cached slices
     void free_merged(MergedProduct& m);
     double* splitk_ws = nullptr;                           // FP64 split-K partials

@@ -181,12 +181,21 @@ struct RectDesc {
     int tiles_r = 0;               // 32-row tiles of the rectangle
     double mul = 1.0;              // factor of the rectangle's values (its product's coefficient
                                    // relative to the class's, folded into the B operand)
+    // batched slicing: the rectangle's own merged operand (null: the launch's operand)
+    uint8_t* out = nullptr;        // [5 slices][rows_p][kpad], zero outside the rectangles
+    double* scale = nullptr;       // [rows_p]
+    unsigned long long* rowmax = nullptr;   // [rows_p]
+    int rows_p = 0, kpad = 0;
 };
 // row maxima over all rectangles of a row, then INT8 slices of every rectangle into out
 // (its rows, scales and slices zeroed first); tile_start[i] = first 32 x 64 tile of
 // rectangle i, ntiles in all
 void rect_slice(const RectDesc* d, const int64_t* tile_start, int n, int64_t ntiles, int ns, SlicedOperand& out,
                 cudaStream_t s);
+// the rectangles of many merged operands (each with its own destination) in one rowmax
+// and one slice launch; rowmax_arena (bytes) holds every destination's row maxima
+void rect_slice_batched(const RectDesc* d, const int64_t* tile_start, int n, int64_t ntiles, int ns,
+                        void* rowmax_arena, size_t rowmax_bytes, cudaStream_t s);
 struct ScatterDesc {
     double* C = nullptr;
     const int64_t* Cm[2] = {nullptr, nullptr};

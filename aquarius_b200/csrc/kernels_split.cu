@@ -882,90 +882,117 @@ __device__ __forceinline__ void rect_tile(const RectDesc& d, int64_t lt, int& r0
     }
 }
 
+// A CTA takes RECT_TPC consecutive tiles: one binary search over the rectangles' first
+// tiles, then a forward walk (a batched launch covers some 10^5 rectangles, and a search
+// per tile was a chain of 17 dependent loads in front of 16 KB of work)
+constexpr int RECT_TPC = 8;
+
+__device__ __forceinline__ int next_rect(const int64_t* __restrict__ ts, int n, int sp, int64_t t, bool first) {
+    if (first) return find_rect(ts, n, t);
+    while (sp + 1 < n && ts[sp + 1] <= t) sp++;
+    return sp;
+}
+
 __global__ void __launch_bounds__(split::STHREADS) rect_rowmax_kernel(const RectDesc* __restrict__ rd,
                                                                       const int64_t* __restrict__ ts, int n,
-                                                                      unsigned long long* rowmax) {
+                                                                      int64_t ntiles, unsigned long long* rowmax) {
     using namespace split;
     __shared__ int64_t sR[SR], sK[SK];
     __shared__ double red[STHREADS / 32][SR];
     __shared__ int sp;
-    if (threadIdx.x == 0) sp = find_rect(ts, n, blockIdx.x);
-    __syncthreads();
-    const RectDesc& d = rd[sp];
-    int r0, k0;
-    double v[SPER];
-    rect_tile(d, blockIdx.x - ts[sp], r0, k0, v, sR, sK);
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (d.kc) {
-#pragma unroll
-        for (int i = 0; i < SPER; i++) {
-            double m = fabs(v[i]);
-            for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-            const int r = (warp >> 1) + 4 * i;
-            if (lane == 0 && r0 + r < d.nrows && m > 0.0)
-                atomicMax(&rowmax[d.row0 + r0 + r], (unsigned long long)__double_as_longlong(m));
-        }
-    } else {
-        double m = 0.0;
-#pragma unroll
-        for (int i = 0; i < SPER; i++) m = fmax(m, fabs(v[i]));
-        red[warp][lane] = m;
+    const int64_t t0 = (int64_t)blockIdx.x * RECT_TPC;
+    const int64_t t1 = t0 + RECT_TPC < ntiles ? t0 + RECT_TPC : ntiles;
+    for (int64_t t = t0; t < t1; t++) {
+        if (threadIdx.x == 0) sp = next_rect(ts, n, sp, t, t == t0);
         __syncthreads();
-        if (warp == 0) {
-            for (int w = 1; w < STHREADS / 32; w++) m = fmax(m, red[w][lane]);
-            if (r0 + lane < d.nrows && m > 0.0)
-                atomicMax(&rowmax[d.row0 + r0 + lane], (unsigned long long)__double_as_longlong(m));
+        const RectDesc& d = rd[sp];
+        unsigned long long* rm = d.rowmax ? d.rowmax : rowmax;
+        int r0, k0;
+        double v[SPER];
+        rect_tile(d, t - ts[sp], r0, k0, v, sR, sK);
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        if (d.kc) {
+#pragma unroll
+            for (int i = 0; i < SPER; i++) {
+                double m = fabs(v[i]);
+                for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+                const int r = (warp >> 1) + 4 * i;
+                if (lane == 0 && r0 + r < d.nrows && m > 0.0)
+                    atomicMax(&rm[d.row0 + r0 + r], (unsigned long long)__double_as_longlong(m));
+            }
+        } else {
+            double m = 0.0;
+#pragma unroll
+            for (int i = 0; i < SPER; i++) m = fmax(m, fabs(v[i]));
+            red[warp][lane] = m;
+            __syncthreads();
+            if (warp == 0) {
+                for (int w = 1; w < STHREADS / 32; w++) m = fmax(m, red[w][lane]);
+                if (r0 + lane < d.nrows && m > 0.0)
+                    atomicMax(&rm[d.row0 + r0 + lane], (unsigned long long)__double_as_longlong(m));
+            }
         }
+        __syncthreads();   // the tables and the reduction slots are reused by the next tile
     }
 }
 
 template <int NS>
 __global__ void __launch_bounds__(split::STHREADS) rect_slice_kernel(const RectDesc* __restrict__ rd,
                                                                      const int64_t* __restrict__ ts, int n,
-                                                                     const unsigned long long* __restrict__ rowmax,
-                                                                     int rows_p, int kpad, uint8_t* __restrict__ out,
-                                                                     double* __restrict__ scale) {
+                                                                     int64_t ntiles, const unsigned long long* rowmax0,
+                                                                     int rows_p0, int kpad0, uint8_t* out0,
+                                                                     double* scale0) {
     using namespace split;
     __shared__ double tile[SR][SK + 1];
     __shared__ int64_t sR[SR], sK[SK];
     __shared__ double sMul[SR];
     __shared__ int sp;
-    if (threadIdx.x == 0) sp = find_rect(ts, n, blockIdx.x);
-    __syncthreads();
-    const RectDesc& d = rd[sp];
-    int r0, k0;
-    double v[SPER];
-    rect_tile(d, blockIdx.x - ts[sp], r0, k0, v, sR, sK);
-    if (threadIdx.x < SR) {
-        const int row = d.row0 + r0 + threadIdx.x;
-        const bool in = r0 + (int)threadIdx.x < d.nrows;
-        const double mx = in ? __longlong_as_double((long long)rowmax[row]) : 0.0;
-        const bool nz = mx > 1e-290;
-        sMul[threadIdx.x] = nz ? 127.0 / mx : 0.0;
-        if (in && d.k0 == 0 && k0 == 0) scale[row] = nz ? mx / 127.0 : 0.0;   // the row's first rectangle
-    }
-#pragma unroll
-    for (int i = 0; i < SPER; i++) {
-        const int e = threadIdx.x + i * STHREADS;
-        const int r = d.kc ? e / SK : e % SR, k = d.kc ? e % SK : e / SR;
-        tile[r][k] = v[i];
-    }
-    __syncthreads();
-    const size_t plane = (size_t)rows_p * kpad;
-#pragma unroll
-    for (int i = 0; i < SPER; i++) {
-        const int e = threadIdx.x + i * STHREADS;
-        const int k = e % SK, r = e / SK;
-        if (r0 + r >= d.nrows || k0 + k >= d.nk) continue;
-        const double mul = sMul[r];
-        const size_t o = (size_t)(d.row0 + r0 + r) * kpad + (size_t)(d.k0 + k0 + k);
-        double y = tile[r][k] * mul;
-#pragma unroll
-        for (int q = 0; q < NS; q++) {
-            const double st = mul > 0.0 ? rint(y) : 0.0;
-            out[q * plane + o] = (uint8_t)(int8_t)(int)st;
-            y = (y - st) * 254.0;
+    const int64_t t0 = (int64_t)blockIdx.x * RECT_TPC;
+    const int64_t t1 = t0 + RECT_TPC < ntiles ? t0 + RECT_TPC : ntiles;
+    for (int64_t t = t0; t < t1; t++) {
+        if (threadIdx.x == 0) sp = next_rect(ts, n, sp, t, t == t0);
+        __syncthreads();
+        const RectDesc& d = rd[sp];
+        // the rectangle's own merged operand, or the launch's
+        const unsigned long long* rowmax = d.out ? d.rowmax : rowmax0;
+        const int rows_p = d.out ? d.rows_p : rows_p0, kpad = d.out ? d.kpad : kpad0;
+        uint8_t* out = d.out ? d.out : out0;
+        double* scale = d.out ? d.scale : scale0;
+        int r0, k0;
+        double v[SPER];
+        rect_tile(d, t - ts[sp], r0, k0, v, sR, sK);
+        if (threadIdx.x < SR) {
+            const int row = d.row0 + r0 + threadIdx.x;
+            const bool in = r0 + (int)threadIdx.x < d.nrows;
+            const double mx = in ? __longlong_as_double((long long)rowmax[row]) : 0.0;
+            const bool nz = mx > 1e-290;
+            sMul[threadIdx.x] = nz ? 127.0 / mx : 0.0;
+            if (in && d.k0 == 0 && k0 == 0) scale[row] = nz ? mx / 127.0 : 0.0;   // the row's first rectangle
         }
+#pragma unroll
+        for (int i = 0; i < SPER; i++) {
+            const int e = threadIdx.x + i * STHREADS;
+            const int r = d.kc ? e / SK : e % SR, k = d.kc ? e % SK : e / SR;
+            tile[r][k] = v[i];
+        }
+        __syncthreads();
+        const size_t plane = (size_t)rows_p * kpad;
+#pragma unroll
+        for (int i = 0; i < SPER; i++) {
+            const int e = threadIdx.x + i * STHREADS;
+            const int k = e % SK, r = e / SK;
+            if (r0 + r >= d.nrows || k0 + k >= d.nk) continue;
+            const double mul = sMul[r];
+            const size_t o = (size_t)(d.row0 + r0 + r) * kpad + (size_t)(d.k0 + k0 + k);
+            double y = tile[r][k] * mul;
+#pragma unroll
+            for (int q = 0; q < NS; q++) {
+                const double st = mul > 0.0 ? rint(y) : 0.0;
+                out[q * plane + o] = (uint8_t)(int8_t)(int)st;
+                y = (y - st) * 254.0;
+            }
+        }
+        __syncthreads();   // the tile, the tables and the row factors are reused by the next tile
     }
 }
 
@@ -1005,10 +1032,24 @@ void rect_slice(const RectDesc* d, const int64_t* tile_start, int n, int64_t nti
     cudaMemsetAsync(rowmax, 0, sizeof(double) * out.rows, s);
     cudaMemsetAsync(out.scale, 0, sizeof(double) * out.rows, s);
     cudaMemsetAsync(out.data, 0, (size_t)ns * out.rows * out.kpad, s);
-    rect_rowmax_kernel<<<(unsigned)ntiles, STHREADS, 0, s>>>(d, tile_start, n, rowmax);
-    if (ns == 3) rect_slice_kernel<3><<<(unsigned)ntiles, STHREADS, 0, s>>>(d, tile_start, n, rowmax, out.rows, out.kpad, out.data, out.scale);
-    else if (ns == 4) rect_slice_kernel<4><<<(unsigned)ntiles, STHREADS, 0, s>>>(d, tile_start, n, rowmax, out.rows, out.kpad, out.data, out.scale);
-    else rect_slice_kernel<5><<<(unsigned)ntiles, STHREADS, 0, s>>>(d, tile_start, n, rowmax, out.rows, out.kpad, out.data, out.scale);
+    const unsigned grid = (unsigned)((ntiles + RECT_TPC - 1) / RECT_TPC);
+    rect_rowmax_kernel<<<grid, STHREADS, 0, s>>>(d, tile_start, n, ntiles, rowmax);
+    if (ns == 3) rect_slice_kernel<3><<<grid, STHREADS, 0, s>>>(d, tile_start, n, ntiles, rowmax, out.rows, out.kpad, out.data, out.scale);
+    else if (ns == 4) rect_slice_kernel<4><<<grid, STHREADS, 0, s>>>(d, tile_start, n, ntiles, rowmax, out.rows, out.kpad, out.data, out.scale);
+    else rect_slice_kernel<5><<<grid, STHREADS, 0, s>>>(d, tile_start, n, ntiles, rowmax, out.rows, out.kpad, out.data, out.scale);
+    g_launches += 2;
+}
+
+void rect_slice_batched(const RectDesc* d, const int64_t* tile_start, int n, int64_t ntiles, int ns,
+                        void* rowmax_arena, size_t rowmax_bytes, cudaStream_t s) {
+    using namespace split;
+    if (n <= 0 || ntiles <= 0) return;
+    cudaMemsetAsync(rowmax_arena, 0, rowmax_bytes, s);
+    const unsigned grid = (unsigned)((ntiles + RECT_TPC - 1) / RECT_TPC);
+    rect_rowmax_kernel<<<grid, STHREADS, 0, s>>>(d, tile_start, n, ntiles, nullptr);
+    if (ns == 3) rect_slice_kernel<3><<<grid, STHREADS, 0, s>>>(d, tile_start, n, ntiles, nullptr, 0, 0, nullptr, nullptr);
+    else if (ns == 4) rect_slice_kernel<4><<<grid, STHREADS, 0, s>>>(d, tile_start, n, ntiles, nullptr, 0, 0, nullptr, nullptr);
+    else rect_slice_kernel<5><<<grid, STHREADS, 0, s>>>(d, tile_start, n, ntiles, nullptr, 0, 0, nullptr, nullptr);
     g_launches += 2;
 }
 

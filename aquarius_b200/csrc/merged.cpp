@@ -162,6 +162,7 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
             }
         }
     }
+    const size_t launch0 = run.launches.size();
     for (const Grid& gr : grids) {
         const std::vector<int>& js = gr.js;
         const std::vector<int>& R = gr.R;
@@ -288,6 +289,7 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
                 d.k0 = koff[k];
                 d.kc = g.a_kcontig ? 1 : 0;
                 d.tiles_r = (g.M + 31) / 32;
+                mp->srcA.push_back({&g.hAm, &g.hAk});
                 tsA.push_back(mp->tilesA);
                 mp->tilesA += (int64_t)d.tiles_r * ((g.K + 63) / 64);
                 A.push_back(d);
@@ -307,6 +309,7 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
                 d.kc = g.b_kcontig ? 1 : 0;
                 d.tiles_r = (g.N + 31) / 32;
                 d.mul = ratio[k];
+                mp->srcB.push_back({&g.hBn, &g.hBk});
                 tsB.push_back(mp->tilesB);
                 mp->tilesB += (int64_t)d.tiles_r * ((g.K + 63) / 64);
                 B.push_back(d);
@@ -381,6 +384,9 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
             }
             merged_cache_bytes += mp->cache_bytes;
         }
+        for (int j : js) mp->self_read |= G(j).tA == G(j).tC || G(j).tB == G(j).tC;
+        mp->hA = A;
+        mp->hB = B;
         mp->nA = (int)A.size();
         mp->nB = (int)B.size();
         mp->dA = (kern::RectDesc*)dmalloc(A.size() * sizeof(kern::RectDesc));
@@ -427,6 +433,154 @@ void Context::build_merged(Plan& p, GemmRun& run, int first, int end, std::vecto
         l.flops = flops;
         run.launches.push_back(l);
     }
+    batch_merged_slicing(run, launch0);
+    for (size_t li = launch0; li < run.launches.size(); li++)
+        if (MergedProduct* m = run.launches[li].merged.get()) {   // build-time copies
+            m->hA.clear();
+            m->hB.clear();
+            m->srcA.clear();
+            m->srcB.clear();
+        }
+}
+
+// The operands of a statement's merged products that are not cached (amplitudes and
+// intermediates) are sliced by ONE rowmax and ONE slice launch for all of them, each into
+// its own operand buffer, before the first merged GEMM: per product, slicing its two
+// operands took four memsets and four launches around a GEMM of a fraction of a
+// millisecond (the D2h ring statement has about 300 merged products).  The buffers keep
+// five slice planes, zero outside the rectangles (zeroed once here: the rectangles cover
+// every row and k below the product's extents, and only they are written).  Skipped when
+// an operand is the statement's output or the buffers would take more than a quarter of
+// the free device memory (CCSD_MERGED_BATCH=0: never).
+void Context::batch_merged_slicing(GemmRun& run, size_t launch0) {
+    const char* env = std::getenv("CCSD_MERGED_BATCH");
+    if (env && env[0] == '0') return;
+    struct Dest {
+        MergedProduct* m;
+        bool a;
+        int rows_p, kpad;
+        int64_t soff, roff;
+    };
+    std::vector<Dest> ds;
+    int64_t slice_bytes = 0, aux_rows = 0;
+    // merged operands with the same rectangles (same tensor, positions, tables and factors)
+    // are sliced once and shared
+    auto same = [](const MergedProduct& x, bool xa, const MergedProduct& y, bool ya) {
+        const auto& rx = xa ? x.hA : x.hB;
+        const auto& ry = ya ? y.hA : y.hB;
+        const auto& sx = xa ? x.srcA : x.srcB;
+        const auto& sy = ya ? y.srcA : y.srcB;
+        if (rx.size() != ry.size() || (xa ? x.M : x.N) != (ya ? y.M : y.N) || x.K != y.K) return false;
+        for (size_t i = 0; i < rx.size(); i++) {
+            const kern::RectDesc &a = rx[i], &b = ry[i];
+            if (a.X != b.X || a.nrows != b.nrows || a.nk != b.nk || a.row0 != b.row0 || a.k0 != b.k0 || a.kc != b.kc ||
+                a.mul != b.mul)
+                return false;
+            if (*sx[i].first != *sy[i].first || *sx[i].second != *sy[i].second) return false;
+        }
+        return true;
+    };
+    auto digest = [](const MergedProduct& x, bool xa) {
+        const auto& rx = xa ? x.hA : x.hB;
+        const auto& sx = xa ? x.srcA : x.srcB;
+        uint64_t h = 1469598103934665603ull;
+        auto mix = [&](uint64_t v) { h = (h ^ v) * 1099511628211ull; };
+        for (size_t i = 0; i < rx.size(); i++) {
+            mix((uint64_t)(uintptr_t)rx[i].X);
+            mix((uint64_t)rx[i].row0 << 32 | (uint32_t)rx[i].k0);
+            mix((uint64_t)rx[i].nrows << 32 | (uint32_t)rx[i].nk);
+            for (int64_t v : *sx[i].first) mix((uint64_t)v);
+            for (int64_t v : *sx[i].second) mix((uint64_t)v);
+        }
+        return h;
+    };
+    std::map<uint64_t, std::vector<std::pair<MergedProduct*, bool>>> seen;
+    std::vector<std::pair<std::pair<MergedProduct*, bool>, std::pair<MergedProduct*, bool>>> shared;
+    for (size_t li = launch0; li < run.launches.size(); li++) {
+        MergedProduct* m = run.launches[li].merged.get();
+        if (!m || m->self_read) continue;
+        for (int side = 0; side < 2; side++) {
+            if (side == 0 ? m->cache_a : m->cache_b) continue;
+            auto& bucket = seen[digest(*m, side == 0)];
+            bool found = false;
+            for (auto& e : bucket)
+                if (same(*e.first, e.second, *m, side == 0)) {
+                    shared.push_back({{m, side == 0}, e});
+                    found = true;
+                    break;
+                }
+            if (found) continue;
+            bucket.push_back({m, side == 0});
+            Dest d;
+            d.m = m;
+            d.a = side == 0;
+            d.rows_p = kern::split_rows_pad(side == 0 ? m->M : m->N);
+            d.kpad = kern::split_k_pad(m->K, kern::SLICE_INT8);
+            d.soff = slice_bytes;
+            d.roff = aux_rows;
+            slice_bytes += (5ll * d.rows_p * d.kpad + 255) / 256 * 256;
+            aux_rows += d.rows_p;
+            ds.push_back(d);
+        }
+    }
+    if (ds.size() < 3 || host_only) return;
+    const int64_t aux_bytes = aux_rows * 2 * (int64_t)sizeof(double);   // scales, then row maxima
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    if ((double)(slice_bytes + aux_bytes) > 0.25 * (double)free_b) return;
+    uint8_t* sl = (uint8_t*)dmalloc(slice_bytes);
+    double* aux = (double*)dmalloc(aux_bytes);
+    CCSD_CUDA(cudaMemsetAsync(sl, 0, slice_bytes, stream));
+    CCSD_CUDA(cudaMemsetAsync(aux, 0, aux_bytes, stream));
+    unsigned long long* rmax = reinterpret_cast<unsigned long long*>(aux + aux_rows);
+    std::vector<kern::RectDesc> rects;
+    std::vector<int64_t> ts;
+    int64_t tiles = 0;
+    for (const Dest& d : ds) {
+        kern::SlicedOperand v;
+        v.data = sl + d.soff;
+        v.scale = aux + d.roff;
+        v.rowmax = reinterpret_cast<double*>(rmax + d.roff);
+        v.rows = d.rows_p;
+        v.kpad = d.kpad;
+        v.kind = kern::SLICE_INT8;
+        v.bytes = 5ll * d.rows_p * d.kpad;
+        for (kern::RectDesc r : d.a ? d.m->hA : d.m->hB) {
+            r.out = v.data;
+            r.scale = v.scale;
+            r.rowmax = rmax + d.roff;
+            r.rows_p = d.rows_p;
+            r.kpad = d.kpad;
+            ts.push_back(tiles);
+            tiles += (int64_t)r.tiles_r * ((r.nk + 63) / 64);
+            rects.push_back(r);
+        }
+        (d.a ? d.m->batched_a : d.m->batched_b) = true;
+        (d.a ? d.m->pa : d.m->pb) = v;
+    }
+    for (auto& sh : shared) {   // the operands sliced once for several products
+        const kern::SlicedOperand& v = sh.second.second ? sh.second.first->pa : sh.second.first->pb;
+        (sh.first.second ? sh.first.first->batched_a : sh.first.first->batched_b) = true;
+        (sh.first.second ? sh.first.first->pa : sh.first.first->pb) = v;
+    }
+    GemmLaunch l;
+    l.kind = GemmLaunch::MERGED_SLICE;
+    l.gemm = run.launches[launch0].merged->first_gemm;   // the statement's slice count
+    l.nprob = (int)rects.size();
+    l.chunks = tiles;
+    l.desc_bytes = rects.size() * sizeof(kern::RectDesc);
+    l.d_desc = dmalloc(l.desc_bytes);
+    l.d_chunks = (int64_t*)dmalloc(ts.size() * sizeof(int64_t));
+    stage_h2d(l.d_desc, rects.data(), l.desc_bytes);
+    stage_h2d(l.d_chunks, ts.data(), ts.size() * sizeof(int64_t));
+    l.arena = sl;
+    l.arena_bytes = slice_bytes;
+    l.aux = aux;
+    l.aux_bytes = aux_bytes;
+    run.launches.insert(run.launches.begin() + launch0, l);
 }
 
 void Context::run_merged(Plan& p, MergedProduct& m, const std::string& label) {
@@ -442,6 +596,11 @@ void Context::run_merged(Plan& p, MergedProduct& m, const std::string& label) {
         prof_end(ev, label + " {merged:" + name + "}", 0.0);
     };
     auto operand = [&](bool is_a) {
+        if (is_a ? m.batched_a : m.batched_b) {   // sliced by the statement's batched launch
+            kern::SlicedOperand v = is_a ? m.pa : m.pb;
+            v.nslices = ns;
+            return v;
+        }
         const int rows = is_a ? m.M : m.N;
         const kern::RectDesc* d = is_a ? m.dA : m.dB;
         const int64_t* ts = is_a ? m.dA_ts : m.dB_ts;
