@@ -180,13 +180,15 @@ typedef struct {
     int    diis_start;    /* default 1     (ccsd.cxx:279-280) */
     double diis_damping;  /* default 0.0   (ccsd.cxx:277-278) */
     int    precision;     /* CCSD_PREC_FP64, CCSD_PREC_SPLIT or CCSD_PREC_SPLIT_I8 */
-    int    slices;        /* split-BF16 slices per operand: 3 (0 = default) or 4 */
+    int    slices;        /* slices per operand: 3 or 4 for BF16, 3, 4 or 5 for INT8
+                             (0 = the precision's default) */
     int    use_graph;     /* capture one iteration as a CUDA graph and replay it */
     double refine_tol;    /* split precision only: once conv < refine_tol, 3-slice
-                             contractions move to 4 slices, and 4-slice ones to native
-                             FP64 if the residual then stalls (0 = never).  About
-                             1000 x conv_tol: the 3-slice floor is near 1e-9, and a
-                             switch close to it leaves DIIS a history of 3-slice noise */
+                             contractions move to 4 slices; if the residual then stalls,
+                             INT8 moves on to 5 slices and then to native FP64 (BF16 from
+                             4 slices to FP64) (0 = never).  10 to 1000 x conv_tol, above
+                             the 3-slice floor (near 1e-9 for BF16, 4e-7 for INT8 at
+                             o=32 v=256); DIIS restarts at every switch */
     double autotune_de;   /* split precision only, > 0: slice count per contraction.  On
                              the first iteration run at 4 or more slices, every statement
                              with split contractions is evaluated once with one slice
